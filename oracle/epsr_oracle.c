@@ -1,0 +1,955 @@
+/*
+ * epsr_oracle.c -- CPU restatement of the EPSR minimum-image pair path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the device path is compared with; it is
+ * never linked into, called by or shipped with the product library.  Only the tests, the
+ * smoke check and the CPU-baseline leg of the benchmark load it.
+ *
+ * Each routine restates the reference translation (IzzyRodger-edb/EPSR_python_translation,
+ * package src/epsr26) statement by statement in float32, with the same operation order.
+ * The reference evaluates every `real` as a NumPy float32 scalar with no fused
+ * multiply-add and calls glibc libm (expf/sinf/cosf/powf) through ctypes; this file is
+ * compiled with -ffp-contract=off and calls the same glibc functions, so on the same
+ * machine its results are bit-identical to the reference's.  Parity is pinned by the
+ * golden vectors under tests/golden, produced by running the reference itself.
+ *
+ * Indexing: molecules, atoms, types and pairs are 0-based; the r-grid index iz and the
+ * Q index keep the reference's 1-based meaning (tables are stored [pair][ld] with iz in
+ * 1..npt, element 0 unused), because the bin arithmetic `ifix(d/stepcl)+2` depends on it.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ Fortran intrinsics */
+
+/* nint: round half away from zero (fortran/fmath.py:222-236, gfortran lroundf). */
+static inline int32_t f_nint(float x) {
+    if (!(x >= -2147483648.0f && x < 2147483648.0f)) return 0;
+    double t = trunc((double)x);
+    double fr = (double)x - t;
+    if (fr >= 0.5) t += 1.0;
+    else if (fr <= -0.5) t -= 1.0;
+    return (int32_t)(int64_t)t;
+}
+
+/* ifix: truncation toward zero; out of range -> INT_MIN (fortran/fmath.py:245-253). */
+static inline int32_t f_ifix(float x) {
+    if (!(x > -2147483649.0f && x < 2147483648.0f)) return INT32_MIN;
+    return (int32_t)x;
+}
+
+/* sign(a,b) for reals: |a| with the sign of b (fortran/fmath.py:284). */
+static inline float f_sign(float a, float b) { return copysignf(fabsf(a), b); }
+
+/* ------------------------------------------------------------------ ran1 */
+/* auxiliary_routines.py:324-391; constants common/ran1com.py:13-21. */
+typedef struct {
+    int32_t idum, iy, mcall;
+    int32_t iv[32];
+} oracle_ran1_state;
+
+#define R_IA 16807
+#define R_IM 2147483647
+#define R_IQ 127773
+#define R_IR 2836
+#define R_NTAB 32
+#define R_NDIV 67108864
+
+float oracle_ran1(oracle_ran1_state *s) {
+    const float am = 4.656612873077393e-10f;   /* f32(1/IM) */
+    const float rnmx = 0.9999998807907104f;    /* f32(1 - 1.2e-7) */
+    int32_t idum = s->idum, iy = s->iy;
+    if (idum <= 0 || iy == 0) {
+        int64_t neg = -(int64_t)idum;
+        int32_t w = (int32_t)(uint32_t)(uint64_t)neg;   /* wrap32 */
+        idum = w > 1 ? w : 1;
+        for (int j = R_NTAB + 8; j >= 1; --j) {
+            int32_t k = idum / R_IQ;
+            idum = R_IA * (idum - k * R_IQ) - R_IR * k;
+            if (idum < 0) idum += R_IM;
+            if (j <= R_NTAB) s->iv[j - 1] = idum;
+        }
+        iy = s->iv[0];
+    }
+    int32_t k = idum / R_IQ;
+    idum = R_IA * (idum - k * R_IQ) - R_IR * k;
+    if (idum < 0) idum += R_IM;
+    int32_t j = iy / R_NDIV;                /* 0-based slot (1 + iy/NDIV in 1-based) */
+    iy = s->iv[j];
+    s->iv[j] = idum;
+    float r = am * (float)iy;
+    if (rnmx < r) r = rnmx;
+    s->idum = idum;
+    s->iy = iy;
+    s->mcall = (int32_t)((uint32_t)s->mcall + 1u);
+    return r;
+}
+
+void oracle_ran1_fill(oracle_ran1_state *s, float *out, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) out[i] = oracle_ran1(s);
+}
+
+/* ------------------------------------------------------------------ system description */
+typedef struct {
+    int32_t nmol, natom, ntype, npairs, nmoltype;
+    const int32_t *naf, *nato, *mtype, *itype; /* 0-based */
+    float *xa, *ya, *za;                       /* atom offsets (box units) */
+    float *xadd, *yadd, *zadd;                 /* molecule centres (box units) */
+    const int32_t *npairref;                   /* [ntype*ntype] 0-based pair index */
+    const float *xstar;                        /* [ld], 1-based */
+    const float *xavs, *xavs1, *ecoul, *ecoul1;/* [npairs*ld] */
+    int32_t ld, npt2;
+    float stepcl;
+    int32_t cubic;
+    float lat[6]; /* alatx, blatx, clatx, blaty, claty, clatz (box units) */
+} oracle_sys;
+
+/* minimagec.py:13-62 */
+static inline void minimagec(const oracle_sys *S, float *x, float *y, float *z) {
+    if (S->cubic) {
+        *z = *z - (float)f_nint(*z);
+        *y = *y - (float)f_nint(*y);
+        *x = *x - (float)f_nint(*x);
+        return;
+    }
+    const float alatx = S->lat[0], blatx = S->lat[1], clatx = S->lat[2];
+    const float blaty = S->lat[3], claty = S->lat[4], clatz = S->lat[5];
+    float fc = *z / clatz;
+    float fb = (*y - fc * claty) / blaty;
+    float fa = (*x - fb * blatx - fc * clatx) / alatx;
+    fc = fc - (float)f_nint(fc);
+    fb = fb - (float)f_nint(fb);
+    fa = fa - (float)f_nint(fa);
+    *z = fc * clatz;
+    *y = fb * blaty + fc * claty;
+    *x = fa * alatx + fb * blatx + fc * clatx;
+}
+
+/* en_atom_inter_scale molfit.py:1251-1279 with scalefac = 1 (no coarse graining). */
+static inline float en_atom_inter(const oracle_sys *S, float x1, float y1, float z1, float x2, float y2,
+                                  float z2, int icref) {
+    float sume = 0.0f;
+    float xd = x2 - x1, yd = y2 - y1, zd = z2 - z1;
+    minimagec(S, &xd, &yd, &zd);
+    float dsq = xd * xd + yd * yd + zd * zd;
+    float dtest = sqrtf(dsq);
+    float rat = dtest / S->stepcl;
+    int32_t iz = f_ifix(rat) + 2;
+    const size_t base = (size_t)icref * (size_t)S->ld;
+    if (iz <= S->npt2) {
+        float dtdif = dtest - S->xstar[iz];
+        sume = S->xavs[base + iz] + S->xavs1[base + iz] * dtdif;
+    }
+    dtest = dtest * 1.0f;
+    rat = dtest / S->stepcl;
+    iz = f_ifix(rat) + 2;
+    if (iz <= S->npt2) {
+        float dtdif = dtest - S->xstar[iz];
+        sume = sume + S->ecoul[base + iz] + S->ecoul1[base + iz] * dtdif;
+    }
+    return sume;
+}
+
+/* en_mole_pair molfit.py:1528-1578 (no tethering, no coordination constraints). */
+float oracle_en_mole_pair(const oracle_sys *S, int im, int jm) {
+    float sume = 0.0f;
+    const int a0 = S->naf[im], a1 = a0 + S->nato[im];
+    const int b0 = S->naf[jm], b1 = b0 + S->nato[jm];
+    for (int ia = a0; ia < a1; ++ia) {
+        const int it = S->itype[ia];
+        const float x1 = S->xa[ia] + S->xadd[im];
+        const float y1 = S->ya[ia] + S->yadd[im];
+        const float z1 = S->za[ia] + S->zadd[im];
+        for (int ja = b0; ja < b1; ++ja) {
+            const int icref = S->npairref[it * S->ntype + S->itype[ja]];
+            const float x2 = S->xa[ja] + S->xadd[jm];
+            const float y2 = S->ya[ja] + S->yadd[jm];
+            const float z2 = S->za[ja] + S->zadd[jm];
+            sume = sume + en_atom_inter(S, x1, y1, z1, x2, y2, z2, icref);
+        }
+    }
+    return sume;
+}
+
+/* ------------------------------------------------------------------ cell list */
+/* cellneighbourlist.py:23-90 (initialise), :97-183 (makecellneighbourlist),
+ * :266-305 (findperiodiccell, cellcoord, atomcellno). Lattice in box units. */
+typedef struct {
+    int32_t ncelldiva, ncelldivb, ncelldivc, ncell, ncellneighb, maxcellno;
+    int32_t *molcellno;   /* [nmol] 1-based cell number */
+    int32_t *cell_start;  /* [ncell+1] CSR offsets (0-based cell index) */
+    int32_t *cell_mols;   /* [nmol] molecules (0-based) in reference order */
+    int32_t *ia_off, *ib_off, *ic_off; /* [ncellneighb] */
+} oracle_cells;
+
+static int cellcoord(float x, int ncelldiv) {
+    float x1 = x - (float)f_nint(x);
+    int ix = f_ifix((x1 + 0.5f) * (float)ncelldiv);
+    while (ix < 0) ix += ncelldiv;
+    while (ix >= ncelldiv) ix -= ncelldiv;
+    return ix;
+}
+
+static int atomcellno(const float *lat, int na, int nb, int nc, float x, float y, float z) {
+    const float alatx = lat[0], blatx = lat[1], clatx = lat[2];
+    const float blaty = lat[3], claty = lat[4], clatz = lat[5];
+    float fc = z / clatz;
+    float fb = (y - fc * claty) / blaty;
+    float fa = (x - fb * blatx - fc * clatx) / alatx;
+    int ia = cellcoord(fa, na), ib = cellcoord(fb, nb), ic = cellcoord(fc, nc);
+    return 1 + ia + na * (ib + nb * ic);
+}
+
+/* First pass: sizes.  Writes ncelldiv*, ncell.  Returns 0. */
+int oracle_cell_dims(int nmolcellin, int nmol, const float *lat, int32_t *dims /* [4] */) {
+    int nmolcell = nmolcellin > nmol ? nmol : nmolcellin;
+    /* ncelldiv = nint(powf(f32(nmol)/f32(nmolcell), 1/3)) */
+    float ratio = (float)nmol / (float)nmolcell;
+    int ncelldiv = f_nint(powf(ratio, 1.0f / 3.0f));
+    if (ncelldiv < 1) ncelldiv = 1;
+    float mn = lat[0];
+    if (lat[3] < mn) mn = lat[3];
+    if (lat[5] < mn) mn = lat[5];
+    /* Python min(alatx, blaty, clatz) returns the first minimal value */
+    float cellsize = 2.0f * mn / (float)ncelldiv;
+    dims[0] = 2 * f_ifix(lat[0] / cellsize) + 1;
+    dims[1] = 2 * f_ifix(lat[3] / cellsize) + 1;
+    dims[2] = 2 * f_ifix(lat[5] / cellsize) + 1;
+    dims[3] = dims[0] * dims[1] * dims[2];
+    return 0;
+}
+
+/* Second pass.  lat9 = alatc[3], blatc[3], clatc[3]. Offsets arrays must hold ncell. */
+int oracle_cell_list(int nmolcellin, const float *xadd, const float *yadd, const float *zadd, int nmol,
+                     float rmax, const float *lat, const float *lat9, oracle_cells *C) {
+    int32_t dims[4];
+    oracle_cell_dims(nmolcellin, nmol, lat, dims);
+    C->ncelldiva = dims[0];
+    C->ncelldivb = dims[1];
+    C->ncelldivc = dims[2];
+    C->ncell = dims[3];
+    const int ncell = C->ncell;
+    int32_t *count = (int32_t *)calloc((size_t)ncell, sizeof(int32_t));
+    int maxc = 0;
+    for (int im = 0; im < nmol; ++im) {
+        int c = atomcellno(lat, dims[0], dims[1], dims[2], xadd[im], yadd[im], zadd[im]);
+        C->molcellno[im] = c;
+        count[c - 1]++;
+        if (count[c - 1] > maxc) maxc = count[c - 1];
+    }
+    C->maxcellno = maxc;
+    C->cell_start[0] = 0;
+    for (int c = 0; c < ncell; ++c) C->cell_start[c + 1] = C->cell_start[c] + count[c];
+    memset(count, 0, sizeof(int32_t) * (size_t)ncell);
+    for (int im = 0; im < nmol; ++im) {
+        int c = C->molcellno[im] - 1;
+        C->cell_mols[C->cell_start[c] + count[c]] = im;
+        count[c]++;
+    }
+    free(count);
+    /* makecellneighbourlist (cellneighbourlist.py:97-183) */
+    const float *alatc = lat9, *blatc = lat9 + 3, *clatc = lat9 + 6;
+    float cella = 1.0f / (float)C->ncelldiva, cellb = 1.0f / (float)C->ncelldivb,
+          cellc = 1.0f / (float)C->ncelldivc;
+    float cella2 = 0.5f * cella, cellb2 = 0.5f * cellb, cellc2 = 0.5f * cellc;
+    float xc[8], yc[8], zc[8];
+    int nf = 0;
+    for (int ic = -1; ic <= 1; ic += 2) {
+        float cx = (float)ic * cellc2 * clatc[0], cy = (float)ic * cellc2 * clatc[1],
+              cz = (float)ic * cellc2 * clatc[2];
+        for (int ib = -1; ib <= 1; ib += 2) {
+            float bx = (float)ib * cellb2 * blatc[0], by = (float)ib * cellb2 * blatc[1],
+                  bz = (float)ib * cellb2 * blatc[2];
+            for (int ia = -1; ia <= 1; ia += 2) {
+                float ax = (float)ia * cella2 * alatc[0], ay = (float)ia * cella2 * alatc[1],
+                      az = (float)ia * cella2 * alatc[2];
+                xc[nf] = ax + bx + cx;
+                yc[nf] = ay + by + cy;
+                zc[nf] = az + bz + cz;
+                nf++;
+            }
+        }
+    }
+    int nra = (C->ncelldiva - 1) / 2, nrb = (C->ncelldivb - 1) / 2, nrc = (C->ncelldivc - 1) / 2;
+    float rmaxsq = rmax * rmax;
+    int found_n = 0;
+    for (int ic = -nrc; ic <= nrc; ++ic) {
+        float cx = (float)ic * cellc * clatc[0], cy = (float)ic * cellc * clatc[1], cz = (float)ic * cellc * clatc[2];
+        for (int ib = -nrb; ib <= nrb; ++ib) {
+            float bx = (float)ib * cellb * blatc[0], by = (float)ib * cellb * blatc[1],
+                  bz = (float)ib * cellb * blatc[2];
+            for (int ia = -nra; ia <= nra; ++ia) {
+                float ax = (float)ia * cella * alatc[0], ay = (float)ia * cella * alatc[1],
+                      az = (float)ia * cella * alatc[2];
+                float xdc = ax + bx + cx, ydc = ay + by + cy, zdc = az + bz + cz;
+                int found = 0;
+                for (int f1 = 0; f1 < 8 && !found; ++f1)
+                    for (int f2 = 0; f2 < 8 && !found; ++f2) {
+                        float xd = xdc + xc[f1] - xc[f2];
+                        float yd = ydc + yc[f1] - yc[f2];
+                        float zd = zdc + zc[f1] - zc[f2];
+                        float r2 = xd * xd + yd * yd + zd * zd;
+                        found = (r2 < rmaxsq) || (ia == 0 && ib == 0 && ic == 0);
+                    }
+                if (found) {
+                    C->ia_off[found_n] = ia;
+                    C->ib_off[found_n] = ib;
+                    C->ic_off[found_n] = ic;
+                    found_n++;
+                }
+            }
+        }
+    }
+    C->ncellneighb = found_n;
+    return 0;
+}
+
+static inline int fold(int x, int n) {
+    while (x < 0) x += n;
+    while (x >= n) x -= n;
+    return x;
+}
+
+/* make_neighbour_list_from_cells cellneighbourlist.py:187-207 (0-based cell ic). */
+int oracle_region(const oracle_cells *C, int ic, int32_t *nbref) {
+    int c0 = ic;
+    int icc = c0 / (C->ncelldiva * C->ncelldivb);
+    int ibb = (c0 - icc * C->ncelldiva * C->ncelldivb) / C->ncelldiva;
+    int iaa = c0 - C->ncelldiva * (ibb + C->ncelldivb * icc);
+    int n = 0;
+    for (int k = 0; k < C->ncellneighb; ++k) {
+        int a = fold(iaa + C->ia_off[k], C->ncelldiva);
+        int b = fold(ibb + C->ib_off[k], C->ncelldivb);
+        int c = fold(icc + C->ic_off[k], C->ncelldivc);
+        int cell = a + C->ncelldiva * (b + C->ncelldivb * c);
+        for (int p = C->cell_start[cell]; p < C->cell_start[cell + 1]; ++p) nbref[n++] = C->cell_mols[p];
+    }
+    return n;
+}
+
+/* get_nnbrefmax cellneighbourlist.py:211-233 */
+int oracle_nnbrefmax(const oracle_cells *C) {
+    int mx = 0;
+    for (int ic = 0; ic < C->ncell; ++ic) {
+        int c0 = ic;
+        int icc = c0 / (C->ncelldiva * C->ncelldivb);
+        int ibb = (c0 - icc * C->ncelldiva * C->ncelldivb) / C->ncelldiva;
+        int iaa = c0 - C->ncelldiva * (ibb + C->ncelldivb * icc);
+        int n = 0;
+        for (int k = 0; k < C->ncellneighb; ++k) {
+            int a = fold(iaa + C->ia_off[k], C->ncelldiva);
+            int b = fold(ibb + C->ib_off[k], C->ncelldivb);
+            int c = fold(icc + C->ic_off[k], C->ncelldivc);
+            int cell = a + C->ncelldiva * (b + C->ncelldivb * c);
+            n += C->cell_start[cell + 1] - C->cell_start[cell];
+        }
+        if (n > mx) mx = n;
+    }
+    return mx;
+}
+
+/* ------------------------------------------------------------------ pair-energy store */
+/* ergpairreference.py:63-126 (initialise_ergpair, set_ergpair), fmolec1
+ * ato_manipulation_rev4.py:2374-2528.  Store layout: molergpair/ergpairref [nmol][nnbrefmax]
+ * (slot-major per molecule, 0-based slots), ergpair[] 0-based values, refs 1-based as in
+ * the reference (ergpairref value k means ergpair[k-1]). */
+typedef struct {
+    int32_t nnbrefmax, nergpair, nergpairmax;
+    int32_t *nergpairm;  /* [nmol] */
+    int32_t *molergpair; /* [nmol*nnbrefmax], partner molecule (0-based) */
+    int32_t *ergpairref; /* [nmol*nnbrefmax], 1-based index into ergpair */
+    float *ergpair;      /* [nergpairmax] */
+} oracle_store;
+
+static void set_ergpair(oracle_store *E, int im, int jm, float energy) {
+    const int M = E->nnbrefmax;
+    if (E->nergpairm[im] < M && E->nergpairm[jm] < M && energy != 0.0f) {
+        E->nergpair++;
+        if (E->nergpair > E->nergpairmax) return; /* caller sizes the store; checked after */
+        E->ergpair[E->nergpair - 1] = energy;
+        if (jm == im) {
+            E->nergpairm[im] = 1;
+            E->molergpair[(size_t)im * M + 0] = im;
+            E->ergpairref[(size_t)im * M + 0] = E->nergpair;
+        } else {
+            E->nergpairm[im]++;
+            E->nergpairm[jm]++;
+            E->molergpair[(size_t)im * M + E->nergpairm[im] - 1] = jm;
+            E->molergpair[(size_t)jm * M + E->nergpairm[jm] - 1] = im;
+            E->ergpairref[(size_t)im * M + E->nergpairm[im] - 1] = E->nergpair;
+            E->ergpairref[(size_t)jm * M + E->nergpairm[jm] - 1] = E->nergpair;
+        }
+    }
+}
+
+/* fmolec1: eintra[] are the en_mole_intra values (an input).  out2 = {ftest, ftestb}
+ * (per molecule, as returned).  Returns 0, or 1 when ergpair capacity was exceeded. */
+int oracle_fmolec1(const oracle_sys *S, const oracle_cells *C, const float *eintra, oracle_store *E,
+                   float *out2) {
+    const int nmol = S->nmol;
+    const int M = E->nnbrefmax;
+    E->nergpair = 0;
+    for (int im = 0; im < nmol; ++im) E->nergpairm[im] = 0;
+    float ftest = 0.0f, ftestb = 0.0f;
+    for (int im = 0; im < nmol; ++im) {
+        float e = eintra[im];
+        ftestb = ftestb + e;
+        set_ergpair(E, im, im, e);
+    }
+    int32_t *nbref = (int32_t *)malloc(sizeof(int32_t) * (size_t)(M > 0 ? M : 1));
+    float *ergold = (float *)malloc(sizeof(float) * (size_t)(M > 0 ? M : 1));
+    for (int ic = 0; ic < C->ncell; ++ic) {
+        if (C->cell_start[ic + 1] - C->cell_start[ic] <= 0) continue;
+        int nn = oracle_region(C, ic, nbref);
+        for (int p = C->cell_start[ic]; p < C->cell_start[ic + 1]; ++p) {
+            int im = C->cell_mols[p];
+            for (int inn = 0; inn < nn; ++inn) {
+                int jm = nbref[inn];
+                ergold[inn] = 0.0f;
+                if (jm > im) ergold[inn] = oracle_en_mole_pair(S, im, jm);
+            }
+            /* the store loop starts at the second neighbour (ato_manipulation_rev4.py:2466-2474) */
+            for (int inn = 1; inn < nn; ++inn) {
+                int jm = nbref[inn];
+                if (ergold[inn] != 0.0f && jm > im) {
+                    set_ergpair(E, im, jm, ergold[inn]);
+                    ftest = ftest + ergold[inn];
+                }
+            }
+        }
+    }
+    free(nbref);
+    free(ergold);
+    out2[0] = ftest / (float)nmol;
+    out2[1] = ftestb / (float)nmol;
+    return E->nergpair > E->nergpairmax ? 1 : 0;
+}
+
+/* ------------------------------------------------------------------ molfit sweep */
+typedef struct {
+    float simt, rejrate, stepr, stepm, trstepmax, trstepmin;
+    int32_t ireset;
+    float *wholerot, *wholetrans;      /* [nmoltype] */
+    int32_t *nwhole, *nmovem;          /* [2*nmoltype]: [0..nmt) tries, [nmt..2nmt) rejections */
+    int32_t *nstepreject;              /* [nmol] */
+    float *internrot, *interntrans;    /* [nmoltype] */
+    const int32_t *ngrot;              /* [nmol] (0 here) */
+} oracle_mcpar;
+
+typedef struct {
+    int32_t nmoves;
+    int32_t *im;     /* [nmol] */
+    float *den;      /* [nmol] en_change value */
+    int32_t *acc;    /* [nmol] */
+    float *cosv;     /* [3*nmol] cos values used (glibc cosf), or NULL */
+    int32_t ncos;
+} oracle_trace;
+
+static float en_change(const oracle_sys *S, int im, const oracle_store *E, float *ergnew) {
+    const int M = E->nnbrefmax;
+    const int nn = E->nergpairm[im];
+    const int32_t *nb = E->molergpair + (size_t)im * M;
+    const int32_t *rf = E->ergpairref + (size_t)im * M;
+    for (int inn = 1; inn < nn; ++inn) ergnew[inn] = 0.0f;
+    for (int inn = 1; inn < nn; ++inn) {
+        int jm = nb[inn];
+        float sume = oracle_en_mole_pair(S, im, jm);
+        ergnew[inn] = ergnew[inn] + sume;
+    }
+    float fdiff = 0.0f;
+    for (int inn = 1; inn < nn; ++inn) fdiff = fdiff + ergnew[inn] - E->ergpair[rf[inn] - 1];
+    return fdiff;
+}
+
+/* rotatm molfit.py:672-711 */
+static void rotatm(oracle_sys *S, int im, float stepsz, oracle_ran1_state *R, oracle_trace *T) {
+    const float pi = 3.14159265358979323846f; /* f32(math.pi) */
+    const int a0 = S->naf[im], a1 = a0 + S->nato[im];
+    if (a1 - 1 > a0) {
+        float phi, cphi, sphi;
+        phi = pi * stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+        cphi = cosf(phi);
+        if (T && T->cosv) T->cosv[T->ncos++] = cphi;
+        sphi = f_sign(sqrtf(1.0f - cphi * cphi), phi);
+        for (int ia = a0; ia < a1; ++ia) {
+            float xs = S->xa[ia] * cphi - S->ya[ia] * sphi;
+            S->ya[ia] = S->xa[ia] * sphi + S->ya[ia] * cphi;
+            S->xa[ia] = xs;
+        }
+        phi = pi * stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+        cphi = cosf(phi);
+        if (T && T->cosv) T->cosv[T->ncos++] = cphi;
+        sphi = f_sign(sqrtf(1.0f - cphi * cphi), phi);
+        for (int ia = a0; ia < a1; ++ia) {
+            float zs = S->za[ia] * cphi - S->xa[ia] * sphi;
+            S->xa[ia] = S->za[ia] * sphi + S->xa[ia] * cphi;
+            S->za[ia] = zs;
+        }
+        phi = pi * stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+        cphi = cosf(phi);
+        if (T && T->cosv) T->cosv[T->ncos++] = cphi;
+        sphi = f_sign(sqrtf(1.0f - cphi * cphi), phi);
+        for (int ia = a0; ia < a1; ++ia) {
+            float ys = S->ya[ia] * cphi - S->za[ia] * sphi;
+            S->za[ia] = S->ya[ia] * sphi + S->za[ia] * cphi;
+            S->ya[ia] = ys;
+        }
+    }
+}
+
+/* movem molfit.py:733-759 (the step is doubled until the position changes). */
+static float movem(oracle_sys *S, int im, float stepsz, oracle_ran1_state *R) {
+    float xs = S->xadd[im], ys = S->yadd[im], zs = S->zadd[im];
+    S->zadd[im] = S->zadd[im] + stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+    S->yadd[im] = S->yadd[im] + stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+    S->xadd[im] = S->xadd[im] + stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+    int nochange = xs == S->xadd[im] && ys == S->yadd[im] && zs == S->zadd[im];
+    while (nochange) {
+        stepsz = stepsz * 2.0f;
+        S->zadd[im] = S->zadd[im] + stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+        S->yadd[im] = S->yadd[im] + stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+        S->xadd[im] = S->xadd[im] + stepsz * (2.0f * oracle_ran1(R) - 1.0f);
+        nochange = xs == S->xadd[im] && ys == S->yadd[im] && zs == S->zadd[im];
+    }
+    return stepsz;
+}
+
+/* One molfit cycle, whole-molecule branch (molfit.py:268-448) plus step adaptation
+ * (:465-536).  fadds is updated in place (molfit.py:538).  Returns 0. */
+int oracle_molfit(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_mcpar *P,
+                  oracle_ran1_state *R, float *fadds, oracle_trace *T) {
+    const int nmt = S->nmoltype;
+    const float temp = 1.0f / P->simt;
+    const float rotstepmax = 1.0f, rotstepmin = 1.0e-5f;
+    for (int k = 0; k < 2 * nmt; ++k) { P->nwhole[k] = 0; P->nmovem[k] = 0; }
+    float fadd = 0.0f;
+    const int M = E->nnbrefmax;
+    float *ergnew = (float *)malloc(sizeof(float) * (size_t)(M > 0 ? M : 1));
+    float xr[4096], yr[4096], zr[4096];
+    if (T) { T->nmoves = 0; T->ncos = 0; }
+    for (int ic = 0; ic < C->ncell; ++ic) {
+        for (int p = C->cell_start[ic]; p < C->cell_start[ic + 1]; ++p) {
+            const int im = C->cell_mols[p];
+            const int n = S->nato[im];
+            const int mt = S->mtype[im];
+            if (P->ngrot[im] == 0) P->internrot[mt] = 0.0f;
+            const int a0 = S->naf[im];
+            for (int k = 0; k < n; ++k) { xr[k] = S->xa[a0 + k]; yr[k] = S->ya[a0 + k]; zr[k] = S->za[a0 + k]; }
+            const float xs = S->xadd[im], ys = S->yadd[im], zs = S->zadd[im];
+            if (P->stepr > 0.0f && n > 1) {
+                if (P->wholerot[mt] <= 0.0f) P->wholerot[mt] = rotstepmin;
+                P->nwhole[mt]++;
+                rotatm(S, im, P->wholerot[mt], R, T);
+            } else {
+                P->wholerot[mt] = 0.0f;
+            }
+            if (P->stepm > 0.0f) {
+                if (P->wholetrans[mt] <= 0.0f) P->wholetrans[mt] = P->trstepmin;
+                P->nmovem[mt]++;
+                P->wholetrans[mt] = movem(S, im, P->wholetrans[mt], R);
+            } else {
+                P->wholetrans[mt] = 0.0f;
+            }
+            float fdiff = en_change(S, im, E, ergnew);
+            float ediff = (fdiff + 0.0f) * temp;
+            float etest;
+            if (ediff <= 0.0f) etest = 10.0f;
+            else if (ediff < 20.0f) etest = expf(-ediff);
+            else etest = 0.0f;
+            int acc = oracle_ran1(R) < etest;
+            if (acc) {
+                P->nstepreject[im] = 0;
+                fadd = fadd + fdiff;
+                const int32_t *rf = E->ergpairref + (size_t)im * M;
+                for (int inn = 1; inn < E->nergpairm[im]; ++inn) E->ergpair[rf[inn] - 1] = ergnew[inn];
+            } else {
+                P->nstepreject[im]++;
+                for (int k = 0; k < n; ++k) { S->xa[a0 + k] = xr[k]; S->ya[a0 + k] = yr[k]; S->za[a0 + k] = zr[k]; }
+                S->xadd[im] = xs;
+                S->yadd[im] = ys;
+                S->zadd[im] = zs;
+                if (P->stepr > 0.0f) P->nwhole[nmt + mt]++;
+                if (P->stepm > 0.0f) P->nmovem[nmt + mt]++;
+            }
+            if (T) {
+                T->im[T->nmoves] = im;
+                T->den[T->nmoves] = fdiff;
+                T->acc[T->nmoves] = acc;
+                T->nmoves++;
+            }
+        }
+    }
+    free(ergnew);
+    if (P->ireset != 1) {
+        for (int t = 0; t < nmt; ++t) {
+            float rat;
+            /* nmovei and ninter stay 0 in this branch, so their ratio is 1.0 (molfit.py:469-497) */
+            P->interntrans[t] = P->interntrans[t] * 1.0f;
+            if (P->interntrans[t] > P->trstepmax) P->interntrans[t] = P->trstepmax;
+            if (P->interntrans[t] < P->trstepmin && P->interntrans[t] != 0.0f) P->interntrans[t] = P->trstepmin;
+            P->internrot[t] = P->internrot[t] * 1.0f;
+            if (P->internrot[t] > rotstepmax) P->internrot[t] = rotstepmax;
+            if (P->internrot[t] < rotstepmin && P->internrot[t] != 0.0f) P->internrot[t] = rotstepmin;
+            if (P->nwhole[nmt + t] > 0) {
+                rat = P->rejrate * (float)P->nwhole[t] / (float)P->nwhole[nmt + t];
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = P->nwhole[t] > 0 ? 1.1f : 1.0f;
+            }
+            P->wholerot[t] = P->wholerot[t] * rat;
+            if (P->wholerot[t] > rotstepmax) P->wholerot[t] = rotstepmax;
+            if (P->wholerot[t] < rotstepmin && P->wholerot[t] != 0.0f) P->wholerot[t] = rotstepmin;
+            if (P->nmovem[nmt + t] > 0) {
+                rat = P->rejrate * (float)P->nmovem[t] / (float)P->nmovem[nmt + t];
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = P->nmovem[t] > 0 ? 1.1f : 1.0f;
+            }
+            P->wholetrans[t] = P->wholetrans[t] * rat;
+            if (P->wholetrans[t] > P->trstepmax) P->wholetrans[t] = P->trstepmax;
+            if (P->wholetrans[t] < P->trstepmin && P->wholetrans[t] != 0.0f) P->wholetrans[t] = P->trstepmin;
+        }
+    }
+    *fadds = *fadds + fadd / (float)S->nmol;
+    return 0;
+}
+
+/* trstepmax/trstepmin of molfit.py:96-101 */
+void oracle_trsteps(int natomr, float *out2) {
+    float t = 1.0f / (float)natomr;
+    t = powf(t, 1.0f / 3.0f);
+    out2[0] = t;
+    float a = 0.0001f * t;
+    out2[1] = a > 1.0e-6f ? a : 1.0e-6f;
+    /* Python max(a, b) returns a when a >= b: same value */
+    if (!(a > 1.0e-6f) && a == 1.0e-6f) out2[1] = a;
+}
+
+/* ------------------------------------------------------------------ atogen */
+/* ato_manipulation_rev4.py:3640-3899, no coarse graining, no container forces.
+ * wav: [2][npairs][ld] (ld >= npt1+1, iz 1-based). ycoh: [ld].  rminex: [npairs].
+ * out_ngrsamples: returned value.  Returns ngrsamples. */
+int oracle_atogen(const oracle_sys *S, float *wav, float *potex, int ngrsamples, int npt1, float sizefactor,
+                  float dmax, const float *rminex, const float *cfrac, int natomr, const float *ycoh,
+                  oracle_ran1_state *R) {
+    const int nmol = S->nmol, npairs = S->npairs, ld = S->ld, ntype = S->ntype;
+    const size_t half = (size_t)npairs * (size_t)ld;
+    for (size_t i = 0; i < 2 * half; ++i) wav[i] = 0.0f;
+    for (int ic = 0; ic < npairs; ++ic) potex[ic] = 0.0f;
+    const float stepcl = S->stepcl;
+    /* intramolecular (:3696-3725) */
+    for (int im = 0; im < nmol; ++im) {
+        if (S->nato[im] > 1) {
+            const int a0 = S->naf[im], a1 = a0 + S->nato[im];
+            for (int ia = a0; ia < a1 - 1; ++ia) {
+                float x1 = S->xa[ia], y1 = S->ya[ia], z1 = S->za[ia];
+                for (int ja = ia + 1; ja < a1; ++ja) {
+                    int icref = S->npairref[S->itype[ia] * ntype + S->itype[ja]];
+                    float xx = (x1 - S->xa[ja]) * sizefactor;
+                    float yy = (y1 - S->ya[ja]) * sizefactor;
+                    float zz = (z1 - S->za[ja]) * sizefactor;
+                    minimagec(S, &xx, &yy, &zz);
+                    float dtest = sqrtf(xx * xx + yy * yy + zz * zz);
+                    int iz1 = f_nint(dtest / stepcl) + 2;
+                    if (iz1 > 1 && iz1 <= npt1) wav[(size_t)icref * ld + iz1] = wav[(size_t)icref * ld + iz1] + 2.0f;
+                }
+            }
+        }
+    }
+    /* intermolecular (:3739-3838) */
+    float *csampled = (float *)calloc((size_t)ntype, sizeof(float));
+    int *molsampled = (int *)calloc((size_t)S->nmoltype, sizeof(int));
+    float *molfraction = (float *)calloc((size_t)S->nmoltype, sizeof(float));
+    int32_t *izv = (int32_t *)calloc((size_t)S->natom, sizeof(int32_t));
+    int32_t *icv = (int32_t *)calloc((size_t)S->natom, sizeof(int32_t));
+    if (ngrsamples <= 0) ngrsamples = 1000;
+    if (ngrsamples > nmol) ngrsamples = nmol;
+    float probaccept = (float)ngrsamples / (float)nmol;
+    for (int im = 0; im < nmol; ++im) molfraction[S->mtype[im]] = molfraction[S->mtype[im]] + 1.0f;
+    for (int t = 0; t < S->nmoltype; ++t) molfraction[t] = molfraction[t] / (float)nmol;
+    int im1 = 0, im2 = nmol - 1;
+    float addwav = 1.0f;
+    if (probaccept >= 1.0f) {
+        im2 = nmol - 2;
+        addwav = 2.0f;
+        const int a0 = S->naf[nmol - 1];
+        for (int ia = a0; ia < a0 + S->nato[nmol - 1]; ++ia) csampled[S->itype[ia]] = csampled[S->itype[ia]] + 1.0f;
+    }
+    for (int im = im1; im <= im2; ++im) {
+        float u = oracle_ran1(R);
+        int mt = S->mtype[im];
+        if (u < probaccept || molsampled[mt] < 1 || molfraction[mt] < probaccept) {
+            molsampled[mt]++;
+            float xc1 = S->xadd[im], yc1 = S->yadd[im], zc1 = S->zadd[im];
+            int jm1 = 0, jm2 = nmol - 1;
+            if (probaccept >= 1.0f) jm1 = im + 1;
+            const int a0 = S->naf[im], a1 = a0 + S->nato[im];
+            for (int ia = a0; ia < a1; ++ia) csampled[S->itype[ia]] = csampled[S->itype[ia]] + 1.0f;
+            for (int ia = a0; ia < a1; ++ia) {
+                float x1 = S->xa[ia] + xc1, y1 = S->ya[ia] + yc1, z1 = S->za[ia] + zc1;
+                int it = S->itype[ia];
+                for (int jm = jm1; jm <= jm2; ++jm) {
+                    const int b0 = S->naf[jm], b1 = b0 + S->nato[jm];
+                    if (jm != im) {
+                        float xc2 = S->xadd[jm], yc2 = S->yadd[jm], zc2 = S->zadd[jm];
+                        for (int ja = b0; ja < b1; ++ja) {
+                            int icref = S->npairref[it * ntype + S->itype[ja]];
+                            float x2 = S->xa[ja] + xc2, y2 = S->ya[ja] + yc2, z2 = S->za[ja] + zc2;
+                            float xx = x1 - x2, yy = y1 - y2, zz = z1 - z2;
+                            minimagec(S, &xx, &yy, &zz);
+                            float dtest = sqrtf(xx * xx + yy * yy + zz * zz);
+                            int iz1 = f_nint(dtest / stepcl) + 2;
+                            if (iz1 > 1 && iz1 <= npt1) {
+                                izv[ja] = iz1;
+                                icv[ja] = icref;
+                            } else {
+                                izv[ja] = 0;
+                            }
+                            float dtt = dtest * dmax;
+                            if (dtt < 1.0f * fabsf(rminex[icref])) potex[icref] = potex[icref] + 1.0f;
+                        }
+                    } else {
+                        for (int ja = b0; ja < b1; ++ja) izv[ja] = 0;
+                    }
+                }
+                int ja0 = S->naf[jm1], ja1 = S->naf[jm2] + S->nato[jm2];
+                for (int ja = ja0; ja < ja1; ++ja) {
+                    if (izv[ja] > 0) {
+                        size_t k = half + (size_t)icv[ja] * ld + izv[ja];
+                        wav[k] = wav[k] + addwav;
+                    }
+                }
+            }
+        }
+    }
+    /* normalisation (:3857-3897) */
+    for (int ic = 0; ic < npairs; ++ic) {
+        int it = -1, jt = -1;
+        for (int a = 0; a < ntype && it < 0; ++a)
+            for (int b = a; b < ntype; ++b)
+                if (S->npairref[a * ntype + b] == ic) { it = a; jt = b; break; }
+        float cprod = cfrac[it] * cfrac[jt] * (float)natomr;
+        float cprod2 = csampled[it] * cfrac[jt];
+        if (it != jt) {
+            cprod = cprod * 2.0f;
+            cprod2 = cprod2 + csampled[jt] * cfrac[it];
+        }
+        float *w1 = wav + (size_t)ic * ld;
+        float *w2 = wav + half + (size_t)ic * ld;
+        if (cprod > 0.0f) {
+            for (int iz = 1; iz <= npt1; ++iz) w1[iz] = w1[iz] / cprod;
+        } else {
+            for (int iz = 1; iz <= npt1; ++iz) w1[iz] = 0.0f;
+        }
+        if (cprod2 > 0.0f) {
+            for (int iz = 1; iz <= npt1; ++iz) w2[iz] = w2[iz] / cprod2;
+            potex[ic] = potex[ic] * cfrac[jt] / cprod2;
+        } else {
+            for (int iz = 1; iz <= npt1; ++iz) w2[iz] = ycoh[iz];
+        }
+    }
+    free(csampled);
+    free(molsampled);
+    free(molfraction);
+    free(izv);
+    free(icv);
+    return ngrsamples;
+}
+
+/* ------------------------------------------------------------------ gensq */
+/* epsr_standalone_rev3.py:4731-4802.  wav [2][npairs][ldw]; foqols [nq+1][ldf] row i holds
+ * F[j,i] for j in 1..npt1 (ldf >= npt1+1); sofq out [2][npairs][nq+1]. natomsphere [ntype]. */
+void oracle_gensq(int nq, int npairs, int npt1, const float *wav, int ldw, const float *foqols, int ldf,
+                  const float *ycoh, const int32_t *n2extr, const float *natomsphere, float *sofq) {
+    const size_t half = (size_t)npairs * (size_t)ldw;
+    const size_t shalf = (size_t)npairs * (size_t)(nq + 1);
+    for (int ic = 0; ic < npairs; ++ic) {
+        const float *w1 = wav + (size_t)ic * ldw;
+        const float *w2 = wav + half + (size_t)ic * ldw;
+        const float nsph = natomsphere[n2extr[ic]];
+        for (int i = 1; i <= nq; ++i) {
+            const float *fq = foqols + (size_t)i * ldf;
+            float sum1 = 0.0f, sum2 = 0.0f, sum3 = 0.0f;
+            for (int j = 2; j <= npt1; ++j) {
+                float add1 = w1[j];
+                if (fabsf(add1) > 0.0f) sum1 = sum1 + add1 * fq[j];
+            }
+            for (int j = 2; j <= npt1; ++j) {
+                float add2 = (w2[j] - ycoh[j]) * nsph;
+                sum2 = sum2 + add2 * fq[j];
+                sum3 = sum3 + w2[j];
+            }
+            if (sum3 <= 0.0f) sum2 = 0.0f;
+            sofq[(size_t)ic * (nq + 1) + i] = sum1;
+            sofq[shalf + (size_t)ic * (nq + 1) + i] = sum2;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ stog */
+/* ato_manipulation_rev4.py:4067-4121. sofq [npairs][ldq] (i 1-based), q [ldq], r [nr+1]
+ * (1-based), gofr out [npairs][nr+1]. */
+static float lorch(float x, float pi) {
+    if (x == 0.0f) return 1.0f;
+    if (x < pi) return sinf(x) / x;
+    return 0.0f;
+}
+
+void oracle_stog(float rho, const float *q, const float *sofq, int ldq, const float *r, float *gofr,
+                 const int32_t *nqmin, const int32_t *nqmax, int nr, int npairs, const float *xwt) {
+    const float pi = 3.14159265358979323846f;
+    const float qstep = q[4] - q[3];
+    const float sfac = 0.5f * qstep / pi / pi / rho;
+    for (int j = 1; j <= nr; ++j) {
+        const float rr = r[j];
+        for (int in = 0; in < npairs; ++in) {
+            const float qmax = pi / q[nqmax[in]];
+            const float *s = sofq + (size_t)in * ldq;
+            float sumi = 0.0f;
+            for (int i = nqmin[in]; i <= nqmax[in]; ++i) {
+                const float qq = q[i];
+                float prod;
+                if (rr > 0.0f) {
+                    float qr = qq * rr;
+                    prod = qq * sinf(qr) * lorch(qmax * qq, pi);
+                } else {
+                    prod = qq * qq * lorch(qmax * qq, pi);
+                }
+                sumi = sumi + s[i] * prod;
+            }
+            float g;
+            if (rr > 0.0f) g = xwt[in] + sfac * sumi / rr;
+            else g = xwt[in] + sfac * sumi;
+            gofr[(size_t)in * (nr + 1) + j] = g;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ fit_expansion */
+/* epsr_standalone_rev3.py:4806-4940 and smoop auxiliary_routines.py:744-763.
+ * yin [npt+1], expr [npt*nterms+1] (1-based flat), yout [npt+1], wt/wtold [nterms+1].
+ * scal[4] in/out = {stepr, acceptr, rejrat, chisqnew}.  Returns the number of trials. */
+static float expand(int nterms, int j, const float *expr, const float *coeff, float summax) {
+    float sum = 0.0f;
+    const float *e = expr + (size_t)(j - 1) * nterms + 1;
+    for (int i = 0; i < nterms; ++i) {
+        sum = sum + e[i] * coeff[i + 1];
+        if (fabsf(sum) > summax) sum = f_sign(summax, sum);
+    }
+    return sum;
+}
+
+static void smoop(int nqmin, int nqmax, int nsmoo, float *diff) {
+    int n1 = nqmin, n2 = nqmax;
+    if (n2 - 2 < n1 || nsmoo == 0) return;
+    for (int it = 0; it < nsmoo; ++it) {
+        float sm = 0.0f, sn = diff[n1];
+        float sum1 = 0.25f * (sm + sn);
+        for (int i = n1; i <= n2; ++i) {
+            sm = sn;
+            int j = i + 1;
+            sn = j <= n2 ? diff[j] : 0.0f;
+            float sum2 = 0.25f * (sm + sn);
+            diff[i] = sum1 + sum2;
+            sum1 = sum2;
+        }
+    }
+}
+
+int64_t oracle_fit_expansion(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
+                             float *scal, int nmin, int npt, int ncfirst, int nterms, int nits, int nfreq,
+                             oracle_ran1_state *R) {
+    const float summax = expf(25.0f);
+    const int nstep = 100, ntry = 150;
+    float stepr = scal[0];
+    float acceptr = 0.05f;
+    float rejrat = scal[2];
+    float chisqnew = scal[3];
+    const int npoints = npt - nmin + 1;
+    int64_t trials = 0;
+    float wtmax = 0.0f;
+    for (int it = 1; it <= nterms; ++it) {
+        wt[it] = wtold[it];
+        float a = fabsf(wt[it]);
+        wtmax = (a >= wtmax) ? a : wtmax;
+    }
+    if (stepr < 1.0e-6f * wtmax) stepr = 2.0e-6f * wtmax;
+    if (nits > 0) {
+        float chisqold;
+        int icount = 0;
+        chisqnew = 0.0f;
+        for (int i = nmin; i <= npt; ++i) {
+            float term = yin[i] - expand(nterms, i, expr, wt, summax);
+            chisqnew = chisqnew + term * term;
+        }
+        chisqold = chisqnew;
+        float chisqtest = -1.0f, chisqfinish = 0.0f;
+        int itry = 0;
+        while (itry < 10 || (itry < ntry && chisqtest < 1.0e-4f)) {
+            itry++;
+            float accept = acceptr * chisqold / (float)npoints;
+            rejrat = 0.0f;
+            float chisqstart = chisqold / (float)npoints;
+            for (int it = 1; it <= nstep; ++it) {
+                trials++;
+                for (int ic = ncfirst; ic <= nterms; ++ic) {
+                    if (fabsf(wtold[ic]) < 1.0f)
+                        wt[ic] = wtold[ic] + stepr * (2.0f * oracle_ran1(R) - 1.0f);
+                    else
+                        wt[ic] = wtold[ic] * (1.0f + stepr * (2.0f * oracle_ran1(R) - 1.0f));
+                }
+                chisqnew = 0.0f;
+                for (int i = nmin; i <= npt; ++i) {
+                    float term = yin[i] - expand(nterms, i, expr, wt, summax);
+                    chisqnew = chisqnew + term * term;
+                }
+                float exponent = (chisqnew - chisqold) / accept;
+                float test;
+                if (exponent > 0.0f && exponent <= 20.0f) test = expf(-exponent) - oracle_ran1(R);
+                else if (exponent > 20.0f) test = -1.0f;
+                else test = 1.0f;
+                if (test >= 0.0f) {
+                    icount++;
+                    if (icount == nfreq) {
+                        icount = 0;
+                        smoop(ncfirst, nterms, 1, wt);
+                        chisqnew = 0.0f;
+                        for (int i = nmin; i <= npt; ++i) {
+                            float term = yin[i] - expand(nterms, i, expr, wt, summax);
+                            chisqnew = chisqnew + term * term;
+                        }
+                    }
+                    chisqold = chisqnew;
+                    for (int ic = 1; ic <= nterms; ++ic) wtold[ic] = wt[ic];
+                } else {
+                    rejrat = rejrat + 1.0f;
+                }
+            }
+            rejrat = rejrat / (float)nstep;
+            chisqfinish = chisqold / (float)npoints;
+            if (chisqstart > 0.0f) chisqtest = (chisqfinish - chisqstart) / chisqstart;
+            else chisqtest = chisqfinish - chisqstart;
+            float rejfac = rejrat > 0.0f ? 0.75f / rejrat : 2.0f;
+            stepr = stepr * rejfac;
+        }
+        for (int ic = 1; ic <= nterms; ++ic) wt[ic] = wtold[ic];
+    }
+    chisqnew = 0.0f;
+    for (int i = 1; i <= npt; ++i) {
+        float term = expand(nterms, i, expr, wt, summax);
+        yout[i] = term;
+        if (i >= nmin) {
+            float d = yin[i] - term;
+            chisqnew = chisqnew + d * d;
+        }
+    }
+    scal[0] = stepr;
+    scal[1] = acceptr;
+    scal[2] = rejrat;
+    scal[3] = chisqnew;
+    return trials;
+}

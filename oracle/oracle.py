@@ -1,0 +1,305 @@
+"""ctypes wrapper of the C oracle (oracle/epsr_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by the tests, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` as the checker.  The product library never loads it.
+
+Functions take ``BoxArrays`` (epsr_python_translation_b200.box) and NumPy arrays and return
+NumPy arrays laid out like the device path's outputs.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "epsr_oracle.c")
+LIB = os.path.join(HERE, "liboracle.so")
+
+f32 = np.float32
+P = C.c_void_p
+
+
+def build(force=False):
+    """Compile the restatement: float32 op order is kept by -ffp-contract=off."""
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+                               "-o", LIB, SRC, "-lm"])
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(LIB)
+        _lib.oracle_ran1.restype = C.c_float
+        _lib.oracle_en_mole_pair.restype = C.c_float
+        _lib.oracle_fit_expansion.restype = C.c_int64
+    return _lib
+
+
+def ptr(a):
+    return a.ctypes.data_as(P) if a is not None else None
+
+
+class Ran1C(C.Structure):
+    _fields_ = [("idum", C.c_int32), ("iy", C.c_int32), ("mcall", C.c_int32), ("iv", C.c_int32 * 32)]
+
+    @staticmethod
+    def of(st):
+        r = Ran1C()
+        r.idum, r.iy, r.mcall = st.idum, st.iy, np.int64(st.mcall).astype(np.int32)
+        for i in range(32):
+            r.iv[i] = int(st.iv[i])
+        return r
+
+    def to_state(self):
+        from epsr_python_translation_b200.box import Ran1State
+        return Ran1State(self.idum, self.iy, self.mcall, np.array(list(self.iv), dtype=np.int32))
+
+
+class SysC(C.Structure):
+    _fields_ = [("nmol", C.c_int32), ("natom", C.c_int32), ("ntype", C.c_int32), ("npairs", C.c_int32),
+                ("nmoltype", C.c_int32), ("naf", P), ("nato", P), ("mtype", P), ("itype", P),
+                ("xa", P), ("ya", P), ("za", P), ("xadd", P), ("yadd", P), ("zadd", P), ("npairref", P),
+                ("xstar", P), ("xavs", P), ("xavs1", P), ("ecoul", P), ("ecoul1", P), ("ld", C.c_int32),
+                ("npt2", C.c_int32), ("stepcl", C.c_float), ("cubic", C.c_int32), ("lat", C.c_float * 6)]
+
+
+class CellsC(C.Structure):
+    _fields_ = [("ncelldiva", C.c_int32), ("ncelldivb", C.c_int32), ("ncelldivc", C.c_int32),
+                ("ncell", C.c_int32), ("ncellneighb", C.c_int32), ("maxcellno", C.c_int32),
+                ("molcellno", P), ("cell_start", P), ("cell_mols", P), ("ia_off", P), ("ib_off", P),
+                ("ic_off", P)]
+
+
+class StoreC(C.Structure):
+    _fields_ = [("nnbrefmax", C.c_int32), ("nergpair", C.c_int32), ("nergpairmax", C.c_int32),
+                ("nergpairm", P), ("molergpair", P), ("ergpairref", P), ("ergpair", P)]
+
+
+class McParC(C.Structure):
+    _fields_ = [("simt", C.c_float), ("rejrate", C.c_float), ("stepr", C.c_float), ("stepm", C.c_float),
+                ("trstepmax", C.c_float), ("trstepmin", C.c_float), ("ireset", C.c_int32),
+                ("wholerot", P), ("wholetrans", P), ("nwhole", P), ("nmovem", P), ("nstepreject", P),
+                ("internrot", P), ("interntrans", P), ("ngrot", P)]
+
+
+class TraceC(C.Structure):
+    _fields_ = [("nmoves", C.c_int32), ("im", P), ("den", P), ("acc", P), ("cosv", P), ("ncos", C.c_int32)]
+
+
+class SysHandle:
+    """Keeps the NumPy arrays alive for a SysC view of a BoxArrays (mutated in place)."""
+
+    def __init__(self, box):
+        self.box = box
+        ld = box.npt + 1
+        self.tabs = [np.ascontiguousarray(t, dtype=f32) for t in (box.xavs, box.xavs1, box.ecoul, box.ecoul1)]
+        self.npairref = np.ascontiguousarray(box.npairref, dtype=np.int32)
+        s = SysC()
+        s.nmol, s.natom, s.ntype, s.npairs, s.nmoltype = box.nmol, box.natom, box.ntype, box.npairs, box.nmoltype
+        s.naf, s.nato, s.mtype, s.itype = ptr(box.naf), ptr(box.nato), ptr(box.mtype), ptr(box.itype)
+        s.xa, s.ya, s.za = ptr(box.xa), ptr(box.ya), ptr(box.za)
+        s.xadd, s.yadd, s.zadd = ptr(box.xadd), ptr(box.yadd), ptr(box.zadd)
+        s.npairref = ptr(self.npairref)
+        s.xstar = ptr(box.xstar)
+        s.xavs, s.xavs1, s.ecoul, s.ecoul1 = [ptr(t) for t in self.tabs]
+        s.ld = ld
+        s.npt2 = box.npt2
+        s.stepcl = box.stepcl
+        s.cubic = 1 if box.cubic else 0
+        for i in range(6):
+            s.lat[i] = float(box.lat6[i])
+        self.c = s
+
+
+# ----------------------------------------------------------------------------- ran1
+def ran1_fill(state, n):
+    r = Ran1C.of(state)
+    out = np.zeros(n, dtype=f32)
+    lib().oracle_ran1_fill(C.byref(r), ptr(out), C.c_int64(n))
+    return out, r.to_state()
+
+
+# ----------------------------------------------------------------------------- cells
+def cell_list(box, nmolcell, rmax):
+    L = lib()
+    dims = np.zeros(4, dtype=np.int32)
+    lat6 = np.ascontiguousarray(box.lat6, dtype=f32)
+    lat9 = np.ascontiguousarray(box.lat9, dtype=f32)
+    L.oracle_cell_dims(nmolcell, box.nmol, ptr(lat6), ptr(dims))
+    ncell = int(dims[3])
+    out = dict(molcellno=np.zeros(box.nmol, np.int32), cell_start=np.zeros(ncell + 1, np.int32),
+               cell_mols=np.zeros(box.nmol, np.int32), ia_off=np.zeros(ncell, np.int32),
+               ib_off=np.zeros(ncell, np.int32), ic_off=np.zeros(ncell, np.int32))
+    c = CellsC()
+    for k, v in out.items():
+        setattr(c, k, ptr(v))
+    L.oracle_cell_list(nmolcell, ptr(box.xadd), ptr(box.yadd), ptr(box.zadd), box.nmol, C.c_float(f32(rmax)),
+                       ptr(lat6), ptr(lat9), C.byref(c))
+    out.update(ncelldiva=c.ncelldiva, ncelldivb=c.ncelldivb, ncelldivc=c.ncelldivc, ncell=c.ncell,
+               ncellneighb=c.ncellneighb, maxcellno=c.maxcellno)
+    out["_keep"] = [out[k] for k in ("molcellno", "cell_start", "cell_mols", "ia_off", "ib_off", "ic_off")]
+    for k in ("ia_off", "ib_off", "ic_off"):
+        out[k] = out[k][: c.ncellneighb].copy()
+    out["_c"] = c
+    out["nnbrefmax"] = int(L.oracle_nnbrefmax(C.byref(c)))
+    return out
+
+
+def region(cells, ic):
+    nb = np.zeros(max(cells["nnbrefmax"], 1), dtype=np.int32)
+    n = lib().oracle_region(C.byref(cells["_c"]), ic, ptr(nb))
+    return nb[:n].copy()
+
+
+# ----------------------------------------------------------------------------- fmolec1
+def fmolec1(box, cells, eintra, capacity=None):
+    M = cells["nnbrefmax"]
+    nmol = box.nmol
+    cap = capacity or 100 * nmol
+    while True:
+        st = dict(nergpairm=np.zeros(nmol, np.int32), molergpair=np.zeros(nmol * M, np.int32),
+                  ergpairref=np.zeros(nmol * M, np.int32), ergpair=np.zeros(cap, f32))
+        E = StoreC()
+        E.nnbrefmax, E.nergpair, E.nergpairmax = M, 0, cap
+        for k, v in st.items():
+            setattr(E, k, ptr(v))
+        out2 = np.zeros(2, f32)
+        h = SysHandle(box)
+        ei = np.ascontiguousarray(eintra, dtype=f32)
+        rc = lib().oracle_fmolec1(C.byref(h.c), C.byref(cells["_c"]), ptr(ei), C.byref(E), ptr(out2))
+        if rc == 0:
+            break
+        cap = cap * 2
+    st["molergpair"] = st["molergpair"].reshape(nmol, M)
+    st["ergpairref"] = st["ergpairref"].reshape(nmol, M)
+    st["nergpair"] = E.nergpair
+    st["nnbrefmax"] = M
+    st["ftest"] = out2[0]
+    st["ftestb"] = out2[1]
+    st["_cap"] = cap
+    return st
+
+
+def store_c(st):
+    E = StoreC()
+    E.nnbrefmax, E.nergpair, E.nergpairmax = st["nnbrefmax"], st["nergpair"], st["ergpair"].shape[0]
+    E.nergpairm = ptr(st["nergpairm"])
+    E.molergpair = ptr(st["molergpair"])
+    E.ergpairref = ptr(st["ergpairref"])
+    E.ergpair = ptr(st["ergpair"])
+    return E
+
+
+def en_mole_pair(box, im, jm):
+    h = SysHandle(box)
+    return f32(lib().oracle_en_mole_pair(C.byref(h.c), im, jm))
+
+
+# ----------------------------------------------------------------------------- molfit
+def trsteps(natomr):
+    out = np.zeros(2, f32)
+    lib().oracle_trsteps(natomr, ptr(out))
+    return out[0], out[1]
+
+
+def molfit(box, cells, st, mc, ran1, fadds=0.0, record_cos=True):
+    """One whole-molecule cycle; mutates box coordinates, st['ergpair'] and the step arrays
+    in ``mc`` (dict of NumPy arrays).  Returns (fadds, trace dict, ran1 state)."""
+    h = SysHandle(box)
+    E = store_c(st)
+    nmt = box.nmoltype
+    par = McParC()
+    par.simt, par.rejrate = box.simt, f32(mc["rejrate"])
+    par.stepr, par.stepm = f32(mc["stepr"]), f32(mc["stepm"])
+    tmax, tmin = trsteps(box.natomr)
+    par.trstepmax, par.trstepmin = tmax, tmin
+    par.ireset = int(mc.get("ireset", 0))
+    for k in ("wholerot", "wholetrans", "internrot", "interntrans"):
+        mc[k] = np.ascontiguousarray(mc[k], dtype=f32)
+        setattr(par, k, ptr(mc[k]))
+    mc["nwhole"] = np.zeros(2 * nmt, np.int32)
+    mc["nmovem"] = np.zeros(2 * nmt, np.int32)
+    mc["nstepreject"] = np.ascontiguousarray(mc.get("nstepreject", np.zeros(box.nmol, np.int32)), np.int32)
+    mc["ngrot"] = np.ascontiguousarray(mc.get("ngrot", np.zeros(box.nmol, np.int32)), np.int32)
+    par.nwhole, par.nmovem = ptr(mc["nwhole"]), ptr(mc["nmovem"])
+    par.nstepreject, par.ngrot = ptr(mc["nstepreject"]), ptr(mc["ngrot"])
+    tr = dict(im=np.zeros(box.nmol, np.int32), den=np.zeros(box.nmol, f32), acc=np.zeros(box.nmol, np.int32),
+              cosv=np.zeros(3 * box.nmol, f32) if record_cos else None)
+    T = TraceC()
+    T.im, T.den, T.acc = ptr(tr["im"]), ptr(tr["den"]), ptr(tr["acc"])
+    T.cosv = ptr(tr["cosv"]) if record_cos else None
+    r = Ran1C.of(ran1)
+    fa = C.c_float(f32(fadds))
+    lib().oracle_molfit(C.byref(h.c), C.byref(cells["_c"]), C.byref(E), C.byref(par), C.byref(r), C.byref(fa),
+                        C.byref(T))
+    tr["nmoves"] = T.nmoves
+    if record_cos:
+        tr["cosv"] = tr["cosv"][: T.ncos].copy()
+    return f32(fa.value), tr, r.to_state()
+
+
+# ----------------------------------------------------------------------------- atogen
+def atogen(box, ngrsamples, ran1, rminex, ycoh=None, sizefactor=1.0):
+    ld = box.npt + 1
+    wav = np.zeros((2, box.npairs, ld), f32)
+    potex = np.zeros(box.npairs, f32)
+    if ycoh is None:
+        ycoh = np.zeros(ld, f32)
+    ycoh = np.ascontiguousarray(ycoh[:ld], dtype=f32)
+    h = SysHandle(box)
+    r = Ran1C.of(ran1)
+    rmx = np.ascontiguousarray(rminex, dtype=f32)
+    ngr = lib().oracle_atogen(C.byref(h.c), ptr(wav), ptr(potex), int(ngrsamples), int(box.npt1),
+                              C.c_float(f32(sizefactor)), C.c_float(f32(box.dmax)), ptr(rmx), ptr(box.cfrac),
+                              int(box.natomr), ptr(ycoh), C.byref(r))
+    return wav, potex, int(ngr), r.to_state()
+
+
+# ----------------------------------------------------------------------------- transforms
+def gensq(nq, npt1, wav, foqols_rows, ycoh, n2extr, natomsphere):
+    """wav (2, npairs, ldw); foqols_rows (nq+1, ldf) with row i = F[:, i]."""
+    npairs, ldw = wav.shape[1], wav.shape[2]
+    ldf = foqols_rows.shape[1]
+    out = np.zeros((2, npairs, nq + 1), f32)
+    lib().oracle_gensq(nq, npairs, npt1, ptr(np.ascontiguousarray(wav, f32)), ldw,
+                       ptr(np.ascontiguousarray(foqols_rows, f32)), ldf, ptr(np.ascontiguousarray(ycoh, f32)),
+                       ptr(np.ascontiguousarray(n2extr, np.int32)), ptr(np.ascontiguousarray(natomsphere, f32)),
+                       ptr(out))
+    return out
+
+
+def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
+    """q (ldq,), sofq_pairs (npairs, ldq) 1-based i; r (nr+1,) 1-based. Returns (npairs, nr+1)."""
+    npairs, ldq = sofq_pairs.shape
+    nr = r.shape[0] - 1
+    out = np.zeros((npairs, nr + 1), f32)
+    lib().oracle_stog(C.c_float(f32(rho)), ptr(np.ascontiguousarray(q, f32)),
+                      ptr(np.ascontiguousarray(sofq_pairs, f32)), ldq, ptr(np.ascontiguousarray(r, f32)), ptr(out),
+                      ptr(np.ascontiguousarray(nqmin, np.int32)), ptr(np.ascontiguousarray(nqmax, np.int32)), nr,
+                      npairs, ptr(np.ascontiguousarray(xwt, f32)))
+    return out
+
+
+def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1):
+    """1-based arrays (index 0 unused).  Returns dict and the new ran1 state."""
+    yin = np.ascontiguousarray(yin, f32)
+    expr = np.ascontiguousarray(expr, f32)
+    wt = np.zeros(nterms + 1, f32)
+    wto = np.ascontiguousarray(wtold, f32).copy()
+    yout = np.zeros(npt + 1, f32)
+    scal = np.array([stepr, 0.0, 0.0, 0.0], f32)
+    r = Ran1C.of(ran1)
+    trials = lib().oracle_fit_expansion(ptr(yin), ptr(expr), ptr(yout), ptr(wt), ptr(wto), ptr(scal), nmin, npt,
+                                        ncfirst, nterms, nits, nfreq, C.byref(r))
+    return dict(wt=wt, wtold=wto, yout=yout, stepr=scal[0], acceptr=scal[1], rejrat=scal[2], chisq=scal[3],
+                trials=int(trials)), r.to_state()
