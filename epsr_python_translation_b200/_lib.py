@@ -1,0 +1,106 @@
+"""ctypes binding of libepsr_gpu.so (the C ABI declared in include/epsr_gpu.h).
+
+The device library is the only compute path: if it is missing or no sm_100 device is
+visible, calls raise ``EpsrGpuError`` -- there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libepsr_gpu.so")
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+F32 = C.c_float
+
+
+class EpsrGpuError(RuntimeError):
+    """A nonzero status from the C ABI (code, message)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"epsr_gpu error {code}: {msg}")
+        self.code = code
+
+
+class Box(C.Structure):
+    _fields_ = [("nmol", I32), ("natom", I32), ("ntype", I32), ("npairs", I32), ("nmoltype", I32),
+                ("naf", P), ("nato", P), ("mtype", P), ("itype", P), ("xa", P), ("ya", P), ("za", P),
+                ("xadd", P), ("yadd", P), ("zadd", P), ("pos", P), ("npairref", P), ("xstar", P), ("tab", P),
+                ("ld", I32), ("npt2", I32), ("izcut", I32), ("stepcl", F32), ("cubic", I32), ("lat", F32 * 6)]
+
+
+class Cells(C.Structure):
+    _fields_ = [("ncelldiva", I32), ("ncelldivb", I32), ("ncelldivc", I32), ("ncell", I32), ("ncellneighb", I32),
+                ("maxcellno", I32), ("molcellno", P), ("cell_start", P), ("cell_mols", P), ("offsets", P)]
+
+
+class Store(C.Structure):
+    _fields_ = [("nnbrefmax", I32), ("capacity", I32), ("nergpairm", P), ("molergpair", P), ("ergpairref", P),
+                ("ergpair", P), ("nergpair", P)]
+
+
+class Mc(C.Structure):
+    _fields_ = [("simt", F32), ("rejrate", F32), ("stepr", F32), ("stepm", F32), ("trstepmax", F32),
+                ("trstepmin", F32), ("ireset", I32), ("wholerot", P), ("wholetrans", P), ("internrot", P),
+                ("interntrans", P), ("nwhole", P), ("nmovem", P), ("nstepreject", P), ("fadds", P), ("ran1", P),
+                ("cos_override", P), ("trace_den", P), ("trace_acc", P), ("strict", I32),
+                ("status", P)]
+
+
+_SIGS = {
+    "epsr_last_error": (C.c_char_p, []),
+    "epsr_version": (C.c_char_p, []),
+    "epsr_device_count": (C.c_int, []),
+    "epsr_ran1_fill": (C.c_int, [P, P, I64, P]),
+    "epsr_cell_dims": (C.c_int, [I32, I32, P, P]),
+    "epsr_cell_list": (C.c_int, [P, P, P, I32, I32, F32, P, P, C.POINTER(Cells), P, I64, P]),
+    "epsr_nnbrefmax": (C.c_int, [C.POINTER(Cells), P, P]),
+    "epsr_box_positions": (C.c_int, [C.POINTER(Box), P]),
+    "epsr_fmolec1_scratch_bytes": (I64, [I32, I32, I32]),
+    "epsr_fmolec1": (C.c_int, [C.POINTER(Box), C.POINTER(Cells), P, C.POINTER(Store), P, I64, I32, P, P]),
+    "epsr_molfit_scratch_bytes": (I64, [I32, I32, I32]),
+    "epsr_molfit": (C.c_int, [C.POINTER(Box), C.POINTER(Cells), C.POINTER(Store), C.POINTER(Mc), P, I64, P]),
+    "epsr_en_change": (C.c_int, [C.POINTER(Box), C.POINTER(Store), I32, P, P, P]),
+    "epsr_en_mole_pair": (C.c_int, [C.POINTER(Box), P, P, I32, P, P]),
+    "epsr_atogen": (C.c_int, [C.POINTER(Box), I32, F32, F32, P, P, P, P, P, I32, P, P, P, I32, P, P, P, I64, P]),
+    "epsr_atogen_scratch_bytes": (I64, [I32, I32, I32, I32]),
+    "epsr_atogen_last_pair_updates": (I64, []),
+    "epsr_gensq": (C.c_int, [I32, I32, I32, P, I32, P, I64, I64, P, P, P, P, P]),
+    "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P]),
+    "epsr_fit_expansion": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, P, P]),
+    "epsr_fit_expansion_scratch_bytes": (I64, [I32, I32]),
+}
+
+_lib = None
+
+
+def exported_symbols():
+    """Names of every entry point the header declares (checked by the CPU test suite)."""
+    return sorted(_SIGS)
+
+
+def load(require_device=False):
+    """Load the library (raising if it is missing); optionally require an sm_100 device."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise EpsrGpuError(-1, f"{LIBPATH} is missing; run epsr_python_translation_b200.csrc.build")
+        lib = C.CDLL(LIBPATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    if require_device and _lib.epsr_device_count() <= 0:
+        raise EpsrGpuError(-1, "no sm_100 (B200) device visible")
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise EpsrGpuError(rc, load().epsr_last_error().decode(errors="replace"))
+    return rc

@@ -142,3 +142,25 @@ class Ran1State:
     def from_golden(z, prefix) -> "Ran1State":
         return Ran1State(int(z[prefix + "idum"]), int(z[prefix + "iy"]), int(z[prefix + "mcall"]),
                          z[prefix + "iv"].astype(np.int32).copy())
+
+
+_libm = None
+
+
+def _powf(x, y):
+    """glibc powf, the function the reference calls through ctypes (fortran/fmath.py:137)."""
+    global _libm
+    if _libm is None:
+        import ctypes
+        import ctypes.util
+        _libm = ctypes.CDLL(ctypes.util.find_library("m"))
+        _libm.powf.restype = ctypes.c_float
+        _libm.powf.argtypes = [ctypes.c_float, ctypes.c_float]
+    return f32(_libm.powf(float(x), float(y)))
+
+
+def trsteps(natomr: int):
+    """Largest and smallest translational step of molfit (molfit.py:96-101), float32."""
+    tmax = _powf(f32(1.0) / f32(natomr), f32(1.0) / f32(3.0))
+    tmin = max(f32(0.0001) * tmax, f32(1.0e-6))
+    return f32(tmax), f32(tmin)

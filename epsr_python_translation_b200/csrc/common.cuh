@@ -1,0 +1,173 @@
+// common.cuh -- device helpers shared by the EPSR pair-path kernels (sm_100a).
+//
+// Bit-exactness: the reference evaluates float32 scalars with no fused multiply-add, IEEE
+// division and sqrt.  Every arithmetic step below that feeds a compared result uses the
+// explicit round-to-nearest intrinsics (__fadd_rn, __fmul_rn, __fdiv_rn, __fsqrt_rn), which
+// the compiler never contracts, and the library is also built with -fmad=false.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/epsr_gpu.h"
+
+namespace epsr {
+
+// ----------------------------------------------------------------- Fortran intrinsics
+// nint: round half away from zero (fortran/fmath.py:222).  x - trunc(x) is exact in float.
+__device__ __forceinline__ float nint_f(float x) {
+    float t = truncf(x);
+    float fr = __fsub_rn(x, t);
+    if (fr >= 0.5f) t = __fadd_rn(t, 1.0f);
+    else if (fr <= -0.5f) t = __fsub_rn(t, 1.0f);
+    return t;
+}
+__device__ __forceinline__ int nint_i(float x) { return (int)nint_f(x); }
+
+// ifix: truncation toward zero (fortran/fmath.py:245)
+__device__ __forceinline__ int ifix(float x) { return __float2int_rz(x); }
+
+__device__ __forceinline__ float fsign(float a, float b) { return copysignf(fabsf(a), b); }
+
+// Transcendentals: evaluated in double and rounded once to float, i.e. the correctly
+// rounded value in all but a vanishing fraction of arguments.  glibc's float functions
+// used by the reference are not correctly rounded (about 1.3% of sinf/cosf arguments and
+// 0.07% of expf arguments differ by one ulp), so these are tolerance-checked, and the
+// Monte Carlo kernel accepts injected cosine values to prove the rest bit-identical.
+__device__ __forceinline__ float cos_r(float x) { return (float)cos((double)x); }
+__device__ __forceinline__ float sin_r(float x) { return (float)sin((double)x); }
+__device__ __forceinline__ float exp_r(float x) { return (float)exp((double)x); }
+
+// ----------------------------------------------------------------- minimum image
+struct Lattice {
+    int cubic;
+    float alatx, blatx, clatx, blaty, claty, clatz;
+};
+
+// minimagec.py:13-45
+__device__ __forceinline__ void minimagec(const Lattice &L, float &x, float &y, float &z) {
+    if (L.cubic) {
+        z = __fsub_rn(z, nint_f(z));
+        y = __fsub_rn(y, nint_f(y));
+        x = __fsub_rn(x, nint_f(x));
+        return;
+    }
+    float fc = __fdiv_rn(z, L.clatz);
+    float fb = __fdiv_rn(__fsub_rn(y, __fmul_rn(fc, L.claty)), L.blaty);
+    float fa = __fdiv_rn(__fsub_rn(__fsub_rn(x, __fmul_rn(fb, L.blatx)), __fmul_rn(fc, L.clatx)), L.alatx);
+    fc = __fsub_rn(fc, nint_f(fc));
+    fb = __fsub_rn(fb, nint_f(fb));
+    fa = __fsub_rn(fa, nint_f(fa));
+    z = __fmul_rn(fc, L.clatz);
+    y = __fadd_rn(__fmul_rn(fb, L.blaty), __fmul_rn(fc, L.claty));
+    x = __fadd_rn(__fadd_rn(__fmul_rn(fa, L.alatx), __fmul_rn(fb, L.blatx)), __fmul_rn(fc, L.clatx));
+}
+
+__device__ __forceinline__ float dist_f(const Lattice &L, float xd, float yd, float zd) {
+    minimagec(L, xd, yd, zd);
+    float dsq = __fadd_rn(__fadd_rn(__fmul_rn(xd, xd), __fmul_rn(yd, yd)), __fmul_rn(zd, zd));
+    return __fsqrt_rn(dsq);
+}
+
+// ----------------------------------------------------------------- pair energy
+struct Tables {
+    const float4 *tab;   // [npairs*ld] {xavs, xavs1, ecoul, ecoul1}
+    const float *xstar;  // [ld]
+    int ld, npt2, izcut;
+    float stepcl;
+};
+
+// en_atom_inter_scale molfit.py:1251-1279 (scalefac = 1).  d is the minimum-image distance.
+// Beyond izcut every table entry is +0, so the reference's value there is exactly +0.
+__device__ __forceinline__ float pair_energy_d(const Tables &T, float d, int icref) {
+    float rat = __fdiv_rn(d, T.stepcl);
+    int iz = ifix(rat) + 2;
+    float sume = 0.0f;
+    if (iz >= 2 && iz <= T.izcut) {  // iz < 2 only for a non-finite distance
+        float4 t = __ldg(T.tab + (size_t)icref * T.ld + iz);
+        float dt = __fsub_rn(d, __ldg(T.xstar + iz));
+        sume = __fadd_rn(t.x, __fmul_rn(t.y, dt));
+        sume = __fadd_rn(__fadd_rn(sume, t.z), __fmul_rn(t.w, dt));
+    }
+    return sume;
+}
+
+__device__ __forceinline__ float pair_energy(const Lattice &L, const Tables &T, float4 p1, float4 p2,
+                                             int icref) {
+    // xdif = x2 - x1 (molfit.py:1257)
+    float d = dist_f(L, __fsub_rn(p2.x, p1.x), __fsub_rn(p2.y, p1.y), __fsub_rn(p2.z, p1.z));
+    return pair_energy_d(T, d, icref);
+}
+
+// ----------------------------------------------------------------- ran1 (device, one lane)
+// auxiliary_routines.py:324-391 with state {idum, iy, mcall, iv[32]}.
+struct Ran1 {
+    int32_t idum, iy, mcall;
+    int32_t iv[32];
+};
+
+__device__ __forceinline__ int32_t ran1_lcg(int32_t idum) {
+    int32_t k = idum / 127773;
+    idum = 16807 * (idum - k * 127773) - 2836 * k;
+    if (idum < 0) idum += 2147483647;
+    return idum;
+}
+
+__device__ __forceinline__ float ran1_out(int32_t iy) {
+    float r = __fmul_rn(4.656612873077393e-10f, (float)iy);
+    return r > 0.9999998807907104f ? 0.9999998807907104f : r;
+}
+
+// Single-thread generator on a state held in shared or local memory.
+__device__ __forceinline__ float ran1_next(Ran1 &s) {
+    int32_t idum = s.idum, iy = s.iy;
+    if (idum <= 0 || iy == 0) {
+        int64_t neg = -(int64_t)idum;
+        int32_t w = (int32_t)(uint32_t)(uint64_t)neg;
+        idum = w > 1 ? w : 1;
+        for (int j = 40; j >= 1; --j) {
+            idum = ran1_lcg(idum);
+            if (j <= 32) s.iv[j - 1] = idum;
+        }
+        iy = s.iv[0];
+    }
+    idum = ran1_lcg(idum);
+    int j = iy >> 26;  // iy / NDIV, NDIV = 2^26, iy >= 0
+    iy = s.iv[j];
+    s.iv[j] = idum;
+    s.idum = idum;
+    s.iy = iy;
+    s.mcall = (int32_t)((uint32_t)s.mcall + 1u);
+    return ran1_out(iy);
+}
+
+__device__ __forceinline__ void ran1_load(Ran1 &s, const int32_t *g) {
+    s.idum = g[0];
+    s.iy = g[1];
+    s.mcall = g[2];
+    for (int i = 0; i < 32; ++i) s.iv[i] = g[3 + i];
+}
+__device__ __forceinline__ void ran1_store(const Ran1 &s, int32_t *g) {
+    g[0] = s.idum;
+    g[1] = s.iy;
+    g[2] = s.mcall;
+    for (int i = 0; i < 32; ++i) g[3 + i] = s.iv[i];
+}
+
+// ----------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace epsr
+
+// Error plumbing shared by the ABI translation units.
+void epsr_set_error(const char *fmt, ...);
+int epsr_cuda_check(cudaError_t e, const char *what);
+#define EPSR_CUDA(call)                                              \
+    do {                                                             \
+        cudaError_t _e = (call);                                     \
+        if (_e != cudaSuccess) return epsr_cuda_check(_e, #call);    \
+    } while (0)

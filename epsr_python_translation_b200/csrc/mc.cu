@@ -1,0 +1,463 @@
+// mc.cu -- molfit whole-molecule cycle (molfit.py:52-541) on one box.
+//
+// Sequential kernel: one CTA walks the molecules in cell-visit order exactly as the
+// reference (the ran1 stream and the accept decisions chain every move to the previous
+// one).  Per move: one thread draws the rotation (rotatm :672) and translation (movem :733,
+// including the step-doubling retry); all threads evaluate the moved molecule against its
+// stored neighbours, one neighbour per thread in the reference's (ia, ja) order so each
+// neighbour energy is bit-identical (en_change :806); then the Metropolis test (:401-408),
+// the store update (save_energies/save_erg_pairs) and the coordinate commit or restore.
+#include "common.cuh"
+
+namespace epsr {
+
+constexpr int MC_THREADS = 512;
+constexpr int MC_MAXAT = 64;  // atoms per molecule handled by the kernel
+
+struct McDev {
+    Lattice L;
+    Tables T;
+    int nmol, ntype, nmoltype, M;
+    const int32_t *naf, *nato, *mtype, *npairref, *visit;
+    float *xa, *ya, *za, *xadd, *yadd, *zadd;
+    float4 *pos;
+    const int32_t *nergpairm, *molergpair, *ergpairref;
+    float *ergpair;
+    // parameters
+    float simt, rejrate, stepr, stepm, trstepmax, trstepmin;
+    int ireset, strict;
+    float *wholerot, *wholetrans, *internrot, *interntrans;
+    int32_t *nwhole, *nmovem, *nstepreject;
+    float *fadds;
+    int32_t *ran1;
+    const float *cos_override;
+    float *trace_den;
+    int32_t *trace_acc;
+    float *ergnew_g;   // [M] global fallback when M is large
+    int use_smem;
+    int32_t *status;
+};
+
+__device__ __forceinline__ float next_cos(const McDev &D, int &kcos, float phi) {
+    if (D.cos_override) return D.cos_override[kcos++];
+    ++kcos;
+    return cos_r(phi);
+}
+
+__global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
+    extern __shared__ float dyn[];  // ergnew[M], ergold[M] when use_smem
+    __shared__ Ran1 R;
+    __shared__ float4 mv[MC_MAXAT];
+    __shared__ float nx[MC_MAXAT], ny[MC_MAXAT], nz[MC_MAXAT];
+    __shared__ int sh_im, sh_n, sh_acc, sh_bad;
+    __shared__ float sh_cx, sh_cy, sh_cz;
+    __shared__ double red[MC_THREADS / 32];
+    float *ergnew = D.use_smem ? dyn : D.ergnew_g;
+    float *ergold = D.use_smem ? dyn + D.M : D.ergnew_g + D.M;
+    const int tid = threadIdx.x;
+    const int nmt = D.nmoltype;
+    const float pi = 3.14159265358979323846f;
+    const float rotstepmin = 1.0e-5f, rotstepmax = 1.0f;
+    int kcos = 0;
+    float fadd = 0.0f;
+    if (tid == 0) {
+        ran1_load(R, D.ran1);
+        for (int k = 0; k < 2 * nmt; ++k) {
+            D.nwhole[k] = 0;
+            D.nmovem[k] = 0;
+        }
+    }
+    const float temp = __fdiv_rn(1.0f, D.simt);
+    __syncthreads();
+    for (int v = 0; v < D.nmol; ++v) {
+        if (tid == 0) {
+            const int im = D.visit[v];
+            const int n = D.nato[im];
+            sh_bad = n > MC_MAXAT;
+        }
+        __syncthreads();
+        if (sh_bad) {
+            if (tid == 0 && D.status) D.status[0] = 1;
+            return;
+        }
+        if (tid == 0) {
+            const int im = D.visit[v];
+            const int n = D.nato[im];
+            const int a0 = D.naf[im];
+            const int mt = D.mtype[im];
+            for (int k = 0; k < n; ++k) {
+                nx[k] = D.xa[a0 + k];
+                ny[k] = D.ya[a0 + k];
+                nz[k] = D.za[a0 + k];
+            }
+            if (D.stepr > 0.0f && n > 1) {
+                if (D.wholerot[mt] <= 0.0f) D.wholerot[mt] = rotstepmin;
+                D.nwhole[mt]++;
+                const float step = D.wholerot[mt];
+                // rotatm: about z, then y, then x (molfit.py:683-710)
+                for (int ax = 0; ax < 3; ++ax) {
+                    float phi = __fmul_rn(__fmul_rn(pi, step), __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f));
+                    float c = next_cos(D, kcos, phi);
+                    float sgn = fsign(__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(c, c))), phi);
+                    for (int k = 0; k < n; ++k) {
+                        if (ax == 0) {
+                            float xs = __fsub_rn(__fmul_rn(nx[k], c), __fmul_rn(ny[k], sgn));
+                            ny[k] = __fadd_rn(__fmul_rn(nx[k], sgn), __fmul_rn(ny[k], c));
+                            nx[k] = xs;
+                        } else if (ax == 1) {
+                            float zs = __fsub_rn(__fmul_rn(nz[k], c), __fmul_rn(nx[k], sgn));
+                            nx[k] = __fadd_rn(__fmul_rn(nz[k], sgn), __fmul_rn(nx[k], c));
+                            nz[k] = zs;
+                        } else {
+                            float ys = __fsub_rn(__fmul_rn(ny[k], c), __fmul_rn(nz[k], sgn));
+                            nz[k] = __fadd_rn(__fmul_rn(ny[k], sgn), __fmul_rn(nz[k], c));
+                            ny[k] = ys;
+                        }
+                    }
+                }
+            } else {
+                D.wholerot[mt] = 0.0f;
+            }
+            float cx = D.xadd[im], cy = D.yadd[im], cz = D.zadd[im];
+            if (D.stepm > 0.0f) {
+                if (D.wholetrans[mt] <= 0.0f) D.wholetrans[mt] = D.trstepmin;
+                D.nmovem[mt]++;
+                float st = D.wholetrans[mt];
+                const float xs = cx, ys = cy, zs = cz;
+                cz = __fadd_rn(cz, __fmul_rn(st, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                cy = __fadd_rn(cy, __fmul_rn(st, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                cx = __fadd_rn(cx, __fmul_rn(st, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                while (xs == cx && ys == cy && zs == cz) {
+                    st = __fmul_rn(st, 2.0f);
+                    cz = __fadd_rn(cz, __fmul_rn(st, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                    cy = __fadd_rn(cy, __fmul_rn(st, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                    cx = __fadd_rn(cx, __fmul_rn(st, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                }
+                D.wholetrans[mt] = st;
+            } else {
+                D.wholetrans[mt] = 0.0f;
+            }
+            for (int k = 0; k < n; ++k)
+                mv[k] = make_float4(__fadd_rn(nx[k], cx), __fadd_rn(ny[k], cy), __fadd_rn(nz[k], cz),
+                                    D.pos[a0 + k].w);
+            sh_cx = cx;
+            sh_cy = cy;
+            sh_cz = cz;
+            sh_im = im;
+            sh_n = n;
+        }
+        __syncthreads();
+        const int im = sh_im, n = sh_n;
+        const size_t row = (size_t)im * D.M;
+        const int nn = D.nergpairm[im];
+        double part = 0.0;
+        for (int inn = 1 + tid; inn < nn; inn += MC_THREADS) {
+            const int jm = D.molergpair[row + inn];
+            const int b0 = D.naf[jm], b1 = b0 + D.nato[jm];
+            float sume = 0.0f;
+            for (int ia = 0; ia < n; ++ia) {
+                const float4 p1 = mv[ia];
+                const int it = __float_as_int(p1.w);
+                for (int ja = b0; ja < b1; ++ja) {
+                    const float4 p2 = D.pos[ja];
+                    const int icref = __ldg(D.npairref + it * D.ntype + __float_as_int(p2.w));
+                    sume = __fadd_rn(sume, pair_energy(D.L, D.T, p1, p2, icref));
+                }
+            }
+            const float en = __fadd_rn(0.0f, sume);
+            const float eo = D.ergpair[D.ergpairref[row + inn] - 1];
+            ergnew[inn] = en;
+            ergold[inn] = eo;
+            part += (double)en - (double)eo;
+        }
+        float fdiff;
+        if (D.strict) {
+            __syncthreads();
+            if (tid == 0) {
+                float f = 0.0f;
+                for (int inn = 1; inn < nn; ++inn) f = __fsub_rn(__fadd_rn(f, ergnew[inn]), ergold[inn]);
+                red[0] = (double)f;
+            }
+            __syncthreads();
+            fdiff = (float)red[0];
+        } else {
+            part = warp_sum_d(part);
+            if ((tid & 31) == 0) red[tid >> 5] = part;
+            __syncthreads();
+            double t = 0.0;
+            for (int w = 0; w < MC_THREADS / 32; ++w) t += red[w];
+            fdiff = (float)t;
+        }
+        if (tid == 0) {
+            const int mt = D.mtype[im];
+            const float ediff = __fmul_rn(__fadd_rn(fdiff, 0.0f), temp);
+            float etest;
+            if (ediff <= 0.0f) etest = 10.0f;
+            else if (ediff < 20.0f) etest = exp_r(-ediff);
+            else etest = 0.0f;
+            const int acc = ran1_next(R) < etest;
+            if (acc) {
+                D.nstepreject[im] = 0;
+                fadd = __fadd_rn(fadd, fdiff);
+            } else {
+                D.nstepreject[im]++;
+                if (D.stepr > 0.0f) D.nwhole[nmt + mt]++;
+                if (D.stepm > 0.0f) D.nmovem[nmt + mt]++;
+            }
+            if (D.trace_den) D.trace_den[v] = fdiff;
+            if (D.trace_acc) D.trace_acc[v] = acc;
+            sh_acc = acc;
+        }
+        __syncthreads();
+        if (sh_acc) {
+            for (int inn = 1 + tid; inn < nn; inn += MC_THREADS) D.ergpair[D.ergpairref[row + inn] - 1] = ergnew[inn];
+            const int a0 = D.naf[im];
+            for (int k = tid; k < n; k += MC_THREADS) {
+                D.xa[a0 + k] = nx[k];
+                D.ya[a0 + k] = ny[k];
+                D.za[a0 + k] = nz[k];
+                D.pos[a0 + k] = mv[k];
+            }
+            if (tid == 0) {
+                D.xadd[im] = sh_cx;
+                D.yadd[im] = sh_cy;
+                D.zadd[im] = sh_cz;
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        // step adaptation (molfit.py:465-536); nmovei and ninter are 0 in this branch
+        if (D.ireset != 1) {
+            for (int t = 0; t < nmt; ++t) {
+                float it = __fmul_rn(D.interntrans[t], 1.0f);
+                if (it > D.trstepmax) it = D.trstepmax;
+                if (it < D.trstepmin && it != 0.0f) it = D.trstepmin;
+                D.interntrans[t] = it;
+                float ir = __fmul_rn(D.internrot[t], 1.0f);
+                if (ir > rotstepmax) ir = rotstepmax;
+                if (ir < rotstepmin && ir != 0.0f) ir = rotstepmin;
+                D.internrot[t] = ir;
+                float rat;
+                if (D.nwhole[nmt + t] > 0) {
+                    rat = __fdiv_rn(__fmul_rn(D.rejrate, (float)D.nwhole[t]), (float)D.nwhole[nmt + t]);
+                    if (rat > 1.1f) rat = 1.1f;
+                    if (rat < 0.9f) rat = 0.9f;
+                } else {
+                    rat = D.nwhole[t] > 0 ? 1.1f : 1.0f;
+                }
+                float wr = __fmul_rn(D.wholerot[t], rat);
+                if (wr > rotstepmax) wr = rotstepmax;
+                if (wr < rotstepmin && wr != 0.0f) wr = rotstepmin;
+                D.wholerot[t] = wr;
+                if (D.nmovem[nmt + t] > 0) {
+                    rat = __fdiv_rn(__fmul_rn(D.rejrate, (float)D.nmovem[t]), (float)D.nmovem[nmt + t]);
+                    if (rat > 1.1f) rat = 1.1f;
+                    if (rat < 0.9f) rat = 0.9f;
+                } else {
+                    rat = D.nmovem[t] > 0 ? 1.1f : 1.0f;
+                }
+                float wt = __fmul_rn(D.wholetrans[t], rat);
+                if (wt > D.trstepmax) wt = D.trstepmax;
+                if (wt < D.trstepmin && wt != 0.0f) wt = D.trstepmin;
+                D.wholetrans[t] = wt;
+            }
+        }
+        D.fadds[0] = __fadd_rn(D.fadds[0], __fdiv_rn(fadd, (float)D.nmol));
+        ran1_store(R, D.ran1);
+    }
+}
+
+// en_change for one molecule at its current coordinates (no move)
+__global__ void en_change_kernel(McDev D, int im, float *ergnew_out, float *fdiff_out) {
+    __shared__ double red[MC_THREADS / 32];
+    const int tid = threadIdx.x;
+    const size_t row = (size_t)im * D.M;
+    const int nn = D.nergpairm[im];
+    const int a0 = D.naf[im], n = D.nato[im];
+    for (int inn = 1 + tid; inn < nn; inn += blockDim.x) {
+        const int jm = D.molergpair[row + inn];
+        const int b0 = D.naf[jm], b1 = b0 + D.nato[jm];
+        float sume = 0.0f;
+        for (int ia = a0; ia < a0 + n; ++ia) {
+            const float4 p1 = D.pos[ia];
+            const int it = __float_as_int(p1.w);
+            for (int ja = b0; ja < b1; ++ja) {
+                const float4 p2 = D.pos[ja];
+                sume = __fadd_rn(sume, pair_energy(D.L, D.T, p1, p2,
+                                                   __ldg(D.npairref + it * D.ntype + __float_as_int(p2.w))));
+            }
+        }
+        ergnew_out[inn] = __fadd_rn(0.0f, sume);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        float f = 0.0f;
+        for (int inn = 1; inn < nn; ++inn)
+            f = __fsub_rn(__fadd_rn(f, ergnew_out[inn]), D.ergpair[D.ergpairref[row + inn] - 1]);
+        *fdiff_out = f;
+    }
+    (void)red;
+}
+
+__global__ void en_mole_pair_kernel(McDev D, const int32_t *im, const int32_t *jm, int n, float *out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = im[k], j = jm[k];
+    float sume = 0.0f;
+    for (int ia = D.naf[i]; ia < D.naf[i] + D.nato[i]; ++ia) {
+        const float4 p1 = D.pos[ia];
+        const int it = __float_as_int(p1.w);
+        for (int ja = D.naf[j]; ja < D.naf[j] + D.nato[j]; ++ja) {
+            const float4 p2 = D.pos[ja];
+            sume = __fadd_rn(sume, pair_energy(D.L, D.T, p1, p2, __ldg(D.npairref + it * D.ntype + __float_as_int(p2.w))));
+        }
+    }
+    out[k] = sume;
+}
+
+McDev make_mcdev(const epsr_box_t *b, const epsr_cells_t *c, const epsr_store_t *s) {
+    McDev D;
+    memset(&D, 0, sizeof(D));
+    D.L.cubic = b->cubic;
+    D.L.alatx = b->lat[0];
+    D.L.blatx = b->lat[1];
+    D.L.clatx = b->lat[2];
+    D.L.blaty = b->lat[3];
+    D.L.claty = b->lat[4];
+    D.L.clatz = b->lat[5];
+    D.T.tab = (const float4 *)b->tab;
+    D.T.xstar = b->xstar;
+    D.T.ld = b->ld;
+    D.T.npt2 = b->npt2;
+    D.T.izcut = b->izcut < b->npt2 ? b->izcut : b->npt2;
+    D.T.stepcl = b->stepcl;
+    D.nmol = b->nmol;
+    D.ntype = b->ntype;
+    D.nmoltype = b->nmoltype;
+    D.naf = b->naf;
+    D.nato = b->nato;
+    D.mtype = b->mtype;
+    D.npairref = b->npairref;
+    D.visit = c ? c->cell_mols : nullptr;
+    D.xa = b->xa;
+    D.ya = b->ya;
+    D.za = b->za;
+    D.xadd = b->xadd;
+    D.yadd = b->yadd;
+    D.zadd = b->zadd;
+    D.pos = (float4 *)b->pos;
+    if (s) {
+        D.M = s->nnbrefmax;
+        D.nergpairm = s->nergpairm;
+        D.molergpair = s->molergpair;
+        D.ergpairref = s->ergpairref;
+        D.ergpair = s->ergpair;
+    }
+    return D;
+}
+
+}  // namespace epsr
+
+using namespace epsr;
+
+extern "C" int64_t epsr_molfit_scratch_bytes(int32_t nmol, int32_t natom, int32_t M) {
+    (void)nmol;
+    (void)natom;
+    return (int64_t)sizeof(float) * 2 * (int64_t)(M > 0 ? M : 1) + 256;
+}
+
+static int check_box(const epsr_box_t *b, const char *who) {
+    if (!b || !b->naf || !b->nato || !b->itype || !b->pos || !b->tab || !b->xstar || !b->npairref) {
+        epsr_set_error("%s: box has null pointers", who);
+        return EPSR_ERR_ARG;
+    }
+    return EPSR_OK;
+}
+
+extern "C" int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
+                           void *scratch, int64_t scratch_bytes, void *stream) {
+    int rc = check_box(box, "epsr_molfit");
+    if (rc) return rc;
+    if (!cells || !store || !mc || !mc->wholerot || !mc->wholetrans || !mc->nwhole || !mc->nmovem ||
+        !mc->nstepreject || !mc->fadds || !mc->ran1 || !mc->internrot || !mc->interntrans) {
+        epsr_set_error("epsr_molfit: null pointer");
+        return EPSR_ERR_ARG;
+    }
+    McDev D = make_mcdev(box, cells, store);
+    D.simt = mc->simt;
+    D.rejrate = mc->rejrate;
+    D.stepr = mc->stepr;
+    D.stepm = mc->stepm;
+    D.trstepmax = mc->trstepmax;
+    D.trstepmin = mc->trstepmin;
+    D.ireset = mc->ireset;
+    D.strict = mc->strict;
+    D.wholerot = mc->wholerot;
+    D.wholetrans = mc->wholetrans;
+    D.internrot = mc->internrot;
+    D.interntrans = mc->interntrans;
+    D.nwhole = mc->nwhole;
+    D.nmovem = mc->nmovem;
+    D.nstepreject = mc->nstepreject;
+    D.fadds = mc->fadds;
+    D.ran1 = mc->ran1;
+    D.cos_override = mc->cos_override;
+    D.trace_den = mc->trace_den;
+    D.trace_acc = mc->trace_acc;
+    D.status = mc->status;
+    const size_t need = sizeof(float) * 2 * (size_t)(D.M > 0 ? D.M : 1);
+    size_t shm = 0;
+    if (need <= 160 * 1024) {
+        D.use_smem = 1;
+        shm = need;
+    } else {
+        if (!scratch || scratch_bytes < (int64_t)need) {
+            epsr_set_error("epsr_molfit: scratch needs %zu bytes", need);
+            return EPSR_ERR_CAPACITY;
+        }
+        D.use_smem = 0;
+        D.ergnew_g = (float *)scratch;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (shm > 48 * 1024)
+        EPSR_CUDA(cudaFuncSetAttribute(molfit_seq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    molfit_seq_kernel<<<1, MC_THREADS, shm, s>>>(D);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
+
+extern "C" int epsr_en_change(const epsr_box_t *box, const epsr_store_t *store, int32_t im, float *ergnew,
+                              float *out_host, void *stream) {
+    int rc = check_box(box, "epsr_en_change");
+    if (rc) return rc;
+    if (!store || !ergnew || !out_host || im < 0 || im >= box->nmol) {
+        epsr_set_error("epsr_en_change: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    McDev D = make_mcdev(box, nullptr, store);
+    cudaStream_t s = (cudaStream_t)stream;
+    float *d = nullptr;
+    EPSR_CUDA(cudaMallocAsync((void **)&d, sizeof(float), s));
+    en_change_kernel<<<1, 256, 0, s>>>(D, im, ergnew, d);
+    EPSR_CUDA(cudaGetLastError());
+    EPSR_CUDA(cudaMemcpyAsync(out_host, d, sizeof(float), cudaMemcpyDeviceToHost, s));
+    EPSR_CUDA(cudaFreeAsync(d, s));
+    EPSR_CUDA(cudaStreamSynchronize(s));
+    return EPSR_OK;
+}
+
+extern "C" int epsr_en_mole_pair(const epsr_box_t *box, const int32_t *im, const int32_t *jm, int32_t n, float *out,
+                                 void *stream) {
+    int rc = check_box(box, "epsr_en_mole_pair");
+    if (rc) return rc;
+    if (!im || !jm || !out || n < 0) {
+        epsr_set_error("epsr_en_mole_pair: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    if (n == 0) return EPSR_OK;
+    McDev D = make_mcdev(box, nullptr, nullptr);
+    en_mole_pair_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(D, im, jm, n, out);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}

@@ -1,0 +1,133 @@
+// transforms.cu -- gensq (epsr_standalone_rev3.py:4731-4802) and stog
+// (ato_manipulation_rev4.py:4067-4121) on the CUDA cores.
+//
+// Both are sums over one index with the other two free; the reference adds sequentially,
+// so each output is one thread's sequential float32 sum (bit-identical for gensq; stog
+// uses the double-evaluated sine, see common.cuh).  Consecutive threads take consecutive
+// Q (gensq) or r (stog) points so every table read is coalesced.
+#include "common.cuh"
+
+namespace epsr {
+
+__global__ void gensq_kernel(int nq, int npairs, int npt1, const float *wav, int ldw, const float *fq, long long sj,
+                             long long si, const float *ycoh, const int32_t *n2extr, const float *natomsphere,
+                             float *sofq) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int ic = blockIdx.y;
+    if (i > nq) return;
+    const float *w1 = wav + (size_t)ic * ldw;
+    const float *w2 = wav + (size_t)(npairs + ic) * ldw;
+    const float nsph = natomsphere[n2extr[ic]];
+    float sum1 = 0.0f, sum2 = 0.0f, sum3 = 0.0f;
+    for (int j = 2; j <= npt1; ++j) {
+        const float f = __ldg(fq + (long long)j * sj + (long long)i * si);
+        const float a1 = __ldg(w1 + j);
+        if (fabsf(a1) > 0.0f) sum1 = __fadd_rn(sum1, __fmul_rn(a1, f));
+        const float b = __ldg(w2 + j);
+        const float a2 = __fmul_rn(__fsub_rn(b, __ldg(ycoh + j)), nsph);
+        sum2 = __fadd_rn(sum2, __fmul_rn(a2, f));
+        sum3 = __fadd_rn(sum3, b);
+    }
+    if (sum3 <= 0.0f) sum2 = 0.0f;
+    sofq[(size_t)ic * (nq + 1) + i] = sum1;
+    sofq[(size_t)(npairs + ic) * (nq + 1) + i] = sum2;
+}
+
+// lorch(x) for every (pair, Q) (ato_manipulation_rev4.py:4113-4121): it depends on the pair
+// only through qmax, so it is tabulated once instead of once per r point.
+__global__ void lorch_kernel(const float *q, int ldq, int npairs, const int32_t *nqmax, float *lw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int in = blockIdx.y;
+    if (i >= ldq) return;
+    const float pi = 3.14159265358979323846f;
+    const float qmax = __fdiv_rn(pi, q[nqmax[in]]);
+    const float x = __fmul_rn(qmax, q[i]);
+    float r;
+    if (x == 0.0f) r = 1.0f;
+    else if (x < pi) r = __fdiv_rn(sin_r(x), x);
+    else r = 0.0f;
+    lw[(size_t)in * ldq + i] = r;
+}
+
+__global__ void stog_kernel(float sfac, const float *q, int ldq, const float *sofq, const float *r, int nr, int npairs,
+                            const int32_t *nqmin, const int32_t *nqmax, const float *xwt, const float *lw,
+                            float *gofr) {
+    const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int in = blockIdx.y;
+    if (j > nr) return;
+    const float rr = r[j];
+    const float *s = sofq + (size_t)in * ldq;
+    const float *l = lw + (size_t)in * ldq;
+    float sumi = 0.0f;
+    const int i0 = nqmin[in], i1 = nqmax[in];
+    if (rr > 0.0f) {
+        for (int i = i0; i <= i1; ++i) {
+            const float qq = __ldg(q + i);
+            const float prod = __fmul_rn(__fmul_rn(qq, sin_r(__fmul_rn(qq, rr))), __ldg(l + i));
+            sumi = __fadd_rn(sumi, __fmul_rn(__ldg(s + i), prod));
+        }
+        gofr[(size_t)in * (nr + 1) + j] = __fadd_rn(xwt[in], __fdiv_rn(__fmul_rn(sfac, sumi), rr));
+    } else {
+        for (int i = i0; i <= i1; ++i) {
+            const float qq = __ldg(q + i);
+            const float prod = __fmul_rn(__fmul_rn(qq, qq), __ldg(l + i));
+            sumi = __fadd_rn(sumi, __fmul_rn(__ldg(s + i), prod));
+        }
+        gofr[(size_t)in * (nr + 1) + j] = __fadd_rn(xwt[in], __fmul_rn(sfac, sumi));
+    }
+}
+
+}  // namespace epsr
+
+using namespace epsr;
+
+extern "C" int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float *wav, int32_t ldw, const float *foqols,
+                          int64_t sj, int64_t si, const float *ycoh, const int32_t *n2extr, const float *natomsphere,
+                          float *sofq, void *stream) {
+    if (!wav || !foqols || !ycoh || !n2extr || !natomsphere || !sofq || nq <= 0 || npairs <= 0 || npt1 + 1 > ldw) {
+        epsr_set_error("epsr_gensq: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    dim3 grid((nq + 127) / 128, npairs);
+    gensq_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(nq, npairs, npt1, wav, ldw, foqols, sj, si, ycoh, n2extr,
+                                                         natomsphere, sofq);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
+
+extern "C" int epsr_stog(float rho, const float *q, int32_t ldq, const float *sofq, const float *r, int32_t nr,
+                         int32_t npairs, const int32_t *nqmin_h, const int32_t *nqmax_h, const float *xwt, float *gofr,
+                         void *stream) {
+    if (!q || !sofq || !r || !nqmin_h || !nqmax_h || !xwt || !gofr || ldq < 5 || nr <= 0 || npairs <= 0) {
+        epsr_set_error("epsr_stog: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    for (int in = 0; in < npairs; ++in)
+        if (nqmin_h[in] < 1 || nqmax_h[in] >= ldq || nqmax_h[in] < 1) {
+            epsr_set_error("epsr_stog: nqmin/nqmax out of range for pair %d", in);
+            return EPSR_ERR_ARG;
+        }
+    cudaStream_t s = (cudaStream_t)stream;
+    float qh[2];
+    EPSR_CUDA(cudaMemcpyAsync(qh, q + 3, sizeof(qh), cudaMemcpyDeviceToHost, s));
+    EPSR_CUDA(cudaStreamSynchronize(s));
+    const float pi = 3.14159265358979323846f;
+    volatile float qstep = qh[1] - qh[0];
+    volatile float t1 = 0.5f * qstep;
+    volatile float t2 = t1 / pi;
+    volatile float t3 = t2 / pi;
+    const float sfac = t3 / rho;
+    int32_t *d_lim = nullptr;
+    float *lw = nullptr;
+    EPSR_CUDA(cudaMallocAsync((void **)&d_lim, sizeof(int32_t) * 2 * npairs, s));
+    EPSR_CUDA(cudaMallocAsync((void **)&lw, sizeof(float) * (size_t)npairs * ldq, s));
+    EPSR_CUDA(cudaMemcpyAsync(d_lim, nqmin_h, sizeof(int32_t) * npairs, cudaMemcpyHostToDevice, s));
+    EPSR_CUDA(cudaMemcpyAsync(d_lim + npairs, nqmax_h, sizeof(int32_t) * npairs, cudaMemcpyHostToDevice, s));
+    lorch_kernel<<<dim3((ldq + 127) / 128, npairs), 128, 0, s>>>(q, ldq, npairs, d_lim + npairs, lw);
+    stog_kernel<<<dim3((nr + 127) / 128, npairs), 128, 0, s>>>(sfac, q, ldq, sofq, r, nr, npairs, d_lim, d_lim + npairs,
+                                                               xwt, lw, gofr);
+    EPSR_CUDA(cudaGetLastError());
+    EPSR_CUDA(cudaFreeAsync(lw, s));
+    EPSR_CUDA(cudaFreeAsync(d_lim, s));
+    return EPSR_OK;
+}

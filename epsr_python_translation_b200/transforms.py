@@ -1,0 +1,74 @@
+"""Device calls for gensq, stog and fit_expansion on PyTorch tensors (C ABI wrappers)."""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+
+f32 = np.float32
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _s():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev(a, dtype=torch.float32):
+    if isinstance(a, torch.Tensor):
+        return a.to(device="cuda", dtype=dtype).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def gensq(nq, npt1, wav, ldw, foqols, sj, si, ycoh, n2extr, natomsphere, npairs):
+    """gensq epsr_standalone_rev3.py:4731.  wav (device, 2*npairs*ldw); foqols with strides
+    (sj, si) for (r index, Q index).  Returns sofq (device, 2*npairs*(nq+1))."""
+    lib = _lib.load(require_device=True)
+    out = torch.zeros(2 * npairs * (nq + 1), dtype=torch.float32, device="cuda")
+    fq = _dev(foqols)
+    yc = _dev(ycoh)
+    n2 = _dev(n2extr, torch.int32)
+    ns = _dev(natomsphere)
+    check(lib.epsr_gensq(nq, npairs, npt1, _p(wav), ldw, _p(fq), sj, si, _p(yc), _p(n2), _p(ns), _p(out), _s()))
+    return out
+
+
+def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
+    """stog ato_manipulation_rev4.py:4067.  q (ldq,), sofq_pairs (npairs, ldq), r (nr+1,)."""
+    lib = _lib.load(require_device=True)
+    npairs, ldq = sofq_pairs.shape
+    nr = r.shape[0] - 1
+    qd, sd, rd, xd = _dev(q), _dev(sofq_pairs), _dev(r), _dev(xwt)
+    out = torch.zeros(npairs * (nr + 1), dtype=torch.float32, device="cuda")
+    nqmin = np.ascontiguousarray(nqmin, np.int32)
+    nqmax = np.ascontiguousarray(nqmax, np.int32)
+    check(lib.epsr_stog(float(f32(rho)), _p(qd), ldq, _p(sd), _p(rd), nr, npairs, nqmin.ctypes.data_as(C.c_void_p),
+                        nqmax.ctypes.data_as(C.c_void_p), _p(xd), _p(out), _s()))
+    return out.view(npairs, nr + 1)
+
+
+def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1_t, acceptr=0.0,
+                  rejrat=0.0, chisqnew=0.0):
+    """fit_expansion epsr_standalone_rev3.py:4806 (1-based arrays).  ran1_t: device int32[35]."""
+    lib = _lib.load(require_device=True)
+    y = _dev(yin)
+    e = _dev(expr)
+    wt = torch.zeros(nterms + 1, dtype=torch.float32, device="cuda")
+    wto = _dev(wtold).clone()
+    yout = torch.zeros(npt + 1, dtype=torch.float32, device="cuda")
+    scal = np.array([stepr, acceptr, rejrat, chisqnew], f32)
+    nb = lib.epsr_fit_expansion_scratch_bytes(npt, nterms)
+    scr = torch.empty(int(nb), dtype=torch.uint8, device="cuda")
+    trials = np.zeros(1, np.int64)
+    check(lib.epsr_fit_expansion(_p(y), _p(e), _p(yout), _p(wt), _p(wto), scal.ctypes.data_as(C.c_void_p), nmin, npt,
+                                 ncfirst, nterms, nits, nfreq, _p(ran1_t), _p(scr), scr.numel(),
+                                 trials.ctypes.data_as(C.c_void_p), _s()))
+    return dict(wt=wt, wtold=wto, yout=yout, stepr=f32(scal[0]), acceptr=f32(scal[1]), rejrat=f32(scal[2]),
+                chisq=f32(scal[3]), trials=int(trials[0]))

@@ -1,0 +1,210 @@
+/*
+ * epsr_gpu.h -- C ABI of the B200 (sm_100a) EPSR minimum-image pair path.
+ *
+ * Every entry point takes device pointers and sizes, a CUDA stream (as void*, NULL = the
+ * legacy default stream) and returns an int status: 0 on success, >0 on an error (text via
+ * epsr_last_error()).  No C++ or framework types cross this boundary.  Calls are
+ * asynchronous on the given stream unless stated otherwise; the reference's routines are
+ * synchronous, so the host bindings synchronise before returning to the reference loop.
+ *
+ * Index conventions: molecules, atoms, types and pairs are 0-based.  The r-grid index iz
+ * and the Q index keep the reference's 1-based meaning: tables are [pair][ld] with iz in
+ * 1..npt (element 0 unused) because the bin arithmetic ifix(d/stepcl)+2 depends on it.
+ * Coordinates are float32 box-fraction units (x_A/dmax) as in the reference.
+ *
+ * Each declaration names the reference routine (IzzyRodger-edb/EPSR_python_translation,
+ * package src/epsr26) it replaces.
+ */
+#ifndef EPSR_GPU_H
+#define EPSR_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EPSR_OK 0
+#define EPSR_ERR_ARG 1        /* bad argument (null pointer, size out of range) */
+#define EPSR_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define EPSR_ERR_CAPACITY 3   /* a caller-sized buffer is too small */
+#define EPSR_ERR_UNSUPPORTED 4/* a feature outside the pair path (see epsr_last_error) */
+#define EPSR_ERR_TIMEOUT 5    /* a bounded device wait gave up */
+
+/* ------------------------------------------------------------------ shared structs */
+
+/* One periodic box.  All pointers are device pointers. */
+typedef struct {
+    int32_t nmol, natom, ntype, npairs, nmoltype;
+    const int32_t *naf;      /* [nmol] first atom of each molecule */
+    const int32_t *nato;     /* [nmol] atoms per molecule */
+    const int32_t *mtype;    /* [nmol] molecule type */
+    const int32_t *itype;    /* [natom] atom type */
+    float *xa, *ya, *za;     /* [natom] atom offsets from the molecule centre */
+    float *xadd, *yadd, *zadd; /* [nmol] molecule centres */
+    float *pos;              /* [4*natom] scratch: absolute positions (xa+xadd, ..., type bits) */
+    const int32_t *npairref; /* [ntype*ntype] pair index of a type pair */
+    const float *xstar;      /* [ld] r grid / dmax, 1-based */
+    const float *tab;        /* [4*npairs*ld] packed {xavs, xavs1, ecoul, ecoul1} per (pair, iz) */
+    int32_t ld;              /* table leading dimension (npt+1) */
+    int32_t npt2;            /* last usable table index (epsr16.npt2) */
+    int32_t izcut;           /* last iz at which any table entry is nonzero (<= npt2) */
+    float stepcl;            /* cellst/dmax */
+    int32_t cubic;           /* 1: cubic minimum image; 0: triclinic via lat */
+    float lat[6];            /* alatx, blatx, clatx, blaty, claty, clatz (box units) */
+} epsr_box_t;
+
+/* Cell list (CSR).  cell_mols in cell order is also the molfit visit order. */
+typedef struct {
+    int32_t ncelldiva, ncelldivb, ncelldivc, ncell, ncellneighb, maxcellno;
+    int32_t *molcellno;   /* [nmol] 1-based cell number (atomcellno) */
+    int32_t *cell_start;  /* [ncell+1] */
+    int32_t *cell_mols;   /* [nmol] */
+    int32_t *offsets;     /* [3*ncell] (ia, ib, ic) neighbour-cell offsets, first ncellneighb used */
+} epsr_cells_t;
+
+/* Pair-energy store of module ergpairreference (ergpairreference.py:63-210). */
+typedef struct {
+    int32_t nnbrefmax;    /* slots per molecule (M) */
+    int32_t capacity;     /* size of ergpair */
+    int32_t *nergpairm;   /* [nmol] used slots */
+    int32_t *molergpair;  /* [nmol*M] partner molecule of each slot */
+    int32_t *ergpairref;  /* [nmol*M] 1-based index into ergpair */
+    float *ergpair;       /* [capacity] shared pair energies */
+    int32_t *nergpair;    /* [1] device counter: entries used */
+} epsr_store_t;
+
+/* ------------------------------------------------------------------ lifecycle / info */
+
+/* Text of the last error on this host thread (static storage). */
+const char *epsr_last_error(void);
+/* Library version string. */
+const char *epsr_version(void);
+/* Number of sm_100 devices visible; <0 if the runtime failed. */
+int epsr_device_count(void);
+
+/* ------------------------------------------------------------------ ran1 */
+/* ran1 auxiliary_routines.py:324-391.  state: device int32[35] = idum, iy, mcall, iv[32].
+ * Writes n deviates to out (device) and advances the state by exactly n draws. */
+int epsr_ran1_fill(int32_t *state, float *out, int64_t n, void *stream);
+
+/* ------------------------------------------------------------------ cell list */
+/* Host-only size computation of initialise_cellneighbourlist cellneighbourlist.py:36-44:
+ * dims[4] = ncelldiva, ncelldivb, ncelldivc, ncell. lat6 as in epsr_box_t.lat. */
+int epsr_cell_dims(int32_t nmolcell, int32_t nmol, const float *lat6_host, int32_t *dims_host);
+
+/* initialise_cellneighbourlist cellneighbourlist.py:23-90 + makecellneighbourlist :97-183.
+ * Counting sort of molecule centres into cells (stable: molecule order within a cell) and
+ * the neighbour-cell offsets within rmax.  cells->cell_start/cell_mols/molcellno/offsets are
+ * caller-allocated (sizes from epsr_cell_dims); scalar fields are written back on the host
+ * (the call synchronises the stream).  lat9 = alatc[3], blatc[3], clatc[3] (host). */
+int epsr_cell_list(const float *xadd, const float *yadd, const float *zadd, int32_t nmol, int32_t nmolcell,
+                   float rmax, const float *lat6_host, const float *lat9_host, epsr_cells_t *cells,
+                   int32_t *scratch_i32, int64_t scratch_len, void *stream);
+
+/* get_nnbrefmax cellneighbourlist.py:211-233 (synchronous; returns the value via out). */
+int epsr_nnbrefmax(const epsr_cells_t *cells, int32_t *out_host, void *stream);
+
+/* ------------------------------------------------------------------ positions */
+/* Refresh box->pos from xa/ya/za + xadd/yadd/zadd (the float adds of en_change
+ * molfit.py:855-857).  Call after any host upload of coordinates. */
+int epsr_box_positions(const epsr_box_t *box, void *stream);
+
+/* ------------------------------------------------------------------ fmolec1 */
+/* fmolec1 ato_manipulation_rev4.py:2374-2528 (intra energies given, no three-body /
+ * coordination / container terms): builds the pair store exactly as the reference
+ * (intra slot first when nonzero, pairs in cell-visit order, the second-neighbour start of
+ * the store loop).  eintra: [nmol] en_mole_intra values.  scratch: device bytes (size from
+ * epsr_fmolec1_scratch_bytes).  out2_host[2] = {ftest, ftestb} per molecule.
+ * strict=1 sums ftest/ftestb sequentially in the reference's order (bit-identical);
+ * strict=0 sums in double.  Synchronous. */
+int64_t epsr_fmolec1_scratch_bytes(int32_t nmol, int32_t ncell, int32_t nnbrefmax);
+int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, const float *eintra, epsr_store_t *store,
+                 void *scratch, int64_t scratch_bytes, int32_t strict, float *out2_host, void *stream);
+
+/* ------------------------------------------------------------------ molfit */
+/* Step sizes, counters and Metropolis parameters of one molfit cycle. */
+typedef struct {
+    float simt, rejrate, stepr, stepm, trstepmax, trstepmin;
+    int32_t ireset;
+    float *wholerot, *wholetrans;   /* [nmoltype] device, updated */
+    float *internrot, *interntrans; /* [nmoltype] device, updated (clamped only) */
+    int32_t *nwhole, *nmovem;       /* [2*nmoltype] device: tries then rejections */
+    int32_t *nstepreject;           /* [nmol] device */
+    float *fadds;                   /* [1] device, updated: fadds += sum(accepted dE)/nmol */
+    int32_t *ran1;                  /* [35] device ran1 state */
+    const float *cos_override;      /* NULL, or [3*nmol] cos values to use instead of the
+                                       device cosine (test hook for bit-identity) */
+    float *trace_den;               /* NULL or [nmol]: en_change value per move */
+    int32_t *trace_acc;             /* NULL or [nmol]: 1 accepted, 0 rejected */
+    int32_t strict;                 /* 1: en_change summed in list order (bit-identical);
+                                       0: summed in double */
+    int32_t *status;                /* [1] device: 0 ok, 1 a molecule exceeds 64 atoms */
+} epsr_mc_t;
+
+/* molfit molfit.py:52-541, whole-molecule branch (:268-448) and step adaptation
+ * (:465-536): every molecule gets rotatm (:672) + movem (:733), en_change (:806) and the
+ * Metropolis test (:401-408) in cell-visit order.  Unsupported (error 4): internal
+ * rotations (ngrot>0 with stepri>0), shake cycles (nisum>=intra), tethering, three-body,
+ * coordination constraints, container forces, coarse graining -- the host refuses those.
+ * scratch: device bytes from epsr_molfit_scratch_bytes. */
+int64_t epsr_molfit_scratch_bytes(int32_t nmol, int32_t natom, int32_t nnbrefmax);
+int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
+                void *scratch, int64_t scratch_bytes, void *stream);
+
+/* en_change molfit.py:806-919 for one molecule at its current coordinates against its
+ * stored list (ergnew out [nnbrefmax], device); *out_host = dE.  Synchronous. */
+int epsr_en_change(const epsr_box_t *box, const epsr_store_t *store, int32_t im, float *ergnew, float *out_host,
+                   void *stream);
+
+/* en_mole_pair molfit.py:1528-1578 for n (im, jm) pairs: out[k] = E(im[k], jm[k]). */
+int epsr_en_mole_pair(const epsr_box_t *box, const int32_t *im, const int32_t *jm, int32_t n, float *out,
+                      void *stream);
+
+/* ------------------------------------------------------------------ atogen */
+/* atogen ato_manipulation_rev4.py:3640-3899 (no coarse graining, no container forces).
+ * wav: device [2*npairs*ldw] (wav(1,iz,ic) at [ic*ldw+iz], wav(2,..) at [(npairs+ic)*ldw+iz]),
+ * potex [npairs]; counts: device uint64 [2*npairs*ldw + npairs] integer histogram scratch
+ * (zeroed inside).  rminex [npairs] (already through irefpcof), cfrac [ntype], ycoh [ldw].
+ * ran1: device state (one draw per origin candidate, as the reference).
+ * *ngrsamples_io (host) in/out as the reference's argument.  Synchronous. */
+int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor, float dmax, const float *rminex,
+                const float *cfrac, const float *ycoh, const int32_t *n1extr, const int32_t *n2extr,
+                int32_t natomr, int32_t *ngrsamples_io, int32_t *ran1, float *wav, int32_t ldw, float *potex,
+                unsigned long long *counts, void *scratch, int64_t scratch_bytes, void *stream);
+int64_t epsr_atogen_scratch_bytes(int32_t nmol, int32_t natom, int32_t nmoltype, int32_t ntype);
+/* pair-updates counted by the last epsr_atogen call on this thread */
+int64_t epsr_atogen_last_pair_updates(void);
+
+/* ------------------------------------------------------------------ gensq / stog */
+/* gensq epsr_standalone_rev3.py:4731-4802.  fq(j,i) = foqols[j*fq_sj + i*fq_si] (j = r
+ * index 1..npt1, i = Q index 1..nq).  sofq out [2*npairs*(nq+1)]: sofq(1,i,ic) at
+ * [ic*(nq+1)+i], sofq(2,i,ic) at [(npairs+ic)*(nq+1)+i]. natomsphere [ntype]. */
+int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float *wav, int32_t ldw, const float *foqols,
+               int64_t fq_sj, int64_t fq_si, const float *ycoh, const int32_t *n2extr, const float *natomsphere,
+               float *sofq, void *stream);
+
+/* stog ato_manipulation_rev4.py:4067-4121 (+ lorch :4113).  q [ldq] 1-based, sofq
+ * [npairs*ldq] (sofq(i,in) at [in*ldq+i]), r [nr+1] 1-based, gofr out [npairs*(nr+1)],
+ * nqmin/nqmax/xwt [npairs].  rho, qstep-derived constants as the reference. */
+int epsr_stog(float rho, const float *q, int32_t ldq, const float *sofq, const float *r, int32_t nr,
+              int32_t npairs, const int32_t *nqmin_host, const int32_t *nqmax_host, const float *xwt, float *gofr,
+              void *stream);
+
+/* ------------------------------------------------------------------ fit_expansion */
+/* fit_expansion epsr_standalone_rev3.py:4806-4921 (+ expand :4924, smoop
+ * auxiliary_routines.py:744).  yin [npt+1], expr [npt*nterms+1] (1-based flat, row-major by
+ * Q row as the reference), yout [npt+1], wt/wtold [nterms+1] (device, 1-based).
+ * scal_host[4] in/out = {stepr, acceptr, rejrat, chisqnew}; returns trials via
+ * *trials_host.  ran1: device state.  Synchronous. */
+int epsr_fit_expansion(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
+                       float *scal_host, int32_t nmin, int32_t npt, int32_t ncfirst, int32_t nterms, int32_t nits,
+                       int32_t nfreq, int32_t *ran1, void *scratch, int64_t scratch_bytes, int64_t *trials_host,
+                       void *stream);
+int64_t epsr_fit_expansion_scratch_bytes(int32_t npt, int32_t nterms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EPSR_GPU_H */

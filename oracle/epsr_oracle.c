@@ -445,7 +445,47 @@ typedef struct {
     int32_t *acc;    /* [nmol] */
     float *cosv;     /* [3*nmol] cos values used (glibc cosf), or NULL */
     int32_t ncos;
+    double *den64;   /* [nmol] FP64 energy change of the proposed move, or NULL */
+    double *scale64; /* [nmol] sum of |FP64 pair energies| before and after the move */
 } oracle_trace;
+
+/* FP64 restatement of en_atom_inter_scale (molfit.py:1251-1279): the same tables and bin
+ * rule evaluated in double precision; the interpolation is continuous across bins, so it
+ * is the reference value the float32 energies are checked against. */
+static double en_atom_inter64(const oracle_sys *S, double x1, double y1, double z1, double x2, double y2,
+                              double z2, int icref) {
+    double xd = x2 - x1, yd = y2 - y1, zd = z2 - z1;
+    xd -= round(xd);
+    yd -= round(yd);
+    zd -= round(zd);
+    double d = sqrt(xd * xd + yd * yd + zd * zd);
+    int iz = (int)(d / (double)S->stepcl) + 2;
+    if (iz > S->npt2) return 0.0;
+    const size_t base = (size_t)icref * (size_t)S->ld;
+    double dt = d - (double)S->xstar[iz];
+    return (double)S->xavs[base + iz] + (double)S->xavs1[base + iz] * dt + (double)S->ecoul[base + iz] +
+           (double)S->ecoul1[base + iz] * dt;
+}
+
+/* FP64 energy of molecule im (atom offsets xo/yo/zo, centre cx/cy/cz) with molecule jm. */
+static double en_mole_pair64(const oracle_sys *S, int im, const float *xo, const float *yo, const float *zo,
+                             float cx, float cy, float cz, int jm, double *absum) {
+    double e = 0.0;
+    const int n = S->nato[im];
+    const int b0 = S->naf[jm], b1 = b0 + S->nato[jm];
+    for (int k = 0; k < n; ++k) {
+        const int it = S->itype[S->naf[im] + k];
+        const double x1 = (double)xo[k] + cx, y1 = (double)yo[k] + cy, z1 = (double)zo[k] + cz;
+        for (int ja = b0; ja < b1; ++ja) {
+            const int icref = S->npairref[it * S->ntype + S->itype[ja]];
+            double v = en_atom_inter64(S, x1, y1, z1, (double)S->xa[ja] + S->xadd[jm], (double)S->ya[ja] + S->yadd[jm],
+                                       (double)S->za[ja] + S->zadd[jm], icref);
+            e += v;
+            *absum += fabs(v);
+        }
+    }
+    return e;
+}
 
 static float en_change(const oracle_sys *S, int im, const oracle_store *E, float *ergnew) {
     const int M = E->nnbrefmax;
@@ -551,6 +591,18 @@ int oracle_molfit(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_
                 P->wholetrans[mt] = movem(S, im, P->wholetrans[mt], R);
             } else {
                 P->wholetrans[mt] = 0.0f;
+            }
+            if (T && T->den64) {
+                double sc = 0.0, dn = 0.0;
+                const int32_t *nb = E->molergpair + (size_t)im * M;
+                for (int inn = 1; inn < E->nergpairm[im]; ++inn) {
+                    const int jm = nb[inn];
+                    dn += en_mole_pair64(S, im, S->xa + a0, S->ya + a0, S->za + a0, S->xadd[im], S->yadd[im],
+                                         S->zadd[im], jm, &sc);
+                    dn -= en_mole_pair64(S, im, xr, yr, zr, xs, ys, zs, jm, &sc);
+                }
+                T->den64[T->nmoves] = dn;
+                T->scale64[T->nmoves] = sc;
             }
             float fdiff = en_change(S, im, E, ergnew);
             float ediff = (fdiff + 0.0f) * temp;

@@ -93,7 +93,8 @@ class McParC(C.Structure):
 
 
 class TraceC(C.Structure):
-    _fields_ = [("nmoves", C.c_int32), ("im", P), ("den", P), ("acc", P), ("cosv", P), ("ncos", C.c_int32)]
+    _fields_ = [("nmoves", C.c_int32), ("im", P), ("den", P), ("acc", P), ("cosv", P), ("ncos", C.c_int32),
+                ("den64", P), ("scale64", P)]
 
 
 class SysHandle:
@@ -234,8 +235,10 @@ def molfit(box, cells, st, mc, ran1, fadds=0.0, record_cos=True):
     par.nwhole, par.nmovem = ptr(mc["nwhole"]), ptr(mc["nmovem"])
     par.nstepreject, par.ngrot = ptr(mc["nstepreject"]), ptr(mc["ngrot"])
     tr = dict(im=np.zeros(box.nmol, np.int32), den=np.zeros(box.nmol, f32), acc=np.zeros(box.nmol, np.int32),
-              cosv=np.zeros(3 * box.nmol, f32) if record_cos else None)
+              cosv=np.zeros(3 * box.nmol, f32) if record_cos else None,
+              den64=np.zeros(box.nmol, np.float64), scale64=np.zeros(box.nmol, np.float64))
     T = TraceC()
+    T.den64, T.scale64 = ptr(tr["den64"]), ptr(tr["scale64"])
     T.im, T.den, T.acc = ptr(tr["im"]), ptr(tr["den"]), ptr(tr["acc"])
     T.cosv = ptr(tr["cosv"]) if record_cos else None
     r = Ran1C.of(ran1)

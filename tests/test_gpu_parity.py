@@ -1,0 +1,304 @@
+"""Device path vs the reference's golden vectors and the C oracle (needs a B200).
+
+Bit-identical where the reference's arithmetic has no transcendental (ran1, cell list,
+pair store, energies, histograms, gensq); the Monte Carlo chain is bit-identical when the
+reference's own cosines are injected, and otherwise checked against an FP64 restatement
+with the north-star tolerance (1e-5 relative to the energy scale of the move).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from epsr_python_translation_b200.box import BoxArrays, Ran1State, trsteps
+from oracle import oracle
+from tests import goldens
+from tests.goldens import assert_bits_equal
+
+pytestmark = pytest.mark.gpu
+f32 = np.float32
+
+ENERGY_RTOL = 1e-5   # relative to the sum of |pair energies| of the move
+
+
+def _device(box):
+    from epsr_python_translation_b200.device import DeviceBox
+    return DeviceBox(box)
+
+
+def _prepare(case, strict=True):
+    z = goldens.load(case)
+    box = BoxArrays.from_golden(z)
+    d = _device(box)
+    d.cell_list(int(z["in_nmolcell"]), f32(z["in_sepmax"]))
+    d.fmolec1(z["in_eintra"], strict=strict)
+    return z, box, d
+
+
+# ----------------------------------------------------------------------------- ran1
+def test_ran1_device_matches_gfortran_blocks():
+    from epsr_python_translation_b200.device import DeviceBox  # noqa: F401  (loads the library)
+    from epsr_python_translation_b200 import _lib
+    _lib.load(require_device=True)
+    z = np.load(goldens.GOLDEN + "/ran1_reference.npz")
+    st = None
+    for k in range(int(z["nblocks"])):
+        head = str(z[f"block{k}_header"])
+        if head.startswith("seed"):
+            st = torch.from_numpy(Ran1State(idum=int(head.split()[1])).as_array()).cuda()
+        out = torch.empty(1000, dtype=torch.float32, device="cuda")
+        import ctypes as C
+        _lib.check(_lib.load().epsr_ran1_fill(C.c_void_p(st.data_ptr()), C.c_void_p(out.data_ptr()), 1000, None))
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), z[f"block{k}_bits"]), head
+        s = st.cpu().numpy()
+        state = z[f"block{k}_state"]
+        assert [int(s[2]), int(s[0]), int(s[1])] == [int(v) for v in state[:3]], head
+        assert np.array_equal(s[3:35], state[3:35].astype(np.int32)), head
+
+
+@pytest.mark.parametrize("n", [1, 31, 32, 33, 1000, 100003])
+def test_ran1_device_lengths_match_oracle(n):
+    from epsr_python_translation_b200.device import DeviceBox
+    z = goldens.load("c1_water")
+    d = DeviceBox(BoxArrays.from_golden(z))
+    st0 = Ran1State.from_golden(z, "mf_ran1_before_")
+    t = d.ran1_tensor(st0)
+    vals = d.ran1_fill(t, n)
+    ref, rst = oracle.ran1_fill(st0, n)
+    assert np.array_equal(vals.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(t.cpu().numpy(), rst.as_array())
+
+
+# ----------------------------------------------------------------------------- cells + store
+@pytest.mark.parametrize("case", goldens.CASES)
+def test_cell_list_device_matches_reference(case):
+    z = goldens.load(case)
+    d = _device(BoxArrays.from_golden(z))
+    d.cell_list(int(z["in_nmolcell"]), f32(z["in_sepmax"]))
+    c = d.download_cells()
+    for k in ("ncelldiva", "ncelldivb", "ncelldivc", "ncell", "maxcellno", "ncellneighb"):
+        assert c[k] == int(z["cell_" + k]), k
+    start, flat = goldens.golden_cells_csr(z)
+    assert np.array_equal(c["cell_start"], start)
+    assert np.array_equal(c["cell_mols"], flat)
+    assert np.array_equal(c["molcellno"], z["cell_molcellno"])
+    assert np.array_equal(c["offsets"][:, 0], z["cell_iacellneighb"])
+    assert np.array_equal(c["offsets"][:, 1], z["cell_ibcellneighb"])
+    assert np.array_equal(c["offsets"][:, 2], z["cell_iccellneighb"])
+    assert c["nnbrefmax"] == int(z["fm_nnbrefmax"])
+
+
+@pytest.mark.parametrize("case", goldens.CASES)
+def test_fmolec1_device_store_matches_reference(case):
+    z, box, d = _prepare(case)
+    st = d.download_store()
+    assert st["nergpair"] == int(z["fm_nergpair"])
+    assert np.array_equal(st["nergpairm"], z["fm_nergpairm"])
+    for im in range(box.nmol):
+        k = st["nergpairm"][im]
+        assert np.array_equal(st["molergpair"][im, :k], z["fm_molergpair"][:k, im] - 1), im
+        assert np.array_equal(st["ergpairref"][im, :k], z["fm_ergpairref"][:k, im]), im
+    assert_bits_equal(st["ergpair"], z["fm_ergpair"], "ergpair")
+
+
+def test_fmolec1_device_sums_strict_and_fast():
+    z = goldens.load("c2_mixture")
+    box = BoxArrays.from_golden(z)
+    d = _device(box)
+    d.cell_list(int(z["in_nmolcell"]), f32(z["in_sepmax"]))
+    ft, fb = d.fmolec1(z["in_eintra"], strict=True)
+    assert_bits_equal(ft, z["fm_ftest"], "ftest")
+    assert_bits_equal(fb, z["fm_ftestb"], "ftestb")
+    ft2, fb2 = d.fmolec1(z["in_eintra"], strict=False)
+    assert abs(float(ft2) - float(ft)) <= 1e-5 * max(1.0, abs(float(ft)))
+
+
+# ----------------------------------------------------------------------------- molfit
+def _mc(d, z, box):
+    tmax, tmin = trsteps(box.natomr)
+    nmt = box.nmoltype
+    d.mc_setup(rejrate=f32(z["in_rejrate"]), stepr=f32(z["in_stepr"]), stepm=f32(z["in_stepm"]),
+               wholerot=z["in_wholerot"], wholetrans=z["in_wholetrans"], internrot=np.zeros(nmt, f32),
+               interntrans=np.zeros(nmt, f32), ran1=Ran1State.from_golden(z, "mf_ran1_before_"), trstepmax=tmax,
+               trstepmin=tmin)
+
+
+@pytest.mark.parametrize("case", goldens.CASES)
+def test_molfit_device_bit_identical_with_reference_cosines(case):
+    """With the reference's own cosf values injected, every coordinate, stored energy, step
+    size, counter and the ran1 state match the reference bit for bit."""
+    z, box, d = _prepare(case)
+    _mc(d, z, box)
+    for cyc in range(int(z["mf_cycles"])):
+        p = f"mf{cyc}_"
+        d.molfit(strict=True, cos_override=z[p + "cos"])
+        m = d.download_mc()
+        assert_bits_equal(m["den"], z[p + "den"], p + "den")
+        co = d.download_coords()
+        for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+            assert_bits_equal(co[k], z[p + k], p + k)
+        st = d.download_store()
+        assert_bits_equal(st["ergpair"], z[p + "ergpair"], p + "ergpair")
+        assert_bits_equal(m["wholerot"], z[p + "wholerot"], p + "wholerot")
+        assert_bits_equal(m["wholetrans"], z[p + "wholetrans"], p + "wholetrans")
+        assert np.array_equal(m["nwhole"], z[p + "nwhole"])
+        assert np.array_equal(m["nmovem"], z[p + "nmovem"])
+        assert np.array_equal(m["nstepreject"], z[p + "nstepreject"])
+        assert_bits_equal(m["fadds"], z[p + "fadds"], p + "fadds")
+        assert m["ran1"].idum == int(z[p + "ran1_after_idum"])
+        assert np.array_equal(m["ran1"].iv, z[p + "ran1_after_iv"])
+
+
+def _check_chain(case, strict):
+    """Device cosines: energies within ENERGY_RTOL of the FP64 restatement and the same
+    accept/reject decisions as the reference, except where the Metropolis margin is inside
+    that tolerance (the chains may then part, and the comparison stops)."""
+    z, box, d = _prepare(case)
+    _mc(d, z, box)
+    ob = BoxArrays.from_golden(z)
+    oc = oracle.cell_list(ob, int(z["in_nmolcell"]), f32(z["in_sepmax"]))
+    ost = oracle.fmolec1(ob, oc, z["in_eintra"])
+    nmt = box.nmoltype
+    omc = dict(rejrate=f32(z["in_rejrate"]), stepr=f32(z["in_stepr"]), stepm=f32(z["in_stepm"]),
+               wholerot=z["in_wholerot"].copy(), wholetrans=z["in_wholetrans"].copy(),
+               internrot=np.zeros(nmt, f32), interntrans=np.zeros(nmt, f32), ireset=0)
+    ran1 = Ran1State.from_golden(z, "mf_ran1_before_")
+    temp = f32(1.0) / box.simt
+    for cyc in range(int(z["mf_cycles"])):
+        d.molfit(strict=strict)
+        m = d.download_mc()
+        _, tr, ran1 = oracle.molfit(ob, oc, ost, omc, ran1)
+        for k in range(tr["nmoves"]):
+            tol = ENERGY_RTOL * tr["scale64"][k] + 1e-6
+            assert abs(float(m["den"][k]) - tr["den64"][k]) <= tol, (cyc, k, m["den"][k], tr["den64"][k], tol)
+            if m["acc"][k] != tr["acc"][k]:
+                # only allowed when the decision sits inside the energy tolerance
+                u_margin = abs(float(tr["den"][k]) - float(m["den"][k]))
+                assert u_margin <= tol * 2, (cyc, k)
+                return
+        co = d.download_coords()
+        for kk in ("xadd", "yadd", "zadd", "xa", "ya", "za"):
+            assert np.max(np.abs(co[kk] - getattr(ob, kk))) < 1e-5, kk
+
+
+@pytest.mark.parametrize("case", goldens.CASES)
+def test_molfit_device_cos_strict_chain(case):
+    _check_chain(case, strict=True)
+
+
+@pytest.mark.parametrize("case", goldens.CASES)
+def test_molfit_device_fast_sum_chain(case):
+    _check_chain(case, strict=False)
+
+
+def test_en_change_and_en_mole_pair_entry_points():
+    z, box, d = _prepare("mix_small")
+    import ctypes as C
+    from epsr_python_translation_b200 import _lib
+    lib = _lib.load()
+    M = d.nnbrefmax
+    erg = torch.zeros(M, dtype=torch.float32, device="cuda")
+    out = np.zeros(1, f32)
+    ob = BoxArrays.from_golden(z)
+    for im in (0, 7, box.nmol - 1):
+        _lib.check(lib.epsr_en_change(C.byref(d.cbox), C.byref(d.store), im, C.c_void_p(erg.data_ptr()),
+                                      out.ctypes.data_as(C.c_void_p), None))
+        # at unchanged coordinates the stored energies equal the fresh ones
+        assert abs(float(out[0])) <= 1e-3
+    ims = torch.tensor([0, 1, 2, 10], dtype=torch.int32, device="cuda")
+    jms = torch.tensor([5, 9, 33, 40], dtype=torch.int32, device="cuda")
+    res = torch.zeros(4, dtype=torch.float32, device="cuda")
+    _lib.check(lib.epsr_en_mole_pair(C.byref(d.cbox), C.c_void_p(ims.data_ptr()), C.c_void_p(jms.data_ptr()), 4,
+                                     C.c_void_p(res.data_ptr()), None))
+    r = res.cpu().numpy()
+    for k, (i, j) in enumerate(zip([0, 1, 2, 10], [5, 9, 33, 40])):
+        assert_bits_equal(r[k], oracle.en_mole_pair(ob, i, j), f"pair {i},{j}")
+
+
+# ----------------------------------------------------------------------------- atogen
+@pytest.mark.parametrize("case", goldens.CASES)
+def test_atogen_device_matches_reference(case):
+    z = goldens.load(case)
+    box = BoxArrays.from_golden(z)
+    last = int(z["mf_cycles"]) - 1
+    for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+        setattr(box, k, z[f"mf{last}_{k}"].copy())
+    d = _device(box)
+    t = d.ran1_tensor(Ran1State.from_golden(z, "ag_ran1_before_"))
+    ngr = d.atogen(int(z["ag_ngrsamples_in"]), t, z["ag_rminex"])
+    assert ngr == int(z["ag_ngrsamples"])
+    wav, potex = d.download_wav()
+    mine = wav[:, :, 1:box.npt1 + 1].transpose(0, 2, 1)
+    assert_bits_equal(mine, z["ag_wav"], "wav")
+    assert_bits_equal(potex, z["ag_potex"], "potex")
+    s = t.cpu().numpy()
+    assert int(s[0]) == int(z["ag_ran1_after_idum"]) and np.array_equal(s[3:35], z["ag_ran1_after_iv"])
+    assert d.last_pair_updates > 0
+
+
+# ----------------------------------------------------------------------------- gensq / stog
+@pytest.mark.parametrize("case", ["c1_water", "mix_small"])
+def test_gensq_device_matches_reference(case):
+    from epsr_python_translation_b200 import transforms
+    z = goldens.load(case)
+    box = BoxArrays.from_golden(z)
+    npt1, nq = box.npt1, int(z["gs_nq"])
+    ld = box.npt + 1
+    wav = np.zeros((2, box.npairs, ld), f32)
+    wav[:, :, 1:npt1 + 1] = z["ag_wav"].transpose(0, 2, 1)
+    F = np.ascontiguousarray(z["gs_foqols"])   # (npt1+1, nq+1): F[j, i], i fastest
+    out = transforms.gensq(nq, npt1, torch.from_numpy(wav.reshape(-1)).cuda(), ld, F, nq + 1, 1,
+                           z["gs_ycoh"][:ld] if z["gs_ycoh"].shape[0] >= ld else np.pad(z["gs_ycoh"], (0, ld)),
+                           box.n2extr, np.ones(box.ntype, f32), box.npairs)
+    o = out.cpu().numpy().reshape(2, box.npairs, nq + 1)
+    assert_bits_equal(o[:, :, 1:].transpose(0, 2, 1), z["gs_sofq"], "sofq")
+
+
+@pytest.mark.parametrize("case", ["c1_water", "mix_small"])
+def test_stog_device_within_tolerance(case):
+    """The sine is the only transcendental; each g(r) value is checked against the
+    reference within 1e-5 of the magnitude of its summed terms."""
+    from epsr_python_translation_b200 import transforms
+    z = goldens.load(case)
+    q = z["gs_q"]
+    nq = q.shape[0] - 1
+    sofq = z["gs_sofq"][1]
+    sp = np.zeros((sofq.shape[1], nq + 1), f32)
+    sp[:, 1:] = sofq.T
+    r = np.zeros(z["sg_r"].shape[0] + 1, f32)
+    r[1:] = z["sg_r"]
+    g = transforms.stog(f32(z["sg_rho"]), q, sp, r, z["sg_nqmin"], z["sg_nqmax"], z["sg_xwt"]).cpu().numpy()
+    ref = z["sg_gofr"]
+    qq = q.astype(np.float64)
+    rho = float(z["sg_rho"])
+    sfac = 0.5 * (qq[4] - qq[3]) / np.pi / np.pi / rho
+    for j in range(1, r.shape[0]):
+        rr = max(float(r[j]), 1e-30)
+        scale = sfac * np.sum(np.abs(sp[:, 2:] * qq[2:] * (qq[2:] if r[j] == 0 else 1.0)), axis=1) / (
+            rr if r[j] > 0 else 1.0)
+        tol = 1e-5 * (scale + np.abs(z["sg_xwt"])) + 1e-7
+        diff = np.abs(g[:, j] - ref[j - 1])
+        assert np.all(diff <= tol), (j, diff.max(), tol.min())
+
+
+# ----------------------------------------------------------------------------- fit_expansion
+@pytest.mark.parametrize("run", [0, 1])
+def test_fit_expansion_device_matches_reference(run):
+    from epsr_python_translation_b200 import transforms
+    from epsr_python_translation_b200.device import DeviceBox  # noqa: F401
+    z = np.load(goldens.GOLDEN + "/fitexp.npz")
+    p = f"fx{run}_"
+    nterms, npt = int(z["fx_nterms"]), int(z["fx_npt"])
+    wtold = np.zeros(nterms + 1, f32)
+    wtold[1:] = z[p + "wtold_in"]
+    st = torch.from_numpy(Ran1State.from_golden(z, p + "ran1_before_").as_array()).cuda()
+    res = transforms.fit_expansion(z["fx_yin"], z["fx_expr"], wtold, f32(z["fx_stepr_in"]), 1, npt,
+                                   int(z[p + "ncfirst"]), nterms, 1000, int(z["fx_nfreq"]), st)
+    assert_bits_equal(res["wt"].cpu().numpy()[1:], z[p + "wt"], "wt")
+    assert_bits_equal(res["wtold"].cpu().numpy()[1:], z[p + "wtold"], "wtold")
+    assert_bits_equal(res["yout"].cpu().numpy()[1:], z[p + "yout"], "yout")
+    for k in ("stepr", "acceptr", "rejrat", "chisq"):
+        assert_bits_equal(res[k], z[p + k], k)
+    s = st.cpu().numpy()
+    assert int(s[0]) == int(z[p + "ran1_after_idum"]) and int(s[2]) == int(z[p + "ran1_after_mcall"])
