@@ -115,7 +115,9 @@ __global__ void __launch_bounds__(AG_THREADS) ag_inter_kernel(AgDev A, const int
     const int nbins = A.npairs * A.ldw;
     unsigned int *hist = (unsigned int *)sm;
     unsigned int *hpot = hist + nbins;
-    float4 *tp = (float4 *)(hpot + ((A.npairs + 3) & ~3));
+    // the float4 tile must start on a 16-byte boundary
+    const size_t tp_off = ((sizeof(unsigned int) * ((size_t)nbins + A.npairs)) + 15) & ~(size_t)15;
+    float4 *tp = (float4 *)(sm + tp_off);
     int *tm = (int *)(tp + tile);
     const int noatoms = *noatoms_p;
     const int t0 = blockIdx.x * tile;
@@ -312,7 +314,8 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
     int tile = 1024;
     const int ychunks = (noatoms + AG_THREADS - 1) / AG_THREADS;
     while (tile > 128 && (long long)ychunks * ((natom + tile - 1) / tile) < 4 * 148) tile >>= 1;
-    const size_t shm = sizeof(unsigned int) * (nbins + ((box->npairs + 3) & ~3)) + (sizeof(float4) + sizeof(int)) * tile;
+    const size_t tp_off = ((sizeof(unsigned int) * (nbins + box->npairs)) + 15) & ~(size_t)15;
+    const size_t shm = tp_off + (sizeof(float4) + sizeof(int)) * tile;
     if (shm > 220 * 1024) {
         epsr_set_error("epsr_atogen: histogram of %zu bins does not fit in shared memory", nbins);
         return EPSR_ERR_UNSUPPORTED;

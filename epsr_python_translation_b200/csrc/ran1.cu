@@ -5,6 +5,11 @@
 // 64-bit modular product with IA^k gives the same value).  The Bays-Durham shuffle is an
 // inherently sequential pointer chase; its 32-entry table lives one entry per lane and
 // each step is a shift plus a warp shuffle.
+//
+// The reference re-initialises on any call that finds idum <= 0 or iy == 0 (:346).  That
+// happens at the first call of a stream and, for the degenerate seed -(2^31-1), again after
+// a step that produced idum == 0; a batch therefore ends after such a step and the next
+// batch starts with the initialisation.
 #include "common.cuh"
 
 namespace epsr {
@@ -15,56 +20,61 @@ __device__ __forceinline__ uint32_t mulmod_im(uint32_t a, uint32_t b) {
 
 __global__ void ran1_fill_kernel(int32_t *state, float *out, int64_t n) {
     const int lane = threadIdx.x & 31;
-    __shared__ int32_t st[35];
-    __shared__ Ran1 init;
-    int32_t idum = state[0], iy = state[1], mcall = state[2];
-    int32_t iv;
-    if (idum <= 0 || iy == 0) {
-        if (lane == 0) {
-            int64_t neg = -(int64_t)idum;
-            int32_t w = (int32_t)(uint32_t)(uint64_t)neg;
-            int32_t d = w > 1 ? w : 1;
-            for (int j = 40; j >= 1; --j) {
-                d = ran1_lcg(d);
-                if (j <= 32) init.iv[j - 1] = d;
-            }
-            init.idum = d;
-            init.iy = init.iv[0];
-        }
-        __syncwarp();
-        idum = init.idum;
-        iy = init.iy;
-        iv = init.iv[lane];
-    } else {
-        iv = state[3 + lane];
-    }
-    uint32_t mul = 16807u;
+    __shared__ int32_t tab[32];
+    __shared__ int32_t ini[2];
+    int32_t idum = state[0], iy = state[1];
+    const int32_t mcall = state[2];
+    int32_t iv = state[3 + lane];
+    __syncwarp();
+    uint32_t mul = 16807u;  // IA^(lane+1) mod IM
     for (int k = 0; k < lane; ++k) mul = mulmod_im(mul, 16807u);
     int64_t done = 0;
     while (done < n) {
-        const int cnt = (n - done) >= 32 ? 32 : (int)(n - done);
-        const int32_t idl = (int32_t)mulmod_im(mul, (uint32_t)idum);
+        if (idum <= 0 || iy == 0) {  // warp-uniform
+            if (lane == 0) {
+                int64_t neg = -(int64_t)idum;
+                int32_t w = (int32_t)(uint32_t)(uint64_t)neg;
+                int32_t d = w > 1 ? w : 1;
+                for (int j = 40; j >= 1; --j) {
+                    d = ran1_lcg(d);
+                    if (j <= 32) tab[j - 1] = d;
+                }
+                ini[0] = d;
+                ini[1] = tab[0];
+            }
+            __syncwarp();
+            idum = ini[0];
+            iy = ini[1];
+            iv = tab[lane];
+            __syncwarp();
+        }
+        int cnt = (n - done) >= 32 ? 32 : (int)(n - done);
+        const int32_t idl = (int32_t)mulmod_im(mul, (uint32_t)idum);  // idum after lane+1 steps
+        const unsigned zero = __ballot_sync(0xffffffffu, lane < cnt && idl == 0);
+        if (zero) cnt = __ffs(zero);  // stop after the first step that leaves idum == 0
         int32_t mine = 0;
-        for (int s = 0; s < cnt; ++s) {
+        int s = 0;
+        while (s < cnt) {
             const int32_t id = __shfl_sync(0xffffffffu, idl, s);
-            const int j = iy >> 26;
+            const int j = iy >> 26;  // iy / NDIV, NDIV = 2^26
             const int32_t nxt = __shfl_sync(0xffffffffu, iv, j);
             if (lane == j) iv = id;
             iy = nxt;
             if (lane == s) mine = iy;
+            ++s;
+            if (iy == 0) break;      // warp-uniform; the next call re-initialises
         }
+        cnt = s;
         idum = __shfl_sync(0xffffffffu, idl, cnt - 1);
         if (lane < cnt) out[done + lane] = ran1_out(mine);
         done += cnt;
     }
-    st[3 + lane] = iv;
-    __syncwarp();
+    state[3 + lane] = iv;
     if (lane == 0) {
         state[0] = idum;
         state[1] = iy;
         state[2] = (int32_t)((uint32_t)mcall + (uint32_t)n);
     }
-    state[3 + lane] = st[3 + lane];
 }
 
 }  // namespace epsr

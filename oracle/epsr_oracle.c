@@ -467,7 +467,8 @@ static double en_atom_inter64(const oracle_sys *S, double x1, double y1, double 
            (double)S->ecoul1[base + iz] * dt;
 }
 
-/* FP64 energy of molecule im (atom offsets xo/yo/zo, centre cx/cy/cz) with molecule jm. */
+/* FP64 energy of molecule im (atom offsets xo/yo/zo, centre cx/cy/cz) with molecule jm;
+ * *absum accumulates the magnitudes of the atom-pair terms. */
 static double en_mole_pair64(const oracle_sys *S, int im, const float *xo, const float *yo, const float *zo,
                              float cx, float cy, float cz, int jm, double *absum) {
     double e = 0.0;
@@ -487,7 +488,10 @@ static double en_mole_pair64(const oracle_sys *S, int im, const float *xo, const
     return e;
 }
 
-static float en_change(const oracle_sys *S, int im, const oracle_store *E, float *ergnew) {
+/* en_change molfit.py:806-919.  d64/sc64 (optional): the exact (double) sum of the same
+ * float32 terms and the sum of their magnitudes -- the FP64 reference of the accumulation. */
+static float en_change(const oracle_sys *S, int im, const oracle_store *E, float *ergnew, double *d64,
+                       double *sc64) {
     const int M = E->nnbrefmax;
     const int nn = E->nergpairm[im];
     const int32_t *nb = E->molergpair + (size_t)im * M;
@@ -499,8 +503,20 @@ static float en_change(const oracle_sys *S, int im, const oracle_store *E, float
         ergnew[inn] = ergnew[inn] + sume;
     }
     float fdiff = 0.0f;
-    for (int inn = 1; inn < nn; ++inn) fdiff = fdiff + ergnew[inn] - E->ergpair[rf[inn] - 1];
+    double d = 0.0, sc = 0.0;
+    for (int inn = 1; inn < nn; ++inn) {
+        const float old = E->ergpair[rf[inn] - 1];
+        fdiff = fdiff + ergnew[inn] - old;
+        d += (double)ergnew[inn] - (double)old;
+        sc += fabs((double)ergnew[inn]) + fabs((double)old);
+    }
+    if (d64) *d64 = d;
+    if (sc64) *sc64 = sc;
     return fdiff;
+}
+
+float oracle_en_change(const oracle_sys *S, int im, const oracle_store *E, float *ergnew, double *d64_sc64) {
+    return en_change(S, im, E, ergnew, d64_sc64, d64_sc64 ? d64_sc64 + 1 : 0);
 }
 
 /* rotatm molfit.py:672-711 */
@@ -592,19 +608,12 @@ int oracle_molfit(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_
             } else {
                 P->wholetrans[mt] = 0.0f;
             }
+            double d64 = 0.0, sc64 = 0.0;
+            float fdiff = en_change(S, im, E, ergnew, &d64, &sc64);
             if (T && T->den64) {
-                double sc = 0.0, dn = 0.0;
-                const int32_t *nb = E->molergpair + (size_t)im * M;
-                for (int inn = 1; inn < E->nergpairm[im]; ++inn) {
-                    const int jm = nb[inn];
-                    dn += en_mole_pair64(S, im, S->xa + a0, S->ya + a0, S->za + a0, S->xadd[im], S->yadd[im],
-                                         S->zadd[im], jm, &sc);
-                    dn -= en_mole_pair64(S, im, xr, yr, zr, xs, ys, zs, jm, &sc);
-                }
-                T->den64[T->nmoves] = dn;
-                T->scale64[T->nmoves] = sc;
+                T->den64[T->nmoves] = d64;
+                T->scale64[T->nmoves] = sc64;
             }
-            float fdiff = en_change(S, im, E, ergnew);
             float ediff = (fdiff + 0.0f) * temp;
             float etest;
             if (ediff <= 0.0f) etest = 10.0f;
@@ -1004,4 +1013,13 @@ int64_t oracle_fit_expansion(const float *yin, const float *expr, float *yout, f
     scal[2] = rejrat;
     scal[3] = chisqnew;
     return trials;
+}
+
+/* FP64 en_mole_pair at the current coordinates; out2 = {energy, sum of |terms|}. */
+void oracle_en_mole_pair64(const oracle_sys *S, int im, int jm, double *out2) {
+    double sc = 0.0;
+    const int a0 = S->naf[im];
+    out2[0] = en_mole_pair64(S, im, S->xa + a0, S->ya + a0, S->za + a0, S->xadd[im], S->yadd[im], S->zadd[im], jm,
+                             &sc);
+    out2[1] = sc;
 }

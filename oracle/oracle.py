@@ -306,3 +306,24 @@ def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfr
                                         ncfirst, nterms, nits, nfreq, C.byref(r))
     return dict(wt=wt, wtold=wto, yout=yout, stepr=scal[0], acceptr=scal[1], rejrat=scal[2], chisq=scal[3],
                 trials=int(trials)), r.to_state()
+
+
+def en_change(box, st, im):
+    """en_change at the current coordinates: (float32 value, exact double sum of the same
+    terms, sum of their magnitudes, ergnew)."""
+    L = lib()
+    L.oracle_en_change.restype = C.c_float
+    h = SysHandle(box)
+    E = store_c(st)
+    ergnew = np.zeros(max(st["nnbrefmax"], 1), f32)
+    d = np.zeros(2, np.float64)
+    v = L.oracle_en_change(C.byref(h.c), int(im), C.byref(E), ptr(ergnew), ptr(d))
+    return f32(v), float(d[0]), float(d[1]), ergnew
+
+
+def en_mole_pair64(box, im, jm):
+    """FP64 en_mole_pair: (energy, sum of |atom-pair terms|)."""
+    h = SysHandle(box)
+    out = np.zeros(2, np.float64)
+    lib().oracle_en_mole_pair64(C.byref(h.c), int(im), int(jm), ptr(out))
+    return float(out[0]), float(out[1])
