@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the EPSR pair path on B200: MC molecule-moves/s (+ g(r) pair-updates/s).
+
+One step = one EPSR iteration of the hot path on configuration C2 (200 DMSO + 400 water,
+3200 atoms, 21 pair types): cell list, fmolec1, 5 molfit cycles (3000 whole-molecule
+moves), atogen over all 5,118,400 atom pairs, gensq, fit_expansion for three datasets, stog.
+``value`` = molecule moves per second of whole-step device time, inputs resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank advances its own independent box (replicas, different ran1
+seeds): there is no data-path collective, so ``scaling`` is "weak".  ``--impl reference``
+times the reference's algorithm (the C restatement in oracle/, single-threaded per
+process) on all host cores with one independent replica per core.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC molecule-moves/s"
+UNIT = "moves/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2_mixture")
+    ap.add_argument("--strict", action="store_true", help="bit-identical sequential sums")
+    ap.add_argument("--cpu-sample-steps", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- CPU side
+def _cpu_worker(args):
+    config, seed, steps, warmup = args
+    from epsr_python_translation_b200 import configs
+    from oracle.workload import CpuIteration
+    wl = configs.make_workload(config)
+    it = CpuIteration(wl, ran1_seed=seed)
+    for _ in range(warmup):
+        it.step()
+    t0 = time.perf_counter()
+    per = []
+    for _ in range(steps):
+        a = time.perf_counter()
+        it.step()
+        per.append(time.perf_counter() - a)
+    return time.perf_counter() - t0, per, it.stage_s, it.pair_updates, wl.ntimes * wl.system.nmol
+
+
+def cpu_info():
+    model = ""
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count() or 1
+
+
+def cpu_baseline(config, steps):
+    """Single core: the oracle (C restatement of the reference) on a bounded sample of the
+    same workload."""
+    wall, per, stages, pairs, moves = _cpu_worker((config, -7, steps, 1))
+    model, n = cpu_info()
+    ms = 1000.0 * statistics.mean(per)
+    return {"value": moves / statistics.mean(per), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} full EPSR iterations of {config} ({moves} moves each) after 1 warm-up, "
+                      f"single-threaded C oracle, {ms:.0f} ms/iteration; pair-updates/s "
+                      f"{pairs / stages.get('atogen', 1e9):.3e}; host {model}, nproc {n}",
+            "stage_s": {k: round(v, 4) for k, v in stages.items()}}
+
+
+def reference_arm(a):
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    model, ncpu = cpu_info()
+    nproc = max(1, ncpu)
+    steps, warmup = a.steps, a.warmup
+    # bounded: a few minutes at most (one C2 iteration is about 1.4 s on one core)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_cpu_worker, [(a.config, -(11 + i), steps, warmup) for i in range(nproc)])
+    wall = time.perf_counter() - t0
+    moves = res[0][4]
+    slowest = max(r[0] for r in res)
+    value = nproc * steps * moves / slowest
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": steps,
+        "warmup": warmup, "ms_per_step": 1000.0 * slowest / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded C2 mixture box)",
+        "config": {"workload": a.config, "moves_per_step_per_replica": moves, "replicas": nproc,
+                   "stages": "cells+fmolec1+5 molfit+atogen+gensq+3 fit_expansion+stog"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
+                         "sample": f"{nproc} independent replicas x {steps} iterations (+{warmup} warm-up) of the "
+                                   f"single-threaded C restatement, one process per core; host {model}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(wall, 2),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- GPU side
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = str(index)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in out.splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9 or f[0] != self.index:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_arm(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from epsr_python_translation_b200 import configs
+    from epsr_python_translation_b200.iteration import STAGES, EpsrIteration
+
+    wl = configs.make_workload(a.config)
+    it = EpsrIteration(wl, strict=a.strict, ran1_seed=-(1 + rank))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+
+    for _ in range(max(3, a.warmup)):
+        it.step()
+    torch.cuda.synchronize()
+
+    # ---------------- device-resident timing (value)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    stage_tot = {k: 0.0 for k in STAGES}
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    idx = vis.split(",")[local] if vis else str(local)
+    clocks = ClockSampler(idx)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    for k in range(a.steps):
+        flush.fill_(float(k))                      # L2 flushed between timed steps (untimed)
+        starts[k].record()
+        it.step()
+        ends[k].record()
+        for s, v in it.stage_ms().items():
+            stage_tot[s] += v
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    tot_ms = sum(step_ms)
+    t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tmax_ms = float(t.item())
+    moves = it.moves_per_step
+    value = world * a.steps * moves / (tmax_ms / 1000.0)
+
+    # ---------------- end to end through the public API with host buffers
+    co = it.d.download_coords()
+    pinned = [torch.from_numpy(co[k]).pin_memory() for k in ("xa", "ya", "za", "xadd", "yadd", "zadd")]
+    h2d = sum(p.numel() * 4 for p in pinned)
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    d2h = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e_start.record()
+    for k in range(a.steps):
+        for name, p in zip(("xa", "ya", "za", "xadd", "yadd", "zadd"), pinned):
+            getattr(it.d, name).copy_(p, non_blocking=True)
+        it.d.refresh_positions()
+        it.step()
+        _, d2h = it.download_outputs()
+    e_end.record()
+    torch.cuda.synchronize()
+    e2e_ms = e_start.elapsed_time(e_end)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * a.steps * moves / (float(t.item()) / 1000.0)
+
+    # ---------------- roofline of the dominant kernel
+    stage_ms = {k: v / a.steps for k, v in stage_tot.items()}
+    roof, extra = roofline(it, stage_ms, a)
+    launches = kernel_launches(it, wl)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": tmax_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded C2 mixture box, synthetic isotope datasets)",
+            "config": {"workload": a.config, "nmol": it.box.nmol, "natom": it.box.natom, "npairs": it.box.npairs,
+                       "moves_per_step": moves, "pair_updates_per_step": it.pair_updates,
+                       "stages": "cells+fmolec1+5 molfit+atogen+gensq+3 fit_expansion+stog",
+                       "l2": "flushed between timed steps (256 MB write)", "sums": "strict" if a.strict else "fast",
+                       "parallelism": f"replicas x{world}"},
+            "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "pair_updates_per_s": it.pair_updates / (stage_ms["atogen"] / 1000.0),
+            "mc_moves_per_s_molfit_only": moves / (stage_ms["molfit"] / 1000.0),
+            "fit_trials_per_step": it.fit_trials,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roof, **extra,
+            "gpu_launches": launches * a.steps,
+            "clocks": clk,
+        }
+        if not a.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(a.config, a.cpu_sample_steps)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def kernel_launches(it, wl):
+    """Own kernels launched per step (counted from the host code paths)."""
+    n = 0
+    n += 5            # cell list: assign, scan, scatter, sort, offsets
+    n += 1            # region count (nnbrefmax)
+    n += 9            # fmolec1: positions, radius, regions, count, 2 scans, intra, write, sort (+ sums)
+    n += 1
+    n += wl.ntimes    # molfit sweeps
+    n += 8            # atogen: positions, ran1, select, intra, molof, prefix, origin atoms, inter, norm (-1)
+    n += 1            # gensq
+    n += 2 * wl.data.shape[0]  # fit_expansion: transpose + persistent fit per dataset
+    n += 2            # stog: lorch + stog
+    return n
+
+
+def roofline(it, stage_ms, a):
+    """Roofline of the dominant stage (largest share of the step)."""
+    import json as _j
+
+    import numpy as np
+    peaks = {}
+    try:
+        peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        src = "of measured"
+    except (OSError, ValueError):
+        src = "of fallback"
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    fp32_peak = 148 * 128 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12  # Top/s, 1 op/lane/clock
+    dom = max(stage_ms, key=stage_ms.get)
+    b = it.box
+    wl = it.wl
+    extra = {"dominant_stage": dom}
+    if dom == "molfit":
+        # algorithmic bytes of one sweep: per move its stored list (partner, ref, old energy,
+        # new energy write: 16 B/entry) and the coordinates of every neighbour atom (16 B/atom)
+        st = it.d.download_store()
+        nn = st["nergpairm"].astype(np.int64)
+        nato = b.nato.astype(np.int64)
+        atoms_per_mol = np.array([int(np.sum(nato[st["molergpair"][m, 1:nn[m]]])) for m in range(b.nmol)])
+        bytes_sweep = int(np.sum(16 * np.maximum(nn - 1, 0)) + np.sum(16 * atoms_per_mol))
+        pairs_sweep = int(np.sum(atoms_per_mol * nato))
+        per_launch_ms = stage_ms["molfit"] / wl.ntimes
+        ach = bytes_sweep / (per_launch_ms / 1000.0) / 1e9
+        extra["fp32_issue"] = {"achieved_Tops": pairs_sweep * 26 / (per_launch_ms / 1000.0) / 1e12,
+                               "peak_Tops": fp32_peak, "ops_per_atom_pair": 26,
+                               "atom_pairs_per_sweep": pairs_sweep}
+        return {"bound": "hbm", "kernel": "molfit_seq_kernel", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": None, "peak_source": src,
+                "algorithmic_bytes_per_launch": bytes_sweep, "launch_ms": per_launch_ms}, extra
+    if dom == "fit_expansion":
+        # per trial the basis is read once: npt*nterms*4 bytes
+        per_launch_ms = stage_ms["fit_expansion"] / wl.data.shape[0]
+        trials = it.fit_trials / wl.data.shape[0]
+        byt = trials * wl.nq * wl.nterms * 4
+        ach = byt / (per_launch_ms / 1000.0) / 1e9
+        return {"bound": "hbm", "kernel": "fitexp_kernel", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": byt,
+                "launch_ms": per_launch_ms}, extra
+    if dom == "atogen":
+        per_launch_ms = stage_ms["atogen"]
+        byt = 16 * b.natom * max(1, b.natom // 256)
+        ach = byt / (per_launch_ms / 1000.0) / 1e9
+        extra["fp32_issue"] = {"achieved_Tops": it.pair_updates * 17 / (per_launch_ms / 1000.0) / 1e12,
+                               "peak_Tops": fp32_peak}
+        return {"bound": "hbm", "kernel": "ag_inter_kernel", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": byt,
+                "launch_ms": per_launch_ms}, extra
+    per_launch_ms = stage_ms[dom]
+    return {"bound": "hbm", "kernel": dom, "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
+            "traffic": None, "peak_source": src, "launch_ms": per_launch_ms}, extra
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return reference_arm(a)
+    return gpu_arm(a)
+
+
+if __name__ == "__main__":
+    import numpy as np  # noqa: F401  (used by roofline)
+    sys.exit(main())

@@ -474,3 +474,81 @@ def fit_problem(nq=600, nterms=116, seed=5, noise=0.005):
     yin = np.zeros(nq + 1, dtype=f32)
     yin[1:] = y.astype(f32)
     return dict(q=q, expr=expr, yin=yin, nterms=nterms, npt=nq)
+
+
+# ----------------------------------------------------------------------------- workloads
+def intra_energies(s: System, k_bond=1000.0):
+    """Per-molecule harmonic bond energies (float32) of the seeded geometry.
+
+    The pair path takes intramolecular energies as an input (they decide whether a
+    molecule's first store slot is its own energy, ergpairreference.py:103-118); for a
+    synthetic box they are the harmonic deviation of each bond from its template length.
+    """
+    out = np.zeros(s.nmol, dtype=f32)
+    for m in range(s.nmol):
+        a0 = int(s.naf[m])
+        e = 0.0
+        for (i, j, length) in s.bonds[int(s.mtype[m])]:
+            d = np.array([s.xa[a0 + i] - s.xa[a0 + j], s.ya[a0 + i] - s.ya[a0 + j], s.za[a0 + i] - s.za[a0 + j]],
+                         dtype=np.float64) * float(s.dmax)
+            e += k_bond * (float(np.sqrt(d @ d)) - abs(length)) ** 2
+        out[m] = f32(e)
+    return out
+
+
+@dataclass
+class Workload:
+    """One EPSR iteration's inputs for the pair path on a box."""
+    name: str
+    system: System
+    eintra: np.ndarray
+    q: np.ndarray            # (nq+1,) 1-based
+    foqols: np.ndarray       # (npt1+1, nq+1): F[j, i] (Q index fastest)
+    ycoh: np.ndarray         # (npt+1,)
+    expr: np.ndarray         # (nq*nterms+1,) 1-based flat, row-major by Q
+    nterms: int
+    data: np.ndarray         # (ndata, nq+1) synthetic interference functions
+    weights: np.ndarray      # (ndata, npairs) pair weights of each dataset
+    wholerot: np.ndarray
+    wholetrans: np.ndarray
+    ntimes: int = 5
+    nmolcell: int = 10
+    rejrate: float = 0.75
+    ngrsamples: int = 0
+    xwt: np.ndarray = None   # (npairs,) stog offsets
+
+    @property
+    def nq(self):
+        return int(self.q.shape[0] - 1)
+
+
+def make_workload(name="c2_mixture", seed=1, nq=600, qstep=0.05, nterms=116, ndata=3, ntimes=5):
+    """Configuration C2: 200 DMSO + 400 water, 5 MC sweeps per iteration, three isotope
+    datasets (deuterated, protiated, 50:50), a 116-term Poisson-like EP basis."""
+    if name == "c2_mixture":
+        s = c2_mixture(seed=seed)
+    elif name == "c1_water":
+        s = c1_water(seed=seed)
+    elif name == "c3_water":
+        s = c3_water(seed=seed)
+    else:
+        raise ValueError(name)
+    rng = np.random.default_rng(seed + 100)
+    q = qgrid(nq, qstep)
+    npt1 = s.grid["npt1"]
+    F, ycoh = transform_table(s, q, npt1)
+    expr = ep_basis(q, nterms)
+    w = rng.uniform(0.2, 1.0, size=(ndata, s.npairs)).astype(f32)
+    w /= w.sum(axis=1, keepdims=True)
+    data = np.zeros((ndata, nq + 1), dtype=f32)
+    qq = q.astype(np.float64)
+    for d in range(ndata):
+        data[d, 1:] = (0.05 * np.sin(2.9 * qq[1:] + d) * np.exp(-0.05 * qq[1:])
+                       + rng.normal(0, 0.005, size=nq)).astype(f32)
+    nmt = s.nmoltype
+    wholerot = np.full(nmt, f32(10.0 / 180.0), dtype=f32)
+    wholetrans = np.full(nmt, f32(0.5) / s.dmax, dtype=f32)
+    xwt = np.linspace(0.5, 1.5, s.npairs).astype(f32)
+    return Workload(name=name, system=s, eintra=intra_energies(s), q=q, foqols=F, ycoh=ycoh, expr=expr,
+                    nterms=nterms, data=data, weights=w, wholerot=wholerot, wholetrans=wholetrans, ntimes=ntimes,
+                    xwt=xwt)

@@ -89,6 +89,10 @@ class DeviceBox:
             getattr(self, name).copy_(torch.from_numpy(np.ascontiguousarray(v, dtype=f32)))
         check(self.lib.epsr_box_positions(C.byref(self.cbox), _stream()))
 
+    def refresh_positions(self):
+        """Recompute the absolute positions after the offset/centre tensors were written."""
+        check(self.lib.epsr_box_positions(C.byref(self.cbox), _stream()))
+
     def download_coords(self):
         torch.cuda.synchronize()
         return {k: getattr(self, k).cpu().numpy() for k in ("xa", "ya", "za", "xadd", "yadd", "zadd")}

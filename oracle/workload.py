@@ -1,0 +1,81 @@
+"""The EPSR iteration of the pair path on the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Used by bench.py's CPU-baseline leg and its reference arm: the same stages, inputs and
+order as epsr_python_translation_b200.iteration.EpsrIteration, computed by the C
+restatement of the reference (single-threaded, as the reference).
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from epsr_python_translation_b200.box import BoxArrays, Ran1State
+from oracle import oracle
+
+f32 = np.float32
+
+
+class CpuIteration:
+    def __init__(self, wl, ran1_seed=0):
+        self.wl = wl
+        self.box = BoxArrays.from_system(wl.system)
+        b = self.box
+        nmt = b.nmoltype
+        self.mc = dict(rejrate=f32(wl.rejrate), stepr=f32(1.0), stepm=f32(1.0), wholerot=wl.wholerot.copy(),
+                       wholetrans=wl.wholetrans.copy(), internrot=np.zeros(nmt, f32),
+                       interntrans=np.zeros(nmt, f32), ireset=0, nstepreject=np.zeros(b.nmol, np.int32))
+        self.ran1 = Ran1State(idum=ran1_seed)
+        ndata = wl.data.shape[0]
+        self.pwtold = [np.zeros(wl.nterms + 1, f32) for _ in range(ndata)]
+        self.stepp = [f32(0.01)] * ndata
+        self.rows = np.ascontiguousarray(wl.foqols.T)   # (nq+1, npt1+1)
+        self.stage_s = {}
+        self.pair_updates = 0
+
+    def step(self, stages=None):
+        wl, b = self.wl, self.box
+        t = {}
+        t0 = time.perf_counter()
+        cells = oracle.cell_list(b, wl.nmolcell, b.sepmax)
+        t["cells"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        st = oracle.fmolec1(b, cells, wl.eintra)
+        t["fmolec1"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(wl.ntimes):
+            _, _, self.ran1 = oracle.molfit(b, cells, st, self.mc, self.ran1, record_cos=False)
+        t["molfit"] = time.perf_counter() - t0
+        if stages == "mc":
+            self.stage_s = t
+            return
+        t0 = time.perf_counter()
+        wav, potex, ngr, self.ran1 = oracle.atogen(b, wl.ngrsamples, self.ran1, np.full(b.npairs, -2.0, f32),
+                                                   ycoh=wl.ycoh)
+        t["atogen"] = time.perf_counter() - t0
+        # pair-updates of a full (probaccept >= 1) histogram: intra pairs + all inter pairs
+        n_at = b.natom
+        intra = int(sum(int(n) * (int(n) - 1) // 2 for n in b.nato))
+        self.pair_updates = n_at * (n_at - 1) // 2 if ngr >= b.nmol else 0
+        self.pair_updates = self.pair_updates if self.pair_updates else intra
+        t0 = time.perf_counter()
+        nq = wl.nq
+        sofq = oracle.gensq(nq, b.npt1, wav, self.rows, wl.ycoh[: b.npt + 1], b.n2extr, np.ones(b.ntype, f32))
+        t["gensq"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        inter = sofq[1]
+        for k in range(wl.data.shape[0]):
+            fit = (wl.weights[k].astype(np.float32) @ inter).astype(f32)
+            dt = (-(wl.data[k] - fit)).astype(f32)
+            res, self.ran1 = oracle.fit_expansion(dt, wl.expr, self.pwtold[k], self.stepp[k], 1, nq, 1, wl.nterms,
+                                                  1000, 10, self.ran1)
+            self.pwtold[k] = res["wtold"]
+            self.stepp[k] = res["stepr"]
+        t["fit_expansion"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        r = b.x[: b.npt1 + 1].copy()
+        oracle.stog(f32(b.natom / wl.system.L ** 3), wl.q, inter, r, np.full(b.npairs, 2, np.int32),
+                    np.full(b.npairs, nq, np.int32), wl.xwt)
+        t["stog"] = time.perf_counter() - t0
+        self.stage_s = t
