@@ -40,7 +40,7 @@ class Cells(C.Structure):
 
 class Store(C.Structure):
     _fields_ = [("nnbrefmax", I32), ("capacity", I32), ("nergpairm", P), ("molergpair", P), ("ergpairref", P),
-                ("ergpair", P), ("nergpair", P)]
+                ("ergpair", P), ("nergpair", P), ("mirror", P)]
 
 
 class Mc(C.Structure):
@@ -63,6 +63,7 @@ _SIGS = {
     "epsr_fmolec1_scratch_bytes": (I64, [I32, I32, I32]),
     "epsr_fmolec1": (C.c_int, [C.POINTER(Box), C.POINTER(Cells), P, C.POINTER(Store), P, I64, I32, P, P]),
     "epsr_molfit_scratch_bytes": (I64, [I32, I32, I32]),
+    "epsr_molfit_spec_scratch_bytes": (I64, [I32, I32, I32, I32]),
     "epsr_molfit": (C.c_int, [C.POINTER(Box), C.POINTER(Cells), C.POINTER(Store), C.POINTER(Mc), P, I64, P]),
     "epsr_en_change": (C.c_int, [C.POINTER(Box), C.POINTER(Store), I32, P, P, P]),
     "epsr_en_mole_pair": (C.c_int, [C.POINTER(Box), P, P, I32, P, P]),
@@ -95,9 +96,16 @@ def load(require_device=False):
             fn.restype = res
             fn.argtypes = args
         _lib = lib
-    if require_device and _lib.epsr_device_count() <= 0:
-        raise EpsrGpuError(-1, "no sm_100 (B200) device visible")
+    if require_device:
+        global _device_ok
+        if _device_ok is None:
+            _device_ok = _lib.epsr_device_count() > 0
+        if not _device_ok:
+            raise EpsrGpuError(-1, "no sm_100 (B200) device visible")
     return _lib
+
+
+_device_ok = None
 
 
 def check(rc):

@@ -7,6 +7,8 @@
 // stored neighbours, one neighbour per thread in the reference's (ia, ja) order so each
 // neighbour energy is bit-identical (en_change :806); then the Metropolis test (:401-408),
 // the store update (save_energies/save_erg_pairs) and the coordinate commit or restore.
+#include <string.h>
+
 #include "common.cuh"
 
 namespace epsr {
@@ -36,6 +38,7 @@ struct McDev {
     float *ergnew_g;   // [M] global fallback when M is large
     int use_smem;
     int32_t *status;
+    const int32_t *run_if;  // when set, the kernel runs only if *run_if != 0
 };
 
 __device__ __forceinline__ float next_cos(const McDev &D, int &kcos, float phi) {
@@ -52,6 +55,7 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
     __shared__ int sh_im, sh_n, sh_acc, sh_bad;
     __shared__ float sh_cx, sh_cy, sh_cz;
     __shared__ double red[MC_THREADS / 32];
+    if (D.run_if && *D.run_if == 0) return;
     float *ergnew = D.use_smem ? dyn : D.ergnew_g;
     float *ergold = D.use_smem ? dyn + D.M : D.ergnew_g + D.M;
     const int tid = threadIdx.x;
@@ -361,10 +365,14 @@ McDev make_mcdev(const epsr_box_t *b, const epsr_cells_t *c, const epsr_store_t 
 
 using namespace epsr;
 
+extern "C" int64_t epsr_molfit_spec_scratch_bytes(int32_t nmol, int32_t natom, int32_t M, int32_t nmoltype);
+
 extern "C" int64_t epsr_molfit_scratch_bytes(int32_t nmol, int32_t natom, int32_t M) {
-    (void)nmol;
-    (void)natom;
-    return (int64_t)sizeof(float) * 2 * (int64_t)(M > 0 ? M : 1) + 256;
+    // the sequential kernel needs 2*M floats when M is too large for shared memory; the fast
+    // path needs its per-cycle buffers (up to 64 molecule types)
+    const int64_t seq = (int64_t)sizeof(float) * 2 * (int64_t)(M > 0 ? M : 1) + 256;
+    const int64_t spec = epsr_molfit_spec_scratch_bytes(nmol, natom, M, 64);
+    return seq > spec ? seq : spec;
 }
 
 static int check_box(const epsr_box_t *b, const char *who) {
@@ -375,15 +383,9 @@ static int check_box(const epsr_box_t *b, const char *who) {
     return EPSR_OK;
 }
 
-extern "C" int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
-                           void *scratch, int64_t scratch_bytes, void *stream) {
-    int rc = check_box(box, "epsr_molfit");
-    if (rc) return rc;
-    if (!cells || !store || !mc || !mc->wholerot || !mc->wholetrans || !mc->nwhole || !mc->nmovem ||
-        !mc->nstepreject || !mc->fadds || !mc->ran1 || !mc->internrot || !mc->interntrans) {
-        epsr_set_error("epsr_molfit: null pointer");
-        return EPSR_ERR_ARG;
-    }
+namespace epsr {
+int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
+                      void *scratch, int64_t scratch_bytes, cudaStream_t s, const int32_t *run_if) {
     McDev D = make_mcdev(box, cells, store);
     D.simt = mc->simt;
     D.rejrate = mc->rejrate;
@@ -392,7 +394,7 @@ extern "C" int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, eps
     D.trstepmax = mc->trstepmax;
     D.trstepmin = mc->trstepmin;
     D.ireset = mc->ireset;
-    D.strict = mc->strict;
+    D.strict = run_if ? 0 : mc->strict;
     D.wholerot = mc->wholerot;
     D.wholetrans = mc->wholetrans;
     D.internrot = mc->internrot;
@@ -406,6 +408,7 @@ extern "C" int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, eps
     D.trace_den = mc->trace_den;
     D.trace_acc = mc->trace_acc;
     D.status = mc->status;
+    D.run_if = run_if;
     const size_t need = sizeof(float) * 2 * (size_t)(D.M > 0 ? D.M : 1);
     size_t shm = 0;
     if (need <= 160 * 1024) {
@@ -419,12 +422,29 @@ extern "C" int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, eps
         D.use_smem = 0;
         D.ergnew_g = (float *)scratch;
     }
-    cudaStream_t s = (cudaStream_t)stream;
     if (shm > 48 * 1024)
         EPSR_CUDA(cudaFuncSetAttribute(molfit_seq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     molfit_seq_kernel<<<1, MC_THREADS, shm, s>>>(D);
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
+}
+}  // namespace epsr
+
+int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
+                     void *scratch, int64_t scratch_bytes, void *stream);
+
+extern "C" int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
+                           void *scratch, int64_t scratch_bytes, void *stream) {
+    int rc = check_box(box, "epsr_molfit");
+    if (rc) return rc;
+    if (!cells || !store || !mc || !mc->wholerot || !mc->wholetrans || !mc->nwhole || !mc->nmovem ||
+        !mc->nstepreject || !mc->fadds || !mc->ran1 || !mc->internrot || !mc->interntrans) {
+        epsr_set_error("epsr_molfit: null pointer");
+        return EPSR_ERR_ARG;
+    }
+    if (mc->strict) return molfit_seq_launch(box, cells, store, mc, scratch, scratch_bytes, (cudaStream_t)stream,
+                                             nullptr);
+    return epsr_molfit_spec(box, cells, store, mc, scratch, scratch_bytes, stream);
 }
 
 extern "C" int epsr_en_change(const epsr_box_t *box, const epsr_store_t *store, int32_t im, float *ergnew,

@@ -18,8 +18,9 @@ __device__ __forceinline__ uint32_t mulmod_im(uint32_t a, uint32_t b) {
     return (uint32_t)(((uint64_t)a * (uint64_t)b) % 2147483647ull);
 }
 
-__global__ void ran1_fill_kernel(int32_t *state, float *out, int64_t n) {
+__global__ void ran1_fill_kernel(int32_t *state, float *out, int64_t n_host, const int32_t *n_dev) {
     const int lane = threadIdx.x & 31;
+    const int64_t n = n_dev ? (int64_t)*n_dev : n_host;
     __shared__ int32_t tab[32];
     __shared__ int32_t ini[2];
     int32_t idum = state[0], iy = state[1];
@@ -77,6 +78,13 @@ __global__ void ran1_fill_kernel(int32_t *state, float *out, int64_t n) {
     }
 }
 
+int ran1_fill_device_count(int32_t *state, float *out, const int32_t *n_dev, int64_t n_max, cudaStream_t s) {
+    (void)n_max;
+    ran1_fill_kernel<<<1, 32, 0, s>>>(state, out, 0, n_dev);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
+
 }  // namespace epsr
 
 extern "C" int epsr_ran1_fill(int32_t *state, float *out, int64_t n, void *stream) {
@@ -85,7 +93,7 @@ extern "C" int epsr_ran1_fill(int32_t *state, float *out, int64_t n, void *strea
         return EPSR_ERR_ARG;
     }
     if (n == 0) return EPSR_OK;
-    epsr::ran1_fill_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(state, out, n);
+    epsr::ran1_fill_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(state, out, n, nullptr);
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
 }

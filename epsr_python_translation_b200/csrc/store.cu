@@ -267,6 +267,34 @@ __global__ void fm_sort_kernel(int M, const int32_t *rowcnt, int32_t *nergpairm,
     if (threadIdx.x == 0) nergpairm[m] = n;
 }
 
+// mirror index: the two entries that reference one energy slot point at each other
+__global__ void mirror_claim_kernel(int nmol, int M, const int32_t *nergpairm, const int32_t *ergpairref,
+                                    int32_t *owners) {
+    const int m = blockIdx.x;
+    const int n = nergpairm[m];
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        const int e = m * M + s;
+        const int r = ergpairref[e] - 1;
+        if (atomicCAS(owners + 2 * r, -1, e) != -1) owners[2 * r + 1] = e;
+    }
+}
+
+__global__ void mirror_set_kernel(int nmol, int M, const int32_t *nergpairm, const int32_t *ergpairref,
+                                  const int32_t *owners, int32_t *mirror) {
+    const int m = blockIdx.x;
+    const int n = nergpairm[m];
+    for (int s = threadIdx.x; s < M; s += blockDim.x) {
+        const int e = m * M + s;
+        int v = -1;
+        if (s < n) {
+            const int r = ergpairref[e] - 1;
+            const int a = owners[2 * r], b = owners[2 * r + 1];
+            v = a == e ? b : a;
+        }
+        mirror[e] = v;
+    }
+}
+
 __global__ void mol_radius_kernel(const int32_t *naf, const int32_t *nato, const float *xa, const float *ya,
                                   const float *za, int nmol, float *rad) {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -371,6 +399,7 @@ extern "C" int64_t epsr_fmolec1_scratch_bytes(int32_t nmol, int32_t ncell, int32
     b += align256(sizeof(float) * (size_t)nmol);        // rad
     b += align256(sizeof(int32_t) * 8);                 // err + misc
     b += align256(sizeof(float) * 2);
+    b += align256(sizeof(int32_t) * 2 * ((size_t)nmol + (size_t)nmol * M / 2 + 16));  // mirror owners
     return (int64_t)b;
 }
 
@@ -402,6 +431,8 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
     float *rad = (float *)take(sizeof(float) * (size_t)nmol);
     int32_t *err = (int32_t *)take(sizeof(int32_t) * 8);
     float *sums = (float *)take(sizeof(float) * 2);
+    const size_t own_n = 2 * ((size_t)nmol + (size_t)nmol * M / 2 + 16);
+    int32_t *owners = (int32_t *)take(sizeof(int32_t) * own_n);
     EPSR_CUDA(cudaMemsetAsync(err, 0, sizeof(int32_t) * 8, s));
 
     BoxDev B = make_boxdev(box);
@@ -449,6 +480,15 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
                                                         (int)shm));
     fm_sort_kernel<<<nmol, 256, shm, s>>>(M, rowcnt, store->nergpairm, store->molergpair, store->ergpairref, cap);
     fm_sums_kernel<<<1, strict ? 32 : 1024, 0, s>>>(store->ergpair, nintra, (int)ntot, eintra, nmol, strict, sums);
+    if (store->mirror) {
+        if ((size_t)2 * ntot > own_n) {
+            epsr_set_error("epsr_fmolec1: mirror scratch too small");
+            return EPSR_ERR_CAPACITY;
+        }
+        EPSR_CUDA(cudaMemsetAsync(owners, 0xff, sizeof(int32_t) * 2 * (size_t)ntot, s));
+        mirror_claim_kernel<<<nmol, 128, 0, s>>>(nmol, M, store->nergpairm, store->ergpairref, owners);
+        mirror_set_kernel<<<nmol, 128, 0, s>>>(nmol, M, store->nergpairm, store->ergpairref, owners, store->mirror);
+    }
     EPSR_CUDA(cudaGetLastError());
     int32_t herr[1];
     int32_t hn = (int32_t)ntot;

@@ -161,6 +161,8 @@ class DeviceBox:
         self.s_ref = torch.zeros(b.nmol * M, dtype=torch.int32, device=self.dev)
         self.s_erg = torch.zeros(cap, dtype=torch.float32, device=self.dev)
         self.s_n = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.s_mirror = torch.zeros(b.nmol * M, dtype=torch.int32, device=self.dev)
+        st.mirror = _ptr(self.s_mirror)
         st.nnbrefmax, st.capacity = M, cap
         st.nergpairm, st.molergpair, st.ergpairref, st.ergpair, st.nergpair = (
             _ptr(t) for t in (self.s_nergpairm, self.s_mol, self.s_ref, self.s_erg, self.s_n))
@@ -229,6 +231,13 @@ class DeviceBox:
         scr = self.scratch("molfit", nb)
         check(self.lib.epsr_molfit(C.byref(self.cbox), C.byref(self.cells), C.byref(self.store), C.byref(m), _ptr(scr),
                                    scr.numel(), _stream()))
+
+    def check_status(self):
+        """Raise if a molfit cycle reported an error (synchronises)."""
+        v = int(self.m_status.item())
+        if v:
+            raise _lib.EpsrGpuError(4 if v == 1 else 5, {1: "molecule larger than 64 atoms",
+                                                         2: "fast-path resolver timed out"}.get(v, str(v)))
 
     def download_mc(self):
         torch.cuda.synchronize()

@@ -72,6 +72,9 @@ typedef struct {
     int32_t *ergpairref;  /* [nmol*M] 1-based index into ergpair */
     float *ergpair;       /* [capacity] shared pair energies */
     int32_t *nergpair;    /* [1] device counter: entries used */
+    int32_t *mirror;      /* [nmol*M] or NULL: index (m*M+s) of the partner's entry that
+                             shares the same energy slot, -1 for an intramolecular entry;
+                             written by epsr_fmolec1, read by the fast molfit path */
 } epsr_store_t;
 
 /* ------------------------------------------------------------------ lifecycle / info */
@@ -137,9 +140,13 @@ typedef struct {
                                        device cosine (test hook for bit-identity) */
     float *trace_den;               /* NULL or [nmol]: en_change value per move */
     int32_t *trace_acc;             /* NULL or [nmol]: 1 accepted, 0 rejected */
-    int32_t strict;                 /* 1: en_change summed in list order (bit-identical);
-                                       0: summed in double */
-    int32_t *status;                /* [1] device: 0 ok, 1 a molecule exceeds 64 atoms */
+    int32_t strict;                 /* 1: the sequential kernel, en_change summed in list
+                                       order (bit-identical); 0: the fast path -- every
+                                       proposal and pair energy of the cycle computed in
+                                       parallel, decisions resolved in visit order, each
+                                       move's change summed in double */
+    int32_t *status;                /* [1] device: 0 ok, 1 a molecule exceeds 64 atoms,
+                                       2 the fast path's resolver timed out (cycle not applied) */
 } epsr_mc_t;
 
 /* molfit molfit.py:52-541, whole-molecule branch (:268-448) and step adaptation
@@ -149,6 +156,8 @@ typedef struct {
  * coordination constraints, container forces, coarse graining -- the host refuses those.
  * scratch: device bytes from epsr_molfit_scratch_bytes. */
 int64_t epsr_molfit_scratch_bytes(int32_t nmol, int32_t natom, int32_t nnbrefmax);
+/* Bytes of the per-cycle buffers of the fast path for nmoltype molecule types. */
+int64_t epsr_molfit_spec_scratch_bytes(int32_t nmol, int32_t natom, int32_t nnbrefmax, int32_t nmoltype);
 int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
                 void *scratch, int64_t scratch_bytes, void *stream);
 

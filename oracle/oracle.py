@@ -203,7 +203,7 @@ def store_c(st):
 
 def en_mole_pair(box, im, jm):
     h = SysHandle(box)
-    return f32(lib().oracle_en_mole_pair(C.byref(h.c), im, jm))
+    return f32(lib().oracle_en_mole_pair(C.byref(h.c), int(im), int(jm)))
 
 
 # ----------------------------------------------------------------------------- molfit

@@ -157,6 +157,46 @@ def test_molfit_device_bit_identical_with_reference_cosines(case):
         assert np.array_equal(m["ran1"].iv, z[p + "ran1_after_iv"])
 
 
+@pytest.mark.parametrize("case", goldens.CASES)
+def test_molfit_fast_path_matches_reference_with_reference_cosines(case):
+    """The speculative cycle (all proposals and pair energies in parallel, decisions resolved
+    in visit order, each move's change summed in double): coordinates, stored energies, step
+    sizes, counters and the ran1 state equal the reference's; the per-move change is within
+    the energy tolerance of the reference's float32 sum."""
+    z, box, d = _prepare(case)
+    _mc(d, z, box)
+    ob = BoxArrays.from_golden(z)
+    oc = oracle.cell_list(ob, int(z["in_nmolcell"]), f32(z["in_sepmax"]))
+    ost = oracle.fmolec1(ob, oc, z["in_eintra"])
+    nmt = box.nmoltype
+    omc = dict(rejrate=f32(z["in_rejrate"]), stepr=f32(z["in_stepr"]), stepm=f32(z["in_stepm"]),
+               wholerot=z["in_wholerot"].copy(), wholetrans=z["in_wholetrans"].copy(),
+               internrot=np.zeros(nmt, f32), interntrans=np.zeros(nmt, f32), ireset=0)
+    ran1 = Ran1State.from_golden(z, "mf_ran1_before_")
+    for cyc in range(int(z["mf_cycles"])):
+        p = f"mf{cyc}_"
+        d.molfit(strict=False, cos_override=z[p + "cos"])
+        d.check_status()
+        m = d.download_mc()
+        _, tr, ran1 = oracle.molfit(ob, oc, ost, omc, ran1)
+        tol = ENERGY_RTOL * tr["scale64"] + 1e-6
+        assert np.all(np.abs(m["den"].astype(np.float64) - tr["den64"]) <= tol), cyc
+        assert np.array_equal(m["acc"], z[p + "den"].shape[0] and tr["acc"]), cyc
+        co = d.download_coords()
+        for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+            assert_bits_equal(co[k], z[p + k], p + k)
+        st = d.download_store()
+        assert_bits_equal(st["ergpair"], z[p + "ergpair"], p + "ergpair")
+        assert_bits_equal(m["wholerot"], z[p + "wholerot"], p + "wholerot")
+        assert_bits_equal(m["wholetrans"], z[p + "wholetrans"], p + "wholetrans")
+        assert np.array_equal(m["nwhole"], z[p + "nwhole"])
+        assert np.array_equal(m["nmovem"], z[p + "nmovem"])
+        assert np.array_equal(m["nstepreject"], z[p + "nstepreject"])
+        assert abs(float(m["fadds"]) - float(z[p + "fadds"])) <= 1e-5 * max(1.0, abs(float(z[p + "fadds"])))
+        assert m["ran1"].idum == int(z[p + "ran1_after_idum"])
+        assert np.array_equal(m["ran1"].iv, z[p + "ran1_after_iv"])
+
+
 def _check_chain(case, strict):
     """Device cosines: energies within ENERGY_RTOL of the FP64 restatement and the same
     accept/reject decisions as the reference, except where the Metropolis margin is inside
