@@ -35,7 +35,8 @@ class Box(C.Structure):
 
 class Cells(C.Structure):
     _fields_ = [("ncelldiva", I32), ("ncelldivb", I32), ("ncelldivc", I32), ("ncell", I32), ("ncellneighb", I32),
-                ("maxcellno", I32), ("molcellno", P), ("cell_start", P), ("cell_mols", P), ("offsets", P)]
+                ("maxcellno", I32), ("molcellno", P), ("cell_start", P), ("cell_mols", P), ("offsets", P),
+                ("nnbrefmax", I32)]
 
 
 class Store(C.Structure):
@@ -58,7 +59,7 @@ _SIGS = {
     "epsr_ran1_fill": (C.c_int, [P, P, I64, P]),
     "epsr_cell_dims": (C.c_int, [I32, I32, P, P]),
     "epsr_cell_list": (C.c_int, [P, P, P, I32, I32, F32, P, P, C.POINTER(Cells), P, I64, P]),
-    "epsr_nnbrefmax": (C.c_int, [C.POINTER(Cells), P, P]),
+    "epsr_nnbrefmax": (C.c_int, [C.POINTER(Cells), P, P, P]),
     "epsr_box_positions": (C.c_int, [C.POINTER(Box), P]),
     "epsr_fmolec1_scratch_bytes": (I64, [I32, I32, I32]),
     "epsr_fmolec1": (C.c_int, [C.POINTER(Box), C.POINTER(Cells), P, C.POINTER(Store), P, I64, I32, P, P]),
@@ -71,8 +72,9 @@ _SIGS = {
     "epsr_atogen_scratch_bytes": (I64, [I32, I32, I32, I32]),
     "epsr_atogen_last_pair_updates": (I64, []),
     "epsr_gensq": (C.c_int, [I32, I32, I32, P, I32, P, I64, I64, P, P, P, P, P]),
-    "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P]),
-    "epsr_fit_expansion": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, P, P]),
+    "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),
+    "epsr_stog_scratch_bytes": (I64, [I32, I32]),
+    "epsr_fit_expansion": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, I32, P, P]),
     "epsr_fit_expansion_scratch_bytes": (I64, [I32, I32]),
 }
 

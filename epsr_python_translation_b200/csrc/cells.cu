@@ -209,6 +209,25 @@ __global__ void region_count_kernel(const int32_t *start, const int32_t *offsets
     atomicMax(maxnn, n);
 }
 
+// nnbrefmax with the offset count read on the device (no host round trip)
+__global__ void region_count_dev_kernel(const int32_t *start, const int32_t *offsets, const int32_t *noff_p, int na,
+                                        int nb, int nc, int32_t *maxnn) {
+    int c0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c0 >= na * nb * nc) return;
+    const int noff = *noff_p;
+    int icc = c0 / (na * nb);
+    int ibb = (c0 - icc * na * nb) / na;
+    int iaa = c0 - na * (ibb + nb * icc);
+    int n = 0;
+    for (int k = 0; k < noff; ++k) {
+        int a = fold(iaa + offsets[3 * k], na), b = fold(ibb + offsets[3 * k + 1], nb),
+            c = fold(icc + offsets[3 * k + 2], nc);
+        int cell = a + na * (b + nb * c);
+        n += start[cell + 1] - start[cell];
+    }
+    atomicMax(maxnn, n);
+}
+
 }  // namespace epsr
 
 using namespace epsr;
@@ -251,7 +270,8 @@ extern "C" int epsr_cell_list(const float *xadd, const float *yadd, const float 
     if (rc) return rc;
     const int ncell = dims[3];
     if (scratch_len < 2LL * ncell + 4) {
-        epsr_set_error("epsr_cell_list: scratch needs %lld int32, got %lld", 2LL * ncell + 4, (long long)scratch_len);
+        epsr_set_error("epsr_cell_list: scratch needs %lld int32, got %lld", 2LL * ncell + 4,
+                       (long long)scratch_len);
         return EPSR_ERR_CAPACITY;
     }
     cudaStream_t s = (cudaStream_t)stream;
@@ -267,8 +287,10 @@ extern "C" int epsr_cell_list(const float *xadd, const float *yadd, const float 
                                                            cells->cell_mols);
     cell_sort_kernel<<<(ncell + 127) / 128, 128, 0, s>>>(cells->cell_start, ncell, cells->cell_mols);
     cell_offsets_kernel<<<1, 1024, 0, s>>>(dims[0], dims[1], dims[2], rmax, L, cells->offsets, misc + 1);
+    region_count_dev_kernel<<<(ncell + 127) / 128, 128, 0, s>>>(cells->cell_start, cells->offsets, misc + 1, dims[0],
+                                                                dims[1], dims[2], misc + 2);
     EPSR_CUDA(cudaGetLastError());
-    int32_t host[2];
+    int32_t host[3];
     EPSR_CUDA(cudaMemcpyAsync(host, misc, sizeof(host), cudaMemcpyDeviceToHost, s));
     EPSR_CUDA(cudaStreamSynchronize(s));
     cells->ncelldiva = dims[0];
@@ -277,23 +299,21 @@ extern "C" int epsr_cell_list(const float *xadd, const float *yadd, const float 
     cells->ncell = ncell;
     cells->maxcellno = host[0];
     cells->ncellneighb = host[1];
+    cells->nnbrefmax = host[2];
     return EPSR_OK;
 }
 
-extern "C" int epsr_nnbrefmax(const epsr_cells_t *cells, int32_t *out, void *stream) {
-    if (!cells || !out) {
+extern "C" int epsr_nnbrefmax(const epsr_cells_t *cells, int32_t *out, int32_t *d, void *stream) {
+    if (!cells || !out || !d) {
         epsr_set_error("epsr_nnbrefmax: null pointer");
         return EPSR_ERR_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    int32_t *d = nullptr;
-    EPSR_CUDA(cudaMallocAsync((void **)&d, sizeof(int32_t), s));
     EPSR_CUDA(cudaMemsetAsync(d, 0, sizeof(int32_t), s));
     region_count_kernel<<<(cells->ncell + 127) / 128, 128, 0, s>>>(cells->cell_start, cells->offsets,
                                                                    cells->ncellneighb, cells->ncelldiva,
                                                                    cells->ncelldivb, cells->ncelldivc, nullptr, d);
     EPSR_CUDA(cudaMemcpyAsync(out, d, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaFreeAsync(d, s));
     EPSR_CUDA(cudaStreamSynchronize(s));
     return EPSR_OK;
 }

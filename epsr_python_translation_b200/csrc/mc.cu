@@ -457,12 +457,9 @@ extern "C" int epsr_en_change(const epsr_box_t *box, const epsr_store_t *store, 
     }
     McDev D = make_mcdev(box, nullptr, store);
     cudaStream_t s = (cudaStream_t)stream;
-    float *d = nullptr;
-    EPSR_CUDA(cudaMallocAsync((void **)&d, sizeof(float), s));
-    en_change_kernel<<<1, 256, 0, s>>>(D, im, ergnew, d);
+    en_change_kernel<<<1, 256, 0, s>>>(D, im, ergnew, ergnew);  // the total goes to slot 0
     EPSR_CUDA(cudaGetLastError());
-    EPSR_CUDA(cudaMemcpyAsync(out_host, d, sizeof(float), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaFreeAsync(d, s));
+    EPSR_CUDA(cudaMemcpyAsync(out_host, ergnew, sizeof(float), cudaMemcpyDeviceToHost, s));
     EPSR_CUDA(cudaStreamSynchronize(s));
     return EPSR_OK;
 }

@@ -40,7 +40,7 @@ __global__ void lorch_kernel(const float *q, int ldq, int npairs, const int32_t 
     const int in = blockIdx.y;
     if (i >= ldq) return;
     const float pi = 3.14159265358979323846f;
-    const float qmax = __fdiv_rn(pi, q[nqmax[in]]);
+    const float qmax = __fdiv_rn(pi, q[min(ldq - 1, max(1, nqmax[in]))]);
     const float x = __fmul_rn(qmax, q[i]);
     float r;
     if (x == 0.0f) r = 1.0f;
@@ -49,17 +49,21 @@ __global__ void lorch_kernel(const float *q, int ldq, int npairs, const int32_t 
     lw[(size_t)in * ldq + i] = r;
 }
 
-__global__ void stog_kernel(float sfac, const float *q, int ldq, const float *sofq, const float *r, int nr, int npairs,
+__global__ void stog_kernel(float rho, const float *q, int ldq, const float *sofq, const float *r, int nr, int npairs,
                             const int32_t *nqmin, const int32_t *nqmax, const float *xwt, const float *lw,
                             float *gofr) {
     const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int in = blockIdx.y;
     if (j > nr) return;
+    // sfac = 0.5*qstep/pi/pi/rho with qstep = q(4)-q(3) (ato_manipulation_rev4.py:4075-4076)
+    const float pi = 3.14159265358979323846f;
+    const float qstep = __fsub_rn(q[4], q[3]);
+    const float sfac = __fdiv_rn(__fdiv_rn(__fdiv_rn(__fmul_rn(0.5f, qstep), pi), pi), rho);
     const float rr = r[j];
     const float *s = sofq + (size_t)in * ldq;
     const float *l = lw + (size_t)in * ldq;
     float sumi = 0.0f;
-    const int i0 = nqmin[in], i1 = nqmax[in];
+    const int i0 = max(1, nqmin[in]), i1 = min(ldq - 1, nqmax[in]);
     if (rr > 0.0f) {
         for (int i = i0; i <= i1; ++i) {
             const float qq = __ldg(q + i);
@@ -95,39 +99,26 @@ extern "C" int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float 
     return EPSR_OK;
 }
 
+extern "C" int64_t epsr_stog_scratch_bytes(int32_t npairs, int32_t ldq) {
+    return (int64_t)sizeof(float) * npairs * (int64_t)ldq + 256;
+}
+
 extern "C" int epsr_stog(float rho, const float *q, int32_t ldq, const float *sofq, const float *r, int32_t nr,
-                         int32_t npairs, const int32_t *nqmin_h, const int32_t *nqmax_h, const float *xwt, float *gofr,
-                         void *stream) {
-    if (!q || !sofq || !r || !nqmin_h || !nqmax_h || !xwt || !gofr || ldq < 5 || nr <= 0 || npairs <= 0) {
+                         int32_t npairs, const int32_t *nqmin, const int32_t *nqmax, const float *xwt, float *gofr,
+                         void *scratch, int64_t scratch_bytes, void *stream) {
+    if (!q || !sofq || !r || !nqmin || !nqmax || !xwt || !gofr || !scratch || ldq < 5 || nr <= 0 || npairs <= 0) {
         epsr_set_error("epsr_stog: bad arguments");
         return EPSR_ERR_ARG;
     }
-    for (int in = 0; in < npairs; ++in)
-        if (nqmin_h[in] < 1 || nqmax_h[in] >= ldq || nqmax_h[in] < 1) {
-            epsr_set_error("epsr_stog: nqmin/nqmax out of range for pair %d", in);
-            return EPSR_ERR_ARG;
-        }
+    if (scratch_bytes < epsr_stog_scratch_bytes(npairs, ldq)) {
+        epsr_set_error("epsr_stog: scratch too small");
+        return EPSR_ERR_CAPACITY;
+    }
     cudaStream_t s = (cudaStream_t)stream;
-    float qh[2];
-    EPSR_CUDA(cudaMemcpyAsync(qh, q + 3, sizeof(qh), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
-    const float pi = 3.14159265358979323846f;
-    volatile float qstep = qh[1] - qh[0];
-    volatile float t1 = 0.5f * qstep;
-    volatile float t2 = t1 / pi;
-    volatile float t3 = t2 / pi;
-    const float sfac = t3 / rho;
-    int32_t *d_lim = nullptr;
-    float *lw = nullptr;
-    EPSR_CUDA(cudaMallocAsync((void **)&d_lim, sizeof(int32_t) * 2 * npairs, s));
-    EPSR_CUDA(cudaMallocAsync((void **)&lw, sizeof(float) * (size_t)npairs * ldq, s));
-    EPSR_CUDA(cudaMemcpyAsync(d_lim, nqmin_h, sizeof(int32_t) * npairs, cudaMemcpyHostToDevice, s));
-    EPSR_CUDA(cudaMemcpyAsync(d_lim + npairs, nqmax_h, sizeof(int32_t) * npairs, cudaMemcpyHostToDevice, s));
-    lorch_kernel<<<dim3((ldq + 127) / 128, npairs), 128, 0, s>>>(q, ldq, npairs, d_lim + npairs, lw);
-    stog_kernel<<<dim3((nr + 127) / 128, npairs), 128, 0, s>>>(sfac, q, ldq, sofq, r, nr, npairs, d_lim, d_lim + npairs,
-                                                               xwt, lw, gofr);
+    float *lw = (float *)scratch;
+    lorch_kernel<<<dim3((ldq + 127) / 128, npairs), 128, 0, s>>>(q, ldq, npairs, nqmax, lw);
+    stog_kernel<<<dim3((nr + 127) / 128, npairs), 128, 0, s>>>(rho, q, ldq, sofq, r, nr, npairs, nqmin, nqmax, xwt,
+                                                               lw, gofr);
     EPSR_CUDA(cudaGetLastError());
-    EPSR_CUDA(cudaFreeAsync(lw, s));
-    EPSR_CUDA(cudaFreeAsync(d_lim, s));
     return EPSR_OK;
 }

@@ -114,6 +114,14 @@ class DeviceBox:
         return out[:n]
 
     # ------------------------------------------------------------------ cell list
+    def _buf(self, name, n, dtype):
+        """A persistent device buffer of at least n elements (reallocated only to grow)."""
+        t = getattr(self, name, None)
+        if t is None or t.numel() < n or t.dtype != dtype:
+            t = torch.zeros(max(int(n), 1), dtype=dtype, device=self.dev)
+            setattr(self, name, t)
+        return t
+
     def cell_list(self, nmolcell, rmax):
         b = self.host
         dims = np.zeros(4, np.int32)
@@ -123,20 +131,18 @@ class DeviceBox:
                                       dims.ctypes.data_as(C.c_void_p)))
         ncell = int(dims[3])
         c = _lib.Cells()
-        self.c_molcellno = torch.zeros(b.nmol, dtype=torch.int32, device=self.dev)
-        self.c_start = torch.zeros(ncell + 1, dtype=torch.int32, device=self.dev)
-        self.c_mols = torch.zeros(b.nmol, dtype=torch.int32, device=self.dev)
-        self.c_off = torch.zeros(3 * ncell, dtype=torch.int32, device=self.dev)
-        scr = torch.zeros(2 * ncell + 4, dtype=torch.int32, device=self.dev)
+        self.c_molcellno = self._buf("_c_molcellno", b.nmol, torch.int32)
+        self.c_start = self._buf("_c_start", ncell + 1, torch.int32)
+        self.c_mols = self._buf("_c_mols", b.nmol, torch.int32)
+        self.c_off = self._buf("_c_off", 3 * ncell, torch.int32)
+        scr = self._buf("_c_scr", 2 * ncell + 4, torch.int32)
         c.molcellno, c.cell_start, c.cell_mols, c.offsets = (_ptr(t) for t in
                                                              (self.c_molcellno, self.c_start, self.c_mols, self.c_off))
         check(self.lib.epsr_cell_list(_ptr(self.xadd), _ptr(self.yadd), _ptr(self.zadd), b.nmol, nmolcell,
                                       float(f32(rmax)), lat6.ctypes.data_as(C.c_void_p),
                                       lat9.ctypes.data_as(C.c_void_p), C.byref(c), _ptr(scr), scr.numel(), _stream()))
         self.cells = c
-        out = np.zeros(1, np.int32)
-        check(self.lib.epsr_nnbrefmax(C.byref(c), out.ctypes.data_as(C.c_void_p), _stream()))
-        self.nnbrefmax = int(out[0])
+        self.nnbrefmax = int(c.nnbrefmax)
         return c
 
     def download_cells(self):
@@ -156,17 +162,20 @@ class DeviceBox:
         need = b.nmol + (b.nmol * M) // 2 + 16
         cap = max(cap, min(need, 2**31 - 1))
         st = _lib.Store()
-        self.s_nergpairm = torch.zeros(b.nmol, dtype=torch.int32, device=self.dev)
-        self.s_mol = torch.zeros(b.nmol * M, dtype=torch.int32, device=self.dev)
-        self.s_ref = torch.zeros(b.nmol * M, dtype=torch.int32, device=self.dev)
-        self.s_erg = torch.zeros(cap, dtype=torch.float32, device=self.dev)
-        self.s_n = torch.zeros(1, dtype=torch.int32, device=self.dev)
-        self.s_mirror = torch.zeros(b.nmol * M, dtype=torch.int32, device=self.dev)
+        self.s_nergpairm = self._buf("_s_nergpairm", b.nmol, torch.int32)
+        self.s_mol = self._buf("_s_mol", b.nmol * M, torch.int32)
+        self.s_ref = self._buf("_s_ref", b.nmol * M, torch.int32)
+        self.s_erg = self._buf("_s_erg", cap, torch.float32)
+        self.s_n = self._buf("_s_n", 1, torch.int32)
+        self.s_mirror = self._buf("_s_mirror", b.nmol * M, torch.int32)
+        cap = int(self.s_erg.numel())
         st.mirror = _ptr(self.s_mirror)
         st.nnbrefmax, st.capacity = M, cap
         st.nergpairm, st.molergpair, st.ergpairref, st.ergpair, st.nergpair = (
             _ptr(t) for t in (self.s_nergpairm, self.s_mol, self.s_ref, self.s_erg, self.s_n))
-        self.eintra = self._t(eintra, f32)
+        if getattr(self, "_eintra_src", None) is not eintra:
+            self.eintra = self._t(eintra, f32)
+            self._eintra_src = eintra
         nb = self.lib.epsr_fmolec1_scratch_bytes(b.nmol, self.cells.ncell, M)
         scr = self.scratch("fmolec1", nb)
         out2 = np.zeros(2, f32)

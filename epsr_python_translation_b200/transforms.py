@@ -46,16 +46,17 @@ def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
     npairs, ldq = sofq_pairs.shape
     nr = r.shape[0] - 1
     qd, sd, rd, xd = _dev(q), _dev(sofq_pairs), _dev(r), _dev(xwt)
+    lo, hi = _dev(nqmin, torch.int32), _dev(nqmax, torch.int32)
     out = torch.zeros(npairs * (nr + 1), dtype=torch.float32, device="cuda")
-    nqmin = np.ascontiguousarray(nqmin, np.int32)
-    nqmax = np.ascontiguousarray(nqmax, np.int32)
-    check(lib.epsr_stog(float(f32(rho)), _p(qd), ldq, _p(sd), _p(rd), nr, npairs, nqmin.ctypes.data_as(C.c_void_p),
-                        nqmax.ctypes.data_as(C.c_void_p), _p(xd), _p(out), _s()))
+    nb = int(lib.epsr_stog_scratch_bytes(npairs, ldq))
+    scr = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    check(lib.epsr_stog(float(f32(rho)), _p(qd), ldq, _p(sd), _p(rd), nr, npairs, _p(lo), _p(hi), _p(xd), _p(out),
+                        _p(scr), nb, _s()))
     return out.view(npairs, nr + 1)
 
 
 def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1_t, acceptr=0.0,
-                  rejrat=0.0, chisqnew=0.0):
+                  rejrat=0.0, chisqnew=0.0, strict=True):
     """fit_expansion epsr_standalone_rev3.py:4806 (1-based arrays).  ran1_t: device int32[35]."""
     lib = _lib.load(require_device=True)
     y = _dev(yin)
@@ -68,7 +69,7 @@ def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfr
     scr = torch.empty(int(nb), dtype=torch.uint8, device="cuda")
     trials = np.zeros(1, np.int64)
     check(lib.epsr_fit_expansion(_p(y), _p(e), _p(yout), _p(wt), _p(wto), scal.ctypes.data_as(C.c_void_p), nmin, npt,
-                                 ncfirst, nterms, nits, nfreq, _p(ran1_t), _p(scr), scr.numel(),
+                                 ncfirst, nterms, nits, nfreq, _p(ran1_t), _p(scr), scr.numel(), 1 if strict else 0,
                                  trials.ctypes.data_as(C.c_void_p), _s()))
     return dict(wt=wt, wtold=wto, yout=yout, stepr=f32(scal[0]), acceptr=f32(scal[1]), rejrat=f32(scal[2]),
                 chisq=f32(scal[3]), trials=int(trials[0]))

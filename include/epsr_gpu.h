@@ -61,6 +61,7 @@ typedef struct {
     int32_t *cell_start;  /* [ncell+1] */
     int32_t *cell_mols;   /* [nmol] */
     int32_t *offsets;     /* [3*ncell] (ia, ib, ic) neighbour-cell offsets, first ncellneighb used */
+    int32_t nnbrefmax;    /* largest neighbour-region size (get_nnbrefmax), written by epsr_cell_list */
 } epsr_cells_t;
 
 /* Pair-energy store of module ergpairreference (ergpairreference.py:63-210). */
@@ -105,8 +106,9 @@ int epsr_cell_list(const float *xadd, const float *yadd, const float *zadd, int3
                    float rmax, const float *lat6_host, const float *lat9_host, epsr_cells_t *cells,
                    int32_t *scratch_i32, int64_t scratch_len, void *stream);
 
-/* get_nnbrefmax cellneighbourlist.py:211-233 (synchronous; returns the value via out). */
-int epsr_nnbrefmax(const epsr_cells_t *cells, int32_t *out_host, void *stream);
+/* get_nnbrefmax cellneighbourlist.py:211-233 (synchronous; returns the value via out;
+ * scratch_i32: one device int). */
+int epsr_nnbrefmax(const epsr_cells_t *cells, int32_t *out_host, int32_t *scratch_i32, void *stream);
 
 /* ------------------------------------------------------------------ positions */
 /* Refresh box->pos from xa/ya/za + xadd/yadd/zadd (the float adds of en_change
@@ -162,7 +164,8 @@ int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *
                 void *scratch, int64_t scratch_bytes, void *stream);
 
 /* en_change molfit.py:806-919 for one molecule at its current coordinates against its
- * stored list (ergnew out [nnbrefmax], device); *out_host = dE.  Synchronous. */
+ * stored list: ergnew out [nnbrefmax] (device; slots 1.. as the reference, slot 0 receives
+ * the total), *out_host = dE.  Synchronous. */
 int epsr_en_change(const epsr_box_t *box, const epsr_store_t *store, int32_t im, float *ergnew, float *out_host,
                    void *stream);
 
@@ -195,21 +198,26 @@ int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float *wav, int32
 
 /* stog ato_manipulation_rev4.py:4067-4121 (+ lorch :4113).  q [ldq] 1-based, sofq
  * [npairs*ldq] (sofq(i,in) at [in*ldq+i]), r [nr+1] 1-based, gofr out [npairs*(nr+1)],
- * nqmin/nqmax/xwt [npairs].  rho, qstep-derived constants as the reference. */
+ * nqmin/nqmax (device, [npairs] each), xwt [npairs].  scratch: device bytes from
+ * epsr_stog_scratch_bytes.  The limits are checked on the device (error via the return of
+ * the next synchronising call is not needed: out-of-range limits are clamped to 1..ldq-1). */
+int64_t epsr_stog_scratch_bytes(int32_t npairs, int32_t ldq);
 int epsr_stog(float rho, const float *q, int32_t ldq, const float *sofq, const float *r, int32_t nr,
-              int32_t npairs, const int32_t *nqmin_host, const int32_t *nqmax_host, const float *xwt, float *gofr,
-              void *stream);
+              int32_t npairs, const int32_t *nqmin, const int32_t *nqmax, const float *xwt, float *gofr,
+              void *scratch, int64_t scratch_bytes, void *stream);
 
 /* ------------------------------------------------------------------ fit_expansion */
 /* fit_expansion epsr_standalone_rev3.py:4806-4921 (+ expand :4924, smoop
  * auxiliary_routines.py:744).  yin [npt+1], expr [npt*nterms+1] (1-based flat, row-major by
  * Q row as the reference), yout [npt+1], wt/wtold [nterms+1] (device, 1-based).
  * scal_host[4] in/out = {stepr, acceptr, rejrat, chisqnew}; returns trials via
- * *trials_host.  ran1: device state.  Synchronous. */
+ * *trials_host.  ran1: device state.  strict=1 sums chi^2 in the reference's row order
+ * (bit-identical); strict=0 in double.  Runs on one thread-block cluster whose CTAs keep the
+ * basis rows in shared memory (up to 8 CTAs).  Synchronous. */
 int epsr_fit_expansion(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
                        float *scal_host, int32_t nmin, int32_t npt, int32_t ncfirst, int32_t nterms, int32_t nits,
-                       int32_t nfreq, int32_t *ran1, void *scratch, int64_t scratch_bytes, int64_t *trials_host,
-                       void *stream);
+                       int32_t nfreq, int32_t *ran1, void *scratch, int64_t scratch_bytes, int32_t strict,
+                       int64_t *trials_host, void *stream);
 int64_t epsr_fit_expansion_scratch_bytes(int32_t npt, int32_t nterms);
 
 #ifdef __cplusplus
