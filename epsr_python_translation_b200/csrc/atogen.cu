@@ -24,43 +24,94 @@ struct AgDev {
     const float *rminex;
 };
 
-// (1) selection.  draws: [nsel_candidates] ran1 values for im in [im1, im2].
-__global__ void ag_select_kernel(AgDev A, const float *draws, int im1, int im2, float probaccept,
-                                 const int32_t *itype, int32_t *origins, int32_t *norigin, float *csampled,
-                                 long long *pairs_out) {
-    if (threadIdx.x != 0) return;
-    // molecular fraction of every type: float adds of 1.0, then / nmol (:3753-3756)
-    int cntt[64];
-    int nmt = A.nmoltype < 64 ? A.nmoltype : 64;
-    for (int t = 0; t < nmt; ++t) cntt[t] = 0;
-    for (int m = 0; m < A.nmol; ++m) cntt[A.mtype[m]]++;
-    int sampled[64];
-    float frac[64];
-    for (int t = 0; t < nmt; ++t) {
-        sampled[t] = 0;
-        frac[t] = __fdiv_rn((float)cntt[t], (float)A.nmol);
+// (1) selection.  draws: one ran1 value per candidate im in [im1, im2] (:3765).  The rule
+// "u < probaccept or type not yet sampled or type fraction < probaccept" is sequential only
+// through "not yet sampled", which holds exactly for the first candidate of each type; so the
+// selection is a parallel filter followed by an ordered compaction (one block).  It also
+// returns the per-type atom counts of the sampled molecules (csampled, exact integers like the
+// reference's float sums of 1.0), the origin-atom prefix and the pair-update count.
+__device__ __forceinline__ int ag_bscan(int v, int *total) {
+    __shared__ int ws[32];
+    __shared__ int wp[33];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
     }
-    for (int t = 0; t < A.ntype; ++t) csampled[t] = 0.0f;
-    long long pairs = 0;
-    if (A.full) {
-        const int m = A.nmol - 1;
-        for (int a = A.naf[m]; a < A.naf[m] + A.nato[m]; ++a) csampled[itype[a]] = __fadd_rn(csampled[itype[a]], 1.0f);
-    }
-    int n = 0;
-    for (int im = im1; im <= im2; ++im) {
-        const float u = draws[im - im1];
-        const int mt = A.mtype[im];
-        if (u < probaccept || sampled[mt] < 1 || frac[mt] < probaccept) {
-            sampled[mt]++;
-            origins[n++] = im;
-            for (int a = A.naf[im]; a < A.naf[im] + A.nato[im]; ++a)
-                csampled[itype[a]] = __fadd_rn(csampled[itype[a]], 1.0f);
-            const long long tgt = A.full ? (long long)(A.natom - A.naf[im] - A.nato[im]) : (long long)(A.natom - A.nato[im]);
-            pairs += (long long)A.nato[im] * tgt;
+    if (lane == 31) ws[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int a = 0;
+        for (int w = 0; w < nw; ++w) {
+            wp[w] = a;
+            a += ws[w];
         }
+        wp[32] = a;
     }
-    *norigin = n;
-    *pairs_out = pairs;
+    __syncthreads();
+    const int r = wp[wid] + incl - v;
+    *total = wp[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void ag_select_kernel(AgDev A, const float *draws, int im1, int im2, float probaccept,
+                                 const int32_t *itype, int32_t *origins, int32_t *prefix, int32_t *counts_out,
+                                 float *csampled, long long *pairs_out) {
+    __shared__ int first[64];
+    __shared__ int cntt[64];
+    __shared__ int catoms[64];
+    __shared__ unsigned long long spairs;
+    const int tid = threadIdx.x;
+    for (int t = tid; t < 64; t += blockDim.x) {
+        first[t] = 0x7fffffff;
+        cntt[t] = 0;
+        catoms[t] = 0;
+    }
+    if (tid == 0) spairs = 0ull;
+    __syncthreads();
+    for (int m = tid; m < A.nmol; m += blockDim.x) atomicAdd(&cntt[A.mtype[m]], 1);
+    for (int im = im1 + tid; im <= im2; im += blockDim.x) atomicMin(&first[A.mtype[im]], im);
+    if (A.full && tid == 0) {
+        const int m = A.nmol - 1;
+        for (int a = A.naf[m]; a < A.naf[m] + A.nato[m]; ++a) atomicAdd(&catoms[itype[a]], 1);
+    }
+    __syncthreads();
+    int carry = 0, acarry = 0;
+    unsigned long long mypairs = 0ull;
+    for (int base = im1; base <= im2; base += blockDim.x) {
+        const int im = base + tid;
+        int sel = 0, na = 0;
+        if (im <= im2) {
+            const int mt = A.mtype[im];
+            const float frac = __fdiv_rn((float)cntt[mt], (float)A.nmol);  // molfraction (:3753-3756)
+            sel = draws[im - im1] < probaccept || first[mt] == im || frac < probaccept;
+            if (sel) {
+                na = A.nato[im];
+                for (int a = A.naf[im]; a < A.naf[im] + na; ++a) atomicAdd(&catoms[itype[a]], 1);
+                const long long tgt = A.full ? (long long)(A.natom - A.naf[im] - na) : (long long)(A.natom - na);
+                mypairs += (unsigned long long)((long long)na * tgt);
+            }
+        }
+        int tot, atot;
+        const int pos = carry + ag_bscan(sel, &tot);
+        const int apos = acarry + ag_bscan(na, &atot);
+        if (sel) {
+            origins[pos] = im;
+            prefix[pos] = apos;
+        }
+        carry += tot;
+        acarry += atot;
+    }
+    atomicAdd(&spairs, mypairs);
+    __syncthreads();
+    for (int t = tid; t < A.ntype; t += blockDim.x) csampled[t] = (float)catoms[t];
+    if (tid == 0) {
+        counts_out[0] = carry;   // sampled molecules
+        counts_out[1] = acarry;  // origin atoms
+        *pairs_out = (long long)spairs;
+    }
 }
 
 // (2) intramolecular pairs
@@ -92,17 +143,6 @@ __global__ void ag_origin_atoms_kernel(AgDev A, const int32_t *origins, const in
     if (k >= *norigin) return;
     const int im = origins[k];
     for (int q = 0; q < A.nato[im]; ++q) oatoms[prefix[k] + q] = make_int2(A.naf[im] + q, im);
-}
-
-__global__ void ag_origin_prefix_kernel(AgDev A, const int32_t *origins, const int32_t *norigin, int32_t *prefix,
-                                        int32_t *natoms_out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int s = 0;
-    for (int k = 0; k < *norigin; ++k) {
-        prefix[k] = s;
-        s += A.nato[origins[k]];
-    }
-    *natoms_out = s;
 }
 
 // (3) intermolecular all-pairs
@@ -300,10 +340,14 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
         rc = epsr_ran1_fill(ran1, draws, ncand, stream);
         if (rc) return rc;
     }
-    ag_select_kernel<<<1, 32, 0, s>>>(A, draws, im1, im2, probaccept, box->itype, origins, misc, csampled, pairc);
+    if (box->ntype > 64) {
+        epsr_set_error("epsr_atogen: at most 64 atom types");
+        return EPSR_ERR_UNSUPPORTED;
+    }
+    ag_select_kernel<<<1, 1024, 0, s>>>(A, draws, im1, im2, probaccept, box->itype, origins, prefix, misc, csampled,
+                                         pairc);
     ag_intra_kernel<<<(nmol + 127) / 128, 128, 0, s>>>(A, box->itype, counts, pairc + 1);
     ag_molof_kernel<<<nmol, 32, 0, s>>>(A, molof);
-    ag_origin_prefix_kernel<<<1, 32, 0, s>>>(A, origins, misc, prefix, misc + 1);
     ag_origin_atoms_kernel<<<(nmol + 127) / 128, 128, 0, s>>>(A, origins, misc, prefix, oatoms);
     EPSR_CUDA(cudaGetLastError());
     int32_t hmisc[2];

@@ -43,13 +43,14 @@ __device__ __forceinline__ uint32_t mulmod_im2(uint32_t a, uint32_t b) {
     return (uint32_t)(((uint64_t)a * (uint64_t)b) % 2147483647ull);
 }
 
-size_t fx_smem_bytes(int nt, int rpc) {
+size_t fx_smem_bytes(int nt, int rpc, int ncta) {
     size_t f = (size_t)nt * rpc + 3 * (size_t)rpc + 2 * (size_t)(nt + 1) + FX_RING;
     size_t b = f * 4;
     b = (b + 15) & ~(size_t)15;
     b += 2 * sizeof(double);
     b += (size_t)FX_CK * FX_CKW * sizeof(int32_t);
     b += (size_t)FX_CK * sizeof(long long);
+    b += sizeof(float) * ((size_t)ncta * rpc + 4);
     return b;
 }
 
@@ -69,6 +70,7 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
     double *part = (double *)(fx_raw + off);        // [2] fast-mode partial sums
     int32_t *ck = (int32_t *)(part + 2);            // [FX_CK][FX_CKW]
     long long *ckpos = (long long *)(ck + FX_CK * FX_CKW);  // [FX_CK]
+    float *gat = (float *)(ckpos + FX_CK);          // [ncta*rpc] gathered residuals (16-byte aligned)
     __shared__ float s_val;
     __shared__ double s_red[FX_THREADS / 32];
     __shared__ int32_t g_tab[32];
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
     auto chisq = [&](long long gen_until, bool write_yout, bool strict_sum) -> float {
         float *sqb = sq + buf * rpc;
         double mypart = 0.0;
+        generate(gen_until);  // the generator warp works while the others evaluate rows
         if (wid != FX_GEN_WARP) {
             const int w = wid > FX_GEN_WARP ? tid - 32 : tid;  // worker index
             const int nw = blockDim.x - 32;
@@ -197,19 +200,32 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
             part[buf] = t;
         }
         cl.sync();  // every CTA's rows of this buffer are complete
-        generate(gen_until);
-        if (tid == 0) {
-            if (strict_sum) {
+        if (strict_sum) {
+            // gather all rows' residuals into this CTA's gather buffer (remote rows through
+            // distributed shared memory, in parallel), then sum them in the reference's order
+            for (int q = 0; q < ncta; ++q) {
+                const float *rs = q == rank ? sqb : cl.map_shared_rank(sq + buf * rpc, q);
+                for (int r = tid; r < rpc; r += blockDim.x) gat[q * rpc + r] = rs[r];
+            }
+            __syncthreads();
+            if (tid == 0) {
+                const int a = F.nmin - 1, b = F.npt;  // 0-based rows a..b-1
                 float c = 0.0f;
-                for (int q = 0; q < ncta; ++q) {
-                    const float *rs = cl.map_shared_rank(sq + buf * rpc, q);
-                    const int r0 = 1 + q * rpc;
-                    const int n = max(0, min(rpc, F.npt - r0 + 1));
-                    const int a = max(0, F.nmin - r0);
-                    for (int r = a; r < n; ++r) c = __fadd_rn(c, rs[r]);
+                int i = a;
+                for (; i < b && (i & 3); ++i) c = __fadd_rn(c, gat[i]);
+                const float4 *g4 = (const float4 *)gat;
+                for (; i + 3 < b; i += 4) {
+                    const float4 v = g4[i >> 2];
+                    c = __fadd_rn(c, v.x);
+                    c = __fadd_rn(c, v.y);
+                    c = __fadd_rn(c, v.z);
+                    c = __fadd_rn(c, v.w);
                 }
+                for (; i < b; ++i) c = __fadd_rn(c, gat[i]);
                 s_val = c;
-            } else {
+            }
+        } else if (tid == 0) {
+            {
                 double t = 0.0;
                 for (int q = 0; q < ncta; ++q) t += *cl.map_shared_rank(part + buf, q);
                 s_val = (float)t;
@@ -348,7 +364,7 @@ static int fx_cluster_size(int npt, int nterms, int *rpc_out) {
     const size_t budget = 200 * 1024;
     for (int c = 1; c <= 8; ++c) {
         const int rpc = (npt + c - 1) / c;
-        if (fx_smem_bytes(nterms, rpc) <= budget) {
+        if (fx_smem_bytes(nterms, rpc, c) <= budget) {
             *rpc_out = rpc;
             return c;
         }
@@ -408,7 +424,7 @@ extern "C" int epsr_fit_expansion(const float *yin, const float *expr, float *yo
     F.ran1 = ran1;
     F.scal = scal;
     F.trials = trials;
-    const size_t shm = fx_smem_bytes(nterms, rpc);
+    const size_t shm = fx_smem_bytes(nterms, rpc, csize);
     EPSR_CUDA(cudaFuncSetAttribute(fitexp_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(csize, 1, 1);

@@ -88,7 +88,7 @@ class EpsrIteration:
             fit = torch.matmul(self.weights[k], inter)         # weighted simulated S(Q)
             dt = -(self.data[k] - fit)
             res = transforms.fit_expansion(dt, self.expr, self.pwtold[k], self.stepp[k], 1, nq, 1, wl.nterms, 1000,
-                                           10, self.ran1)
+                                           10, self.ran1, strict=self.strict)
             self.pwtold[k] = res["wtold"]
             self.stepp[k] = res["stepr"]
             self.fit_trials += res["trials"]
