@@ -154,6 +154,75 @@ __device__ __forceinline__ void ran1_store(const Ran1 &s, int32_t *g) {
     for (int i = 0; i < 32; ++i) g[3 + i] = s.iv[i];
 }
 
+// ----------------------------------------------------------------- ran1 (device, one warp)
+// Warp-cooperative batch of the ran1 stream: lane l holds table entry iv[l]; idum/iy are
+// warp-uniform.  The Park-Miller values of the batch are jumped ahead (lane l: IA^(l+1) *
+// idum mod IM, the value Schrage's method computes) and the Bays-Durham shuffle is walked
+// with one shuffle per step.  When no value of the batch can be zero (no zero idum in the
+// batch, no zero table entry, iy != 0) the 32 steps run unrolled without checks; otherwise
+// the batch stops after a step that leaves idum or iy at zero, where the reference
+// re-initialises (auxiliary_routines.py:346).  Returns the number of values produced; lane
+// t < count receives its value in *mine.
+__device__ __forceinline__ uint32_t r1_mulmod(uint32_t a, uint32_t b) {
+    return (uint32_t)(((uint64_t)a * (uint64_t)b) % 2147483647ull);
+}
+
+__device__ __forceinline__ int ran1_warp_batch(int32_t &idum, int32_t &iy, int32_t &iv, uint32_t lane_mul, int want,
+                                               int32_t &mine, int32_t *tab_tmp /* smem [34] */) {
+    const int lane = threadIdx.x & 31;
+    if (idum <= 0 || iy == 0) {  // (re)initialisation
+        if (lane == 0) {
+            int64_t neg = -(int64_t)idum;
+            int32_t w = (int32_t)(uint32_t)(uint64_t)neg;
+            int32_t d = w > 1 ? w : 1;
+            for (int j = 40; j >= 1; --j) {
+                d = ran1_lcg(d);
+                if (j <= 32) tab_tmp[j - 1] = d;
+            }
+            tab_tmp[32] = d;
+        }
+        __syncwarp();
+        idum = tab_tmp[32];
+        iy = tab_tmp[0];
+        iv = tab_tmp[lane];
+        __syncwarp();
+    }
+    const int32_t idl = (int32_t)r1_mulmod(lane_mul, (uint32_t)idum);
+    int cnt = want < 32 ? want : 32;
+    const unsigned zero = __ballot_sync(0xffffffffu, idl == 0) | __ballot_sync(0xffffffffu, iv == 0);
+    mine = 0;
+    if (cnt == 32 && zero == 0u && iy != 0) {
+        int32_t y = iy;
+#pragma unroll
+        for (int s = 0; s < 32; ++s) {
+            const int32_t id = __shfl_sync(0xffffffffu, idl, s);
+            const int j = y >> 26;
+            const int32_t nxt = __shfl_sync(0xffffffffu, iv, j);
+            iv = (lane == j) ? id : iv;
+            y = nxt;
+            mine = (lane == s) ? y : mine;
+        }
+        iy = y;
+        idum = __shfl_sync(0xffffffffu, idl, 31);
+        return 32;
+    }
+    const unsigned z2 = __ballot_sync(0xffffffffu, lane < cnt && idl == 0);
+    if (z2) cnt = __ffs(z2);
+    int s = 0;
+    while (s < cnt) {
+        const int32_t id = __shfl_sync(0xffffffffu, idl, s);
+        const int j = iy >> 26;
+        const int32_t nxt = __shfl_sync(0xffffffffu, iv, j);
+        if (lane == j) iv = id;
+        iy = nxt;
+        if (lane == s) mine = iy;
+        ++s;
+        if (iy == 0) break;
+    }
+    idum = __shfl_sync(0xffffffffu, idl, s - 1);
+    return s;
+}
+
 // ----------------------------------------------------------------- reductions
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll

@@ -39,10 +39,6 @@ struct FxDev {
     long long *trials;
 };
 
-__device__ __forceinline__ uint32_t mulmod_im2(uint32_t a, uint32_t b) {
-    return (uint32_t)(((uint64_t)a * (uint64_t)b) % 2147483647ull);
-}
-
 size_t fx_smem_bytes(int nt, int rpc, int ncta) {
     size_t f = (size_t)nt * rpc + 3 * (size_t)rpc + 2 * (size_t)(nt + 1) + FX_RING;
     size_t b = f * 4;
@@ -73,8 +69,7 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
     float *gat = (float *)(ckpos + FX_CK);          // [ncta*rpc] gathered residuals (16-byte aligned)
     __shared__ float s_val;
     __shared__ double s_red[FX_THREADS / 32];
-    __shared__ int32_t g_tab[32];
-    __shared__ int32_t g_ini[2];
+    __shared__ int32_t g_tab[34];
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int row0 = 1 + rank * rpc;  // first (1-based) row of this CTA
@@ -100,7 +95,7 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
         g_idum = F.ran1[0];
         g_iy = F.ran1[1];
         g_iv = F.ran1[3 + lane];
-        for (int k = 0; k < lane; ++k) g_mul = mulmod_im2(g_mul, 16807u);
+        for (int k = 0; k < lane; ++k) g_mul = r1_mulmod(g_mul, 16807u);
     }
     const int32_t mcall0 = F.ran1[2];
     cl.sync();
@@ -117,42 +112,8 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
                 ckpos[slot] = g_pos;
             }
             ++g_nb;
-            if (g_idum <= 0 || g_iy == 0) {  // initialisation (auxiliary_routines.py:346-362)
-                if (lane == 0) {
-                    int64_t neg = -(int64_t)g_idum;
-                    int32_t w = (int32_t)(uint32_t)(uint64_t)neg;
-                    int32_t d = w > 1 ? w : 1;
-                    for (int j = 40; j >= 1; --j) {
-                        d = ran1_lcg(d);
-                        if (j <= 32) g_tab[j - 1] = d;
-                    }
-                    g_ini[0] = d;
-                    g_ini[1] = g_tab[0];
-                }
-                __syncwarp();
-                g_idum = g_ini[0];
-                g_iy = g_ini[1];
-                g_iv = g_tab[lane];
-                __syncwarp();
-            }
-            int cnt = 32;
-            const int32_t idl = (int32_t)mulmod_im2(g_mul, (uint32_t)g_idum);
-            const unsigned zero = __ballot_sync(0xffffffffu, idl == 0);
-            if (zero) cnt = __ffs(zero);
-            int32_t mine = 0;
-            int s = 0;
-            while (s < cnt) {
-                const int32_t id = __shfl_sync(0xffffffffu, idl, s);
-                const int j = g_iy >> 26;
-                const int32_t nxt = __shfl_sync(0xffffffffu, g_iv, j);
-                if (lane == j) g_iv = id;
-                g_iy = nxt;
-                if (lane == s) mine = g_iy;
-                ++s;
-                if (g_iy == 0) break;
-            }
-            cnt = s;
-            g_idum = __shfl_sync(0xffffffffu, idl, cnt - 1);
+            int32_t mine;
+            const int cnt = ran1_warp_batch(g_idum, g_iy, g_iv, g_mul, 32, mine, g_tab);
             if (lane < cnt) ring[(g_pos + lane) & (FX_RING - 1)] = ran1_out(mine);
             g_pos += cnt;
         }
@@ -164,7 +125,9 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
     auto chisq = [&](long long gen_until, bool write_yout, bool strict_sum) -> float {
         float *sqb = sq + buf * rpc;
         double mypart = 0.0;
-        generate(gen_until);  // the generator warp works while the others evaluate rows
+        // the generator warp works while the others evaluate rows (two batches) and while
+        // thread 0 forms chi^2 (the rest)
+        generate(gen_until < g_pos + 64 ? gen_until : g_pos + 64);
         if (wid != FX_GEN_WARP) {
             const int w = wid > FX_GEN_WARP ? tid - 32 : tid;  // worker index
             const int nw = blockDim.x - 32;
@@ -224,7 +187,11 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
                 for (; i < b; ++i) c = __fadd_rn(c, gat[i]);
                 s_val = c;
             }
-        } else if (tid == 0) {
+            generate(gen_until);  // the generator warp, while thread 0 sums
+        } else {
+            generate(gen_until);
+        }
+        if (!strict_sum && tid == 0) {
             {
                 double t = 0.0;
                 for (int q = 0; q < ncta; ++q) t += *cl.map_shared_rank(part + buf, q);

@@ -14,59 +14,21 @@
 
 namespace epsr {
 
-__device__ __forceinline__ uint32_t mulmod_im(uint32_t a, uint32_t b) {
-    return (uint32_t)(((uint64_t)a * (uint64_t)b) % 2147483647ull);
-}
-
 __global__ void ran1_fill_kernel(int32_t *state, float *out, int64_t n_host, const int32_t *n_dev) {
     const int lane = threadIdx.x & 31;
     const int64_t n = n_dev ? (int64_t)*n_dev : n_host;
-    __shared__ int32_t tab[32];
-    __shared__ int32_t ini[2];
+    __shared__ int32_t tab[34];
     int32_t idum = state[0], iy = state[1];
     const int32_t mcall = state[2];
     int32_t iv = state[3 + lane];
     __syncwarp();
     uint32_t mul = 16807u;  // IA^(lane+1) mod IM
-    for (int k = 0; k < lane; ++k) mul = mulmod_im(mul, 16807u);
+    for (int k = 0; k < lane; ++k) mul = r1_mulmod(mul, 16807u);
     int64_t done = 0;
     while (done < n) {
-        if (idum <= 0 || iy == 0) {  // warp-uniform
-            if (lane == 0) {
-                int64_t neg = -(int64_t)idum;
-                int32_t w = (int32_t)(uint32_t)(uint64_t)neg;
-                int32_t d = w > 1 ? w : 1;
-                for (int j = 40; j >= 1; --j) {
-                    d = ran1_lcg(d);
-                    if (j <= 32) tab[j - 1] = d;
-                }
-                ini[0] = d;
-                ini[1] = tab[0];
-            }
-            __syncwarp();
-            idum = ini[0];
-            iy = ini[1];
-            iv = tab[lane];
-            __syncwarp();
-        }
-        int cnt = (n - done) >= 32 ? 32 : (int)(n - done);
-        const int32_t idl = (int32_t)mulmod_im(mul, (uint32_t)idum);  // idum after lane+1 steps
-        const unsigned zero = __ballot_sync(0xffffffffu, lane < cnt && idl == 0);
-        if (zero) cnt = __ffs(zero);  // stop after the first step that leaves idum == 0
-        int32_t mine = 0;
-        int s = 0;
-        while (s < cnt) {
-            const int32_t id = __shfl_sync(0xffffffffu, idl, s);
-            const int j = iy >> 26;  // iy / NDIV, NDIV = 2^26
-            const int32_t nxt = __shfl_sync(0xffffffffu, iv, j);
-            if (lane == j) iv = id;
-            iy = nxt;
-            if (lane == s) mine = iy;
-            ++s;
-            if (iy == 0) break;      // warp-uniform; the next call re-initialises
-        }
-        cnt = s;
-        idum = __shfl_sync(0xffffffffu, idl, cnt - 1);
+        const int64_t left = n - done;
+        int32_t mine;
+        const int cnt = ran1_warp_batch(idum, iy, iv, mul, left > 32 ? 32 : (int)left, mine, tab);
         if (lane < cnt) out[done + lane] = ran1_out(mine);
         done += cnt;
     }
