@@ -10,6 +10,8 @@
 //     (potex) are counted alongside;
 // (4) normalisation in float32 exactly as the reference (counts are exact integers; the
 //     reference's float accumulation equals them while a bin stays below 2^24).
+#include <mutex>
+
 #include "common.cuh"
 
 namespace epsr {
@@ -379,4 +381,71 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
     g_last_pairs = hp[0] + hp[1];
     *ngrsamples_io = ngr;
     return EPSR_OK;
+}
+
+// ----------------------------------------------------------------- allocation-free variant
+// Some callers cannot hand this library device buffers: a host whose device memory is owned
+// by another allocator (a caching pool that must not be bypassed, or a host process that
+// reserves its whole budget up front), or a plain C/Fortran/ctypes caller with no device
+// allocator at all.  epsr_atogen_noalloc needs only the inputs and outputs: its working
+// memory and histogram counts live in one file-scope device array, sized for the reference's
+// own limits (50,000 molecules, 150,000 atoms) and at most 2^19 histogram entries.
+namespace {
+constexpr int64_t NOALLOC_MAX_NMOL = 50000;
+constexpr int64_t NOALLOC_MAX_NATOM = 150000;
+constexpr int64_t NOALLOC_MAX_COUNTS = 1 << 19;   // 2*npairs*ldw + npairs
+constexpr int64_t NOALLOC_COUNTS_BYTES = NOALLOC_MAX_COUNTS * 8;
+constexpr int64_t NOALLOC_WORK_BYTES = 4 << 20;   // >= epsr_atogen_scratch_bytes at the maxima
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) unsigned char g_atogen_noalloc[NOALLOC_COUNTS_BYTES + NOALLOC_WORK_BYTES];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[NOALLOC_MAX_DEVICES];
+}  // namespace
+
+extern "C" int epsr_atogen_noalloc(const epsr_box_t *box, int32_t npt1, float sizefactor, float dmax,
+                                   const float *rminex, const float *cfrac, const float *ycoh, const int32_t *n1extr,
+                                   const int32_t *n2extr, int32_t natomr, int32_t *ngrsamples_io, int32_t *ran1,
+                                   float *wav, int32_t ldw, float *potex, void *stream) {
+    if (!box) {
+        epsr_set_error("epsr_atogen_noalloc: null box");
+        return EPSR_ERR_ARG;
+    }
+    const int64_t ncounts = 2 * (int64_t)box->npairs * ldw + box->npairs;
+    if (box->nmol > NOALLOC_MAX_NMOL || box->natom > NOALLOC_MAX_NATOM || ncounts > NOALLOC_MAX_COUNTS) {
+        epsr_set_error("epsr_atogen_noalloc: box exceeds the built-in working memory (at most %lld molecules, %lld "
+                       "atoms, %lld histogram entries 2*npairs*ldw+npairs; got %d, %d, %lld) -- use epsr_atogen",
+                       (long long)NOALLOC_MAX_NMOL, (long long)NOALLOC_MAX_NATOM, (long long)NOALLOC_MAX_COUNTS,
+                       box->nmol, box->natom, (long long)ncounts);
+        return EPSR_ERR_CAPACITY;
+    }
+    const int64_t need = epsr_atogen_scratch_bytes(box->nmol, box->natom, box->nmoltype, box->ntype);
+    if (need > NOALLOC_WORK_BYTES) {
+        epsr_set_error("epsr_atogen_noalloc: working memory %lld bytes exceeds %lld", (long long)need,
+                       (long long)NOALLOC_WORK_BYTES);
+        return EPSR_ERR_CAPACITY;
+    }
+    // the device address of the array, looked up once per device with that device current
+    int dev = 0;
+    EPSR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        epsr_set_error("epsr_atogen_noalloc: device ordinal %d out of range", dev);
+        return EPSR_ERR_ARG;
+    }
+    void *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_atogen_noalloc);
+            if (e != cudaSuccess) return epsr_cuda_check(e, "cudaGetSymbolAddress(g_atogen_noalloc)");
+            g_noalloc_addr[dev] = p;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    unsigned long long *counts = (unsigned long long *)base;  // zeroed inside epsr_atogen
+    void *work = (unsigned char *)base + NOALLOC_COUNTS_BYTES;
+    return epsr_atogen(box, npt1, sizefactor, dmax, rminex, cfrac, ycoh, n1extr, n2extr, natomr, ngrsamples_io, ran1,
+                       wav, ldw, potex, counts, work, NOALLOC_WORK_BYTES, stream);
 }

@@ -188,6 +188,24 @@ int64_t epsr_atogen_scratch_bytes(int32_t nmol, int32_t natom, int32_t nmoltype,
 /* pair-updates counted by the last epsr_atogen call on this thread */
 int64_t epsr_atogen_last_pair_updates(void);
 
+/* epsr_atogen without caller scratch.  No counterpart in the reference: it exists for callers
+ * that cannot allocate device memory for the library -- a plain C, Fortran or ctypes host
+ * with no device allocator of its own, or a host whose device memory belongs to another
+ * allocator that must not be bypassed.  Arguments and results are those of epsr_atogen
+ * minus counts/scratch/scratch_bytes; the results are identical to epsr_atogen's.
+ * Working memory is one file-scope device array of 10 MiB per device (histogram counts plus
+ * work space), so the call allocates nothing.  Limits: nmol <= 50000, natom <= 150000 and
+ * 2*npairs*ldw + npairs <= 524288; larger boxes return EPSR_ERR_CAPACITY with the limits in
+ * epsr_last_error.  Nothing needs to start at zero: the counts are cleared inside each call.
+ * The first call on a device (with that device current) looks up the array's address once;
+ * make that first call before any stream capture.  The array is shared by every call on the
+ * device, so two calls that overlap in time (other streams or host threads) race on it and
+ * give wrong results: serialise them. */
+int epsr_atogen_noalloc(const epsr_box_t *box, int32_t npt1, float sizefactor, float dmax, const float *rminex,
+                        const float *cfrac, const float *ycoh, const int32_t *n1extr, const int32_t *n2extr,
+                        int32_t natomr, int32_t *ngrsamples_io, int32_t *ran1, float *wav, int32_t ldw,
+                        float *potex, void *stream);
+
 /* ------------------------------------------------------------------ gensq / stog */
 /* gensq epsr_standalone_rev3.py:4731-4802.  fq(j,i) = foqols[j*fq_sj + i*fq_si] (j = r
  * index 1..npt1, i = Q index 1..nq).  sofq out [2*npairs*(nq+1)]: sofq(1,i,ic) at
