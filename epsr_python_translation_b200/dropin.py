@@ -1,0 +1,517 @@
+"""Drop-in replacements for the reference's pair-path routines, with their signatures.
+
+The reference translation (package ``epsr26``) keeps its state in COMMON-block modules
+(``epsr26.common.molecom``, ``clustercom``, ``epsr16``, ``potential_par``, ``lattice``,
+``ran1com``, ``cellneighbourlist``, ``ergpairreference``, ``molecom_mod`` ...) as 1-based,
+Fortran-ordered NumPy arrays, and its callers look routines up through their module at
+call time.  ``PairPath`` holds a ``DeviceBox`` mirror of that state and provides, with the
+reference's argument lists and return values:
+
+* ``initialise_cellneighbourlist`` (library/cellneighbourlist.py:23)
+* ``fmolec1`` (library/ato_manipulation_rev4.py:2374)
+* ``molfit`` (library/molfit.py:52), whole-molecule branch
+* ``en_change`` / ``en_mole_pair`` (library/molfit.py:806 / :1528)
+* ``atogen`` (library/ato_manipulation_rev4.py:3640)
+* ``gensq`` (programs/epsr_standalone_rev3.py:4731)
+* ``stog`` (library/ato_manipulation_rev4.py:4067)
+* ``fit_expansion`` (programs/epsr_standalone_rev3.py:4806)
+
+``install()`` assigns them onto the given modules (the reference's own rerouting
+mechanism, trace.py:94-125) and keeps the originals.
+
+State protocol.  Every call is synchronous, as the reference's routines are.  On entry
+the wrapper compares the COMMON arrays it depends on with what it last wrote or uploaded
+(coordinates, potential tables, stored pair energies) and uploads what the host changed;
+the ran1 state is always uploaded.  On return it writes everything the routine changes
+back into the COMMON arrays in place (same array objects, so aliases held by other
+routines stay valid).  A call that needs a feature outside the pair path (shake or
+internal-rotation cycles, tethering, three-body terms, coordination constraints,
+container forces, coarse graining, molecules of more than 64 atoms) runs the reference's
+own routine on the host instead; the next device call picks up whatever it changed.
+
+The cell list must come from the installed ``initialise_cellneighbourlist`` (the
+reference loop rebuilds it every iteration, epsr_standalone_rev3.py:1265); a cell list
+built elsewhere is detected and refused with ``EpsrGpuError``.  Log lines the reference
+writes to unit 6 inside these routines are not reproduced.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib, transforms
+from ._lib import EpsrGpuError, check
+from .box import BoxArrays, Ran1State, trsteps
+
+f32 = np.float32
+ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit", "atogen", "stog", "gensq", "fit_expansion",
+            "en_change", "en_mole_pair")
+# en_change / en_mole_pair are per-molecule calls: rerouting them makes every host caller
+# (including host fallbacks) launch one kernel per call, so they are installed only on request.
+DEFAULT_ROUTINES = ROUTINES[:7]
+# module that owns each routine in the reference
+OWNER = {"initialise_cellneighbourlist": "cellneighbourlist", "fmolec1": "ato_manipulation_rev4",
+         "atogen": "ato_manipulation_rev4", "stog": "ato_manipulation_rev4", "molfit": "molfit",
+         "en_change": "molfit", "en_mole_pair": "molfit", "gensq": "program", "fit_expansion": "program"}
+
+
+def _fortran(shape, dtype):
+    """A zeroed 1-based Fortran-order array of the reference's form (extent + 1 per axis)."""
+    return np.zeros(tuple(int(s) + 1 for s in shape), dtype=dtype, order="F")
+
+
+def _mcall_advance(old, dev32):
+    """The reference's ran1 call counter (a Python int) after the device advanced its
+    32-bit copy from ``old`` to ``dev32``."""
+    return int(old) + ((int(np.int64(dev32) & 0xFFFFFFFF) - (int(old) & 0xFFFFFFFF)) & 0xFFFFFFFF)
+
+
+def _idiv(a, b):
+    """Fortran integer division (truncation toward zero)."""
+    q = abs(int(a)) // abs(int(b))
+    return q if (a >= 0) == (b > 0) else -q
+
+
+class PairPath:
+    """The GPU pair path bound to one set of COMMON-block modules.
+
+    ``common``: an object whose attributes are the reference's COMMON modules (the
+    package ``epsr26.common`` itself).  ``modules``: the modules that own the routines,
+    keyed ``cellneighbourlist`` (library), ``ato_manipulation_rev4``, ``molfit`` and
+    ``program`` (the loaded ``epsr`` program module holding gensq and fit_expansion).
+    ``strict``: 1 runs the sequential MC kernel and the reference's float32 summation
+    order everywhere (bit-identical apart from transcendentals); 0 runs the speculative
+    MC cycle and double sums (within the stated tolerance).
+    """
+
+    def __init__(self, common, modules, strict=False, device="cuda"):
+        self.c = common
+        self.mods = dict(modules)
+        self.strict = bool(strict)
+        self.device = device
+        self.orig = {}
+        self.d = None
+        self._snap = {}
+        self._mirror_ok = False
+        self.cos_override = None      # test hook: [3*nmol] cosines for the next molfit call
+
+    # ------------------------------------------------------------------ install
+    def install(self, routines=DEFAULT_ROUTINES):
+        for name in routines:
+            mod = self.mods[OWNER[name]]
+            if name not in self.orig:
+                self.orig[name] = getattr(mod, name)
+            setattr(mod, name, getattr(self, name))
+        return self
+
+    def uninstall(self):
+        for name, f in self.orig.items():
+            setattr(self.mods[OWNER[name]], name, f)
+        self.orig = {}
+
+    def _host(self, name, *args):
+        """Run the reference's own routine (the one replaced at install, else the module's)."""
+        f = self.orig.get(name) or getattr(self.mods[OWNER[name]], name)
+        return f(*args)
+
+    # ------------------------------------------------------------------ COMMON -> host box
+    def box_from_common(self) -> BoxArrays:
+        c = self.c
+        mc, cc, e16, pp, lat = c.molecom, c.clustercom, c.epsr16, c.potential_par, c.lattice
+        nmol, natom, ntype, npairs = int(cc.nmol), int(mc.natom), int(mc.ntype), int(mc.npairs)
+        npt = int(e16.npt)
+        ld = npt + 1
+        tab = lambda a: np.ascontiguousarray(np.asarray(a)[:ld, 1:npairs + 1].T, dtype=f32)  # noqa: E731
+        return BoxArrays(
+            naf=np.asarray(cc.naf[1:nmol + 1], np.int32) - 1, nato=np.asarray(cc.nato[1:nmol + 1], np.int32),
+            mtype=np.asarray(cc.mtype[1:nmol + 1], np.int32) - 1,
+            itype=np.asarray(mc.itype[1:natom + 1], np.int32) - 1,
+            xa=np.array(mc.xa[1:natom + 1], f32), ya=np.array(mc.ya[1:natom + 1], f32),
+            za=np.array(mc.za[1:natom + 1], f32), xadd=np.array(cc.xadd[1:nmol + 1], f32),
+            yadd=np.array(cc.yadd[1:nmol + 1], f32), zadd=np.array(cc.zadd[1:nmol + 1], f32),
+            npairref=np.ascontiguousarray(np.asarray(mc.npairref)[1:ntype + 1, 1:ntype + 1], np.int32) - 1,
+            n1extr=np.asarray(mc.n1extr[1:npairs + 1], np.int32) - 1,
+            n2extr=np.asarray(mc.n2extr[1:npairs + 1], np.int32) - 1,
+            nmoltype=int(cc.nmoltype), dmax=f32(cc.dmax), cellst=f32(e16.cellst),
+            x=np.array(e16.x[:ld], f32), xstar=np.array(e16.xstar[:ld], f32), npt=npt, npt1=int(e16.npt1),
+            npt2=int(e16.npt2), nptmax=int(e16.nptmax), xavs=tab(pp.xavs), xavs1=tab(pp.xavs1),
+            ecoul=tab(pp.ecoul), ecoul1=tab(pp.ecoul1), simt=f32(mc.simt),
+            cfrac=np.array(mc.cfrac[1:ntype + 1], f32), natomr=int(mc.natomr), cubic=bool(lat.cubic),
+            lat6=np.array([lat.alatx, lat.blatx, lat.clatx, lat.blaty, lat.claty, lat.clatz], f32),
+            lat9=np.array(list(lat.alatc[1:4]) + list(lat.blatc[1:4]) + list(lat.clatc[1:4]), f32),
+            maxmolsize=f32(mc.maxmolsize))
+
+    # ------------------------------------------------------------------ state sync
+    @staticmethod
+    def _topology(b):
+        return (b.nmol, b.natom, b.ntype, b.npairs, b.nmoltype, b.npt, b.npt1, b.npt2, b.cubic,
+                b.naf.tobytes(), b.nato.tobytes(), b.mtype.tobytes(), b.itype.tobytes(), b.npairref.tobytes(),
+                b.n1extr.tobytes(), b.n2extr.tobytes(), b.lat6.tobytes(), float(b.dmax), float(b.cellst))
+
+    @staticmethod
+    def _tables(b):
+        return (b.xavs, b.xavs1, b.ecoul, b.ecoul1, b.xstar, b.cfrac)
+
+    def _sync_in(self):
+        """Bring the device mirror up to date with the COMMON blocks; returns the host box."""
+        from .device import DeviceBox
+        b = self.box_from_common()
+        topo = self._topology(b)
+        s = self._snap
+        if self.d is None or s.get("topo") != topo:
+            self.d = DeviceBox(b, device=self.device)
+            self._mirror_ok = False
+            s.clear()
+            s["topo"] = topo
+        elif any(not np.array_equal(u, v) for u, v in zip(self._tables(b), s["tables"])) \
+                or float(b.simt) != s["simt"] or int(b.natomr) != s["natomr"]:
+            self.d.upload(b)                   # tables changed (generate_ep): full re-upload
+        elif any(not np.array_equal(getattr(b, k), s["coords"][k]) for k in ("xa", "ya", "za", "xadd", "yadd",
+                                                                              "zadd")):
+            self.d.host = b
+            self.d.upload_coords(b.xa, b.ya, b.za, b.xadd, b.yadd, b.zadd)
+        else:
+            self.d.host = b
+        s["tables"] = tuple(np.array(t) for t in self._tables(b))
+        s["simt"], s["natomr"] = float(b.simt), int(b.natomr)
+        s["coords"] = {k: np.array(getattr(b, k)) for k in ("xa", "ya", "za", "xadd", "yadd", "zadd")}
+        return b
+
+    def _coords_out(self):
+        co = self.d.download_coords()
+        mc, cc = self.c.molecom, self.c.clustercom
+        na, nm = co["xa"].shape[0], co["xadd"].shape[0]
+        mc.xa[1:na + 1], mc.ya[1:na + 1], mc.za[1:na + 1] = co["xa"], co["ya"], co["za"]
+        cc.xadd[1:nm + 1], cc.yadd[1:nm + 1], cc.zadd[1:nm + 1] = co["xadd"], co["yadd"], co["zadd"]
+        self._snap["coords"] = {k: np.array(v) for k, v in co.items()}
+
+    def _ran1_in(self):
+        r = self.c.ran1com
+        st = Ran1State(idum=int(r.idum), iy=int(r.iy), mcall=int(np.int64(r.mcall) & 0xFFFFFFFF),
+                       iv=np.asarray(r.iv[1:33], np.int32).copy())
+        self._mcall0 = int(r.mcall)
+        return self.d.ran1_tensor(st)
+
+    def _ran1_out(self, t):
+        torch.cuda.synchronize()
+        a = t.cpu().numpy()
+        r = self.c.ran1com
+        r.idum, r.iy = int(a[0]), int(a[1])
+        r.iv[1:33] = a[3:35]
+        r.mcall = _mcall_advance(self._mcall0, a[2])
+
+    def _check_cells(self):
+        cnl = self.c.cellneighbourlist
+        s = self._snap.get("cells")
+        if self.d.cells is None or s is None or cnl.molcellno is None or \
+                not np.array_equal(np.asarray(cnl.molcellno[1:]), s["molcellno"]) or \
+                not np.array_equal(np.asarray(cnl.nmolsincell[1:]), s["nmolsincell"]) or \
+                int(cnl.ncellneighb) != s["ncellneighb"]:
+            raise EpsrGpuError(4, "cell list was not built by the GPU initialise_cellneighbourlist")
+
+    def _store_in(self):
+        """Upload pair energies (or the whole store) that the host changed since the last sync."""
+        erd = self.c.ergpairreference
+        s = self._snap.get("store")
+        if s is None:
+            raise EpsrGpuError(4, "pair store was not built by the GPU fmolec1")
+        nmol, M = self.d.host.nmol, int(erd.nnbrefmax)
+        n = int(erd.nergpair)
+        nm = np.asarray(erd.nergpairm[1:nmol + 1], np.int32)
+        mol = np.ascontiguousarray(np.asarray(erd.molergpair)[1:M + 1, 1:nmol + 1].T, np.int32) - 1
+        ref = np.ascontiguousarray(np.asarray(erd.ergpairref)[1:M + 1, 1:nmol + 1].T, np.int32)
+        erg = np.array(erd.ergpair[1:n + 1], f32)
+        if M != s["M"] or n != s["n"] or not (np.array_equal(nm, s["nergpairm"]) and np.array_equal(mol, s["mol"])
+                                             and np.array_equal(ref, s["ref"])):
+            if M != self.d.nnbrefmax or n > self.d.s_erg.numel():
+                raise EpsrGpuError(4, "pair store resized outside the GPU path")
+            d = self.d
+            d.s_nergpairm[:nmol].copy_(torch.from_numpy(nm))
+            d.s_mol[:nmol * M].copy_(torch.from_numpy(mol.reshape(-1)))
+            d.s_ref[:nmol * M].copy_(torch.from_numpy(ref.reshape(-1)))
+            d.s_n[:1].copy_(torch.tensor([n], dtype=torch.int32))
+            self._mirror_ok = False            # the fast sweep's mirror index is stale
+        if not np.array_equal(erg, s["erg"]):
+            self.d.s_erg[:n].copy_(torch.from_numpy(erg))
+        s.update(M=M, n=n, nergpairm=nm, mol=mol, ref=ref, erg=erg)
+
+    def _store_out(self, values_only):
+        erd = self.c.ergpairreference
+        st = self.d.download_store()
+        nmol, M, n = self.d.host.nmol, st["nnbrefmax"], st["nergpair"]
+        if not values_only:
+            # allocation of initialise_ergpair (ergpairreference.py:63-100) and the 20%
+            # growth of reallocate_ergpair (:128-147) for n stored energies
+            cap = 100 * nmol
+            while n > cap:
+                cap = _idiv((cap + 10) * 12, 10)
+            erd.nmolhere = nmol
+            erd.nnbrefmax = M
+            erd.nergpairmax = cap
+            erd.ergpair = _fortran((cap,), f32)
+            erd.molergpair = _fortran((M, nmol), np.int32)
+            erd.ergpairref = _fortran((M, nmol), np.int32)
+            erd.nergpairm = _fortran((nmol,), np.int32)
+            erd.nnbref = 0
+            erd.ergold = _fortran((M,), f32)
+            erd.ergnew = _fortran((M,), f32)
+            erd.nbref = _fortran((M,), np.int32)
+            mol = st["molergpair"].copy()
+            for im in range(nmol):                 # unused slots stay 0 as in the reference
+                mol[im, st["nergpairm"][im]:] = -1
+            erd.molergpair[1:M + 1, 1:nmol + 1] = (mol + 1).T
+            ref = st["ergpairref"].copy()
+            for im in range(nmol):
+                ref[im, st["nergpairm"][im]:] = 0
+            erd.ergpairref[1:M + 1, 1:nmol + 1] = ref.T
+            erd.nergpairm[1:nmol + 1] = st["nergpairm"]
+            erd.nergpair = n
+        erd.ergpair[1:n + 1] = st["ergpair"]
+        nm = np.asarray(erd.nergpairm[1:nmol + 1], np.int32)
+        self._snap["store"] = dict(
+            M=M, n=n, nergpairm=nm,
+            mol=np.ascontiguousarray(np.asarray(erd.molergpair)[1:M + 1, 1:nmol + 1].T, np.int32) - 1,
+            ref=np.ascontiguousarray(np.asarray(erd.ergpairref)[1:M + 1, 1:nmol + 1].T, np.int32),
+            erg=np.array(st["ergpair"], f32))
+
+    # ------------------------------------------------------------------ feature checks
+    def _outside_path(self):
+        c = self.c
+        nmol = int(c.clustercom.nmol)
+        if getattr(c.molecom_mod, "coarsegraining", False):
+            return True
+        if int(getattr(c.threebody_mod, "nthreeb", 0)) > 0:
+            return True
+        if int(getattr(c.coordconstraints_mod, "ncoordconstraints", 0)) > 0:
+            return True
+        if float(getattr(c.containerforces_mod, "numcontainerforces", 0)) > 0.0:
+            return True
+        teth = getattr(c.clustercom, "tethered", None)
+        if teth is not None and bool(np.any(np.asarray(teth[1:nmol + 1]))):
+            return True
+        return int(np.max(np.asarray(c.clustercom.nato[1:nmol + 1]))) > 64
+
+    # ------------------------------------------------------------------ routines
+    def initialise_cellneighbourlist(self, nmolcellin, xadd, yadd, zadd, nmol, rmax):
+        """cellneighbourlist.py:23-90: fills the COMMON cell arrays (molsincell, offsets...)."""
+        cnl = self.c.cellneighbourlist
+        cnl.nmolcell = min(int(nmolcellin), int(nmol))
+        cc = self.c.clustercom
+        if xadd is not cc.xadd or yadd is not cc.yadd or zadd is not cc.zadd or int(nmol) != int(cc.nmol):
+            return self._host("initialise_cellneighbourlist", nmolcellin, xadd, yadd, zadd, nmol, rmax)
+        self._sync_in()
+        self.d.cell_list(int(nmolcellin), f32(rmax))
+        cl = self.d.download_cells()
+        ncell, mx = int(cl["ncell"]), int(cl["maxcellno"])
+        cnl.ncelldiva, cnl.ncelldivb, cnl.ncelldivc = int(cl["ncelldiva"]), int(cl["ncelldivb"]), int(cl["ncelldivc"])
+        cnl.ncell = ncell
+        cnl.ncelldivsq = cnl.ncelldiva * cnl.ncelldivb
+        cnl.maxcellno = mx
+        cnl.ncellneighb = int(cl["ncellneighb"])
+        start, mols = cl["cell_start"], cl["cell_mols"]
+        counts = np.diff(start[:ncell + 1]).astype(np.int32)
+        cnl.nmolsincell = _fortran((ncell,), np.int32)
+        cnl.nmolsincell[1:] = counts
+        cnl.molcellno = _fortran((int(nmol),), np.int32)
+        cnl.molcellno[1:] = cl["molcellno"][: int(nmol)]
+        cnl.molsincell = _fortran((mx, ncell), np.int32)
+        for c in range(ncell):
+            k = int(counts[c])
+            if k:
+                cnl.molsincell[1:k + 1, c + 1] = mols[start[c]:start[c] + k] + 1
+        for i, name in enumerate(("iacellneighb", "ibcellneighb", "iccellneighb")):
+            a = _fortran((ncell,), np.int32)
+            a[1:cnl.ncellneighb + 1] = cl["offsets"][:, i]
+            setattr(cnl, name, a)
+        self._snap["cells"] = dict(molcellno=np.array(cnl.molcellno[1:]), nmolsincell=np.array(cnl.nmolsincell[1:]),
+                                   ncellneighb=int(cnl.ncellneighb))
+        return None
+
+    def fmolec1(self, ierr, num_threads_input, ftest, ftestb, ftethered, fcoordconstraints):
+        """ato_manipulation_rev4.py:2374-2528: rebuilds the pair store in the COMMON block;
+        returns (ierr, num_threads_input, ftest, ftestb, ftethered, fcoordconstraints)."""
+        if self._outside_path():
+            return self._host("fmolec1", ierr, num_threads_input, ftest, ftestb, ftethered, fcoordconstraints)
+        if num_threads_input <= 0:
+            num_threads_input = 0          # idiv(omp_get_max_threads(), 2) with the reference's 1-thread stubs
+        mc = self.c.molecom
+        mc.tempangwt = mc.tempangreq
+        mc.tempdihwt = mc.tempdihreq
+        mc.tempang = mc.tempangwt
+        mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
+        b = self._sync_in()
+        self._check_cells()
+        # intramolecular energies from the reference's own host routine (molfit.py:1327)
+        en_mole_intra = self.mods["molfit"].en_mole_intra
+        sv = sa = sd = f32(0.0)
+        eintra = np.zeros(b.nmol, f32)
+        for im in range(1, b.nmol + 1):
+            e, sv, sa, sd = en_mole_intra(im, sv, sa, sd)
+            eintra[im - 1] = e
+        ft, fb = self.d.fmolec1(eintra, strict=True)
+        self._store_out(values_only=False)
+        self._mirror_ok = True
+        nmol = f32(b.nmol)
+        return 0, num_threads_input, f32(ft), f32(fb), f32(0.0) / nmol, f32(0.0) / nmol
+
+    def molfit(self, fadds, faddbs, nisum, intra, rotfreq, ireset):
+        """molfit.py:52-541 (whole-molecule branch on the device); returns (fadds, faddbs, nisum)."""
+        c = self.c
+        mc, cc = c.molecom, c.clustercom
+        nmol = int(cc.nmol)
+        internal = False
+        if float(mc.stepri) > 0.0:
+            ngrot = np.asarray(cc.ngrot[1:nmol + 1])
+            internal = bool(np.any(ngrot > 0)) and nisum == rotfreq * _idiv(nisum, rotfreq)
+        if nisum >= intra or internal or self._outside_path():
+            return self._host("molfit", fadds, faddbs, nisum, intra, rotfreq, ireset)
+        b = self._sync_in()
+        self._check_cells()
+        self._store_in()
+        # host-side prologue of molfit (:87-118)
+        mc.tol = f32(mc.tolout) / f32(cc.dmax)
+        nmt = int(cc.nmoltype)
+        for name in ("nmovei", "ninter", "nwhole", "nmovem"):
+            getattr(cc, name)[1:3, 1:nmt + 1] = 0
+        mc.tempang = mc.tempangwt
+        mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
+        tmax, tmin = trsteps(b.natomr)
+        d = self.d
+        d.mc_setup(rejrate=f32(c.epsr16.rejrate), stepr=f32(mc.stepr), stepm=f32(mc.stepm),
+                   wholerot=np.asarray(cc.wholerot[1:nmt + 1], f32), wholetrans=np.asarray(cc.wholetrans[1:nmt + 1], f32),
+                   internrot=np.asarray(cc.internrot[1:nmt + 1], f32),
+                   interntrans=np.asarray(cc.interntrans[1:nmt + 1], f32),
+                   nstepreject=np.asarray(cc.nstepreject[1:nmol + 1], np.int32), ran1=Ran1State(),
+                   trstepmax=tmax, trstepmin=tmin, ireset=int(ireset), fadds=f32(fadds))
+        d.m_ran1 = self._ran1_in()
+        d.cmc.ran1 = C.c_void_p(d.m_ran1.data_ptr())
+        cos = self.cos_override
+        self.cos_override = None
+        d.molfit(strict=self.strict or not self._mirror_ok, cos_override=cos)
+        d.check_status()
+        out = d.download_mc()
+        self._ran1_out(d.m_ran1)
+        cc.wholerot[1:nmt + 1], cc.wholetrans[1:nmt + 1] = out["wholerot"], out["wholetrans"]
+        cc.internrot[1:nmt + 1], cc.interntrans[1:nmt + 1] = out["internrot"], out["interntrans"]
+        cc.nwhole[1:3, 1:nmt + 1] = out["nwhole"]
+        cc.nmovem[1:3, 1:nmt + 1] = out["nmovem"]
+        cc.nstepreject[1:nmol + 1] = out["nstepreject"]
+        self._coords_out()
+        self._store_out(values_only=True)
+        faddbs = f32(faddbs) + f32(0.0) / f32(nmol)     # faddb stays 0 in the whole-molecule branch
+        return out["fadds"], faddbs, nisum + 1
+
+    def en_change(self, im):
+        """molfit.py:806-919 for molecule im (1-based) against its stored list; fills
+        ergpairreference.ergnew and returns the energy change."""
+        self._sync_in()
+        self._store_in()
+        d = self.d
+        M = d.nnbrefmax
+        erg = torch.zeros(max(M, 1), dtype=torch.float32, device=d.dev)
+        out = np.zeros(1, f32)
+        check(d.lib.epsr_en_change(C.byref(d.cbox), C.byref(d.store), int(im) - 1, C.c_void_p(erg.data_ptr()),
+                                   out.ctypes.data_as(C.c_void_p), None))
+        torch.cuda.synchronize()
+        erd = self.c.ergpairreference
+        n = int(erd.nergpairm[im])
+        if n > 1:
+            erd.ergnew[2:n + 1] = erg[1:n].cpu().numpy()
+        return f32(out[0])
+
+    def en_mole_pair(self, im, jm):
+        """molfit.py:1528-1578: energy of molecules im and jm (1-based)."""
+        self._sync_in()
+        d = self.d
+        ij = torch.tensor([int(im) - 1, int(jm) - 1], dtype=torch.int32, device=d.dev)
+        res = torch.zeros(1, dtype=torch.float32, device=d.dev)
+        check(d.lib.epsr_en_mole_pair(C.byref(d.cbox), C.c_void_p(ij.data_ptr()), C.c_void_p(ij.data_ptr() + 4), 1,
+                                      C.c_void_p(res.data_ptr()), None))
+        return f32(res.cpu().numpy()[0])
+
+    def atogen(self, wav, ngrsamples):
+        """ato_manipulation_rev4.py:3640-3899: fills wav(2,npt1,npairs) and potex in place;
+        returns ngrsamples."""
+        if self._outside_path():
+            return self._host("atogen", wav, ngrsamples)
+        c = self.c
+        b = self._sync_in()
+        pp = c.potential_par
+        rminex = np.array([pp.rminex[int(pp.irefpcof[p + 1])] for p in range(b.npairs)], f32)
+        t = self._ran1_in()
+        n = self.d.atogen(int(ngrsamples), t, rminex, ycoh=np.asarray(c.epsr16.ycoh, f32),
+                          sizefactor=f32(c.molecom.sizefactor))
+        w, potex = self.d.download_wav()
+        self._ran1_out(t)
+        wav[1:3, 1:b.npt1 + 1, 1:b.npairs + 1] = w[:, :, 1:b.npt1 + 1].transpose(0, 2, 1)
+        pp.potex[1:b.npairs + 1] = potex
+        pp.potexmax[1:b.npairs + 1] = 0.0
+        return n
+
+    def gensq(self, nq, q, sofq, wav):
+        """epsr_standalone_rev3.py:4731-4802: fills sofq(2,nq,npairs) in place."""
+        c = self.c
+        if getattr(c.molecom_mod, "coarsegraining", False):
+            return self._host("gensq", nq, q, sofq, wav)
+        e16, mc = c.epsr16, c.molecom
+        npairs, npt1, ntype = int(mc.npairs), int(e16.npt1), int(mc.ntype)
+        ld = npt1 + 1
+        w = np.ascontiguousarray(np.asarray(wav)[1:3, :ld, 1:npairs + 1].transpose(0, 2, 1), f32)
+        fq = np.ascontiguousarray(np.asarray(e16.foqols)[:ld, :nq + 1], f32)
+        out = transforms.gensq(int(nq), npt1, torch.from_numpy(w.reshape(-1)).cuda(), ld, fq, nq + 1, 1,
+                               np.asarray(e16.ycoh[:ld], f32), np.asarray(mc.n2extr[1:npairs + 1], np.int32) - 1,
+                               np.asarray(c.molecom_mod.natomsphere[1:ntype + 1], f32), npairs)
+        o = out.cpu().numpy().reshape(2, npairs, nq + 1)
+        sofq[1:3, 1:nq + 1, 1:npairs + 1] = o[:, :, 1:].transpose(0, 2, 1)
+        return None
+
+    def stog(self, rho, q, sofq, r, gofr, nqmin, nqmax, nr, npairs, nqdim, nrdim, npdim, xwt):
+        """ato_manipulation_rev4.py:4067-4110: fills gofr(nr, npairs) in place."""
+        ldq = int(nqdim) + 1
+        qs = np.asarray(q[:ldq], f32)
+        sp = np.ascontiguousarray(np.asarray(sofq)[:ldq, 1:npairs + 1].T, f32)
+        g = transforms.stog(f32(rho), qs, torch.from_numpy(sp).cuda(), np.asarray(r[:nr + 1], f32),
+                            np.asarray(nqmin[1:npairs + 1], np.int32), np.asarray(nqmax[1:npairs + 1], np.int32),
+                            np.asarray(xwt[1:npairs + 1], f32))
+        gofr[1:nr + 1, 1:npairs + 1] = g.cpu().numpy()[:, 1:nr + 1].T
+        return None
+
+    def fit_expansion(self, yin, expr, yout, wt, wtold, stepr, acceptr, rejrat, chisqnew, nmin, npt, ncfirst,
+                      nterms, nits, nfreq):
+        """epsr_standalone_rev3.py:4806-4921: fills wt, wtold, yout in place; returns
+        (stepr, acceptr, rejrat, chisqnew)."""
+        from .device import DeviceBox  # noqa: F401  (loads the library with a device check)
+        _lib.load(require_device=True)
+        r = self.c.ran1com
+        st = Ran1State(idum=int(r.idum), iy=int(r.iy), mcall=int(np.int64(r.mcall) & 0xFFFFFFFF),
+                       iv=np.asarray(r.iv[1:33], np.int32).copy())
+        self._mcall0 = int(r.mcall)
+        t = torch.from_numpy(st.as_array()).cuda()
+        res = transforms.fit_expansion(np.asarray(yin[:npt + 1], f32), np.asarray(expr[:npt * nterms + 1], f32),
+                                       np.asarray(wtold[:nterms + 1], f32), f32(stepr), int(nmin), int(npt),
+                                       int(ncfirst), int(nterms), int(nits), int(nfreq), t, acceptr=f32(acceptr),
+                                       rejrat=f32(rejrat), chisqnew=f32(chisqnew), strict=self.strict)
+        self._ran1_out(t)
+        wt[1:nterms + 1] = res["wt"].cpu().numpy()[1:nterms + 1]
+        wtold[1:nterms + 1] = res["wtold"].cpu().numpy()[1:nterms + 1]
+        yout[1:npt + 1] = res["yout"].cpu().numpy()[1:npt + 1]
+        return res["stepr"], res["acceptr"], res["rejrat"], res["chisq"]
+
+
+def install_reference(program, strict=False, routines=DEFAULT_ROUTINES):
+    """Install the GPU path into a running reference process.
+
+    ``program``: the loaded epsr program module (``epsr26.programs.load("epsr")``).  The
+    library modules and the COMMON package are imported by name from ``epsr26``."""
+    import importlib
+    common = importlib.import_module("epsr26.common")
+    mods = {"cellneighbourlist": importlib.import_module("epsr26.library.cellneighbourlist"),
+            "ato_manipulation_rev4": importlib.import_module("epsr26.library.ato_manipulation_rev4"),
+            "molfit": importlib.import_module("epsr26.library.molfit"), "program": program}
+    for name in ("molecom", "clustercom", "epsr16", "potential_par", "lattice", "ran1com", "cellneighbourlist",
+                 "ergpairreference", "molecom_mod", "threebody_mod", "coordconstraints_mod", "containerforces_mod"):
+        importlib.import_module("epsr26.common." + name)
+    return PairPath(common, mods, strict=strict).install(routines)
