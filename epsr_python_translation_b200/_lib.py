@@ -76,6 +76,9 @@ _SIGS = {
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),
     "epsr_stog_scratch_bytes": (I64, [I32, I32]),
     "epsr_fit_expansion": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, I32, P, P]),
+    "epsr_fit_expansion_batch": (C.c_int, [I32, P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, I32, P,
+                                           P]),
+    "epsr_fit_expansion_batch_scratch_bytes": (I64, [I32, I32, I32]),
     "epsr_fit_expansion_scratch_bytes": (I64, [I32, I32]),
 }
 

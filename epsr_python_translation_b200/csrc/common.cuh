@@ -155,6 +155,44 @@ __device__ __forceinline__ void ran1_store(const Ran1 &s, int32_t *g) {
 }
 
 // ----------------------------------------------------------------- ran1 (device, one warp)
+// a*b mod (2^31 - 1) for a, b < 2^31 - 1: the product is below 2^62 and 2^31 = 1 modulo the
+// Mersenne prime, so the high and low 31-bit halves are added and at most two moduli
+// subtracted -- the exact residue, as Schrage's method computes it.
+__device__ __forceinline__ uint32_t r1_mulmod(uint32_t a, uint32_t b) {
+    const uint64_t x = (uint64_t)a * (uint64_t)b;
+    uint32_t r = (uint32_t)(x & 0x7fffffffull) + (uint32_t)(x >> 31);
+    r = r >= 2147483647u ? r - 2147483647u : r;
+    r = r >= 2147483647u ? r - 2147483647u : r;
+    return r;
+}
+
+// 32 steps of the shuffle when no value of the batch can be zero: idl is this lane's Park-
+// Miller value of the batch (step lane+1), iv this lane's table entry, iy warp-uniform.  The
+// chain only needs the slot index of the next step (the top 5 bits of the value read), so
+// each lane also keeps its entry's top bits and one shuffle per step carries the chain; the
+// value itself is fetched beside it.  Returns the value of step `lane`; updates iv and iy.
+__device__ __forceinline__ int32_t ran1_chain32(int32_t idl, int32_t &iv, int32_t &iy) {
+    const int lane = threadIdx.x & 31;
+    int t5 = iv >> 26;
+    const int c5 = idl >> 26;
+    int j = iy >> 26;
+    int32_t y = iy, mine = 0;
+#pragma unroll
+    for (int s = 0; s < 32; ++s) {
+        const int jn = __shfl_sync(0xffffffffu, t5, j);
+        const int32_t out = __shfl_sync(0xffffffffu, iv, j);
+        const int32_t id = __shfl_sync(0xffffffffu, idl, s);
+        const int c = __shfl_sync(0xffffffffu, c5, s);
+        iv = (lane == j) ? id : iv;
+        t5 = (lane == j) ? c : t5;
+        mine = (lane == s) ? out : mine;
+        y = out;
+        j = jn;
+    }
+    iy = y;
+    return mine;
+}
+
 // Warp-cooperative batch of the ran1 stream: lane l holds table entry iv[l]; idum/iy are
 // warp-uniform.  The Park-Miller values of the batch are jumped ahead (lane l: IA^(l+1) *
 // idum mod IM, the value Schrage's method computes) and the Bays-Durham shuffle is walked
@@ -163,10 +201,6 @@ __device__ __forceinline__ void ran1_store(const Ran1 &s, int32_t *g) {
 // the batch stops after a step that leaves idum or iy at zero, where the reference
 // re-initialises (auxiliary_routines.py:346).  Returns the number of values produced; lane
 // t < count receives its value in *mine.
-__device__ __forceinline__ uint32_t r1_mulmod(uint32_t a, uint32_t b) {
-    return (uint32_t)(((uint64_t)a * (uint64_t)b) % 2147483647ull);
-}
-
 __device__ __forceinline__ int ran1_warp_batch(int32_t &idum, int32_t &iy, int32_t &iv, uint32_t lane_mul, int want,
                                                int32_t &mine, int32_t *tab_tmp /* smem [34] */) {
     const int lane = threadIdx.x & 31;
@@ -192,17 +226,7 @@ __device__ __forceinline__ int ran1_warp_batch(int32_t &idum, int32_t &iy, int32
     const unsigned zero = __ballot_sync(0xffffffffu, idl == 0) | __ballot_sync(0xffffffffu, iv == 0);
     mine = 0;
     if (cnt == 32 && zero == 0u && iy != 0) {
-        int32_t y = iy;
-#pragma unroll
-        for (int s = 0; s < 32; ++s) {
-            const int32_t id = __shfl_sync(0xffffffffu, idl, s);
-            const int j = y >> 26;
-            const int32_t nxt = __shfl_sync(0xffffffffu, iv, j);
-            iv = (lane == j) ? id : iv;
-            y = nxt;
-            mine = (lane == s) ? y : mine;
-        }
-        iy = y;
+        mine = ran1_chain32(idl, iv, iy);
         idum = __shfl_sync(0xffffffffu, idl, 31);
         return 32;
     }
@@ -222,6 +246,45 @@ __device__ __forceinline__ int ran1_warp_batch(int32_t &idum, int32_t &iy, int32
     idum = __shfl_sync(0xffffffffu, idl, s - 1);
     return s;
 }
+
+// A warp's ran1 stream in batches of 32, the Park-Miller values of the next batch computed
+// while the current batch's shuffle chain runs (they depend only on the batch's last value).
+// Bit-identical to ran1_warp_batch, which it falls back to for batches that can meet a zero
+// or a re-initialisation.
+struct Ran1Warp {
+    int32_t idum, iy, iv;   // idum, iy warp-uniform; iv this lane's table entry
+    uint32_t mul;           // IA^(lane+1) mod IM
+    int32_t idl;            // this lane's Park-Miller value of the next batch, when idl_ok
+    bool idl_ok;
+
+    __device__ __forceinline__ void load(const int32_t *state) {
+        const int lane = threadIdx.x & 31;
+        idum = state[0];
+        iy = state[1];
+        iv = state[3 + lane];
+        mul = 16807u;
+        for (int k = 0; k < lane; ++k) mul = r1_mulmod(mul, 16807u);
+        idl_ok = false;
+    }
+    // Up to `want` (<= 32) values; lane t < return value receives value t in `mine`.
+    __device__ __forceinline__ int next(int want, int32_t &mine, int32_t *tab_tmp) {
+        if (want == 32 && idum > 0 && iy != 0) {
+            if (!idl_ok) idl = (int32_t)r1_mulmod(mul, (uint32_t)idum);
+            const unsigned zero = __ballot_sync(0xffffffffu, idl == 0) | __ballot_sync(0xffffffffu, iv == 0);
+            if (zero == 0u) {
+                const int32_t last = __shfl_sync(0xffffffffu, idl, 31);
+                const int32_t nidl = (int32_t)r1_mulmod(mul, (uint32_t)last);
+                mine = ran1_chain32(idl, iv, iy);
+                idum = last;
+                idl = nidl;
+                idl_ok = true;
+                return 32;
+            }
+        }
+        idl_ok = false;
+        return ran1_warp_batch(idum, iy, iv, mul, want, mine, tab_tmp);
+    }
+};
 
 // ----------------------------------------------------------------- reductions
 __device__ __forceinline__ double warp_sum_d(double v) {

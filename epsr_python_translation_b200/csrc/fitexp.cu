@@ -2,20 +2,34 @@
 //
 // The Monte Carlo fit is a chain of trials: perturb every coefficient (one ran1 draw each),
 // evaluate chi^2 over all Q rows, Metropolis-accept (one more draw when 0 < exponent <= 20),
-// smooth the coefficients every nfreq acceptances (smoop auxiliary_routines.py:744).
+// smooth the coefficients every nfreq acceptances (smoop auxiliary_routines.py:744).  One
+// launch fits any number of data sets in turn on the same basis, continuing one ran1
+// stream, as the reference's successive calls do.
 //
-// The basis rows are split over the CTAs of a cluster so that each CTA keeps its rows in
-// shared memory for the whole fit.  Per trial a CTA evaluates its rows (expand :4924, the
-// sequential clamped sum of a row) and every CTA then forms the same chi^2 -- in the
-// reference's row order through distributed shared memory (strict), or as a double sum
-// (fast) -- so all CTAs take the same decisions without a second exchange.  A row is first
-// summed without the clamp while tracking the largest partial sum; only a row whose partial
-// sums could reach the clamp (|sum| > e^25) is summed again with it, so the result is the
-// reference's either way.
+// Layout.  The basis rows are split over the CTAs of a cluster; each keeps its rows in
+// shared memory for the whole launch, four terms to a 16-byte word, and evaluates one row
+// per thread per trial (expand :4924, the sequential clamped sum of a row).  Every partial
+// sum of a row is bounded by the row's L1 norm times the largest |coefficient|; when that
+// bound stays below the clamp level (e^25) the clamp cannot act and the plain sequential
+// sum is the reference's value, otherwise the row is summed with the clamp.  The CTAs
+// exchange their chi^2 contributions through distributed shared memory: each pushes its
+// part (a double partial, or every residual for the reference's sequential float sum) into
+// every CTA and arrives on that CTA's mbarrier; each then forms the same chi^2, so all take
+// the same decisions without a second exchange.  Thread 0 of each CTA takes every decision
+// (Metropolis test, smoothing, stopping) and broadcasts it through shared memory, so all
+// threads pass the same barriers.
 //
-// ran1: every CTA runs the same stream.  One warp generates the values of the next trial
-// while thread 0 forms chi^2, keeping generation off the critical path; the state the
-// reference leaves after the fit is rebuilt from the generator's batch checkpoints.
+// ran1.  The chain is sequential; warp 15 of every CTA generates the same stream into a
+// ring in its CTA's shared memory, running ahead of the trials (bounded by the ring) and
+// publishing how many values exist.  Rows and coefficients are handled by the warps of the
+// other three schedulers of the SM (warps 0-2, 4-6, 8-10, 12-14), so the generator's
+// scheduler is left to it; warps 3, 7 and 11 only take part in the barriers.  The workers
+// synchronise among themselves with a named barrier that the generator warp is not part of.
+// At the end the state the reference leaves after exactly the values the fit consumed is
+// rebuilt from the generator's per-batch checkpoints.
+//
+// Every wait (ring, exchange, ring space) is bounded in time: on timeout the kernel records
+// status 1, stops the fit and returns.
 #include <cooperative_groups.h>
 
 #include "common.cuh"
@@ -25,235 +39,461 @@ namespace cg = cooperative_groups;
 namespace epsr {
 
 constexpr int FX_THREADS = 512;
-constexpr int FX_GEN_WARP = 1;    // the warp that generates ran1 values
-constexpr int FX_RING = 1024;     // ran1 values held (power of two)
-constexpr int FX_CK = 64;         // batch checkpoints (power of two)
-constexpr int FX_CKW = 36;        // ints per checkpoint: idum, iy, iv[32], pad[2]
+constexpr int FX_WARPS = FX_THREADS / 32;
+constexpr int FX_GEN_WARP = 15;                 // the stream warp
+constexpr int FX_NBAR = 480;                    // threads of the worker barrier (warps 0-14)
+constexpr int FX_SLOTS = 384;                   // row / coefficient slots (12 warps, schedulers 0-2)
+constexpr int FX_RING = 2048;                   // ran1 values held per worker CTA (power of two)
+constexpr int FX_CK = 128;                      // batch checkpoints (power of two)
+constexpr int FX_CKW = 36;                      // ints per checkpoint: idum, iy, iv[32], pad[2]
+constexpr unsigned long long FX_WAIT_NS = 2000000000ull;  // a wait gives up after 2 s
 
 struct FxDev {
-    const float *yin, *expr;  // expr[(i-1)*nterms + m] (1-based flat, row-major by Q)
-    float *yout, *wt_g, *wtold_g;
-    int nmin, npt, ncfirst, nterms, nits, nfreq, strict, rpc;  // rpc: rows per CTA
+    const float *expr;        // expr[(i-1)*nterms + m] (1-based flat, row-major by Q)
+    const float *yin;         // [nprob][npt+1]
+    float *yout;              // [nprob][npt+1]
+    float *wt_g, *wtold_g;    // [nprob][nterms+1]
+    float *scal;              // [nprob][4] {stepr, acceptr, rejrat, chisq}
+    long long *trials;        // [nprob]
+    int *status;              // [1]: 0 ok, 1 a bounded wait gave up
+    int nprob, nmin, npt, ncfirst, nterms, nits, nfreq, strict, rpc;
     int32_t *ran1;
-    float *scal;              // {stepr, acceptr, rejrat, chisq}
-    long long *trials;
 };
 
-size_t fx_smem_bytes(int nt, int rpc, int ncta) {
-    size_t f = (size_t)nt * rpc + 3 * (size_t)rpc + 2 * (size_t)(nt + 1) + FX_RING;
-    size_t b = f * 4;
+// ------------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t map_rank(uint32_t a, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_cl_f32(uint32_t a, float v) {
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_cl_f64(uint32_t a, double v) {
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_cl_s64(uint32_t a, long long v) {
+    asm volatile("st.shared::cluster.b64 [%0], %1;" ::"r"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_release_cl_s64(uint32_t a, long long v) {
+    asm volatile("st.release.cluster.shared::cluster.b64 [%0], %1;" ::"r"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_release_cl_s32(uint32_t a, int v) {
+    asm volatile("st.release.cluster.shared::cluster.b32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ long long ld_relaxed_cl_s64(uint32_t a) {
+    long long v;
+    asm volatile("ld.relaxed.cluster.shared::cluster.b64 %0, [%1];" : "=l"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ long long ld_acquire_s64(const long long *p) {
+    long long v;
+    asm volatile("ld.acquire.cluster.shared::cta.b64 %0, [%1];" : "=l"(v) : "r"(smem_addr(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_acquire_s32(const int *p) {
+    int v;
+    asm volatile("ld.acquire.cluster.shared::cta.b32 %0, [%1];" : "=r"(v) : "r"(smem_addr(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t a) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void fence_cluster() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+// Barrier of the worker warps (0-14) after code in which a warp may have diverged (a
+// bounded spin, a branch on the thread index): the warp is reconverged first, because the
+// barrier requires every thread of a warp to arrive together.
+__device__ __forceinline__ void block_sync() {
+    __syncwarp();
+    asm volatile("bar.sync 1, %0;" ::"n"(FX_NBAR) : "memory");
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct FxShared {                 // statically sized control block (one per CTA)
+    long long prod;               // ring values present (written by the generator warp)
+    long long cons;               // lowest stream index the workers may still read
+    int done;                     // set by the workers when the fit is over
+    int abort, stop;
+    int accept, smooth, draw;     // thread 0's decision of the current trial
+    float val;                    // chi^2 broadcast
+    float wfix;                   // largest |wt| of the unperturbed terms 1..ncfirst-1
+    float wmx[FX_WARPS];          // largest |wt| of the terms each warp perturbed
+    double red[FX_WARPS];
+};
+
+__host__ __device__ inline int fx_ntq(int nt) { return (nt + 3) / 4; }
+
+size_t fx_smem_bytes(int nt, int rpc, int nw) {
+    const int ntq = fx_ntq(nt);
+    size_t b = 0;
+    b += 16 * (size_t)ntq * rpc;                        // ex4
+    b += sizeof(float) * (size_t)rpc;                   // yr
+    b += sizeof(float) * (size_t)rpc;                   // e1 (row L1 norms)
     b = (b + 15) & ~(size_t)15;
-    b += 2 * sizeof(double);
-    b += (size_t)FX_CK * FX_CKW * sizeof(int32_t);
-    b += (size_t)FX_CK * sizeof(long long);
-    b += sizeof(float) * ((size_t)ncta * rpc + 4);
+    b += sizeof(float) * (4 + 4 * (size_t)ntq);         // wt (wt + 1 16-byte aligned)
+    b += sizeof(float) * (size_t)(nt + 1);              // wtold
+    b += sizeof(float) * FX_RING;                       // ring
+    b = (b + 15) & ~(size_t)15;
+    b += sizeof(float) * 2 * (size_t)nw * rpc;          // gat[2][nw*rpc]
+    b = (b + 15) & ~(size_t)15;
+    b += sizeof(double) * 2 * (size_t)nw;               // parts[2][nw]
+    b += sizeof(uint64_t) * 2;                          // exchange mbarriers
+    b += sizeof(long long) * FX_CK;                     // ckpos
+    b += sizeof(int32_t) * FX_CK * FX_CKW;              // checkpoints
     return b;
 }
 
-__global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
+__global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
-    const int ncta = (int)cl.num_blocks();
+    const int nw = (int)cl.num_blocks();
     extern __shared__ __align__(16) unsigned char fx_raw[];
-    const int nt = F.nterms, rpc = F.rpc;
-    float *ex = (float *)fx_raw;                    // [nt*rpc] term-major: ex[(m-1)*rpc + r]
-    float *sq = ex + (size_t)nt * rpc;              // [2*rpc] double-buffered squared residuals
-    float *yr = sq + 2 * rpc;                       // [rpc]
-    float *wt = yr + rpc;                           // [nt+1]
-    float *wtold = wt + (nt + 1);                   // [nt+1]
-    float *ring = wtold + (nt + 1);                 // [FX_RING]
-    size_t off = ((size_t)((unsigned char *)(ring + FX_RING) - fx_raw) + 15) & ~(size_t)15;
-    double *part = (double *)(fx_raw + off);        // [2] fast-mode partial sums
-    int32_t *ck = (int32_t *)(part + 2);            // [FX_CK][FX_CKW]
-    long long *ckpos = (long long *)(ck + FX_CK * FX_CKW);  // [FX_CK]
-    float *gat = (float *)(ckpos + FX_CK);          // [ncta*rpc] gathered residuals (16-byte aligned)
-    __shared__ float s_val;
-    __shared__ double s_red[FX_THREADS / 32];
+    __shared__ FxShared S;
     __shared__ int32_t g_tab[34];
+    const int nt = F.nterms, rpc = F.rpc, ntq = fx_ntq(nt);
+    float4 *ex4 = (float4 *)fx_raw;                     // [ntq*rpc]: ex4[q*rpc + r] = terms 4q..4q+3 of row r
+    float *yr = (float *)(ex4 + (size_t)ntq * rpc);     // [rpc]
+    float *e1 = yr + rpc;                               // [rpc] sum over terms of |basis value|
+    size_t off = ((size_t)((unsigned char *)(e1 + rpc) - fx_raw) + 15) & ~(size_t)15;
+    float *wt = (float *)(fx_raw + off) + 3;            // wt[0..4*ntq]; wt + 1 is 16-byte aligned
+    float *wtold = wt + 1 + 4 * ntq;                    // [nt+1]
+    float *ring = wtold + (nt + 1);                     // [FX_RING]
+    off = ((size_t)((unsigned char *)(ring + FX_RING) - fx_raw) + 15) & ~(size_t)15;
+    float *gat = (float *)(fx_raw + off);               // [2][nw*rpc] residuals by global row
+    off = ((off + sizeof(float) * 2 * (size_t)nw * rpc) + 15) & ~(size_t)15;
+    double *parts = (double *)(fx_raw + off);           // [2][nw]
+    uint64_t *xbar = (uint64_t *)(parts + 2 * nw);      // [2]
+    long long *ckpos = (long long *)(xbar + 2);         // [FX_CK]
+    int32_t *ck = (int32_t *)(ckpos + FX_CK);           // [FX_CK][FX_CKW]
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int row0 = 1 + rank * rpc;  // first (1-based) row of this CTA
+    volatile FxShared *vs = &S;
+    const int row0 = 1 + rank * rpc;                    // first (1-based) row of this CTA
     const int nrow = max(0, min(rpc, F.npt - row0 + 1));
-    const float summax = exp_r(25.0f);
-    const int K = nt - F.ncfirst + 1;  // draws per trial
-
-    for (int idx = tid; idx < nt * rpc; idx += blockDim.x) {
-        const int m = idx / rpc, r = idx - m * rpc;
-        ex[idx] = r < nrow ? F.expr[1 + (size_t)(row0 - 1 + r) * nt + m] : 0.0f;
+    for (int idx = tid; idx < ntq * rpc; idx += blockDim.x) {
+        const int q = idx / rpc, r = idx - q * rpc;
+        float e[4];
+        for (int j = 0; j < 4; ++j) {
+            const int m = 4 * q + j;                    // 0-based term
+            e[j] = (r < nrow && m < nt) ? F.expr[1 + (size_t)(row0 - 1 + r) * nt + m] : 0.0f;
+        }
+        ex4[idx] = make_float4(e[0], e[1], e[2], e[3]);
     }
-    for (int r = tid; r < rpc; r += blockDim.x) yr[r] = r < nrow ? F.yin[row0 + r] : 0.0f;
-    for (int i = tid; i <= nt; i += blockDim.x) {
-        wtold[i] = F.wtold_g[i];
-        wt[i] = wtold[i];
+    for (int i = tid; i <= 4 * ntq; i += blockDim.x) wt[i] = 0.0f;   // terms past nterms stay zero
+    for (int r = tid; r < rpc; r += blockDim.x) {
+        float a = 0.0f;
+        for (int m = 0; m < nt && r < nrow; ++m) a = __fadd_ru(a, fabsf(F.expr[1 + (size_t)(row0 - 1 + r) * nt + m]));
+        e1[r] = a;
     }
     for (int i = tid; i < FX_CK; i += blockDim.x) ckpos[i] = -1;
-    // generator warp state (the shuffle table lives one entry per lane)
-    int32_t g_iv = 0, g_idum = 0, g_iy = 0;
-    long long g_pos = 0, g_nb = 0;
-    uint32_t g_mul = 16807u;
-    if (wid == FX_GEN_WARP) {
-        g_idum = F.ran1[0];
-        g_iy = F.ran1[1];
-        g_iv = F.ran1[3 + lane];
-        for (int k = 0; k < lane; ++k) g_mul = r1_mulmod(g_mul, 16807u);
+    if (tid < FX_WARPS) S.wmx[tid] = 0.0f;
+    if (tid == 0) {
+        S.prod = 0;
+        S.cons = 0;
+        S.done = 0;
+        S.abort = 0;
+        S.stop = 0;
+        mbar_init(&xbar[0], (uint32_t)nw);
+        mbar_init(&xbar[1], (uint32_t)nw);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     const int32_t mcall0 = F.ran1[2];
     cl.sync();
 
-    // generate values up to stream index `until` (exclusive); warp FX_GEN_WARP only
-    auto generate = [&](long long until) {
-        if (wid != FX_GEN_WARP) return;
-        while (g_pos < until) {
-            const int slot = (int)(g_nb & (FX_CK - 1));
-            ck[slot * FX_CKW + 2 + lane] = g_iv;
+    // ================================================================ stream warp
+    if (wid == FX_GEN_WARP) {
+        Ran1Warp g;
+        g.load(F.ran1);
+        long long pos = 0, nb = 0;
+        unsigned long long t0 = 0;
+        // every control decision of the loop is lane 0's, broadcast to the warp, so the warp
+        // stays converged for the shuffles of the batch
+        while (true) {
+            int stopnow = 0, full = 0;
             if (lane == 0) {
-                ck[slot * FX_CKW + 0] = g_idum;
-                ck[slot * FX_CKW + 1] = g_iy;
-                ckpos[slot] = g_pos;
-            }
-            ++g_nb;
-            int32_t mine;
-            const int cnt = ran1_warp_batch(g_idum, g_iy, g_iv, g_mul, 32, mine, g_tab);
-            if (lane < cnt) ring[(g_pos + lane) & (FX_RING - 1)] = ran1_out(mine);
-            g_pos += cnt;
-        }
-    };
-
-    // chi^2 of the current wt over rows nmin..npt (all CTAs); while thread 0 sums, the
-    // generator warp produces values up to `gen_until`.  Optionally writes yout (all rows).
-    int buf = 0;
-    auto chisq = [&](long long gen_until, bool write_yout, bool strict_sum) -> float {
-        float *sqb = sq + buf * rpc;
-        double mypart = 0.0;
-        // the generator warp works while the others evaluate rows (two batches) and while
-        // thread 0 forms chi^2 (the rest)
-        generate(gen_until < g_pos + 64 ? gen_until : g_pos + 64);
-        if (wid != FX_GEN_WARP) {
-            const int w = wid > FX_GEN_WARP ? tid - 32 : tid;  // worker index
-            const int nw = blockDim.x - 32;
-            for (int r = w; r < nrow; r += nw) {
-                const int i = row0 + r;
-                float sum = 0.0f, mx = 0.0f;
-                for (int m = 1; m <= nt; ++m) {
-                    sum = __fadd_rn(sum, __fmul_rn(ex[(m - 1) * rpc + r], wt[m]));
-                    mx = fmaxf(mx, fabsf(sum));
+                stopnow = vs->done;
+                if (!stopnow && pos + 32 > vs->cons + FX_RING) {   // ring full
+                    full = 1;
+                    const unsigned long long t = now_ns();
+                    if (t0 == 0) t0 = t;
+                    else if (t - t0 > FX_WAIT_NS) {
+                        atomicExch(F.status, 1);
+                        vs->abort = 1;
+                        stopnow = 1;
+                    }
                 }
-                if (mx > summax) {  // the clamp may act: the reference's clamped sum
-                    sum = 0.0f;
-                    for (int m = 1; m <= nt; ++m) {
-                        sum = __fadd_rn(sum, __fmul_rn(ex[(m - 1) * rpc + r], wt[m]));
+            }
+            stopnow = __shfl_sync(0xffffffffu, stopnow, 0);
+            full = __shfl_sync(0xffffffffu, full, 0);
+            if (stopnow) break;
+            if (full) {
+                __nanosleep(64);
+                continue;
+            }
+            t0 = 0;
+            const int slot = (int)(nb & (FX_CK - 1));
+            ck[slot * FX_CKW + 2 + lane] = g.iv;
+            if (lane == 0) {
+                ck[slot * FX_CKW + 0] = g.idum;
+                ck[slot * FX_CKW + 1] = g.iy;
+                ckpos[slot] = pos;
+            }
+            ++nb;
+            int32_t mine;
+            const int cnt = g.next(32, mine, g_tab);
+            if (lane < cnt) ring[(pos + lane) & (FX_RING - 1)] = ran1_out(mine);
+            pos += cnt;
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                vs->prod = pos;
+            }
+        }
+        __syncwarp();
+        __syncthreads();   // meets the workers after they set done (barrier 0, all 512 threads)
+        cl.sync();
+        return;
+    }
+
+    // ================================================================ workers (warps 0-14)
+    const float summax = exp_r(25.0f);
+    const int K = nt - F.ncfirst + 1;                   // draws per trial
+    // row / coefficient slot of this thread: the warps of schedulers 0-2, -1 otherwise
+    const int slot = (wid & 3) != 3 ? (wid - (wid >> 2)) * 32 + lane : -1;
+    const int swarp = (wid & 3) != 3 ? wid - (wid >> 2) : -1;   // slot warp 0..11
+
+    // wait until stream value `idx` is in the ring (bounded; gives up at once after an abort)
+    auto need = [&](long long idx) {
+        if (vs->prod > idx) {
+            __threadfence_block();
+            return;
+        }
+        const unsigned long long t0 = now_ns();
+        while (vs->prod <= idx) {
+            if (vs->abort) return;
+            if (now_ns() - t0 > FX_WAIT_NS) {
+                atomicExch(F.status, 1);
+                vs->abort = 1;
+                return;
+            }
+            __nanosleep(32);
+        }
+        __threadfence_block();
+    };
+    auto val = [&](long long idx) { return ring[idx & (FX_RING - 1)]; };
+
+    int xb = 0;                                         // exchange buffer
+    uint32_t xph = 0u;                                  // mbarrier phase parity, bit b for buffer b
+    // chi^2 of the current wt over rows nmin..npt, the same value in every CTA.  strict_sum:
+    // the reference's sequential float sum over rows; else a double sum.  yout, if given,
+    // receives this CTA's row sums.  Two worker barriers; the result is returned to all.
+    auto chisq = [&](bool strict_sum, float *yout) -> float {
+        float *gb = gat + (size_t)xb * nw * rpc;
+        double mypart = 0.0;
+        if (slot >= 0) {
+            float wmax = vs->wfix;
+            for (int k = 0; k < FX_WARPS; ++k) wmax = fmaxf(wmax, vs->wmx[k]);
+            for (int r = slot; r < nrow; r += FX_SLOTS) {
+                const int i = row0 + r;
+                const float4 *e4 = ex4 + r;
+                float sum = 0.0f;
+                // every partial sum is at most e1[r] * max|wt| (times 1 + 2^-20 for rounding)
+                if (__fmul_ru(__fmul_ru(e1[r], wmax), 1.001f) < summax) {
+                    const float4 *w4 = (const float4 *)(wt + 1);
+#pragma unroll 2
+                    for (int q = 0; q < ntq; ++q) {
+                        const float4 e = e4[(size_t)q * rpc];
+                        const float4 c = w4[q];
+                        sum = __fadd_rn(sum, __fmul_rn(e.x, c.x));
+                        sum = __fadd_rn(sum, __fmul_rn(e.y, c.y));
+                        sum = __fadd_rn(sum, __fmul_rn(e.z, c.z));
+                        sum = __fadd_rn(sum, __fmul_rn(e.w, c.w));
+                    }
+                } else {  // the reference's clamped sum (expand :4924)
+                    for (int m = 0; m < nt; ++m) {
+                        const float *ee = (const float *)(e4 + (size_t)(m >> 2) * rpc);
+                        sum = __fadd_rn(sum, __fmul_rn(ee[m & 3], wt[1 + m]));
                         if (fabsf(sum) > summax) sum = fsign(summax, sum);
                     }
                 }
                 const float term = __fsub_rn(yr[r], sum);
-                const float q = __fmul_rn(term, term);
-                sqb[r] = q;
-                if (i >= F.nmin) mypart += (double)q;
-                if (write_yout) F.yout[i] = sum;
+                const float q2 = __fmul_rn(term, term);
+                if (yout) yout[i] = sum;
+                if (strict_sum) {
+                    const uint32_t la = smem_addr(gb + (rank * rpc + r));
+                    for (int d = 0; d < nw; ++d) st_cl_f32(map_rank(la, (uint32_t)d), q2);
+                } else if (i >= F.nmin) {
+                    mypart += (double)q2;
+                }
             }
         }
-        if (!strict_sum) {
-            mypart = warp_sum_d(mypart);
-            if (lane == 0) s_red[wid] = mypart;
-        }
-        __syncthreads();
-        if (!strict_sum && tid == 0) {
-            double t = 0.0;
-            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += s_red[k];
-            part[buf] = t;
-        }
-        cl.sync();  // every CTA's rows of this buffer are complete
+        __syncwarp();
         if (strict_sum) {
-            // gather all rows' residuals into this CTA's gather buffer (remote rows through
-            // distributed shared memory, in parallel), then sum them in the reference's order
-            for (int q = 0; q < ncta; ++q) {
-                const float *rs = q == rank ? sqb : cl.map_shared_rank(sq + buf * rpc, q);
-                for (int r = tid; r < rpc; r += blockDim.x) gat[q * rpc + r] = rs[r];
+            fence_cluster();
+        } else {
+            mypart = warp_sum_d(mypart);
+            if (lane == 0) vs->red[wid] = mypart;
+        }
+        block_sync();
+        if (tid == 0) {
+            const uint32_t pa = smem_addr(parts + xb * nw + rank);
+            const uint32_t ba = smem_addr(&xbar[xb]);
+            if (!strict_sum) {
+                double t = 0.0;
+                for (int k = 0; k < FX_GEN_WARP; ++k) t += vs->red[k];
+                for (int d = 0; d < nw; ++d) st_cl_f64(map_rank(pa, (uint32_t)d), t);
             }
-            __syncthreads();
-            if (tid == 0) {
-                const int a = F.nmin - 1, b = F.npt;  // 0-based rows a..b-1
+            for (int d = 0; d < nw; ++d) mbar_arrive_cluster(map_rank(ba, (uint32_t)d));
+            const uint32_t par = (xph >> xb) & 1u;
+            if (!mbar_test(ba, par)) {
+                const unsigned long long t0 = now_ns();
+                while (!mbar_test(ba, par)) {
+                    if (vs->abort || now_ns() - t0 > FX_WAIT_NS) {
+                        atomicExch(F.status, 1);
+                        vs->abort = 1;
+                        break;
+                    }
+                }
+            }
+            float v;
+            if (strict_sum) {
+                const int a = F.nmin - 1, b = F.npt;    // 0-based rows a..b-1
                 float c = 0.0f;
                 int i = a;
-                for (; i < b && (i & 3); ++i) c = __fadd_rn(c, gat[i]);
-                const float4 *g4 = (const float4 *)gat;
+                for (; i < b && (i & 3); ++i) c = __fadd_rn(c, gb[i]);
+                const float4 *g4 = (const float4 *)gb;
                 for (; i + 3 < b; i += 4) {
-                    const float4 v = g4[i >> 2];
-                    c = __fadd_rn(c, v.x);
-                    c = __fadd_rn(c, v.y);
-                    c = __fadd_rn(c, v.z);
-                    c = __fadd_rn(c, v.w);
+                    const float4 u = g4[i >> 2];
+                    c = __fadd_rn(c, u.x);
+                    c = __fadd_rn(c, u.y);
+                    c = __fadd_rn(c, u.z);
+                    c = __fadd_rn(c, u.w);
                 }
-                for (; i < b; ++i) c = __fadd_rn(c, gat[i]);
-                s_val = c;
-            }
-            generate(gen_until);  // the generator warp, while thread 0 sums
-        } else {
-            generate(gen_until);
-        }
-        if (!strict_sum && tid == 0) {
-            {
+                for (; i < b; ++i) c = __fadd_rn(c, gb[i]);
+                v = c;
+            } else {
                 double t = 0.0;
-                for (int q = 0; q < ncta; ++q) t += *cl.map_shared_rank(part + buf, q);
-                s_val = (float)t;
+                for (int q = 0; q < nw; ++q) t += parts[xb * nw + q];
+                v = (float)t;
             }
+            vs->val = v;
         }
-        __syncthreads();
-        buf ^= 1;
-        return s_val;
+        xph ^= 1u << xb;
+        xb ^= 1;
+        block_sync();
+        return vs->val;
+    };
+    // the largest |wt| over the perturbed terms, for the clamp bound (thread 0; a barrier
+    // follows before any row reads it)
+    auto wmax_all = [&]() {
+        float b = 0.0f;
+        for (int m = F.ncfirst; m <= nt; ++m) b = fmaxf(b, fabsf(wt[m]));
+        vs->wmx[0] = b;
+        for (int k = 1; k < FX_WARPS; ++k) vs->wmx[k] = 0.0f;
     };
 
-    float stepr = F.scal[0];
-    float rejrat = F.scal[2];
-    float chisqnew = F.scal[3];
+    long long cursor = 0;
     const float acceptr = 0.05f;
     const int npoints = F.npt - F.nmin + 1;
-    long long trials = 0, cursor = 0;
-    float wtmax = 0.0f;
-    for (int it = 1; it <= nt; ++it) {
-        const float a = fabsf(wt[it]);
-        wtmax = (a >= wtmax) ? a : wtmax;
-    }
-    if (stepr < __fmul_rn(1.0e-6f, wtmax)) stepr = __fmul_rn(2.0e-6f, wtmax);
-    if (F.nits > 0) {
-        int icount = 0;
-        chisqnew = chisq(cursor + K, false, F.strict);
-        float chisqold = chisqnew;
-        float chisqtest = -1.0f;
-        int itry = 0;
-        while (itry < 10 || (itry < 150 && chisqtest < 1.0e-4f)) {
-            ++itry;
-            const float accept = __fdiv_rn(__fmul_rn(acceptr, chisqold), (float)npoints);
-            rejrat = 0.0f;
-            const float chisqstart = __fdiv_rn(chisqold, (float)npoints);
-            for (int st = 1; st <= 100; ++st) {
-                ++trials;
-                // perturb coefficients ncfirst..nterms with the next K values (:4856-4861)
-                for (int ic = F.ncfirst + tid; ic <= nt; ic += blockDim.x) {
-                    const float u = ring[(cursor + ic - F.ncfirst) & (FX_RING - 1)];
-                    const float du = __fsub_rn(__fmul_rn(2.0f, u), 1.0f);
-                    if (fabsf(wtold[ic]) < 1.0f) wt[ic] = __fadd_rn(wtold[ic], __fmul_rn(stepr, du));
-                    else wt[ic] = __fmul_rn(wtold[ic], __fadd_rn(1.0f, __fmul_rn(stepr, du)));
-                }
-                cursor += K;
-                __syncthreads();
-                // the conditional draw of this trial and the next trial's K draws
-                chisqnew = chisq(cursor + 1 + K, false, F.strict);
-                const float exponent = __fdiv_rn(__fsub_rn(chisqnew, chisqold), accept);
-                float test;
-                if (exponent > 0.0f && exponent <= 20.0f) {
-                    test = __fsub_rn(exp_r(-exponent), ring[cursor & (FX_RING - 1)]);
-                    cursor += 1;
-                } else if (exponent > 20.0f) {
-                    test = -1.0f;
-                } else {
-                    test = 1.0f;
-                }
-                if (test >= 0.0f) {
-                    ++icount;
-                    if (icount == F.nfreq) {
-                        icount = 0;
-                        if (tid == 0) {  // smoop(ncfirst, nterms, 1, wt)
+    for (int pi = 0; pi < F.nprob; ++pi) {
+        const float *yin = F.yin + (size_t)pi * (F.npt + 1);
+        float *yout = F.yout + (size_t)pi * (F.npt + 1);
+        const float *wto_g = F.wtold_g + (size_t)pi * (nt + 1);
+        float *scal = F.scal + (size_t)pi * 4;
+        for (int r = tid; r < rpc; r += FX_NBAR) yr[r] = r < nrow ? yin[row0 + r] : 0.0f;
+        for (int i = tid; i <= nt; i += FX_NBAR) {
+            wtold[i] = wto_g[i];
+            wt[i] = wtold[i];
+        }
+        block_sync();
+        if (tid == 0) {
+            float a = 0.0f;
+            for (int m = 1; m < F.ncfirst; ++m) a = fmaxf(a, fabsf(wt[m]));
+            vs->wfix = a;
+            wmax_all();
+        }
+        block_sync();
+        float stepr = scal[0];
+        float rejrat = scal[2];
+        float chisqnew = scal[3];
+        long long trials = 0;
+        float wtmax = 0.0f;
+        for (int it = 1; it <= nt; ++it) {
+            const float a = fabsf(wt[it]);
+            wtmax = (a >= wtmax) ? a : wtmax;
+        }
+        if (stepr < __fmul_rn(1.0e-6f, wtmax)) stepr = __fmul_rn(2.0e-6f, wtmax);
+        if (F.nits > 0 && !vs->stop) {
+            int icount = 0;
+            chisqnew = chisq(F.strict != 0, nullptr);
+            float chisqold = chisqnew;
+            float chisqtest = -1.0f;
+            int itry = 0;
+            bool stop = false;
+            while (!stop && (itry < 10 || (itry < 150 && chisqtest < 1.0e-4f))) {
+                ++itry;
+                const float accept = __fdiv_rn(__fmul_rn(acceptr, chisqold), (float)npoints);
+                rejrat = 0.0f;
+                const float chisqstart = __fdiv_rn(chisqold, (float)npoints);
+                for (int st = 1; st <= 100; ++st) {
+                    ++trials;
+                    // perturb coefficients ncfirst..nterms with the next K values (:4856-4861);
+                    // one lane per warp waits for the warp's last value
+                    if (swarp >= 0 && swarp * 32 < K) {
+                        if (lane == 0) need(cursor + min(K, swarp * 32 + 32) - 1);
+                        __syncwarp();
+                        const int ic = F.ncfirst + slot;
+                        float a = 0.0f;
+                        if (ic <= nt) {
+                            const float du = __fsub_rn(__fmul_rn(2.0f, val(cursor + slot)), 1.0f);
+                            float v;
+                            if (fabsf(wtold[ic]) < 1.0f) v = __fadd_rn(wtold[ic], __fmul_rn(stepr, du));
+                            else v = __fmul_rn(wtold[ic], __fadd_rn(1.0f, __fmul_rn(stepr, du)));
+                            wt[ic] = v;
+                            a = fabsf(v);
+                        }
+                        a = __int_as_float((int)__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(a)));
+                        if (lane == 0) vs->wmx[swarp] = a;
+                    }
+                    cursor += K;
+                    block_sync();
+                    const float cn = chisq(F.strict != 0, nullptr);
+                    if (tid == 0) {   // the Metropolis test (:4871-4880) and the smoothing (:4882-4893)
+                        const float exponent = __fdiv_rn(__fsub_rn(cn, chisqold), accept);
+                        float test;
+                        int draw = 0;
+                        if (exponent > 0.0f && exponent <= 20.0f) {
+                            need(cursor);
+                            test = __fsub_rn(exp_r(-exponent), val(cursor));
+                            draw = 1;
+                        } else if (exponent > 20.0f) {
+                            test = -1.0f;
+                        } else {
+                            test = 1.0f;
+                        }
+                        const int acc = test >= 0.0f;
+                        int sm = 0;
+                        if (acc && icount + 1 == F.nfreq) {
+                            sm = 1;        // smoop(ncfirst, nterms, 1, wt)
                             const int n1 = F.ncfirst, n2 = nt;
                             if (!(n2 - 2 < n1)) {
                                 float sm_ = 0.0f, sn = wt[n1];
@@ -266,59 +506,87 @@ __global__ void __launch_bounds__(FX_THREADS) fitexp_cluster_kernel(FxDev F) {
                                     sum1 = sum2;
                                 }
                             }
+                            wmax_all();
                         }
-                        __syncthreads();
-                        chisqnew = chisq(cursor + K, false, F.strict);
+                        vs->accept = acc;
+                        vs->smooth = sm;
+                        vs->draw = draw;
+                        vs->stop = vs->abort;
+                        vs->cons = cursor + draw;
                     }
-                    chisqold = chisqnew;
-                    for (int ic = 1 + tid; ic <= nt; ic += blockDim.x) wtold[ic] = wt[ic];
-                } else {
-                    rejrat = __fadd_rn(rejrat, 1.0f);
+                    block_sync();
+                    const int acc = vs->accept, sm = vs->smooth;
+                    stop = vs->stop != 0;
+                    cursor += vs->draw;
+                    chisqnew = cn;
+                    if (acc) {
+                        ++icount;
+                        if (sm) {
+                            icount = 0;
+                            chisqnew = chisq(F.strict != 0, nullptr);
+                        }
+                        chisqold = chisqnew;
+                        for (int k = 1 + tid; k <= nt; k += FX_NBAR) wtold[k] = wt[k];
+                    } else {
+                        rejrat = __fadd_rn(rejrat, 1.0f);
+                    }
+                    block_sync();
+                    if (stop) break;
                 }
-                __syncthreads();
+                rejrat = __fdiv_rn(rejrat, 100.0f);
+                const float chisqfinish = __fdiv_rn(chisqold, (float)npoints);
+                if (chisqstart > 0.0f) chisqtest = __fdiv_rn(__fsub_rn(chisqfinish, chisqstart), chisqstart);
+                else chisqtest = __fsub_rn(chisqfinish, chisqstart);
+                const float rejfac = rejrat > 0.0f ? __fdiv_rn(0.75f, rejrat) : 2.0f;
+                stepr = __fmul_rn(stepr, rejfac);
             }
-            rejrat = __fdiv_rn(rejrat, 100.0f);
-            const float chisqfinish = __fdiv_rn(chisqold, (float)npoints);
-            if (chisqstart > 0.0f) chisqtest = __fdiv_rn(__fsub_rn(chisqfinish, chisqstart), chisqstart);
-            else chisqtest = __fsub_rn(chisqfinish, chisqstart);
-            const float rejfac = rejrat > 0.0f ? __fdiv_rn(0.75f, rejrat) : 2.0f;
-            stepr = __fmul_rn(stepr, rejfac);
+            for (int k = 1 + tid; k <= nt; k += FX_NBAR) wt[k] = wtold[k];
+            block_sync();
+            if (tid == 0) wmax_all();
+            block_sync();
         }
-        for (int ic = 1 + tid; ic <= nt; ic += blockDim.x) wt[ic] = wtold[ic];
-        __syncthreads();
-    }
-    // final fit over rows 1..npt, chi^2 from nmin (:4908-4914); the chi^2 is strict here
-    chisqnew = chisq(cursor, true, true);
-    if (rank == 0) {
-        for (int ic = tid; ic <= nt; ic += blockDim.x) {
-            F.wt_g[ic] = wt[ic];
-            F.wtold_g[ic] = wtold[ic];
-        }
-        if (tid == 0) {
-            F.scal[0] = stepr;
-            F.scal[1] = acceptr;
-            F.scal[2] = rejrat;
-            F.scal[3] = chisqnew;
-            *F.trials = trials;
-            // the stream state after exactly `cursor` draws: the last batch checkpoint at or
-            // before it, advanced one draw at a time
-            int best = -1;
-            for (int k = 0; k < FX_CK; ++k)
-                if (ckpos[k] >= 0 && ckpos[k] <= cursor && (best < 0 || ckpos[k] > ckpos[best])) best = k;
-            Ran1 R;
-            if (best >= 0) {
-                R.idum = ck[best * FX_CKW + 0];
-                R.iy = ck[best * FX_CKW + 1];
-                for (int i = 0; i < 32; ++i) R.iv[i] = ck[best * FX_CKW + 2 + i];
-                for (long long k = ckpos[best]; k < cursor; ++k) ran1_next(R);
-            } else {
-                ran1_load(R, F.ran1);
+        // final fit over rows 1..npt, chi^2 from nmin (:4908-4914), in the reference's order
+        chisqnew = chisq(true, yout);
+        if (rank == 0) {
+            float *wt_g = F.wt_g + (size_t)pi * (nt + 1);
+            float *wtold_o = F.wtold_g + (size_t)pi * (nt + 1);
+            for (int k = tid; k <= nt; k += FX_NBAR) {
+                wt_g[k] = wt[k];
+                wtold_o[k] = wtold[k];
             }
-            R.mcall = (int32_t)((uint32_t)mcall0 + (uint32_t)cursor);
-            ran1_store(R, F.ran1);
+            if (tid == 0) {
+                scal[0] = stepr;
+                scal[1] = acceptr;
+                scal[2] = rejrat;
+                scal[3] = chisqnew;
+                F.trials[pi] = trials;
+            }
         }
+        block_sync();
     }
-    cl.sync();  // no CTA leaves while others may still read its shared memory
+    // stop the stream warp, then rebuild the state after exactly `cursor` draws from the
+    // last checkpoint at or before it (or from the launch's state when none is left)
+    if (tid == 0) vs->done = 1;
+    __syncwarp();
+    __syncthreads();
+    if (rank == 0 && tid == 0 && !vs->abort) {
+        int best = -1;
+        for (int k = 0; k < FX_CK; ++k)
+            if (ckpos[k] >= 0 && ckpos[k] <= cursor && (best < 0 || ckpos[k] > ckpos[best])) best = k;
+        Ran1 R;
+        long long from = 0;
+        ran1_load(R, F.ran1);
+        if (best >= 0) {
+            R.idum = ck[best * FX_CKW + 0];
+            R.iy = ck[best * FX_CKW + 1];
+            for (int i = 0; i < 32; ++i) R.iv[i] = ck[best * FX_CKW + 2 + i];
+            from = ckpos[best];
+        }
+        for (long long k = from; k < cursor; ++k) ran1_next(R);
+        R.mcall = (int32_t)((uint32_t)mcall0 + (uint32_t)cursor);
+        ran1_store(R, F.ran1);
+    }
+    cl.sync();  // no CTA leaves while others may still write into its shared memory
 }
 
 }  // namespace epsr
@@ -327,11 +595,13 @@ using namespace epsr;
 
 static inline size_t al256f(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static int fx_cluster_size(int npt, int nterms, int *rpc_out) {
-    const size_t budget = 200 * 1024;
+// Smallest cluster whose CTAs hold their rows in shared memory with one row per slot
+// thread (at most 8 CTAs).
+static int fx_workers(int npt, int nterms, int *rpc_out) {
+    const size_t budget = 220 * 1024;
     for (int c = 1; c <= 8; ++c) {
         const int rpc = (npt + c - 1) / c;
-        if (fx_smem_bytes(nterms, rpc, c) <= budget) {
+        if (rpc <= FX_SLOTS && fx_smem_bytes(nterms, rpc, c) <= budget) {
             *rpc_out = rpc;
             return c;
         }
@@ -339,47 +609,60 @@ static int fx_cluster_size(int npt, int nterms, int *rpc_out) {
     return 0;
 }
 
-extern "C" int64_t epsr_fit_expansion_scratch_bytes(int32_t npt, int32_t nterms) {
+extern "C" int64_t epsr_fit_expansion_batch_scratch_bytes(int32_t nprob, int32_t npt, int32_t nterms) {
     (void)npt;
     (void)nterms;
-    return (int64_t)(al256f(sizeof(float) * 4) + al256f(sizeof(long long)));
+    if (nprob < 1) nprob = 1;
+    return (int64_t)(al256f(sizeof(float) * 4 * (size_t)nprob) + al256f(sizeof(long long) * (size_t)nprob) +
+                     al256f(sizeof(int)));
 }
 
-extern "C" int epsr_fit_expansion(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
-                                  float *scal_host, int32_t nmin, int32_t npt, int32_t ncfirst, int32_t nterms,
-                                  int32_t nits, int32_t nfreq, int32_t *ran1, void *scratch, int64_t scratch_bytes,
-                                  int32_t strict, int64_t *trials_host, void *stream) {
-    if (!yin || !expr || !yout || !wt || !wtold || !scal_host || !ran1 || !scratch || !trials_host || npt <= 0 ||
-        nterms <= 0 || nmin < 1 || ncfirst < 1 || ncfirst > nterms) {
+extern "C" int64_t epsr_fit_expansion_scratch_bytes(int32_t npt, int32_t nterms) {
+    return epsr_fit_expansion_batch_scratch_bytes(1, npt, nterms);
+}
+
+extern "C" int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const float *expr, float *yout, float *wt,
+                                        float *wtold, float *scal_host, int32_t nmin, int32_t npt, int32_t ncfirst,
+                                        int32_t nterms, int32_t nits, int32_t nfreq, int32_t *ran1, void *scratch,
+                                        int64_t scratch_bytes, int32_t strict, int64_t *trials_host, void *stream) {
+    if (nprob <= 0 || !yin || !expr || !yout || !wt || !wtold || !scal_host || !ran1 || !scratch || !trials_host ||
+        npt <= 0 || nterms <= 0 || nmin < 1 || nmin > npt || ncfirst < 1 || ncfirst > nterms) {
         epsr_set_error("epsr_fit_expansion: bad arguments");
         return EPSR_ERR_ARG;
     }
-    if (scratch_bytes < epsr_fit_expansion_scratch_bytes(npt, nterms)) {
+    if (scratch_bytes < epsr_fit_expansion_batch_scratch_bytes(nprob, npt, nterms)) {
         epsr_set_error("epsr_fit_expansion: scratch too small");
         return EPSR_ERR_CAPACITY;
     }
-    if (nterms + 64 > FX_RING) {
-        epsr_set_error("epsr_fit_expansion: at most %d terms", FX_RING - 64);
+    if (nterms - ncfirst + 1 > FX_SLOTS) {
+        epsr_set_error("epsr_fit_expansion: at most %d perturbed terms", FX_SLOTS);
         return EPSR_ERR_UNSUPPORTED;
     }
     int rpc = 0;
-    const int csize = fx_cluster_size(npt, nterms, &rpc);
-    if (!csize) {
+    const int nw = fx_workers(npt, nterms, &rpc);
+    if (!nw) {
         epsr_set_error("epsr_fit_expansion: %d rows x %d terms exceed 8 CTAs of shared memory", npt, nterms);
         return EPSR_ERR_UNSUPPORTED;
     }
     cudaStream_t s = (cudaStream_t)stream;
     char *p = (char *)scratch;
     float *scal = (float *)p;
-    p += al256f(sizeof(float) * 4);
+    p += al256f(sizeof(float) * 4 * (size_t)nprob);
     long long *trials = (long long *)p;
-    EPSR_CUDA(cudaMemcpyAsync(scal, scal_host, sizeof(float) * 4, cudaMemcpyHostToDevice, s));
+    p += al256f(sizeof(long long) * (size_t)nprob);
+    int *status = (int *)p;
+    EPSR_CUDA(cudaMemcpyAsync(scal, scal_host, sizeof(float) * 4 * (size_t)nprob, cudaMemcpyHostToDevice, s));
+    EPSR_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));
     FxDev F;
-    F.yin = yin;
     F.expr = expr;
+    F.yin = yin;
     F.yout = yout;
     F.wt_g = wt;
     F.wtold_g = wtold;
+    F.scal = scal;
+    F.trials = trials;
+    F.status = status;
+    F.nprob = nprob;
     F.nmin = nmin;
     F.npt = npt;
     F.ncfirst = ncfirst;
@@ -389,27 +672,37 @@ extern "C" int epsr_fit_expansion(const float *yin, const float *expr, float *yo
     F.strict = strict ? 1 : 0;
     F.rpc = rpc;
     F.ran1 = ran1;
-    F.scal = scal;
-    F.trials = trials;
-    const size_t shm = fx_smem_bytes(nterms, rpc, csize);
+    const size_t shm = fx_smem_bytes(nterms, rpc, nw);
     EPSR_CUDA(cudaFuncSetAttribute(fitexp_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(csize, 1, 1);
+    cfg.gridDim = dim3(nw, 1, 1);
     cfg.blockDim = dim3(FX_THREADS, 1, 1);
     cfg.dynamicSmemBytes = shm;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = csize;
+    attr[0].val.clusterDim.x = nw;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     EPSR_CUDA(cudaLaunchKernelEx(&cfg, fitexp_cluster_kernel, F));
-    long long th = 0;
-    EPSR_CUDA(cudaMemcpyAsync(scal_host, scal, sizeof(float) * 4, cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaMemcpyAsync(&th, trials, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    int hstatus = 0;
+    EPSR_CUDA(cudaMemcpyAsync(scal_host, scal, sizeof(float) * 4 * (size_t)nprob, cudaMemcpyDeviceToHost, s));
+    EPSR_CUDA(cudaMemcpyAsync(trials_host, trials, sizeof(long long) * (size_t)nprob, cudaMemcpyDeviceToHost, s));
+    EPSR_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, s));
     EPSR_CUDA(cudaStreamSynchronize(s));
-    *trials_host = th;
+    if (hstatus) {
+        epsr_set_error("epsr_fit_expansion: a bounded device wait gave up (results invalid)");
+        return EPSR_ERR_TIMEOUT;
+    }
     return EPSR_OK;
+}
+
+extern "C" int epsr_fit_expansion(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
+                                  float *scal_host, int32_t nmin, int32_t npt, int32_t ncfirst, int32_t nterms,
+                                  int32_t nits, int32_t nfreq, int32_t *ran1, void *scratch, int64_t scratch_bytes,
+                                  int32_t strict, int64_t *trials_host, void *stream) {
+    return epsr_fit_expansion_batch(1, yin, expr, yout, wt, wtold, scal_host, nmin, npt, ncfirst, nterms, nits, nfreq,
+                                    ran1, scratch, scratch_bytes, strict, trials_host, stream);
 }

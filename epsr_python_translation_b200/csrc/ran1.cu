@@ -4,7 +4,7 @@
 // holds idum after l+1 more steps (Schrage's method computes IA*idum mod IM exactly, so a
 // 64-bit modular product with IA^k gives the same value).  The Bays-Durham shuffle is an
 // inherently sequential pointer chase; its 32-entry table lives one entry per lane and
-// each step is a shift plus a warp shuffle.
+// each step is a warp shuffle (Ran1Warp in common.cuh).
 //
 // The reference re-initialises on any call that finds idum <= 0 or iy == 0 (:346).  That
 // happens at the first call of a stream and, for the degenerate seed -(2^31-1), again after
@@ -18,24 +18,22 @@ __global__ void ran1_fill_kernel(int32_t *state, float *out, int64_t n_host, con
     const int lane = threadIdx.x & 31;
     const int64_t n = n_dev ? (int64_t)*n_dev : n_host;
     __shared__ int32_t tab[34];
-    int32_t idum = state[0], iy = state[1];
+    Ran1Warp g;
+    g.load(state);
     const int32_t mcall = state[2];
-    int32_t iv = state[3 + lane];
     __syncwarp();
-    uint32_t mul = 16807u;  // IA^(lane+1) mod IM
-    for (int k = 0; k < lane; ++k) mul = r1_mulmod(mul, 16807u);
     int64_t done = 0;
     while (done < n) {
         const int64_t left = n - done;
         int32_t mine;
-        const int cnt = ran1_warp_batch(idum, iy, iv, mul, left > 32 ? 32 : (int)left, mine, tab);
+        const int cnt = g.next(left > 32 ? 32 : (int)left, mine, tab);
         if (lane < cnt) out[done + lane] = ran1_out(mine);
         done += cnt;
     }
-    state[3 + lane] = iv;
+    state[3 + lane] = g.iv;
     if (lane == 0) {
-        state[0] = idum;
-        state[1] = iy;
+        state[0] = g.idum;
+        state[1] = g.iy;
         state[2] = (int32_t)((uint32_t)mcall + (uint32_t)n);
     }
 }

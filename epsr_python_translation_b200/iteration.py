@@ -44,8 +44,9 @@ class EpsrIteration:
         self.rminex = np.full(b.npairs, f32(-2.0), dtype=f32)
         self.xwt = torch.from_numpy(wl.xwt).to(dev)
         ndata = wl.data.shape[0]
-        self.pwtold = [torch.zeros(wl.nterms + 1, dtype=torch.float32, device=dev) for _ in range(ndata)]
-        self.stepp = [f32(0.01)] * ndata
+        self.pwtold = torch.zeros(ndata, wl.nterms + 1, dtype=torch.float32, device=dev)
+        self.stepp = np.full(ndata, f32(0.01), f32)
+        self._fit_scratch = torch.empty(4096, dtype=torch.uint8, device=dev)
         self.r = torch.from_numpy(b.x[: b.npt1 + 1].copy()).to(dev)
         self.nqmin = np.full(b.npairs, 2, np.int32)
         self.nqmax = np.full(b.npairs, wl.nq, np.int32)
@@ -80,18 +81,16 @@ class EpsrIteration:
         sofq = transforms.gensq(nq, b.npt1, d.a_wav, ld, self.foqols, nq + 1, 1, self.ycoh, d.n2extr,
                                 self.natomsphere, b.npairs)
         self.sofq = sofq.view(2, b.npairs, nq + 1)
+        inter = self.sofq[1]                                   # (npairs, nq+1)
+        # per data set: the difference between the data and the weighted simulated S(Q)
+        dt = -(self.data - torch.matmul(self.weights, inter))  # (ndata, nq+1)
         self._mark("gensq", True)
         self._mark("fit_expansion")
-        inter = self.sofq[1]                                   # (npairs, nq+1)
-        self.fit_trials = 0
-        for k in range(wl.data.shape[0]):
-            fit = torch.matmul(self.weights[k], inter)         # weighted simulated S(Q)
-            dt = -(self.data[k] - fit)
-            res = transforms.fit_expansion(dt, self.expr, self.pwtold[k], self.stepp[k], 1, nq, 1, wl.nterms, 1000,
-                                           10, self.ran1, strict=self.strict)
-            self.pwtold[k] = res["wtold"]
-            self.stepp[k] = res["stepr"]
-            self.fit_trials += res["trials"]
+        res = transforms.fit_expansion_batch(dt, self.expr, self.pwtold, self.stepp, 1, nq, 1, wl.nterms, 1000, 10,
+                                             self.ran1, strict=self.strict, scratch=self._fit_scratch)
+        self.pwtold = res["wtold"]
+        self.stepp = res["stepr"]
+        self.fit_trials = int(res["trials"].sum())
         self._mark("fit_expansion", True)
         self._mark("stog")
         self.gofr = transforms.stog(float(b.natom) / float(wl.system.L) ** 3, self.q, inter, self.r, self.nqmin,
@@ -113,6 +112,6 @@ class EpsrIteration:
         coefficients (generate_ep).  Returns the arrays and their total bytes."""
         co = self.d.download_coords()
         wav = self.d.a_wav.cpu().numpy()
-        pw = [t.cpu().numpy() for t in self.pwtold]
-        nbytes = sum(v.nbytes for v in co.values()) + wav.nbytes + sum(p.nbytes for p in pw)
+        pw = self.pwtold.cpu().numpy()
+        nbytes = sum(v.nbytes for v in co.values()) + wav.nbytes + pw.nbytes
         return (co, wav, pw), nbytes

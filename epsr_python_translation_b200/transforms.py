@@ -73,3 +73,30 @@ def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfr
                                  trials.ctypes.data_as(C.c_void_p), _s()))
     return dict(wt=wt, wtold=wto, yout=yout, stepr=f32(scal[0]), acceptr=f32(scal[1]), rejrat=f32(scal[2]),
                 chisq=f32(scal[3]), trials=int(trials[0]))
+
+
+def fit_expansion_batch(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1_t, strict=True,
+                        scratch=None):
+    """fit_expansion for each row of yin (nprob, npt+1) in turn on one ran1 stream, in one
+    launch (the reference's successive calls per data set, epsr_standalone_rev3.py:3936).
+    wtold (nprob, nterms+1) and stepr (nprob,) are the per-set inputs.  Returns a dict of
+    per-set outputs (tensors with a leading nprob axis, host arrays for the scalars)."""
+    lib = _lib.load(require_device=True)
+    y = _dev(yin)
+    nprob = y.shape[0]
+    e = _dev(expr)
+    wt = torch.zeros(nprob, nterms + 1, dtype=torch.float32, device="cuda")
+    wto = _dev(wtold).clone()
+    yout = torch.zeros(nprob, npt + 1, dtype=torch.float32, device="cuda")
+    scal = np.zeros((nprob, 4), f32)
+    scal[:, 0] = np.asarray(stepr, f32)
+    nb = int(lib.epsr_fit_expansion_batch_scratch_bytes(nprob, npt, nterms))
+    scr = scratch if scratch is not None and scratch.numel() >= nb else torch.empty(nb, dtype=torch.uint8,
+                                                                                     device="cuda")
+    trials = np.zeros(nprob, np.int64)
+    check(lib.epsr_fit_expansion_batch(nprob, _p(y), _p(e), _p(yout), _p(wt), _p(wto),
+                                       scal.ctypes.data_as(C.c_void_p), nmin, npt, ncfirst, nterms, nits, nfreq,
+                                       _p(ran1_t), _p(scr), scr.numel(), 1 if strict else 0,
+                                       trials.ctypes.data_as(C.c_void_p), _s()))
+    return dict(wt=wt, wtold=wto, yout=yout, stepr=scal[:, 0].copy(), acceptr=scal[:, 1].copy(),
+                rejrat=scal[:, 2].copy(), chisq=scal[:, 3].copy(), trials=trials)

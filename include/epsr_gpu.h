@@ -231,12 +231,24 @@ int epsr_stog(float rho, const float *q, int32_t ldq, const float *sofq, const f
  * scal_host[4] in/out = {stepr, acceptr, rejrat, chisqnew}; returns trials via
  * *trials_host.  ran1: device state.  strict=1 sums chi^2 in the reference's row order
  * (bit-identical); strict=0 in double.  Runs on one thread-block cluster whose CTAs keep the
- * basis rows in shared memory (up to 8 CTAs).  Synchronous. */
+ * basis rows in shared memory (up to 8 CTAs, one row per worker thread: npt <= 8*480).
+ * Returns EPSR_ERR_TIMEOUT if a bounded device wait gave up.  Synchronous. */
 int epsr_fit_expansion(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
                        float *scal_host, int32_t nmin, int32_t npt, int32_t ncfirst, int32_t nterms, int32_t nits,
                        int32_t nfreq, int32_t *ran1, void *scratch, int64_t scratch_bytes, int32_t strict,
                        int64_t *trials_host, void *stream);
 int64_t epsr_fit_expansion_scratch_bytes(int32_t npt, int32_t nterms);
+
+/* fit_expansion for nprob data sets in one launch, in order, on one ran1 stream -- what the
+ * reference's successive calls for each data set do (ptgnsq epsr_standalone_rev3.py:3936-3944).
+ * yin, yout [nprob*(npt+1)], wt, wtold [nprob*(nterms+1)], scal_host [nprob*4],
+ * trials_host [nprob]; expr and the other arguments as epsr_fit_expansion.  Returns
+ * EPSR_ERR_TIMEOUT if a bounded device wait gave up.  Synchronous. */
+int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const float *expr, float *yout, float *wt,
+                             float *wtold, float *scal_host, int32_t nmin, int32_t npt, int32_t ncfirst,
+                             int32_t nterms, int32_t nits, int32_t nfreq, int32_t *ran1, void *scratch,
+                             int64_t scratch_bytes, int32_t strict, int64_t *trials_host, void *stream);
+int64_t epsr_fit_expansion_batch_scratch_bytes(int32_t nprob, int32_t npt, int32_t nterms);
 
 #ifdef __cplusplus
 }

@@ -353,3 +353,61 @@ def test_fit_expansion_device_matches_reference(run):
         assert_bits_equal(res[k], z[p + k], k)
     s = st.cpu().numpy()
     assert int(s[0]) == int(z[p + "ran1_after_idum"]) and int(s[2]) == int(z[p + "ran1_after_mcall"])
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_fit_expansion_batch_equals_successive_calls(strict):
+    """One launch over three data sets equals three successive calls on the same ran1
+    stream (the reference's ptgnsq loop), bit for bit, in both summation modes; the C2-size
+    basis (600 Q rows x 116 terms) runs on a two-CTA cluster."""
+    from epsr_python_translation_b200 import configs, transforms
+    wl = configs.make_workload("c2_mixture")
+    nq, nt = wl.nq, wl.nterms
+    rng = np.random.default_rng(3)
+    ndata = 3
+    yin = np.zeros((ndata, nq + 1), f32)
+    yin[:, 1:] = (rng.standard_normal((ndata, nq)) * 0.05).astype(f32)
+    wtold = np.zeros((ndata, nt + 1), f32)
+    wtold[:, 1:] = (rng.standard_normal((ndata, nt)) * 0.01).astype(f32)
+    stepr = np.array([0.01, 0.02, 0.005], f32)
+    seed = Ran1State(idum=-99)
+    st1 = torch.from_numpy(seed.as_array()).cuda()
+    single = []
+    for k in range(ndata):
+        single.append(transforms.fit_expansion(yin[k], wl.expr, wtold[k], stepr[k], 1, nq, 1, nt, 1000, 10, st1,
+                                               strict=strict))
+    st2 = torch.from_numpy(seed.as_array()).cuda()
+    b = transforms.fit_expansion_batch(yin, wl.expr, wtold, stepr, 1, nq, 1, nt, 1000, 10, st2, strict=strict)
+    for k in range(ndata):
+        for name in ("wt", "wtold", "yout"):
+            assert_bits_equal(b[name][k].cpu().numpy(), single[k][name].cpu().numpy(), f"{name} {k}")
+        for name in ("stepr", "acceptr", "rejrat", "chisq"):
+            assert_bits_equal(b[name][k], single[k][name], f"{name} {k}")
+        assert int(b["trials"][k]) == single[k]["trials"]
+    assert np.array_equal(st1.cpu().numpy(), st2.cpu().numpy())
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_fit_expansion_c2_size_strict_matches_oracle(seed):
+    """At the C2 size (600 Q rows x 116 terms, 116 draws per trial, a two-worker cluster with
+    the ran1 stream generated on its own CTA) the strict fit equals the C oracle bit for bit:
+    coefficients, fitted curve, step, rates, chi^2 and the ran1 state."""
+    from epsr_python_translation_b200 import configs, transforms
+    wl = configs.make_workload("c2_mixture")
+    nq, nt = wl.nq, wl.nterms
+    rng = np.random.default_rng(seed)
+    yin = np.zeros(nq + 1, f32)
+    yin[1:] = (rng.standard_normal(nq) * 0.05).astype(f32)
+    wtold = np.zeros(nt + 1, f32)
+    wtold[1:] = (rng.standard_normal(nt) * 0.01).astype(f32)
+    st0 = Ran1State(idum=-seed)
+    t = torch.from_numpy(st0.as_array()).cuda()
+    res = transforms.fit_expansion(yin, wl.expr, wtold, f32(0.01), 1, nq, 1, nt, 1000, 10, t, strict=True)
+    ref, rst = oracle.fit_expansion(yin, wl.expr, wtold.copy(), f32(0.01), 1, nq, 1, nt, 1000, 10, st0)
+    assert_bits_equal(res["wt"].cpu().numpy()[1:], ref["wt"][1:], "wt")
+    assert_bits_equal(res["wtold"].cpu().numpy()[1:], ref["wtold"][1:], "wtold")
+    assert_bits_equal(res["yout"].cpu().numpy()[1:], ref["yout"][1:], "yout")
+    for k in ("stepr", "acceptr", "rejrat", "chisq"):
+        assert_bits_equal(res[k], ref[k], k)
+    assert res["trials"] == ref["trials"]
+    assert np.array_equal(t.cpu().numpy(), rst.as_array())
