@@ -367,7 +367,7 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
         return EPSR_ERR_UNSUPPORTED;
     }
     if (shm > 48 * 1024)
-        EPSR_CUDA(cudaFuncSetAttribute(ag_inter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        EPSR_SMEM_OPTIN(ag_inter_kernel);
     if (noatoms > 0) {
         dim3 grid((natom + tile - 1) / tile, ychunks);
         ag_inter_kernel<<<grid, AG_THREADS, shm, s>>>(A, oatoms, misc + 1, molof, tile, counts, counts + 2 * nbins);

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/epsr_gpu.h"
 
 namespace epsr {
@@ -302,4 +304,25 @@ int epsr_cuda_check(cudaError_t e, const char *what);
     do {                                                             \
         cudaError_t _e = (call);                                     \
         if (_e != cudaSuccess) return epsr_cuda_check(_e, #call);    \
+    } while (0)
+
+// Raise a kernel's dynamic shared-memory limit to the device's opt-in maximum (less the
+// kernel's static shared memory), once per
+// kernel and device (ordinal < 64).  Changing a kernel's attribute waits for its running
+// instances, so a call on every launch would serialise the same kernel across streams;
+// after the first call no launch touches the attribute again.
+#define EPSR_SMEM_OPTIN(kernel)                                                                      \
+    do {                                                                                             \
+        static std::atomic<unsigned long long> _optin_done{0};                                       \
+        int _dev = 0;                                                                                \
+        EPSR_CUDA(cudaGetDevice(&_dev));                                                             \
+        if (_dev < 0 || _dev >= 64 || !((_optin_done.load() >> _dev) & 1ull)) {                      \
+            int _mx = 0;                                                                             \
+            cudaFuncAttributes _fa;                                                                  \
+            EPSR_CUDA(cudaDeviceGetAttribute(&_mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, _dev));  \
+            EPSR_CUDA(cudaFuncGetAttributes(&_fa, kernel));                                          \
+            EPSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                           _mx - (int)_fa.sharedSizeBytes));                         \
+            if (_dev >= 0 && _dev < 64) _optin_done.fetch_or(1ull << _dev);                          \
+        }                                                                                            \
     } while (0)

@@ -673,7 +673,7 @@ extern "C" int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const f
     F.rpc = rpc;
     F.ran1 = ran1;
     const size_t shm = fx_smem_bytes(nterms, rpc, nw);
-    EPSR_CUDA(cudaFuncSetAttribute(fitexp_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    EPSR_SMEM_OPTIN(fitexp_cluster_kernel);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nw, 1, 1);
     cfg.blockDim = dim3(FX_THREADS, 1, 1);

@@ -684,8 +684,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     EPSR_CUDA(cudaMemsetAsync(S.nearc, 0, sizeof(double) * (size_t)N * SP_W, s));
     spec_corr_kernel<<<N, 128, 0, s>>>(S);
     const size_t bits = sizeof(unsigned) * (((size_t)N + 31) / 32);
-    if (bits > 48 * 1024) EPSR_CUDA(cudaFuncSetAttribute(spec_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)bits));
+    if (bits > 48 * 1024) EPSR_SMEM_OPTIN(spec_resolve_kernel);
     spec_resolve_kernel<<<1, 512, bits, s>>>(S);
     spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
     spec_commit_store_kernel<<<N, 128, 0, s>>>(S);

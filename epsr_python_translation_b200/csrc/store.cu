@@ -476,8 +476,7 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
         epsr_set_error("epsr_fmolec1: nnbrefmax %d too large for the row sort", M);
         return EPSR_ERR_CAPACITY;
     }
-    if (shm > 48 * 1024) EPSR_CUDA(cudaFuncSetAttribute(fm_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                        (int)shm));
+    if (shm > 48 * 1024) EPSR_SMEM_OPTIN(fm_sort_kernel);
     fm_sort_kernel<<<nmol, 256, shm, s>>>(M, rowcnt, store->nergpairm, store->molergpair, store->ergpairref, cap);
     fm_sums_kernel<<<1, strict ? 32 : 1024, 0, s>>>(store->ergpair, nintra, (int)ntot, eintra, nmol, strict, sums);
     if (store->mirror) {
