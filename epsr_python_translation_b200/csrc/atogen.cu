@@ -353,8 +353,7 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
     ag_origin_atoms_kernel<<<(nmol + 127) / 128, 128, 0, s>>>(A, origins, misc, prefix, oatoms);
     EPSR_CUDA(cudaGetLastError());
     int32_t hmisc[2];
-    EPSR_CUDA(cudaMemcpyAsync(hmisc, misc, sizeof(hmisc), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_D2H(hmisc, misc, sizeof(hmisc), s);
     const int noatoms = hmisc[1];
     // tile of target atoms: enough blocks to fill the GPU several times over
     int tile = 1024;
@@ -376,8 +375,7 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
                                                 addwav, ycoh, wav, potex);
     EPSR_CUDA(cudaGetLastError());
     long long hp[2];
-    EPSR_CUDA(cudaMemcpyAsync(hp, pairc, sizeof(hp), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_D2H(hp, pairc, sizeof(hp), s);
     g_last_pairs = hp[0] + hp[1];
     *ngrsamples_io = ngr;
     return EPSR_OK;

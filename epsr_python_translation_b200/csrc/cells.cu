@@ -291,8 +291,7 @@ extern "C" int epsr_cell_list(const float *xadd, const float *yadd, const float 
                                                                 dims[1], dims[2], misc + 2);
     EPSR_CUDA(cudaGetLastError());
     int32_t host[3];
-    EPSR_CUDA(cudaMemcpyAsync(host, misc, sizeof(host), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_D2H(host, misc, sizeof(host), s);
     cells->ncelldiva = dims[0];
     cells->ncelldivb = dims[1];
     cells->ncelldivc = dims[2];
@@ -313,7 +312,6 @@ extern "C" int epsr_nnbrefmax(const epsr_cells_t *cells, int32_t *out, int32_t *
     region_count_kernel<<<(cells->ncell + 127) / 128, 128, 0, s>>>(cells->cell_start, cells->offsets,
                                                                    cells->ncellneighb, cells->ncelldiva,
                                                                    cells->ncelldivb, cells->ncelldivc, nullptr, d);
-    EPSR_CUDA(cudaMemcpyAsync(out, d, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_D2H(out, d, sizeof(int32_t), s);
     return EPSR_OK;
 }

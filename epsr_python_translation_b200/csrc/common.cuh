@@ -300,6 +300,19 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 // Error plumbing shared by the ABI translation units.
 void epsr_set_error(const char *fmt, ...);
 int epsr_cuda_check(cudaError_t e, const char *what);
+int epsr_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s);
+int epsr_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s);
+// device -> pageable host copy after the stream drained (epsr_d2h); returns on error
+#define EPSR_D2H(dst, src, bytes, s)                             \
+    do {                                                         \
+        const int _r = epsr_d2h((dst), (src), (bytes), (s));     \
+        if (_r) return _r;                                       \
+    } while (0)
+#define EPSR_H2D(dst, src, bytes, s)                             \
+    do {                                                         \
+        const int _r = epsr_h2d((dst), (src), (bytes), (s));     \
+        if (_r) return _r;                                       \
+    } while (0)
 #define EPSR_CUDA(call)                                              \
     do {                                                             \
         cudaError_t _e = (call);                                     \

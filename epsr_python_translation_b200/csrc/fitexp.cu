@@ -651,7 +651,7 @@ extern "C" int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const f
     long long *trials = (long long *)p;
     p += al256f(sizeof(long long) * (size_t)nprob);
     int *status = (int *)p;
-    EPSR_CUDA(cudaMemcpyAsync(scal, scal_host, sizeof(float) * 4 * (size_t)nprob, cudaMemcpyHostToDevice, s));
+    EPSR_H2D(scal, scal_host, sizeof(float) * 4 * (size_t)nprob, s);
     EPSR_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));
     FxDev F;
     F.expr = expr;
@@ -688,10 +688,9 @@ extern "C" int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const f
     cfg.numAttrs = 1;
     EPSR_CUDA(cudaLaunchKernelEx(&cfg, fitexp_cluster_kernel, F));
     int hstatus = 0;
-    EPSR_CUDA(cudaMemcpyAsync(scal_host, scal, sizeof(float) * 4 * (size_t)nprob, cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaMemcpyAsync(trials_host, trials, sizeof(long long) * (size_t)nprob, cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_D2H(scal_host, scal, sizeof(float) * 4 * (size_t)nprob, s);
+    EPSR_D2H(trials_host, trials, sizeof(long long) * (size_t)nprob, s);
+    EPSR_D2H(&hstatus, status, sizeof(int), s);
     if (hstatus) {
         epsr_set_error("epsr_fit_expansion: a bounded device wait gave up (results invalid)");
         return EPSR_ERR_TIMEOUT;

@@ -459,8 +459,7 @@ extern "C" int epsr_en_change(const epsr_box_t *box, const epsr_store_t *store, 
     cudaStream_t s = (cudaStream_t)stream;
     en_change_kernel<<<1, 256, 0, s>>>(D, im, ergnew, ergnew);  // the total goes to slot 0
     EPSR_CUDA(cudaGetLastError());
-    EPSR_CUDA(cudaMemcpyAsync(out_host, ergnew, sizeof(float), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_D2H(out_host, ergnew, sizeof(float), s);
     return EPSR_OK;
 }
 

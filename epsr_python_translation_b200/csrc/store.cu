@@ -455,9 +455,8 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
     scan1_kernel<<<1, 1024, 0, s>>>(nullptr, nmol, iidx, 1, eintra);
     EPSR_CUDA(cudaGetLastError());
     int32_t totals[2];
-    EPSR_CUDA(cudaMemcpyAsync(&totals[0], iidx + nmol, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaMemcpyAsync(&totals[1], off + nmol, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_D2H(&totals[0], iidx + nmol, sizeof(int32_t), s);
+    EPSR_D2H(&totals[1], off + nmol, sizeof(int32_t), s);
     const int nintra = totals[0], npair = totals[1];
     const int64_t ntot = (int64_t)nintra + npair;
     if (ntot > store->capacity) {
@@ -491,10 +490,9 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
     EPSR_CUDA(cudaGetLastError());
     int32_t herr[1];
     int32_t hn = (int32_t)ntot;
-    EPSR_CUDA(cudaMemcpyAsync(store->nergpair, &hn, sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    EPSR_CUDA(cudaMemcpyAsync(herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaMemcpyAsync(out2_host, sums, sizeof(float) * 2, cudaMemcpyDeviceToHost, s));
-    EPSR_CUDA(cudaStreamSynchronize(s));
+    EPSR_H2D(store->nergpair, &hn, sizeof(int32_t), s);
+    EPSR_D2H(herr, err, sizeof(int32_t), s);
+    EPSR_D2H(out2_host, sums, sizeof(float) * 2, s);
     if (herr[0]) {
         epsr_set_error("epsr_fmolec1: neighbour region or row exceeds nnbrefmax=%d (code %d)", M, herr[0]);
         return EPSR_ERR_CAPACITY;

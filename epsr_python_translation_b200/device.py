@@ -266,8 +266,15 @@ class DeviceBox:
         self.a_wav = torch.zeros(2 * b.npairs * ld, dtype=torch.float32, device=self.dev)
         self.a_potex = torch.zeros(b.npairs, dtype=torch.float32, device=self.dev)
         counts = self.scratch("atogen_counts", 8 * (2 * b.npairs * ld + b.npairs))
-        self.a_rminex = self._t(rminex, f32)
-        self.a_ycoh = self._t(np.zeros(ld, f32) if ycoh is None else np.asarray(ycoh, f32)[:ld], f32)
+        # device tensors are used as given (no upload per call); host arrays are copied
+        if isinstance(rminex, torch.Tensor):
+            self.a_rminex = rminex
+        else:
+            self.a_rminex = self._t(rminex, f32)
+        if isinstance(ycoh, torch.Tensor):
+            self.a_ycoh = ycoh
+        else:
+            self.a_ycoh = self._t(np.zeros(ld, f32) if ycoh is None else np.asarray(ycoh, f32)[:ld], f32)
         nb = self.lib.epsr_atogen_scratch_bytes(b.nmol, b.natom, b.nmoltype, b.ntype)
         scr = self.scratch("atogen", nb)
         ngr = np.array([ngrsamples], np.int32)

@@ -36,20 +36,20 @@ class EpsrIteration:
         dev = self.d.dev
         self.q = torch.from_numpy(wl.q).to(dev)
         self.foqols = torch.from_numpy(np.ascontiguousarray(wl.foqols)).to(dev)
-        self.ycoh = torch.from_numpy(np.ascontiguousarray(wl.ycoh[: b.npt + 1])).to(dev)
+        self.ycoh = torch.from_numpy(np.ascontiguousarray(wl.ycoh[: b.npt + 1], f32)).to(dev)
         self.expr = torch.from_numpy(wl.expr).to(dev)
         self.data = torch.from_numpy(wl.data).to(dev)
         self.weights = torch.from_numpy(wl.weights).to(dev)
         self.natomsphere = torch.ones(b.ntype, dtype=torch.float32, device=dev)
-        self.rminex = np.full(b.npairs, f32(-2.0), dtype=f32)
+        self.rminex = torch.full((b.npairs,), -2.0, dtype=torch.float32, device=dev)
         self.xwt = torch.from_numpy(wl.xwt).to(dev)
         ndata = wl.data.shape[0]
         self.pwtold = torch.zeros(ndata, wl.nterms + 1, dtype=torch.float32, device=dev)
         self.stepp = np.full(ndata, f32(0.01), f32)
         self._fit_scratch = torch.empty(4096, dtype=torch.uint8, device=dev)
         self.r = torch.from_numpy(b.x[: b.npt1 + 1].copy()).to(dev)
-        self.nqmin = np.full(b.npairs, 2, np.int32)
-        self.nqmax = np.full(b.npairs, wl.nq, np.int32)
+        self.nqmin = torch.full((b.npairs,), 2, dtype=torch.int32, device=dev)
+        self.nqmax = torch.full((b.npairs,), wl.nq, dtype=torch.int32, device=dev)
         self.events = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                        for k in STAGES}
         self.moves_per_step = wl.ntimes * b.nmol
@@ -72,7 +72,7 @@ class EpsrIteration:
             d.molfit(strict=self.strict)
         self._mark("molfit", True)
         self._mark("atogen")
-        d.atogen(wl.ngrsamples, self.ran1, self.rminex, ycoh=wl.ycoh)
+        d.atogen(wl.ngrsamples, self.ran1, self.rminex, ycoh=self.ycoh)
         self.pair_updates = d.last_pair_updates
         self._mark("atogen", True)
         self._mark("gensq")
