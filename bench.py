@@ -2,16 +2,20 @@
 """Benchmark of the EPSR pair path on B200: MC molecule-moves/s (+ g(r) pair-updates/s).
 
 One step = one EPSR iteration of the hot path on configuration C2 (200 DMSO + 400 water,
-3200 atoms, 21 pair types): cell list, fmolec1, 5 molfit cycles (3000 whole-molecule
-moves), atogen over all 5,118,400 atom pairs, gensq, fit_expansion for three datasets, stog.
-``value`` = molecule moves per second of whole-step device time, inputs resident in HBM.
+3200 atoms, 21 pair types) for each of R independent boxes on the GPU (``--replicas``,
+default 16): cell list, fmolec1, 5 molfit cycles (3000 whole-molecule moves), atogen over
+all 5,118,400 atom pairs, gensq, fit_expansion for three datasets, stog.  Each box has its
+own ran1 seed, CUDA stream and host thread; a box's chain is sequential (Metropolis, one
+ran1 stream), so independent boxes are how one GPU is filled.  ``value`` = molecule moves
+of all boxes per second of device time, inputs resident in HBM; ``single_box`` reports one
+box alone (its stage breakdown feeds the roofline).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--replicas R] [--impl ours|reference]
 
-Under torchrun each rank advances its own independent box (replicas, different ran1
-seeds): there is no data-path collective, so ``scaling`` is "weak".  ``--impl reference``
-times the reference's algorithm (the C restatement in oracle/, single-threaded per
-process) on all host cores with one independent replica per core.
+Under torchrun each rank advances its own R boxes: there is no data-path collective, so
+``scaling`` is "weak".  ``--impl reference`` times the reference's algorithm (the C
+restatement in oracle/, single-threaded per process) on all host cores with one
+independent box per core.
 """
 
 from __future__ import annotations
@@ -38,6 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2_mixture")
+    ap.add_argument("--replicas", type=int, default=16, help="independent boxes per GPU (one stream each)")
     ap.add_argument("--strict", action="store_true", help="bit-identical sequential sums")
     ap.add_argument("--cpu-sample-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -167,7 +172,9 @@ class ClockSampler:
 
 
 def gpu_arm(a):
-    import numpy as np
+    import threading
+
+    import numpy as np  # noqa: F401
     import torch
     import torch.distributed as dist
 
@@ -182,17 +189,79 @@ def gpu_arm(a):
     from epsr_python_translation_b200.iteration import STAGES, EpsrIteration
 
     wl = configs.make_workload(a.config)
-    it = EpsrIteration(wl, strict=a.strict, ran1_seed=-(1 + rank))
+    R = max(1, a.replicas)
+    # independent boxes (own ran1 seeds), each driven by its own host thread on its own stream
+    streams = [torch.cuda.Stream() for _ in range(R)]
+    its = []
+    for r in range(R):
+        with torch.cuda.stream(streams[r]):
+            its.append(EpsrIteration(wl, strict=a.strict, ran1_seed=-(1 + rank * R + r)))
+    torch.cuda.synchronize()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+    main = torch.cuda.current_stream()
+
+    class Boxes:
+        """R persistent host threads, one per box; run(body) advances every box by one step
+        concurrently and returns the device time of that round (ms)."""
+
+        def __init__(self):
+            self.go = [threading.Event() for _ in range(R)]
+            self.fin = [threading.Event() for _ in range(R)]
+            self.body = None
+            self.e0 = None
+            self.done = [torch.cuda.Event() for _ in range(R)]
+            self.err = []
+            self.th = [threading.Thread(target=self._loop, args=(r,), daemon=True) for r in range(R)]
+            for t in self.th:
+                t.start()
+
+        def _loop(self, r):
+            while True:
+                self.go[r].wait()
+                self.go[r].clear()
+                if self.body is None:
+                    return
+                try:
+                    with torch.cuda.stream(streams[r]):
+                        streams[r].wait_event(self.e0)
+                        self.body(r)
+                        self.done[r].record(streams[r])
+                except Exception as e:  # reported by run()
+                    self.err.append(e)
+                self.fin[r].set()
+
+        def run(self, body):
+            self.body = body
+            self.e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            self.e0.record(main)
+            for ev in self.go:
+                ev.set()
+            for ev in self.fin:
+                ev.wait()
+                ev.clear()
+            if self.err:
+                raise self.err[0]
+            for ev in self.done:
+                main.wait_event(ev)
+            e1.record(main)
+            e1.synchronize()
+            return self.e0.elapsed_time(e1)
+
+        def close(self):
+            self.body = None
+            for ev in self.go:
+                ev.set()
+            for t in self.th:
+                t.join()
+
+    boxes = Boxes()
+    run_round = boxes.run
 
     for _ in range(max(3, a.warmup)):
-        it.step()
+        run_round(lambda r: its[r].step())
     torch.cuda.synchronize()
 
-    # ---------------- device-resident timing (value)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
-    stage_tot = {k: 0.0 for k in STAGES}
+    # ---------------- device-resident timing (value): R boxes x K steps
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     idx = vis.split(",")[local] if vis else str(local)
     clocks = ClockSampler(idx)
@@ -201,52 +270,65 @@ def gpu_arm(a):
     torch.cuda.synchronize()
     clocks.start()
     time.sleep(0.3)
+    round_ms = []
     for k in range(a.steps):
-        flush.fill_(float(k))                      # L2 flushed between timed steps (untimed)
-        starts[k].record()
-        it.step()
-        ends[k].record()
-        for s, v in it.stage_ms().items():
-            stage_tot[s] += v
+        flush.fill_(float(k))                      # L2 flushed between timed rounds (untimed)
+        torch.cuda.synchronize()
+        round_ms.append(run_round(lambda r: its[r].step()))
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    tot_ms = sum(step_ms)
+    tot_ms = sum(round_ms)
     t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     tmax_ms = float(t.item())
-    moves = it.moves_per_step
-    value = world * a.steps * moves / (tmax_ms / 1000.0)
+    moves = its[0].moves_per_step
+    value = world * R * a.steps * moves / (tmax_ms / 1000.0)
+
+    # ---------------- one box alone: stage breakdown and the roofline of the dominant kernel
+    it = its[0]
+    stage_tot = {k: 0.0 for k in STAGES}
+    single_ms = 0.0
+    with torch.cuda.stream(streams[0]):
+        for k in range(a.steps):
+            flush.fill_(float(k))
+            streams[0].wait_stream(main)
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
+            it.step()
+            s1.record()
+            for st, v in it.stage_ms().items():
+                stage_tot[st] += v
+            single_ms += s0.elapsed_time(s1)
+    torch.cuda.synchronize()
 
     # ---------------- end to end through the public API with host buffers
-    co = it.d.download_coords()
-    pinned = [torch.from_numpy(co[k]).pin_memory() for k in ("xa", "ya", "za", "xadd", "yadd", "zadd")]
-    h2d = sum(p.numel() * 4 for p in pinned)
-    e_start = torch.cuda.Event(enable_timing=True)
-    e_end = torch.cuda.Event(enable_timing=True)
-    d2h = 0
+    pinned, d2h = [], [0] * R
+    for r in range(R):
+        co = its[r].d.download_coords()
+        pinned.append([torch.from_numpy(co[k]).pin_memory() for k in ("xa", "ya", "za", "xadd", "yadd", "zadd")])
+    h2d = sum(p.numel() * 4 for p in pinned[0])
+
+    def e2e_body(r):
+        d = its[r].d
+        for name, p in zip(("xa", "ya", "za", "xadd", "yadd", "zadd"), pinned[r]):
+            getattr(d, name).copy_(p, non_blocking=True)
+        d.refresh_positions()
+        its[r].step()
+        _, d2h[r] = its[r].download_outputs()
+
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    e_start.record()
-    for k in range(a.steps):
-        for name, p in zip(("xa", "ya", "za", "xadd", "yadd", "zadd"), pinned):
-            getattr(it.d, name).copy_(p, non_blocking=True)
-        it.d.refresh_positions()
-        it.step()
-        _, d2h = it.download_outputs()
-    e_end.record()
-    torch.cuda.synchronize()
-    e2e_ms = e_start.elapsed_time(e_end)
+    e2e_ms = sum(run_round(e2e_body) for _ in range(a.steps))
     t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * a.steps * moves / (float(t.item()) / 1000.0)
+    e2e_value = world * R * a.steps * moves / (float(t.item()) / 1000.0)
 
-    # ---------------- roofline of the dominant kernel
+    boxes.close()
     stage_ms = {k: v / a.steps for k, v in stage_tot.items()}
     roof, extra = roofline(it, stage_ms, a)
     launches = kernel_launches(it, wl)
@@ -255,19 +337,25 @@ def gpu_arm(a):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": tmax_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded C2 mixture box, synthetic isotope datasets)",
+            "dtype": "f32", "data": "synthetic (seeded C2 mixture boxes, synthetic isotope datasets)",
             "config": {"workload": a.config, "nmol": it.box.nmol, "natom": it.box.natom, "npairs": it.box.npairs,
-                       "moves_per_step": moves, "pair_updates_per_step": it.pair_updates,
+                       "moves_per_step_per_box": moves, "boxes_per_gpu": R,
+                       "pair_updates_per_step_per_box": it.pair_updates,
                        "stages": "cells+fmolec1+5 molfit+atogen+gensq+fit_expansion (3 data sets)+stog",
+                       "step": f"one EPSR iteration of each of the {R} independent boxes on this GPU, each box on "
+                               "its own stream and host thread",
                        "l2": "flushed between timed steps (256 MB write)", "sums": "strict" if a.strict else "fast",
-                       "parallelism": f"replicas x{world}"},
-            "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
-            "pair_updates_per_s": it.pair_updates / (stage_ms["atogen"] / 1000.0),
-            "mc_moves_per_s_molfit_only": moves / (stage_ms["molfit"] / 1000.0),
-            "fit_trials_per_step": it.fit_trials,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                       "parallelism": f"replicas: {R} boxes per GPU x {world} GPU(s)"},
+            "single_box": {"ms_per_step": single_ms / a.steps,
+                           "moves_per_s": moves / (single_ms / a.steps / 1000.0),
+                           "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+                           "pair_updates_per_s": it.pair_updates / (stage_ms["atogen"] / 1000.0),
+                           "mc_moves_per_s_molfit_only": moves / (stage_ms["molfit"] / 1000.0),
+                           "fit_trials_per_step": it.fit_trials},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": R * h2d,
+                    "d2h_bytes_per_step": sum(d2h)},
             "roofline": roof, **extra,
-            "gpu_launches": launches * a.steps,
+            "gpu_launches": launches * a.steps * R,
             "clocks": clk,
         }
         if not a.no_cpu_baseline and world == 1:
