@@ -32,6 +32,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MC molecule-moves/s"
+# dram__bytes_read.sum + dram__bytes_write.sum of one fitexp_cluster_kernel launch on the C2
+# fit, from an ncu --set full capture of one launch (independent of the trial count: the
+# basis is read from HBM once per launch)
+FIT_DRAM_BYTES_PER_LAUNCH = 401152
+# SM cycles per ran1 value of the warp shuffle chain on an otherwise idle SM (clock64 timing)
+FIT_CHAIN_CYCLES_PER_VALUE = 46.0
 UNIT = "moves/s"
 
 
@@ -421,10 +427,16 @@ def roofline(it, stage_ms, a):
         per_launch_ms = stage_ms["fit_expansion"]
         byt = it.fit_trials * wl.nq * wl.nterms * 4
         ach = byt / (per_launch_ms / 1000.0) / 1e9
-        extra["fit_us_per_trial"] = 1000.0 * per_launch_ms / max(it.fit_trials, 1)
+        us_trial = 1000.0 * per_launch_ms / max(it.fit_trials, 1)
+        extra["fit_us_per_trial"] = us_trial
+        # The kernel is latency-bound: every trial consumes nterms+1 ran1 values from one
+        # sequential shuffle chain, measured at 46 SM cycles per value on an otherwise idle SM.
+        chain_us = (wl.nterms + 1) * FIT_CHAIN_CYCLES_PER_VALUE / (float(peaks.get("sm_max_mhz", 1965.0)))
+        extra["fit_chain_bound"] = {"us_per_trial": chain_us, "frac": chain_us / us_trial,
+                                    "cycles_per_value": FIT_CHAIN_CYCLES_PER_VALUE}
         return {"bound": "hbm", "kernel": "fitexp_cluster_kernel", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": byt,
-                "launch_ms": per_launch_ms}, extra
+                "frac": ach / hbm, "traffic": FIT_DRAM_BYTES_PER_LAUNCH, "peak_source": src,
+                "algorithmic_bytes_per_launch": byt, "launch_ms": per_launch_ms}, extra
     if dom == "atogen":
         per_launch_ms = stage_ms["atogen"]
         byt = 16 * b.natom * max(1, b.natom // 256)
