@@ -177,6 +177,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def box_seed(rank, boxes, r):
+    """ran1 seed of box r of a rank: distinct over every box of every rank."""
+    return -(1 + rank * boxes + r)
+
+
+def max_over_ranks(x, dist, device):
+    """The largest value of x over all ranks (x itself when not distributed)."""
+    import torch
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def gpu_arm(a):
     import threading
 
@@ -201,7 +216,7 @@ def gpu_arm(a):
     its = []
     for r in range(R):
         with torch.cuda.stream(streams[r]):
-            its.append(EpsrIteration(wl, strict=a.strict, ran1_seed=-(1 + rank * R + r)))
+            its.append(EpsrIteration(wl, strict=a.strict, ran1_seed=box_seed(rank, R, r)))
     torch.cuda.synchronize()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
     main = torch.cuda.current_stream()
@@ -285,11 +300,7 @@ def gpu_arm(a):
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    tot_ms = sum(round_ms)
-    t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    tmax_ms = float(t.item())
+    tmax_ms = max_over_ranks(sum(round_ms), dist, "cuda")
     moves = its[0].moves_per_step
     value = world * R * a.steps * moves / (tmax_ms / 1000.0)
 
@@ -328,11 +339,8 @@ def gpu_arm(a):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    e2e_ms = sum(run_round(e2e_body) for _ in range(a.steps))
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * R * a.steps * moves / (float(t.item()) / 1000.0)
+    e2e_ms = max_over_ranks(sum(run_round(e2e_body) for _ in range(a.steps)), dist, "cuda")
+    e2e_value = world * R * a.steps * moves / (e2e_ms / 1000.0)
 
     boxes.close()
     stage_ms = {k: v / a.steps for k, v in stage_tot.items()}
