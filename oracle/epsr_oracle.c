@@ -428,6 +428,66 @@ int oracle_fmolec1(const oracle_sys *S, const oracle_cells *C, const float *eint
 }
 
 /* ------------------------------------------------------------------ molfit sweep */
+/* ------------------------------------------------------------------ press */
+/* press ato_manipulation_rev4.py:3903-4062 without three-body terms or coordination
+ * constraints: for every molecule im but the last (0..nmol-2) and every stored partner
+ * jm > im, in store order, the energy (ergold, float32, ia outer / ja inner) and the virial
+ * term (ergnew: float32 add of prwt, then double add of prpot, stored back as float32) of
+ * all atom pairs with iz <= npt1 (:3960-4040); then sumc += ergold in float32 and presst +=
+ * ergnew in double over (im, jref) (:4041-4044).  Returns sumc; *presst_out = presst. */
+float oracle_press(const oracle_sys *S, const oracle_store *E, int32_t npt1, double *presst_out) {
+    const int M = E->nnbrefmax;
+    float sumc = 0.0f;
+    double presst = 0.0;
+    for (int im = 0; im < S->nmol - 1; ++im) {
+        const float xc1 = S->xadd[im], yc1 = S->yadd[im], zc1 = S->zadd[im];
+        const int a0 = S->naf[im], a1 = a0 + S->nato[im];
+        const int nn = E->nergpairm[im];
+        for (int s = 0; s < nn; ++s) {
+            const int jm = E->molergpair[(size_t)im * M + s];
+            float ergold = 0.0f, ergnew = 0.0f;
+            if (jm > im) {
+                const int b0 = S->naf[jm], b1 = b0 + S->nato[jm];
+                for (int ia = a0; ia < a1; ++ia) {
+                    const int it = S->itype[ia];
+                    const float x1 = S->xa[ia] + xc1, y1 = S->ya[ia] + yc1, z1 = S->za[ia] + zc1;
+                    for (int ja = b0; ja < b1; ++ja) {
+                        const float xc2 = S->xadd[jm], yc2 = S->yadd[jm], zc2 = S->zadd[jm];
+                        const int icref = S->npairref[it * S->ntype + S->itype[ja]];
+                        const float x2 = S->xa[ja] + xc2, y2 = S->ya[ja] + yc2, z2 = S->za[ja] + zc2;
+                        float xdif = x2 - x1, ydif = y2 - y1, zdif = z2 - z1;
+                        minimagec(S, &xdif, &ydif, &zdif);
+                        float xcdif = xc2 - xc1, ycdif = yc2 - yc1, zcdif = zc2 - zc1;
+                        minimagec(S, &xcdif, &ycdif, &zcdif);
+                        const float dsq = xdif * xdif + ydif * ydif + zdif * zdif;
+                        const float dtest = sqrtf(dsq);
+                        const float rat = dtest / S->stepcl;
+                        const int32_t iz = f_ifix(rat) + 2;
+                        if (iz <= npt1) {
+                            const size_t b = (size_t)icref * (size_t)S->ld;
+                            const float dtdif = dtest - S->xstar[iz];
+                            const int32_t ipz = iz;
+                            float prfac;
+                            if (dtest > 0.0f) prfac = (xcdif * xdif + ycdif * ydif + zcdif * zdif) / dtest;
+                            else prfac = 0.0f;
+                            const float enpot = S->ecoul[b + iz] + S->ecoul1[b + iz] * dtdif;
+                            const double prpot = (double)(0.5f * (S->ecoul1[b + ipz] + S->ecoul1[b + ipz - 1]) * prfac);
+                            const float enwt = S->xavs[b + iz] + S->xavs1[b + iz] * dtdif;
+                            const float prwt = 0.5f * (S->xavs1[b + ipz] + S->xavs1[b + ipz - 1]) * prfac;
+                            ergold = ergold + enwt + enpot;
+                            ergnew = (float)((double)(ergnew + prwt) + prpot);
+                        }
+                    }
+                }
+            }
+            sumc = sumc + ergold;
+            presst = presst + (double)ergnew;
+        }
+    }
+    *presst_out = presst;
+    return sumc;
+}
+
 typedef struct {
     float simt, rejrate, stepr, stepm, trstepmax, trstepmin;
     int32_t ireset;

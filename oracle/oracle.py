@@ -206,6 +206,36 @@ def en_mole_pair(box, im, jm):
     return f32(lib().oracle_en_mole_pair(C.byref(h.c), int(im), int(jm)))
 
 
+# ----------------------------------------------------------------------------- press
+def press_scalars(nmol, sumc, presst, simt, volume):
+    """The closing lines of press (ato_manipulation_rev4.py:4051-4056): energy per molecule
+    (float32) and pressure in kbar (double arithmetic, stored as float32)."""
+    energy = f32(f32(sumc) / f32(nmol))
+    pressc = f32(((float(f32(nmol) * f32(simt)) - float(presst) / 3.0) * 100.0)
+                 / float(f32(6.0222) * f32(volume)))
+    return energy, pressc
+
+
+def press_file_terms(nmol, energf, pressf, wsum, volume):
+    """Per-file rescaling at the end of press (:4057-4060), float32."""
+    ef = f32(energf) / (f32(nmol) * f32(wsum))
+    pf = ((-f32(pressf) / f32(3.0)) * f32(100.0)) / (f32(6.0222) * f32(volume) * f32(wsum))
+    return f32(ef), f32(pf)
+
+
+def press(box, st, npt1, simt, volume):
+    """press on the stored pairs (no three-body or coordination terms): returns sumc,
+    presst and the energy and pressure the reference returns."""
+    h = SysHandle(box)
+    E = store_c(st)
+    L = lib()
+    L.oracle_press.restype = C.c_float
+    d = np.zeros(1, np.float64)
+    sumc = f32(L.oracle_press(C.byref(h.c), C.byref(E), int(npt1), ptr(d)))
+    energy, pressc = press_scalars(box.nmol, sumc, d[0], simt, volume)
+    return dict(sumc=sumc, presst=float(d[0]), energy=energy, pressc=pressc)
+
+
 # ----------------------------------------------------------------------------- molfit
 def trsteps(natomr):
     out = np.zeros(2, f32)
