@@ -4,7 +4,7 @@
 One step = one EPSR iteration of the hot path on configuration C2 (200 DMSO + 400 water,
 3200 atoms, 21 pair types) for each of R independent boxes on the GPU (``--replicas``,
 default 16): cell list, fmolec1, 5 molfit cycles (3000 whole-molecule moves), atogen over
-all 5,118,400 atom pairs, gensq, fit_expansion for three datasets, stog.  Each box has its
+all 5,118,400 atom pairs, gensq, press, fit_expansion for three datasets, stog.  Each box has its
 own ran1 seed, CUDA stream and host thread; a box's chain is sequential (Metropolis, one
 ran1 stream), so independent boxes are how one GPU is filled.  ``value`` = molecule moves
 of all boxes per second of device time, inputs resident in HBM; ``single_box`` reports one
@@ -120,7 +120,7 @@ def reference_arm(a):
         "warmup": warmup, "ms_per_step": 1000.0 * slowest / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded C2 mixture box)",
         "config": {"workload": a.config, "moves_per_step_per_replica": moves, "replicas": nproc,
-                   "stages": "cells+fmolec1+5 molfit+atogen+gensq+fit_expansion (3 data sets)+stog"},
+                   "stages": "cells+fmolec1+5 molfit+atogen+gensq+press+fit_expansion (3 data sets)+stog"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
                          "sample": f"{nproc} independent replicas x {steps} iterations (+{warmup} warm-up) of the "
                                    f"single-threaded C restatement, one process per core; host {model}"},
@@ -355,7 +355,7 @@ def gpu_arm(a):
             "config": {"workload": a.config, "nmol": it.box.nmol, "natom": it.box.natom, "npairs": it.box.npairs,
                        "moves_per_step_per_box": moves, "boxes_per_gpu": R,
                        "pair_updates_per_step_per_box": it.pair_updates,
-                       "stages": "cells+fmolec1+5 molfit+atogen+gensq+fit_expansion (3 data sets)+stog",
+                       "stages": "cells+fmolec1+5 molfit+atogen+gensq+press+fit_expansion (3 data sets)+stog",
                        "step": f"one EPSR iteration of each of the {R} independent boxes on this GPU, each box on "
                                "its own stream and host thread",
                        "l2": "flushed between timed steps (256 MB write)", "sums": "strict" if a.strict else "fast",
@@ -390,6 +390,7 @@ def kernel_launches(it, wl):
     #                      epilogue, sequential retry (launched always, runs only if flagged)
     n += 8            # atogen: positions, ran1, select, intra, molecule map, origin atoms, inter, norm
     n += 1            # gensq
+    n += 3            # press: positions, pair terms, sums
     n += 1            # fit_expansion: one cluster launch for every data set
     n += 2            # stog: lorch + stog
     return n

@@ -72,6 +72,8 @@ _SIGS = {
     "epsr_atogen_scratch_bytes": (I64, [I32, I32, I32, I32]),
     "epsr_atogen_last_pair_updates": (I64, []),
     "epsr_atogen_noalloc": (C.c_int, [C.POINTER(Box), I32, F32, F32, P, P, P, P, P, I32, P, P, P, I32, P, P]),
+    "epsr_press": (C.c_int, [C.POINTER(Box), C.POINTER(Store), I32, P, I64, I32, P, P]),
+    "epsr_press_scratch_bytes": (I64, [I32, I32]),
     "epsr_gensq": (C.c_int, [I32, I32, I32, P, I32, P, I64, I64, P, P, P, P, P]),
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),
     "epsr_stog_scratch_bytes": (I64, [I32, I32]),

@@ -28,6 +28,15 @@ def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def press_scalars(nmol, sumc, presst, simt, volume):
+    """The closing lines of press (ato_manipulation_rev4.py:4051-4056): the energy per
+    molecule in float32 and the pressure in kbar (double arithmetic, stored as float32)."""
+    energy = f32(f32(sumc) / f32(nmol))
+    pressc = f32(((float(f32(nmol) * f32(simt)) - float(presst) / 3.0) * 100.0)
+                 / float(f32(6.0222) * f32(volume)))
+    return energy, pressc
+
+
 def table_cutoff(*tabs) -> int:
     """Last grid index at which any table entry is nonzero (bitwise, so -0 counts)."""
     last = 1
@@ -284,6 +293,19 @@ class DeviceBox:
                                    _ptr(self.a_potex), _ptr(counts), _ptr(scr), scr.numel(), _stream()))
         self.last_pair_updates = int(self.lib.epsr_atogen_last_pair_updates())
         return int(ngr[0])
+
+    # ------------------------------------------------------------------ press
+    def press(self, npt1=None, strict=True):
+        """press ato_manipulation_rev4.py:3903-4062 on the current store: returns (sumc,
+        presst) -- the float32 energy sum and the double virial sum over the stored pairs."""
+        b = self.host
+        npt1 = b.npt1 if npt1 is None else npt1
+        nb = self.lib.epsr_press_scratch_bytes(b.nmol, self.nnbrefmax)
+        scr = self.scratch("press", nb)
+        sums = np.zeros(2, np.float64)
+        check(self.lib.epsr_press(C.byref(self.cbox), C.byref(self.store), int(npt1), _ptr(scr), scr.numel(),
+                                  1 if strict else 0, sums.ctypes.data_as(C.c_void_p), _stream()))
+        return f32(sums[0]), float(sums[1])
 
     def download_wav(self):
         torch.cuda.synchronize()

@@ -15,6 +15,7 @@ reference's argument lists and return values:
 * ``gensq`` (programs/epsr_standalone_rev3.py:4731)
 * ``stog`` (library/ato_manipulation_rev4.py:4067)
 * ``fit_expansion`` (programs/epsr_standalone_rev3.py:4806)
+* ``press`` (library/ato_manipulation_rev4.py:3903)
 
 ``install()`` assigns them onto the given modules (the reference's own rerouting
 mechanism, trace.py:94-125) and keeps the originals.
@@ -48,13 +49,14 @@ from .box import BoxArrays, Ran1State, trsteps
 
 f32 = np.float32
 ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit", "atogen", "stog", "gensq", "fit_expansion",
-            "en_change", "en_mole_pair")
+            "press", "en_change", "en_mole_pair")
 # en_change / en_mole_pair are per-molecule calls: rerouting them makes every host caller
 # (including host fallbacks) launch one kernel per call, so they are installed only on request.
-DEFAULT_ROUTINES = ROUTINES[:7]
+DEFAULT_ROUTINES = ROUTINES[:8]
 # module that owns each routine in the reference
 OWNER = {"initialise_cellneighbourlist": "cellneighbourlist", "fmolec1": "ato_manipulation_rev4",
-         "atogen": "ato_manipulation_rev4", "stog": "ato_manipulation_rev4", "molfit": "molfit",
+         "atogen": "ato_manipulation_rev4", "stog": "ato_manipulation_rev4", "press": "ato_manipulation_rev4",
+         "molfit": "molfit",
          "en_change": "molfit", "en_mole_pair": "molfit", "gensq": "program", "fit_expansion": "program"}
 
 
@@ -450,6 +452,29 @@ class PairPath:
         pp.potex[1:b.npairs + 1] = potex
         pp.potexmax[1:b.npairs + 1] = 0.0
         return n
+
+    def press(self, energy, pressc, energf, pressf, energabs, energthreeb, prthreebout):
+        """ato_manipulation_rev4.py:3903-4062: energy and pressure of the stored pairs on the
+        device; abs_energy_ep and the per-file rescaling of energf/pressf (in place) on the
+        host as the reference; returns (energy, pressc, energabs, energthreeb, prthreebout)."""
+        if self._outside_path():
+            return self._host("press", energy, pressc, energf, pressf, energabs, energthreeb, prthreebout)
+        from .device import press_scalars
+        c = self.c
+        cc = c.clustercom
+        b = self._sync_in()
+        self._check_cells()
+        self._store_in()
+        energabs = self.mods["ato_manipulation_rev4"].abs_energy_ep()
+        sumc, presst = self.d.press(int(c.epsr16.npt1), strict=self.strict)
+        energy, pressc = press_scalars(b.nmol, sumc, presst, c.molecom.simt, cc.volume)
+        nmol = f32(b.nmol)
+        vol = f32(cc.volume)
+        wsum = c.potential_par.wsum
+        for i in range(1, int(c.epsr16.nfile) + 1):
+            energf[i] = f32(energf[i]) / (nmol * f32(wsum[i]))
+            pressf[i] = ((-f32(pressf[i]) / f32(3.0)) * f32(100.0)) / (f32(6.0222) * vol * f32(wsum[i]))
+        return energy, pressc, energabs, f32(0.0), prthreebout
 
     def gensq(self, nq, q, sofq, wav):
         """epsr_standalone_rev3.py:4731-4802: fills sofq(2,nq,npairs) in place."""

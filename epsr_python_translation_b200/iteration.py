@@ -16,10 +16,10 @@ import torch
 from . import transforms
 from .box import BoxArrays, Ran1State, trsteps
 from .configs import Workload
-from .device import DeviceBox
+from .device import DeviceBox, press_scalars
 
 f32 = np.float32
-STAGES = ("cells", "fmolec1", "molfit", "atogen", "gensq", "fit_expansion", "stog")
+STAGES = ("cells", "fmolec1", "molfit", "atogen", "gensq", "press", "fit_expansion", "stog")
 
 
 class EpsrIteration:
@@ -53,6 +53,7 @@ class EpsrIteration:
         self.events = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                        for k in STAGES}
         self.moves_per_step = wl.ntimes * b.nmol
+        self.volume = f32(float(wl.system.L) ** 3)          # box volume (A^3) for press
         self.pair_updates = 0
         self.fit_trials = 0
 
@@ -85,6 +86,10 @@ class EpsrIteration:
         # per data set: the difference between the data and the weighted simulated S(Q)
         dt = -(self.data - torch.matmul(self.weights, inter))  # (ndata, nq+1)
         self._mark("gensq", True)
+        self._mark("press")
+        sumc, presst = d.press(b.npt1, strict=self.strict)
+        self.energy, self.pressc = press_scalars(b.nmol, sumc, presst, b.simt, self.volume)
+        self._mark("press", True)
         self._mark("fit_expansion")
         res = transforms.fit_expansion_batch(dt, self.expr, self.pwtold, self.stepp, 1, nq, 1, wl.nterms, 1000, 10,
                                              self.ran1, strict=self.strict, scratch=self._fit_scratch)

@@ -206,6 +206,19 @@ int epsr_atogen_noalloc(const epsr_box_t *box, int32_t npt1, float sizefactor, f
                         int32_t natomr, int32_t *ngrsamples_io, int32_t *ran1, float *wav, int32_t ldw,
                         float *potex, void *stream);
 
+/* ------------------------------------------------------------------ press */
+/* press ato_manipulation_rev4.py:3903-4062 over the stored pairs (no three-body terms, no
+ * coordination constraints): for every molecule but the last and every stored partner
+ * jm > im, the energy and virial of all atom pairs with bin iz <= npt1, summed in store
+ * order.  sums_host[2] = {sumc (a float32 value), presst}; the caller forms the energy
+ * sumc/nmol and the pressure as the reference's closing lines do (:4051-4056).  strict=1
+ * sums sumc in float32 and presst in double sequentially (bit-identical); strict=0 sums
+ * both in double in parallel.  scratch: device bytes from epsr_press_scratch_bytes.
+ * Synchronous. */
+int64_t epsr_press_scratch_bytes(int32_t nmol, int32_t nnbrefmax);
+int epsr_press(const epsr_box_t *box, const epsr_store_t *store, int32_t npt1, void *scratch,
+               int64_t scratch_bytes, int32_t strict, double *sums_host, void *stream);
+
 /* ------------------------------------------------------------------ gensq / stog */
 /* gensq epsr_standalone_rev3.py:4731-4802.  fq(j,i) = foqols[j*fq_sj + i*fq_si] (j = r
  * index 1..npt1, i = Q index 1..nq).  sofq out [2*npairs*(nq+1)]: sofq(1,i,ic) at

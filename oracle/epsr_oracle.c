@@ -434,11 +434,13 @@ int oracle_fmolec1(const oracle_sys *S, const oracle_cells *C, const float *eint
  * jm > im, in store order, the energy (ergold, float32, ia outer / ja inner) and the virial
  * term (ergnew: float32 add of prwt, then double add of prpot, stored back as float32) of
  * all atom pairs with iz <= npt1 (:3960-4040); then sumc += ergold in float32 and presst +=
- * ergnew in double over (im, jref) (:4041-4044).  Returns sumc; *presst_out = presst. */
-float oracle_press(const oracle_sys *S, const oracle_store *E, int32_t npt1, double *presst_out) {
+ * ergnew in double over (im, jref) (:4041-4044).  Returns sumc; out2[0] = presst and, for
+ * checking sums made in another order, out2[1] = the double sum of the same float32 ergold
+ * values. */
+float oracle_press(const oracle_sys *S, const oracle_store *E, int32_t npt1, double *out2) {
     const int M = E->nnbrefmax;
     float sumc = 0.0f;
-    double presst = 0.0;
+    double presst = 0.0, sum64 = 0.0;
     for (int im = 0; im < S->nmol - 1; ++im) {
         const float xc1 = S->xadd[im], yc1 = S->yadd[im], zc1 = S->zadd[im];
         const int a0 = S->naf[im], a1 = a0 + S->nato[im];
@@ -482,9 +484,11 @@ float oracle_press(const oracle_sys *S, const oracle_store *E, int32_t npt1, dou
             }
             sumc = sumc + ergold;
             presst = presst + (double)ergnew;
+            sum64 += (double)ergold;
         }
     }
-    *presst_out = presst;
+    out2[0] = presst;
+    out2[1] = sum64;
     return sumc;
 }
 

@@ -225,15 +225,16 @@ def press_file_terms(nmol, energf, pressf, wsum, volume):
 
 def press(box, st, npt1, simt, volume):
     """press on the stored pairs (no three-body or coordination terms): returns sumc,
-    presst and the energy and pressure the reference returns."""
+    presst, the double sum of the same float32 pair energies (sum64) and the energy and
+    pressure the reference returns."""
     h = SysHandle(box)
     E = store_c(st)
     L = lib()
     L.oracle_press.restype = C.c_float
-    d = np.zeros(1, np.float64)
+    d = np.zeros(2, np.float64)
     sumc = f32(L.oracle_press(C.byref(h.c), C.byref(E), int(npt1), ptr(d)))
     energy, pressc = press_scalars(box.nmol, sumc, d[0], simt, volume)
-    return dict(sumc=sumc, presst=float(d[0]), energy=energy, pressc=pressc)
+    return dict(sumc=sumc, presst=float(d[0]), sum64=float(d[1]), energy=energy, pressc=pressc)
 
 
 # ----------------------------------------------------------------------------- molfit

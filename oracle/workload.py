@@ -64,6 +64,9 @@ class CpuIteration:
         sofq = oracle.gensq(nq, b.npt1, wav, self.rows, wl.ycoh[: b.npt + 1], b.n2extr, np.ones(b.ntype, f32))
         t["gensq"] = time.perf_counter() - t0
         t0 = time.perf_counter()
+        self.press = oracle.press(b, st, b.npt1, b.simt, f32(wl.system.L ** 3))
+        t["press"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
         inter = sofq[1]
         for k in range(wl.data.shape[0]):
             fit = (wl.weights[k].astype(np.float32) @ inter).astype(f32)

@@ -52,13 +52,14 @@ def common_from_golden(z):
     mc.xa[1:], mc.ya[1:], mc.za[1:] = z["sys_xa"], z["sys_ya"], z["sys_za"]
     e16 = NS(cellst=f32(z["sys_cellst"]), npt=npt, npt1=int(z["sys_npt1"]), npt2=int(z["sys_npt2"]),
              nptmin=int(z["sys_nptmin"]), nptmax=int(z["sys_nptmax"]), rejrate=f32(z["in_rejrate"]), x=fa(mpz),
-             xstar=fa(mpz), ycoh=fa(mpz), foqols=None)
+             xstar=fa(mpz), ycoh=fa(mpz), foqols=None, nfile=0)
     e16.x[: npt + 1] = z["sys_x"]
     e16.xstar[: npt + 1] = z["sys_xstar"]
     if "gs_foqols" in z.files:          # ycoh stays zero until the gensq stage, as when the golden was made
         e16.foqols = np.asfortranarray(z["gs_foqols"])
     pp = NS(xavs=fa(mpz, npairs), xavs1=fa(mpz, npairs), ecoul=fa(mpz, npairs), ecoul1=fa(mpz, npairs),
-            irefpcof=fa(npairs, dtype=np.int32), rminex=fa(npairs), potex=fa(npairs), potexmax=fa(npairs))
+            irefpcof=fa(npairs, dtype=np.int32), rminex=fa(npairs), potex=fa(npairs), potexmax=fa(npairs),
+            wsum=fa(4))
     for p in range(npairs):
         pp.xavs[: npt + 1, p + 1] = z["sys_xavs"][p]
         pp.xavs1[: npt + 1, p + 1] = z["sys_xavs1"][p]
@@ -98,7 +99,9 @@ def routine_modules(z, calls):
         return f32(eintra[im - 1]), sv, sa, sd
     return {"cellneighbourlist": NS(initialise_cellneighbourlist=rec("host:initialise_cellneighbourlist")),
             "ato_manipulation_rev4": NS(fmolec1=rec("host:fmolec1", (0, 0, f32(0), f32(0), f32(0), f32(0))),
-                                        atogen=rec("host:atogen", 0), stog=rec("host:stog")),
+                                        atogen=rec("host:atogen", 0), stog=rec("host:stog"),
+                                        press=rec("host:press", (f32(0), f32(0), f32(0), f32(0), f32(0))),
+                                        abs_energy_ep=lambda: f32(0.0)),
             "molfit": NS(molfit=rec("host:molfit", (f32(0), f32(0), 1)), en_change=rec("host:en_change"),
                          en_mole_pair=rec("host:en_mole_pair"), en_mole_intra=en_mole_intra),
             "program": NS(gensq=rec("host:gensq"), fit_expansion=rec("host:fit_expansion"))}

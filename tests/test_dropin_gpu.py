@@ -159,3 +159,25 @@ def test_dropin_sees_host_changes_between_calls():
     c.cellneighbourlist.molcellno[1] += 1
     with pytest.raises(dropin.EpsrGpuError):
         mods["molfit"].molfit(f32(0), f32(0), 1, 100, 5, 0)
+
+
+@pytest.mark.parametrize("case", ["c1_water", "mix_small", "silica"])
+def test_dropin_press_matches_reference(case):
+    """press through the installed routine, right after fmolec1 (the state the press golden
+    was made in): energy, pressure and the per-file rescaling bit for bit."""
+    from tests.test_press_oracle import press_case
+    p = press_case(case)
+    z, c, mods, path, calls = _setup(case, True)
+    _cells_and_store(z, c, mods)
+    c.clustercom.volume = p[case + "_volume"]
+    c.epsr16.nfile = 1
+    c.potential_par.wsum[1] = f32(1.0)
+    energf, pressf = fake_common.fa(4), fake_common.fa(4)
+    energf[1], pressf[1] = p[case + "_energf_in"], p[case + "_pressf_in"]
+    energy, pressc, energabs, energthreeb, prthree = mods["ato_manipulation_rev4"].press(
+        f32(0), f32(0), energf, pressf, f32(0), f32(0), f32(0))
+    assert_bits_equal(energy, p[case + "_energy"], "energy")
+    assert_bits_equal(pressc, p[case + "_pressc"], "pressc")
+    assert_bits_equal(energf[1], p[case + "_energf"], "energf")
+    assert_bits_equal(pressf[1], p[case + "_pressf"], "pressf")
+    assert energabs == 0 and energthreeb == 0 and calls == []
