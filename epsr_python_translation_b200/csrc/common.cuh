@@ -169,27 +169,20 @@ __device__ __forceinline__ uint32_t r1_mulmod(uint32_t a, uint32_t b) {
 }
 
 // 32 steps of the shuffle when no value of the batch can be zero: idl is this lane's Park-
-// Miller value of the batch (step lane+1), iv this lane's table entry, iy warp-uniform.  The
-// chain only needs the slot index of the next step (the top 5 bits of the value read), so
-// each lane also keeps its entry's top bits and one shuffle per step carries the chain; the
-// value itself is fetched beside it.  Returns the value of step `lane`; updates iv and iy.
+// Miller value of the batch (step lane+1), iv this lane's table entry, iy warp-uniform.  A
+// step is two shuffles: the value in slot j (whose top 5 bits give the next slot: the only
+// dependence from step to step) and the step's Park-Miller value from the lane that holds
+// it, which the lane owning slot j keeps.  Returns the value of step `lane`; updates iv, iy.
 __device__ __forceinline__ int32_t ran1_chain32(int32_t idl, int32_t &iv, int32_t &iy) {
     const int lane = threadIdx.x & 31;
-    int t5 = iv >> 26;
-    const int c5 = idl >> 26;
-    int j = iy >> 26;
     int32_t y = iy, mine = 0;
 #pragma unroll
     for (int s = 0; s < 32; ++s) {
-        const int jn = __shfl_sync(0xffffffffu, t5, j);
-        const int32_t out = __shfl_sync(0xffffffffu, iv, j);
+        const int j = y >> 26;   // iy / NDIV, NDIV = 2^26
         const int32_t id = __shfl_sync(0xffffffffu, idl, s);
-        const int c = __shfl_sync(0xffffffffu, c5, s);
+        y = __shfl_sync(0xffffffffu, iv, j);
         iv = (lane == j) ? id : iv;
-        t5 = (lane == j) ? c : t5;
-        mine = (lane == s) ? out : mine;
-        y = out;
-        j = jn;
+        mine = (lane == s) ? y : mine;
     }
     iy = y;
     return mine;

@@ -7,8 +7,9 @@
 // stream, as the reference's successive calls do.
 //
 // Layout.  The basis rows are split over the CTAs of a cluster; each keeps its rows in
-// shared memory for the whole launch, four terms to a 16-byte word, and evaluates one row
-// per thread per trial (expand :4924, the sequential clamped sum of a row).  Every partial
+// shared memory for the whole launch, four terms to a 16-byte word, and evaluates two rows
+// per thread per trial, their two sequential sums interleaved (expand :4924, the sequential
+// clamped sum of a row).  Every partial
 // sum of a row is bounded by the row's L1 norm times the largest |coefficient|; when that
 // bound stays below the clamp level (e^25) the clamp cannot act and the plain sequential
 // sum is the reference's value, otherwise the row is summed with the clamp.  The CTAs
@@ -44,7 +45,8 @@ constexpr int FX_GEN_WARP = 15;                 // the stream warp
 constexpr int FX_NBAR = 480;                    // threads of the worker barrier (warps 0-14)
 constexpr int FX_SLOTS = 384;                   // row / coefficient slots (12 warps, schedulers 0-2)
 constexpr int FX_RING = 2048;                   // ran1 values held per worker CTA (power of two)
-constexpr int FX_CK = 128;                      // batch checkpoints (power of two)
+constexpr int FX_CK = 128;                      // generator checkpoints (power of two)
+constexpr int FX_CKE = 8;                       // batches between checkpoints (power of two)
 constexpr int FX_CKW = 36;                      // ints per checkpoint: idum, iy, iv[32], pad[2]
 constexpr unsigned long long FX_WAIT_NS = 2000000000ull;  // a wait gives up after 2 s
 
@@ -129,7 +131,6 @@ __device__ __forceinline__ unsigned long long now_ns() {
 }
 
 struct FxShared {                 // statically sized control block (one per CTA)
-    long long prod;               // ring values present (written by the generator warp)
     long long cons;               // lowest stream index the workers may still read
     int done;                     // set by the workers when the fit is over
     int abort, stop;
@@ -141,6 +142,9 @@ struct FxShared {                 // statically sized control block (one per CTA
 };
 
 __host__ __device__ inline int fx_ntq(int nt) { return (nt + 3) / 4; }
+// floats per exchange buffer: every row of the cluster, padded to whole 16-byte words so the
+// second buffer starts 16-byte aligned (it is read four rows at a time)
+__host__ __device__ inline int fx_gstride(int nw, int rpc) { return (nw * rpc + 3) & ~3; }
 
 size_t fx_smem_bytes(int nt, int rpc, int nw) {
     const int ntq = fx_ntq(nt);
@@ -151,9 +155,10 @@ size_t fx_smem_bytes(int nt, int rpc, int nw) {
     b = (b + 15) & ~(size_t)15;
     b += sizeof(float) * (4 + 4 * (size_t)ntq);         // wt (wt + 1 16-byte aligned)
     b += sizeof(float) * (size_t)(nt + 1);              // wtold
-    b += sizeof(float) * FX_RING;                       // ring
     b = (b + 15) & ~(size_t)15;
-    b += sizeof(float) * 2 * (size_t)nw * rpc;          // gat[2][nw*rpc]
+    b += sizeof(unsigned long long) * FX_RING;          // ring
+    b = (b + 15) & ~(size_t)15;
+    b += sizeof(float) * 2 * (size_t)fx_gstride(nw, rpc);   // gat[2][gstride]
     b = (b + 15) & ~(size_t)15;
     b += sizeof(double) * 2 * (size_t)nw;               // parts[2][nw]
     b += sizeof(uint64_t) * 2;                          // exchange mbarriers
@@ -176,10 +181,13 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
     size_t off = ((size_t)((unsigned char *)(e1 + rpc) - fx_raw) + 15) & ~(size_t)15;
     float *wt = (float *)(fx_raw + off) + 3;            // wt[0..4*ntq]; wt + 1 is 16-byte aligned
     float *wtold = wt + 1 + 4 * ntq;                    // [nt+1]
-    float *ring = wtold + (nt + 1);                     // [FX_RING]
+    off = ((size_t)((unsigned char *)(wtold + nt + 1) - fx_raw) + 15) & ~(size_t)15;
+    // [FX_RING] stream values, each with its position + 1 in the high word, so a reader knows
+    // from the one 8-byte load whether the value it wants is there yet
+    unsigned long long *ring = (unsigned long long *)(fx_raw + off);
     off = ((size_t)((unsigned char *)(ring + FX_RING) - fx_raw) + 15) & ~(size_t)15;
-    float *gat = (float *)(fx_raw + off);               // [2][nw*rpc] residuals by global row
-    off = ((off + sizeof(float) * 2 * (size_t)nw * rpc) + 15) & ~(size_t)15;
+    float *gat = (float *)(fx_raw + off);               // [2][gstride] residuals by global row
+    off = ((off + sizeof(float) * 2 * (size_t)fx_gstride(nw, rpc)) + 15) & ~(size_t)15;
     double *parts = (double *)(fx_raw + off);           // [2][nw]
     uint64_t *xbar = (uint64_t *)(parts + 2 * nw);      // [2]
     long long *ckpos = (long long *)(xbar + 2);         // [FX_CK]
@@ -205,9 +213,9 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
         e1[r] = a;
     }
     for (int i = tid; i < FX_CK; i += blockDim.x) ckpos[i] = -1;
+    for (int i = tid; i < FX_RING; i += blockDim.x) ring[i] = 0ull;   // no position yet
     if (tid < FX_WARPS) S.wmx[tid] = 0.0f;
     if (tid == 0) {
-        S.prod = 0;
         S.cons = 0;
         S.done = 0;
         S.abort = 0;
@@ -225,48 +233,45 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
         g.load(F.ran1);
         long long pos = 0, nb = 0;
         unsigned long long t0 = 0;
-        // every control decision of the loop is lane 0's, broadcast to the warp, so the warp
-        // stays converged for the shuffles of the batch
+        // the warp is converged at the top of every pass, so each control word is read by one
+        // warp-wide load and every lane takes the same branch
         while (true) {
-            int stopnow = 0, full = 0;
-            if (lane == 0) {
-                stopnow = vs->done;
-                if (!stopnow && pos + 32 > vs->cons + FX_RING) {   // ring full
-                    full = 1;
+            __syncwarp();
+            if (vs->done) break;
+            if (pos + 32 > vs->cons + FX_RING) {   // ring full: wait for the workers (bounded)
+                int give_up = 0;
+                if (lane == 0) {
                     const unsigned long long t = now_ns();
                     if (t0 == 0) t0 = t;
-                    else if (t - t0 > FX_WAIT_NS) {
+                    else if (t - t0 > FX_WAIT_NS || vs->abort) {
                         atomicExch(F.status, 1);
                         vs->abort = 1;
-                        stopnow = 1;
+                        give_up = 1;
                     }
                 }
-            }
-            stopnow = __shfl_sync(0xffffffffu, stopnow, 0);
-            full = __shfl_sync(0xffffffffu, full, 0);
-            if (stopnow) break;
-            if (full) {
+                if (__shfl_sync(0xffffffffu, give_up, 0)) break;
                 __nanosleep(64);
                 continue;
             }
             t0 = 0;
-            const int slot = (int)(nb & (FX_CK - 1));
-            ck[slot * FX_CKW + 2 + lane] = g.iv;
-            if (lane == 0) {
-                ck[slot * FX_CKW + 0] = g.idum;
-                ck[slot * FX_CKW + 1] = g.iy;
-                ckpos[slot] = pos;
+            if ((nb & (FX_CKE - 1)) == 0) {   // the state before this batch, every FX_CKE batches
+                const int slot = (int)((nb / FX_CKE) & (FX_CK - 1));
+                ck[slot * FX_CKW + 2 + lane] = g.iv;
+                if (lane == 0) {
+                    ck[slot * FX_CKW + 0] = g.idum;
+                    ck[slot * FX_CKW + 1] = g.iy;
+                    ckpos[slot] = pos;
+                }
             }
             ++nb;
             int32_t mine;
             const int cnt = g.next(32, mine, g_tab);
-            if (lane < cnt) ring[(pos + lane) & (FX_RING - 1)] = ran1_out(mine);
-            pos += cnt;
-            __syncwarp();
-            if (lane == 0) {
-                __threadfence_block();
-                vs->prod = pos;
+            if (lane < cnt) {
+                const long long q = pos + lane;
+                ring[q & (FX_RING - 1)] =
+                    ((unsigned long long)(uint32_t)(q + 1) << 32) | (unsigned long long)__float_as_uint(ran1_out(mine));
             }
+            pos += cnt;
         }
         __syncwarp();
         __syncthreads();   // meets the workers after they set done (barrier 0, all 512 threads)
@@ -280,70 +285,155 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
     // row / coefficient slot of this thread: the warps of schedulers 0-2, -1 otherwise
     const int slot = (wid & 3) != 3 ? (wid - (wid >> 2)) * 32 + lane : -1;
     const int swarp = (wid & 3) != 3 ? wid - (wid >> 2) : -1;   // slot warp 0..11
+    const int ic = (slot >= 0 && slot < K) ? F.ncfirst + slot : -1;   // coefficient this thread perturbs
 
-    // wait until stream value `idx` is in the ring (bounded; gives up at once after an abort)
-    auto need = [&](long long idx) {
-        if (vs->prod > idx) {
-            __threadfence_block();
-            return;
-        }
-        const unsigned long long t0 = now_ns();
-        while (vs->prod <= idx) {
-            if (vs->abort) return;
-            if (now_ns() - t0 > FX_WAIT_NS) {
-                atomicExch(F.status, 1);
-                vs->abort = 1;
-                return;
+    // stream value idx, once the generator has written it (a bounded wait, given up at once
+    // after an abort)
+    auto get = [&](long long idx) -> float {
+        const volatile unsigned long long *e = ring + (idx & (FX_RING - 1));
+        const uint32_t want = (uint32_t)(idx + 1);
+        unsigned long long v = *e;
+        if ((uint32_t)(v >> 32) != want) {
+            const unsigned long long t0 = now_ns();
+            while (true) {
+                __nanosleep(32);
+                v = *e;
+                if ((uint32_t)(v >> 32) == want || vs->abort) break;
+                if (now_ns() - t0 > FX_WAIT_NS) {
+                    atomicExch(F.status, 1);
+                    vs->abort = 1;
+                    break;
+                }
             }
-            __nanosleep(32);
         }
-        __threadfence_block();
+        return __uint_as_float((uint32_t)v);
     };
-    auto val = [&](long long idx) { return ring[idx & (FX_RING - 1)]; };
+
+    // state of the trial loop that thread 0's Metropolis decision reads (the same in every
+    // worker thread)
+    long long cursor = 0;
+    float chisqold = 0.0f, accept = 0.0f;
+    int icount = 0;
+
+    // the largest |wt| over the perturbed terms, for the clamp bound (thread 0; a barrier
+    // follows before any row reads it)
+    auto wmax_all = [&]() {
+        float b = 0.0f;
+        for (int m = F.ncfirst; m <= nt; ++m) b = fmaxf(b, fabsf(wt[m]));
+        vs->wmx[0] = b;
+        for (int k = 1; k < FX_WARPS; ++k) vs->wmx[k] = 0.0f;
+    };
+    // the Metropolis test (:4871-4880) and the smoothing (:4882-4893) of trial chi^2 cn,
+    // taken by thread 0 and published in the control block
+    auto decide = [&](float cn) {
+        const float exponent = __fdiv_rn(__fsub_rn(cn, chisqold), accept);
+        float test;
+        int draw = 0;
+        if (exponent > 0.0f && exponent <= 20.0f) {
+            test = __fsub_rn(exp_r(-exponent), get(cursor));
+            draw = 1;
+        } else if (exponent > 20.0f) {
+            test = -1.0f;
+        } else {
+            test = 1.0f;
+        }
+        const int acc = test >= 0.0f;
+        int sm = 0;
+        if (acc && icount + 1 == F.nfreq) {
+            sm = 1;        // smoop(ncfirst, nterms, 1, wt)
+            const int n1 = F.ncfirst, n2 = nt;
+            if (!(n2 - 2 < n1)) {
+                float sm_ = 0.0f, sn = wt[n1];
+                float sum1 = __fmul_rn(0.25f, __fadd_rn(sm_, sn));
+                for (int i = n1; i <= n2; ++i) {
+                    sm_ = sn;
+                    sn = (i + 1) <= n2 ? wt[i + 1] : 0.0f;
+                    const float sum2 = __fmul_rn(0.25f, __fadd_rn(sm_, sn));
+                    wt[i] = __fadd_rn(sum1, sum2);
+                    sum1 = sum2;
+                }
+            }
+            wmax_all();
+        }
+        vs->accept = acc;
+        vs->smooth = sm;
+        vs->draw = draw;
+        vs->stop = vs->abort;
+        vs->cons = cursor + draw;
+    };
 
     int xb = 0;                                         // exchange buffer
     uint32_t xph = 0u;                                  // mbarrier phase parity, bit b for buffer b
-    // chi^2 of the current wt over rows nmin..npt, the same value in every CTA.  strict_sum:
-    // the reference's sequential float sum over rows; else a double sum.  yout, if given,
-    // receives this CTA's row sums.  Two worker barriers; the result is returned to all.
-    auto chisq = [&](bool strict_sum, float *yout) -> float {
-        float *gb = gat + (size_t)xb * nw * rpc;
+    // chi^2 of the current wt over rows nmin..npt, the same value in every CTA, returned to
+    // all workers; with `trial`, thread 0 also takes the Metropolis decision on it before the
+    // result is published.  Rows, a worker barrier, then warp 0 alone: it forms this CTA's
+    // part, lane d pushes it into CTA d and arrives on CTA d's mbarrier (the nw pushes in
+    // parallel), lane 0 waits for every CTA's part and thread 0 forms the total in a fixed
+    // order; a second barrier publishes it.  strict_sum: the reference's sequential float sum
+    // over rows of the residuals that every row thread pushed to every CTA; else a double sum.
+    // yout, if given, receives this CTA's row sums.
+    auto chisq = [&](bool strict_sum, float *yout, bool trial) -> float {
+        float *gb = gat + (size_t)xb * fx_gstride(nw, rpc);
         double mypart = 0.0;
         if (slot >= 0) {
             float wmax = vs->wfix;
-            for (int k = 0; k < FX_WARPS; ++k) wmax = fmaxf(wmax, vs->wmx[k]);
-            for (int r = slot; r < nrow; r += FX_SLOTS) {
-                const int i = row0 + r;
-                const float4 *e4 = ex4 + r;
-                float sum = 0.0f;
+            const float *wm = (const float *)S.wmx;   // complete since the last barrier
+#pragma unroll
+            for (int k = 0; k < FX_WARPS; ++k) wmax = fmaxf(wmax, wm[k]);
+            // rows slot and slot + hr: two independent chains of adds per thread sharing
+            // each coefficient load
+            const int hr = (nrow + 1) >> 1;
+            if (slot < hr) {
+                const int ra = slot, rb = slot + hr;
+                const bool hb = rb < nrow;
                 // every partial sum is at most e1[r] * max|wt| (times 1 + 2^-20 for rounding)
-                if (__fmul_ru(__fmul_ru(e1[r], wmax), 1.001f) < summax) {
+                const bool fa = __fmul_ru(__fmul_ru(e1[ra], wmax), 1.001f) < summax;
+                const bool fb = !hb || __fmul_ru(__fmul_ru(e1[rb], wmax), 1.001f) < summax;
+                float sa = 0.0f, sb = 0.0f;
+                if (fa && fb) {
+                    const float4 *pa = ex4 + ra, *pb = ex4 + (hb ? rb : ra);
                     const float4 *w4 = (const float4 *)(wt + 1);
 #pragma unroll 2
                     for (int q = 0; q < ntq; ++q) {
-                        const float4 e = e4[(size_t)q * rpc];
                         const float4 c = w4[q];
-                        sum = __fadd_rn(sum, __fmul_rn(e.x, c.x));
-                        sum = __fadd_rn(sum, __fmul_rn(e.y, c.y));
-                        sum = __fadd_rn(sum, __fmul_rn(e.z, c.z));
-                        sum = __fadd_rn(sum, __fmul_rn(e.w, c.w));
+                        const float4 x = pa[q * rpc], y = pb[q * rpc];
+                        sa = __fadd_rn(sa, __fmul_rn(x.x, c.x));
+                        sb = __fadd_rn(sb, __fmul_rn(y.x, c.x));
+                        sa = __fadd_rn(sa, __fmul_rn(x.y, c.y));
+                        sb = __fadd_rn(sb, __fmul_rn(y.y, c.y));
+                        sa = __fadd_rn(sa, __fmul_rn(x.z, c.z));
+                        sb = __fadd_rn(sb, __fmul_rn(y.z, c.z));
+                        sa = __fadd_rn(sa, __fmul_rn(x.w, c.w));
+                        sb = __fadd_rn(sb, __fmul_rn(y.w, c.w));
                     }
-                } else {  // the reference's clamped sum (expand :4924)
-                    for (int m = 0; m < nt; ++m) {
-                        const float *ee = (const float *)(e4 + (size_t)(m >> 2) * rpc);
-                        sum = __fadd_rn(sum, __fmul_rn(ee[m & 3], wt[1 + m]));
-                        if (fabsf(sum) > summax) sum = fsign(summax, sum);
+                } else {  // a row the clamp may reach: the reference's clamped sum (expand :4924)
+                    auto clamped = [&](int r) {
+                        const float4 *e4 = ex4 + r;
+                        float sum = 0.0f;
+                        for (int m = 0; m < nt; ++m) {
+                            const float *ee = (const float *)(e4 + (m >> 2) * rpc);
+                            sum = __fadd_rn(sum, __fmul_rn(ee[m & 3], wt[1 + m]));
+                            if (fabsf(sum) > summax) sum = fsign(summax, sum);
+                        }
+                        return sum;
+                    };
+                    sa = clamped(ra);
+                    if (hb) sb = clamped(rb);
+                }
+                auto finish = [&](int r, float sum) {
+                    const int i = row0 + r;
+                    const float term = __fsub_rn(yr[r], sum);
+                    const float q2 = __fmul_rn(term, term);
+                    if (yout) yout[i] = sum;
+                    if (strict_sum) {
+                        const uint32_t la = smem_addr(gb + (rank * rpc + r));
+                        for (int d = 0; d < nw; ++d) st_cl_f32(map_rank(la, (uint32_t)d), q2);
+                    } else if (i >= F.nmin) {
+                        mypart += (double)q2;
                     }
-                }
-                const float term = __fsub_rn(yr[r], sum);
-                const float q2 = __fmul_rn(term, term);
-                if (yout) yout[i] = sum;
-                if (strict_sum) {
-                    const uint32_t la = smem_addr(gb + (rank * rpc + r));
-                    for (int d = 0; d < nw; ++d) st_cl_f32(map_rank(la, (uint32_t)d), q2);
-                } else if (i >= F.nmin) {
-                    mypart += (double)q2;
-                }
+                };
+                finish(ra, sa);
+                if (hb) finish(rb, sb);
             }
         }
         __syncwarp();
@@ -354,64 +444,57 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
             if (lane == 0) vs->red[wid] = mypart;
         }
         block_sync();
-        if (tid == 0) {
-            const uint32_t pa = smem_addr(parts + xb * nw + rank);
+        if (wid == 0) {
             const uint32_t ba = smem_addr(&xbar[xb]);
-            if (!strict_sum) {
-                double t = 0.0;
-                for (int k = 0; k < FX_GEN_WARP; ++k) t += vs->red[k];
-                for (int d = 0; d < nw; ++d) st_cl_f64(map_rank(pa, (uint32_t)d), t);
+            double t = 0.0;
+            if (!strict_sum) t = warp_sum_d(lane < FX_GEN_WARP ? vs->red[lane] : 0.0);
+            if (lane < nw) {
+                if (!strict_sum) st_cl_f64(map_rank(smem_addr(parts + xb * nw + rank), (uint32_t)lane), t);
+                mbar_arrive_cluster(map_rank(ba, (uint32_t)lane));
             }
-            for (int d = 0; d < nw; ++d) mbar_arrive_cluster(map_rank(ba, (uint32_t)d));
-            const uint32_t par = (xph >> xb) & 1u;
-            if (!mbar_test(ba, par)) {
-                const unsigned long long t0 = now_ns();
-                while (!mbar_test(ba, par)) {
-                    if (vs->abort || now_ns() - t0 > FX_WAIT_NS) {
-                        atomicExch(F.status, 1);
-                        vs->abort = 1;
-                        break;
+            if (lane == 0) {
+                const uint32_t par = (xph >> xb) & 1u;
+                if (!mbar_test(ba, par)) {
+                    const unsigned long long t0 = now_ns();
+                    while (!mbar_test(ba, par)) {
+                        if (vs->abort || now_ns() - t0 > FX_WAIT_NS) {
+                            atomicExch(F.status, 1);
+                            vs->abort = 1;
+                            break;
+                        }
                     }
                 }
-            }
-            float v;
-            if (strict_sum) {
-                const int a = F.nmin - 1, b = F.npt;    // 0-based rows a..b-1
-                float c = 0.0f;
-                int i = a;
-                for (; i < b && (i & 3); ++i) c = __fadd_rn(c, gb[i]);
-                const float4 *g4 = (const float4 *)gb;
-                for (; i + 3 < b; i += 4) {
-                    const float4 u = g4[i >> 2];
-                    c = __fadd_rn(c, u.x);
-                    c = __fadd_rn(c, u.y);
-                    c = __fadd_rn(c, u.z);
-                    c = __fadd_rn(c, u.w);
+                float v;
+                if (strict_sum) {
+                    const int a = F.nmin - 1, b = F.npt;    // 0-based rows a..b-1
+                    float c = 0.0f;
+                    int i = a;
+                    for (; i < b && (i & 3); ++i) c = __fadd_rn(c, gb[i]);
+                    const float4 *g4 = (const float4 *)gb;
+                    for (; i + 3 < b; i += 4) {
+                        const float4 u = g4[i >> 2];
+                        c = __fadd_rn(c, u.x);
+                        c = __fadd_rn(c, u.y);
+                        c = __fadd_rn(c, u.z);
+                        c = __fadd_rn(c, u.w);
+                    }
+                    for (; i < b; ++i) c = __fadd_rn(c, gb[i]);
+                    v = c;
+                } else {
+                    double u = 0.0;
+                    for (int q = 0; q < nw; ++q) u += parts[xb * nw + q];
+                    v = (float)u;
                 }
-                for (; i < b; ++i) c = __fadd_rn(c, gb[i]);
-                v = c;
-            } else {
-                double t = 0.0;
-                for (int q = 0; q < nw; ++q) t += parts[xb * nw + q];
-                v = (float)t;
+                vs->val = v;
+                if (trial) decide(v);
             }
-            vs->val = v;
         }
         xph ^= 1u << xb;
         xb ^= 1;
         block_sync();
         return vs->val;
     };
-    // the largest |wt| over the perturbed terms, for the clamp bound (thread 0; a barrier
-    // follows before any row reads it)
-    auto wmax_all = [&]() {
-        float b = 0.0f;
-        for (int m = F.ncfirst; m <= nt; ++m) b = fmaxf(b, fabsf(wt[m]));
-        vs->wmx[0] = b;
-        for (int k = 1; k < FX_WARPS; ++k) vs->wmx[k] = 0.0f;
-    };
 
-    long long cursor = 0;
     const float acceptr = 0.05f;
     const int npoints = F.npt - F.nmin + 1;
     for (int pi = 0; pi < F.nprob; ++pi) {
@@ -443,28 +526,25 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
         }
         if (stepr < __fmul_rn(1.0e-6f, wtmax)) stepr = __fmul_rn(2.0e-6f, wtmax);
         if (F.nits > 0 && !vs->stop) {
-            int icount = 0;
-            chisqnew = chisq(F.strict != 0, nullptr);
-            float chisqold = chisqnew;
+            icount = 0;
+            chisqnew = chisq(F.strict != 0, nullptr, false);
+            chisqold = chisqnew;
             float chisqtest = -1.0f;
             int itry = 0;
             bool stop = false;
             while (!stop && (itry < 10 || (itry < 150 && chisqtest < 1.0e-4f))) {
                 ++itry;
-                const float accept = __fdiv_rn(__fmul_rn(acceptr, chisqold), (float)npoints);
+                accept = __fdiv_rn(__fmul_rn(acceptr, chisqold), (float)npoints);
                 rejrat = 0.0f;
                 const float chisqstart = __fdiv_rn(chisqold, (float)npoints);
                 for (int st = 1; st <= 100; ++st) {
                     ++trials;
-                    // perturb coefficients ncfirst..nterms with the next K values (:4856-4861);
-                    // one lane per warp waits for the warp's last value
+                    // perturb coefficients ncfirst..nterms with the next K values (:4856-4861),
+                    // each thread waiting for its own value
                     if (swarp >= 0 && swarp * 32 < K) {
-                        if (lane == 0) need(cursor + min(K, swarp * 32 + 32) - 1);
-                        __syncwarp();
-                        const int ic = F.ncfirst + slot;
                         float a = 0.0f;
-                        if (ic <= nt) {
-                            const float du = __fsub_rn(__fmul_rn(2.0f, val(cursor + slot)), 1.0f);
+                        if (ic > 0) {
+                            const float du = __fsub_rn(__fmul_rn(2.0f, get(cursor + slot)), 1.0f);
                             float v;
                             if (fabsf(wtold[ic]) < 1.0f) v = __fadd_rn(wtold[ic], __fmul_rn(stepr, du));
                             else v = __fmul_rn(wtold[ic], __fadd_rn(1.0f, __fmul_rn(stepr, du)));
@@ -476,45 +556,8 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
                     }
                     cursor += K;
                     block_sync();
-                    const float cn = chisq(F.strict != 0, nullptr);
-                    if (tid == 0) {   // the Metropolis test (:4871-4880) and the smoothing (:4882-4893)
-                        const float exponent = __fdiv_rn(__fsub_rn(cn, chisqold), accept);
-                        float test;
-                        int draw = 0;
-                        if (exponent > 0.0f && exponent <= 20.0f) {
-                            need(cursor);
-                            test = __fsub_rn(exp_r(-exponent), val(cursor));
-                            draw = 1;
-                        } else if (exponent > 20.0f) {
-                            test = -1.0f;
-                        } else {
-                            test = 1.0f;
-                        }
-                        const int acc = test >= 0.0f;
-                        int sm = 0;
-                        if (acc && icount + 1 == F.nfreq) {
-                            sm = 1;        // smoop(ncfirst, nterms, 1, wt)
-                            const int n1 = F.ncfirst, n2 = nt;
-                            if (!(n2 - 2 < n1)) {
-                                float sm_ = 0.0f, sn = wt[n1];
-                                float sum1 = __fmul_rn(0.25f, __fadd_rn(sm_, sn));
-                                for (int i = n1; i <= n2; ++i) {
-                                    sm_ = sn;
-                                    sn = (i + 1) <= n2 ? wt[i + 1] : 0.0f;
-                                    const float sum2 = __fmul_rn(0.25f, __fadd_rn(sm_, sn));
-                                    wt[i] = __fadd_rn(sum1, sum2);
-                                    sum1 = sum2;
-                                }
-                            }
-                            wmax_all();
-                        }
-                        vs->accept = acc;
-                        vs->smooth = sm;
-                        vs->draw = draw;
-                        vs->stop = vs->abort;
-                        vs->cons = cursor + draw;
-                    }
-                    block_sync();
+                    // chi^2 of the trial and thread 0's decision on it (Metropolis, smoothing)
+                    const float cn = chisq(F.strict != 0, nullptr, true);
                     const int acc = vs->accept, sm = vs->smooth;
                     stop = vs->stop != 0;
                     cursor += vs->draw;
@@ -523,14 +566,15 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
                         ++icount;
                         if (sm) {
                             icount = 0;
-                            chisqnew = chisq(F.strict != 0, nullptr);
+                            chisqnew = chisq(F.strict != 0, nullptr, false);
                         }
                         chisqold = chisqnew;
-                        for (int k = 1 + tid; k <= nt; k += FX_NBAR) wtold[k] = wt[k];
+                        // each thread keeps the coefficient it perturbs (terms below ncfirst
+                        // never change); the next trial's perturbation reads only its own
+                        if (ic > 0) wtold[ic] = wt[ic];
                     } else {
                         rejrat = __fadd_rn(rejrat, 1.0f);
                     }
-                    block_sync();
                     if (stop) break;
                 }
                 rejrat = __fdiv_rn(rejrat, 100.0f);
@@ -540,13 +584,14 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
                 const float rejfac = rejrat > 0.0f ? __fdiv_rn(0.75f, rejrat) : 2.0f;
                 stepr = __fmul_rn(stepr, rejfac);
             }
+            block_sync();   // every thread's own wtold update is in
             for (int k = 1 + tid; k <= nt; k += FX_NBAR) wt[k] = wtold[k];
             block_sync();
             if (tid == 0) wmax_all();
             block_sync();
         }
         // final fit over rows 1..npt, chi^2 from nmin (:4908-4914), in the reference's order
-        chisqnew = chisq(true, yout);
+        chisqnew = chisq(true, yout, false);
         if (rank == 0) {
             float *wt_g = F.wt_g + (size_t)pi * (nt + 1);
             float *wtold_o = F.wtold_g + (size_t)pi * (nt + 1);
@@ -595,13 +640,13 @@ using namespace epsr;
 
 static inline size_t al256f(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Smallest cluster whose CTAs hold their rows in shared memory with one row per slot
+// Smallest cluster whose CTAs hold their rows in shared memory with two rows per slot
 // thread (at most 8 CTAs).
 static int fx_workers(int npt, int nterms, int *rpc_out) {
     const size_t budget = 220 * 1024;
     for (int c = 1; c <= 8; ++c) {
         const int rpc = (npt + c - 1) / c;
-        if (rpc <= FX_SLOTS && fx_smem_bytes(nterms, rpc, c) <= budget) {
+        if (rpc <= 2 * FX_SLOTS && fx_smem_bytes(nterms, rpc, c) <= budget) {
             *rpc_out = rpc;
             return c;
         }

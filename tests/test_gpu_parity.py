@@ -411,3 +411,35 @@ def test_fit_expansion_c2_size_strict_matches_oracle(seed):
         assert_bits_equal(res[k], ref[k], k)
     assert res["trials"] == ref["trials"]
     assert np.array_equal(t.cpu().numpy(), rst.as_array())
+
+
+@pytest.mark.parametrize("npt,scale", [(1000, 1.0), (1700, 1.0), (600, 3.0e12)])
+def test_fit_expansion_cluster_shapes_strict_match_oracle(npt, scale):
+    """The fit's two row layouts against the C oracle, strict sums, bit for bit: 1000 Q rows
+    (the C3 S(Q)) hold their basis in registers on a six-CTA cluster; 1700 rows exceed the
+    register layout (192 rows per CTA, 8 CTAs) and keep the rows in shared memory; a basis
+    scaled so that row sums reach the clamp level (e^25) takes the clamped sum in registers."""
+    from epsr_python_translation_b200 import configs, transforms
+    nt = 116
+    q = configs.qgrid(npt, 0.05)
+    expr = configs.ep_basis(q, nt)
+    if scale != 1.0:
+        expr = (expr * f32(scale)).astype(f32)
+    rng = np.random.default_rng(npt)
+    yin = np.zeros(npt + 1, f32)
+    yin[1:] = (rng.standard_normal(npt) * 0.05 * scale).astype(f32)
+    wtold = np.zeros(nt + 1, f32)
+    wtold[1:] = (rng.standard_normal(nt) * 0.01).astype(f32)
+    st0 = Ran1State(idum=-5)
+    t = torch.from_numpy(st0.as_array()).cuda()
+    res = transforms.fit_expansion(yin, expr, wtold, f32(0.01), 1, npt, 1, nt, 1000, 10, t, strict=True)
+    ref, rst = oracle.fit_expansion(yin, expr, wtold.copy(), f32(0.01), 1, npt, 1, nt, 1000, 10, st0)
+    if scale != 1.0:
+        assert np.any(np.abs(ref["yout"][1:]) >= np.float32(np.exp(25.0)) * 0.999)   # the clamp acted
+    assert_bits_equal(res["wt"].cpu().numpy()[1:], ref["wt"][1:], "wt")
+    assert_bits_equal(res["wtold"].cpu().numpy()[1:], ref["wtold"][1:], "wtold")
+    assert_bits_equal(res["yout"].cpu().numpy()[1:], ref["yout"][1:], "yout")
+    for k in ("stepr", "acceptr", "rejrat", "chisq"):
+        assert_bits_equal(res[k], ref[k], k)
+    assert res["trials"] == ref["trials"]
+    assert np.array_equal(t.cpu().numpy(), rst.as_array())
