@@ -415,10 +415,10 @@ def test_fit_expansion_c2_size_strict_matches_oracle(seed):
 
 @pytest.mark.parametrize("npt,scale", [(1000, 1.0), (1700, 1.0), (600, 3.0e12)])
 def test_fit_expansion_cluster_shapes_strict_match_oracle(npt, scale):
-    """The fit's two row layouts against the C oracle, strict sums, bit for bit: 1000 Q rows
-    (the C3 S(Q)) hold their basis in registers on a six-CTA cluster; 1700 rows exceed the
-    register layout (192 rows per CTA, 8 CTAs) and keep the rows in shared memory; a basis
-    scaled so that row sums reach the clamp level (e^25) takes the clamped sum in registers."""
+    """Cluster shapes of the fit against the C oracle, strict sums, bit for bit: 1000 Q rows
+    (the C3 S(Q)) on three CTAs, 1700 rows on four (odd row counts per CTA, so the exchange
+    buffers need their padding), and a basis scaled so that row sums reach the clamp level
+    (e^25), which takes the clamped sum for those rows."""
     from epsr_python_translation_b200 import configs, transforms
     nt = 116
     q = configs.qgrid(npt, 0.05)
