@@ -7,9 +7,9 @@
 // stream, as the reference's successive calls do.
 //
 // Layout.  The basis rows are split over the CTAs of a cluster; each keeps its rows in
-// shared memory for the whole launch, four terms to a 16-byte word, and evaluates two rows
-// per thread per trial, their two sequential sums interleaved (expand :4924, the sequential
-// clamped sum of a row).  Every partial
+// shared memory for the whole launch, four terms to a 16-byte word, except the first 64
+// terms of each row, which its thread holds in registers; a thread evaluates its row per
+// trial (expand :4924, the sequential clamped sum of a row).  Every partial
 // sum of a row is bounded by the row's L1 norm times the largest |coefficient|; when that
 // bound stays below the clamp level (e^25) the clamp cannot act and the plain sequential
 // sum is the reference's value, otherwise the row is summed with the clamp.  The CTAs
@@ -44,6 +44,7 @@ constexpr int FX_WARPS = FX_THREADS / 32;
 constexpr int FX_GEN_WARP = 15;                 // the stream warp
 constexpr int FX_NBAR = 480;                    // threads of the worker barrier (warps 0-14)
 constexpr int FX_SLOTS = 384;                   // row / coefficient slots (12 warps, schedulers 0-2)
+constexpr int FX_RQ = 16;                       // leading quads of a row held in its thread's registers
 constexpr int FX_RING = 2048;                   // ran1 values held per worker CTA (power of two)
 constexpr int FX_CK = 128;                      // generator checkpoints (power of two)
 constexpr int FX_CKE = 8;                       // batches between checkpoints (power of two)
@@ -142,6 +143,8 @@ struct FxShared {                 // statically sized control block (one per CTA
 };
 
 __host__ __device__ inline int fx_ntq(int nt) { return (nt + 3) / 4; }
+// quads of a row kept in shared memory (those after the first FX_RQ)
+__host__ __device__ inline int fx_nsq(int nt) { return fx_ntq(nt) > FX_RQ ? fx_ntq(nt) - FX_RQ : 0; }
 // floats per exchange buffer: every row of the cluster, padded to whole 16-byte words so the
 // second buffer starts 16-byte aligned (it is read four rows at a time)
 __host__ __device__ inline int fx_gstride(int nw, int rpc) { return (nw * rpc + 3) & ~3; }
@@ -149,7 +152,7 @@ __host__ __device__ inline int fx_gstride(int nw, int rpc) { return (nw * rpc + 
 size_t fx_smem_bytes(int nt, int rpc, int nw) {
     const int ntq = fx_ntq(nt);
     size_t b = 0;
-    b += 16 * (size_t)ntq * rpc;                        // ex4
+    b += 16 * (size_t)fx_nsq(nt) * rpc;                 // ex4
     b += sizeof(float) * (size_t)rpc;                   // yr
     b += sizeof(float) * (size_t)rpc;                   // e1 (row L1 norms)
     b = (b + 15) & ~(size_t)15;
@@ -175,8 +178,10 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
     __shared__ FxShared S;
     __shared__ int32_t g_tab[34];
     const int nt = F.nterms, rpc = F.rpc, ntq = fx_ntq(nt);
-    float4 *ex4 = (float4 *)fx_raw;                     // [ntq*rpc]: ex4[q*rpc + r] = terms 4q..4q+3 of row r
-    float *yr = (float *)(ex4 + (size_t)ntq * rpc);     // [rpc]
+    const int nsq = fx_nsq(nt);
+    // [nsq*rpc]: ex4[q*rpc + r] = terms 4(FX_RQ+q)..4(FX_RQ+q)+3 of row r
+    float4 *ex4 = (float4 *)fx_raw;
+    float *yr = (float *)(ex4 + (size_t)nsq * rpc);     // [rpc]
     float *e1 = yr + rpc;                               // [rpc] sum over terms of |basis value|
     size_t off = ((size_t)((unsigned char *)(e1 + rpc) - fx_raw) + 15) & ~(size_t)15;
     float *wt = (float *)(fx_raw + off) + 3;            // wt[0..4*ntq]; wt + 1 is 16-byte aligned
@@ -197,11 +202,11 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
     volatile FxShared *vs = &S;
     const int row0 = 1 + rank * rpc;                    // first (1-based) row of this CTA
     const int nrow = max(0, min(rpc, F.npt - row0 + 1));
-    for (int idx = tid; idx < ntq * rpc; idx += blockDim.x) {
+    for (int idx = tid; idx < nsq * rpc; idx += blockDim.x) {
         const int q = idx / rpc, r = idx - q * rpc;
         float e[4];
         for (int j = 0; j < 4; ++j) {
-            const int m = 4 * q + j;                    // 0-based term
+            const int m = 4 * (FX_RQ + q) + j;          // 0-based term
             e[j] = (r < nrow && m < nt) ? F.expr[1 + (size_t)(row0 - 1 + r) * nt + m] : 0.0f;
         }
         ex4[idx] = make_float4(e[0], e[1], e[2], e[3]);
@@ -286,6 +291,19 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
     const int slot = (wid & 3) != 3 ? (wid - (wid >> 2)) * 32 + lane : -1;
     const int swarp = (wid & 3) != 3 ? wid - (wid >> 2) : -1;   // slot warp 0..11
     const int ic = (slot >= 0 && slot < K) ? F.ncfirst + slot : -1;   // coefficient this thread perturbs
+    // the first FX_RQ quads of this thread's row (row `slot`), in registers for the launch
+    float4 rq[FX_RQ];
+#pragma unroll
+    for (int k = 0; k < FX_RQ; ++k) {
+        float e[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (slot >= 0 && slot < nrow) {
+            for (int j = 0; j < 4; ++j) {
+                const int m = 4 * k + j;
+                if (m < nt) e[j] = F.expr[1 + (size_t)(row0 - 1 + slot) * nt + m];
+            }
+        }
+        rq[k] = make_float4(e[0], e[1], e[2], e[3]);
+    }
 
     // stream value idx, once the generator has written it (a bounded wait, given up at once
     // after an abort)
@@ -380,60 +398,61 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
             const float *wm = (const float *)S.wmx;   // complete since the last barrier
 #pragma unroll
             for (int k = 0; k < FX_WARPS; ++k) wmax = fmaxf(wmax, wm[k]);
-            // rows slot and slot + hr: two independent chains of adds per thread sharing
-            // each coefficient load
-            const int hr = (nrow + 1) >> 1;
-            if (slot < hr) {
-                const int ra = slot, rb = slot + hr;
-                const bool hb = rb < nrow;
+            if (slot < nrow) {
+                const int r = slot;
+                float sum = 0.0f;
+                const float4 *w4 = (const float4 *)(wt + 1);
+                const float4 *e4 = ex4 + r;
                 // every partial sum is at most e1[r] * max|wt| (times 1 + 2^-20 for rounding)
-                const bool fa = __fmul_ru(__fmul_ru(e1[ra], wmax), 1.001f) < summax;
-                const bool fb = !hb || __fmul_ru(__fmul_ru(e1[rb], wmax), 1.001f) < summax;
-                float sa = 0.0f, sb = 0.0f;
-                if (fa && fb) {
-                    const float4 *pa = ex4 + ra, *pb = ex4 + (hb ? rb : ra);
-                    const float4 *w4 = (const float4 *)(wt + 1);
-#pragma unroll 2
-                    for (int q = 0; q < ntq; ++q) {
-                        const float4 c = w4[q];
-                        const float4 x = pa[q * rpc], y = pb[q * rpc];
-                        sa = __fadd_rn(sa, __fmul_rn(x.x, c.x));
-                        sb = __fadd_rn(sb, __fmul_rn(y.x, c.x));
-                        sa = __fadd_rn(sa, __fmul_rn(x.y, c.y));
-                        sb = __fadd_rn(sb, __fmul_rn(y.y, c.y));
-                        sa = __fadd_rn(sa, __fmul_rn(x.z, c.z));
-                        sb = __fadd_rn(sb, __fmul_rn(y.z, c.z));
-                        sa = __fadd_rn(sa, __fmul_rn(x.w, c.w));
-                        sb = __fadd_rn(sb, __fmul_rn(y.w, c.w));
-                    }
-                } else {  // a row the clamp may reach: the reference's clamped sum (expand :4924)
-                    auto clamped = [&](int r) {
-                        const float4 *e4 = ex4 + r;
-                        float sum = 0.0f;
-                        for (int m = 0; m < nt; ++m) {
-                            const float *ee = (const float *)(e4 + (m >> 2) * rpc);
-                            sum = __fadd_rn(sum, __fmul_rn(ee[m & 3], wt[1 + m]));
-                            if (fabsf(sum) > summax) sum = fsign(summax, sum);
+                if (__fmul_ru(__fmul_ru(e1[r], wmax), 1.001f) < summax) {
+#pragma unroll
+                    for (int k = 0; k < FX_RQ; ++k) {
+                        if (k < ntq) {
+                            const float4 c = w4[k];
+                            sum = __fadd_rn(sum, __fmul_rn(rq[k].x, c.x));
+                            sum = __fadd_rn(sum, __fmul_rn(rq[k].y, c.y));
+                            sum = __fadd_rn(sum, __fmul_rn(rq[k].z, c.z));
+                            sum = __fadd_rn(sum, __fmul_rn(rq[k].w, c.w));
                         }
-                        return sum;
-                    };
-                    sa = clamped(ra);
-                    if (hb) sb = clamped(rb);
-                }
-                auto finish = [&](int r, float sum) {
-                    const int i = row0 + r;
-                    const float term = __fsub_rn(yr[r], sum);
-                    const float q2 = __fmul_rn(term, term);
-                    if (yout) yout[i] = sum;
-                    if (strict_sum) {
-                        const uint32_t la = smem_addr(gb + (rank * rpc + r));
-                        for (int d = 0; d < nw; ++d) st_cl_f32(map_rank(la, (uint32_t)d), q2);
-                    } else if (i >= F.nmin) {
-                        mypart += (double)q2;
                     }
-                };
-                finish(ra, sa);
-                if (hb) finish(rb, sb);
+#pragma unroll 2
+                    for (int q = 0; q < nsq; ++q) {
+                        const float4 c = w4[FX_RQ + q];
+                        const float4 e = e4[q * rpc];
+                        sum = __fadd_rn(sum, __fmul_rn(e.x, c.x));
+                        sum = __fadd_rn(sum, __fmul_rn(e.y, c.y));
+                        sum = __fadd_rn(sum, __fmul_rn(e.z, c.z));
+                        sum = __fadd_rn(sum, __fmul_rn(e.w, c.w));
+                    }
+                } else {  // the reference's clamped sum (expand :4924)
+#pragma unroll
+                    for (int k = 0; k < FX_RQ; ++k) {
+                        const float ev[4] = {rq[k].x, rq[k].y, rq[k].z, rq[k].w};
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int m = 4 * k + j;
+                            if (m < nt) {
+                                sum = __fadd_rn(sum, __fmul_rn(ev[j], wt[1 + m]));
+                                if (fabsf(sum) > summax) sum = fsign(summax, sum);
+                            }
+                        }
+                    }
+                    for (int m = 4 * FX_RQ; m < nt; ++m) {
+                        const float *ee = (const float *)(e4 + ((m >> 2) - FX_RQ) * rpc);
+                        sum = __fadd_rn(sum, __fmul_rn(ee[m & 3], wt[1 + m]));
+                        if (fabsf(sum) > summax) sum = fsign(summax, sum);
+                    }
+                }
+                const int i = row0 + r;
+                const float term = __fsub_rn(yr[r], sum);
+                const float q2 = __fmul_rn(term, term);
+                if (yout) yout[i] = sum;
+                if (strict_sum) {
+                    const uint32_t la = smem_addr(gb + (rank * rpc + r));
+                    for (int d = 0; d < nw; ++d) st_cl_f32(map_rank(la, (uint32_t)d), q2);
+                } else if (i >= F.nmin) {
+                    mypart += (double)q2;
+                }
             }
         }
         __syncwarp();
@@ -640,13 +659,12 @@ using namespace epsr;
 
 static inline size_t al256f(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Smallest cluster whose CTAs hold their rows in shared memory with two rows per slot
-// thread (at most 8 CTAs).
+// Smallest cluster whose CTAs hold their rows with one row per slot thread (at most 8 CTAs).
 static int fx_workers(int npt, int nterms, int *rpc_out) {
     const size_t budget = 220 * 1024;
     for (int c = 1; c <= 8; ++c) {
         const int rpc = (npt + c - 1) / c;
-        if (rpc <= 2 * FX_SLOTS && fx_smem_bytes(nterms, rpc, c) <= budget) {
+        if (rpc <= FX_SLOTS && fx_smem_bytes(nterms, rpc, c) <= budget) {
             *rpc_out = rpc;
             return c;
         }
