@@ -81,17 +81,18 @@ struct Tables {
 
 // en_atom_inter_scale molfit.py:1251-1279 (scalefac = 1).  d is the minimum-image distance.
 // Beyond izcut every table entry is +0, so the reference's value there is exactly +0.
+// Branch-free: the table is read at iz clamped into 2..izcut and the result replaced by +0
+// outside that range, so the loads of consecutive pairs can be in flight together.
 __device__ __forceinline__ float pair_energy_d(const Tables &T, float d, int icref) {
     float rat = __fdiv_rn(d, T.stepcl);
     int iz = ifix(rat) + 2;
-    float sume = 0.0f;
-    if (iz >= 2 && iz <= T.izcut) {  // iz < 2 only for a non-finite distance
-        float4 t = __ldg(T.tab + (size_t)icref * T.ld + iz);
-        float dt = __fsub_rn(d, __ldg(T.xstar + iz));
-        sume = __fadd_rn(t.x, __fmul_rn(t.y, dt));
-        sume = __fadd_rn(__fadd_rn(sume, t.z), __fmul_rn(t.w, dt));
-    }
-    return sume;
+    const bool in = iz >= 2 && iz <= T.izcut;  // iz < 2 only for a non-finite distance
+    const int izc = min(max(iz, 2), T.izcut);
+    const float4 t = __ldg(T.tab + (size_t)icref * T.ld + izc);
+    const float dt = __fsub_rn(d, __ldg(T.xstar + izc));
+    float sume = __fadd_rn(t.x, __fmul_rn(t.y, dt));
+    sume = __fadd_rn(__fadd_rn(sume, t.z), __fmul_rn(t.w, dt));
+    return in ? sume : 0.0f;
 }
 
 __device__ __forceinline__ float pair_energy(const Lattice &L, const Tables &T, float4 p1, float4 p2,

@@ -30,8 +30,8 @@ namespace epsr {
 
 constexpr int SP_W = 32;        // near window of the resolver (moves)
 constexpr int SP_RING = 64;     // far-sum ring (moves)
-constexpr int SP_PB = 16;       // partner atoms held in registers
 constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
+constexpr int SP_ET = 256;      // threads of a move's energy CTA (its stored partners)
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
 
 struct SpecDev {
@@ -238,37 +238,25 @@ __global__ void spec_propose_kernel(SpecDev S) {
 }
 
 // ----------------------------------------------------------------- energies
-// E(a, b): a's atoms in shared memory (sa), b's absolute positions in global memory.  The
-// sum runs ia outer, ja inner as en_change (molfit.py:851-882); b is held in registers.
+// E(a, b): a's atoms in shared memory (sa), b's absolute positions in global memory (read
+// through the L1 cache for every atom of a, which keeps registers -- and so resident warps --
+// free for latency hiding).  The sum runs ia outer, ja inner as en_change (molfit.py:851-882).
 __device__ __forceinline__ float mol_energy(const Lattice &L, const Tables &T, const float4 *sa, int na,
                                             const float4 *__restrict__ pb, int nb, const int *spr, int ntype) {
     float sume = 0.0f;
-    if (nb <= SP_PB) {
-        float4 b[SP_PB];
-#pragma unroll
-        for (int j = 0; j < SP_PB; ++j)
-            if (j < nb) b[j] = pb[j];
-        for (int ia = 0; ia < na; ++ia) {
-            const float4 p1 = sa[ia];
-            const int *row = spr + __float_as_int(p1.w) * ntype;
-#pragma unroll
-            for (int j = 0; j < SP_PB; ++j)
-                if (j < nb) sume = __fadd_rn(sume, pair_energy(L, T, p1, b[j], row[__float_as_int(b[j].w)]));
-        }
-    } else {
-        for (int ia = 0; ia < na; ++ia) {
-            const float4 p1 = sa[ia];
-            const int *row = spr + __float_as_int(p1.w) * ntype;
-            for (int j = 0; j < nb; ++j) {
-                const float4 p2 = pb[j];
-                sume = __fadd_rn(sume, pair_energy(L, T, p1, p2, row[__float_as_int(p2.w)]));
-            }
+    for (int ia = 0; ia < na; ++ia) {
+        const float4 p1 = sa[ia];
+        const int *row = spr + __float_as_int(p1.w) * ntype;
+#pragma unroll 4
+        for (int j = 0; j < nb; ++j) {
+            const float4 p2 = __ldg(pb + j);
+            sume = __fadd_rn(sume, pair_energy(L, T, p1, p2, row[__float_as_int(p2.w)]));
         }
     }
     return sume;
 }
 
-__global__ void __launch_bounds__(128) spec_energy_kernel(SpecDev S) {
+__global__ void __launch_bounds__(SP_ET) spec_energy_kernel(SpecDev S) {
     extern __shared__ int spr[];  // npairref [ntype*ntype]
     __shared__ float4 sa[SP_MAXAT];
     if (S.flags[0]) return;
@@ -280,12 +268,18 @@ __global__ void __launch_bounds__(128) spec_energy_kernel(SpecDev S) {
     __syncthreads();
     const int nn = S.nergpairm[m];
     const size_t row = (size_t)m * S.M;
-    for (int s = 1 + threadIdx.x; s < nn; s += blockDim.x) {
+    // work items: A for partners 1..nn-1, then B for the same partners (kept only when the
+    // partner is earlier in the visit order), one item per thread at a time
+    const int np = nn - 1;
+    for (int it = threadIdx.x; it < 2 * np; it += blockDim.x) {
+        const bool second = it >= np;
+        const int s = 1 + (second ? it - np : it);
         const int p = S.molergpair[row + s];
+        if (second && S.vpos[p] >= k) continue;
         const int b0 = S.naf[p], nb = S.nato[p];
-        S.A[row + s] = __fadd_rn(0.0f, mol_energy(S.L, S.T, sa, na, S.pos + b0, nb, spr, S.ntype));
-        if (S.vpos[p] < k)
-            S.B[row + s] = __fadd_rn(0.0f, mol_energy(S.L, S.T, sa, na, S.npos + b0, nb, spr, S.ntype));
+        const float e = __fadd_rn(0.0f, mol_energy(S.L, S.T, sa, na, (second ? S.npos : S.pos) + b0, nb, spr, S.ntype));
+        if (second) S.B[row + s] = e;
+        else S.A[row + s] = e;
     }
 }
 
@@ -680,7 +674,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     if (rc) return rc;
     spec_propose_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
     const size_t spr_bytes = sizeof(int) * (size_t)box->ntype * box->ntype;
-    spec_energy_kernel<<<N, 128, spr_bytes, s>>>(S);
+    spec_energy_kernel<<<N, SP_ET, spr_bytes, s>>>(S);
     EPSR_CUDA(cudaMemsetAsync(S.nearc, 0, sizeof(double) * (size_t)N * SP_W, s));
     spec_corr_kernel<<<N, 128, 0, s>>>(S);
     const size_t bits = sizeof(unsigned) * (((size_t)N + 31) / 32);

@@ -9,14 +9,16 @@
 //
 // Device plan: (1) region lists per cell; (2) per visit position, count nonzero pairs;
 // (3) scans give every pair its g; (4) rewrite pairs at g and append (g, partner) to both
-// molecules' rows; (5) sort each row by g.  Pair energies are evaluated in the reference's
-// operation order, so the store is bit-identical; they are computed twice (count, then
-// write) instead of buffering nmol x nnbrefmax candidates.
+// molecules' rows; (5) sort each row by g.  Pair energies are evaluated once, in the
+// reference's operation order (so the store is bit-identical), by the counting pass, which
+// keeps them for the writing pass in an nmol x nnbrefmax buffer.
 #include <math.h>
 
 #include "common.cuh"
 
 namespace epsr {
+
+constexpr int FM_THREADS = 256;   // threads of a visit position's CTA (its region entries)
 
 struct BoxDev {
     Lattice L;
@@ -131,9 +133,11 @@ __device__ __forceinline__ bool far_apart(const Prefilter &P, int im, int jm) {
     return d - P.rad[im] - P.rad[jm] > P.cut;
 }
 
-// (2) count of stored pairs at each visit position
-__global__ void fm_count_kernel(BoxDev B, Prefilter P, const int32_t *visit, const int32_t *molcellno,
-                                const int32_t *reg, const int32_t *nn, int M, int32_t *cnt) {
+// (2) the pair energies of each visit position's region entries (0 where not evaluated),
+// and the count of nonzero ones
+__global__ void __launch_bounds__(FM_THREADS) fm_count_kernel(BoxDev B, Prefilter P, const int32_t *visit,
+                                                              const int32_t *molcellno, const int32_t *reg,
+                                                              const int32_t *nn, int M, float *ebuf, int32_t *cnt) {
     const int v = blockIdx.x;
     const int im = visit[v];
     const int c = molcellno[im] - 1;
@@ -141,9 +145,10 @@ __global__ void fm_count_kernel(BoxDev B, Prefilter P, const int32_t *visit, con
     int mine = 0;
     for (int inn = 1 + threadIdx.x; inn < n; inn += blockDim.x) {
         const int jm = reg[(size_t)c * M + inn];
-        if (jm > im && !far_apart(P, im, jm)) {
-            if (en_mole_pair_dev(B, im, jm) != 0.0f) ++mine;
-        }
+        float e = 0.0f;
+        if (jm > im && !far_apart(P, im, jm)) e = en_mole_pair_dev(B, im, jm);
+        ebuf[(size_t)v * M + inn] = e;
+        if (e != 0.0f) ++mine;
     }
     int tot;
     bscan(mine, &tot);
@@ -182,10 +187,11 @@ __global__ void fm_intra_kernel(const float *eintra, const int32_t *iidx, int nm
 }
 
 // (4) write the pairs at their store index and append to both rows (unordered)
-__global__ void fm_write_kernel(BoxDev B, Prefilter P, const int32_t *visit, const int32_t *molcellno,
-                                const int32_t *reg, const int32_t *nn, int M, const int32_t *off, int nintra,
-                                float *ergpair, int32_t *rowcnt, int32_t *molergpair, int32_t *ergpairref,
-                                int32_t *err) {
+__global__ void __launch_bounds__(FM_THREADS) fm_write_kernel(const int32_t *visit, const int32_t *molcellno,
+                                                              const int32_t *reg, const int32_t *nn, int M,
+                                                              const float *ebuf, const int32_t *off, int nintra,
+                                                              float *ergpair, int32_t *rowcnt, int32_t *molergpair,
+                                                              int32_t *ergpairref, int32_t *err) {
     const int v = blockIdx.x;
     const int im = visit[v];
     const int c = molcellno[im] - 1;
@@ -197,10 +203,8 @@ __global__ void fm_write_kernel(BoxDev B, Prefilter P, const int32_t *visit, con
         int jm = -1, flag = 0;
         if (inn < n) {
             jm = reg[(size_t)c * M + inn];
-            if (jm > im && !far_apart(P, im, jm)) {
-                e = en_mole_pair_dev(B, im, jm);
-                flag = e != 0.0f;
-            }
+            e = ebuf[(size_t)v * M + inn];
+            flag = e != 0.0f;
         }
         int tot;
         const int rank = carry + bscan(flag, &tot);
@@ -400,6 +404,7 @@ extern "C" int64_t epsr_fmolec1_scratch_bytes(int32_t nmol, int32_t ncell, int32
     b += align256(sizeof(int32_t) * 8);                 // err + misc
     b += align256(sizeof(float) * 2);
     b += align256(sizeof(int32_t) * 2 * ((size_t)nmol + (size_t)nmol * M / 2 + 16));  // mirror owners
+    b += align256(sizeof(float) * (size_t)nmol * M);    // pair energies of the region entries
     return (int64_t)b;
 }
 
@@ -433,6 +438,7 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
     float *sums = (float *)take(sizeof(float) * 2);
     const size_t own_n = 2 * ((size_t)nmol + (size_t)nmol * M / 2 + 16);
     int32_t *owners = (int32_t *)take(sizeof(int32_t) * own_n);
+    float *ebuf = (float *)take(sizeof(float) * (size_t)nmol * M);
     EPSR_CUDA(cudaMemsetAsync(err, 0, sizeof(int32_t) * 8, s));
 
     BoxDev B = make_boxdev(box);
@@ -450,7 +456,7 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
     region_build_kernel<<<ncell, 256, sizeof(int32_t) * 2 * (size_t)noff, s>>>(
         cells->cell_start, cells->cell_mols, cells->offsets, noff, cells->ncelldiva, cells->ncelldivb,
         cells->ncelldivc, M, reg, nn, err);
-    fm_count_kernel<<<nmol, 128, 0, s>>>(B, P, cells->cell_mols, cells->molcellno, reg, nn, M, cnt);
+    fm_count_kernel<<<nmol, FM_THREADS, 0, s>>>(B, P, cells->cell_mols, cells->molcellno, reg, nn, M, ebuf, cnt);
     scan1_kernel<<<1, 1024, 0, s>>>(cnt, nmol, off, 0, nullptr);
     scan1_kernel<<<1, 1024, 0, s>>>(nullptr, nmol, iidx, 1, eintra);
     EPSR_CUDA(cudaGetLastError());
@@ -465,8 +471,8 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
     }
     fm_intra_kernel<<<(nmol + 127) / 128, 128, 0, s>>>(eintra, iidx, nmol, M, store->ergpair, rowcnt,
                                                       store->molergpair, store->ergpairref);
-    fm_write_kernel<<<nmol, 128, 0, s>>>(B, P, cells->cell_mols, cells->molcellno, reg, nn, M, off, nintra,
-                                         store->ergpair, rowcnt, store->molergpair, store->ergpairref, err);
+    fm_write_kernel<<<nmol, FM_THREADS, 0, s>>>(cells->cell_mols, cells->molcellno, reg, nn, M, ebuf, off, nintra,
+                                                store->ergpair, rowcnt, store->molergpair, store->ergpairref, err);
     int maxrow = M;
     int cap = 1;
     while (cap < maxrow) cap <<= 1;
