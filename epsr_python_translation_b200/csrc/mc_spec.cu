@@ -257,25 +257,57 @@ __device__ __forceinline__ float mol_energy(const Lattice &L, const Tables &T, c
 }
 
 __global__ void __launch_bounds__(SP_ET) spec_energy_kernel(SpecDev S) {
-    extern __shared__ int spr[];  // npairref [ntype*ntype]
+    extern __shared__ int sdyn[];   // npairref [ntype*ntype], then the work list [2*M]
     __shared__ float4 sa[SP_MAXAT];
+    __shared__ int cnt[SP_MAXAT + 2];
     if (S.flags[0]) return;
+    int *spr = sdyn;
+    int *list = sdyn + ((S.ntype * S.ntype + 3) & ~3);
     const int k = blockIdx.x;
     const int m = S.visit[k];
     const int na = S.nato[m], a0 = S.naf[m];
     for (int i = threadIdx.x; i < S.ntype * S.ntype; i += blockDim.x) spr[i] = S.npairref[i];
     for (int i = threadIdx.x; i < na; i += blockDim.x) sa[i] = S.npos[a0 + i];
+    for (int i = threadIdx.x; i < SP_MAXAT + 2; i += blockDim.x) cnt[i] = 0;
     __syncthreads();
     const int nn = S.nergpairm[m];
     const size_t row = (size_t)m * S.M;
-    // work items: A for partners 1..nn-1, then B for the same partners (kept only when the
-    // partner is earlier in the visit order), one item per thread at a time
+    // work items: A for partners 1..nn-1 (item s-1), then B for the same partners (item
+    // np+s-1) when the partner is earlier in the visit order.  The items are listed by the
+    // partner's atom count, so the lanes of a warp run loops of the same length.
     const int np = nn - 1;
+    auto item_nb = [&](int it) -> int {   // atom count (1..SP_MAXAT) of the item's partner, 0 if no item
+        const bool second = it >= np;
+        const int p = S.molergpair[row + 1 + (second ? it - np : it)];
+        if (second && S.vpos[p] >= k) return 0;
+        return S.nato[p];
+    };
     for (int it = threadIdx.x; it < 2 * np; it += blockDim.x) {
+        const int nb = item_nb(it);
+        if (nb > 0) atomicAdd(&cnt[nb], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {   // cnt[b] -> first list position of atom count b; cnt[SP_MAXAT+1] = total
+        int a = 0;
+        for (int b = 0; b <= SP_MAXAT; ++b) {
+            const int c = cnt[b];
+            cnt[b] = a;
+            a += c;
+        }
+        cnt[SP_MAXAT + 1] = a;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < 2 * np; it += blockDim.x) {
+        const int nb = item_nb(it);
+        if (nb > 0) list[atomicAdd(&cnt[nb], 1)] = it;
+    }
+    __syncthreads();
+    const int total = cnt[SP_MAXAT + 1];
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        const int it = list[q];
         const bool second = it >= np;
         const int s = 1 + (second ? it - np : it);
         const int p = S.molergpair[row + s];
-        if (second && S.vpos[p] >= k) continue;
         const int b0 = S.naf[p], nb = S.nato[p];
         const float e = __fadd_rn(0.0f, mol_energy(S.L, S.T, sa, na, (second ? S.npos : S.pos) + b0, nb, spr, S.ntype));
         if (second) S.B[row + s] = e;
@@ -673,8 +705,9 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     int rc = ran1_fill_device_count(S.ran1_next, S.draws, S.off + N, (int64_t)N * 7 + 1, s);
     if (rc) return rc;
     spec_propose_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
-    const size_t spr_bytes = sizeof(int) * (size_t)box->ntype * box->ntype;
-    spec_energy_kernel<<<N, SP_ET, spr_bytes, s>>>(S);
+    const size_t en_bytes = sizeof(int) * ((((size_t)box->ntype * box->ntype + 3) & ~(size_t)3) + 2 * (size_t)M);
+    if (en_bytes > 48 * 1024) EPSR_SMEM_OPTIN(spec_energy_kernel);
+    spec_energy_kernel<<<N, SP_ET, en_bytes, s>>>(S);
     EPSR_CUDA(cudaMemsetAsync(S.nearc, 0, sizeof(double) * (size_t)N * SP_W, s));
     spec_corr_kernel<<<N, 128, 0, s>>>(S);
     const size_t bits = sizeof(unsigned) * (((size_t)N + 31) / 32);
