@@ -32,20 +32,56 @@ struct PressDev {
 };
 
 __global__ void __launch_bounds__(PR_THREADS) press_pairs_kernel(PressDev P) {
+    extern __shared__ int list[];   // [M] slots with a partner jm > im, by partner atom count
     __shared__ float4 sa[PR_MAXAT];
+    __shared__ int bk[PR_MAXAT + 2];
     const int im = blockIdx.x;
     const int a0 = P.naf[im], na = P.nato[im];
     const bool in_smem = na <= PR_MAXAT;   // larger molecules are read from global memory
     if (in_smem)
         for (int i = threadIdx.x; i < na; i += blockDim.x) sa[i] = P.pos[a0 + i];
+    for (int i = threadIdx.x; i < PR_MAXAT + 2; i += blockDim.x) bk[i] = 0;
     __syncthreads();
     const float xc1 = P.xadd[im], yc1 = P.yadd[im], zc1 = P.zadd[im];
     const int nn = P.nergpairm[im];
     const size_t row = (size_t)im * P.M;
+    // slots whose partner comes later are evaluated, listed by the partner's atom count so the
+    // lanes of a warp run loops of the same length; the others hold 0
+    auto nb_of = [&](int s) -> int {
+        const int jm = P.molergpair[row + s];
+        return jm > im ? min(P.nato[jm], PR_MAXAT) : 0;
+    };
     for (int s = threadIdx.x; s < nn; s += blockDim.x) {
+        const int nb = nb_of(s);
+        if (nb > 0) {
+            atomicAdd(&bk[nb], 1);
+        } else {
+            P.ergold[row + s] = 0.0f;
+            P.ergnew[row + s] = 0.0f;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {   // bk[b] -> first list position of atom count b; bk[PR_MAXAT+1] = total
+        int a = 0;
+        for (int b = 0; b <= PR_MAXAT; ++b) {
+            const int t = bk[b];
+            bk[b] = a;
+            a += t;
+        }
+        bk[PR_MAXAT + 1] = a;
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < nn; s += blockDim.x) {
+        const int nb = nb_of(s);
+        if (nb > 0) list[atomicAdd(&bk[nb], 1)] = s;
+    }
+    __syncthreads();
+    const int total = bk[PR_MAXAT + 1];
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        const int s = list[q];
         const int jm = P.molergpair[row + s];
         float eo = 0.0f, en = 0.0f;
-        if (jm > im) {
+        {
             // separation of the centres (the same for every atom pair of im, jm)
             float xcdif = __fsub_rn(P.xadd[jm], xc1), ycdif = __fsub_rn(P.yadd[jm], yc1),
                   zcdif = __fsub_rn(P.zadd[jm], zc1);
@@ -62,23 +98,27 @@ __global__ void __launch_bounds__(PR_THREADS) press_pairs_kernel(PressDev P) {
                         __fadd_rn(__fadd_rn(__fmul_rn(xdif, xdif), __fmul_rn(ydif, ydif)), __fmul_rn(zdif, zdif));
                     const float dtest = __fsqrt_rn(dsq);
                     const int iz = ifix(__fdiv_rn(dtest, P.stepcl)) + 2;
-                    if (iz >= 2 && iz <= P.npt1) {
-                        const int icref = __ldg(prow + __float_as_int(p2.w));
-                        const float4 t = __ldg(P.tab + (size_t)icref * P.ld + iz);       // bin iz
-                        const float4 tm = __ldg(P.tab + (size_t)icref * P.ld + iz - 1);  // bin iz-1
-                        const float dtdif = __fsub_rn(dtest, __ldg(P.xstar + iz));
-                        float prfac = 0.0f;
-                        if (dtest > 0.0f)
-                            prfac = __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(xcdif, xdif), __fmul_rn(ycdif, ydif)),
-                                                        __fmul_rn(zcdif, zdif)),
-                                              dtest);
-                        const float enpot = __fadd_rn(t.z, __fmul_rn(t.w, dtdif));
-                        const double prpot = (double)__fmul_rn(__fmul_rn(0.5f, __fadd_rn(t.w, tm.w)), prfac);
-                        const float enwt = __fadd_rn(t.x, __fmul_rn(t.y, dtdif));
-                        const float prwt = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(t.y, tm.y)), prfac);
-                        eo = __fadd_rn(__fadd_rn(eo, enwt), enpot);
-                        en = __double2float_rn(__dadd_rn((double)__fadd_rn(en, prwt), prpot));
-                    }
+                    // branch-free: tables read at iz clamped into 2..npt1, the sums kept unchanged
+                    // outside that range, so consecutive pairs' loads can be in flight together
+                    const bool in = iz >= 2 && iz <= P.npt1;
+                    const int izc = min(max(iz, 2), P.npt1);
+                    const int icref = __ldg(prow + __float_as_int(p2.w));
+                    const float4 t = __ldg(P.tab + (size_t)icref * P.ld + izc);       // bin iz
+                    const float4 tm = __ldg(P.tab + (size_t)icref * P.ld + izc - 1);  // bin iz-1
+                    const float dtdif = __fsub_rn(dtest, __ldg(P.xstar + izc));
+                    const float prfac =
+                        dtest > 0.0f ? __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(xcdif, xdif), __fmul_rn(ycdif, ydif)),
+                                                           __fmul_rn(zcdif, zdif)),
+                                                 dtest)
+                                     : 0.0f;
+                    const float enpot = __fadd_rn(t.z, __fmul_rn(t.w, dtdif));
+                    const double prpot = (double)__fmul_rn(__fmul_rn(0.5f, __fadd_rn(t.w, tm.w)), prfac);
+                    const float enwt = __fadd_rn(t.x, __fmul_rn(t.y, dtdif));
+                    const float prwt = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(t.y, tm.y)), prfac);
+                    const float eo2 = __fadd_rn(__fadd_rn(eo, enwt), enpot);
+                    const float en2 = __double2float_rn(__dadd_rn((double)__fadd_rn(en, prwt), prpot));
+                    eo = in ? eo2 : eo;
+                    en = in ? en2 : en;
                 }
             }
         }
@@ -194,7 +234,9 @@ extern "C" int epsr_press(const epsr_box_t *box, const epsr_store_t *store, int3
     int rc = epsr_box_positions(box, stream);
     if (rc) return rc;
     if (nmol > 1) {
-        press_pairs_kernel<<<nmol - 1, PR_THREADS, 0, s>>>(P);
+        const size_t list_bytes = sizeof(int) * (size_t)M;
+        if (list_bytes > 48 * 1024) EPSR_SMEM_OPTIN(press_pairs_kernel);
+        press_pairs_kernel<<<nmol - 1, PR_THREADS, list_bytes, s>>>(P);
         EPSR_CUDA(cudaGetLastError());
         if (strict) press_sum_strict_kernel<<<1, 1, 0, s>>>(P, nmol);
         else press_sum_fast_kernel<<<1, 1024, 0, s>>>(P, nmol);

@@ -19,6 +19,7 @@
 namespace epsr {
 
 constexpr int FM_THREADS = 256;   // threads of a visit position's CTA (its region entries)
+constexpr int FM_MAXAT = 64;      // atom-count buckets of the evaluation list (larger share the last)
 
 struct BoxDev {
     Lattice L;
@@ -138,15 +139,47 @@ __device__ __forceinline__ bool far_apart(const Prefilter &P, int im, int jm) {
 __global__ void __launch_bounds__(FM_THREADS) fm_count_kernel(BoxDev B, Prefilter P, const int32_t *visit,
                                                               const int32_t *molcellno, const int32_t *reg,
                                                               const int32_t *nn, int M, float *ebuf, int32_t *cnt) {
+    extern __shared__ int list[];   // [M] region entries to evaluate, by partner atom count
+    __shared__ int bk[FM_MAXAT + 2];
     const int v = blockIdx.x;
     const int im = visit[v];
     const int c = molcellno[im] - 1;
     const int n = nn[c];
-    int mine = 0;
-    for (int inn = 1 + threadIdx.x; inn < n; inn += blockDim.x) {
+    for (int i = threadIdx.x; i < FM_MAXAT + 2; i += blockDim.x) bk[i] = 0;
+    __syncthreads();
+    // entries evaluated: partner later in molecule order and not certainly beyond the cutoff;
+    // the others store 0.  Listing them by the partner's atom count gives the lanes of a warp
+    // loops of the same length.
+    auto nb_of = [&](int inn) -> int {
         const int jm = reg[(size_t)c * M + inn];
-        float e = 0.0f;
-        if (jm > im && !far_apart(P, im, jm)) e = en_mole_pair_dev(B, im, jm);
+        return (jm > im && !far_apart(P, im, jm)) ? min(B.nato[jm], FM_MAXAT) : 0;
+    };
+    for (int inn = 1 + threadIdx.x; inn < n; inn += blockDim.x) {
+        const int nb = nb_of(inn);
+        if (nb > 0) atomicAdd(&bk[nb], 1);
+        else ebuf[(size_t)v * M + inn] = 0.0f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {   // bk[b] -> first list position of atom count b; bk[FM_MAXAT+1] = total
+        int a = 0;
+        for (int b = 0; b <= FM_MAXAT; ++b) {
+            const int t = bk[b];
+            bk[b] = a;
+            a += t;
+        }
+        bk[FM_MAXAT + 1] = a;
+    }
+    __syncthreads();
+    for (int inn = 1 + threadIdx.x; inn < n; inn += blockDim.x) {
+        const int nb = nb_of(inn);
+        if (nb > 0) list[atomicAdd(&bk[nb], 1)] = inn;
+    }
+    __syncthreads();
+    const int total = bk[FM_MAXAT + 1];
+    int mine = 0;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        const int inn = list[q];
+        const float e = en_mole_pair_dev(B, im, reg[(size_t)c * M + inn]);
         ebuf[(size_t)v * M + inn] = e;
         if (e != 0.0f) ++mine;
     }
@@ -456,7 +489,10 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
     region_build_kernel<<<ncell, 256, sizeof(int32_t) * 2 * (size_t)noff, s>>>(
         cells->cell_start, cells->cell_mols, cells->offsets, noff, cells->ncelldiva, cells->ncelldivb,
         cells->ncelldivc, M, reg, nn, err);
-    fm_count_kernel<<<nmol, FM_THREADS, 0, s>>>(B, P, cells->cell_mols, cells->molcellno, reg, nn, M, ebuf, cnt);
+    const size_t list_bytes = sizeof(int) * (size_t)M;
+    if (list_bytes > 48 * 1024) EPSR_SMEM_OPTIN(fm_count_kernel);
+    fm_count_kernel<<<nmol, FM_THREADS, list_bytes, s>>>(B, P, cells->cell_mols, cells->molcellno, reg, nn, M, ebuf,
+                                                         cnt);
     scan1_kernel<<<1, 1024, 0, s>>>(cnt, nmol, off, 0, nullptr);
     scan1_kernel<<<1, 1024, 0, s>>>(nullptr, nmol, iidx, 1, eintra);
     EPSR_CUDA(cudaGetLastError());
