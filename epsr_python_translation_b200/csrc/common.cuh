@@ -246,12 +246,14 @@ __device__ __forceinline__ int ran1_warp_batch(int32_t &idum, int32_t &iy, int32
 // A warp's ran1 stream in batches of 32, the Park-Miller values of the next batch computed
 // while the current batch's shuffle chain runs (they depend only on the batch's last value).
 // Bit-identical to ran1_warp_batch, which it falls back to for batches that can meet a zero
-// or a re-initialisation.
+// or a re-initialisation.  Once a batch has started from idum in 1..IM-1 with no zero table
+// entry, every later value is a Park-Miller value of such an idum and so nonzero (IM is
+// prime): the stream is `clean` and the checks are skipped from then on.
 struct Ran1Warp {
     int32_t idum, iy, iv;   // idum, iy warp-uniform; iv this lane's table entry
     uint32_t mul;           // IA^(lane+1) mod IM
     int32_t idl;            // this lane's Park-Miller value of the next batch, when idl_ok
-    bool idl_ok;
+    bool idl_ok, clean;
 
     __device__ __forceinline__ void load(const int32_t *state) {
         const int lane = threadIdx.x & 31;
@@ -261,21 +263,21 @@ struct Ran1Warp {
         mul = 16807u;
         for (int k = 0; k < lane; ++k) mul = r1_mulmod(mul, 16807u);
         idl_ok = false;
+        clean = false;
     }
     // Up to `want` (<= 32) values; lane t < return value receives value t in `mine`.
     __device__ __forceinline__ int next(int want, int32_t &mine, int32_t *tab_tmp) {
-        if (want == 32 && idum > 0 && iy != 0) {
+        if (want == 32 && (clean || (idum > 0 && idum < 2147483647 && iy != 0 &&
+                                     __ballot_sync(0xffffffffu, iv == 0) == 0u))) {
+            clean = true;
             if (!idl_ok) idl = (int32_t)r1_mulmod(mul, (uint32_t)idum);
-            const unsigned zero = __ballot_sync(0xffffffffu, idl == 0) | __ballot_sync(0xffffffffu, iv == 0);
-            if (zero == 0u) {
-                const int32_t last = __shfl_sync(0xffffffffu, idl, 31);
-                const int32_t nidl = (int32_t)r1_mulmod(mul, (uint32_t)last);
-                mine = ran1_chain32(idl, iv, iy);
-                idum = last;
-                idl = nidl;
-                idl_ok = true;
-                return 32;
-            }
+            const int32_t last = __shfl_sync(0xffffffffu, idl, 31);
+            const int32_t nidl = (int32_t)r1_mulmod(mul, (uint32_t)last);
+            mine = ran1_chain32(idl, iv, iy);
+            idum = last;
+            idl = nidl;
+            idl_ok = true;
+            return 32;
         }
         idl_ok = false;
         return ran1_warp_batch(idum, iy, iv, mul, want, mine, tab_tmp);

@@ -48,6 +48,7 @@ constexpr int FX_RQ = 16;                       // leading quads of a row held i
 constexpr int FX_RING = 2048;                   // ran1 values held per worker CTA (power of two)
 constexpr int FX_CK = 128;                      // generator checkpoints (power of two)
 constexpr int FX_CKE = 8;                       // batches between checkpoints (power of two)
+constexpr int FX_GB = 4;                        // generator batches between reads of the control words
 constexpr int FX_CKW = 36;                      // ints per checkpoint: idum, iy, iv[32], pad[2]
 constexpr unsigned long long FX_WAIT_NS = 2000000000ull;  // a wait gives up after 2 s
 
@@ -243,7 +244,8 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
         while (true) {
             __syncwarp();
             if (vs->done) break;
-            if (pos + 32 > vs->cons + FX_RING) {   // ring full: wait for the workers (bounded)
+            const long long room = vs->cons + FX_RING - pos;
+            if (room < 32) {   // ring full: wait for the workers (bounded)
                 int give_up = 0;
                 if (lane == 0) {
                     const unsigned long long t = now_ns();
@@ -259,24 +261,28 @@ __global__ void __launch_bounds__(FX_THREADS, 1) fitexp_cluster_kernel(FxDev F) 
                 continue;
             }
             t0 = 0;
-            if ((nb & (FX_CKE - 1)) == 0) {   // the state before this batch, every FX_CKE batches
-                const int slot = (int)((nb / FX_CKE) & (FX_CK - 1));
-                ck[slot * FX_CKW + 2 + lane] = g.iv;
-                if (lane == 0) {
-                    ck[slot * FX_CKW + 0] = g.idum;
-                    ck[slot * FX_CKW + 1] = g.iy;
-                    ckpos[slot] = pos;
+            // up to FX_GB batches before the control words are read again
+            const int nbat = room >= 32 * FX_GB ? FX_GB : (int)(room >> 5);
+            for (int bi = 0; bi < nbat; ++bi) {
+                if ((nb & (FX_CKE - 1)) == 0) {   // the state before this batch, every FX_CKE batches
+                    const int slot = (int)((nb / FX_CKE) & (FX_CK - 1));
+                    ck[slot * FX_CKW + 2 + lane] = g.iv;
+                    if (lane == 0) {
+                        ck[slot * FX_CKW + 0] = g.idum;
+                        ck[slot * FX_CKW + 1] = g.iy;
+                        ckpos[slot] = pos;
+                    }
                 }
+                ++nb;
+                int32_t mine;
+                const int cnt = g.next(32, mine, g_tab);
+                if (lane < cnt) {
+                    const long long q = pos + lane;
+                    ring[q & (FX_RING - 1)] = ((unsigned long long)(uint32_t)(q + 1) << 32) |
+                                              (unsigned long long)__float_as_uint(ran1_out(mine));
+                }
+                pos += cnt;
             }
-            ++nb;
-            int32_t mine;
-            const int cnt = g.next(32, mine, g_tab);
-            if (lane < cnt) {
-                const long long q = pos + lane;
-                ring[q & (FX_RING - 1)] =
-                    ((unsigned long long)(uint32_t)(q + 1) << 32) | (unsigned long long)__float_as_uint(ran1_out(mine));
-            }
-            pos += cnt;
         }
         __syncwarp();
         __syncthreads();   // meets the workers after they set done (barrier 0, all 512 threads)

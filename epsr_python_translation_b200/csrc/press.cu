@@ -143,21 +143,22 @@ __global__ void press_sum_strict_kernel(PressDev P, int nmol) {
     P.sums[1] = presst;
 }
 
-// both sums in double, in parallel (one CTA; a fixed order, so the result is reproducible)
+// both sums in double, in parallel (one CTA; a fixed order, so the result is reproducible):
+// warp w takes molecules w, w+32, ..., its lanes the slots of each
 __global__ void __launch_bounds__(1024) press_sum_fast_kernel(PressDev P, int nmol) {
     __shared__ double r0[32], r1[32];
     double a = 0.0, b = 0.0;
-    const size_t total = (size_t)(nmol - 1) * P.M;
-    for (size_t k = threadIdx.x; k < total; k += blockDim.x) {
-        const int im = (int)(k / P.M), s = (int)(k - (size_t)im * P.M);
-        if (s < P.nergpairm[im]) {
-            a += (double)P.ergold[k];
-            b += (double)P.ergnew[k];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int im = wid; im < nmol - 1; im += nwarp) {
+        const size_t row = (size_t)im * P.M;
+        const int nn = P.nergpairm[im];
+        for (int s = lane; s < nn; s += 32) {
+            a += (double)P.ergold[row + s];
+            b += (double)P.ergnew[row + s];
         }
     }
     a = warp_sum_d(a);
     b = warp_sum_d(b);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) {
         r0[wid] = a;
         r1[wid] = b;
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(1024) press_sum_fast_kernel(PressDev P, int nm
     __syncthreads();
     if (threadIdx.x == 0) {
         double ta = 0.0, tb = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        for (int w = 0; w < nwarp; ++w) {
             ta += r0[w];
             tb += r1[w];
         }

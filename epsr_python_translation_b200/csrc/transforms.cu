@@ -19,10 +19,12 @@ __global__ void gensq_kernel(int nq, int npairs, int npt1, const float *wav, int
     const float *w2 = wav + (size_t)(npairs + ic) * ldw;
     const float nsph = natomsphere[n2extr[ic]];
     float sum1 = 0.0f, sum2 = 0.0f, sum3 = 0.0f;
-    for (int j = 2; j <= npt1; ++j) {
+#pragma unroll 4
+    for (int j = 2; j <= npt1; ++j) {   // branch-free, so the loads of several j are in flight
         const float f = __ldg(fq + (long long)j * sj + (long long)i * si);
         const float a1 = __ldg(w1 + j);
-        if (fabsf(a1) > 0.0f) sum1 = __fadd_rn(sum1, __fmul_rn(a1, f));
+        const float t1 = __fadd_rn(sum1, __fmul_rn(a1, f));
+        sum1 = fabsf(a1) > 0.0f ? t1 : sum1;
         const float b = __ldg(w2 + j);
         const float a2 = __fmul_rn(__fsub_rn(b, __ldg(ycoh + j)), nsph);
         sum2 = __fadd_rn(sum2, __fmul_rn(a2, f));
