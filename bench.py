@@ -35,9 +35,10 @@ METRIC = "MC molecule-moves/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one fitexp_cluster_kernel launch on the C2
 # fit, from an ncu --set full capture of one launch (independent of the trial count: the
 # basis is read from HBM once per launch)
-FIT_DRAM_BYTES_PER_LAUNCH = 401152
-# SM cycles per ran1 value of the warp shuffle chain on an otherwise idle SM (clock64 timing)
-FIT_CHAIN_CYCLES_PER_VALUE = 46.0
+FIT_DRAM_BYTES_PER_LAUNCH = 409856
+# SM cycles per ran1 value of the warp shuffle chain (two shuffles a step) on an otherwise
+# idle SM (clock64 timing of 640,000 values)
+FIT_CHAIN_CYCLES_PER_VALUE = 40.0
 UNIT = "moves/s"
 
 

@@ -75,6 +75,7 @@ _SIGS = {
     "epsr_press": (C.c_int, [C.POINTER(Box), C.POINTER(Store), I32, P, I64, I32, P, P]),
     "epsr_press_scratch_bytes": (I64, [I32, I32]),
     "epsr_gensq": (C.c_int, [I32, I32, I32, P, I32, P, I64, I64, P, P, P, P, P]),
+    "epsr_ptgnsq_difference": (C.c_int, [I32, I32, I32, P, P, P, P, P]),
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),
     "epsr_stog_scratch_bytes": (I64, [I32, I32]),
     "epsr_fit_expansion": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, I32, P, P]),

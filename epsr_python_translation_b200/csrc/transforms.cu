@@ -83,9 +83,35 @@ __global__ void stog_kernel(float rho, const float *q, int ldq, const float *sof
     }
 }
 
+// The simulated fit of each data set (ptgnsq epsr_standalone_rev3.py:3844-3867): the sum
+// over atom pairs of weight x intermolecular S(Q), sequential in float32 as the reference,
+// and its difference from the data, negated: out = -(data - sum).  Thread per (set, Q).
+__global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *data, const float *cwt,
+                                   const float *qwind, float *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int d = blockIdx.y;
+    if (i > nq) return;
+    const float *w = cwt + (size_t)d * npairs;
+    float sum = 0.0f;
+    for (int ic = 0; ic < npairs; ++ic) sum = __fadd_rn(sum, __fmul_rn(__ldg(w + ic), __ldg(qwind + (size_t)ic * (nq + 1) + i)));
+    out[(size_t)d * (nq + 1) + i] = -__fsub_rn(data[(size_t)d * (nq + 1) + i], sum);
+}
+
 }  // namespace epsr
 
 using namespace epsr;
+
+extern "C" int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const float *cwt,
+                                      const float *qwind, float *out, void *stream) {
+    if (ndata <= 0 || npairs <= 0 || nq <= 0 || !data || !cwt || !qwind || !out) {
+        epsr_set_error("epsr_ptgnsq_difference: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    ptgnsq_diff_kernel<<<dim3((nq + 1 + 127) / 128, ndata), 128, 0, (cudaStream_t)stream>>>(ndata, npairs, nq, data,
+                                                                                           cwt, qwind, out);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
 
 extern "C" int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float *wav, int32_t ldw, const float *foqols,
                           int64_t sj, int64_t si, const float *ycoh, const int32_t *n2extr, const float *natomsphere,

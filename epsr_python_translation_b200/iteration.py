@@ -39,7 +39,8 @@ class EpsrIteration:
         self.ycoh = torch.from_numpy(np.ascontiguousarray(wl.ycoh[: b.npt + 1], f32)).to(dev)
         self.expr = torch.from_numpy(wl.expr).to(dev)
         self.data = torch.from_numpy(wl.data).to(dev)
-        self.weights = torch.from_numpy(wl.weights).to(dev)
+        self.weights = torch.from_numpy(np.ascontiguousarray(wl.weights, dtype=np.float32)).to(dev)
+        self._dt = torch.empty_like(self.data)
         self.natomsphere = torch.ones(b.ntype, dtype=torch.float32, device=dev)
         self.rminex = torch.full((b.npairs,), -2.0, dtype=torch.float32, device=dev)
         self.xwt = torch.from_numpy(wl.xwt).to(dev)
@@ -84,7 +85,7 @@ class EpsrIteration:
         self.sofq = sofq.view(2, b.npairs, nq + 1)
         inter = self.sofq[1]                                   # (npairs, nq+1)
         # per data set: the difference between the data and the weighted simulated S(Q)
-        dt = -(self.data - torch.matmul(self.weights, inter))  # (ndata, nq+1)
+        dt = transforms.ptgnsq_difference(self.data, self.weights, inter, out=self._dt)   # (ndata, nq+1)
         self._mark("gensq", True)
         self._mark("press")
         sumc, presst = d.press(b.npt1, strict=self.strict)

@@ -40,6 +40,20 @@ def gensq(nq, npt1, wav, ldw, foqols, sj, si, ycoh, n2extr, natomsphere, npairs)
     return out
 
 
+def ptgnsq_difference(data, cwt, qwind, out=None):
+    """The simulated fit of each data set and its negated difference from the data
+    (ptgnsq epsr_standalone_rev3.py:3844-3867): -(data - cwt @ qwind), the sum over atom
+    pairs sequential in float32.  data (ndata, nq+1), cwt (ndata, npairs), qwind
+    (npairs, nq+1), all on the device."""
+    lib = _lib.load(require_device=True)
+    ndata, ld = data.shape
+    npairs = cwt.shape[1]
+    if out is None:
+        out = torch.empty_like(data)
+    check(lib.epsr_ptgnsq_difference(ndata, npairs, ld - 1, _p(data), _p(cwt), _p(qwind), _p(out), _s()))
+    return out
+
+
 def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
     """stog ato_manipulation_rev4.py:4067.  q (ldq,), sofq_pairs (npairs, ldq), r (nr+1,)."""
     lib = _lib.load(require_device=True)

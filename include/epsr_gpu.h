@@ -227,6 +227,14 @@ int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float *wav, int32
                int64_t fq_sj, int64_t fq_si, const float *ycoh, const int32_t *n2extr, const float *natomsphere,
                float *sofq, void *stream);
 
+/* ptgnsq epsr_standalone_rev3.py:3844-3867 (the simulated fit of each data set, for the
+ * potential refinement): out[d][i] = -(data[d][i] - sum_ic cwt[d][ic] * qwind[ic][i]), the
+ * sum sequential in float32 over atom pairs ic.  data, out: [ndata][nq+1]; cwt:
+ * [ndata][npairs]; qwind: [npairs][nq+1] (the intermolecular S(Q) of gensq).  Device
+ * pointers; asynchronous on `stream`. */
+int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const float *cwt,
+                           const float *qwind, float *out, void *stream);
+
 /* stog ato_manipulation_rev4.py:4067-4121 (+ lorch :4113).  q [ldq] 1-based, sofq
  * [npairs*ldq] (sofq(i,in) at [in*ldq+i]), r [nr+1] 1-based, gofr out [npairs*(nr+1)],
  * nqmin/nqmax (device, [npairs] each), xwt [npairs].  scratch: device bytes from

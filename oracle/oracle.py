@@ -300,6 +300,22 @@ def atogen(box, ngrsamples, ran1, rminex, ycoh=None, sizefactor=1.0):
 
 
 # ----------------------------------------------------------------------------- transforms
+def ptgnsq_difference(data, cwt, qwind):
+    """ptgnsq epsr_standalone_rev3.py:3844-3867: the simulated fit of data set d at Q index i
+    is the float32 sum over atom pairs ic, in order, of cwt[d, ic] * qwind[ic, i] (:3853-3854);
+    returned negated as the difference from the data, -(data - sum)."""
+    data = np.asarray(data, np.float32)
+    cwt = np.asarray(cwt, np.float32)
+    qwind = np.asarray(qwind, np.float32)
+    out = np.empty_like(data)
+    for d in range(data.shape[0]):
+        s = np.zeros(qwind.shape[1], np.float32)
+        for ic in range(qwind.shape[0]):
+            s = (s + (cwt[d, ic] * qwind[ic]).astype(np.float32)).astype(np.float32)
+        out[d] = -(data[d] - s)
+    return out
+
+
 def gensq(nq, npt1, wav, foqols_rows, ycoh, n2extr, natomsphere):
     """wav (2, npairs, ldw); foqols_rows (nq+1, ldf) with row i = F[:, i]."""
     npairs, ldw = wav.shape[1], wav.shape[2]

@@ -68,9 +68,9 @@ class CpuIteration:
         t["press"] = time.perf_counter() - t0
         t0 = time.perf_counter()
         inter = sofq[1]
+        dts = oracle.ptgnsq_difference(wl.data, wl.weights, inter)
         for k in range(wl.data.shape[0]):
-            fit = (wl.weights[k].astype(np.float32) @ inter).astype(f32)
-            dt = (-(wl.data[k] - fit)).astype(f32)
+            dt = dts[k]
             res, self.ran1 = oracle.fit_expansion(dt, wl.expr, self.pwtold[k], self.stepp[k], 1, nq, 1, wl.nterms,
                                                   1000, 10, self.ran1)
             self.pwtold[k] = res["wtold"]

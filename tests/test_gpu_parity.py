@@ -443,3 +443,18 @@ def test_fit_expansion_cluster_shapes_strict_match_oracle(npt, scale):
         assert_bits_equal(res[k], ref[k], k)
     assert res["trials"] == ref["trials"]
     assert np.array_equal(t.cpu().numpy(), rst.as_array())
+
+
+@pytest.mark.gpu
+def test_ptgnsq_difference_bit_identical():
+    """The per-data-set simulated fit and its difference from the data (ptgnsq
+    epsr_standalone_rev3.py:3844-3867) equals the oracle's sequential float32 sum bit for bit."""
+    from epsr_python_translation_b200 import transforms
+    rng = np.random.default_rng(11)
+    ndata, npairs, nq = 3, 21, 600
+    data = rng.standard_normal((ndata, nq + 1)).astype(f32)
+    cwt = rng.uniform(0.0, 0.2, (ndata, npairs)).astype(f32)
+    qwind = (rng.standard_normal((npairs, nq + 1)) * 0.3).astype(f32)
+    got = transforms.ptgnsq_difference(torch.from_numpy(data).cuda(), torch.from_numpy(cwt).cuda(),
+                                       torch.from_numpy(qwind).cuda()).cpu().numpy()
+    assert_bits_equal(got, oracle.ptgnsq_difference(data, cwt, qwind), "ptgnsq difference")
