@@ -440,7 +440,7 @@ def roofline(it, stage_ms, a):
         us_trial = 1000.0 * per_launch_ms / max(it.fit_trials, 1)
         extra["fit_us_per_trial"] = us_trial
         # The kernel is latency-bound: every trial consumes nterms+1 ran1 values from one
-        # sequential shuffle chain, measured at 46 SM cycles per value on an otherwise idle SM.
+        # sequential shuffle chain, measured at 40 SM cycles per value on an otherwise idle SM.
         chain_us = (wl.nterms + 1) * FIT_CHAIN_CYCLES_PER_VALUE / (float(peaks.get("sm_max_mhz", 1965.0)))
         extra["fit_chain_bound"] = {"us_per_trial": chain_us, "frac": chain_us / us_trial,
                                     "cycles_per_value": FIT_CHAIN_CYCLES_PER_VALUE}
