@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--strict", action="store_true", help="bit-identical sequential sums")
     ap.add_argument("--cpu-sample-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--python-driver", action="store_true",
+                    help="drive each iteration's routines from Python instead of epsr_iteration_step")
     return ap.parse_args()
 
 
@@ -217,7 +219,7 @@ def gpu_arm(a):
     its = []
     for r in range(R):
         with torch.cuda.stream(streams[r]):
-            its.append(EpsrIteration(wl, strict=a.strict, ran1_seed=box_seed(rank, R, r)))
+            its.append(EpsrIteration(wl, strict=a.strict, ran1_seed=box_seed(rank, R, r), native=not a.python_driver))
     torch.cuda.synchronize()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
     main = torch.cuda.current_stream()

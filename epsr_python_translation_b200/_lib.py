@@ -52,6 +52,31 @@ class Mc(C.Structure):
                 ("status", P)]
 
 
+class Iteration(C.Structure):
+    """epsr_iteration_t: one EPSR iteration of the path, driven natively."""
+    _fields_ = [("box", P), ("mc", P),
+                ("nmolcell", I32), ("rmax", F32), ("lat6", F32 * 6), ("lat9", F32 * 9),
+                ("cell_molcellno", P), ("cell_start", P), ("cell_mols", P), ("cell_offsets", P),
+                ("cell_scratch", P), ("cell_scratch_n", I64),
+                ("store_m", I32), ("store_capacity", I32),
+                ("nergpairm", P), ("molergpair", P), ("ergpairref", P), ("mirror", P), ("nergpair", P),
+                ("ergpair", P), ("eintra", P), ("ntimes", I32),
+                ("npt1", I32), ("natomr", I32), ("ngrsamples", I32), ("sizefactor", F32), ("dmax", F32),
+                ("rminex", P), ("cfrac", P), ("ycoh", P), ("n1extr", P), ("n2extr", P),
+                ("wav", P), ("ldw", I32), ("potex", P), ("counts", P),
+                ("nq", I32), ("ndata", I32), ("foqols", P), ("foqols_sj", I64), ("foqols_si", I64),
+                ("natomsphere", P), ("sofq", P), ("data", P), ("cwt", P), ("dt", P),
+                ("expr", P), ("nterms", I32), ("ncfirst", I32), ("nits", I32), ("nfreq", I32),
+                ("fit_wt", P), ("fit_wtold", P), ("fit_yout", P), ("fit_scal_host", P), ("fit_trials_host", P),
+                ("rho", F32), ("q", P), ("r", P), ("nr", I32), ("nqmin", P), ("nqmax", P), ("xwt", P),
+                ("gofr", P), ("scratch", P), ("scratch_bytes", I64), ("strict", I32), ("stage_events", P * 16)]
+
+
+class IterationReport(C.Structure):
+    _fields_ = [("nnbrefmax", I32), ("ftest", F32 * 2), ("ngrsamples", I32), ("pair_updates", I64),
+                ("press", C.c_double * 2)]
+
+
 _SIGS = {
     "epsr_last_error": (C.c_char_p, []),
     "epsr_version": (C.c_char_p, []),
@@ -83,6 +108,8 @@ _SIGS = {
                                            P]),
     "epsr_fit_expansion_batch_scratch_bytes": (I64, [I32, I32, I32]),
     "epsr_fit_expansion_scratch_bytes": (I64, [I32, I32]),
+    "epsr_iteration_scratch_bytes": (I64, [C.POINTER(Iteration)]),
+    "epsr_iteration_step": (C.c_int, [C.POINTER(Iteration), C.POINTER(IterationReport), P]),
 }
 
 _lib = None

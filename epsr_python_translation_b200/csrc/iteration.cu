@@ -1,0 +1,158 @@
+// iteration.cu -- one EPSR iteration of the pair path on one box, driven from native code.
+//
+// The iteration body of runepsr17 (epsr_standalone_rev3.py:1235-1842) restricted to this
+// path, in its order: the cell list (:1259), fmolec1 (:1265), ntimes molfit cycles
+// (:1280-1318), atogen (:1397), gensq (:1400), the per-data-set differences of ptgnsq
+// (:3844-3867), press (:1842 -> ato_manipulation_rev4.py:3903), fit_expansion for every
+// data set (ptgnsq :3936) and stog of the simulated S(Q) (:1987).  Every stage is the C ABI
+// routine of that name, launched on the caller's stream from this thread, so a host that
+// advances many boxes on many threads does no per-launch work in an interpreter.  Host
+// reads happen where the routines need them (the cell list's region size, store and
+// capacity counts, the fit's per-set scalars).
+#include <string.h>
+
+#include "common.cuh"
+
+using namespace epsr;
+
+namespace {
+
+inline int64_t imax64(int64_t a, int64_t b) { return a > b ? a : b; }
+
+int cell_dims(const epsr_iteration_t *it, int32_t dims[4]) {
+    return epsr_cell_dims(it->nmolcell, it->box->nmol, it->lat6, dims);
+}
+
+void mark(const epsr_iteration_t *it, int stage, int end, cudaStream_t s) {
+    void *ev = it->stage_events[2 * stage + end];
+    if (ev) cudaEventRecord((cudaEvent_t)ev, s);
+}
+
+}  // namespace
+
+extern "C" int64_t epsr_iteration_scratch_bytes(const epsr_iteration_t *it) {
+    if (!it || !it->box) return -1;
+    int32_t dims[4];
+    if (cell_dims(it, dims)) return -1;
+    const epsr_box_t *b = it->box;
+    const int ldq = it->nq + 1;
+    int64_t n = epsr_fmolec1_scratch_bytes(b->nmol, dims[3], it->store_m);
+    n = imax64(n, epsr_molfit_scratch_bytes(b->nmol, b->natom, it->store_m));
+    n = imax64(n, epsr_atogen_scratch_bytes(b->nmol, b->natom, b->nmoltype, b->ntype));
+    n = imax64(n, epsr_press_scratch_bytes(b->nmol, it->store_m));
+    n = imax64(n, epsr_fit_expansion_batch_scratch_bytes(it->ndata, it->nq, it->nterms));
+    n = imax64(n, epsr_stog_scratch_bytes(b->npairs, ldq));
+    return n;
+}
+
+extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_report_t *rep, void *stream) {
+    if (!it || !rep || !it->box || !it->mc || !it->scratch) {
+        epsr_set_error("epsr_iteration_step: null pointer");
+        return EPSR_ERR_ARG;
+    }
+    const int64_t need = epsr_iteration_scratch_bytes(it);
+    if (need < 0 || it->scratch_bytes < need) {
+        epsr_set_error("epsr_iteration_step: scratch too small (%lld < %lld bytes)", (long long)it->scratch_bytes,
+                       (long long)need);
+        return EPSR_ERR_CAPACITY;
+    }
+    memset(rep, 0, sizeof(*rep));
+    const epsr_box_t *b = it->box;
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc;
+
+    // ---- cell list (initialise_cellneighbourlist)
+    mark(it, 0, 0, s);
+    epsr_cells_t cells;
+    memset(&cells, 0, sizeof(cells));
+    cells.molcellno = it->cell_molcellno;
+    cells.cell_start = it->cell_start;
+    cells.cell_mols = it->cell_mols;
+    cells.offsets = it->cell_offsets;
+    rc = epsr_cell_list(b->xadd, b->yadd, b->zadd, b->nmol, it->nmolcell, it->rmax, it->lat6, it->lat9, &cells,
+                        it->cell_scratch, it->cell_scratch_n, stream);
+    if (rc) return rc;
+    rep->nnbrefmax = cells.nnbrefmax;
+    if (cells.nnbrefmax > it->store_m) {   // nothing of the box has changed yet
+        epsr_set_error("epsr_iteration_step: region size %d exceeds the store's %d slots per molecule",
+                       cells.nnbrefmax, it->store_m);
+        return EPSR_ERR_CAPACITY;
+    }
+    mark(it, 0, 1, s);
+
+    // ---- fmolec1: the pair store
+    mark(it, 1, 0, s);
+    epsr_store_t store;
+    store.nnbrefmax = cells.nnbrefmax;
+    store.capacity = it->store_capacity;
+    store.nergpairm = it->nergpairm;
+    store.molergpair = it->molergpair;
+    store.ergpairref = it->ergpairref;
+    store.ergpair = it->ergpair;
+    store.nergpair = it->nergpair;
+    store.mirror = it->mirror;
+    rc = epsr_fmolec1(b, &cells, it->eintra, &store, it->scratch, it->scratch_bytes, it->strict, rep->ftest, stream);
+    if (rc) return rc;
+    mark(it, 1, 1, s);
+
+    // ---- molfit cycles
+    mark(it, 2, 0, s);
+    epsr_mc_t *mc = it->mc;
+    mc->strict = it->strict;
+    mc->cos_override = nullptr;
+    for (int t = 0; t < it->ntimes; ++t) {
+        rc = epsr_molfit(b, &cells, &store, mc, it->scratch, it->scratch_bytes, stream);
+        if (rc) return rc;
+    }
+    mark(it, 2, 1, s);
+
+    // ---- atogen: the partial g(r) histograms
+    mark(it, 3, 0, s);
+    EPSR_CUDA(cudaMemsetAsync(it->wav, 0, sizeof(float) * 2 * (size_t)b->npairs * it->ldw, s));
+    EPSR_CUDA(cudaMemsetAsync(it->potex, 0, sizeof(float) * (size_t)b->npairs, s));
+    int32_t ngr = it->ngrsamples;
+    rc = epsr_atogen(b, it->npt1, it->sizefactor, it->dmax, it->rminex, it->cfrac, it->ycoh, it->n1extr, it->n2extr,
+                     it->natomr, &ngr, mc->ran1, it->wav, it->ldw, it->potex, it->counts, it->scratch,
+                     it->scratch_bytes, stream);
+    if (rc) return rc;
+    rep->ngrsamples = ngr;
+    rep->pair_updates = epsr_atogen_last_pair_updates();
+    mark(it, 3, 1, s);
+
+    // ---- gensq and the data-set differences the fit works on
+    mark(it, 4, 0, s);
+    const int ldq = it->nq + 1;
+    rc = epsr_gensq(it->nq, b->npairs, it->npt1, it->wav, it->ldw, it->foqols, it->foqols_sj, it->foqols_si, it->ycoh,
+                    it->n2extr, it->natomsphere, it->sofq, stream);
+    if (rc) return rc;
+    const float *inter = it->sofq + (size_t)b->npairs * ldq;   // intermolecular S(Q) per pair
+    rc = epsr_ptgnsq_difference(it->ndata, b->npairs, it->nq, it->data, it->cwt, inter, it->dt, stream);
+    if (rc) return rc;
+    mark(it, 4, 1, s);
+
+    // ---- press
+    mark(it, 5, 0, s);
+    rc = epsr_press(b, &store, it->npt1, it->scratch, it->scratch_bytes, it->strict, rep->press, stream);
+    if (rc) return rc;
+    mark(it, 5, 1, s);
+
+    // ---- fit_expansion for every data set, one launch
+    mark(it, 6, 0, s);
+    for (int d = 0; d < it->ndata; ++d)   // stepr carries over; acceptr, rejrat, chisq start at 0
+        for (int k = 1; k < 4; ++k) it->fit_scal_host[4 * d + k] = 0.0f;
+    EPSR_CUDA(cudaMemsetAsync(it->fit_wt, 0, sizeof(float) * (size_t)it->ndata * (it->nterms + 1), s));
+    EPSR_CUDA(cudaMemsetAsync(it->fit_yout, 0, sizeof(float) * (size_t)it->ndata * ldq, s));
+    rc = epsr_fit_expansion_batch(it->ndata, it->dt, it->expr, it->fit_yout, it->fit_wt, it->fit_wtold,
+                                  it->fit_scal_host, 1, it->nq, it->ncfirst, it->nterms, it->nits, it->nfreq, mc->ran1,
+                                  it->scratch, it->scratch_bytes, it->strict, it->fit_trials_host, stream);
+    if (rc) return rc;
+    mark(it, 6, 1, s);
+
+    // ---- stog of the simulated intermolecular S(Q)
+    mark(it, 7, 0, s);
+    rc = epsr_stog(it->rho, it->q, ldq, inter, it->r, it->nr, b->npairs, it->nqmin, it->nqmax, it->xwt, it->gofr,
+                   it->scratch, it->scratch_bytes, stream);
+    if (rc) return rc;
+    mark(it, 7, 1, s);
+    return EPSR_OK;
+}

@@ -13,7 +13,9 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import transforms
+import ctypes as C
+
+from . import _lib, transforms
 from .box import BoxArrays, Ran1State, trsteps
 from .configs import Workload
 from .device import DeviceBox, press_scalars
@@ -23,9 +25,11 @@ STAGES = ("cells", "fmolec1", "molfit", "atogen", "gensq", "press", "fit_expansi
 
 
 class EpsrIteration:
-    def __init__(self, wl: Workload, device="cuda", strict=False, ran1_seed=0):
+    def __init__(self, wl: Workload, device="cuda", strict=False, ran1_seed=0, native=False):
         self.wl = wl
         self.strict = strict
+        self.native = native          # steps after the first through epsr_iteration_step
+        self._plan = None
         self.box = BoxArrays.from_system(wl.system)
         self.d = DeviceBox(self.box, device=device)
         b = self.box
@@ -62,6 +66,18 @@ class EpsrIteration:
         self.events[stage][1 if end else 0].record()
 
     def step(self):
+        if self.native and self._plan is not None:
+            try:
+                return self._step_native()
+            except _lib.EpsrGpuError as e:
+                if e.code != 3:             # capacity: this iteration sizes its buffers below
+                    raise
+                self._plan = None
+        self._step_python()
+        if self.native:
+            self._build_plan()
+
+    def _step_python(self):
         wl, d, b = self.wl, self.d, self.box
         self._mark("cells")
         d.cell_list(wl.nmolcell, b.sepmax)
@@ -102,6 +118,85 @@ class EpsrIteration:
         self.gofr = transforms.stog(float(b.natom) / float(wl.system.L) ** 3, self.q, inter, self.r, self.nqmin,
                                     self.nqmax, self.xwt)
         self._mark("stog", True)
+
+    # ------------------------------------------------------------------ native driver
+    def _build_plan(self):
+        """The epsr_iteration_t of this box, on the buffers the Python step sized (device
+        tensors kept on self so the pointers stay valid)."""
+        wl, d, b = self.wl, self.d, self.box
+        nq, ld = wl.nq, b.npt + 1
+        ndata = self.data.shape[0]
+        dev = d.dev
+        P = lambda t: C.c_void_p(t.data_ptr())
+        it = _lib.Iteration()
+        it.box = C.cast(C.pointer(d.cbox), C.c_void_p)
+        it.mc = C.cast(C.pointer(d.cmc), C.c_void_p)
+        it.nmolcell, it.rmax = wl.nmolcell, float(np.float32(b.sepmax))
+        for i in range(6):
+            it.lat6[i] = float(b.lat6[i])
+        for i in range(9):
+            it.lat9[i] = float(np.asarray(b.lat9, np.float32).reshape(-1)[i])
+        it.cell_molcellno, it.cell_start, it.cell_mols, it.cell_offsets = (
+            P(t) for t in (d.c_molcellno, d.c_start, d.c_mols, d.c_off))
+        it.cell_scratch, it.cell_scratch_n = P(d._c_scr), d._c_scr.numel()
+        it.store_m = d.s_mol.numel() // b.nmol
+        it.store_capacity = d.s_erg.numel()
+        it.nergpairm, it.molergpair, it.ergpairref, it.mirror, it.nergpair, it.ergpair = (
+            P(t) for t in (d.s_nergpairm, d.s_mol, d.s_ref, d.s_mirror, d.s_n, d.s_erg))
+        it.eintra = P(d.eintra)
+        it.ntimes = wl.ntimes
+        it.npt1, it.natomr, it.ngrsamples = b.npt1, b.natomr, wl.ngrsamples
+        it.sizefactor, it.dmax = 1.0, float(b.dmax)
+        self._n_wav = torch.zeros(2 * b.npairs * ld, dtype=torch.float32, device=dev)
+        self._n_potex = torch.zeros(b.npairs, dtype=torch.float32, device=dev)
+        self._n_counts = torch.zeros(2 * b.npairs * ld + b.npairs, dtype=torch.int64, device=dev)
+        it.rminex, it.cfrac, it.ycoh, it.n1extr, it.n2extr = (
+            P(t) for t in (self.rminex, d.cfrac, self.ycoh, d.n1extr, d.n2extr))
+        it.wav, it.ldw, it.potex, it.counts = P(self._n_wav), ld, P(self._n_potex), P(self._n_counts)
+        self._n_sofq = torch.zeros(2 * b.npairs * (nq + 1), dtype=torch.float32, device=dev)
+        it.nq, it.ndata = nq, ndata
+        it.foqols, it.foqols_sj, it.foqols_si = P(self.foqols), nq + 1, 1
+        it.natomsphere, it.sofq = P(self.natomsphere), P(self._n_sofq)
+        it.data, it.cwt, it.dt = P(self.data), P(self.weights), P(self._dt)
+        self._n_wt = torch.zeros(ndata, wl.nterms + 1, dtype=torch.float32, device=dev)
+        self._n_wtold = self.pwtold.clone()
+        self._n_yout = torch.zeros(ndata, nq + 1, dtype=torch.float32, device=dev)
+        self._n_scal = np.zeros((ndata, 4), np.float32)
+        self._n_trials = np.zeros(ndata, np.int64)
+        it.expr, it.nterms, it.ncfirst, it.nits, it.nfreq = P(self.expr), wl.nterms, 1, 1000, 10
+        it.fit_wt, it.fit_wtold, it.fit_yout = P(self._n_wt), P(self._n_wtold), P(self._n_yout)
+        it.fit_scal_host = self._n_scal.ctypes.data_as(C.c_void_p)
+        it.fit_trials_host = self._n_trials.ctypes.data_as(C.c_void_p)
+        self._n_gofr = torch.zeros(b.npairs, self.r.numel(), dtype=torch.float32, device=dev)
+        it.rho = float(np.float32(float(b.natom) / float(wl.system.L) ** 3))
+        it.q, it.r, it.nr = P(self.q), P(self.r), self.r.numel() - 1
+        it.nqmin, it.nqmax, it.xwt, it.gofr = P(self.nqmin), P(self.nqmax), P(self.xwt), P(self._n_gofr)
+        it.strict = 1 if self.strict else 0
+        for k, name in enumerate(STAGES):       # the Python step has created these events
+            it.stage_events[2 * k] = self.events[name][0].cuda_event
+            it.stage_events[2 * k + 1] = self.events[name][1].cuda_event
+        nb = int(d.lib.epsr_iteration_scratch_bytes(C.byref(it)))
+        self._n_scratch = torch.empty(max(nb, 256), dtype=torch.uint8, device=dev)
+        it.scratch, it.scratch_bytes = P(self._n_scratch), self._n_scratch.numel()
+        self._plan = it
+        self._rep = _lib.IterationReport()
+
+    def _step_native(self):
+        wl, b = self.wl, self.box
+        self._n_scal[:, 0] = self.stepp
+        _lib.check(self.d.lib.epsr_iteration_step(C.byref(self._plan), C.byref(self._rep),
+                                                  C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        r = self._rep
+        self.d.nnbrefmax = int(r.nnbrefmax)
+        self.ftest = (np.float32(r.ftest[0]), np.float32(r.ftest[1]))
+        self.pair_updates = int(r.pair_updates)
+        self.energy, self.pressc = press_scalars(b.nmol, np.float32(r.press[0]), float(r.press[1]), b.simt,
+                                                 self.volume)
+        self.pwtold = self._n_wtold
+        self.stepp = self._n_scal[:, 0].copy()
+        self.fit_trials = int(self._n_trials.sum())
+        self.sofq = self._n_sofq.view(2, b.npairs, wl.nq + 1)
+        self.gofr = self._n_gofr
 
     def stage_ms(self):
         torch.cuda.synchronize()

@@ -271,6 +271,81 @@ int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const float *expr,
                              int64_t scratch_bytes, int32_t strict, int64_t *trials_host, void *stream);
 int64_t epsr_fit_expansion_batch_scratch_bytes(int32_t nprob, int32_t npt, int32_t nterms);
 
+/* ------------------------------------------------------------------ one iteration */
+
+/* One EPSR iteration of the path on one box, driven from native code: the iteration body of
+ * runepsr17 (epsr_standalone_rev3.py:1235-1842) restricted to this path -- cell list,
+ * fmolec1, ntimes molfit cycles, atogen, gensq, the per-data-set differences of ptgnsq,
+ * press, fit_expansion over all data sets, stog -- each stage the routine of that name
+ * above, launched on `stream` from the calling thread.  The caller owns every buffer. */
+typedef struct {
+    const epsr_box_t *box;
+    epsr_mc_t *mc;                    /* mc->ran1: the one ran1 stream of every stage */
+    /* cell list */
+    int32_t nmolcell;
+    float rmax;                       /* sepmax (epsr_standalone_rev3.py:1259), box units */
+    float lat6[6], lat9[9];           /* host */
+    int32_t *cell_molcellno, *cell_start, *cell_mols, *cell_offsets;
+    int32_t *cell_scratch;            /* int32 elements, see epsr_cell_list */
+    int64_t cell_scratch_n;
+    /* pair store: rows of store_m slots, store_capacity shared energies */
+    int32_t store_m, store_capacity;
+    int32_t *nergpairm, *molergpair, *ergpairref, *mirror, *nergpair;
+    float *ergpair;
+    const float *eintra;              /* [nmol] intramolecular energies */
+    int32_t ntimes;                   /* molfit cycles per iteration */
+    /* atogen */
+    int32_t npt1, natomr, ngrsamples;
+    float sizefactor, dmax;
+    const float *rminex, *cfrac, *ycoh;
+    const int32_t *n1extr, *n2extr;
+    float *wav;                       /* [2][npairs][ldw] */
+    int32_t ldw;
+    float *potex;                     /* [npairs] */
+    unsigned long long *counts;       /* [2*npairs*ldw + npairs] */
+    /* gensq and the data-set differences */
+    int32_t nq, ndata;
+    const float *foqols;
+    int64_t foqols_sj, foqols_si;
+    const float *natomsphere;
+    float *sofq;                      /* [2][npairs][nq+1] */
+    const float *data, *cwt;          /* [ndata][nq+1], [ndata][npairs] */
+    float *dt;                        /* [ndata][nq+1] -(data - weighted S(Q)) */
+    /* fit_expansion */
+    const float *expr;
+    int32_t nterms, ncfirst, nits, nfreq;
+    float *fit_wt, *fit_wtold, *fit_yout;   /* [ndata][nterms+1], same, [ndata][nq+1] */
+    float *fit_scal_host;             /* [ndata][4] host: stepr in/out; acceptr, rejrat, chisq out */
+    int64_t *fit_trials_host;         /* [ndata] host */
+    /* stog */
+    float rho;
+    const float *q;                   /* [nq+1] */
+    const float *r;                   /* [nr+1] */
+    int32_t nr;
+    const int32_t *nqmin, *nqmax;     /* [npairs] */
+    const float *xwt;                 /* [npairs] */
+    float *gofr;                      /* [npairs][nr+1] */
+    /* one scratch block shared by the stages (epsr_iteration_scratch_bytes) */
+    void *scratch;
+    int64_t scratch_bytes;
+    int32_t strict;
+    void *stage_events[16];           /* NULL or CUDA events recorded at the start and end of
+                                         cells, fmolec1, molfit, atogen, gensq, press, fit, stog */
+} epsr_iteration_t;
+
+typedef struct {
+    int32_t nnbrefmax;                /* region size of this iteration's cell list */
+    float ftest[2];                   /* fmolec1's ftest, ftestb */
+    int32_t ngrsamples;               /* atogen's sampled origins */
+    int64_t pair_updates;             /* atogen's pair-updates */
+    double press[2];                  /* press sums: float32 energy sum, double virial sum */
+} epsr_iteration_report_t;
+
+int64_t epsr_iteration_scratch_bytes(const epsr_iteration_t *it);
+/* Returns EPSR_ERR_CAPACITY, before anything of the box has changed, when this iteration's
+ * cell list needs more than store_m slots per molecule (rep->nnbrefmax says how many). */
+int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_report_t *rep, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
