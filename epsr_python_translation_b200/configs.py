@@ -522,9 +522,15 @@ class Workload:
         return int(self.q.shape[0] - 1)
 
 
-def make_workload(name="c2_mixture", seed=1, nq=600, qstep=0.05, nterms=116, ndata=3, ntimes=5):
-    """Configuration C2: 200 DMSO + 400 water, 5 MC sweeps per iteration, three isotope
-    datasets (deuterated, protiated, 50:50), a 116-term Poisson-like EP basis."""
+def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, ndata=None, ntimes=5):
+    """One iteration's inputs on a named configuration, 5 MC sweeps per iteration and a
+    116-term Poisson-like EP basis.  C2 (c2_mixture): 200 DMSO + 400 water, three isotope
+    data sets (deuterated, protiated, 50:50), Q to 30 A^-1 (600 points).  C3 (c3_water):
+    20,000 water, one data set, Q to 50 A^-1 (1,000 points).  C1 (c1_water): 100 water."""
+    if nq is None:
+        nq = 1000 if name == "c3_water" else 600
+    if ndata is None:
+        ndata = 1 if name == "c3_water" else 3
     if name == "c2_mixture":
         s = c2_mixture(seed=seed)
     elif name == "c1_water":

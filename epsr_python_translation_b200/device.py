@@ -198,9 +198,10 @@ class DeviceBox:
         torch.cuda.synchronize()
         M = self.nnbrefmax
         n = int(self.s_n.item())
+        nm = self.host.nmol * M          # the buffers may be larger, kept from a larger region size
         return dict(nnbrefmax=M, nergpair=n, nergpairm=self.s_nergpairm.cpu().numpy(),
-                    molergpair=self.s_mol.cpu().numpy().reshape(-1, M), ergpairref=self.s_ref.cpu().numpy().reshape(-1, M),
-                    ergpair=self.s_erg[:n].cpu().numpy())
+                    molergpair=self.s_mol[:nm].cpu().numpy().reshape(-1, M),
+                    ergpairref=self.s_ref[:nm].cpu().numpy().reshape(-1, M), ergpair=self.s_erg[:n].cpu().numpy())
 
     # ------------------------------------------------------------------ molfit
     def mc_setup(self, *, rejrate, stepr, stepm, wholerot, wholetrans, internrot=None, interntrans=None,
