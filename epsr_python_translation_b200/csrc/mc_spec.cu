@@ -32,6 +32,7 @@ constexpr int SP_W = 32;        // near window of the resolver (moves)
 constexpr int SP_RING = 64;     // far-sum ring (moves)
 constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
 constexpr int SP_ET = 256;      // threads of a move's energy CTA (its stored partners)
+constexpr int SP_RT = 1024;     // resolver CTA: the resolver warp and 31 far-sum helper warps
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
 
 struct SpecDev {
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
 }
 
 // ----------------------------------------------------------------- resolve
-__global__ void __launch_bounds__(512) spec_resolve_kernel(SpecDev S) {
+__global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
     extern __shared__ unsigned accbits_raw[];
     volatile unsigned *accbits = accbits_raw;
     __shared__ volatile int progress;
@@ -434,10 +435,19 @@ __global__ void __launch_bounds__(512) spec_resolve_kernel(SpecDev S) {
             const int m = S.visit[k];
             const int nn = S.nergpairm[m];
             const size_t row = (size_t)m * S.M;
+            // two partners per lane in flight; the correction is read whether or not it applies
+            // (a stale value is masked), so its load does not wait for the partner's index
             double sum = 0.0;
-            for (int s = 1 + lane; s < nn; s += 32) {
-                const int kp = S.fv[row + s];
-                if (kp >= 0 && ((accbits[kp >> 5] >> (kp & 31)) & 1u)) sum += S.farc[row + s];
+            for (int s = 1 + lane; s < nn; s += 64) {
+                const bool h2 = s + 32 < nn;
+                const int kp0 = S.fv[row + s];
+                const int kp1 = h2 ? S.fv[row + s + 32] : -1;
+                const double f0 = S.farc[row + s];
+                const double f1 = h2 ? S.farc[row + s + 32] : 0.0;
+                const bool u0 = kp0 >= 0 && ((accbits[kp0 >> 5] >> (kp0 & 31)) & 1u);
+                const bool u1 = kp1 >= 0 && ((accbits[kp1 >> 5] >> (kp1 & 31)) & 1u);
+                sum += u0 ? f0 : 0.0;
+                sum += u1 ? f1 : 0.0;
             }
             sum = warp_sum_d(sum);
             if (lane == 0) {
@@ -712,7 +722,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     spec_corr_kernel<<<N, 128, 0, s>>>(S);
     const size_t bits = sizeof(unsigned) * (((size_t)N + 31) / 32);
     if (bits > 48 * 1024) EPSR_SMEM_OPTIN(spec_resolve_kernel);
-    spec_resolve_kernel<<<1, 512, bits, s>>>(S);
+    spec_resolve_kernel<<<1, SP_RT, bits, s>>>(S);
     spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
     spec_commit_store_kernel<<<N, 128, 0, s>>>(S);
     spec_epilogue_kernel<<<1, 32, 0, s>>>(S);
