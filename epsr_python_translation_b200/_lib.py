@@ -69,7 +69,9 @@ class Iteration(C.Structure):
                 ("expr", P), ("nterms", I32), ("ncfirst", I32), ("nits", I32), ("nfreq", I32),
                 ("fit_wt", P), ("fit_wtold", P), ("fit_yout", P), ("fit_scal_host", P), ("fit_trials_host", P),
                 ("rho", F32), ("q", P), ("r", P), ("nr", I32), ("nqmin", P), ("nqmax", P), ("xwt", P),
-                ("gofr", P), ("scratch", P), ("scratch_bytes", I64), ("strict", I32), ("stage_events", P * 16)]
+                ("gofr", P), ("nsum", I32), ("soqintra", P), ("soqinter", P), ("sq2intra", P), ("sq2inter", P),
+                ("gorintra", P), ("gorinter", P), ("gr2intra", P), ("gr2inter", P), ("entsig", P),
+                ("scratch", P), ("scratch_bytes", I64), ("strict", I32), ("stage_events", P * 20)]
 
 
 class IterationReport(C.Structure):
@@ -101,6 +103,8 @@ _SIGS = {
     "epsr_press_scratch_bytes": (I64, [I32, I32]),
     "epsr_gensq": (C.c_int, [I32, I32, I32, P, I32, P, I64, I64, P, P, P, P, P]),
     "epsr_ptgnsq_difference": (C.c_int, [I32, I32, I32, P, P, P, P, P]),
+    "epsr_sumgr": (C.c_int, [I32, I32, P, I32, P, C.c_double, C.c_double, P, P, P, P, P, P]),
+    "epsr_sumsq": (C.c_int, [I32, I32, P, I32, C.c_double, C.c_double, P, P, P, P, P]),
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),
     "epsr_stog_scratch_bytes": (I64, [I32, I32]),
     "epsr_fit_expansion": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, I32, P, P]),

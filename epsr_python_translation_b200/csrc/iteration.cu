@@ -4,7 +4,8 @@
 // path, in its order: the cell list (:1259), fmolec1 (:1265), ntimes molfit cycles
 // (:1280-1318), atogen (:1397), gensq (:1400), the per-data-set differences of ptgnsq
 // (:3844-3867), press (:1842 -> ato_manipulation_rev4.py:3903), fit_expansion for every
-// data set (ptgnsq :3936) and stog of the simulated S(Q) (:1987).  Every stage is the C ABI
+// data set (ptgnsq :3936), the running averages sumsq and sumgr (:1611-1642) and stog of the
+// simulated S(Q) (:1987).  Every stage is the C ABI
 // routine of that name, launched on the caller's stream from this thread, so a host that
 // advances many boxes on many threads does no per-launch work in an interpreter.  Host
 // reads happen where the routines need them (the cell list's region size, store and
@@ -148,11 +149,27 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
     if (rc) return rc;
     mark(it, 6, 1, s);
 
-    // ---- stog of the simulated intermolecular S(Q)
+    // ---- running averages of S(Q) and g(r) (runepsr17 :1611-1642)
     mark(it, 7, 0, s);
+    if (it->nsum < 1) {
+        epsr_set_error("epsr_iteration_step: nsum %d < 1", it->nsum);
+        return EPSR_ERR_ARG;
+    }
+    const double fc1 = (double)(1.0f / (float)it->nsum);
+    const double fc2 = (double)(float)(it->nsum - 1) * fc1;
+    rc = epsr_sumsq(it->nq, b->npairs, it->sofq, ldq, fc1, fc2, it->soqintra, it->soqinter, it->sq2intra,
+                    it->sq2inter, stream);
+    if (rc) return rc;
+    rc = epsr_sumgr(it->npt1, b->npairs, it->wav, it->ldw, it->ycoh, fc1, fc2, it->gorintra, it->gorinter,
+                    it->gr2intra, it->gr2inter, it->entsig, stream);
+    if (rc) return rc;
+    mark(it, 7, 1, s);
+
+    // ---- stog of the simulated intermolecular S(Q)
+    mark(it, 8, 0, s);
     rc = epsr_stog(it->rho, it->q, ldq, inter, it->r, it->nr, b->npairs, it->nqmin, it->nqmax, it->xwt, it->gofr,
                    it->scratch, it->scratch_bytes, stream);
     if (rc) return rc;
-    mark(it, 7, 1, s);
+    mark(it, 8, 1, s);
     return EPSR_OK;
 }

@@ -49,15 +49,16 @@ from .box import BoxArrays, Ran1State, trsteps
 
 f32 = np.float32
 ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit", "atogen", "stog", "gensq", "fit_expansion",
-            "press", "en_change", "en_mole_pair")
+            "press", "sumgr", "sumsq", "en_change", "en_mole_pair")
 # en_change / en_mole_pair are per-molecule calls: rerouting them makes every host caller
 # (including host fallbacks) launch one kernel per call, so they are installed only on request.
-DEFAULT_ROUTINES = ROUTINES[:8]
+DEFAULT_ROUTINES = ROUTINES[:10]
 # module that owns each routine in the reference
 OWNER = {"initialise_cellneighbourlist": "cellneighbourlist", "fmolec1": "ato_manipulation_rev4",
          "atogen": "ato_manipulation_rev4", "stog": "ato_manipulation_rev4", "press": "ato_manipulation_rev4",
          "molfit": "molfit",
-         "en_change": "molfit", "en_mole_pair": "molfit", "gensq": "program", "fit_expansion": "program"}
+         "en_change": "molfit", "en_mole_pair": "molfit", "gensq": "program", "fit_expansion": "program",
+         "sumgr": "program", "sumsq": "program"}
 
 
 def _fortran(shape, dtype):
@@ -492,6 +493,41 @@ class PairPath:
         o = out.cpu().numpy().reshape(2, npairs, nq + 1)
         sofq[1:3, 1:nq + 1, 1:npairs + 1] = o[:, :, 1:].transpose(0, 2, 1)
         return None
+
+    def _running_sums(self, names, n, first, host_arrays, sample, call):
+        """Upload the epsr16 accumulators (rows first..n of the reference's (point, pair)
+        arrays), run `call` on them and the (2, points, pairs) sample on the device, write
+        the rows back in place."""
+        npairs = int(self.c.molecom.npairs)
+        ld = n + 1
+        acc = {k: torch.from_numpy(np.ascontiguousarray(np.asarray(host_arrays[k])[:ld, 1:npairs + 1].T, f32)).cuda()
+               for k in names}
+        w = np.ascontiguousarray(np.asarray(sample)[1:3, :ld, 1:npairs + 1].transpose(0, 2, 1), f32)
+        call(torch.from_numpy(w.reshape(-1)).cuda(), acc)
+        for k in names:
+            host_arrays[k][first:ld, 1:npairs + 1] = acc[k].cpu().numpy()[:, first:ld].T
+        return None
+
+    def sumgr(self, nz, wav):
+        """epsr_standalone_rev3.py:3578-3637: updates the running g(r) means, error bars and
+        zero limits of epsr16 in place, with the weights fc1, fc2 of sumvalues."""
+        c = self.c
+        e16, sv = c.epsr16, c.sumvalues
+        nz = int(nz)
+        yc = torch.from_numpy(np.ascontiguousarray(np.asarray(e16.ycoh)[: nz + 1], f32)).cuda()
+        arrays = {k: getattr(e16, k) for k in transforms.GR_ARRAYS}
+        return self._running_sums(transforms.GR_ARRAYS, nz, 1, arrays, wav,
+                                  lambda w, acc: transforms.sumgr(nz, w, yc, float(sv.fc1), float(sv.fc2), acc))
+
+    def sumsq(self, nq, qwind):
+        """epsr_standalone_rev3.py:3642-3677: updates the running S(Q) means and error bars
+        of epsr16 in place."""
+        c = self.c
+        e16, sv = c.epsr16, c.sumvalues
+        nq = int(nq)
+        arrays = {k: getattr(e16, k) for k in transforms.SQ_ARRAYS}
+        return self._running_sums(transforms.SQ_ARRAYS, nq, 1, arrays, qwind,
+                                  lambda w, acc: transforms.sumsq(nq, w, float(sv.fc1), float(sv.fc2), acc))
 
     def stog(self, rho, q, sofq, r, gofr, nqmin, nqmax, nr, npairs, nqdim, nrdim, npdim, xwt):
         """ato_manipulation_rev4.py:4067-4110: fills gofr(nr, npairs) in place."""

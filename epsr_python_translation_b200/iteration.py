@@ -21,7 +21,7 @@ from .configs import Workload
 from .device import DeviceBox, press_scalars
 
 f32 = np.float32
-STAGES = ("cells", "fmolec1", "molfit", "atogen", "gensq", "press", "fit_expansion", "stog")
+STAGES = ("cells", "fmolec1", "molfit", "atogen", "gensq", "press", "fit_expansion", "sums", "stog")
 
 
 class EpsrIteration:
@@ -52,6 +52,13 @@ class EpsrIteration:
         self.pwtold = torch.zeros(ndata, wl.nterms + 1, dtype=torch.float32, device=dev)
         self.stepp = np.full(ndata, f32(0.01), f32)
         self._fit_scratch = torch.empty(4096, dtype=torch.uint8, device=dev)
+        # running averages of S(Q) and g(r) with their error bars (epsr16 soq*/sq2*, gor*/gr2*,
+        # entsig), accumulated every iteration as runepsr17 does (:1611-1642)
+        self.nsum = 0
+        self.sums_sq = {k: torch.zeros(b.npairs, wl.nq + 1, dtype=torch.float32, device=dev)
+                        for k in transforms.SQ_ARRAYS}
+        self.sums_gr = {k: torch.zeros(b.npairs, b.npt + 1, dtype=torch.float32, device=dev)
+                        for k in transforms.GR_ARRAYS}
         self.r = torch.from_numpy(b.x[: b.npt1 + 1].copy()).to(dev)
         self.nqmin = torch.full((b.npairs,), 2, dtype=torch.int32, device=dev)
         self.nqmax = torch.full((b.npairs,), wl.nq, dtype=torch.int32, device=dev)
@@ -114,6 +121,13 @@ class EpsrIteration:
         self.stepp = res["stepr"]
         self.fit_trials = int(res["trials"].sum())
         self._mark("fit_expansion", True)
+        self._mark("sums")
+        self.nsum += 1
+        fc1 = float(np.float32(1.0) / np.float32(self.nsum))
+        fc2 = float(np.float32(self.nsum - 1)) * fc1
+        transforms.sumsq(nq, sofq, fc1, fc2, self.sums_sq)
+        transforms.sumgr(b.npt1, d.a_wav, self.ycoh, fc1, fc2, self.sums_gr)
+        self._mark("sums", True)
         self._mark("stog")
         self.gofr = transforms.stog(float(b.natom) / float(wl.system.L) ** 3, self.q, inter, self.r, self.nqmin,
                                     self.nqmax, self.xwt)
@@ -171,6 +185,9 @@ class EpsrIteration:
         it.rho = float(np.float32(float(b.natom) / float(wl.system.L) ** 3))
         it.q, it.r, it.nr = P(self.q), P(self.r), self.r.numel() - 1
         it.nqmin, it.nqmax, it.xwt, it.gofr = P(self.nqmin), P(self.nqmax), P(self.xwt), P(self._n_gofr)
+        it.soqintra, it.soqinter, it.sq2intra, it.sq2inter = (P(self.sums_sq[k]) for k in transforms.SQ_ARRAYS)
+        it.gorintra, it.gorinter, it.gr2intra, it.gr2inter, it.entsig = (
+            P(self.sums_gr[k]) for k in transforms.GR_ARRAYS)
         it.strict = 1 if self.strict else 0
         for k, name in enumerate(STAGES):       # the Python step has created these events
             it.stage_events[2 * k] = self.events[name][0].cuda_event
@@ -184,6 +201,7 @@ class EpsrIteration:
     def _step_native(self):
         wl, b = self.wl, self.box
         self._n_scal[:, 0] = self.stepp
+        self._plan.nsum = self.nsum + 1
         _lib.check(self.d.lib.epsr_iteration_step(C.byref(self._plan), C.byref(self._rep),
                                                   C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         r = self._rep
@@ -195,6 +213,7 @@ class EpsrIteration:
         self.pwtold = self._n_wtold
         self.stepp = self._n_scal[:, 0].copy()
         self.fit_trials = int(self._n_trials.sum())
+        self.nsum += 1
         self.sofq = self._n_sofq.view(2, b.npairs, wl.nq + 1)
         self.gofr = self._n_gofr
 

@@ -54,6 +54,33 @@ def ptgnsq_difference(data, cwt, qwind, out=None):
     return out
 
 
+GR_ARRAYS = ("gorintra", "gorinter", "gr2intra", "gr2inter", "entsig")
+SQ_ARRAYS = ("soqintra", "soqinter", "sq2intra", "sq2inter")
+
+
+def sumgr(nz, wav, ycoh, fc1, fc2, acc):
+    """sumgr epsr_standalone_rev3.py:3578-3637 on the device: folds the new partial g(r) into
+    the running means and error bars with weights fc2 (old) and fc1 (new) and recomputes the
+    zero limit.  wav (device, 2*npairs*ldw); ycoh (device, ldw); acc a dict of device
+    float32 tensors (npairs, ldw) named as GR_ARRAYS, updated in place."""
+    lib = _lib.load(require_device=True)
+    npairs, ldw = acc["gorintra"].shape
+    check(lib.epsr_sumgr(int(nz), npairs, _p(wav), ldw, _p(ycoh), float(fc1), float(fc2),
+                         *(_p(acc[k]) for k in GR_ARRAYS), _s()))
+    return acc
+
+
+def sumsq(nq, qwind, fc1, fc2, acc):
+    """sumsq epsr_standalone_rev3.py:3642-3677 on the device: the same for the partial S(Q).
+    qwind (device, 2*npairs*ldq), gensq's output; acc a dict of device float32 tensors
+    (npairs, ldq) named as SQ_ARRAYS, updated in place."""
+    lib = _lib.load(require_device=True)
+    npairs, ldq = acc["soqintra"].shape
+    check(lib.epsr_sumsq(int(nq), npairs, _p(qwind), ldq, float(fc1), float(fc2),
+                         *(_p(acc[k]) for k in SQ_ARRAYS), _s()))
+    return acc
+
+
 def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
     """stog ato_manipulation_rev4.py:4067.  q (ldq,), sofq_pairs (npairs, ldq), r (nr+1,)."""
     lib = _lib.load(require_device=True)

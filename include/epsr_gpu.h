@@ -271,12 +271,29 @@ int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const float *expr,
                              int64_t scratch_bytes, int32_t strict, int64_t *trials_host, void *stream);
 int64_t epsr_fit_expansion_batch_scratch_bytes(int32_t nprob, int32_t npt, int32_t nterms);
 
+/* ------------------------------------------------------------------ running averages */
+
+/* sumgr epsr_standalone_rev3.py:3578-3637: folds the new partial g(r) (wav/ycoh, 0 where
+ * ycoh <= 0) into the running means and error bars, weights fc2 (old) and fc1 (new) as
+ * runepsr17 sets them (:1614-1618), and recomputes the zero limit entsig.  wav
+ * [2][npairs][ldw]; ycoh [ldw]; gorintra, gorinter, gr2intra, gr2inter, entsig
+ * [npairs][ldw] (r index 1-based, points 2..nz updated), in place.  Bit-identical. */
+int epsr_sumgr(int32_t nz, int32_t npairs, const float *wav, int32_t ldw, const float *ycoh, double fc1,
+               double fc2, float *gorintra, float *gorinter, float *gr2intra, float *gr2inter, float *entsig,
+               void *stream);
+/* sumsq epsr_standalone_rev3.py:3642-3677: the same for the partial S(Q).  qwind
+ * [2][npairs][ldq] (gensq's intra and inter S(Q)); soqintra, soqinter, sq2intra, sq2inter
+ * [npairs][ldq] (Q index 1-based, points 1..nq), in place.  Bit-identical. */
+int epsr_sumsq(int32_t nq, int32_t npairs, const float *qwind, int32_t ldq, double fc1, double fc2,
+               float *soqintra, float *soqinter, float *sq2intra, float *sq2inter, void *stream);
+
 /* ------------------------------------------------------------------ one iteration */
 
 /* One EPSR iteration of the path on one box, driven from native code: the iteration body of
  * runepsr17 (epsr_standalone_rev3.py:1235-1842) restricted to this path -- cell list,
  * fmolec1, ntimes molfit cycles, atogen, gensq, the per-data-set differences of ptgnsq,
- * press, fit_expansion over all data sets, stog -- each stage the routine of that name
+ * press, fit_expansion over all data sets, the running averages sumsq and sumgr, stog --
+ * each stage the routine of that name
  * above, launched on `stream` from the calling thread.  The caller owns every buffer. */
 typedef struct {
     const epsr_box_t *box;
@@ -325,12 +342,18 @@ typedef struct {
     const int32_t *nqmin, *nqmax;     /* [npairs] */
     const float *xwt;                 /* [npairs] */
     float *gofr;                      /* [npairs][nr+1] */
+    /* running averages (sumsq, sumgr): nsum is the accumulation count including this step
+     * (runepsr17 :1611-1615: fc1 = 1/nsum, fc2 = (nsum-1)*fc1) */
+    int32_t nsum;
+    float *soqintra, *soqinter, *sq2intra, *sq2inter;           /* [npairs][nq+1] */
+    float *gorintra, *gorinter, *gr2intra, *gr2inter, *entsig;  /* [npairs][ldw] */
     /* one scratch block shared by the stages (epsr_iteration_scratch_bytes) */
     void *scratch;
     int64_t scratch_bytes;
     int32_t strict;
-    void *stage_events[16];           /* NULL or CUDA events recorded at the start and end of
-                                         cells, fmolec1, molfit, atogen, gensq, press, fit, stog */
+    void *stage_events[20];           /* NULL or CUDA events recorded at the start and end of
+                                         cells, fmolec1, molfit, atogen, gensq, press, fit, sums,
+                                         stog */
 } epsr_iteration_t;
 
 typedef struct {

@@ -915,6 +915,63 @@ void oracle_gensq(int nq, int npairs, int npt1, const float *wav, int ldw, const
     }
 }
 
+/* ------------------------------------------------------------------ running averages */
+/* One element of the running average with its error bar (the k loop of sumgr
+ * epsr_standalone_rev3.py:3619-3629 and sumsq :3667-3677), in double as the reference's
+ * real*8 work space: the stored error bar and mean give back the mean square, both are
+ * folded with the new sample by fc2 (old) and fc1 (new), and the error bar is the square
+ * root of the variance (0 when it is not positive).  *mean and *err are the float32 arrays. */
+static void sum_update(double add1, double fc1, double fc2, float *mean, float *err) {
+    double sumtot1 = (double)*mean, sumtot2 = (double)*err;
+    const double add2 = add1 * add1;
+    sumtot2 = sumtot2 * sumtot2 + sumtot1 * sumtot1;
+    sumtot1 = fc2 * sumtot1 + fc1 * add1;
+    sumtot2 = fc2 * sumtot2 + fc1 * add2;
+    double errort = sumtot2 - sumtot1 * sumtot1;
+    errort = errort > 0.0 ? sqrt(errort) : 0.0;
+    *mean = (float)sumtot1;
+    *err = (float)errort;
+}
+
+/* sumgr epsr_standalone_rev3.py:3578-3637: wav [2][npairs][ldw] (r index 1-based, 2..nz
+ * used), ycoh [ldw]; gorintra, gorinter, gr2intra, gr2inter, entsig [npairs][ldw].  The new
+ * sample is wav/ycoh in float32 (0 where ycoh <= 0); entsig[j] is the running double sum
+ * over j of ycoh*(gorinter-1) in float32 (the "zero limit"), entsig[1] = 0. */
+void oracle_sumgr(int nz, int npairs, const float *wav, int ldw, const float *ycoh, double fc1, double fc2,
+                  float *gorintra, float *gorinter, float *gr2intra, float *gr2inter, float *entsig) {
+    const size_t half = (size_t)npairs * (size_t)ldw;
+    for (int id = 0; id < npairs; ++id) {
+        const size_t row = (size_t)id * ldw;
+        entsig[row + 1] = 0.0f;
+        double zerolimit = 0.0;
+        for (int j = 2; j <= nz; ++j) {
+            double a1 = 0.0, a2 = 0.0;
+            if (ycoh[j] > 0.0f) {
+                a1 = (double)(wav[row + j] / ycoh[j]);
+                a2 = (double)(wav[half + row + j] / ycoh[j]);
+            }
+            sum_update(a1, fc1, fc2, &gorintra[row + j], &gr2intra[row + j]);
+            sum_update(a2, fc1, fc2, &gorinter[row + j], &gr2inter[row + j]);
+            zerolimit = zerolimit + (double)(ycoh[j] * (gorinter[row + j] - 1.0f));
+            entsig[row + j] = (float)zerolimit;
+        }
+    }
+}
+
+/* sumsq epsr_standalone_rev3.py:3642-3677: qwind [2][npairs][ldq] (Q index 1-based, 1..nq);
+ * soqintra, soqinter, sq2intra, sq2inter [npairs][ldq]. */
+void oracle_sumsq(int nq, int npairs, const float *qwind, int ldq, double fc1, double fc2, float *soqintra,
+                  float *soqinter, float *sq2intra, float *sq2inter) {
+    const size_t half = (size_t)npairs * (size_t)ldq;
+    for (int id = 0; id < npairs; ++id) {
+        const size_t row = (size_t)id * ldq;
+        for (int j = 1; j <= nq; ++j) {
+            sum_update((double)qwind[row + j], fc1, fc2, &soqintra[row + j], &sq2intra[row + j]);
+            sum_update((double)qwind[half + row + j], fc1, fc2, &soqinter[row + j], &sq2inter[row + j]);
+        }
+    }
+}
+
 /* ------------------------------------------------------------------ stog */
 /* ato_manipulation_rev4.py:4067-4121. sofq [npairs][ldq] (i 1-based), q [ldq], r [nr+1]
  * (1-based), gofr out [npairs][nr+1]. */

@@ -328,6 +328,30 @@ def gensq(nq, npt1, wav, foqols_rows, ycoh, n2extr, natomsphere):
     return out
 
 
+def sumgr(nz, wav, ycoh, fc1, fc2, acc):
+    """sumgr epsr_standalone_rev3.py:3578-3637 (C restatement).  wav (2, npairs, ldw); acc a
+    dict of (npairs, ldw) float32 arrays gorintra, gorinter, gr2intra, gr2inter, entsig,
+    returned updated (copies)."""
+    npairs, ldw = wav.shape[1], wav.shape[2]
+    out = {k: np.ascontiguousarray(acc[k], f32).copy() for k in ("gorintra", "gorinter", "gr2intra", "gr2inter",
+                                                                  "entsig")}
+    lib().oracle_sumgr(int(nz), npairs, ptr(np.ascontiguousarray(wav, f32)), ldw, ptr(np.ascontiguousarray(ycoh, f32)),
+                       C.c_double(fc1), C.c_double(fc2), ptr(out["gorintra"]), ptr(out["gorinter"]),
+                       ptr(out["gr2intra"]), ptr(out["gr2inter"]), ptr(out["entsig"]))
+    return out
+
+
+def sumsq(nq, qwind, fc1, fc2, acc):
+    """sumsq epsr_standalone_rev3.py:3642-3677 (C restatement).  qwind (2, npairs, ldq); acc a
+    dict of (npairs, ldq) float32 arrays soqintra, soqinter, sq2intra, sq2inter."""
+    npairs, ldq = qwind.shape[1], qwind.shape[2]
+    out = {k: np.ascontiguousarray(acc[k], f32).copy() for k in ("soqintra", "soqinter", "sq2intra", "sq2inter")}
+    lib().oracle_sumsq(int(nq), npairs, ptr(np.ascontiguousarray(qwind, f32)), ldq, C.c_double(fc1),
+                       C.c_double(fc2), ptr(out["soqintra"]), ptr(out["soqinter"]), ptr(out["sq2intra"]),
+                       ptr(out["sq2inter"]))
+    return out
+
+
 def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
     """q (ldq,), sofq_pairs (npairs, ldq) 1-based i; r (nr+1,) 1-based. Returns (npairs, nr+1)."""
     npairs, ldq = sofq_pairs.shape

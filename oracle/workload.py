@@ -77,6 +77,18 @@ class CpuIteration:
             self.stepp[k] = res["stepr"]
         t["fit_expansion"] = time.perf_counter() - t0
         t0 = time.perf_counter()
+        self.nsum = getattr(self, "nsum", 0) + 1
+        fc1 = float(f32(1.0) / f32(self.nsum))
+        fc2 = float(f32(self.nsum - 1)) * fc1
+        if not hasattr(self, "sums"):
+            ld = b.npt + 1
+            self.sums = {k: np.zeros((b.npairs, nq + 1), f32) for k in ("soqintra", "soqinter", "sq2intra", "sq2inter")}
+            self.sums.update({k: np.zeros((b.npairs, ld), f32)
+                              for k in ("gorintra", "gorinter", "gr2intra", "gr2inter", "entsig")})
+        self.sums.update(oracle.sumsq(nq, sofq, fc1, fc2, self.sums))
+        self.sums.update(oracle.sumgr(b.npt1, wav, wl.ycoh[: b.npt + 1], fc1, fc2, self.sums))
+        t["sums"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
         r = b.x[: b.npt1 + 1].copy()
         oracle.stog(f32(b.natom / wl.system.L ** 3), wl.q, inter, r, np.full(b.npairs, 2, np.int32),
                     np.full(b.npairs, nq, np.int32), wl.xwt)

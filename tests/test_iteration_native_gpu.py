@@ -33,6 +33,10 @@ def test_native_iteration_matches_python_driver(strict):
     assert a.pair_updates == b.pair_updates
     assert np.float32(a.energy) == np.float32(b.energy) and np.float32(a.pressc) == np.float32(b.pressc)
     assert tuple(map(np.float32, a.ftest)) == tuple(map(np.float32, b.ftest))
+    assert a.nsum == b.nsum == 3
+    for k, v in {**a.sums_sq, **a.sums_gr}.items():
+        w = {**b.sums_sq, **b.sums_gr}[k]
+        assert np.array_equal(v.cpu().numpy().view(np.uint32), w.cpu().numpy().view(np.uint32)), k
 
 
 def test_native_iteration_c2_runs_and_matches():
