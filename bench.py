@@ -393,9 +393,10 @@ def kernel_launches(it, wl):
     n += 11 * wl.ntimes  # molfit cycle: plan, ran1 fill + copy, propose, energy, corr, resolve, 2 commits,
     #                      epilogue, sequential retry (launched always, runs only if flagged)
     n += 8            # atogen: positions, ran1, select, intra, molecule map, origin atoms, inter, norm
-    n += 1            # gensq
+    n += 2            # gensq, data-set differences (ptgnsq)
     n += 3            # press: positions, pair terms, sums
     n += 1            # fit_expansion: one cluster launch for every data set
+    n += 2            # running averages: sumsq, sumgr
     n += 2            # stog: lorch + stog
     return n
 
