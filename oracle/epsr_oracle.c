@@ -972,6 +972,115 @@ void oracle_sumsq(int nq, int npairs, const float *qwind, int ldq, double fc1, d
     }
 }
 
+/* ------------------------------------------------------------------ generate_ep */
+/* generate_ep epsr_standalone_rev3.py:5876-5995 with the Poisson basis already built
+ * (calc_pwrexpr_grad, host): expgr [npt2][nterms] (row j-1 of the reference's flat expgr).
+ * pcoefp [nsets][nterms+1] (coefficient ic at [set][ic], 1-based ic), iref [npairs] the set of
+ * each pair (irefpcof - 1); tables xavs, xavs1, xavtot, xavtot1, ecoul [npairs][ld] (r index
+ * 1-based), xstar, wfac [ld].  par = {absolute_energy, erequnit, ereqstep, potfacamp}.
+ * Updates the tables, pcoefp (multiply_pot_coeffs), pwtold (the last pair's coefficients)
+ * and *potfac; returns energabs and pressfac in out2. */
+void oracle_generate_ep(int npairs, int npt, int npt2, int nterms, const float *expgr, float *pcoefp, int nsets,
+                        const int32_t *iref, float dmax, const float *xstar, const float *wfac, const float *ecoul,
+                        float *xavs, float *xavs1, float *xavtot, float *xavtot1, int ld, float *pwtold,
+                        const float *par, float *potfac, int changepotfac, float *out2) {
+    const float summax = expf(25.0f);
+    const int w = nterms + 1;
+    /* the EP gradient of every pair from its coefficients (:5905-5920) */
+    for (int ip = 0; ip < npairs; ++ip) {
+        const float *pc = pcoefp + (size_t)iref[ip] * w;
+        for (int ic = 2; ic <= nterms; ++ic) pwtold[ic] = pc[ic];
+        pwtold[1] = 0.0f;
+        for (int j = 1; j <= npt2; ++j) {
+            const float *e = expgr + (size_t)(j - 1) * nterms;
+            float sum = 0.0f;
+            for (int i = 1; i <= nterms; ++i) {     /* expand :4924 */
+                sum = sum + e[i - 1] * pwtold[i];
+                if (fabsf(sum) > summax) sum = copysignf(summax, sum);
+            }
+            xavs1[(size_t)ip * ld + j] = sum * pc[1];
+        }
+    }
+    /* the potential integrated from the last point, then truncated (:5922-5948) */
+    for (int ip = 0; ip < npairs; ++ip) {
+        float *s = xavs + (size_t)ip * ld, *s1 = xavs1 + (size_t)ip * ld;
+        for (int j = 1; j <= npt2; ++j) s1[j] = s1[j] * dmax;
+        s[npt] = 0.0f;
+        s1[npt] = 0.0f;
+        float x1 = xstar[npt], xts1 = s1[npt];
+        for (int j = 1; j <= npt2; ++j) {
+            const int jref = npt - j;
+            const float x2 = xstar[jref], xts2 = s1[jref];
+            s[jref] = s[jref + 1] - 0.5f * (x1 - x2) * (xts1 + xts2);
+            x1 = x2;
+            xts1 = xts2;
+        }
+        for (int j = 1; j <= npt2; ++j) s[j] = s[j] * wfac[j];
+    }
+    /* abs_energy_ep ato_manipulation_rev4.py:4128-4157 and the potential factor (:5950-5962) */
+    float energabs = 0.0f;
+    for (int k = 0; k < nsets; ++k) {
+        float lo = 0.0f, hi = 0.0f;
+        for (int i = 2; i <= nterms; ++i) {
+            const float t = pcoefp[(size_t)k * w + i];
+            lo = fminf(lo, t);
+            hi = fmaxf(hi, t);
+        }
+        energabs = fmaxf(energabs, hi - lo);
+    }
+    const float absolute_energy = par[0], erequnit = par[1], ereqstep = par[2], potfacamp = par[3];
+    float pressfac = 1.0f;
+    if (fabsf(absolute_energy) == 0.0f) {
+        pressfac = 0.0f;
+        energabs = 0.0f;
+    } else if (fabsf(energabs) > 0.0f) {
+        if (fabsf(energabs) < fabsf(erequnit)) {
+            pressfac = fabsf(erequnit) / fabsf(energabs);
+        } else {
+            pressfac = fabsf(absolute_energy) / fabsf(energabs);
+            if (pressfac > 1.0f && ereqstep == 0.0f) pressfac = 1.0f;
+        }
+    }
+    /* multiply_pot_coeffs :5215 (once per pair, so a set shared by pairs is scaled again) */
+    for (int ip = 0; ip < npairs; ++ip)
+        for (int ic = 2; ic <= nterms; ++ic) pcoefp[(size_t)iref[ip] * w + ic] *= pressfac;
+    /* scaled EP, total potential and both gradients (:5964-5985) */
+    for (int ip = 0; ip < npairs; ++ip) {
+        float *s = xavs + (size_t)ip * ld, *s1 = xavs1 + (size_t)ip * ld;
+        float *t = xavtot + (size_t)ip * ld, *t1 = xavtot1 + (size_t)ip * ld;
+        const float *ec = ecoul + (size_t)ip * ld;
+        for (int j = 1; j <= npt2; ++j) {
+            s[j] = s[j] * pressfac;
+            t[j] = ec[j] + s[j];
+        }
+        float sums1 = s[1], sumtot1 = t[1], x1 = xstar[1];
+        for (int j = 2; j <= npt; ++j) {
+            const float x2 = xstar[j], xdif = x2 - x1;
+            const float sums2 = s[j], sumtot2 = t[j];
+            s1[j - 1] = (sums2 - sums1) / xdif;
+            t1[j - 1] = (sumtot2 - sumtot1) / xdif;
+            x1 = x2;
+            sums1 = sums2;
+            sumtot1 = sumtot2;
+        }
+        s1[npt] = 0.0f;
+        t1[npt] = 0.0f;
+    }
+    /* the step of the potential factor (:5987-5995) */
+    if (changepotfac && absolute_energy > 0.0f) {
+        if (*potfac > 0.000001f && potfacamp > 0.0f) {
+            float absediff = (absolute_energy - energabs) / fabsf(potfacamp * absolute_energy);
+            if (fabsf(absediff) > 0.1f) absediff = copysignf(0.1f, absediff);
+            float pf = *potfac * (1.0f + absediff);
+            pf = fmaxf(pf, 0.000001f);
+            pf = fminf(pf, 1.0f);
+            *potfac = pf;
+        }
+    }
+    out2[0] = energabs;
+    out2[1] = pressfac;
+}
+
 /* ------------------------------------------------------------------ stog */
 /* ato_manipulation_rev4.py:4067-4121. sofq [npairs][ldq] (i 1-based), q [ldq], r [nr+1]
  * (1-based), gofr out [npairs][nr+1]. */
