@@ -105,6 +105,10 @@ _SIGS = {
     "epsr_ptgnsq_difference": (C.c_int, [I32, I32, I32, P, P, P, P, P]),
     "epsr_sumgr": (C.c_int, [I32, I32, P, I32, P, C.c_double, C.c_double, P, P, P, P, P, P]),
     "epsr_sumsq": (C.c_int, [I32, I32, P, I32, C.c_double, C.c_double, P, P, P, P, P]),
+    "epsr_generate_ep": (C.c_int, [I32, I32, I32, I32, P, P, I32, I32, P, F32, P, P, P, P, P, P, P, I32, P, F32, F32,
+                                   F32, F32, P, I32, P, P]),
+    "epsr_calc_pwrexpr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
+    "epsr_calc_gaussr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),
     "epsr_stog_scratch_bytes": (I64, [I32, I32]),
     "epsr_fit_expansion": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32, I32, P, P, I64, I32, P, P]),

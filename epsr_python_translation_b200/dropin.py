@@ -16,6 +16,8 @@ reference's argument lists and return values:
 * ``stog`` (library/ato_manipulation_rev4.py:4067)
 * ``fit_expansion`` (programs/epsr_standalone_rev3.py:4806)
 * ``press`` (library/ato_manipulation_rev4.py:3903)
+* ``sumgr`` / ``sumsq`` (programs/epsr_standalone_rev3.py:3578 / :3642)
+* ``generate_ep`` (programs/epsr_standalone_rev3.py:5876)
 
 ``install()`` assigns them onto the given modules (the reference's own rerouting
 mechanism, trace.py:94-125) and keeps the originals.
@@ -49,16 +51,16 @@ from .box import BoxArrays, Ran1State, trsteps
 
 f32 = np.float32
 ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit", "atogen", "stog", "gensq", "fit_expansion",
-            "press", "sumgr", "sumsq", "en_change", "en_mole_pair")
+            "press", "sumgr", "sumsq", "generate_ep", "en_change", "en_mole_pair")
 # en_change / en_mole_pair are per-molecule calls: rerouting them makes every host caller
 # (including host fallbacks) launch one kernel per call, so they are installed only on request.
-DEFAULT_ROUTINES = ROUTINES[:10]
+DEFAULT_ROUTINES = tuple(r for r in ROUTINES if r not in ("en_change", "en_mole_pair"))
 # module that owns each routine in the reference
 OWNER = {"initialise_cellneighbourlist": "cellneighbourlist", "fmolec1": "ato_manipulation_rev4",
          "atogen": "ato_manipulation_rev4", "stog": "ato_manipulation_rev4", "press": "ato_manipulation_rev4",
          "molfit": "molfit",
          "en_change": "molfit", "en_mole_pair": "molfit", "gensq": "program", "fit_expansion": "program",
-         "sumgr": "program", "sumsq": "program"}
+         "sumgr": "program", "sumsq": "program", "generate_ep": "program"}
 
 
 def _fortran(shape, dtype):
@@ -528,6 +530,45 @@ class PairPath:
         arrays = {k: getattr(e16, k) for k in transforms.SQ_ARRAYS}
         return self._running_sums(transforms.SQ_ARRAYS, nq, 1, arrays, qwind,
                                   lambda w, acc: transforms.sumsq(nq, w, float(sv.fc1), float(sv.fc2), acc))
+
+    def generate_ep(self, changepotfac):
+        """epsr_standalone_rev3.py:5876-6022: rebuilds xavs, xavs1, xavtot and xavtot1 of
+        potential_par from the coefficients pcoefp, scales pcoefp by pressfac
+        (multiply_pot_coeffs), and sets pwtold, expgr and (with changepotfac) potfac, in place.
+        The basis matrix is built on the host once per grid and basis parameters."""
+        from . import potential
+        _lib.load(require_device=True)
+        c = self.c
+        pp, e16 = c.potential_par, c.epsr16
+        npt, npt2, nterms = int(e16.npt), int(e16.npt2), int(pp.ncoeffp)
+        npairs, nsets = int(c.molecom.npairs), int(pp.npairspcof)
+        ld = npt + 1
+        x = np.array(e16.x[:ld], f32)
+        bp = (bool(pp.gaussian), f32(pp.pdmin), f32(pp.pdstep), f32(pp.pdmax), f32(pp.psigma2), f32(e16.rho),
+              f32(c.epsrinput_par.rbroad))
+        key = (npt2, nterms, *(float(v) for v in bp), x[: npt2 + 1].tobytes())
+        cache = self._snap.get("ep_basis")
+        if cache is None or cache[0] != key:
+            expgr, _ = potential.basis(npt2, nterms, x, *bp)
+            cache = (key, expgr, torch.from_numpy(expgr).cuda())
+            self._snap["ep_basis"] = cache
+        pp.expgr[1: npt2 * nterms + 1] = cache[1]
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, f32)).cuda()  # noqa: E731
+        tab = lambda a: dev(np.asarray(a)[:ld, 1:npairs + 1].T)  # noqa: E731
+        tabs = {k: tab(getattr(pp, k)) for k in potential.TABLES}
+        pc = dev(np.asarray(pp.pcoefp)[: nterms + 1, 1:nsets + 1].T)
+        pw = dev(np.asarray(pp.pwtold)[: nterms + 1])
+        pf = dev([pp.potfac])
+        potential.generate_ep(npt, npt2, nterms, cache[2], pc, np.asarray(pp.irefpcof[1:npairs + 1], np.int32) - 1,
+                              f32(c.clustercom.dmax), dev(np.asarray(e16.xstar)[:ld]), dev(np.asarray(pp.wfac)[:ld]),
+                              tab(pp.ecoul), tabs, pw, f32(pp.absolute_energy), f32(pp.erequnit), f32(pp.ereqstep),
+                              f32(pp.potfacamp), pf, bool(changepotfac))
+        for k in potential.TABLES:
+            getattr(pp, k)[1:ld, 1:npairs + 1] = tabs[k].cpu().numpy()[:, 1:ld].T
+        pp.pcoefp[2: nterms + 1, 1:nsets + 1] = pc.cpu().numpy()[:, 2:].T
+        pp.pwtold[1: nterms + 1] = pw.cpu().numpy()[1:]
+        pp.potfac = f32(pf.cpu().numpy()[0])
+        return None
 
     def stog(self, rho, q, sofq, r, gofr, nqmin, nqmax, nr, npairs, nqdim, nrdim, npdim, xwt):
         """ato_manipulation_rev4.py:4067-4110: fills gofr(nr, npairs) in place."""

@@ -1,0 +1,81 @@
+"""The empirical potential (EP) rebuilt from its coefficients: generate_ep
+(epsr_standalone_rev3.py:5876-6022) on the device, with the basis matrix built once on the
+host (calc_pwrexpr_grad :5230 or calc_gaussr_grad :5046, the C library's logf/expf as the
+reference).
+
+Layouts (the device form of the reference's 1-based COMMON arrays of potential_par):
+coefficient sets ``pcoefp`` (nsets, ldc) with coefficient ic of set k at [k, ic]; tables
+``xavs``, ``xavs1``, ``xavtot``, ``xavtot1``, ``ecoul`` (npairs, ld) with the r index j at
+[pair, j]; ``xstar`` and ``wfac`` (ld,); ``iref`` the 0-based set of each pair (irefpcof - 1).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+
+f32 = np.float32
+TABLES = ("xavs", "xavs1", "xavtot", "xavtot1")
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _s():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def basis(npt2, nterms, x, gaussian, pdmin, pdstep, pdmax, psigma2, rho, rbroad, rmin=0.0, fbroad=1.0, ncfirst=0):
+    """The r-space basis generate_ep builds on entry (epsr_standalone_rev3.py:5907-5912):
+    calc_gaussr_grad when ``gaussian`` else calc_pwrexpr_grad, on points x[1..npt2] (x 1-based).
+    Host computation.  Returns (expgr (npt2*nterms,) float32 -- the reference's
+    expgr(1..npt2*nterms) --, ncfirst)."""
+    lib = _lib.load()
+    xs = np.ascontiguousarray(np.asarray(x, f32)[: npt2 + 1])
+    out = np.zeros(int(npt2) * int(nterms), f32)
+    nc = C.c_int32(int(ncfirst))
+    xp, op = xs.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)
+    if gaussian:
+        rc = lib.epsr_calc_gaussr_grad(int(npt2), int(nterms), f32(pdstep), f32(pdmax), f32(psigma2), f32(rho), xp,
+                                       op, f32(rmin), C.byref(nc), f32(fbroad), f32(rbroad))
+    else:
+        rc = lib.epsr_calc_pwrexpr_grad(int(npt2), int(nterms), f32(pdmin), f32(pdstep), f32(pdmax), f32(psigma2),
+                                        f32(rho), xp, op, f32(rmin), C.byref(nc), f32(fbroad), f32(rbroad))
+    check(rc)
+    return out, int(nc.value)
+
+
+def generate_ep(npt, npt2, nterms, expgr, pcoefp, iref, dmax, xstar, wfac, ecoul, tabs, pwtold, absolute_energy,
+                erequnit, ereqstep, potfacamp, potfac, changepotfac=True, result=None):
+    """generate_ep epsr_standalone_rev3.py:5876-6022 on device tensors, in place: ``tabs``
+    (dict of the four tables), ``pcoefp``, ``pwtold`` (nterms+1,) and ``potfac`` (1,).
+    ``iref`` is a host int array.  Returns the device tensor (energabs, pressfac)."""
+    lib = _lib.load(require_device=True)
+    npairs, ld = ecoul.shape
+    nsets, ldc = pcoefp.shape
+    if result is None:
+        result = torch.zeros(2, dtype=torch.float32, device=ecoul.device)
+    ir = np.ascontiguousarray(np.asarray(iref, np.int32))
+    if ir.shape[0] != npairs:
+        raise ValueError(f"iref has {ir.shape[0]} entries for {npairs} pairs")
+    for t in (expgr, pcoefp, xstar, wfac, ecoul, pwtold, potfac, result, *tabs.values()):
+        if t.dtype != torch.float32 or not t.is_contiguous() or not t.is_cuda:
+            raise ValueError("generate_ep takes contiguous float32 device tensors")
+    if pwtold.numel() < nterms + 1 or potfac.numel() < 1 or result.numel() < 2 or xstar.numel() < ld or \
+            wfac.numel() < ld or expgr.numel() < npt2 * nterms:
+        raise ValueError("generate_ep: pwtold, potfac, result, xstar, wfac or expgr is too short")
+    for k in TABLES:
+        if tuple(tabs[k].shape) != (npairs, ld):
+            raise ValueError(f"table {k} has shape {tuple(tabs[k].shape)}, not {(npairs, ld)}")
+    check(lib.epsr_generate_ep(int(npairs), int(npt), int(npt2), int(nterms), _p(expgr), _p(pcoefp), int(nsets),
+                               int(ldc), ir.ctypes.data_as(C.c_void_p), f32(dmax), _p(xstar), _p(wfac), _p(ecoul),
+                               _p(tabs["xavs"]), _p(tabs["xavs1"]), _p(tabs["xavtot"]), _p(tabs["xavtot1"]), int(ld),
+                               _p(pwtold), f32(absolute_energy), f32(erequnit), f32(ereqstep), f32(potfacamp),
+                               _p(potfac), int(bool(changepotfac)), _p(result), _s()))
+    return result

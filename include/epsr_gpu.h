@@ -287,6 +287,40 @@ int epsr_sumgr(int32_t nz, int32_t npairs, const float *wav, int32_t ldw, const 
 int epsr_sumsq(int32_t nq, int32_t npairs, const float *qwind, int32_t ldq, double fc1, double fc2,
                float *soqintra, float *soqinter, float *sq2intra, float *sq2inter, void *stream);
 
+/* ------------------------------------------------------------------ empirical potential */
+
+/* generate_ep epsr_standalone_rev3.py:5876-6022 from the basis matrix the reference builds
+ * at its start (calc_pwrexpr_grad / calc_gaussr_grad, below): for every pair, the EP gradient
+ * on r points 1..npt2 (expand :4924, clamped at +-exp(25) after every term) x pcoefp(1) x
+ * dmax, the potential integrated from the last point, x wfac, x pressfac (abs_energy_ep
+ * ato_manipulation_rev4.py:4128 and the rules of :5966-5977), + ecoul, and both
+ * forward-difference gradients; multiply_pot_coeffs (:6493) by pressfac; pwtold = the last
+ * pair's coefficients with pwtold(1) = 0; and, if changepotfac, the step of *potfac
+ * (:6015-6022).  Bit-identical.
+ *   expgr    device [npt2][nterms] (the reference's expgr(1..npt2*nterms))
+ *   pcoefp   device [nsets][ldc], coefficient ic of set k at [k*ldc + ic] (ic 1..nterms),
+ *            updated in place
+ *   irefpcof_host  host [npairs]: 0-based coefficient set of each pair (npairs <= 960)
+ *   xstar, wfac    device [ld] (1-based r index); ecoul device [npairs][ld]
+ *   xavs, xavs1, xavtot, xavtot1  device [npairs][ld], updated in place (the call also reads
+ *            entries it does not rewrite, as the reference: xavs1(npt-1), xavtot(npt2+1..npt))
+ *   pwtold   device [nterms+1]; potfac device [1] in/out; result device [2] = {energabs,
+ *            pressfac}.  1 <= npt2 <= npt-1, npt+1 <= ld.  Asynchronous on `stream`. */
+int epsr_generate_ep(int32_t npairs, int32_t npt, int32_t npt2, int32_t nterms, const float *expgr, float *pcoefp,
+                     int32_t nsets, int32_t ldc, const int32_t *irefpcof_host, float dmax, const float *xstar,
+                     const float *wfac, const float *ecoul, float *xavs, float *xavs1, float *xavtot, float *xavtot1,
+                     int32_t ld, float *pwtold, float absolute_energy, float erequnit, float ereqstep,
+                     float potfacamp, float *potfac, int32_t changepotfac, float *result, void *stream);
+
+/* calc_pwrexpr_grad epsr_standalone_rev3.py:5230-5309 (the power-exponential basis, with the
+ * spacing of dnext :5312) and calc_gaussr_grad :5046-5096 (the Gaussian basis): host
+ * functions, the C library's logf/expf as the reference.  xin host [lpt+1] (1-based), expr
+ * host out [lpt][nterms] (the reference's expr(1..lpt*nterms)); *ncfirst in/out. */
+int epsr_calc_pwrexpr_grad(int32_t lpt, int32_t nterms, float dmin, float dstep, float dmax, float sigmab, float rho,
+                           const float *xin, float *expr, float rmin, int32_t *ncfirst, float fbroad, float rbroad);
+int epsr_calc_gaussr_grad(int32_t lpt, int32_t nterms, float dstep, float dmax, float sigmab, float rho,
+                          const float *xin, float *expr, float rmin, int32_t *ncfirst, float fbroad, float rbroad);
+
 /* ------------------------------------------------------------------ one iteration */
 
 /* One EPSR iteration of the path on one box, driven from native code: the iteration body of

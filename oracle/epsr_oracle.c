@@ -975,17 +975,18 @@ void oracle_sumsq(int nq, int npairs, const float *qwind, int ldq, double fc1, d
 /* ------------------------------------------------------------------ generate_ep */
 /* generate_ep epsr_standalone_rev3.py:5876-5995 with the Poisson basis already built
  * (calc_pwrexpr_grad, host): expgr [npt2][nterms] (row j-1 of the reference's flat expgr).
- * pcoefp [nsets][nterms+1] (coefficient ic at [set][ic], 1-based ic), iref [npairs] the set of
+ * pcoefp [nsets][ldc] (coefficient ic at [set][ic], 1-based ic), iref [npairs] the set of
  * each pair (irefpcof - 1); tables xavs, xavs1, xavtot, xavtot1, ecoul [npairs][ld] (r index
  * 1-based), xstar, wfac [ld].  par = {absolute_energy, erequnit, ereqstep, potfacamp}.
  * Updates the tables, pcoefp (multiply_pot_coeffs), pwtold (the last pair's coefficients)
  * and *potfac; returns energabs and pressfac in out2. */
 void oracle_generate_ep(int npairs, int npt, int npt2, int nterms, const float *expgr, float *pcoefp, int nsets,
-                        const int32_t *iref, float dmax, const float *xstar, const float *wfac, const float *ecoul,
+                        int ldc, const int32_t *iref, float dmax, const float *xstar, const float *wfac, const float *ecoul,
                         float *xavs, float *xavs1, float *xavtot, float *xavtot1, int ld, float *pwtold,
                         const float *par, float *potfac, int changepotfac, float *out2) {
-    const float summax = expf(25.0f);
-    const int w = nterms + 1;
+    volatile float e25 = 25.0f;   /* exp(25) from the C library at run time, as the reference */
+    const float summax = expf(e25);
+    const int w = ldc;
     /* the EP gradient of every pair from its coefficients (:5905-5920) */
     for (int ip = 0; ip < npairs; ++ip) {
         const float *pc = pcoefp + (size_t)iref[ip] * w;

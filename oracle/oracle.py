@@ -355,8 +355,8 @@ def sumsq(nq, qwind, fc1, fc2, acc):
 def generate_ep(npt, npt2, nterms, expgr, pcoefp, iref, dmax, xstar, wfac, ecoul, tabs, pwtold, par, potfac,
                 changepotfac=True):
     """generate_ep epsr_standalone_rev3.py:5876-6022 (C restatement) from the basis matrix
-    expgr (npt2*nterms,) the reference's calc_pwrexpr_grad builds.  pcoefp (nsets, nterms+1)
-    [set, ic]; iref (npairs,) 0-based set of each pair; ecoul and tabs["xavs", "xavs1",
+    expgr (npt2*nterms,) the reference's calc_pwrexpr_grad builds.  pcoefp (nsets, ldc >=
+    nterms+1) [set, ic]; iref (npairs,) 0-based set of each pair; ecoul and tabs["xavs", "xavs1",
     "xavtot", "xavtot1"] (npairs, ld) [pair, j]; pwtold (nterms+1,); par (absolute_energy,
     erequnit, ereqstep, potfacamp).  Returns (tabs, pcoefp, pwtold, potfac, energabs,
     pressfac), all updated copies."""
@@ -368,7 +368,7 @@ def generate_ep(npt, npt2, nterms, expgr, pcoefp, iref, dmax, xstar, wfac, ecoul
     pf = np.array([potfac], f32)
     o2 = np.zeros(2, f32)
     lib().oracle_generate_ep(npairs, int(npt), int(npt2), int(nterms), ptr(np.ascontiguousarray(expgr, f32)), ptr(pc),
-                             nsets, ptr(np.ascontiguousarray(iref, np.int32)), C.c_float(f32(dmax)),
+                             nsets, pc.shape[1], ptr(np.ascontiguousarray(iref, np.int32)), C.c_float(f32(dmax)),
                              ptr(np.ascontiguousarray(xstar, f32)), ptr(np.ascontiguousarray(wfac, f32)),
                              ptr(np.ascontiguousarray(ecoul, f32)), ptr(out["xavs"]), ptr(out["xavs1"]),
                              ptr(out["xavtot"]), ptr(out["xavtot1"]), ld, ptr(pw), ptr(np.ascontiguousarray(par, f32)),

@@ -37,7 +37,8 @@ f32 = np.float32
 REF = "/root/reference"
 
 
-def run_case(name, ep, npairs, rmaxgr, absolute_energy, erequnit, ereqstep, seed, out, ncalls=2, iref=None):
+def run_case(name, ep, npairs, rmaxgr, absolute_energy, erequnit, ereqstep, seed, out, ncalls=2, iref=None,
+             gaussian=False, psigma2=0.004, rbroad=0.0):
     from epsr26.common import clustercom, epsr16, epsrinput_par, molecom, potential_par as pp
     from epsr26.fortran import r4
     rng = np.random.default_rng(seed)
@@ -50,13 +51,13 @@ def run_case(name, ep, npairs, rmaxgr, absolute_energy, erequnit, ereqstep, seed
     epsr16.xstar[: npt + 1] = (g["x"] / dmax).astype(f32)
     epsr16.rho = f32(0.1)
     molecom.npairs = npairs
-    epsrinput_par.rminpt, epsrinput_par.rmaxpt, epsrinput_par.rbroad = f32(9.0), f32(12.0), f32(0.0)
+    epsrinput_par.rminpt, epsrinput_par.rmaxpt, epsrinput_par.rbroad = f32(9.0), f32(12.0), f32(rbroad)
     pp.pdstep = r4(0.1)
     pp.pdmin = r4(1.0) + pp.pdstep / epsrinput_par.rminpt
     pp.pdmax = epsrinput_par.rmaxpt
     pp.ncoeffp = nterms = 116
-    pp.psigma2 = r4(0.004)
-    pp.gaussian = False
+    pp.psigma2 = r4(psigma2)
+    pp.gaussian = bool(gaussian)
     iref = list(range(1, npairs + 1)) if iref is None else list(iref)   # 1-based set of each pair
     nsets = max(iref)
     pp.npairspcof = nsets
@@ -90,6 +91,9 @@ def run_case(name, ep, npairs, rmaxgr, absolute_energy, erequnit, ereqstep, seed
     out[f"{name}_dims"] = np.array([npairs, npt, npt2, nterms, ncalls])
     out[f"{name}_iref"] = np.array(iref, np.int32) - 1
     out[f"{name}_scal"] = np.array([dmax, absolute_energy, erequnit, ereqstep, 0.2, 0.5], f32)
+    # the basis parameters: gaussian, pdmin, pdstep, pdmax, psigma2, rho, rbroad
+    out[f"{name}_basis"] = np.array([float(gaussian), pp.pdmin, pp.pdstep, pp.pdmax, pp.psigma2, epsr16.rho,
+                                     epsrinput_par.rbroad], f32)
     for c in range(ncalls):
         ep.generate_ep(True)
         if c == 0:
@@ -120,7 +124,10 @@ if __name__ == "__main__":
              ncalls=3)
     common.reset()
     run_case("shared", ep, npairs=3, rmaxgr=15.0, absolute_energy=3.0, erequnit=0.5, ereqstep=0.0, seed=6, out=out,
-             iref=[1, 2, 1])
+             iref=[1, 2, 1], rbroad=0.02)
+    common.reset()
+    run_case("gauss", ep, npairs=3, rmaxgr=14.0, absolute_energy=1.0, erequnit=0.2, ereqstep=0.0, seed=7, out=out,
+             gaussian=True, psigma2=0.1, rbroad=0.02)
     path = os.path.join(HERE, "ep.npz")
     np.savez_compressed(path, **out)
     print("wrote", path)

@@ -10,7 +10,7 @@ from oracle import oracle
 from tests.goldens import GOLDEN, assert_bits_equal
 
 TABS = ("xavs", "xavs1", "xavtot", "xavtot1")
-CASES = ["small", "noabs", "unit", "cap", "shrink", "shared"]
+CASES = ["small", "noabs", "unit", "cap", "shrink", "shared", "gauss"]
 
 
 def case_arrays(z, name):
