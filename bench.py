@@ -123,7 +123,8 @@ def reference_arm(a):
         "warmup": warmup, "ms_per_step": 1000.0 * slowest / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded C2 mixture box)",
         "config": {"workload": a.config, "moves_per_step_per_replica": moves, "replicas": nproc,
-                   "stages": "cells+fmolec1+5 molfit+atogen+gensq+ptgnsq differences+press+fit_expansion+sums+stog"},
+                   "stages": "cells+fmolec1+5 molfit+atogen+gensq+ptgnsq differences+press+fit_expansion+"
+                             "EP refinement+sums+stog"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
                          "sample": f"{nproc} independent replicas x {steps} iterations (+{warmup} warm-up) of the "
                                    f"single-threaded C restatement, one process per core; host {model}"},
@@ -359,7 +360,9 @@ def gpu_arm(a):
                        "moves_per_step_per_box": moves, "boxes_per_gpu": R,
                        "pair_updates_per_step_per_box": it.pair_updates,
                        "stages": f"cells+fmolec1+{wl.ntimes} molfit+atogen+gensq+ptgnsq differences+press+"
-                                 f"fit_expansion ({wl.data.shape[0]} data sets)+sums (sumsq, sumgr)+stog",
+                                 f"fit_expansion ({wl.data.shape[0]} data sets)+"
+                                 f"{'EP refinement (coefficient increment, generate_ep, packed tables)+' if wl.ep else ''}"
+                                 "sums (sumsq, sumgr)+stog",
                        "step": f"one EPSR iteration of each of the {R} independent boxes on this GPU, each box on "
                                "its own stream and host thread",
                        "l2": "flushed between timed steps (256 MB write)", "sums": "strict" if a.strict else "fast",
@@ -396,6 +399,8 @@ def kernel_launches(it, wl):
     n += 2            # gensq, data-set differences (ptgnsq)
     n += 3            # press: positions, pair terms, sums
     n += 1            # fit_expansion: one cluster launch for every data set
+    if wl.ep is not None:
+        n += 4        # EP refinement: coefficient increment, per-pair rebuild, coefficient scaling, pack
     n += 2            # running averages: sumsq, sumgr
     n += 2            # stog: lorch + stog
     return n

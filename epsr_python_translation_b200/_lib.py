@@ -71,6 +71,10 @@ class Iteration(C.Structure):
                 ("rho", F32), ("q", P), ("r", P), ("nr", I32), ("nqmin", P), ("nqmax", P), ("xwt", P),
                 ("gofr", P), ("nsum", I32), ("soqintra", P), ("soqinter", P), ("sq2intra", P), ("sq2inter", P),
                 ("gorintra", P), ("gorinter", P), ("gr2intra", P), ("gr2inter", P), ("entsig", P),
+                ("refine", I32), ("pcoefp", P), ("nsets", I32), ("ldc", I32), ("irefpcof_host", P), ("efacp", P),
+                ("cwtpot", P), ("expgr", P), ("wfac", P), ("ecoul", P), ("ecoul1", P), ("xavs", P), ("xavs1", P),
+                ("xavtot", P), ("xavtot1", P), ("ep_pwtold", P), ("potfac", P), ("ep_result", P), ("pfact", F32),
+                ("absolute_energy", F32), ("erequnit", F32), ("ereqstep", F32), ("potfacamp", F32), ("tab", P),
                 ("scratch", P), ("scratch_bytes", I64), ("strict", I32), ("stage_events", P * 20)]
 
 
@@ -107,6 +111,8 @@ _SIGS = {
     "epsr_sumsq": (C.c_int, [I32, I32, P, I32, C.c_double, C.c_double, P, P, P, P, P]),
     "epsr_generate_ep": (C.c_int, [I32, I32, I32, I32, P, P, I32, I32, P, F32, P, P, P, P, P, P, P, I32, P, F32, F32,
                                    F32, F32, P, I32, P, P]),
+    "epsr_ep_update": (C.c_int, [I32, I32, I32, P, I32, I32, P, P, P, P, I32, F32, P]),
+    "epsr_pack_tables": (C.c_int, [I32, I32, P, P, P, P, P, P]),
     "epsr_calc_pwrexpr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
     "epsr_calc_gaussr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),

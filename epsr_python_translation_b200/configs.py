@@ -463,6 +463,33 @@ def ep_basis(q, nterms, sigma=0.35, seed=3):
     return expr
 
 
+def pwrexpq_basis(q, nterms, dmin, dstep, sigmab):
+    """The Q-space transforms of the power-exponential EP basis functions, shaped and spaced as
+    calc_pwrexpq (epsr_standalone_rev3.py:5100-5153, positions from dnext :5312), in double
+    precision: ``expr[(i-1)*nterms + m]`` (1-based flat).  The fit of a workload that refines
+    its EP uses these, so that the fitted coefficients are those of the r-space basis that
+    generate_ep expands."""
+    nq = q.shape[0] - 1
+    qq = q[1:].astype(np.float64)
+    expr = np.zeros(nq * nterms + 1, dtype=f32)
+    d, rootd = float(dstep), 1.0
+    for m in range(1, nterms + 1):
+        sigma = rootd * float(sigmab)
+        n = int(d / sigma - 1.0) if (sigma <= d and sigma > 0.0 and m > 1) else 0
+        qs = qq * sigma
+        alpha = np.arctan(qs)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            term = np.where(qs > 0, 2.0 * np.cos(n * alpha) + (1.0 - qs * qs) * np.sin(n * alpha) / np.where(
+                qs > 0, qs, 1.0), n + 2.0)
+        logden = 0.5 * (4 + n) * np.log1p(qs * qs)
+        expr[1 + np.arange(nq) * nterms + (m - 1)] = (term / (n + 2.0) * np.exp(-logden)).astype(f32)
+        dn, dtest = d + float(dstep), d * float(dmin)
+        if dtest > dn:
+            dn, rootd = dtest, rootd * math.sqrt(float(dmin))
+        d = dn
+    return expr
+
+
 def fit_problem(nq=600, nterms=116, seed=5, noise=0.005):
     """Synthetic fit_expansion inputs: yin = basis . c_true + Gaussian noise (1-based)."""
     rng = np.random.default_rng(seed)
@@ -497,6 +524,47 @@ def intra_energies(s: System, k_bond=1000.0):
 
 
 @dataclass
+class EpRefinement:
+    """The potential-refinement state of potential_par that ptgnsq and generate_ep read
+    (epsr_standalone_rev3.py:3946-3962, :5876-6022): one coefficient set per atom pair
+    (irefpcof(ip) = ip), the r-space Poisson basis parameters of the reference's defaults
+    (pdstep 0.1, pdmin 1 + pdstep/rminpt, pdmax rmaxpt), the truncation wfac and the
+    amplitude controls."""
+    pcoefp: np.ndarray       # (nsets, nterms+1) [set, ic]: ic = 1 the amplitude, 2.. the terms
+    iref: np.ndarray         # (npairs,) 0-based set of each pair
+    efacp: np.ndarray        # (nsets,)
+    wfac: np.ndarray         # (npt+1,) truncate(r, rminpt, rmaxpt), 0 at npt
+    pdmin: float
+    pdstep: float
+    pdmax: float
+    psigma2: float
+    rho: float
+    rbroad: float = 0.0
+    potfac: float = 0.2
+    absolute_energy: float = 10.0
+    erequnit: float = 1.0
+    ereqstep: float = 0.0
+    potfacamp: float = 0.5
+
+
+def ep_refinement(s, nterms, seed=7):
+    """Seeded potential-refinement state for system ``s`` (an EPSR run in progress: unit
+    amplitudes and small nonzero coefficients)."""
+    rng = np.random.default_rng(seed)
+    npairs = s.npairs
+    pc = np.zeros((npairs, nterms + 1), dtype=f32)
+    pc[:, 1] = 1.0
+    pc[:, 2:] = (rng.standard_normal((npairs, nterms - 1)) * 0.02).astype(f32)
+    npt = s.grid["npt"]
+    wfac = truncate_lj(s.grid["x"].astype(np.float64), s.rminpt, s.rmaxpt).astype(f32)
+    wfac[npt] = 0.0
+    pdstep = f32(0.1)
+    return EpRefinement(pcoefp=pc, iref=np.arange(npairs, dtype=np.int32), efacp=np.ones(npairs, f32), wfac=wfac,
+                        pdmin=float(f32(1.0) + pdstep / f32(s.rminpt)), pdstep=float(pdstep), pdmax=float(s.rmaxpt),
+                        psigma2=0.01, rho=float(f32(0.1)))
+
+
+@dataclass
 class Workload:
     """One EPSR iteration's inputs for the pair path on a box."""
     name: str
@@ -516,17 +584,20 @@ class Workload:
     rejrate: float = 0.75
     ngrsamples: int = 0
     xwt: np.ndarray = None   # (npairs,) stog offsets
+    ep: EpRefinement = None  # potential refinement after the fits (None: the EP stays fixed)
 
     @property
     def nq(self):
         return int(self.q.shape[0] - 1)
 
 
-def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, ndata=None, ntimes=5):
+def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, ndata=None, ntimes=5, refine=True):
     """One iteration's inputs on a named configuration, 5 MC sweeps per iteration and a
     116-term Poisson-like EP basis.  C2 (c2_mixture): 200 DMSO + 400 water, three isotope
     data sets (deuterated, protiated, 50:50), Q to 30 A^-1 (600 points).  C3 (c3_water):
-    20,000 water, one data set, Q to 50 A^-1 (1,000 points).  C1 (c1_water): 100 water."""
+    20,000 water, one data set, Q to 50 A^-1 (1,000 points).  C1 (c1_water): 100 water.
+    ``refine``: each iteration also refines the EP from the fits (ptgnsq's coefficient
+    increment and generate_ep), as the reference does while its potential factor is on."""
     if nq is None:
         nq = 1000 if name == "c3_water" else 600
     if ndata is None:
@@ -543,7 +614,8 @@ def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, nd
     q = qgrid(nq, qstep)
     npt1 = s.grid["npt1"]
     F, ycoh = transform_table(s, q, npt1)
-    expr = ep_basis(q, nterms)
+    ep = ep_refinement(s, nterms) if refine else None
+    expr = pwrexpq_basis(q, nterms, ep.pdmin, ep.pdstep, ep.psigma2) if refine else ep_basis(q, nterms)
     w = rng.uniform(0.2, 1.0, size=(ndata, s.npairs)).astype(f32)
     w /= w.sum(axis=1, keepdims=True)
     data = np.zeros((ndata, nq + 1), dtype=f32)
@@ -557,4 +629,4 @@ def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, nd
     xwt = np.linspace(0.5, 1.5, s.npairs).astype(f32)
     return Workload(name=name, system=s, eintra=intra_energies(s), q=q, foqols=F, ycoh=ycoh, expr=expr,
                     nterms=nterms, data=data, weights=w, wholerot=wholerot, wholetrans=wholetrans, ntimes=ntimes,
-                    xwt=xwt)
+                    xwt=xwt, ep=ep)

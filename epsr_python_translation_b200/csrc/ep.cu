@@ -204,9 +204,89 @@ __global__ void __launch_bounds__(EP_COEF_THREADS) ep_coeff_kernel(const __grid_
     }
 }
 
+// The coefficient increment of ptgnsq epsr_standalone_rev3.py:3948-3962 for every data set in
+// turn: pcoefp(ic, k) += ((pfact * efacp(k)) * cwtpot(ip, id)) * pwtold_id(ic) for each pair ip
+// of set k, in pair order, float32 throughout.  One thread per (set, coefficient).
+struct EpUpdate {
+    int ndata, npairs, nterms, nsets, ldc, ldw;
+    float pfact;
+    float *pcoefp;
+    const float *efacp, *cwtpot, *pwtold;
+    int32_t iref[EP_MAX_PAIRS];
+};
+
+__global__ void ep_update_kernel(const __grid_constant__ EpUpdate u) {
+    const int w = u.nterms - 1;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= u.nsets * w) return;
+    const int k = q / w, ic = 2 + q % w;
+    float *p = u.pcoefp + (size_t)k * u.ldc + ic;
+    float v = *p;
+    const float fk = __fmul_rn(u.pfact, u.efacp[k]);
+    for (int id = 0; id < u.ndata; ++id) {
+        const float pw = u.pwtold[(size_t)id * u.ldw + ic];
+        for (int ip = 0; ip < u.npairs; ++ip)
+            if (u.iref[ip] == k) v = __fadd_rn(v, __fmul_rn(__fmul_rn(fk, u.cwtpot[(size_t)id * u.npairs + ip]), pw));
+    }
+    *p = v;
+}
+
+// The packed pair tables the energy kernels read: tab[(pair*ld + j)*4 + {0,1,2,3}] =
+// {xavs, xavs1, ecoul, ecoul1}(j).
+__global__ void ep_pack_kernel(int n, const float *xavs, const float *xavs1, const float *ecoul, const float *ecoul1,
+                               float4 *tab) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) tab[i] = make_float4(xavs[i], xavs1[i], ecoul[i], ecoul1[i]);
+}
+
 }  // namespace epsr
 
 using namespace epsr;
+
+extern "C" int epsr_ep_update(int32_t ndata, int32_t npairs, int32_t nterms, float *pcoefp, int32_t nsets,
+                              int32_t ldc, const int32_t *irefpcof_host, const float *efacp, const float *cwtpot,
+                              const float *pwtold, int32_t ldw, float pfact, void *stream) {
+    if (ndata < 1 || npairs < 1 || npairs > EP_MAX_PAIRS || nterms < 2 || nsets < 1 || ldc < nterms + 1 ||
+        ldw < nterms + 1 || !pcoefp || !irefpcof_host || !efacp || !cwtpot || !pwtold) {
+        epsr_set_error("epsr_ep_update: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    EpUpdate u;
+    u.ndata = ndata;
+    u.npairs = npairs;
+    u.nterms = nterms;
+    u.nsets = nsets;
+    u.ldc = ldc;
+    u.ldw = ldw;
+    u.pfact = pfact;
+    u.pcoefp = pcoefp;
+    u.efacp = efacp;
+    u.cwtpot = cwtpot;
+    u.pwtold = pwtold;
+    for (int ip = 0; ip < npairs; ++ip) {
+        if (irefpcof_host[ip] < 0 || irefpcof_host[ip] >= nsets) {
+            epsr_set_error("epsr_ep_update: pair %d refers to coefficient set %d of %d", ip, irefpcof_host[ip], nsets);
+            return EPSR_ERR_ARG;
+        }
+        u.iref[ip] = irefpcof_host[ip];
+    }
+    const int n = nsets * (nterms - 1);
+    ep_update_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(u);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
+
+extern "C" int epsr_pack_tables(int32_t npairs, int32_t ld, const float *xavs, const float *xavs1,
+                                const float *ecoul, const float *ecoul1, float *tab, void *stream) {
+    if (npairs < 1 || ld < 2 || !xavs || !xavs1 || !ecoul || !ecoul1 || !tab || ((uintptr_t)tab & 15)) {
+        epsr_set_error("epsr_pack_tables: bad arguments (tab must be 16-byte aligned)");
+        return EPSR_ERR_ARG;
+    }
+    const int n = npairs * ld;
+    ep_pack_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, xavs, xavs1, ecoul, ecoul1, (float4 *)tab);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
 
 extern "C" int epsr_generate_ep(int32_t npairs, int32_t npt, int32_t npt2, int32_t nterms, const float *expgr,
                                 float *pcoefp, int32_t nsets, int32_t ldc, const int32_t *irefpcof_host, float dmax,

@@ -4,8 +4,9 @@
 // path, in its order: the cell list (:1259), fmolec1 (:1265), ntimes molfit cycles
 // (:1280-1318), atogen (:1397), gensq (:1400), the per-data-set differences of ptgnsq
 // (:3844-3867), press (:1842 -> ato_manipulation_rev4.py:3903), fit_expansion for every
-// data set (ptgnsq :3936), the running averages sumsq and sumgr (:1611-1642) and stog of the
-// simulated S(Q) (:1987).  Every stage is the C ABI
+// data set (ptgnsq :3936), optionally the EP refinement that follows the fits (ptgnsq
+// :3948-3962 and generate_ep :4014, then the packed tables of the next iteration's energies),
+// the running averages sumsq and sumgr (:1611-1642) and stog of the simulated S(Q) (:1987).  Every stage is the C ABI
 // routine of that name, launched on the caller's stream from this thread, so a host that
 // advances many boxes on many threads does no per-launch work in an interpreter.  Host
 // reads happen where the routines need them (the cell list's region size, store and
@@ -57,8 +58,16 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
                        (long long)need);
         return EPSR_ERR_CAPACITY;
     }
-    memset(rep, 0, sizeof(*rep));
     const epsr_box_t *b = it->box;
+    if (it->refine && (b->izcut != b->npt2 || !it->pcoefp || !it->irefpcof_host || !it->efacp || !it->cwtpot ||
+                       !it->expgr || !it->wfac || !it->ecoul || !it->ecoul1 || !it->xavs || !it->xavs1 ||
+                       !it->xavtot || !it->xavtot1 || !it->ep_pwtold || !it->potfac || !it->ep_result || !it->tab ||
+                       it->tab != b->tab)) {
+        epsr_set_error("epsr_iteration_step: EP refinement needs its buffers, tab == box->tab and izcut == npt2 "
+                       "(izcut %d, npt2 %d)", b->izcut, b->npt2);
+        return EPSR_ERR_ARG;
+    }
+    memset(rep, 0, sizeof(*rep));
     cudaStream_t s = (cudaStream_t)stream;
     int rc;
 
@@ -149,8 +158,24 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
     if (rc) return rc;
     mark(it, 6, 1, s);
 
-    // ---- running averages of S(Q) and g(r) (runepsr17 :1611-1642)
+    // ---- EP refinement: ptgnsq's coefficient increment, generate_ep(.false.), the packed tables
     mark(it, 7, 0, s);
+    if (it->refine) {
+        rc = epsr_ep_update(it->ndata, b->npairs, it->nterms, it->pcoefp, it->nsets, it->ldc, it->irefpcof_host,
+                            it->efacp, it->cwtpot, it->fit_wtold, it->nterms + 1, it->pfact, stream);
+        if (rc) return rc;
+        rc = epsr_generate_ep(b->npairs, b->ld - 1, b->npt2, it->nterms, it->expgr, it->pcoefp, it->nsets, it->ldc,
+                              it->irefpcof_host, it->dmax, b->xstar, it->wfac, it->ecoul, it->xavs, it->xavs1,
+                              it->xavtot, it->xavtot1, b->ld, it->ep_pwtold, it->absolute_energy, it->erequnit,
+                              it->ereqstep, it->potfacamp, it->potfac, 0, it->ep_result, stream);
+        if (rc) return rc;
+        rc = epsr_pack_tables(b->npairs, b->ld, it->xavs, it->xavs1, it->ecoul, it->ecoul1, it->tab, stream);
+        if (rc) return rc;
+    }
+    mark(it, 7, 1, s);
+
+    // ---- running averages of S(Q) and g(r) (runepsr17 :1611-1642)
+    mark(it, 8, 0, s);
     if (it->nsum < 1) {
         epsr_set_error("epsr_iteration_step: nsum %d < 1", it->nsum);
         return EPSR_ERR_ARG;
@@ -163,13 +188,13 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
     rc = epsr_sumgr(it->npt1, b->npairs, it->wav, it->ldw, it->ycoh, fc1, fc2, it->gorintra, it->gorinter,
                     it->gr2intra, it->gr2inter, it->entsig, stream);
     if (rc) return rc;
-    mark(it, 7, 1, s);
+    mark(it, 8, 1, s);
 
     // ---- stog of the simulated intermolecular S(Q)
-    mark(it, 8, 0, s);
+    mark(it, 9, 0, s);
     rc = epsr_stog(it->rho, it->q, ldq, inter, it->r, it->nr, b->npairs, it->nqmin, it->nqmax, it->xwt, it->gofr,
                    it->scratch, it->scratch_bytes, stream);
     if (rc) return rc;
-    mark(it, 8, 1, s);
+    mark(it, 9, 1, s);
     return EPSR_OK;
 }

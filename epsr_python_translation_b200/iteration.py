@@ -2,9 +2,11 @@
 epsr_standalone_rev3.py:1235-1842, restricted to the hot path).
 
 Per call of ``step()``: cell list (:1265), fmolec1 (:1280), ``ntimes`` molfit cycles
-(:1314-1318), atogen (:1397), gensq (:1400), one fit_expansion per dataset on the
-difference between data and the weighted simulated S(Q) (ptgnsq :3846-3944), and stog of
-the simulated S(Q) (:1987).  All state stays on the GPU; per-stage device times are
+(:1314-1318), atogen (:1397), gensq (:1400), press (:1655), one fit_expansion per dataset on
+the difference between data and the weighted simulated S(Q) (ptgnsq :3846-3944), the EP
+refinement that follows the fits when the workload has one (ptgnsq :3948-3962, generate_ep
+:4014; the next iteration's energies use the refined tables), the running averages
+(:1611-1642) and stog of the simulated S(Q) (:1987).  All state stays on the GPU; per-stage device times are
 recorded with CUDA events on the launching stream.
 """
 
@@ -15,13 +17,13 @@ import torch
 
 import ctypes as C
 
-from . import _lib, transforms
+from . import _lib, potential, transforms
 from .box import BoxArrays, Ran1State, trsteps
 from .configs import Workload
 from .device import DeviceBox, press_scalars
 
 f32 = np.float32
-STAGES = ("cells", "fmolec1", "molfit", "atogen", "gensq", "press", "fit_expansion", "sums", "stog")
+STAGES = ("cells", "fmolec1", "molfit", "atogen", "gensq", "press", "fit_expansion", "ep", "sums", "stog")
 
 
 class EpsrIteration:
@@ -62,12 +64,48 @@ class EpsrIteration:
         self.r = torch.from_numpy(b.x[: b.npt1 + 1].copy()).to(dev)
         self.nqmin = torch.full((b.npairs,), 2, dtype=torch.int32, device=dev)
         self.nqmax = torch.full((b.npairs,), wl.nq, dtype=torch.int32, device=dev)
+        self.ep = wl.ep
+        if self.ep is not None:
+            self._ep_setup()
         self.events = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                        for k in STAGES}
         self.moves_per_step = wl.ntimes * b.nmol
         self.volume = f32(float(wl.system.L) ** 3)          # box volume (A^3) for press
         self.pair_updates = 0
         self.fit_trials = 0
+
+    def _ep_setup(self):
+        """Device state of the EP refinement: the r-space basis (built once on the host; the
+        reference rebuilds the same matrix inside every generate_ep call), the coefficient
+        sets, the unpacked tables and the potential factor.  A refined EP's gradient is
+        nonzero at the last table point, so the energies read the tables up to npt2."""
+        ep, b, d, wl = self.ep, self.box, self.d, self.wl
+        dev = d.dev
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, f32)).to(dev)  # noqa: E731
+        expgr, _ = potential.basis(b.npt2, wl.nterms, b.x, False, ep.pdmin, ep.pdstep, ep.pdmax, ep.psigma2, ep.rho,
+                                   ep.rbroad)
+        self.ep_expgr = t(expgr)
+        self.ep_pcoefp = t(ep.pcoefp)
+        self.ep_iref = np.ascontiguousarray(ep.iref, np.int32)
+        self.ep_efacp = t(ep.efacp)
+        self.ep_wfac = t(ep.wfac)
+        self.ep_ecoul, self.ep_ecoul1 = t(b.ecoul), t(b.ecoul1)
+        self.ep_tabs = {"xavs": t(b.xavs), "xavs1": t(b.xavs1), "xavtot": t(b.ecoul + b.xavs),
+                        "xavtot1": t(b.ecoul1 + b.xavs1)}
+        self.ep_pwtold = torch.zeros(wl.nterms + 1, dtype=torch.float32, device=dev)
+        self.ep_potfac = t([ep.potfac])
+        self.ep_result = torch.zeros(2, dtype=torch.float32, device=dev)
+        d.izcut = b.npt2
+        d.cbox.izcut = b.npt2
+
+    def _ep_refine(self):
+        ep, b, d, wl = self.ep, self.box, self.d, self.wl
+        potential.ep_update(self.ep_pcoefp, self.ep_iref, self.ep_efacp, self.weights, self.pwtold, ep.potfac)
+        potential.generate_ep(b.npt, b.npt2, wl.nterms, self.ep_expgr, self.ep_pcoefp, self.ep_iref, b.dmax, d.xstar,
+                              self.ep_wfac, self.ep_ecoul, self.ep_tabs, self.ep_pwtold, ep.absolute_energy,
+                              ep.erequnit, ep.ereqstep, ep.potfacamp, self.ep_potfac, changepotfac=False,
+                              result=self.ep_result)
+        potential.pack_tables(self.ep_tabs["xavs"], self.ep_tabs["xavs1"], self.ep_ecoul, self.ep_ecoul1, d.tab)
 
     def _mark(self, stage, end=False):
         self.events[stage][1 if end else 0].record()
@@ -121,6 +159,10 @@ class EpsrIteration:
         self.stepp = res["stepr"]
         self.fit_trials = int(res["trials"].sum())
         self._mark("fit_expansion", True)
+        self._mark("ep")
+        if self.ep is not None:
+            self._ep_refine()
+        self._mark("ep", True)
         self._mark("sums")
         self.nsum += 1
         fc1 = float(np.float32(1.0) / np.float32(self.nsum))
@@ -188,6 +230,18 @@ class EpsrIteration:
         it.soqintra, it.soqinter, it.sq2intra, it.sq2inter = (P(self.sums_sq[k]) for k in transforms.SQ_ARRAYS)
         it.gorintra, it.gorinter, it.gr2intra, it.gr2inter, it.entsig = (
             P(self.sums_gr[k]) for k in transforms.GR_ARRAYS)
+        if self.ep is not None:
+            ep = self.ep
+            it.refine = 1
+            it.pcoefp, it.nsets, it.ldc = P(self.ep_pcoefp), self.ep_pcoefp.shape[0], self.ep_pcoefp.shape[1]
+            it.irefpcof_host = self.ep_iref.ctypes.data_as(C.c_void_p)
+            it.efacp, it.cwtpot, it.expgr, it.wfac = P(self.ep_efacp), P(self.weights), P(self.ep_expgr), P(self.ep_wfac)
+            it.ecoul, it.ecoul1 = P(self.ep_ecoul), P(self.ep_ecoul1)
+            it.xavs, it.xavs1, it.xavtot, it.xavtot1 = (P(self.ep_tabs[k]) for k in potential.TABLES)
+            it.ep_pwtold, it.potfac, it.ep_result = P(self.ep_pwtold), P(self.ep_potfac), P(self.ep_result)
+            it.pfact, it.absolute_energy, it.erequnit = ep.potfac, ep.absolute_energy, ep.erequnit
+            it.ereqstep, it.potfacamp = ep.ereqstep, ep.potfacamp
+            it.tab = P(d.tab)
         it.strict = 1 if self.strict else 0
         for k, name in enumerate(STAGES):       # the Python step has created these events
             it.stage_events[2 * k] = self.events[name][0].cuda_event

@@ -79,3 +79,28 @@ def generate_ep(npt, npt2, nterms, expgr, pcoefp, iref, dmax, xstar, wfac, ecoul
                                _p(pwtold), f32(absolute_energy), f32(erequnit), f32(ereqstep), f32(potfacamp),
                                _p(potfac), int(bool(changepotfac)), _p(result), _s()))
     return result
+
+
+def ep_update(pcoefp, iref, efacp, cwtpot, pwtold, pfact):
+    """ptgnsq's coefficient increment (epsr_standalone_rev3.py:3948-3962) after the fits of all
+    data sets, in place on ``pcoefp`` (nsets, ldc): efacp (nsets,), cwtpot (ndata, npairs) and
+    pwtold (ndata, ldw) device tensors, iref a host int array, pfact the potential factor."""
+    lib = _lib.load(require_device=True)
+    nsets, ldc = pcoefp.shape
+    ndata, npairs = cwtpot.shape
+    ldw = pwtold.shape[1]
+    ir = np.ascontiguousarray(np.asarray(iref, np.int32))
+    if ir.shape[0] != npairs or pwtold.shape[0] != ndata or efacp.numel() < nsets:
+        raise ValueError("ep_update: inconsistent shapes")
+    check(lib.epsr_ep_update(int(ndata), int(npairs), int(ldw - 1), _p(pcoefp), int(nsets), int(ldc),
+                             ir.ctypes.data_as(C.c_void_p), _p(efacp), _p(cwtpot), _p(pwtold), int(ldw), f32(pfact),
+                             _s()))
+
+
+def pack_tables(xavs, xavs1, ecoul, ecoul1, tab):
+    """The packed {xavs, xavs1, ecoul, ecoul1} table of the energy kernels (npairs*ld*4,)."""
+    lib = _lib.load(require_device=True)
+    npairs, ld = xavs.shape
+    if tab.numel() < 4 * npairs * ld or any(tuple(t.shape) != (npairs, ld) for t in (xavs1, ecoul, ecoul1)):
+        raise ValueError("pack_tables: inconsistent shapes")
+    check(lib.epsr_pack_tables(int(npairs), int(ld), _p(xavs), _p(xavs1), _p(ecoul), _p(ecoul1), _p(tab), _s()))

@@ -312,6 +312,24 @@ int epsr_generate_ep(int32_t npairs, int32_t npt, int32_t npt2, int32_t nterms, 
                      int32_t ld, float *pwtold, float absolute_energy, float erequnit, float ereqstep,
                      float potfacamp, float *potfac, int32_t changepotfac, float *result, void *stream);
 
+/* The coefficient increment of ptgnsq epsr_standalone_rev3.py:3948-3962 after the fits of all
+ * ndata data sets: for each data set id in turn, each coefficient ic = 2..nterms and each pair
+ * ip in order, pcoefp(ic, k) += ((pfact * efacp(k)) * cwtpot(ip, id)) * pwtold_id(ic) with k the
+ * pair's set (float32, bit-identical).  pfact is the reference's potadd (= potfac).
+ *   pcoefp   device [nsets][ldc] in place; irefpcof_host host [npairs] (0-based sets,
+ *            npairs <= 960); efacp device [nsets]; cwtpot device [ndata][npairs];
+ *   pwtold   device [ndata][ldw] (each data set's fitted coefficients, 1-based).
+ * Asynchronous on `stream`. */
+int epsr_ep_update(int32_t ndata, int32_t npairs, int32_t nterms, float *pcoefp, int32_t nsets, int32_t ldc,
+                   const int32_t *irefpcof_host, const float *efacp, const float *cwtpot, const float *pwtold,
+                   int32_t ldw, float pfact, void *stream);
+
+/* The packed tables of epsr_box_t.tab from the four tables: tab[(pair*ld + j)*4 + {0,1,2,3}] =
+ * {xavs, xavs1, ecoul, ecoul1}[pair*ld + j] (device, [npairs][ld] each; tab 16-byte aligned).
+ * No reference counterpart: the reference reads the four arrays directly.  Asynchronous. */
+int epsr_pack_tables(int32_t npairs, int32_t ld, const float *xavs, const float *xavs1, const float *ecoul,
+                     const float *ecoul1, float *tab, void *stream);
+
 /* calc_pwrexpr_grad epsr_standalone_rev3.py:5230-5309 (the power-exponential basis, with the
  * spacing of dnext :5312) and calc_gaussr_grad :5046-5096 (the Gaussian basis): host
  * functions, the C library's logf/expf as the reference.  xin host [lpt+1] (1-based), expr
@@ -326,7 +344,8 @@ int epsr_calc_gaussr_grad(int32_t lpt, int32_t nterms, float dstep, float dmax, 
 /* One EPSR iteration of the path on one box, driven from native code: the iteration body of
  * runepsr17 (epsr_standalone_rev3.py:1235-1842) restricted to this path -- cell list,
  * fmolec1, ntimes molfit cycles, atogen, gensq, the per-data-set differences of ptgnsq,
- * press, fit_expansion over all data sets, the running averages sumsq and sumgr, stog --
+ * press, fit_expansion over all data sets, the EP refinement (optional), the running averages
+ * sumsq and sumgr, stog --
  * each stage the routine of that name
  * above, launched on `stream` from the calling thread.  The caller owns every buffer. */
 typedef struct {
@@ -381,13 +400,28 @@ typedef struct {
     int32_t nsum;
     float *soqintra, *soqinter, *sq2intra, *sq2inter;           /* [npairs][nq+1] */
     float *gorintra, *gorinter, *gr2intra, *gr2inter, *entsig;  /* [npairs][ldw] */
+    /* EP refinement after the fits, when refine != 0: ptgnsq's coefficient increment
+     * (:3948-3962, epsr_ep_update) with pfact = potadd, generate_ep(.false.) (:4014) and the
+     * repacked box->tab for the next iteration.  Tables [npairs][box->ld]; box->izcut must be
+     * box->npt2 (a refined EP's gradient is nonzero at the last table point). */
+    int32_t refine;
+    float *pcoefp;                    /* [nsets][ldc] */
+    int32_t nsets, ldc;
+    const int32_t *irefpcof_host;     /* [npairs] host, 0-based */
+    const float *efacp, *cwtpot;      /* [nsets], [ndata][npairs] */
+    const float *expgr, *wfac;        /* [npt2][nterms] basis, [ld] truncation */
+    const float *ecoul, *ecoul1;      /* [npairs][ld] */
+    float *xavs, *xavs1, *xavtot, *xavtot1;   /* [npairs][ld] */
+    float *ep_pwtold, *potfac, *ep_result;    /* [nterms+1], [1], [2] = {energabs, pressfac} */
+    float pfact, absolute_energy, erequnit, ereqstep, potfacamp;
+    float *tab;                       /* box->tab, written */
     /* one scratch block shared by the stages (epsr_iteration_scratch_bytes) */
     void *scratch;
     int64_t scratch_bytes;
     int32_t strict;
     void *stage_events[20];           /* NULL or CUDA events recorded at the start and end of
-                                         cells, fmolec1, molfit, atogen, gensq, press, fit, sums,
-                                         stog */
+                                         cells, fmolec1, molfit, atogen, gensq, press, fit, ep,
+                                         sums, stog */
 } epsr_iteration_t;
 
 typedef struct {

@@ -1082,6 +1082,60 @@ void oracle_generate_ep(int npairs, int npt, int npt2, int nterms, const float *
     out2[1] = pressfac;
 }
 
+/* calc_pwrexpr_grad epsr_standalone_rev3.py:5230-5309 (with fctrln lngamma_mod.py:16-32 and
+ * dnext :5312-5326): expr [lpt][nterms] from xin[1..lpt]; returns ncfirst, or -1 when a term
+ * needs a log-factorial beyond the table (an index error in the reference). */
+int oracle_calc_pwrexpr_grad(int lpt, int nterms, float dmin, float dstep, float dmax, float sigmab, float rho,
+                             const float *xin, float *expr, float rmin, int ncfirst, float fbroad, float rbroad) {
+    const float pi = 3.141592653f, expmax = 25.0f;
+    const int ntmax = (int)(dmax / sigmab + 3.0f);
+    double *gamln = (double *)malloc(sizeof(double) * (size_t)(ntmax + 2));
+    double g = 0.0, a = 0.0;
+    for (int i = 1; i <= ntmax + 1; ++i) {
+        gamln[i] = g;
+        a = a + 1.0;
+        g = g + log(a);
+    }
+    float d = dstep, rootd = 1.0f;
+    for (int m = 1; m <= nterms; ++m) {
+        if (d < rmin) ncfirst = m + 1;
+        const float sigma = rootd * fbroad * sigmab;
+        const int n = (sigma <= d && sigma > 0.0f && m > 1) ? (int)(d / sigma - 1.0f) : 0;
+        const int nref = n + 3;
+        if (nref > ntmax + 1) {
+            free(gamln);
+            return -1;
+        }
+        const float gfac = 4.0f * pi * rho * sigma * sigma * sigma;
+        float sigln = (float)(gamln[nref] + (double)logf(gfac));
+        if (m == 1) sigln = sigln - rmin / sigma;
+        for (int i = 1; i <= lpt; ++i) {
+            const float r = xin[i], rsigma = r / sigma;
+            float fact = rbroad * r, expon;
+            if (r > 0.0f) {
+                expon = (float)n * logf(rsigma) - rsigma - sigln - fact;
+                fact = (float)n / r - 1.0f / sigma - rbroad;
+            } else if (n == 0 || n == 1) {
+                expon = -rsigma - sigln - fact;
+                fact = n == 0 ? -(1.0f / sigma + rbroad) : 1.0f / sigma;
+            } else {
+                expon = -2.0f * expmax;
+                fact = 0.0f;
+            }
+            expr[(size_t)(i - 1) * nterms + (m - 1)] = expon > -expmax ? fact * expf(expon) : 0.0f;
+        }
+        float dn = d + dstep;
+        const float dtest = d * dmin;
+        if (dtest > dn) {
+            dn = dtest;
+            rootd = rootd * sqrtf(dmin);
+        }
+        d = dn;
+    }
+    free(gamln);
+    return ncfirst;
+}
+
 /* ------------------------------------------------------------------ stog */
 /* ato_manipulation_rev4.py:4067-4121. sofq [npairs][ldq] (i 1-based), q [ldq], r [nr+1]
  * (1-based), gofr out [npairs][nr+1]. */

@@ -376,6 +376,35 @@ def generate_ep(npt, npt2, nterms, expgr, pcoefp, iref, dmax, xstar, wfac, ecoul
     return out, pc, pw, pf[0], o2[0], o2[1]
 
 
+def calc_pwrexpr_grad(lpt, nterms, dmin, dstep, dmax, sigmab, rho, x, rmin=0.0, fbroad=1.0, rbroad=0.0):
+    """calc_pwrexpr_grad epsr_standalone_rev3.py:5230-5309 (C restatement): the r-space basis
+    (lpt*nterms,) on x[1..lpt] (x 1-based)."""
+    out = np.zeros(int(lpt) * int(nterms), f32)
+    nc = lib().oracle_calc_pwrexpr_grad(int(lpt), int(nterms), C.c_float(f32(dmin)), C.c_float(f32(dstep)),
+                                        C.c_float(f32(dmax)), C.c_float(f32(sigmab)), C.c_float(f32(rho)),
+                                        ptr(np.ascontiguousarray(x, f32)), ptr(out), C.c_float(f32(rmin)), 0,
+                                        C.c_float(f32(fbroad)), C.c_float(f32(rbroad)))
+    if nc < 0:
+        raise IndexError("calc_pwrexpr_grad: log-factorial table too short")
+    return out
+
+
+def ep_update(pcoefp, iref, efacp, cwtpot, pwtold, pfact):
+    """ptgnsq's coefficient increment epsr_standalone_rev3.py:3948-3962, per data set id in
+    turn: pcoefp(ic, k) += ((pfact * efacp(k)) * cwtpot(ip, id)) * pwtold_id(ic) for ic =
+    2..nterms and every pair ip (set k = iref[ip]) in order, float32.  pcoefp (nsets, ldc)
+    [set, ic]; cwtpot (ndata, npairs); pwtold (ndata, nterms+1).  Returns an updated copy."""
+    pc = np.array(pcoefp, f32)
+    pfact = f32(pfact)
+    nterms = pwtold.shape[1] - 1
+    for d in range(cwtpot.shape[0]):
+        pw = np.asarray(pwtold[d, 2: nterms + 1], f32)
+        for ip, k in enumerate(np.asarray(iref)):
+            fk = f32(pfact * f32(efacp[k]))
+            pc[k, 2: nterms + 1] = pc[k, 2: nterms + 1] + f32(fk * f32(cwtpot[d, ip])) * pw
+    return pc
+
+
 def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
     """q (ldq,), sofq_pairs (npairs, ldq) 1-based i; r (nr+1,) 1-based. Returns (npairs, nr+1)."""
     npairs, ldq = sofq_pairs.shape

@@ -33,6 +33,14 @@ class CpuIteration:
         self.rows = np.ascontiguousarray(wl.foqols.T)   # (nq+1, npt1+1)
         self.stage_s = {}
         self.pair_updates = 0
+        ep = wl.ep
+        if ep is not None:
+            b = self.box
+            self.pcoefp = np.array(ep.pcoefp, f32)
+            self.ep_pwtold = np.zeros(wl.nterms + 1, f32)
+            self.ep_tabs = {"xavs": b.xavs, "xavs1": b.xavs1, "xavtot": (b.ecoul + b.xavs).astype(f32),
+                            "xavtot1": (b.ecoul1 + b.xavs1).astype(f32)}
+            self.ep_par = np.array([ep.absolute_energy, ep.erequnit, ep.ereqstep, ep.potfacamp], f32)
 
     def step(self, stages=None):
         wl, b = self.wl, self.box
@@ -76,6 +84,22 @@ class CpuIteration:
             self.pwtold[k] = res["wtold"]
             self.stepp[k] = res["stepr"]
         t["fit_expansion"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ep = wl.ep
+        if ep is not None:
+            # ptgnsq's coefficient increment, then generate_ep(.false.), which rebuilds its basis
+            # on every call as the reference does; the next iteration's energies read the tables
+            expgr = oracle.calc_pwrexpr_grad(b.npt2, wl.nterms, ep.pdmin, ep.pdstep, ep.pdmax, ep.psigma2, ep.rho, b.x,
+                                             rbroad=ep.rbroad)
+            self.pcoefp = oracle.ep_update(self.pcoefp, ep.iref, ep.efacp, wl.weights, np.stack(self.pwtold),
+                                           ep.potfac)
+            tabs, self.pcoefp, self.ep_pwtold, _, _, _ = oracle.generate_ep(
+                b.npt, b.npt2, wl.nterms, expgr, self.pcoefp, ep.iref, b.dmax, b.xstar, ep.wfac, b.ecoul, self.ep_tabs,
+                self.ep_pwtold, self.ep_par, ep.potfac, False)
+            b.xavs[...] = tabs["xavs"]
+            b.xavs1[...] = tabs["xavs1"]
+            self.ep_tabs = {"xavs": b.xavs, "xavs1": b.xavs1, "xavtot": tabs["xavtot"], "xavtot1": tabs["xavtot1"]}
+        t["ep"] = time.perf_counter() - t0
         t0 = time.perf_counter()
         self.nsum = getattr(self, "nsum", 0) + 1
         fc1 = float(f32(1.0) / f32(self.nsum))

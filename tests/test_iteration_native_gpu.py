@@ -34,6 +34,9 @@ def test_native_iteration_matches_python_driver(strict):
     assert np.float32(a.energy) == np.float32(b.energy) and np.float32(a.pressc) == np.float32(b.pressc)
     assert tuple(map(np.float32, a.ftest)) == tuple(map(np.float32, b.ftest))
     assert a.nsum == b.nsum == 3
+    assert a.ep is not None              # the workload refines its EP every iteration
+    assert np.array_equal(a.ep_pcoefp.cpu().numpy().view(np.uint32), b.ep_pcoefp.cpu().numpy().view(np.uint32))
+    assert np.array_equal(a.d.tab.cpu().numpy().view(np.uint32), b.d.tab.cpu().numpy().view(np.uint32))
     for k, v in {**a.sums_sq, **a.sums_gr}.items():
         w = {**b.sums_sq, **b.sums_gr}[k]
         assert np.array_equal(v.cpu().numpy().view(np.uint32), w.cpu().numpy().view(np.uint32)), k
