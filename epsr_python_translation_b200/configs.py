@@ -576,7 +576,7 @@ class Workload:
     expr: np.ndarray         # (nq*nterms+1,) 1-based flat, row-major by Q
     nterms: int
     data: np.ndarray         # (ndata, nq+1) synthetic interference functions
-    weights: np.ndarray      # (ndata, npairs) pair weights of each dataset
+    weights: np.ndarray      # (ndata, npairs) float64 pair weights of each dataset (real*8 cwt)
     wholerot: np.ndarray
     wholetrans: np.ndarray
     ntimes: int = 5
@@ -616,7 +616,7 @@ def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, nd
     F, ycoh = transform_table(s, q, npt1)
     ep = ep_refinement(s, nterms) if refine else None
     expr = pwrexpq_basis(q, nterms, ep.pdmin, ep.pdstep, ep.psigma2) if refine else ep_basis(q, nterms)
-    w = rng.uniform(0.2, 1.0, size=(ndata, s.npairs)).astype(f32)
+    w = rng.uniform(0.2, 1.0, size=(ndata, s.npairs))
     w /= w.sum(axis=1, keepdims=True)
     data = np.zeros((ndata, nq + 1), dtype=f32)
     qq = q.astype(np.float64)

@@ -205,13 +205,15 @@ __global__ void __launch_bounds__(EP_COEF_THREADS) ep_coeff_kernel(const __grid_
 }
 
 // The coefficient increment of ptgnsq epsr_standalone_rev3.py:3948-3962 for every data set in
-// turn: pcoefp(ic, k) += ((pfact * efacp(k)) * cwtpot(ip, id)) * pwtold_id(ic) for each pair ip
-// of set k, in pair order, float32 throughout.  One thread per (set, coefficient).
+// turn: pcoefp(ic, k) = real(dble(pcoefp(ic, k)) + (dble(pfact * efacp(k)) * cwtpot(ip, id)) *
+// dble(pwtold_id(ic))) for each pair ip of set k, in pair order -- cwtpot is real*8, so the
+// increment is formed in double and rounded once per step.  One thread per (set, coefficient).
 struct EpUpdate {
     int ndata, npairs, nterms, nsets, ldc, ldw;
     float pfact;
     float *pcoefp;
-    const float *efacp, *cwtpot, *pwtold;
+    const float *efacp, *pwtold;
+    const double *cwtpot;
     int32_t iref[EP_MAX_PAIRS];
 };
 
@@ -222,11 +224,13 @@ __global__ void ep_update_kernel(const __grid_constant__ EpUpdate u) {
     const int k = q / w, ic = 2 + q % w;
     float *p = u.pcoefp + (size_t)k * u.ldc + ic;
     float v = *p;
-    const float fk = __fmul_rn(u.pfact, u.efacp[k]);
+    const double fk = (double)__fmul_rn(u.pfact, u.efacp[k]);
     for (int id = 0; id < u.ndata; ++id) {
-        const float pw = u.pwtold[(size_t)id * u.ldw + ic];
+        const double pw = (double)u.pwtold[(size_t)id * u.ldw + ic];
         for (int ip = 0; ip < u.npairs; ++ip)
-            if (u.iref[ip] == k) v = __fadd_rn(v, __fmul_rn(__fmul_rn(fk, u.cwtpot[(size_t)id * u.npairs + ip]), pw));
+            if (u.iref[ip] == k)
+                v = __double2float_rn(
+                    __dadd_rn((double)v, __dmul_rn(__dmul_rn(fk, u.cwtpot[(size_t)id * u.npairs + ip]), pw)));
     }
     *p = v;
 }
@@ -244,7 +248,7 @@ __global__ void ep_pack_kernel(int n, const float *xavs, const float *xavs1, con
 using namespace epsr;
 
 extern "C" int epsr_ep_update(int32_t ndata, int32_t npairs, int32_t nterms, float *pcoefp, int32_t nsets,
-                              int32_t ldc, const int32_t *irefpcof_host, const float *efacp, const float *cwtpot,
+                              int32_t ldc, const int32_t *irefpcof_host, const float *efacp, const double *cwtpot,
                               const float *pwtold, int32_t ldw, float pfact, void *stream) {
     if (ndata < 1 || npairs < 1 || npairs > EP_MAX_PAIRS || nterms < 2 || nsets < 1 || ldc < nterms + 1 ||
         ldw < nterms + 1 || !pcoefp || !irefpcof_host || !efacp || !cwtpot || !pwtold) {

@@ -84,16 +84,20 @@ __global__ void stog_kernel(float rho, const float *q, int ldq, const float *sof
 }
 
 // The simulated fit of each data set (ptgnsq epsr_standalone_rev3.py:3844-3867): the sum
-// over atom pairs of weight x intermolecular S(Q), sequential in float32 as the reference,
-// and its difference from the data, negated: out = -(data - sum).  Thread per (set, Q).
-__global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *data, const float *cwt,
+// over atom pairs of weight x intermolecular S(Q), sequential over pairs as the reference --
+// the weights are real*8, so each step is sum = real(dble(sum) + cwt * dble(qwind)), one
+// rounding to float32 per pair -- and its difference from the data, negated:
+// out = -(data - sum).  Thread per (set, Q).
+__global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *data, const double *cwt,
                                    const float *qwind, float *out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int d = blockIdx.y;
     if (i > nq) return;
-    const float *w = cwt + (size_t)d * npairs;
+    const double *w = cwt + (size_t)d * npairs;
     float sum = 0.0f;
-    for (int ic = 0; ic < npairs; ++ic) sum = __fadd_rn(sum, __fmul_rn(__ldg(w + ic), __ldg(qwind + (size_t)ic * (nq + 1) + i)));
+    for (int ic = 0; ic < npairs; ++ic)
+        sum = __double2float_rn(__dadd_rn((double)sum, __dmul_rn(__ldg(w + ic),
+                                                                 (double)__ldg(qwind + (size_t)ic * (nq + 1) + i))));
     out[(size_t)d * (nq + 1) + i] = -__fsub_rn(data[(size_t)d * (nq + 1) + i], sum);
 }
 
@@ -101,7 +105,7 @@ __global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *d
 
 using namespace epsr;
 
-extern "C" int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const float *cwt,
+extern "C" int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const double *cwt,
                                       const float *qwind, float *out, void *stream) {
     if (ndata <= 0 || npairs <= 0 || nq <= 0 || !data || !cwt || !qwind || !out) {
         epsr_set_error("epsr_ptgnsq_difference: bad arguments");

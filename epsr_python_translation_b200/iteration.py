@@ -45,7 +45,8 @@ class EpsrIteration:
         self.ycoh = torch.from_numpy(np.ascontiguousarray(wl.ycoh[: b.npt + 1], f32)).to(dev)
         self.expr = torch.from_numpy(wl.expr).to(dev)
         self.data = torch.from_numpy(wl.data).to(dev)
-        self.weights = torch.from_numpy(np.ascontiguousarray(wl.weights, dtype=np.float32)).to(dev)
+        # the data-set weights cwt (and the potential weights cwtpot, the same here) are real*8
+        self.weights = torch.from_numpy(np.ascontiguousarray(wl.weights, dtype=np.float64)).to(dev)
         self._dt = torch.empty_like(self.data)
         self.natomsphere = torch.ones(b.ntype, dtype=torch.float32, device=dev)
         self.rminex = torch.full((b.npairs,), -2.0, dtype=torch.float32, device=dev)

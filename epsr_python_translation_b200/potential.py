@@ -83,8 +83,11 @@ def generate_ep(npt, npt2, nterms, expgr, pcoefp, iref, dmax, xstar, wfac, ecoul
 
 def ep_update(pcoefp, iref, efacp, cwtpot, pwtold, pfact):
     """ptgnsq's coefficient increment (epsr_standalone_rev3.py:3948-3962) after the fits of all
-    data sets, in place on ``pcoefp`` (nsets, ldc): efacp (nsets,), cwtpot (ndata, npairs) and
-    pwtold (ndata, ldw) device tensors, iref a host int array, pfact the potential factor."""
+    data sets, in place on ``pcoefp`` (nsets, ldc): efacp (nsets,), cwtpot (ndata, npairs,
+    float64: real*8 in the reference) and pwtold (ndata, ldw) device tensors, iref a host int
+    array, pfact the potential factor."""
+    if cwtpot.dtype != torch.float64:
+        raise ValueError("ep_update: cwtpot is real*8 in the reference; pass a float64 tensor")
     lib = _lib.load(require_device=True)
     nsets, ldc = pcoefp.shape
     ndata, npairs = cwtpot.shape

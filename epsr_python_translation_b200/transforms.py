@@ -43,8 +43,11 @@ def gensq(nq, npt1, wav, ldw, foqols, sj, si, ycoh, n2extr, natomsphere, npairs)
 def ptgnsq_difference(data, cwt, qwind, out=None):
     """The simulated fit of each data set and its negated difference from the data
     (ptgnsq epsr_standalone_rev3.py:3844-3867): -(data - cwt @ qwind), the sum over atom
-    pairs sequential in float32.  data (ndata, nq+1), cwt (ndata, npairs), qwind
-    (npairs, nq+1), all on the device."""
+    pairs sequential, each step in double and rounded to float32 (the weights are real*8).
+    data (ndata, nq+1) float32, cwt (ndata, npairs) float64, qwind (npairs, nq+1) float32,
+    all on the device."""
+    if cwt.dtype != torch.float64:
+        raise ValueError("ptgnsq_difference: cwt is real*8 in the reference; pass a float64 tensor")
     lib = _lib.load(require_device=True)
     ndata, ld = data.shape
     npairs = cwt.shape[1]

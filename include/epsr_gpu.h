@@ -229,10 +229,11 @@ int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float *wav, int32
 
 /* ptgnsq epsr_standalone_rev3.py:3844-3867 (the simulated fit of each data set, for the
  * potential refinement): out[d][i] = -(data[d][i] - sum_ic cwt[d][ic] * qwind[ic][i]), the
- * sum sequential in float32 over atom pairs ic.  data, out: [ndata][nq+1]; cwt:
- * [ndata][npairs]; qwind: [npairs][nq+1] (the intermolecular S(Q) of gensq).  Device
- * pointers; asynchronous on `stream`. */
-int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const float *cwt,
+ * sum sequential over atom pairs ic with the reference's real*8 weights: each step
+ * sum = real(dble(sum) + cwt * dble(qwind)).  data, out: [ndata][nq+1] float; cwt:
+ * [ndata][npairs] double; qwind: [npairs][nq+1] (the intermolecular S(Q) of gensq).  Device
+ * pointers; asynchronous on `stream`.  Bit-identical. */
+int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const double *cwt,
                            const float *qwind, float *out, void *stream);
 
 /* stog ato_manipulation_rev4.py:4067-4121 (+ lorch :4113).  q [ldq] 1-based, sofq
@@ -315,13 +316,14 @@ int epsr_generate_ep(int32_t npairs, int32_t npt, int32_t npt2, int32_t nterms, 
 /* The coefficient increment of ptgnsq epsr_standalone_rev3.py:3948-3962 after the fits of all
  * ndata data sets: for each data set id in turn, each coefficient ic = 2..nterms and each pair
  * ip in order, pcoefp(ic, k) += ((pfact * efacp(k)) * cwtpot(ip, id)) * pwtold_id(ic) with k the
- * pair's set (float32, bit-identical).  pfact is the reference's potadd (= potfac).
+ * pair's set: cwtpot is real*8, so the increment is formed in double and rounded once to
+ * float32 per step (bit-identical).  pfact is the reference's potadd (= potfac).
  *   pcoefp   device [nsets][ldc] in place; irefpcof_host host [npairs] (0-based sets,
- *            npairs <= 960); efacp device [nsets]; cwtpot device [ndata][npairs];
+ *            npairs <= 960); efacp device [nsets]; cwtpot device double [ndata][npairs];
  *   pwtold   device [ndata][ldw] (each data set's fitted coefficients, 1-based).
  * Asynchronous on `stream`. */
 int epsr_ep_update(int32_t ndata, int32_t npairs, int32_t nterms, float *pcoefp, int32_t nsets, int32_t ldc,
-                   const int32_t *irefpcof_host, const float *efacp, const float *cwtpot, const float *pwtold,
+                   const int32_t *irefpcof_host, const float *efacp, const double *cwtpot, const float *pwtold,
                    int32_t ldw, float pfact, void *stream);
 
 /* The packed tables of epsr_box_t.tab from the four tables: tab[(pair*ld + j)*4 + {0,1,2,3}] =
@@ -379,7 +381,8 @@ typedef struct {
     int64_t foqols_sj, foqols_si;
     const float *natomsphere;
     float *sofq;                      /* [2][npairs][nq+1] */
-    const float *data, *cwt;          /* [ndata][nq+1], [ndata][npairs] */
+    const float *data;                /* [ndata][nq+1] */
+    const double *cwt;                /* [ndata][npairs] (real*8, as the reference's weights) */
     float *dt;                        /* [ndata][nq+1] -(data - weighted S(Q)) */
     /* fit_expansion */
     const float *expr;
@@ -408,7 +411,8 @@ typedef struct {
     float *pcoefp;                    /* [nsets][ldc] */
     int32_t nsets, ldc;
     const int32_t *irefpcof_host;     /* [npairs] host, 0-based */
-    const float *efacp, *cwtpot;      /* [nsets], [ndata][npairs] */
+    const float *efacp;               /* [nsets] */
+    const double *cwtpot;             /* [ndata][npairs] (real*8) */
     const float *expgr, *wfac;        /* [npt2][nterms] basis, [ld] truncation */
     const float *ecoul, *ecoul1;      /* [npairs][ld] */
     float *xavs, *xavs1, *xavtot, *xavtot1;   /* [npairs][ld] */

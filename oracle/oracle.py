@@ -302,16 +302,18 @@ def atogen(box, ngrsamples, ran1, rminex, ycoh=None, sizefactor=1.0):
 # ----------------------------------------------------------------------------- transforms
 def ptgnsq_difference(data, cwt, qwind):
     """ptgnsq epsr_standalone_rev3.py:3844-3867: the simulated fit of data set d at Q index i
-    is the float32 sum over atom pairs ic, in order, of cwt[d, ic] * qwind[ic, i] (:3853-3854);
-    returned negated as the difference from the data, -(data - sum)."""
+    is the sum over atom pairs ic, in order, of cwt[d, ic] * qwind[ic, i] (:3853-3854); the
+    weights are real*8 (weights.py:23), so each step is sum = real(dble(sum) + cwt *
+    dble(qwind)): product and sum in double, one rounding to float32.  Returned negated as
+    the difference from the data, -(data - sum)."""
     data = np.asarray(data, np.float32)
-    cwt = np.asarray(cwt, np.float32)
+    cwt = np.asarray(cwt, np.float64)
     qwind = np.asarray(qwind, np.float32)
     out = np.empty_like(data)
     for d in range(data.shape[0]):
         s = np.zeros(qwind.shape[1], np.float32)
         for ic in range(qwind.shape[0]):
-            s = (s + (cwt[d, ic] * qwind[ic]).astype(np.float32)).astype(np.float32)
+            s = (s.astype(np.float64) + cwt[d, ic] * qwind[ic].astype(np.float64)).astype(np.float32)
         out[d] = -(data[d] - s)
     return out
 
@@ -391,17 +393,20 @@ def calc_pwrexpr_grad(lpt, nterms, dmin, dstep, dmax, sigmab, rho, x, rmin=0.0, 
 
 def ep_update(pcoefp, iref, efacp, cwtpot, pwtold, pfact):
     """ptgnsq's coefficient increment epsr_standalone_rev3.py:3948-3962, per data set id in
-    turn: pcoefp(ic, k) += ((pfact * efacp(k)) * cwtpot(ip, id)) * pwtold_id(ic) for ic =
-    2..nterms and every pair ip (set k = iref[ip]) in order, float32.  pcoefp (nsets, ldc)
-    [set, ic]; cwtpot (ndata, npairs); pwtold (ndata, nterms+1).  Returns an updated copy."""
+    turn: pcoefp(ic, k) = real(dble(pcoefp) + (dble(pfact * efacp(k)) * cwtpot(ip, id)) *
+    dble(pwtold_id(ic))) for ic = 2..nterms and every pair ip (set k = iref[ip]) in order;
+    cwtpot is real*8 (weights.py:25), so each increment is formed in double and rounded once.
+    pcoefp (nsets, ldc) [set, ic]; cwtpot (ndata, npairs); pwtold (ndata, nterms+1).
+    Returns an updated copy."""
     pc = np.array(pcoefp, f32)
     pfact = f32(pfact)
     nterms = pwtold.shape[1] - 1
-    for d in range(cwtpot.shape[0]):
-        pw = np.asarray(pwtold[d, 2: nterms + 1], f32)
+    cw = np.asarray(cwtpot, np.float64)
+    for d in range(cw.shape[0]):
+        pw = np.asarray(pwtold[d, 2: nterms + 1], f32).astype(np.float64)
         for ip, k in enumerate(np.asarray(iref)):
-            fk = f32(pfact * f32(efacp[k]))
-            pc[k, 2: nterms + 1] = pc[k, 2: nterms + 1] + f32(fk * f32(cwtpot[d, ip])) * pw
+            fk = float(f32(pfact * f32(efacp[k])))
+            pc[k, 2: nterms + 1] = (pc[k, 2: nterms + 1].astype(np.float64) + (fk * cw[d, ip]) * pw).astype(f32)
     return pc
 
 

@@ -25,10 +25,10 @@ def test_ep_update_matches_oracle_with_shared_sets():
     pc = (rng.standard_normal((nsets, ldc)) * 0.1).astype(f32)
     iref = rng.integers(0, nsets, npairs).astype(np.int32)
     efacp = rng.uniform(0.5, 1.5, nsets).astype(f32)
-    cwtpot = rng.uniform(0.0, 1.0, (ndata, npairs)).astype(f32)
+    cwtpot = rng.uniform(0.0, 1.0, (ndata, npairs))            # real*8, general doubles
     pw = (rng.standard_normal((ndata, nterms + 1)) * 0.3).astype(f32)
     d = _dev(pc)
-    potential.ep_update(d, iref, _dev(efacp), _dev(cwtpot), _dev(pw), f32(0.2))
+    potential.ep_update(d, iref, _dev(efacp), _dev(cwtpot, torch.float64), _dev(pw), f32(0.2))
     want = oracle.ep_update(pc, iref, efacp, cwtpot, pw, f32(0.2))
     assert_bits_equal(d.cpu().numpy(), want, "pcoefp")
     assert not np.array_equal(want, pc)

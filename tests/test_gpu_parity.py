@@ -448,12 +448,13 @@ def test_fit_expansion_cluster_shapes_strict_match_oracle(npt, scale):
 @pytest.mark.gpu
 def test_ptgnsq_difference_bit_identical():
     """The per-data-set simulated fit and its difference from the data (ptgnsq
-    epsr_standalone_rev3.py:3844-3867) equals the oracle's sequential float32 sum bit for bit."""
+    epsr_standalone_rev3.py:3844-3867) equals the oracle's sequential sum (real*8 weights, one
+    float32 rounding per pair) bit for bit; the weights are general doubles."""
     from epsr_python_translation_b200 import transforms
     rng = np.random.default_rng(11)
     ndata, npairs, nq = 3, 21, 600
     data = rng.standard_normal((ndata, nq + 1)).astype(f32)
-    cwt = rng.uniform(0.0, 0.2, (ndata, npairs)).astype(f32)
+    cwt = rng.uniform(0.0, 0.2, (ndata, npairs))
     qwind = (rng.standard_normal((npairs, nq + 1)) * 0.3).astype(f32)
     got = transforms.ptgnsq_difference(torch.from_numpy(data).cuda(), torch.from_numpy(cwt).cuda(),
                                        torch.from_numpy(qwind).cuda()).cpu().numpy()
