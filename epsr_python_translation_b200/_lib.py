@@ -52,6 +52,14 @@ class Mc(C.Structure):
                 ("status", P)]
 
 
+class Intra(C.Structure):
+    """epsr_intra_t: the intramolecular model of en_atom_intra (device pointers)."""
+    _fields_ = [("nbond", P), ("iabond", P), ("tbond", P), ("maxbond", I32), ("imageatom", P), ("qtype", P),
+                ("amassa", P), ("amassr", P), ("xav", P), ("xav1", P), ("ngrot", P), ("stepcl", F32),
+                ("sizefactor", F32), ("tempb", F32), ("tempang", F32), ("simt", F32), ("refine_intra", I32),
+                ("refine_intra_fac", F32)]
+
+
 class Iteration(C.Structure):
     """epsr_iteration_t: one EPSR iteration of the path, driven natively."""
     _fields_ = [("box", P), ("mc", P),
@@ -113,6 +121,9 @@ _SIGS = {
                                    F32, F32, P, I32, P, P]),
     "epsr_ep_update": (C.c_int, [I32, I32, I32, P, I32, I32, P, P, P, P, I32, F32, P]),
     "epsr_pack_tables": (C.c_int, [I32, I32, P, P, P, P, P, P]),
+    "epsr_en_mole_intra": (C.c_int, [P, P, P, P]),
+    "epsr_molfit_shake_scratch_bytes": (I64, [I32, I32]),
+    "epsr_molfit_shake": (C.c_int, [P, P, P, P, F32, P, P, P, I64, P]),
     "epsr_calc_pwrexpr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
     "epsr_calc_gaussr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),

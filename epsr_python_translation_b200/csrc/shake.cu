@@ -1,0 +1,538 @@
+// shake.cu -- the intramolecular branch of molfit (molfit.py:124-174, the cycle taken when
+// nisum >= intra): every molecule's atoms moved at random (movei :545, movea :556), the change of
+// its intramolecular energy (en_change_intra :763 -> en_mole_intra :1327 -> en_atom_intra :923),
+// the Metropolis test and, on acceptance, the centre of mass put back at the molecule centre
+// (centreofmassi ato_manipulation_rev4.py:442); then the step adaptation (:465-536).  The
+// internal rotations of rotational groups (:175-245) are not part of this path: a box with
+// rotational groups is refused.
+//
+// Every moved molecule draws three values per atom and one for its test, so its place in the
+// ran1 stream is known before the cycle starts.  The stream is generated once; every
+// molecule's trial coordinates and new intramolecular energy are computed in parallel (one
+// thread per molecule, the atom pairs in the reference's order); one thread then walks the
+// molecules in order for the little that chains them: the first stored energy the test
+// compares against (the reference's ergold(1), which a molecule with an empty list inherits
+// from the molecule before it, and which an earlier accepted molecule rewrites when the two
+// share that slot), the running float32 sum faddb and the per-type counts.  Accepted moves are
+// applied in parallel.
+#include <string.h>
+
+#include "common.cuh"
+
+namespace epsr {
+
+constexpr int SH_THREADS = 1024;
+constexpr int SH_TILE = 1024;       // molecules per tile of the ordered pass
+
+struct IntraDev {
+    Lattice L;
+    const int32_t *naf, *nato, *mtype, *itype, *npairref, *ngrot;
+    const int32_t *nbond, *iabond, *imageatom, *qtype;
+    const float *tbond, *amassa, *amassr, *xav, *xav1, *xstar;
+    const float4 *tab;
+    int32_t maxbond, ld, npt2, ntype, natom, refine_intra;
+    float stepcl, sizefactor, tempb, tempang, simt, refine_intra_fac;
+};
+
+IntraDev make_intradev(const epsr_box_t *b, const epsr_intra_t *in) {
+    IntraDev I;
+    memset(&I, 0, sizeof(I));
+    I.L.cubic = b->cubic;
+    I.L.alatx = b->lat[0];
+    I.L.blatx = b->lat[1];
+    I.L.clatx = b->lat[2];
+    I.L.blaty = b->lat[3];
+    I.L.claty = b->lat[4];
+    I.L.clatz = b->lat[5];
+    I.naf = b->naf;
+    I.nato = b->nato;
+    I.mtype = b->mtype;
+    I.itype = b->itype;
+    I.npairref = b->npairref;
+    I.ngrot = in->ngrot;
+    I.nbond = in->nbond;
+    I.iabond = in->iabond;
+    I.imageatom = in->imageatom;
+    I.qtype = in->qtype;
+    I.tbond = in->tbond;
+    I.amassa = in->amassa;
+    I.amassr = in->amassr;
+    I.xav = in->xav;
+    I.xav1 = in->xav1;
+    I.xstar = b->xstar;
+    I.tab = (const float4 *)b->tab;
+    I.maxbond = in->maxbond;
+    I.ld = b->ld;
+    I.npt2 = b->npt2;
+    I.ntype = b->ntype;
+    I.natom = b->natom;
+    I.refine_intra = in->refine_intra;
+    I.stepcl = in->stepcl;
+    I.sizefactor = in->sizefactor;
+    I.tempb = in->tempb;
+    I.tempang = in->tempang;
+    I.simt = in->simt;
+    I.refine_intra_fac = in->refine_intra_fac;
+    return I;
+}
+
+// The bond of atom `a` to atom `ja` (first in a's list), or -1.
+__device__ __forceinline__ int find_bond(const IntraDev &I, int a, int ja) {
+    const int nb = min(I.nbond[a], I.maxbond);
+    for (int k = 0; k < nb; ++k)
+        if (I.iabond[(size_t)a * I.maxbond + k] == ja) return k;
+    return -1;
+}
+
+// The EP term refine_intra adds (molfit.py:993-996 / :1037-1040).
+__device__ __forceinline__ float ep_term(const IntraDev &I, int iz, int icref, float dtdif) {
+    const float4 t = I.tab[(size_t)icref * I.ld + iz];
+    return __fmul_rn(I.refine_intra_fac, __fadd_rn(t.x, __fmul_rn(t.y, dtdif)));
+}
+
+// en_atom_intra molfit.py:923-1045 for atoms ia, ja (0-based) of a molecule without rotational
+// groups (so no dihedral exclusions apply).
+__device__ float en_atom_intra_d(const IntraDev &I, int ia, int ja, float x1, float y1, float z1, float x2, float y2,
+                                 float z2) {
+    if (ja == I.imageatom[ia]) return 0.0f;
+    const int icref = I.npairref[I.itype[ia] * I.ntype + I.itype[ja]];
+    const bool notq = I.qtype[ia] == 0 && I.qtype[ja] == 0;
+    const float xdifs = __fsub_rn(x2, x1), ydifs = __fsub_rn(y2, y1), zdifs = __fsub_rn(z2, z1);
+    int image = ia, jref = find_bond(I, ia, ja);
+    if (jref < 0) {
+        image = I.imageatom[ia];
+        jref = (image >= 0 && image < I.natom) ? find_bond(I, image, ja) : -1;
+    }
+    if (jref >= 0) {
+        float xd = xdifs, yd = ydifs, zd = zdifs;
+        minimagec(I.L, xd, yd, zd);
+        const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(xd, xd), __fmul_rn(yd, yd)), __fmul_rn(zd, zd));
+        const float dtest = __fsqrt_rn(dsq);
+        const int iz = ifix(__fdiv_rn(dtest, I.stepcl)) + 2;
+        const float tbv = I.tbond[(size_t)image * I.maxbond + jref];
+        const float atb = fabsf(tbv);
+        const float tb = atb > I.stepcl ? atb : I.stepcl;      // max(stepcl, |tbond|)
+        float wtm = __fdiv_rn(I.amassr[icref], tb);
+        if (tbv < 0.0f) wtm = __fmul_rn(wtm, I.tempang);
+        const float ddif = __fsub_rn(tb, dtest);
+        float sume = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(wtm, ddif), ddif), I.tempb), I.simt);
+        if (I.refine_intra && iz <= I.npt2 && notq) sume = __fadd_rn(sume, ep_term(I, iz, icref, __fsub_rn(dtest, I.xstar[iz])));
+        return sume;
+    }
+    float xd = __fmul_rn(xdifs, I.sizefactor), yd = __fmul_rn(ydifs, I.sizefactor), zd = __fmul_rn(zdifs, I.sizefactor);
+    minimagec(I.L, xd, yd, zd);
+    const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(xd, xd), __fmul_rn(yd, yd)), __fmul_rn(zd, zd));
+    const float dtest = __fsqrt_rn(dsq);
+    const int iz = ifix(__fdiv_rn(dtest, I.stepcl)) + 2;
+    float sume = 0.0f;
+    if (iz <= I.npt2) {
+        const float dtdif = __fsub_rn(dtest, I.xstar[iz]);
+        const size_t k = (size_t)icref * I.ld + iz;
+        sume = __fadd_rn(I.xav[k], __fmul_rn(I.xav1[k], dtdif));
+        if (I.refine_intra && notq) sume = __fadd_rn(sume, ep_term(I, iz, icref, dtdif));
+    }
+    return sume;
+}
+
+// en_mole_intra molfit.py:1327-1350 on the coordinates x/y/z (indexed by global atom).
+__device__ float en_mole_intra_d(const IntraDev &I, int im, const float *x, const float *y, const float *z) {
+    const int a0 = I.naf[im], n = I.nato[im];
+    float e = 0.0f;
+    for (int i = 0; i < n - 1; ++i) {
+        const int ia = a0 + i;
+        const float x1 = x[ia], y1 = y[ia], z1 = z[ia];
+        for (int j = i + 1; j < n; ++j) {
+            const int ja = a0 + j;
+            e = __fadd_rn(e, en_atom_intra_d(I, ia, ja, x1, y1, z1, x[ja], y[ja], z[ja]));
+        }
+    }
+    return e;
+}
+
+__global__ void en_mole_intra_kernel(IntraDev I, int nmol, const float *xa, const float *ya, const float *za,
+                                     float *out) {
+    const int im = blockIdx.x * blockDim.x + threadIdx.x;
+    if (im < nmol) out[im] = en_mole_intra_d(I, im, xa, ya, za);
+}
+
+// ---------------------------------------------------------------- the cycle
+
+struct ShakeDev {
+    IntraDev I;
+    int nmol, nmoltype, M, ireset;
+    float stepmi, simt, rejrate, trstepmax, trstepmin;
+    float *xa, *ya, *za;
+    const int32_t *nergpairm, *molergpair, *ergpairref;
+    float *ergpair;
+    float *wholerot, *wholetrans, *internrot, *interntrans, *fadds, *faddbs;
+    int32_t *nwhole, *nmovem, *nmovei;
+    // scratch
+    long long *off;      // [nmol] first ran1 value of each molecule, -1: not moved
+    long long *total;    // [1]
+    int32_t *status;     // [1] 1: a molecule with rotational groups
+    const float *vals;   // [total] the cycle's ran1 values
+    float *xt, *yt, *zt; // [natom] trial coordinates
+    float *enew;         // [nmol]
+    int32_t *acc;        // [nmol]
+};
+
+// The draws of every molecule (3 per atom + 1 when it is moved), their offsets in the stream,
+// and the per-type settings the reference makes while it walks the molecules: interntrans(mt)
+// set to trstepmin where it was 0 for types with a moved molecule (:135-138), internrot(mt) = 0
+// for types with a molecule without rotational groups (:246-247).
+__global__ void __launch_bounds__(SH_THREADS) shake_plan_kernel(ShakeDev D) {
+    __shared__ long long wsum[SH_THREADS / 32];
+    __shared__ long long carry;
+    __shared__ int moved_t[64], plain_t[64], bad;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid == 0) {
+        carry = 0;
+        bad = 0;
+    }
+    for (int t = tid; t < 64; t += blockDim.x) moved_t[t] = plain_t[t] = 0;
+    __syncthreads();
+    for (int base = 0; base < D.nmol; base += SH_THREADS) {
+        const int m = base + tid;
+        long long d = 0;
+        if (m < D.nmol) {
+            const int n = D.I.nato[m];
+            if (D.I.ngrot[m] > 0) atomicOr(&bad, 1);
+            const int mt = D.I.mtype[m];
+            if (n > 1 && D.stepmi > 0.0f) {
+                d = 3LL * n + 1;
+                if (mt < 64) moved_t[mt] = 1;
+            }
+            if (mt < 64) plain_t[mt] = 1;
+        }
+        long long v = d;   // inclusive warp scan
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        if (lane == 31) wsum[w] = v;
+        __syncthreads();
+        if (w == 0) {
+            long long s = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long u = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += u;
+            }
+            wsum[lane] = s;
+        }
+        __syncthreads();
+        const long long excl = carry + (w > 0 ? wsum[w - 1] : 0) + v - d;
+        if (m < D.nmol) D.off[m] = d > 0 ? excl : -1;
+        __syncthreads();
+        if (tid == 0) carry += wsum[31];
+        __syncthreads();
+    }
+    if (tid == 0) {
+        D.total[0] = carry;
+        D.status[0] = bad;
+    }
+    if (bad) return;
+    for (int t = tid; t < D.nmoltype && t < 64; t += blockDim.x) {
+        if (moved_t[t] && D.interntrans[t] == 0.0f) D.interntrans[t] = D.trstepmin;
+        if (plain_t[t]) D.internrot[t] = 0.0f;
+    }
+}
+
+// movei/movea (:545-567): atom by atom, z then y then x, x += step * (2 r - 1); then the new
+// intramolecular energy of the trial coordinates.
+__global__ void shake_trial_kernel(ShakeDev D) {
+    const int im = blockIdx.x * blockDim.x + threadIdx.x;
+    if (im >= D.nmol) return;
+    const long long o = D.off[im];
+    if (o < 0) return;
+    const int a0 = D.I.naf[im], n = D.I.nato[im];
+    const float step = D.interntrans[D.I.mtype[im]];
+    const float *r = D.vals + o;
+    for (int k = 0; k < n; ++k) {
+        const int a = a0 + k;
+        D.zt[a] = __fadd_rn(D.za[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, r[3 * k]), 1.0f)));
+        D.yt[a] = __fadd_rn(D.ya[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, r[3 * k + 1]), 1.0f)));
+        D.xt[a] = __fadd_rn(D.xa[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, r[3 * k + 2]), 1.0f)));
+    }
+    D.enew[im] = en_mole_intra_d(D.I, im, D.xt, D.yt, D.zt);
+}
+
+// The ordered pass (:119-170 per molecule) and the step adaptation (:465-536).
+__global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
+    __shared__ float s_enew[SH_TILE], s_r[SH_TILE], s_v1[SH_TILE];
+    __shared__ int s_nn[SH_TILE], s_prev[SH_TILE], s_mt[SH_TILE];
+    __shared__ int s_slot[SH_TILE];
+    __shared__ unsigned char s_mv[SH_TILE];
+    __shared__ int cnt[2 * 64];
+    __shared__ float s_faddb, s_ergold1;
+    const int tid = threadIdx.x;
+    const float temp = __fdiv_rn(1.0f, D.simt);
+    for (int t = tid; t < 2 * 64; t += blockDim.x) cnt[t] = 0;
+    if (tid == 0) {
+        s_faddb = 0.0f;
+        s_ergold1 = 0.0f;   // a molecule with an empty list before any loaded one compares against 0
+    }
+    __syncthreads();
+    for (int base = 0; base < D.nmol; base += SH_TILE) {
+        const int nt = min(SH_TILE, D.nmol - base);
+        for (int k = tid; k < nt; k += blockDim.x) {
+            const int m = base + k;
+            const long long o = D.off[m];
+            const int nn = D.nergpairm[m];
+            s_nn[k] = nn;
+            s_mt[k] = D.I.mtype[m];
+            s_mv[k] = o >= 0;
+            if (o >= 0) {
+                s_enew[k] = D.enew[m];
+                s_r[k] = D.vals[o + 3LL * D.I.nato[m]];
+            }
+            int prev = -1, slot = 0;
+            float v1 = 0.0f;
+            if (nn >= 1) {
+                const size_t row = (size_t)m * D.M;
+                slot = D.ergpairref[row];
+                v1 = D.ergpair[slot - 1];
+                // an earlier molecule whose first slot is the same stored energy (a shared pair
+                // that is the first entry of both lists) rewrites it when its move is accepted
+                const int p = D.molergpair[row];
+                if (p >= 0 && p < m && D.nergpairm[p] >= 1 && D.ergpairref[(size_t)p * D.M] == slot) prev = p;
+            }
+            s_slot[k] = slot;
+            s_v1[k] = v1;
+            s_prev[k] = prev;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float faddb = s_faddb, ergold1 = s_ergold1;
+            for (int k = 0; k < nt; ++k) {
+                const int m = base + k;
+                if (s_nn[k] >= 1) {
+                    const int p = s_prev[k];
+                    ergold1 = (p >= 0 && D.acc[p]) ? D.enew[p] : s_v1[k];   // make_neighbour_list_from_mols
+                }
+                int a = 0;
+                if (s_mv[k]) {
+                    const int mt = s_mt[k];
+                    const float fdiffb = __fsub_rn(s_enew[k], ergold1);
+                    const float ediff = __fmul_rn(fdiffb, temp);
+                    float etest;
+                    if (ediff <= 0.0f) etest = 10.0f;
+                    else if (ediff < 20.0f) etest = exp_r(-ediff);
+                    else etest = 0.0f;
+                    a = s_r[k] < etest;
+                    if (mt < 64) {
+                        ++cnt[mt];
+                        if (!a) ++cnt[64 + mt];
+                    }
+                    if (a) {
+                        faddb = __fadd_rn(faddb, fdiffb);
+                        if (s_nn[k] >= 1) {          // save_energies + save_erg_pairs
+                            ergold1 = s_enew[k];
+                            D.ergpair[s_slot[k] - 1] = ergold1;
+                        }
+                    }
+                }
+                D.acc[m] = a;
+            }
+            s_faddb = faddb;
+            s_ergold1 = ergold1;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const int nmt = D.nmoltype;
+        const float rotstepmin = 1.0e-5f, rotstepmax = 1.0f;
+        for (int t = 0; t < nmt; ++t) {
+            const int tries = t < 64 ? cnt[t] : 0, rej = t < 64 ? cnt[64 + t] : 0;
+            D.nmovei[t] = tries;
+            D.nmovei[nmt + t] = rej;
+            D.nwhole[t] = D.nwhole[nmt + t] = 0;
+            D.nmovem[t] = D.nmovem[nmt + t] = 0;
+            if (D.ireset != 1) {
+                float rat;
+                if (rej > 0) {
+                    rat = __fdiv_rn(__fmul_rn(D.rejrate, (float)tries), (float)rej);
+                    if (rat > 1.1f) rat = 1.1f;
+                    if (rat < 0.9f) rat = 0.9f;
+                } else {
+                    rat = tries > 0 ? 1.1f : 1.0f;
+                }
+                float it = __fmul_rn(D.interntrans[t], rat);
+                if (it > D.trstepmax) it = D.trstepmax;
+                if (it < D.trstepmin && it != 0.0f) it = D.trstepmin;
+                D.interntrans[t] = it;
+                float ir = __fmul_rn(D.internrot[t], 1.0f);      // no internal rotations: ninter 0
+                if (ir > rotstepmax) ir = rotstepmax;
+                if (ir < rotstepmin && ir != 0.0f) ir = rotstepmin;
+                D.internrot[t] = ir;
+                float wr = __fmul_rn(D.wholerot[t], 1.0f);       // no whole-molecule moves this cycle
+                if (wr > rotstepmax) wr = rotstepmax;
+                if (wr < rotstepmin && wr != 0.0f) wr = rotstepmin;
+                D.wholerot[t] = wr;
+                float wt = __fmul_rn(D.wholetrans[t], 1.0f);
+                if (wt > D.trstepmax) wt = D.trstepmax;
+                if (wt < D.trstepmin && wt != 0.0f) wt = D.trstepmin;
+                D.wholetrans[t] = wt;
+            }
+        }
+        D.fadds[0] = __fadd_rn(D.fadds[0], __fdiv_rn(0.0f, (float)D.nmol));
+        D.faddbs[0] = __fadd_rn(D.faddbs[0], __fdiv_rn(s_faddb, (float)D.nmol));
+    }
+}
+
+// Accepted moves: the trial coordinates, then centreofmassi (mass-weighted centre of the
+// non-q atoms, summed in atom order, subtracted from every atom).
+__global__ void shake_apply_kernel(ShakeDev D) {
+    const int im = blockIdx.x * blockDim.x + threadIdx.x;
+    if (im >= D.nmol || D.off[im] < 0 || !D.acc[im]) return;
+    const int a0 = D.I.naf[im], n = D.I.nato[im];
+    float x1 = 0.0f, y1 = 0.0f, z1 = 0.0f, summass = 0.0f;
+    for (int k = 0; k < n; ++k) {
+        const int a = a0 + k;
+        if (D.I.qtype[a] == 0) {
+            const float am = D.I.amassa[D.I.itype[a]];
+            x1 = __fadd_rn(x1, __fmul_rn(D.xt[a], am));
+            y1 = __fadd_rn(y1, __fmul_rn(D.yt[a], am));
+            z1 = __fadd_rn(z1, __fmul_rn(D.zt[a], am));
+            summass = __fadd_rn(summass, am);
+        }
+    }
+    if (summass > 0.0f) {
+        x1 = __fdiv_rn(x1, summass);
+        y1 = __fdiv_rn(y1, summass);
+        z1 = __fdiv_rn(z1, summass);
+    }
+    for (int k = 0; k < n; ++k) {
+        const int a = a0 + k;
+        D.xa[a] = __fsub_rn(D.xt[a], x1);
+        D.ya[a] = __fsub_rn(D.yt[a], y1);
+        D.za[a] = __fsub_rn(D.zt[a], z1);
+    }
+}
+
+size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+}  // namespace epsr
+
+using namespace epsr;
+
+static int intra_check(const epsr_box_t *box, const epsr_intra_t *in, const char *who) {
+    if (!box || !in || !in->nbond || !in->iabond || !in->tbond || in->maxbond < 1 || !in->imageatom || !in->qtype ||
+        !in->amassa || !in->amassr || !in->xav || !in->xav1 || !in->ngrot || !(in->stepcl > 0.0f)) {
+        epsr_set_error("%s: bad arguments", who);
+        return EPSR_ERR_ARG;
+    }
+    return EPSR_OK;
+}
+
+extern "C" int epsr_en_mole_intra(const epsr_box_t *box, const epsr_intra_t *in, float *out, void *stream) {
+    int rc = intra_check(box, in, "epsr_en_mole_intra");
+    if (rc) return rc;
+    if (!out || box->nmol < 1) {
+        epsr_set_error("epsr_en_mole_intra: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    const IntraDev I = make_intradev(box, in);
+    en_mole_intra_kernel<<<(box->nmol + 127) / 128, 128, 0, (cudaStream_t)stream>>>(I, box->nmol, box->xa, box->ya,
+                                                                                  box->za, out);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
+
+extern "C" int64_t epsr_molfit_shake_scratch_bytes(int32_t nmol, int32_t natom) {
+    if (nmol < 1 || natom < 1) return -1;
+    return (int64_t)(al256(8 * (size_t)nmol) + 256 + 256 + al256(4 * (3 * (size_t)natom + nmol)) +
+                     3 * al256(4 * (size_t)natom) + al256(4 * (size_t)nmol) + al256(4 * (size_t)nmol));
+}
+
+extern "C" int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, epsr_mc_t *mc, const epsr_intra_t *in,
+                                 float stepmi, int32_t *nmovei, float *faddbs, void *scratch, int64_t scratch_bytes,
+                                 void *stream) {
+    int rc = intra_check(box, in, "epsr_molfit_shake");
+    if (rc) return rc;
+    if (!store || !mc || !nmovei || !faddbs || !scratch || !mc->ran1 || !mc->fadds || !mc->internrot ||
+        !mc->interntrans || !mc->wholerot || !mc->wholetrans || !mc->nwhole || !mc->nmovem || box->nmoltype > 64) {
+        epsr_set_error("epsr_molfit_shake: bad arguments (at most 64 molecule types)");
+        return EPSR_ERR_ARG;
+    }
+    const int64_t need = epsr_molfit_shake_scratch_bytes(box->nmol, box->natom);
+    if (scratch_bytes < need) {
+        epsr_set_error("epsr_molfit_shake: scratch %lld < %lld bytes", (long long)scratch_bytes, (long long)need);
+        return EPSR_ERR_CAPACITY;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    ShakeDev D;
+    memset(&D, 0, sizeof(D));
+    D.I = make_intradev(box, in);
+    D.nmol = box->nmol;
+    D.nmoltype = box->nmoltype;
+    D.M = store->nnbrefmax;
+    D.ireset = mc->ireset;
+    D.stepmi = stepmi;
+    D.simt = mc->simt;
+    D.rejrate = mc->rejrate;
+    D.trstepmax = mc->trstepmax;
+    D.trstepmin = mc->trstepmin;
+    D.xa = box->xa;
+    D.ya = box->ya;
+    D.za = box->za;
+    D.nergpairm = store->nergpairm;
+    D.molergpair = store->molergpair;
+    D.ergpairref = store->ergpairref;
+    D.ergpair = store->ergpair;
+    D.wholerot = mc->wholerot;
+    D.wholetrans = mc->wholetrans;
+    D.internrot = mc->internrot;
+    D.interntrans = mc->interntrans;
+    D.fadds = mc->fadds;
+    D.faddbs = faddbs;
+    D.nwhole = mc->nwhole;
+    D.nmovem = mc->nmovem;
+    D.nmovei = nmovei;
+    unsigned char *p = (unsigned char *)scratch;
+    D.off = (long long *)p;
+    p += al256(8 * (size_t)D.nmol);
+    D.total = (long long *)p;
+    p += 256;
+    D.status = (int32_t *)p;
+    p += 256;
+    float *vals = (float *)p;
+    D.vals = vals;
+    p += al256(4 * (3 * (size_t)box->natom + D.nmol));
+    D.xt = (float *)p;
+    p += al256(4 * (size_t)box->natom);
+    D.yt = (float *)p;
+    p += al256(4 * (size_t)box->natom);
+    D.zt = (float *)p;
+    p += al256(4 * (size_t)box->natom);
+    D.enew = (float *)p;
+    p += al256(4 * (size_t)D.nmol);
+    D.acc = (int32_t *)p;
+
+    shake_plan_kernel<<<1, SH_THREADS, 0, s>>>(D);
+    EPSR_CUDA(cudaGetLastError());
+    long long total = 0;
+    int32_t status = 0;
+    EPSR_D2H(&total, D.total, sizeof(total), s);
+    EPSR_D2H(&status, D.status, sizeof(status), s);
+    if (status) {
+        epsr_set_error("epsr_molfit_shake: molecules with rotational groups (internal rotations and dihedral terms "
+                       "are outside this path)");
+        return EPSR_ERR_UNSUPPORTED;
+    }
+    if (total > 3LL * box->natom + D.nmol) {
+        epsr_set_error("epsr_molfit_shake: %lld draws exceed the stream buffer", total);
+        return EPSR_ERR_CAPACITY;
+    }
+    if (total > 0) {
+        rc = epsr_ran1_fill(mc->ran1, vals, total, stream);
+        if (rc) return rc;
+    }
+    const int nb = (D.nmol + 127) / 128;
+    shake_trial_kernel<<<nb, 128, 0, s>>>(D);
+    EPSR_CUDA(cudaGetLastError());
+    shake_resolve_kernel<<<1, SH_THREADS, 0, s>>>(D);
+    EPSR_CUDA(cudaGetLastError());
+    shake_apply_kernel<<<nb, 128, 0, s>>>(D);
+    EPSR_CUDA(cudaGetLastError());
+    return epsr_box_positions(box, stream);
+}

@@ -173,6 +173,49 @@ int epsr_en_change(const epsr_box_t *box, const epsr_store_t *store, int32_t im,
 int epsr_en_mole_pair(const epsr_box_t *box, const int32_t *im, const int32_t *jm, int32_t n, float *out,
                       void *stream);
 
+/* ------------------------------------------------------------------ intramolecular moves */
+
+/* The intramolecular model of en_atom_intra molfit.py:923-1045 (molecom arrays; all pointers
+ * device, atoms 0-based).  Molecules with rotational groups (ngrot > 0: dihedral terms and the
+ * internal rotations of rotati :589) are outside this path. */
+typedef struct {
+    const int32_t *nbond;      /* [natom] bonds listed for each atom */
+    const int32_t *iabond;     /* [natom*maxbond] 0-based partner atom of each bond */
+    const float *tbond;        /* [natom*maxbond] bond length (box units); < 0: a bond-angle pair */
+    int32_t maxbond;
+    const int32_t *imageatom;  /* [natom] 0-based image atom, -1 for none */
+    const int32_t *qtype;      /* [natom] */
+    const float *amassa;       /* [ntype] atom masses (centreofmassi) */
+    const float *amassr;       /* [npairs] bond weights */
+    const float *xav, *xav1;   /* [npairs][box->ld] reference potential of non-bonded intra pairs */
+    const int32_t *ngrot;      /* [nmol] rotational groups of each molecule */
+    float stepcl;              /* cellst / dmaxmol */
+    float sizefactor, tempb, tempang, simt;
+    int32_t refine_intra;      /* 1: add refine_intra_fac x EP (box->tab) to non-q pairs */
+    float refine_intra_fac;
+} epsr_intra_t;
+
+/* en_mole_intra molfit.py:1327-1350 of every molecule at its current coordinates: out [nmol]
+ * device (the intramolecular energies fmolec1 stores first).  Bit-identical.  Asynchronous. */
+int epsr_en_mole_intra(const epsr_box_t *box, const epsr_intra_t *intra, float *out, void *stream);
+
+/* The intramolecular cycle of molfit (molfit.py:124-174, taken when nisum >= intra, then the
+ * step adaptation :465-536): for every molecule of more than one atom (stepmi > 0) in order,
+ * movei :545 (3 ran1 values per atom, z y x), en_change_intra :763 against the first stored
+ * energy, the Metropolis test (one ran1 value) and, on acceptance, the store's first entry
+ * and centreofmassi ato_manipulation_rev4.py:442.  mc: simt, rejrate, trstepmax/min, ireset,
+ * the step arrays (interntrans adapted from this cycle's counts; internrot set to 0 for
+ * molecule types without rotational groups), nwhole/nmovem zeroed, fadds, ran1.  nmovei
+ * [2*nmoltype] device out (tries, then rejections); faddbs [1] device in/out.  A molecule
+ * with an empty pair list before any loaded one compares against 0 (the reference uses
+ * whatever its work array last held).  Returns EPSR_ERR_UNSUPPORTED, before any change, for
+ * molecules with rotational groups.  Bit-identical with the reference's exp values.
+ * Synchronous (reads the draw count); scratch from epsr_molfit_shake_scratch_bytes. */
+int64_t epsr_molfit_shake_scratch_bytes(int32_t nmol, int32_t natom);
+int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, epsr_mc_t *mc, const epsr_intra_t *intra,
+                      float stepmi, int32_t *nmovei, float *faddbs, void *scratch, int64_t scratch_bytes,
+                      void *stream);
+
 /* ------------------------------------------------------------------ atogen */
 /* atogen ato_manipulation_rev4.py:3640-3899 (no coarse graining, no container forces).
  * wav: device [2*npairs*ldw] (wav(1,iz,ic) at [ic*ldw+iz], wav(2,..) at [(npairs+ic)*ldw+iz]),

@@ -972,6 +972,192 @@ void oracle_sumsq(int nq, int npairs, const float *qwind, int ldq, double fc1, d
     }
 }
 
+/* ------------------------------------------------------------------ intramolecular moves */
+typedef struct {
+    const int32_t *nbond, *iabond; /* [natom], [natom*maxbond] 0-based partners */
+    const float *tbond;            /* [natom*maxbond] */
+    int32_t maxbond;
+    const int32_t *imageatom;      /* [natom] 0-based, -1 none */
+    const int32_t *qtype;          /* [natom] */
+    const float *amassa, *amassr;  /* [ntype], [npairs] */
+    const float *xav, *xav1;       /* [npairs*ld] */
+    const int32_t *ngrot;          /* [nmol] */
+    float stepcl, sizefactor, tempb, tempang, simt;
+    int32_t refine_intra;
+    float refine_intra_fac;
+} oracle_intra;
+
+/* en_atom_intra molfit.py:923-1045 (molecules without rotational groups: no dihedral pairs) */
+static float en_atom_intra(const oracle_sys *S, const oracle_intra *I, int ia, int ja, float x1, float y1, float z1,
+                           float x2, float y2, float z2) {
+    if (ja == I->imageatom[ia]) return 0.0f;
+    const int icref = S->npairref[S->itype[ia] * S->ntype + S->itype[ja]];
+    const int notq = I->qtype[ia] == 0 && I->qtype[ja] == 0;
+    float sume = 0.0f;
+    const float xdifs = x2 - x1, ydifs = y2 - y1, zdifs = z2 - z1;
+    int image = ia, iflag = -1;
+    for (int k = 0; k < I->nbond[image] && iflag < 0; ++k)
+        if (I->iabond[(size_t)image * I->maxbond + k] == ja) iflag = k;
+    if (iflag < 0) {
+        image = I->imageatom[ia];
+        if (image >= 0)
+            for (int k = 0; k < I->nbond[image] && iflag < 0; ++k)
+                if (I->iabond[(size_t)image * I->maxbond + k] == ja) iflag = k;
+    }
+    if (iflag >= 0) {
+        float xdif = xdifs, ydif = ydifs, zdif = zdifs;
+        minimagec(S, &xdif, &ydif, &zdif);
+        const float dtest = sqrtf(xdif * xdif + ydif * ydif + zdif * zdif);
+        const int iz = f_ifix(dtest / I->stepcl) + 2;
+        const float t = I->tbond[(size_t)image * I->maxbond + iflag];
+        const float tb = fabsf(t) > I->stepcl ? fabsf(t) : I->stepcl;
+        float wtm = I->amassr[icref] / tb;
+        if (t < 0.0f) wtm = wtm * I->tempang;
+        const float ddif = tb - dtest;
+        sume = wtm * ddif * ddif * I->tempb * I->simt;
+        if (I->refine_intra && iz <= S->npt2 && notq) {
+            const float dtdif = dtest - S->xstar[iz];
+            const size_t k = (size_t)icref * S->ld + iz;
+            sume = sume + I->refine_intra_fac * (S->xavs[k] + S->xavs1[k] * dtdif);
+        }
+    } else {
+        float xdif = xdifs * I->sizefactor, ydif = ydifs * I->sizefactor, zdif = zdifs * I->sizefactor;
+        minimagec(S, &xdif, &ydif, &zdif);
+        const float dtest = sqrtf(xdif * xdif + ydif * ydif + zdif * zdif);
+        const int iz = f_ifix(dtest / I->stepcl) + 2;
+        if (iz <= S->npt2) {
+            const float dtdif = dtest - S->xstar[iz];
+            const size_t k = (size_t)icref * S->ld + iz;
+            sume = I->xav[k] + I->xav1[k] * dtdif;
+            if (I->refine_intra && notq) sume = sume + I->refine_intra_fac * (S->xavs[k] + S->xavs1[k] * dtdif);
+        }
+    }
+    return sume;
+}
+
+/* en_mole_intra molfit.py:1327-1350 */
+float oracle_en_mole_intra(const oracle_sys *S, const oracle_intra *I, int im) {
+    const int a0 = S->naf[im], n = S->nato[im];
+    float e = 0.0f;
+    for (int ia = a0; ia < a0 + n - 1; ++ia)
+        for (int ja = ia + 1; ja < a0 + n; ++ja)
+            e = e + en_atom_intra(S, I, ia, ja, S->xa[ia], S->ya[ia], S->za[ia], S->xa[ja], S->ya[ja], S->za[ja]);
+    return e;
+}
+
+void oracle_en_mole_intra_all(const oracle_sys *S, const oracle_intra *I, float *out) {
+    for (int im = 0; im < S->nmol; ++im) out[im] = oracle_en_mole_intra(S, I, im);
+}
+
+/* The intramolecular branch of molfit (molfit.py:119-174 with :246-247; no rotational groups),
+ * then the step adaptation :465-536, in the reference's order.  *ergold1 is the reference's
+ * work value ergold(1) (in/out).  Returns 1 for a molecule with rotational groups. */
+int oracle_molfit_shake(oracle_sys *S, oracle_store *E, oracle_mcpar *P, const oracle_intra *I, float stepmi,
+                        oracle_ran1_state *R, float *fadds, float *faddbs, int32_t *nmovei, float *ergold1) {
+    const int nmt = S->nmoltype, M = E->nnbrefmax;
+    for (int im = 0; im < S->nmol; ++im)
+        if (I->ngrot[im] > 0) return 1;
+    for (int t = 0; t < 2 * nmt; ++t) {
+        nmovei[t] = 0;
+        P->nwhole[t] = 0;
+        P->nmovem[t] = 0;
+    }
+    const float temp = 1.0f / P->simt;
+    float faddb = 0.0f, eo1 = *ergold1;
+    float xr[4096], yr[4096], zr[4096];
+    for (int im = 0; im < S->nmol; ++im) {
+        const int nn = E->nergpairm[im];
+        if (nn >= 1) eo1 = E->ergpair[E->ergpairref[(size_t)im * M] - 1];   /* make_neighbour_list_from_mols */
+        const int n = S->nato[im], a0 = S->naf[im], mt = S->mtype[im];
+        if (n > 1 && stepmi > 0.0f && n <= 4096) {
+            float step = P->interntrans[mt];
+            if (stepmi > 0.0f && step == 0.0f) step = P->trstepmin;
+            P->interntrans[mt] = step;
+            for (int k = 0; k < n; ++k) {
+                xr[k] = S->xa[a0 + k];
+                yr[k] = S->ya[a0 + k];
+                zr[k] = S->za[a0 + k];
+            }
+            nmovei[mt] += 1;
+            for (int k = 0; k < n; ++k) {                                    /* movei / movea */
+                const int a = a0 + k;
+                S->za[a] = S->za[a] + step * (2.0f * oracle_ran1(R) - 1.0f);
+                S->ya[a] = S->ya[a] + step * (2.0f * oracle_ran1(R) - 1.0f);
+                S->xa[a] = S->xa[a] + step * (2.0f * oracle_ran1(R) - 1.0f);
+            }
+            const float enew = oracle_en_mole_intra(S, I, im);
+            const float fdiffb = enew - eo1;
+            const float ediff = fdiffb * temp;
+            const float etest = ediff <= 0.0f ? 10.0f : (ediff < 20.0f ? expf(-ediff) : 0.0f);
+            if (oracle_ran1(R) < etest) {
+                faddb = faddb + fdiffb;
+                if (nn >= 1) {                                                 /* save_energies */
+                    eo1 = enew;
+                    E->ergpair[E->ergpairref[(size_t)im * M] - 1] = eo1;     /* save_erg_pairs */
+                }
+                float x1 = 0.0f, y1 = 0.0f, z1 = 0.0f, summass = 0.0f;        /* centreofmassi */
+                for (int k = 0; k < n; ++k) {
+                    const int a = a0 + k;
+                    if (I->qtype[a] == 0) {
+                        const float am = I->amassa[S->itype[a]];
+                        x1 = x1 + S->xa[a] * am;
+                        y1 = y1 + S->ya[a] * am;
+                        z1 = z1 + S->za[a] * am;
+                        summass = summass + am;
+                    }
+                }
+                if (summass > 0.0f) {
+                    x1 = x1 / summass;
+                    y1 = y1 / summass;
+                    z1 = z1 / summass;
+                }
+                for (int k = 0; k < n; ++k) {
+                    S->xa[a0 + k] = S->xa[a0 + k] - x1;
+                    S->ya[a0 + k] = S->ya[a0 + k] - y1;
+                    S->za[a0 + k] = S->za[a0 + k] - z1;
+                }
+            } else {
+                nmovei[nmt + mt] += 1;
+                for (int k = 0; k < n; ++k) {
+                    S->xa[a0 + k] = xr[k];
+                    S->ya[a0 + k] = yr[k];
+                    S->za[a0 + k] = zr[k];
+                }
+            }
+        }
+        P->internrot[mt] = 0.0f;   /* no rotational groups (:246-247) */
+    }
+    if (P->ireset != 1) {
+        const float rotstepmin = 1.0e-5f, rotstepmax = 1.0f;
+        for (int t = 0; t < nmt; ++t) {
+            float rat;
+            if (nmovei[nmt + t] > 0) {
+                rat = P->rejrate * (float)nmovei[t] / (float)nmovei[nmt + t];
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = nmovei[t] > 0 ? 1.1f : 1.0f;
+            }
+            P->interntrans[t] = P->interntrans[t] * rat;
+            if (P->interntrans[t] > P->trstepmax) P->interntrans[t] = P->trstepmax;
+            if (P->interntrans[t] < P->trstepmin && P->interntrans[t] != 0.0f) P->interntrans[t] = P->trstepmin;
+            P->internrot[t] = P->internrot[t] * 1.0f;
+            if (P->internrot[t] > rotstepmax) P->internrot[t] = rotstepmax;
+            if (P->internrot[t] < rotstepmin && P->internrot[t] != 0.0f) P->internrot[t] = rotstepmin;
+            P->wholerot[t] = P->wholerot[t] * 1.0f;
+            if (P->wholerot[t] > rotstepmax) P->wholerot[t] = rotstepmax;
+            if (P->wholerot[t] < rotstepmin && P->wholerot[t] != 0.0f) P->wholerot[t] = rotstepmin;
+            P->wholetrans[t] = P->wholetrans[t] * 1.0f;
+            if (P->wholetrans[t] > P->trstepmax) P->wholetrans[t] = P->trstepmax;
+            if (P->wholetrans[t] < P->trstepmin && P->wholetrans[t] != 0.0f) P->wholetrans[t] = P->trstepmin;
+        }
+    }
+    *fadds = *fadds + 0.0f / (float)S->nmol;
+    *faddbs = *faddbs + faddb / (float)S->nmol;
+    *ergold1 = eo1;
+    return 0;
+}
+
 /* ------------------------------------------------------------------ generate_ep */
 /* generate_ep epsr_standalone_rev3.py:5876-5995 with the Poisson basis already built
  * (calc_pwrexpr_grad, host): expgr [npt2][nterms] (row j-1 of the reference's flat expgr).

@@ -282,6 +282,75 @@ def molfit(box, cells, st, mc, ran1, fadds=0.0, record_cos=True):
     return f32(fa.value), tr, r.to_state()
 
 
+# ----------------------------------------------------------------------------- intramolecular
+class IntraC(C.Structure):
+    _fields_ = [("nbond", P), ("iabond", P), ("tbond", P), ("maxbond", C.c_int32), ("imageatom", P), ("qtype", P),
+                ("amassa", P), ("amassr", P), ("xav", P), ("xav1", P), ("ngrot", P), ("stepcl", C.c_float),
+                ("sizefactor", C.c_float), ("tempb", C.c_float), ("tempang", C.c_float), ("simt", C.c_float),
+                ("refine_intra", C.c_int32), ("refine_intra_fac", C.c_float)]
+
+
+class IntraHandle:
+    """Keeps the NumPy arrays of an intramolecular model alive for its IntraC view.  ``m``: dict
+    with nbond (natom,), iabond/tbond (natom, maxbond) 0-based, amassa, amassr, xav/xav1
+    (npairs, ld), stepcl, sizefactor, tempb, tempang, simt, refine_intra, refine_intra_fac and
+    optional imageatom/qtype/ngrot."""
+
+    def __init__(self, box, m):
+        self.a = dict(nbond=np.ascontiguousarray(m["nbond"], np.int32),
+                      iabond=np.ascontiguousarray(m["iabond"], np.int32),
+                      tbond=np.ascontiguousarray(m["tbond"], f32),
+                      imageatom=np.ascontiguousarray(m.get("imageatom", np.full(box.natom, -1)), np.int32),
+                      qtype=np.ascontiguousarray(m.get("qtype", np.zeros(box.natom)), np.int32),
+                      amassa=np.ascontiguousarray(m["amassa"], f32), amassr=np.ascontiguousarray(m["amassr"], f32),
+                      xav=np.ascontiguousarray(m["xav"], f32), xav1=np.ascontiguousarray(m["xav1"], f32),
+                      ngrot=np.ascontiguousarray(m.get("ngrot", np.zeros(box.nmol)), np.int32))
+        c = IntraC()
+        for k, v in self.a.items():
+            setattr(c, k, ptr(v))
+        c.maxbond = self.a["iabond"].shape[1]
+        for k in ("stepcl", "sizefactor", "tempb", "tempang", "simt", "refine_intra_fac"):
+            setattr(c, k, f32(m[k]))
+        c.refine_intra = int(bool(m["refine_intra"]))
+        self.c = c
+
+
+def en_mole_intra_all(box, m):
+    """en_mole_intra molfit.py:1327-1350 of every molecule (C restatement)."""
+    h, ih = SysHandle(box), IntraHandle(box, m)
+    out = np.zeros(box.nmol, f32)
+    lib().oracle_en_mole_intra_all(C.byref(h.c), C.byref(ih.c), ptr(out))
+    return out
+
+
+def molfit_shake(box, st, mc, m, stepmi, ran1, fadds, faddbs, ergold1=0.0):
+    """The intramolecular cycle of molfit (molfit.py:119-174, :246-247, then :465-536), C
+    restatement.  Mutates the box coordinates, st["ergpair"] and the step arrays in ``mc``.
+    Returns (fadds, faddbs, nmovei (2*nmt,), ergold1, ran1 state)."""
+    h, ih = SysHandle(box), IntraHandle(box, m)
+    E = store_c(st)
+    nmt = box.nmoltype
+    par = McParC()
+    par.simt, par.rejrate = box.simt, f32(mc["rejrate"])
+    tmax, tmin = trsteps(box.natomr)
+    par.trstepmax, par.trstepmin = tmax, tmin
+    par.ireset = int(mc.get("ireset", 0))
+    for k in ("wholerot", "wholetrans", "internrot", "interntrans"):
+        mc[k] = np.ascontiguousarray(mc[k], dtype=f32)
+        setattr(par, k, ptr(mc[k]))
+    mc["nwhole"] = np.zeros(2 * nmt, np.int32)
+    mc["nmovem"] = np.zeros(2 * nmt, np.int32)
+    par.nwhole, par.nmovem = ptr(mc["nwhole"]), ptr(mc["nmovem"])
+    nmovei = np.zeros(2 * nmt, np.int32)
+    r = Ran1C.of(ran1)
+    fa, fb, eo = C.c_float(f32(fadds)), C.c_float(f32(faddbs)), C.c_float(f32(ergold1))
+    rc = lib().oracle_molfit_shake(C.byref(h.c), C.byref(E), C.byref(par), C.byref(ih.c), C.c_float(f32(stepmi)),
+                                   C.byref(r), C.byref(fa), C.byref(fb), ptr(nmovei), C.byref(eo))
+    if rc:
+        raise ValueError("molfit_shake: molecules with rotational groups")
+    return f32(fa.value), f32(fb.value), nmovei, f32(eo.value), r.to_state()
+
+
 # ----------------------------------------------------------------------------- atogen
 def atogen(box, ngrsamples, ran1, rminex, ycoh=None, sizefactor=1.0):
     ld = box.npt + 1
