@@ -349,21 +349,51 @@ class PairPath:
         mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
         b = self._sync_in()
         self._check_cells()
-        # intramolecular energies from the reference's own host routine (molfit.py:1327)
-        en_mole_intra = self.mods["molfit"].en_mole_intra
-        sv = sa = sd = f32(0.0)
-        eintra = np.zeros(b.nmol, f32)
-        for im in range(1, b.nmol + 1):
-            e, sv, sa, sd = en_mole_intra(im, sv, sa, sd)
-            eintra[im - 1] = e
+        model = self._intra_model(b)
+        if model is not None:
+            # intramolecular energies (molfit.py:1327) on the device
+            eintra = model.en_mole_intra()
+        else:
+            # rotational groups (dihedral terms): the reference's own host routine
+            en_mole_intra = self.mods["molfit"].en_mole_intra
+            sv = sa = sd = f32(0.0)
+            eintra = np.zeros(b.nmol, f32)
+            for im in range(1, b.nmol + 1):
+                e, sv, sa, sd = en_mole_intra(im, sv, sa, sd)
+                eintra[im - 1] = e
         ft, fb = self.d.fmolec1(eintra, strict=True)
         self._store_out(values_only=False)
         self._mirror_ok = True
         nmol = f32(b.nmol)
         return 0, num_threads_input, f32(ft), f32(fb), f32(0.0) / nmol, f32(0.0) / nmol
 
+    def _intra_model(self, b):
+        """The device intramolecular model (en_atom_intra molfit.py:923) from molecom, or None
+        when a molecule has rotational groups (their dihedral terms and internal rotations stay
+        on the host) or the COMMON blocks carry no bond lists."""
+        from .intra import IntraModel
+        c = self.c
+        mc, cc, pp, e16 = c.molecom, c.clustercom, c.potential_par, c.epsr16
+        nmol, natom, npairs = b.nmol, b.natom, b.npairs
+        if getattr(mc, "nbond", None) is None or getattr(pp, "xav", None) is None or \
+                bool(np.any(np.asarray(cc.ngrot[1:nmol + 1]) > 0)):
+            return None
+        nb = np.asarray(mc.nbond[1:natom + 1], np.int32)
+        mb = max(1, int(nb.max()) if natom else 1)
+        ld = b.npt + 1
+        return IntraModel(self.d, nbond=nb, iabond=np.asarray(mc.iabond)[1:natom + 1, 1:mb + 1].astype(np.int32) - 1,
+                          tbond=np.asarray(mc.tbond)[1:natom + 1, 1:mb + 1].astype(f32),
+                          imageatom=np.asarray(mc.imageatom[1:natom + 1], np.int32) - 1,
+                          qtype=np.asarray(mc.qtype[1:natom + 1], np.int32),
+                          amassa=np.asarray(mc.amassa[1:b.ntype + 1], f32), amassr=np.asarray(mc.amassr[1:npairs + 1], f32),
+                          xav=np.asarray(pp.xav)[:ld, 1:npairs + 1].T, xav1=np.asarray(pp.xav1)[:ld, 1:npairs + 1].T,
+                          stepcl=f32(e16.cellst) / f32(mc.dmaxmol), simt=f32(mc.simt), sizefactor=f32(mc.sizefactor),
+                          tempb=f32(mc.tempb), tempang=f32(mc.tempang), refine_intra=bool(getattr(mc, "refine_intra", False)),
+                          refine_intra_fac=f32(getattr(mc, "refine_intra_fac", 0.0)))
+
     def molfit(self, fadds, faddbs, nisum, intra, rotfreq, ireset):
-        """molfit.py:52-541 (whole-molecule branch on the device); returns (fadds, faddbs, nisum)."""
+        """molfit.py:52-541: the whole-molecule branch and, for boxes without rotational groups,
+        the intramolecular branch (:124-174) on the device; returns (fadds, faddbs, nisum)."""
         c = self.c
         mc, cc = c.molecom, c.clustercom
         nmol = int(cc.nmol)
@@ -371,6 +401,10 @@ class PairPath:
         if float(mc.stepri) > 0.0:
             ngrot = np.asarray(cc.ngrot[1:nmol + 1])
             internal = bool(np.any(ngrot > 0)) and nisum == rotfreq * _idiv(nisum, rotfreq)
+        if nisum >= intra and not self._outside_path():
+            r = self._molfit_intra(fadds, faddbs, ireset)
+            if r is not None:
+                return r
         if nisum >= intra or internal or self._outside_path():
             return self._host("molfit", fadds, faddbs, nisum, intra, rotfreq, ireset)
         b = self._sync_in()
@@ -408,6 +442,45 @@ class PairPath:
         self._store_out(values_only=True)
         faddbs = f32(faddbs) + f32(0.0) / f32(nmol)     # faddb stays 0 in the whole-molecule branch
         return out["fadds"], faddbs, nisum + 1
+
+    def _molfit_intra(self, fadds, faddbs, ireset):
+        """The intramolecular cycle of molfit (:119-174, :246-247, step adaptation :465-536) on
+        the device; None when the box has rotational groups (the host runs the cycle)."""
+        c = self.c
+        mc, cc = c.molecom, c.clustercom
+        nmol = int(cc.nmol)
+        if bool(np.any(np.asarray(cc.ngrot[1:nmol + 1]) > 0)) or getattr(mc, "nbond", None) is None:
+            return None
+        b = self._sync_in()
+        self._check_cells()
+        self._store_in()
+        mc.tol = f32(mc.tolout) / f32(cc.dmax)
+        nmt = int(cc.nmoltype)
+        for name in ("nmovei", "ninter", "nwhole", "nmovem"):
+            getattr(cc, name)[1:3, 1:nmt + 1] = 0
+        mc.tempang = mc.tempangwt
+        mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
+        model = self._intra_model(b)
+        tmax, tmin = trsteps(b.natomr)
+        d = self.d
+        d.mc_setup(rejrate=f32(c.epsr16.rejrate), stepr=f32(mc.stepr), stepm=f32(mc.stepm),
+                   wholerot=np.asarray(cc.wholerot[1:nmt + 1], f32), wholetrans=np.asarray(cc.wholetrans[1:nmt + 1], f32),
+                   internrot=np.asarray(cc.internrot[1:nmt + 1], f32),
+                   interntrans=np.asarray(cc.interntrans[1:nmt + 1], f32),
+                   nstepreject=np.asarray(cc.nstepreject[1:nmol + 1], np.int32), ran1=Ran1State(),
+                   trstepmax=tmax, trstepmin=tmin, ireset=int(ireset), fadds=f32(fadds))
+        d.m_ran1 = self._ran1_in()
+        d.cmc.ran1 = C.c_void_p(d.m_ran1.data_ptr())
+        fb = torch.tensor([float(f32(faddbs))], dtype=torch.float32, device=d.dev)
+        nmovei = model.molfit_shake(f32(mc.stepmi), fb).cpu().numpy()
+        out = d.download_mc()
+        self._ran1_out(d.m_ran1)
+        cc.wholerot[1:nmt + 1], cc.wholetrans[1:nmt + 1] = out["wholerot"], out["wholetrans"]
+        cc.internrot[1:nmt + 1], cc.interntrans[1:nmt + 1] = out["internrot"], out["interntrans"]
+        cc.nmovei[1:3, 1:nmt + 1] = nmovei.reshape(2, nmt)
+        self._coords_out()
+        self._store_out(values_only=True)
+        return out["fadds"], f32(fb.cpu().numpy()[0]), 1
 
     def en_change(self, im):
         """molfit.py:806-919 for molecule im (1-based) against its stored list; fills

@@ -81,10 +81,15 @@ def run_case(name, s, out, *, refine_intra=False, seed=0, cycles=2, interntrans_
     out[p + "internrot_in"] = np.array(clustercom.internrot[1: nmt + 1], f32)
     out[p + "wholerot_in"] = np.array(clustercom.wholerot[1: nmt + 1], f32)
     out[p + "wholetrans_in"] = np.array(clustercom.wholetrans[1: nmt + 1], f32)
+    # the keys the drop-in tests' COMMON stand-ins read (tests/fake_common.py)
+    out[p + "in_wholerot"], out[p + "in_wholetrans"] = out[p + "wholerot_in"], out[p + "wholetrans_in"]
+    out[p + "in_stepr"], out[p + "in_stepm"] = f32(molecom.stepr), f32(molecom.stepm)
+    out[p + "in_rejrate"] = f32(epsr16.rejrate)
     out[p + "in_natomr"] = np.int32(molecom.natomr)
     out[p + "in_maxmolsize"] = f32(molecom.maxmolsize)
     # cell list, intramolecular energies and the pair store, as the reference loop builds them
     sepmax = epsr16.xstar[epsr16.nptmax] + molecom.maxmolsize + r4(3.0) / clustercom.dmax
+    out[p + "in_sepmax"], out[p + "in_nmolcell"] = f32(sepmax), np.int32(10)
     cellneighbourlist.initialise_cellneighbourlist(10, clustercom.xadd, clustercom.yadd, clustercom.zadd,
                                                    clustercom.nmol, sepmax)
     for im in range(1, s.nmol + 1):
