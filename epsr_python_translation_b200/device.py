@@ -182,7 +182,10 @@ class DeviceBox:
         st.nnbrefmax, st.capacity = M, cap
         st.nergpairm, st.molergpair, st.ergpairref, st.ergpair, st.nergpair = (
             _ptr(t) for t in (self.s_nergpairm, self.s_mol, self.s_ref, self.s_erg, self.s_n))
-        if getattr(self, "_eintra_src", None) is not eintra:
+        if isinstance(eintra, torch.Tensor):              # already on the device (epsr_en_mole_intra)
+            self.eintra = eintra.to(device=self.dev, dtype=torch.float32).contiguous()
+            self._eintra_src = None
+        elif getattr(self, "_eintra_src", None) is not eintra:
             self.eintra = self._t(eintra, f32)
             self._eintra_src = eintra
         nb = self.lib.epsr_fmolec1_scratch_bytes(b.nmol, self.cells.ncell, M)
