@@ -347,6 +347,7 @@ def gpu_arm(a):
     e2e_value = world * R * a.steps * moves / (e2e_ms / 1000.0)
 
     boxes.close()
+    intra = intra_cycle(it, wl, a) if rank == 0 else None
     stage_ms = {k: v / a.steps for k, v in stage_tot.items()}
     roof, extra = roofline(it, stage_ms, a)
     launches = kernel_launches(it, wl)
@@ -376,6 +377,7 @@ def gpu_arm(a):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": R * h2d,
                     "d2h_bytes_per_step": sum(d2h)},
             "roofline": roof, **extra,
+            "intra_cycle": intra,
             "gpu_launches": launches * a.steps * R,
             "clocks": clk,
         }
@@ -386,6 +388,56 @@ def gpu_arm(a):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def intra_cycle(it, wl, a):
+    """The intramolecular branch of molfit (molfit.py:124-174) on box 0 after the timed steps:
+    device time of one cycle over every molecule (CUDA events, after 3 warm-up cycles), and the
+    single-threaded C oracle on the same starting state."""
+    import numpy as np
+
+    from epsr_python_translation_b200 import configs
+    from epsr_python_translation_b200.intra import IntraModel
+    from oracle import oracle
+    s = wl.system
+    m = configs.intra_model(s)
+    d = it.d
+    model = IntraModel(d, **m)
+    stepmi = 1.0
+    faddbs = torch.zeros(1, dtype=torch.float32, device=d.dev)
+    # start state for the oracle (coordinates, store, steps, ran1) before the timed cycles
+    box = it.box.copy()
+    for k, v in d.download_coords().items():
+        getattr(box, k)[:] = v
+    st = d.download_store()
+    st = dict(nnbrefmax=st["nnbrefmax"], nergpair=st["nergpair"], nergpairm=st["nergpairm"].astype(np.int32),
+              molergpair=np.ascontiguousarray(st["molergpair"], np.int32).reshape(-1),
+              ergpairref=np.ascontiguousarray(st["ergpairref"], np.int32).reshape(-1),
+              ergpair=st["ergpair"].astype(np.float32).copy())
+    mc0 = d.download_mc()
+    for _ in range(3):
+        model.molfit_shake(stepmi, faddbs)
+    torch.cuda.synchronize()
+    n = max(3, a.steps)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(n):
+        model.molfit_shake(stepmi, faddbs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    moved = int(np.sum(box.nato > 1))
+    out = {"ms": ms, "moves_per_s": moved / (ms / 1000.0), "molecules_moved": moved,
+           "workload": f"one intramolecular cycle of box 0 ({a.config}: every molecule of more than one atom, "
+                       "harmonic bonds and bond-angle pairs of the templates)"}
+    if not a.no_cpu_baseline:
+        mc = {k: np.array(mc0[k], np.float32) for k in ("wholerot", "wholetrans", "internrot", "interntrans")}
+        mc.update(rejrate=np.float32(wl.rejrate), ireset=0)
+        t0 = time.perf_counter()
+        oracle.molfit_shake(box, st, mc, m, stepmi, mc0["ran1"], 0.0, 0.0)
+        out["cpu_ms"] = 1000.0 * (time.perf_counter() - t0)
+        out["cpu_kind"] = "port (single-threaded C oracle)"
+    return out
 
 
 def kernel_launches(it, wl):

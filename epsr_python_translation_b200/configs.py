@@ -503,6 +503,31 @@ def fit_problem(nq=600, nterms=116, seed=5, noise=0.005):
     return dict(q=q, expr=expr, yin=yin, nterms=nterms, npt=nq)
 
 
+def intra_model(s: System):
+    """The intramolecular model of en_atom_intra (molfit.py:923) for system ``s``: the
+    templates' harmonic bonds in both atoms' lists (box units; a negative length marks a
+    bond-angle pair), per-type masses, unit bond weights x dmax, and the reference potential
+    (ecoul) for the non-bonded pairs inside a molecule."""
+    natom = int(s.itype.shape[0])
+    lists = [[] for _ in range(natom)]
+    for m in range(s.nmol):
+        a0 = int(s.naf[m])
+        for (i, j, length) in s.bonds[int(s.mtype[m])]:
+            for (a, b) in ((a0 + i, a0 + j), (a0 + j, a0 + i)):
+                lists[a].append((b, f32(length) / f32(s.dmax)))
+    mb = max(1, max(len(v) for v in lists))
+    iabond = np.full((natom, mb), -1, np.int32)
+    tbond = np.zeros((natom, mb), f32)
+    for a, v in enumerate(lists):
+        for k, (b, t) in enumerate(v):
+            iabond[a, k], tbond[a, k] = b, t
+    return dict(nbond=np.array([len(v) for v in lists], np.int32), iabond=iabond, tbond=tbond,
+                amassa=np.array([TYPE_PARAMS[lab][3] for lab in s.type_labels], f32),
+                amassr=np.full(s.npairs, f32(1.0) * f32(s.dmax), f32), xav=s.ecoul, xav1=s.ecoul1,
+                stepcl=f32(s.cellst) / f32(s.dmax), simt=f32(s.simt), sizefactor=f32(1.0), tempb=f32(1.0),
+                tempang=f32(1.0), refine_intra=False, refine_intra_fac=f32(0.0))
+
+
 # ----------------------------------------------------------------------------- workloads
 def intra_energies(s: System, k_bond=1000.0):
     """Per-molecule harmonic bond energies (float32) of the seeded geometry.
