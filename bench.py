@@ -395,6 +395,7 @@ def intra_cycle(it, wl, a):
     device time of one cycle over every molecule (CUDA events, after 3 warm-up cycles), and the
     single-threaded C oracle on the same starting state."""
     import numpy as np
+    import torch
 
     from epsr_python_translation_b200 import configs
     from epsr_python_translation_b200.intra import IntraModel

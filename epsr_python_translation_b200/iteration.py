@@ -261,6 +261,8 @@ class EpsrIteration:
                                                   C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         r = self._rep
         self.d.nnbrefmax = int(r.nnbrefmax)
+        if self.d.store is not None:        # the store struct other calls take follows the driver's layout
+            self.d.store.nnbrefmax = int(r.nnbrefmax)
         self.ftest = (np.float32(r.ftest[0]), np.float32(r.ftest[1]))
         self.pair_updates = int(r.pair_updates)
         self.energy, self.pressc = press_scalars(b.nmol, np.float32(r.press[0]), float(r.press[1]), b.simt,
