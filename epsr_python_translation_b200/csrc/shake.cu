@@ -168,8 +168,8 @@ struct ShakeDev {
     int32_t *nwhole, *nmovem, *nmovei;
     // scratch
     long long *off;      // [nmol] first ran1 value of each molecule, -1: not moved
-    long long *total;    // [1]
-    int32_t *status;     // [1] 1: a molecule with rotational groups
+    long long *total;    // [2]: the draw count, then the status (1: a molecule with rotational groups)
+    int32_t *status;     // = (int32_t *)(total + 1)
     const float *vals;   // [total] the cycle's ran1 values
     float *xt, *yt, *zt; // [natom] trial coordinates
     float *enew;         // [nmol]
@@ -256,9 +256,17 @@ __global__ void shake_trial_kernel(ShakeDev D) {
     D.enew[im] = en_mole_intra_d(D.I, im, D.xt, D.yt, D.zt);
 }
 
+// The Metropolis test value of en_change_intra's difference (molfit.py:147-154).
+__device__ __forceinline__ float metropolis_etest(float enew, float eold, float temp) {
+    const float ediff = __fmul_rn(__fsub_rn(enew, eold), temp);
+    if (ediff <= 0.0f) return 10.0f;
+    if (ediff < 20.0f) return exp_r(-ediff);
+    return 0.0f;
+}
+
 // The ordered pass (:119-170 per molecule) and the step adaptation (:465-536).
 __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
-    __shared__ float s_enew[SH_TILE], s_r[SH_TILE], s_v1[SH_TILE];
+    __shared__ float s_enew[SH_TILE], s_r[SH_TILE], s_v1[SH_TILE], s_et[SH_TILE];
     __shared__ int s_nn[SH_TILE], s_prev[SH_TILE], s_mt[SH_TILE];
     __shared__ int s_slot[SH_TILE];
     __shared__ unsigned char s_mv[SH_TILE];
@@ -299,6 +307,7 @@ __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
             s_slot[k] = slot;
             s_v1[k] = v1;
             s_prev[k] = prev;
+            if (o >= 0 && nn >= 1) s_et[k] = metropolis_etest(s_enew[k], v1, temp);   // the usual case
         }
         __syncthreads();
         if (tid == 0) {
@@ -313,11 +322,10 @@ __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
                 if (s_mv[k]) {
                     const int mt = s_mt[k];
                     const float fdiffb = __fsub_rn(s_enew[k], ergold1);
-                    const float ediff = __fmul_rn(fdiffb, temp);
-                    float etest;
-                    if (ediff <= 0.0f) etest = 10.0f;
-                    else if (ediff < 20.0f) etest = exp_r(-ediff);
-                    else etest = 0.0f;
+                    // the test value was formed in parallel against the molecule's own first stored
+                    // energy; it is formed again only when the chain changed that energy
+                    const float etest = (s_nn[k] >= 1 && __float_as_uint(ergold1) == __float_as_uint(s_v1[k]))
+                                            ? s_et[k] : metropolis_etest(s_enew[k], ergold1, temp);
                     a = s_r[k] < etest;
                     if (mt < 64) {
                         ++cnt[mt];
@@ -492,8 +500,8 @@ extern "C" int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, eps
     D.off = (long long *)p;
     p += al256(8 * (size_t)D.nmol);
     D.total = (long long *)p;
+    D.status = (int32_t *)(D.total + 1);
     p += 256;
-    D.status = (int32_t *)p;
     p += 256;
     float *vals = (float *)p;
     D.vals = vals;
@@ -510,10 +518,10 @@ extern "C" int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, eps
 
     shake_plan_kernel<<<1, SH_THREADS, 0, s>>>(D);
     EPSR_CUDA(cudaGetLastError());
-    long long total = 0;
-    int32_t status = 0;
-    EPSR_D2H(&total, D.total, sizeof(total), s);
-    EPSR_D2H(&status, D.status, sizeof(status), s);
+    long long tot2[2] = {0, 0};
+    EPSR_D2H(tot2, D.total, sizeof(tot2), s);
+    const long long total = tot2[0];
+    const int32_t status = (int32_t)(tot2[1] & 0xffffffff);
     if (status) {
         epsr_set_error("epsr_molfit_shake: molecules with rotational groups (internal rotations and dihedral terms "
                        "are outside this path)");
