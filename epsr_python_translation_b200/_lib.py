@@ -60,6 +60,17 @@ class Intra(C.Structure):
                 ("refine_intra_fac", F32)]
 
 
+class Rp(C.Structure):
+    """epsr_rp_t: inputs and outputs of generate_mp + generate_rp (host pointers)."""
+    _fields_ = [("npairs", I32), ("npt", I32), ("npt2", I32), ("ld", I32), ("x", P), ("xstar", P), ("wfac", P),
+                ("wfacc", P), ("power", F32), ("ecore", F32), ("dcore", F32), ("sizefactor", F32),
+                ("refpotfac", F32), ("expecf", F32), ("expecfpwr", F32), ("harmonic", I32), ("modmorse", I32),
+                ("coul_intra", I32), ("coul_intra_fac", F32), ("n1extr", P), ("n2extr", P), ("irefpcof", P),
+                ("qradius", P), ("ecor", P), ("qcor", P), ("dcor", P), ("coulfac", P), ("pcoefex", P),
+                ("rminex", P), ("npgauss", P), ("maxgauss", I32), ("wpgauss", P), ("rpgauss", P), ("hpgauss", P),
+                ("epot", P), ("epot1", P), ("ecoul", P), ("ecoul1", P), ("xav", P), ("xav1", P)]
+
+
 class Iteration(C.Structure):
     """epsr_iteration_t: one EPSR iteration of the path, driven natively."""
     _fields_ = [("box", P), ("mc", P),
@@ -124,6 +135,7 @@ _SIGS = {
     "epsr_en_mole_intra": (C.c_int, [P, P, P, P]),
     "epsr_molfit_shake_scratch_bytes": (I64, [I32, I32]),
     "epsr_molfit_shake": (C.c_int, [P, P, P, P, F32, P, P, P, I64, P]),
+    "epsr_generate_rp": (C.c_int, [P]),
     "epsr_calc_pwrexpr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
     "epsr_calc_gaussr_grad": (C.c_int, [I32, I32, F32, F32, F32, F32, P, P, F32, P, F32, F32]),
     "epsr_stog": (C.c_int, [F32, P, I32, P, P, I32, I32, P, P, P, P, P, I64, P]),

@@ -18,6 +18,7 @@ reference's argument lists and return values:
 * ``press`` (library/ato_manipulation_rev4.py:3903)
 * ``sumgr`` / ``sumsq`` (programs/epsr_standalone_rev3.py:3578 / :3642)
 * ``generate_ep`` (programs/epsr_standalone_rev3.py:5876)
+* ``generate_rp`` (programs/epsr_standalone_rev3.py:5675, with generate_mp)
 
 ``install()`` assigns them onto the given modules (the reference's own rerouting
 mechanism, trace.py:94-125) and keeps the originals.
@@ -51,7 +52,7 @@ from .box import BoxArrays, Ran1State, trsteps
 
 f32 = np.float32
 ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit", "atogen", "stog", "gensq", "fit_expansion",
-            "press", "sumgr", "sumsq", "generate_ep", "en_change", "en_mole_pair")
+            "press", "sumgr", "sumsq", "generate_ep", "generate_rp", "en_change", "en_mole_pair")
 # en_change / en_mole_pair are per-molecule calls: rerouting them makes every host caller
 # (including host fallbacks) launch one kernel per call, so they are installed only on request.
 DEFAULT_ROUTINES = tuple(r for r in ROUTINES if r not in ("en_change", "en_mole_pair"))
@@ -60,7 +61,7 @@ OWNER = {"initialise_cellneighbourlist": "cellneighbourlist", "fmolec1": "ato_ma
          "atogen": "ato_manipulation_rev4", "stog": "ato_manipulation_rev4", "press": "ato_manipulation_rev4",
          "molfit": "molfit",
          "en_change": "molfit", "en_mole_pair": "molfit", "gensq": "program", "fit_expansion": "program",
-         "sumgr": "program", "sumsq": "program", "generate_ep": "program"}
+         "sumgr": "program", "sumsq": "program", "generate_ep": "program", "generate_rp": "program"}
 
 
 def _fortran(shape, dtype):
@@ -641,6 +642,36 @@ class PairPath:
         pp.pcoefp[2: nterms + 1, 1:nsets + 1] = pc.cpu().numpy()[:, 2:].T
         pp.pwtold[1: nterms + 1] = pw.cpu().numpy()[1:]
         pp.potfac = f32(pf.cpu().numpy()[0])
+        return None
+
+    def generate_rp(self):
+        """epsr_standalone_rev3.py:5675-5873 (generate_mp ato_manipulation_rev4.py:2816 first): the
+        reference potential tables epot, epot1, ecoul, ecoul1, xav, xav1 of potential_par,
+        rebuilt on the host by the library (the C library's float functions, as the reference)
+        and written in place; the next device call uploads the changed tables.  Sets with
+        container forces (rmaxex > 0) run the reference's own routine."""
+        from . import potential
+        c = self.c
+        pp, mc, e16, ip = c.potential_par, c.molecom, c.epsr16, c.epsrinput_par
+        npairs, npt, npt2 = int(mc.npairs), int(e16.npt), int(e16.npt2)
+        iref = np.asarray(pp.irefpcof[1:npairs + 1], np.int32) - 1
+        nsets = int(iref.max()) + 1
+        if bool(np.any(np.asarray(pp.rmaxex[1:nsets + 1]) > 0.0)):
+            return self._host("generate_rp")
+        npg = np.asarray(pp.npgauss[1:nsets + 1], np.int32)
+        maxg = max(1, int(npg.max()))
+        g = lambda a: np.asarray(a)[1:maxg + 1, 1:nsets + 1].T  # noqa: E731
+        ld = npt + 1
+        out = potential.reference_potential(
+            np.asarray(e16.x)[:ld], np.asarray(e16.xstar)[:ld], np.asarray(pp.wfac)[:ld], np.asarray(pp.wfacc)[:ld], npt,
+            npt2, np.asarray(mc.n1extr[1:npairs + 1], np.int32) - 1, np.asarray(mc.n2extr[1:npairs + 1], np.int32) - 1,
+            iref, np.asarray(mc.qradius)[1:], np.asarray(mc.ecor[1:npairs + 1]), np.asarray(mc.qcor[1:npairs + 1]),
+            np.asarray(mc.dcor[1:npairs + 1]), np.asarray(pp.coulfac[1:nsets + 1]), np.asarray(pp.pcoefex[1:nsets + 1]),
+            np.asarray(pp.rminex[1:nsets + 1]), mc.power, mc.ecore, mc.dcore, mc.sizefactor, pp.refpotfac, ip.expecf,
+            ip.expecfpwr, bool(pp.harmonic), pp.addpotential == "modmorse", bool(mc.coul_intra), mc.coul_intra_fac, npg,
+            g(pp.wpgauss), g(pp.rpgauss), g(pp.hpgauss))
+        for k in potential.RP_TABLES:
+            getattr(pp, k)[1:ld, 1:npairs + 1] = out[k][:, 1:ld].T
         return None
 
     def stog(self, rho, q, sofq, r, gofr, nqmin, nqmax, nr, npairs, nqdim, nrdim, npdim, xwt):

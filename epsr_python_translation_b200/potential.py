@@ -107,3 +107,44 @@ def pack_tables(xavs, xavs1, ecoul, ecoul1, tab):
     if tab.numel() < 4 * npairs * ld or any(tuple(t.shape) != (npairs, ld) for t in (xavs1, ecoul, ecoul1)):
         raise ValueError("pack_tables: inconsistent shapes")
     check(lib.epsr_pack_tables(int(npairs), int(ld), _p(xavs), _p(xavs1), _p(ecoul), _p(ecoul1), _p(tab), _s()))
+
+
+RP_TABLES = ("epot", "epot1", "ecoul", "ecoul1", "xav", "xav1")
+
+
+def reference_potential(x, xstar, wfac, wfacc, npt, npt2, n1extr, n2extr, irefpcof, qradius, ecor, qcor, dcor, coulfac,
+                        pcoefex, rminex, power, ecore, dcore, sizefactor=1.0, refpotfac=1.0, expecf=0.0,
+                        expecfpwr=0.0, harmonic=False, modmorse=False, coul_intra=False, coul_intra_fac=0.0,
+                        npgauss=None, wpgauss=None, rpgauss=None, hpgauss=None, out=None):
+    """generate_mp + generate_rp (ato_manipulation_rev4.py:2816, epsr_standalone_rev3.py:5675) on
+    the host through the library: returns the tables epot, epot1, ecoul, ecoul1, xav, xav1
+    ((npairs, npt+1) float32 each, r index 1-based).  Types and sets are 0-based; the Gaussian
+    arrays are (nsets, maxgauss)."""
+    lib = _lib.load()
+    npairs = len(n1extr)
+    ld = int(npt) + 1
+    a = lambda v, dt=f32: np.ascontiguousarray(np.asarray(v, dt))  # noqa: E731
+    nsets = len(coulfac)
+    npg = a(np.zeros(nsets) if npgauss is None else npgauss, np.int32)
+    maxg = 0 if wpgauss is None else np.asarray(wpgauss).reshape(nsets, -1).shape[1]
+    keep = dict(x=a(x)[:ld], xstar=a(xstar)[:ld], wfac=a(wfac)[:ld], wfacc=a(wfacc)[:ld], n1extr=a(n1extr, np.int32),
+                n2extr=a(n2extr, np.int32), irefpcof=a(irefpcof, np.int32), qradius=a(qradius), ecor=a(ecor),
+                qcor=a(qcor), dcor=a(dcor), coulfac=a(coulfac), pcoefex=a(pcoefex), rminex=a(rminex), npgauss=npg)
+    for k, v in (("wpgauss", wpgauss), ("rpgauss", rpgauss), ("hpgauss", hpgauss)):
+        keep[k] = a(np.zeros((nsets, 1)) if v is None else np.asarray(v).reshape(nsets, -1))
+    out = out if out is not None else {k: np.zeros((npairs, ld), f32) for k in RP_TABLES}
+    r = _lib.Rp()
+    r.npairs, r.npt, r.npt2, r.ld = npairs, int(npt), int(npt2), ld
+    for k, v in keep.items():
+        setattr(r, k, v.ctypes.data_as(C.c_void_p))
+    for k in RP_TABLES:
+        if out[k].shape != (npairs, ld) or out[k].dtype != f32 or not out[k].flags.c_contiguous:
+            raise ValueError(f"reference_potential: table {k} must be a contiguous float32 ({npairs}, {ld}) array")
+        setattr(r, k, out[k].ctypes.data_as(C.c_void_p))
+    r.power, r.ecore, r.dcore, r.sizefactor = (float(f32(v)) for v in (power, ecore, dcore, sizefactor))
+    r.refpotfac, r.expecf, r.expecfpwr = (float(f32(v)) for v in (refpotfac, expecf, expecfpwr))
+    r.harmonic, r.modmorse, r.coul_intra = int(bool(harmonic)), int(bool(modmorse)), int(bool(coul_intra))
+    r.coul_intra_fac = float(f32(coul_intra_fac))
+    r.maxgauss = int(maxg)
+    check(lib.epsr_generate_rp(C.byref(r)))
+    return out

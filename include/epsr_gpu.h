@@ -375,6 +375,33 @@ int epsr_ep_update(int32_t ndata, int32_t npairs, int32_t nterms, float *pcoefp,
 int epsr_pack_tables(int32_t npairs, int32_t ld, const float *xavs, const float *xavs1, const float *ecoul,
                      const float *ecoul1, float *tab, void *stream);
 
+/* The reference potential tables, host pointers throughout: generate_mp ato_manipulation_rev4.py:
+ * 2816-2902 (the WCA core xav of intramolecular pairs) then generate_rp epsr_standalone_rev3.py:
+ * 5675-5873 (n-6 Lennard-Jones + charged-sphere Coulomb, Gaussians or gauss6pot's modified
+ * Morse, the repulsive core, forward-difference gradients).  Tables [npairs][ld] with the r
+ * index 1-based; sets are 0-based (irefpcof).  Pairs whose set has rmaxex > 0 (container
+ * forces) are outside this path.  Host computation with the C library's single-precision
+ * functions, bit-identical. */
+typedef struct {
+    int32_t npairs, npt, npt2, ld;
+    const float *x, *xstar, *wfac, *wfacc;     /* [ld] */
+    float power, ecore, dcore, sizefactor, refpotfac, expecf, expecfpwr;
+    int32_t harmonic;                          /* repulsive core: 0 exponential, 1 harmonic */
+    int32_t modmorse;                          /* addpotential == "modmorse" */
+    int32_t coul_intra;
+    float coul_intra_fac;
+    const int32_t *n1extr, *n2extr;            /* [npairs] 0-based atom types */
+    const int32_t *irefpcof;                   /* [npairs] 0-based sets */
+    const float *qradius;                      /* [ntype] */
+    const float *ecor, *qcor, *dcor;           /* [npairs] */
+    const float *coulfac, *pcoefex, *rminex;   /* [nsets] */
+    const int32_t *npgauss;                    /* [nsets] */
+    int32_t maxgauss;
+    const float *wpgauss, *rpgauss, *hpgauss;  /* [nsets][maxgauss] */
+    float *epot, *epot1, *ecoul, *ecoul1, *xav, *xav1;   /* out, [npairs][ld] */
+} epsr_rp_t;
+int epsr_generate_rp(const epsr_rp_t *rp);
+
 /* calc_pwrexpr_grad epsr_standalone_rev3.py:5230-5309 (the power-exponential basis, with the
  * spacing of dnext :5312) and calc_gaussr_grad :5046-5096 (the Gaussian basis): host
  * functions, the C library's logf/expf as the reference.  xin host [lpt+1] (1-based), expr

@@ -105,4 +105,5 @@ def routine_modules(z, calls):
             "molfit": NS(molfit=rec("host:molfit", (f32(0), f32(0), 1)), en_change=rec("host:en_change"),
                          en_mole_pair=rec("host:en_mole_pair"), en_mole_intra=en_mole_intra),
             "program": NS(gensq=rec("host:gensq"), fit_expansion=rec("host:fit_expansion"), sumgr=rec("host:sumgr"),
-                          sumsq=rec("host:sumsq"), generate_ep=rec("host:generate_ep"))}
+                          sumsq=rec("host:sumsq"), generate_ep=rec("host:generate_ep"),
+                          generate_rp=rec("host:generate_rp"))}
