@@ -149,10 +149,43 @@ __device__ float en_mole_intra_d(const IntraDev &I, int im, const float *x, cons
     return e;
 }
 
-__global__ void en_mole_intra_kernel(IntraDev I, int nmol, const float *xa, const float *ya, const float *za,
-                                     float *out) {
-    const int im = blockIdx.x * blockDim.x + threadIdx.x;
-    if (im < nmol) out[im] = en_mole_intra_d(I, im, xa, ya, za);
+// en_mole_intra with the molecule's atom pairs spread over the lanes of one warp: every lane
+// evaluates pairs (flattened in the reference's (ia, ja) order) into the warp's slice of
+// shared memory, then lane 0 sums them in that order.  Molecules of more than SH_WAT atoms fall
+// back to one thread.  The value is returned on lane 0.
+constexpr int SH_WAT = 64;
+constexpr int SH_WPAIRS = SH_WAT * (SH_WAT - 1) / 2;
+constexpr int SH_WARPS = 4;   // warps (molecules) per CTA of the warp kernels
+
+__device__ float warp_en_mole_intra(const IntraDev &I, int im, const float *x, const float *y, const float *z,
+                                    float *pe, int lane) {
+    const int a0 = I.naf[im], n = I.nato[im];
+    if (n > SH_WAT) return lane == 0 ? en_mole_intra_d(I, im, x, y, z) : 0.0f;
+    const int np = n * (n - 1) / 2;
+    for (int p = lane; p < np; p += 32) {
+        int i = 0, q = p;
+        while (q >= n - 1 - i) {   // row i holds the pairs (i, i+1..n-1)
+            q -= n - 1 - i;
+            ++i;
+        }
+        const int ia = a0 + i, ja = a0 + i + 1 + q;
+        pe[p] = en_atom_intra_d(I, ia, ja, x[ia], y[ia], z[ia], x[ja], y[ja], z[ja]);
+    }
+    __syncwarp();
+    float e = 0.0f;
+    if (lane == 0)
+        for (int p = 0; p < np; ++p) e = __fadd_rn(e, pe[p]);
+    return e;
+}
+
+__global__ void __launch_bounds__(32 * SH_WARPS) en_mole_intra_kernel(IntraDev I, int nmol, const float *xa,
+                                                                       const float *ya, const float *za, float *out) {
+    __shared__ float pe[SH_WARPS][SH_WPAIRS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int im = blockIdx.x * SH_WARPS + w;
+    if (im >= nmol) return;
+    const float e = warp_en_mole_intra(I, im, xa, ya, za, pe[w], lane);
+    if (lane == 0) out[im] = e;
 }
 
 // ---------------------------------------------------------------- the cycle
@@ -238,22 +271,26 @@ __global__ void __launch_bounds__(SH_THREADS) shake_plan_kernel(ShakeDev D) {
 }
 
 // movei/movea (:545-567): atom by atom, z then y then x, x += step * (2 r - 1); then the new
-// intramolecular energy of the trial coordinates.
-__global__ void shake_trial_kernel(ShakeDev D) {
-    const int im = blockIdx.x * blockDim.x + threadIdx.x;
+// intramolecular energy of the trial coordinates.  One warp per molecule.
+__global__ void __launch_bounds__(32 * SH_WARPS) shake_trial_kernel(ShakeDev D) {
+    __shared__ float pe[SH_WARPS][SH_WPAIRS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int im = blockIdx.x * SH_WARPS + w;
     if (im >= D.nmol) return;
     const long long o = D.off[im];
     if (o < 0) return;
     const int a0 = D.I.naf[im], n = D.I.nato[im];
     const float step = D.interntrans[D.I.mtype[im]];
     const float *r = D.vals + o;
-    for (int k = 0; k < n; ++k) {
+    for (int k = lane; k < n; k += 32) {
         const int a = a0 + k;
         D.zt[a] = __fadd_rn(D.za[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, r[3 * k]), 1.0f)));
         D.yt[a] = __fadd_rn(D.ya[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, r[3 * k + 1]), 1.0f)));
         D.xt[a] = __fadd_rn(D.xa[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, r[3 * k + 2]), 1.0f)));
     }
-    D.enew[im] = en_mole_intra_d(D.I, im, D.xt, D.yt, D.zt);
+    __syncwarp();
+    const float e = warp_en_mole_intra(D.I, im, D.xt, D.yt, D.zt, pe[w], lane);
+    if (lane == 0) D.enew[im] = e;
 }
 
 // The Metropolis test value of en_change_intra's difference (molfit.py:147-154).
@@ -440,7 +477,8 @@ extern "C" int epsr_en_mole_intra(const epsr_box_t *box, const epsr_intra_t *in,
         return EPSR_ERR_ARG;
     }
     const IntraDev I = make_intradev(box, in);
-    en_mole_intra_kernel<<<(box->nmol + 127) / 128, 128, 0, (cudaStream_t)stream>>>(I, box->nmol, box->xa, box->ya,
+    en_mole_intra_kernel<<<(box->nmol + SH_WARPS - 1) / SH_WARPS, 32 * SH_WARPS, 0, (cudaStream_t)stream>>>(
+        I, box->nmol, box->xa, box->ya,
                                                                                   box->za, out);
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
@@ -536,7 +574,7 @@ extern "C" int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, eps
         if (rc) return rc;
     }
     const int nb = (D.nmol + 127) / 128;
-    shake_trial_kernel<<<nb, 128, 0, s>>>(D);
+    shake_trial_kernel<<<(D.nmol + SH_WARPS - 1) / SH_WARPS, 32 * SH_WARPS, 0, s>>>(D);
     EPSR_CUDA(cudaGetLastError());
     shake_resolve_kernel<<<1, SH_THREADS, 0, s>>>(D);
     EPSR_CUDA(cudaGetLastError());
