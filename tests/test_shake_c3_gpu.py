@@ -43,7 +43,8 @@ def test_intramolecular_cycle_full_size_matches_oracle(config):
     nmt = ob.nmoltype
     tmax, tmin = trsteps(ob.natomr)
     it0 = np.full(nmt, f32(0.02) / f32(ob.dmax), f32)
-    it0[0] = 0.0                                   # the trstepmin start for the first type
+    if nmt > 1:
+        it0[0] = 0.0                               # the trstepmin start for the first type
     rot, tra = np.full(nmt, f32(10.0 / 180.0), f32), np.full(nmt, f32(0.5) / f32(ob.dmax), f32)
     ran1 = Ran1State(idum=-11)
     d.mc_setup(rejrate=f32(0.75), stepr=f32(1.0), stepm=f32(1.0), wholerot=rot, wholetrans=tra,
