@@ -102,8 +102,14 @@ class DeviceBox:
         """Recompute the absolute positions after the offset/centre tensors were written."""
         check(self.lib.epsr_box_positions(C.byref(self.cbox), _stream()))
 
-    def download_coords(self):
-        torch.cuda.synchronize()
+    def download_coords(self, stream_only=False):
+        """Host copies of the coordinates.  stream_only: the box's work was all launched on the
+        current stream, so only that stream is waited for (other boxes on other streams keep
+        running); otherwise the whole device is synchronised first."""
+        if stream_only:
+            torch.cuda.current_stream().synchronize()
+        else:
+            torch.cuda.synchronize()
         return {k: getattr(self, k).cpu().numpy() for k in ("xa", "ya", "za", "xadd", "yadd", "zadd")}
 
     def scratch(self, name, nbytes):

@@ -285,10 +285,12 @@ class EpsrIteration:
 
     def download_outputs(self):
         """Device -> host copy of what the host consumers of the loop read after an
-        iteration: coordinates (.ato writer), the histograms (sumgr) and the EP
-        coefficients (generate_ep).  Returns the arrays and their total bytes."""
-        co = self.d.download_coords()
-        wav = self.d.a_wav.cpu().numpy()
-        pw = self.pwtold.cpu().numpy()
+        iteration: coordinates (.ato writer), the histograms of this iteration and the EP
+        coefficients (the refined pcoefp when the EP is refined, else the fits' coefficients).
+        Returns the arrays and their total bytes."""
+        co = self.d.download_coords(stream_only=True)   # this box's stream only
+        native = self.native and self._plan is not None
+        wav = (self._n_wav if native else self.d.a_wav).cpu().numpy()
+        pw = (self.ep_pcoefp if self.ep is not None else self.pwtold).cpu().numpy()
         nbytes = sum(v.nbytes for v in co.values()) + wav.nbytes + pw.nbytes
         return (co, wav, pw), nbytes
