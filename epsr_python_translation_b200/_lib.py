@@ -94,12 +94,14 @@ class Iteration(C.Structure):
                 ("cwtpot", P), ("expgr", P), ("wfac", P), ("ecoul", P), ("ecoul1", P), ("xavs", P), ("xavs1", P),
                 ("xavtot", P), ("xavtot1", P), ("ep_pwtold", P), ("potfac", P), ("ep_result", P), ("pfact", F32),
                 ("absolute_energy", F32), ("erequnit", F32), ("ereqstep", F32), ("potfacamp", F32), ("tab", P),
+                ("intra", I32), ("nisum", I32), ("stepmi", F32), ("intra_model", P), ("faddbs", P),
+                ("eintra_work", P), ("nmovei", P),
                 ("scratch", P), ("scratch_bytes", I64), ("strict", I32), ("stage_events", P * 20)]
 
 
 class IterationReport(C.Structure):
     _fields_ = [("nnbrefmax", I32), ("ftest", F32 * 2), ("ngrsamples", I32), ("pair_updates", I64),
-                ("press", C.c_double * 2)]
+                ("press", C.c_double * 2), ("nisum", I32)]
 
 
 _SIGS = {
@@ -133,6 +135,7 @@ _SIGS = {
     "epsr_ep_update": (C.c_int, [I32, I32, I32, P, I32, I32, P, P, P, P, I32, F32, P]),
     "epsr_pack_tables": (C.c_int, [I32, I32, P, P, P, P, P, P]),
     "epsr_en_mole_intra": (C.c_int, [P, P, P, P]),
+    "epsr_minimage_centres": (C.c_int, [P, P]),
     "epsr_molfit_shake_scratch_bytes": (I64, [I32, I32]),
     "epsr_molfit_shake": (C.c_int, [P, P, P, P, F32, P, P, P, I64, P]),
     "epsr_generate_rp": (C.c_int, [P]),

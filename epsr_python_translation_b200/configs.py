@@ -610,19 +610,24 @@ class Workload:
     ngrsamples: int = 0
     xwt: np.ndarray = None   # (npairs,) stog offsets
     ep: EpRefinement = None  # potential refinement after the fits (None: the EP stays fixed)
+    intra: int = 0           # molfit cycles between intramolecular cycles (0: rigid molecules, none)
+    stepmi: float = 1.0      # intramolecular step flag (> 0 moves the atoms of multi-atom molecules)
 
     @property
     def nq(self):
         return int(self.q.shape[0] - 1)
 
 
-def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, ndata=None, ntimes=5, refine=True):
+def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, ndata=None, ntimes=5, refine=True,
+                  intra=0):
     """One iteration's inputs on a named configuration, 5 MC sweeps per iteration and a
     116-term Poisson-like EP basis.  C2 (c2_mixture): 200 DMSO + 400 water, three isotope
     data sets (deuterated, protiated, 50:50), Q to 30 A^-1 (600 points).  C3 (c3_water):
     20,000 water, one data set, Q to 50 A^-1 (1,000 points).  C1 (c1_water): 100 water.
     ``refine``: each iteration also refines the EP from the fits (ptgnsq's coefficient
-    increment and generate_ep), as the reference does while its potential factor is on."""
+    increment and generate_ep), as the reference does while its potential factor is on.
+    ``intra`` > 0: flexible molecules -- every intra-th molfit cycle is an intramolecular one
+    (the templates' bonds and bond-angle pairs, intra_model), as molfit's nisum counter picks."""
     if nq is None:
         nq = 1000 if name == "c3_water" else 600
     if ndata is None:
@@ -654,4 +659,4 @@ def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, nd
     xwt = np.linspace(0.5, 1.5, s.npairs).astype(f32)
     return Workload(name=name, system=s, eintra=intra_energies(s), q=q, foqols=F, ycoh=ycoh, expr=expr,
                     nterms=nterms, data=data, weights=w, wholerot=wholerot, wholetrans=wholetrans, ntimes=ntimes,
-                    xwt=xwt, ep=ep)
+                    xwt=xwt, ep=ep, intra=int(intra))

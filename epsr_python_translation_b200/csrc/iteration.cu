@@ -44,6 +44,7 @@ extern "C" int64_t epsr_iteration_scratch_bytes(const epsr_iteration_t *it) {
     n = imax64(n, epsr_press_scratch_bytes(b->nmol, it->store_m));
     n = imax64(n, epsr_fit_expansion_batch_scratch_bytes(it->ndata, it->nq, it->nterms));
     n = imax64(n, epsr_stog_scratch_bytes(b->npairs, ldq));
+    if (it->intra > 0) n = imax64(n, epsr_molfit_shake_scratch_bytes(b->nmol, b->natom));
     return n;
 }
 
@@ -59,6 +60,10 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
         return EPSR_ERR_CAPACITY;
     }
     const epsr_box_t *b = it->box;
+    if (it->intra > 0 && (!it->intra_model || !it->faddbs || !it->eintra_work || !it->nmovei)) {
+        epsr_set_error("epsr_iteration_step: intramolecular cycles need intra_model, faddbs, eintra_work, nmovei");
+        return EPSR_ERR_ARG;
+    }
     if (it->refine && (b->izcut != b->npt2 || !it->pcoefp || !it->irefpcof_host || !it->efacp || !it->cwtpot ||
                        !it->expgr || !it->wfac || !it->ecoul || !it->ecoul1 || !it->xavs || !it->xavs1 ||
                        !it->xavtot || !it->xavtot1 || !it->ep_pwtold || !it->potfac || !it->ep_result || !it->tab ||
@@ -101,19 +106,43 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
     store.ergpair = it->ergpair;
     store.nergpair = it->nergpair;
     store.mirror = it->mirror;
-    rc = epsr_fmolec1(b, &cells, it->eintra, &store, it->scratch, it->scratch_bytes, it->strict, rep->ftest, stream);
+    const float *eintra = it->eintra;
+    if (it->intra > 0) {   // the intramolecular energies of the model the intramolecular cycles use
+        rc = epsr_en_mole_intra(b, it->intra_model, it->eintra_work, stream);
+        if (rc) return rc;
+        eintra = it->eintra_work;
+    }
+    rc = epsr_fmolec1(b, &cells, eintra, &store, it->scratch, it->scratch_bytes, it->strict, rep->ftest, stream);
     if (rc) return rc;
     mark(it, 1, 1, s);
 
-    // ---- molfit cycles
+    // ---- molfit cycles (runepsr17 :1313-1345): molfit's branch by nisum, and after an
+    // intramolecular cycle the centres put back in the box and the pair store rebuilt
     mark(it, 2, 0, s);
     epsr_mc_t *mc = it->mc;
     mc->strict = it->strict;
     mc->cos_override = nullptr;
+    int32_t nisum = it->nisum;
     for (int t = 0; t < it->ntimes; ++t) {
-        rc = epsr_molfit(b, &cells, &store, mc, it->scratch, it->scratch_bytes, stream);
-        if (rc) return rc;
+        if (it->intra > 0 && nisum >= it->intra) {
+            rc = epsr_molfit_shake(b, &store, mc, it->intra_model, it->stepmi, it->nmovei, it->faddbs, it->scratch,
+                                   it->scratch_bytes, stream);
+            if (rc) return rc;
+            nisum = 1;
+            rc = epsr_minimage_centres(b, stream);
+            if (rc) return rc;
+            rc = epsr_en_mole_intra(b, it->intra_model, it->eintra_work, stream);
+            if (rc) return rc;
+            rc = epsr_fmolec1(b, &cells, it->eintra_work, &store, it->scratch, it->scratch_bytes, it->strict,
+                              rep->ftest, stream);
+            if (rc) return rc;
+        } else {
+            rc = epsr_molfit(b, &cells, &store, mc, it->scratch, it->scratch_bytes, stream);
+            if (rc) return rc;
+            nisum += 1;
+        }
     }
+    rep->nisum = nisum;
     mark(it, 2, 1, s);
 
     // ---- atogen: the partial g(r) histograms

@@ -454,6 +454,16 @@ __global__ void shake_apply_kernel(ShakeDev D) {
     }
 }
 
+__global__ void minimage_centres_kernel(Lattice L, int nmol, float *xadd, float *yadd, float *zadd) {
+    const int im = blockIdx.x * blockDim.x + threadIdx.x;
+    if (im >= nmol) return;
+    float x = xadd[im], y = yadd[im], z = zadd[im];
+    minimagec(L, x, y, z);
+    xadd[im] = x;
+    yadd[im] = y;
+    zadd[im] = z;
+}
+
 size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 }  // namespace epsr
@@ -482,6 +492,25 @@ extern "C" int epsr_en_mole_intra(const epsr_box_t *box, const epsr_intra_t *in,
                                                                                   box->za, out);
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
+}
+
+extern "C" int epsr_minimage_centres(const epsr_box_t *box, void *stream) {
+    if (!box || box->nmol < 1 || !box->xadd || !box->yadd || !box->zadd) {
+        epsr_set_error("epsr_minimage_centres: bad arguments");
+        return EPSR_ERR_ARG;
+    }
+    Lattice L;
+    L.cubic = box->cubic;
+    L.alatx = box->lat[0];
+    L.blatx = box->lat[1];
+    L.clatx = box->lat[2];
+    L.blaty = box->lat[3];
+    L.claty = box->lat[4];
+    L.clatz = box->lat[5];
+    minimage_centres_kernel<<<(box->nmol + 127) / 128, 128, 0, (cudaStream_t)stream>>>(L, box->nmol, box->xadd,
+                                                                                       box->yadd, box->zadd);
+    EPSR_CUDA(cudaGetLastError());
+    return epsr_box_positions(box, stream);
 }
 
 extern "C" int64_t epsr_molfit_shake_scratch_bytes(int32_t nmol, int32_t natom) {

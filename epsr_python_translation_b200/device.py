@@ -102,6 +102,10 @@ class DeviceBox:
         """Recompute the absolute positions after the offset/centre tensors were written."""
         check(self.lib.epsr_box_positions(C.byref(self.cbox), _stream()))
 
+    def minimage_centres(self):
+        """The molecule centres put back in the box (runepsr17 after an intramolecular cycle)."""
+        check(self.lib.epsr_minimage_centres(C.byref(self.cbox), _stream()))
+
     def download_coords(self, stream_only=False):
         """Host copies of the coordinates.  stream_only: the box's work was all launched on the
         current stream, so only that stream is waited for (other boxes on other streams keep

@@ -68,6 +68,16 @@ class EpsrIteration:
         self.ep = wl.ep
         if self.ep is not None:
             self._ep_setup()
+        # flexible molecules: intramolecular cycles every wl.intra molfit cycles (molfit.py:124)
+        self.intra_model = None
+        self.nisum_mc = 1
+        if wl.intra > 0:
+            from . import configs
+            from .intra import IntraModel
+            self.intra_model = IntraModel(self.d, **configs.intra_model(wl.system))
+            self.faddbs = torch.zeros(1, dtype=torch.float32, device=dev)
+            self._eintra_work = torch.zeros(b.nmol, dtype=torch.float32, device=dev)
+            self._nmovei = torch.zeros(2 * b.nmoltype, dtype=torch.int32, device=dev)
         self.events = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                        for k in STAGES}
         self.moves_per_step = wl.ntimes * b.nmol
@@ -129,11 +139,20 @@ class EpsrIteration:
         d.cell_list(wl.nmolcell, b.sepmax)
         self._mark("cells", True)
         self._mark("fmolec1")
-        self.ftest = d.fmolec1(wl.eintra, strict=self.strict)
+        eintra = wl.eintra if self.intra_model is None else self.intra_model.en_mole_intra(self._eintra_work)
+        self.ftest = d.fmolec1(eintra, strict=self.strict)
         self._mark("fmolec1", True)
         self._mark("molfit")
         for _ in range(wl.ntimes):
-            d.molfit(strict=self.strict)
+            if self.intra_model is not None and self.nisum_mc >= wl.intra:
+                # molfit's intramolecular branch, then runepsr17's minimage and store rebuild
+                self._nmovei.copy_(self.intra_model.molfit_shake(wl.stepmi, self.faddbs))
+                self.nisum_mc = 1
+                d.minimage_centres()
+                self.ftest = d.fmolec1(self.intra_model.en_mole_intra(self._eintra_work), strict=self.strict)
+            else:
+                d.molfit(strict=self.strict)
+                self.nisum_mc += 1
         self._mark("molfit", True)
         self._mark("atogen")
         d.atogen(wl.ngrsamples, self.ran1, self.rminex, ycoh=self.ycoh)
@@ -243,6 +262,10 @@ class EpsrIteration:
             it.pfact, it.absolute_energy, it.erequnit = ep.potfac, ep.absolute_energy, ep.erequnit
             it.ereqstep, it.potfacamp = ep.ereqstep, ep.potfacamp
             it.tab = P(d.tab)
+        if self.intra_model is not None:
+            it.intra, it.stepmi = wl.intra, float(f32(wl.stepmi))
+            it.intra_model = C.cast(C.pointer(self.intra_model.c), C.c_void_p)
+            it.faddbs, it.eintra_work, it.nmovei = P(self.faddbs), P(self._eintra_work), P(self._nmovei)
         it.strict = 1 if self.strict else 0
         for k, name in enumerate(STAGES):       # the Python step has created these events
             it.stage_events[2 * k] = self.events[name][0].cuda_event
@@ -257,10 +280,13 @@ class EpsrIteration:
         wl, b = self.wl, self.box
         self._n_scal[:, 0] = self.stepp
         self._plan.nsum = self.nsum + 1
+        self._plan.nisum = self.nisum_mc
         _lib.check(self.d.lib.epsr_iteration_step(C.byref(self._plan), C.byref(self._rep),
                                                   C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         r = self._rep
         self.d.nnbrefmax = int(r.nnbrefmax)
+        if self.intra_model is not None:
+            self.nisum_mc = int(r.nisum)
         if self.d.store is not None:        # the store struct other calls take follows the driver's layout
             self.d.store.nnbrefmax = int(r.nnbrefmax)
         self.ftest = (np.float32(r.ftest[0]), np.float32(r.ftest[1]))

@@ -195,6 +195,11 @@ typedef struct {
     float refine_intra_fac;
 } epsr_intra_t;
 
+/* The molecule centres put back in the box (minimagec minimagec.py:13-62 of xadd, yadd, zadd),
+ * as runepsr17 does after an intramolecular cycle (epsr_standalone_rev3.py:1332-1335), and the
+ * atom positions refreshed.  Asynchronous. */
+int epsr_minimage_centres(const epsr_box_t *box, void *stream);
+
 /* en_mole_intra molfit.py:1327-1350 of every molecule at its current coordinates: out [nmol]
  * device (the intramolecular energies fmolec1 stores first).  Bit-identical.  Asynchronous. */
 int epsr_en_mole_intra(const epsr_box_t *box, const epsr_intra_t *intra, float *out, void *stream);
@@ -489,6 +494,18 @@ typedef struct {
     float *ep_pwtold, *potfac, *ep_result;    /* [nterms+1], [1], [2] = {energabs, pressfac} */
     float pfact, absolute_energy, erequnit, ereqstep, potfacamp;
     float *tab;                       /* box->tab, written */
+    /* intramolecular cycles, when intra > 0: molfit's branch when nisum >= intra (molfit.py:
+     * 124-174, epsr_molfit_shake) in place of a whole-molecule cycle, nisum kept as the
+     * reference's counter (nisum in, rep->nisum out), and after each intramolecular cycle the
+     * molecule centres put back in the box and the pair store rebuilt (runepsr17 :1328-1345).
+     * With intra > 0 the stored intramolecular energies are intra_model's (epsr_en_mole_intra
+     * into eintra_work) instead of eintra. */
+    int32_t intra, nisum;
+    float stepmi;
+    const epsr_intra_t *intra_model;
+    float *faddbs;                    /* [1] device */
+    float *eintra_work;               /* [nmol] device */
+    int32_t *nmovei;                  /* [2*nmoltype] device: the last intramolecular cycle's counts */
     /* one scratch block shared by the stages (epsr_iteration_scratch_bytes) */
     void *scratch;
     int64_t scratch_bytes;
@@ -504,6 +521,7 @@ typedef struct {
     int32_t ngrsamples;               /* atogen's sampled origins */
     int64_t pair_updates;             /* atogen's pair-updates */
     double press[2];                  /* press sums: float32 energy sum, double virial sum */
+    int32_t nisum;                    /* molfit's counter after the cycles (intra > 0) */
 } epsr_iteration_report_t;
 
 int64_t epsr_iteration_scratch_bytes(const epsr_iteration_t *it);
