@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--strict", action="store_true", help="bit-identical sequential sums")
     ap.add_argument("--cpu-sample-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--intra", type=int, default=0,
+                    help="flexible molecules: an intramolecular molfit cycle every INTRA cycles (0: rigid)")
     ap.add_argument("--python-driver", action="store_true",
                     help="drive each iteration's routines from Python instead of epsr_iteration_step")
     return ap.parse_args()
@@ -60,10 +62,10 @@ def parse():
 
 # ----------------------------------------------------------------------------- CPU side
 def _cpu_worker(args):
-    config, seed, steps, warmup = args
+    config, seed, steps, warmup, intra = args
     from epsr_python_translation_b200 import configs
     from oracle.workload import CpuIteration
-    wl = configs.make_workload(config)
+    wl = configs.make_workload(config, intra=intra)
     it = CpuIteration(wl, ran1_seed=seed)
     for _ in range(warmup):
         it.step()
@@ -88,10 +90,10 @@ def cpu_info():
     return model, os.cpu_count() or 1
 
 
-def cpu_baseline(config, steps):
+def cpu_baseline(config, steps, intra=0):
     """Single core: the oracle (C restatement of the reference) on a bounded sample of the
     same workload."""
-    wall, per, stages, pairs, moves = _cpu_worker((config, -7, steps, 1))
+    wall, per, stages, pairs, moves = _cpu_worker((config, -7, steps, 1, intra))
     model, n = cpu_info()
     ms = 1000.0 * statistics.mean(per)
     return {"value": moves / statistics.mean(per), "unit": UNIT, "cores": 1, "kind": "port",
@@ -113,7 +115,7 @@ def reference_arm(a):
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(nproc) as pool:
-        res = pool.map(_cpu_worker, [(a.config, -(11 + i), steps, warmup) for i in range(nproc)])
+        res = pool.map(_cpu_worker, [(a.config, -(11 + i), steps, warmup, a.intra) for i in range(nproc)])
     wall = time.perf_counter() - t0
     moves = res[0][4]
     slowest = max(r[0] for r in res)
@@ -213,7 +215,7 @@ def gpu_arm(a):
     from epsr_python_translation_b200 import configs
     from epsr_python_translation_b200.iteration import STAGES, EpsrIteration
 
-    wl = configs.make_workload(a.config)
+    wl = configs.make_workload(a.config, intra=a.intra)
     R = max(1, a.replicas)
     # independent boxes (own ran1 seeds), each driven by its own host thread on its own stream
     streams = [torch.cuda.Stream() for _ in range(R)]
@@ -369,6 +371,8 @@ def gpu_arm(a):
             "ms_per_step": tmax_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": f"synthetic (seeded {a.config} boxes, synthetic data sets)",
             "config": {"workload": a.config, "nmol": it.box.nmol, "natom": it.box.natom, "npairs": it.box.npairs,
+                       "molecules": "flexible: every %d-th molfit cycle intramolecular" % a.intra if a.intra > 0
+                       else "rigid (whole-molecule moves only)",
                        "moves_per_step_per_box": moves, "boxes_per_gpu": R,
                        "pair_updates_per_step_per_box": it.pair_updates,
                        "stages": f"cells+fmolec1+{wl.ntimes} molfit+atogen+gensq+ptgnsq differences+press+"
@@ -395,7 +399,7 @@ def gpu_arm(a):
             "clocks": clk,
         }
         if not a.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(a.config, a.cpu_sample_steps)
+            line["cpu_baseline"] = cpu_baseline(a.config, a.cpu_sample_steps, a.intra)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

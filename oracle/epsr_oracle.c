@@ -1035,6 +1035,11 @@ static float en_atom_intra(const oracle_sys *S, const oracle_intra *I, int ia, i
     return sume;
 }
 
+/* runepsr17 epsr_standalone_rev3.py:1332-1335: every molecule centre put back in the box */
+void oracle_minimage_centres(oracle_sys *S) {
+    for (int im = 0; im < S->nmol; ++im) minimagec(S, &S->xadd[im], &S->yadd[im], &S->zadd[im]);
+}
+
 /* en_mole_intra molfit.py:1327-1350 */
 float oracle_en_mole_intra(const oracle_sys *S, const oracle_intra *I, int im) {
     const int a0 = S->naf[im], n = S->nato[im];

@@ -315,6 +315,12 @@ class IntraHandle:
         self.c = c
 
 
+def minimage_centres(box):
+    """runepsr17 epsr_standalone_rev3.py:1332-1335 (minimagec of every centre), in place."""
+    h = SysHandle(box)
+    lib().oracle_minimage_centres(C.byref(h.c))
+
+
 def en_mole_intra_all(box, m):
     """en_mole_intra molfit.py:1327-1350 of every molecule (C restatement)."""
     h, ih = SysHandle(box), IntraHandle(box, m)

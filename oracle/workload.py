@@ -33,6 +33,7 @@ class CpuIteration:
         self.rows = np.ascontiguousarray(wl.foqols.T)   # (nq+1, npt1+1)
         self.stage_s = {}
         self.pair_updates = 0
+        self.nisum_mc, self.fadds, self.faddbs, self.ergold1 = 1, f32(0.0), f32(0.0), f32(0.0)
         ep = wl.ep
         if ep is not None:
             b = self.box
@@ -49,11 +50,24 @@ class CpuIteration:
         cells = oracle.cell_list(b, wl.nmolcell, b.sepmax)
         t["cells"] = time.perf_counter() - t0
         t0 = time.perf_counter()
-        st = oracle.fmolec1(b, cells, wl.eintra)
+        model = None
+        if wl.intra > 0:
+            from epsr_python_translation_b200 import configs
+            model = configs.intra_model(wl.system)
+        st = oracle.fmolec1(b, cells, wl.eintra if model is None else oracle.en_mole_intra_all(b, model))
         t["fmolec1"] = time.perf_counter() - t0
         t0 = time.perf_counter()
         for _ in range(wl.ntimes):
-            _, _, self.ran1 = oracle.molfit(b, cells, st, self.mc, self.ran1, record_cos=False)
+            if model is not None and self.nisum_mc >= wl.intra:
+                # molfit's intramolecular branch, then runepsr17's minimage and store rebuild
+                self.fadds, self.faddbs, _, self.ergold1, self.ran1 = oracle.molfit_shake(
+                    b, st, self.mc, model, wl.stepmi, self.ran1, self.fadds, self.faddbs, self.ergold1)
+                self.nisum_mc = 1
+                oracle.minimage_centres(b)
+                st = oracle.fmolec1(b, cells, oracle.en_mole_intra_all(b, model))
+            else:
+                _, _, self.ran1 = oracle.molfit(b, cells, st, self.mc, self.ran1, record_cos=False)
+                self.nisum_mc += 1
         t["molfit"] = time.perf_counter() - t0
         if stages == "mc":
             self.stage_s = t
