@@ -414,6 +414,25 @@ def silica(seed=1, natom=300, rho_atoms=0.0662, temperature=1500.0):
                         temperature=temperature, seed=seed, min_heavy=1.4)
 
 
+def c4_batch(seed=1, nbox=64, amin=300, amax=30000):
+    """Configuration C4: ``nbox`` independent boxes whose atom counts are log-uniform in
+    [amin, amax] (seeded), alternately rigid water (0.1 atoms/A^3) and SiO2-like single-atom
+    boxes (0.0662 atoms/A^3), temperatures uniform in 298-1500 K."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(amin), math.log(amax), nbox))
+    temps = rng.uniform(298.0, 1500.0, nbox)
+    out = []
+    for b in range(nbox):
+        if b % 2 == 0:
+            nmol = max(4, int(round(sizes[b] / 3.0)))
+            L = (3 * nmol / 0.1) ** (1.0 / 3.0)
+            out.append(build_system("c4_water", [water_template()], [nmol], L, temperature=float(temps[b]),
+                                    seed=seed * 1000 + b))
+        else:
+            out.append(silica(seed=seed * 1000 + b, natom=max(12, int(round(sizes[b]))), temperature=float(temps[b])))
+    return out
+
+
 # ----------------------------------------------------------------------------- transforms
 def qgrid(nq, qstep):
     """Q grid of ``inita`` (epsr_standalone_rev3.py:3025-3026): q[i] = qstep*(i-1), 1-based."""
