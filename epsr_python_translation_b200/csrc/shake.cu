@@ -301,12 +301,22 @@ __device__ __forceinline__ float metropolis_etest(float enew, float eold, float 
     return 0.0f;
 }
 
-// The ordered pass (:119-170 per molecule) and the step adaptation (:465-536).
+// The same, out of line: the ordered pass calls it only when a chained energy changed the
+// comparison, so the exponential stays off its path.
+__device__ __noinline__ float metropolis_etest_call(float enew, float eold, float temp) {
+    return metropolis_etest(enew, eold, temp);
+}
+
+// The ordered pass (:119-170 per molecule) and the step adaptation (:465-536).  Per tile of
+// molecules: every thread loads one molecule's inputs and forms its Metropolis value against
+// its own first stored energy; one thread walks the tile in order carrying ergold(1) and faddb
+// in registers and writing only the decisions; the threads then count tries and rejections
+// per type.
 __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
     __shared__ float s_enew[SH_TILE], s_r[SH_TILE], s_v1[SH_TILE], s_et[SH_TILE];
     __shared__ int s_nn[SH_TILE], s_prev[SH_TILE], s_mt[SH_TILE];
     __shared__ int s_slot[SH_TILE];
-    __shared__ unsigned char s_mv[SH_TILE];
+    __shared__ unsigned char s_mv[SH_TILE], s_acc[SH_TILE];
     __shared__ int cnt[2 * 64];
     __shared__ float s_faddb, s_ergold1;
     const int tid = threadIdx.x;
@@ -350,36 +360,43 @@ __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
         if (tid == 0) {
             float faddb = s_faddb, ergold1 = s_ergold1;
             for (int k = 0; k < nt; ++k) {
-                const int m = base + k;
-                if (s_nn[k] >= 1) {
+                const int nn = s_nn[k];
+                if (nn >= 1) {
                     const int p = s_prev[k];
-                    ergold1 = (p >= 0 && D.acc[p]) ? D.enew[p] : s_v1[k];   // make_neighbour_list_from_mols
+                    ergold1 = s_v1[k];                                   // make_neighbour_list_from_mols
+                    if (p >= 0 && (p >= base ? s_acc[p - base] : D.acc[p])) ergold1 = D.enew[p];
                 }
                 int a = 0;
                 if (s_mv[k]) {
-                    const int mt = s_mt[k];
-                    const float fdiffb = __fsub_rn(s_enew[k], ergold1);
+                    const float en = s_enew[k];
+                    const float fdiffb = __fsub_rn(en, ergold1);
                     // the test value was formed in parallel against the molecule's own first stored
                     // energy; it is formed again only when the chain changed that energy
-                    const float etest = (s_nn[k] >= 1 && __float_as_uint(ergold1) == __float_as_uint(s_v1[k]))
-                                            ? s_et[k] : metropolis_etest(s_enew[k], ergold1, temp);
+                    float etest;
+                    if (nn >= 1 && __float_as_uint(ergold1) == __float_as_uint(s_v1[k])) etest = s_et[k];
+                    else etest = metropolis_etest_call(en, ergold1, temp);
                     a = s_r[k] < etest;
-                    if (mt < 64) {
-                        ++cnt[mt];
-                        if (!a) ++cnt[64 + mt];
-                    }
                     if (a) {
                         faddb = __fadd_rn(faddb, fdiffb);
-                        if (s_nn[k] >= 1) {          // save_energies + save_erg_pairs
-                            ergold1 = s_enew[k];
-                            D.ergpair[s_slot[k] - 1] = ergold1;
+                        if (nn >= 1) {                                   // save_energies + save_erg_pairs
+                            ergold1 = en;
+                            D.ergpair[s_slot[k] - 1] = en;
                         }
                     }
                 }
-                D.acc[m] = a;
+                s_acc[k] = (unsigned char)a;
             }
             s_faddb = faddb;
             s_ergold1 = ergold1;
+        }
+        __syncthreads();
+        for (int k = tid; k < nt; k += blockDim.x) {
+            const int a = s_acc[k];
+            D.acc[base + k] = a;
+            if (s_mv[k] && s_mt[k] < 64) {
+                atomicAdd(&cnt[s_mt[k]], 1);
+                if (!a) atomicAdd(&cnt[64 + s_mt[k]], 1);
+            }
         }
         __syncthreads();
     }
