@@ -3,7 +3,9 @@
  *
  * Every entry point takes device pointers and sizes, a CUDA stream (as void*, NULL = the
  * legacy default stream) and returns an int status: 0 on success, >0 on an error (text via
- * epsr_last_error()).  No C++ or framework types cross this boundary.  Calls are
+ * epsr_last_error()).  Host pointers appear only where an argument's name ends in _host and
+ * in the host-side table builders (epsr_calc_pwrexpr_grad, epsr_calc_gaussr_grad,
+ * epsr_generate_rp), which take no stream.  No C++ or framework types cross this boundary.  Calls are
  * asynchronous on the given stream unless stated otherwise; the reference's routines are
  * synchronous, so the host bindings synchronise before returning to the reference loop.
  *
