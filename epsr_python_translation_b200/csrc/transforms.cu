@@ -87,18 +87,48 @@ __global__ void stog_kernel(float rho, const float *q, int ldq, const float *sof
 // over atom pairs of weight x intermolecular S(Q), sequential over pairs as the reference --
 // the weights are real*8, so each step is sum = real(dble(sum) + cwt * dble(qwind)), one
 // rounding to float32 per pair -- and its difference from the data, negated:
-// out = -(data - sum).  Thread per (set, Q).
+// out = -qtemp with the reference's Q window (:3856-3867): below max(qmin, q(nqmin)) the data
+// are replaced by 0 or, when szeros is set, by the straight line from szeros at Q = q(1) to the
+// data at nqmin; between nqmin and nqmax qtemp = data - sum; above nqmax 0.  Without window
+// arrays (NULL) nqmin = 1, nqmax = nq, szeros = 0 and qmin = 0.  Thread per (set, Q).
 __global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *data, const double *cwt,
-                                   const float *qwind, float *out) {
+                                   const float *qwind, const float *q, const int32_t *nqmin, const int32_t *nqmax,
+                                   const float *szeros, float qmin, float *out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int d = blockIdx.y;
     if (i > nq) return;
     const double *w = cwt + (size_t)d * npairs;
+    const float *dd = data + (size_t)d * (nq + 1);
     float sum = 0.0f;
     for (int ic = 0; ic < npairs; ++ic)
         sum = __double2float_rn(__dadd_rn((double)sum, __dmul_rn(__ldg(w + ic),
                                                                  (double)__ldg(qwind + (size_t)ic * (nq + 1) + i))));
-    out[(size_t)d * (nq + 1) + i] = -__fsub_rn(data[(size_t)d * (nq + 1) + i], sum);
+    float qtemp;
+    if (!q) {
+        qtemp = __fsub_rn(dd[i], sum);
+    } else {
+        const int nqmn = nqmin ? nqmin[d] : 1, nqmx = nqmax ? nqmax[d] : nq;
+        const float sz = szeros ? szeros[d] : 0.0f;
+        const float qn = q[nqmn];
+        const float qthr = qn > qmin ? qn : qmin;          // max(qminptemp, q(nqmn))
+        if (q[i] < qthr) {
+            if (sz != 0.0f) {
+                float grads0 = 0.0f, conss0 = 0.0f;
+                if (nqmn > 1) {
+                    grads0 = __fdiv_rn(__fsub_rn(dd[nqmn], sz), __fsub_rn(qn, q[1]));
+                    conss0 = sz;
+                }
+                qtemp = __fsub_rn(__fadd_rn(conss0, __fmul_rn(grads0, __fsub_rn(q[i], q[1]))), sum);
+            } else {
+                qtemp = 0.0f;
+            }
+        } else if (i >= nqmn && i <= nqmx) {
+            qtemp = __fsub_rn(dd[i], sum);
+        } else {
+            qtemp = 0.0f;
+        }
+    }
+    out[(size_t)d * (nq + 1) + i] = -qtemp;
 }
 
 }  // namespace epsr
@@ -106,13 +136,14 @@ __global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *d
 using namespace epsr;
 
 extern "C" int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const double *cwt,
-                                      const float *qwind, float *out, void *stream) {
+                                      const float *qwind, const float *q, const int32_t *nqmin, const int32_t *nqmax,
+                                      const float *szeros, float qmin, float *out, void *stream) {
     if (ndata <= 0 || npairs <= 0 || nq <= 0 || !data || !cwt || !qwind || !out) {
         epsr_set_error("epsr_ptgnsq_difference: bad arguments");
         return EPSR_ERR_ARG;
     }
-    ptgnsq_diff_kernel<<<dim3((nq + 1 + 127) / 128, ndata), 128, 0, (cudaStream_t)stream>>>(ndata, npairs, nq, data,
-                                                                                           cwt, qwind, out);
+    ptgnsq_diff_kernel<<<dim3((nq + 1 + 127) / 128, ndata), 128, 0, (cudaStream_t)stream>>>(
+        ndata, npairs, nq, data, cwt, qwind, q, nqmin, nqmax, szeros, qmin, out);
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
 }

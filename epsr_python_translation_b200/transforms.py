@@ -40,12 +40,14 @@ def gensq(nq, npt1, wav, ldw, foqols, sj, si, ycoh, n2extr, natomsphere, npairs)
     return out
 
 
-def ptgnsq_difference(data, cwt, qwind, out=None):
+def ptgnsq_difference(data, cwt, qwind, out=None, q=None, nqmin=None, nqmax=None, szeros=None, qmin=0.0):
     """The simulated fit of each data set and its negated difference from the data
     (ptgnsq epsr_standalone_rev3.py:3844-3867): -(data - cwt @ qwind), the sum over atom
     pairs sequential, each step in double and rounded to float32 (the weights are real*8).
     data (ndata, nq+1) float32, cwt (ndata, npairs) float64, qwind (npairs, nq+1) float32,
-    all on the device."""
+    all on the device.  With q ((nq+1,), 1-based) the reference's Q window applies: per data
+    set nqmin, nqmax, szeros (host or device; None: 1, nq, 0) and qmin (qminp, or qminm when
+    qminp <= 0)."""
     if cwt.dtype != torch.float64:
         raise ValueError("ptgnsq_difference: cwt is real*8 in the reference; pass a float64 tensor")
     lib = _lib.load(require_device=True)
@@ -53,7 +55,13 @@ def ptgnsq_difference(data, cwt, qwind, out=None):
     npairs = cwt.shape[1]
     if out is None:
         out = torch.empty_like(data)
-    check(lib.epsr_ptgnsq_difference(ndata, npairs, ld - 1, _p(data), _p(cwt), _p(qwind), _p(out), _s()))
+    win = []
+    if q is not None:
+        win = [_dev(q), None if nqmin is None else _dev(nqmin, torch.int32),
+               None if nqmax is None else _dev(nqmax, torch.int32), None if szeros is None else _dev(szeros)]
+    qp, n0, n1, sz = (win + [None] * 4)[:4]
+    check(lib.epsr_ptgnsq_difference(ndata, npairs, ld - 1, _p(data), _p(cwt), _p(qwind), _p(qp), _p(n0), _p(n1), _p(sz),
+                                     f32(qmin), _p(out), _s()))
     return out
 
 

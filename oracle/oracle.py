@@ -375,12 +375,13 @@ def atogen(box, ngrsamples, ran1, rminex, ycoh=None, sizefactor=1.0):
 
 
 # ----------------------------------------------------------------------------- transforms
-def ptgnsq_difference(data, cwt, qwind):
+def ptgnsq_difference(data, cwt, qwind, q=None, nqmin=None, nqmax=None, szeros=None, qmin=0.0):
     """ptgnsq epsr_standalone_rev3.py:3844-3867: the simulated fit of data set d at Q index i
     is the sum over atom pairs ic, in order, of cwt[d, ic] * qwind[ic, i] (:3853-3854); the
     weights are real*8 (weights.py:23), so each step is sum = real(dble(sum) + cwt *
     dble(qwind)): product and sum in double, one rounding to float32.  Returned negated as
-    the difference from the data, -(data - sum)."""
+    the difference from the data, -qtemp, with the Q window of :3856-3867 when q is given
+    (per data set nqmin, nqmax, szeros; qmin the reference's qminptemp)."""
     data = np.asarray(data, np.float32)
     cwt = np.asarray(cwt, np.float64)
     qwind = np.asarray(qwind, np.float32)
@@ -389,7 +390,28 @@ def ptgnsq_difference(data, cwt, qwind):
         s = np.zeros(qwind.shape[1], np.float32)
         for ic in range(qwind.shape[0]):
             s = (s.astype(np.float64) + cwt[d, ic] * qwind[ic].astype(np.float64)).astype(np.float32)
-        out[d] = -(data[d] - s)
+        if q is None:
+            out[d] = -(data[d] - s)
+            continue
+        f = np.float32
+        nq = data.shape[1] - 1
+        nqmn = 1 if nqmin is None else int(nqmin[d])
+        nqmx = nq if nqmax is None else int(nqmax[d])
+        sz = f(0.0) if szeros is None else f(szeros[d])
+        qq = np.asarray(q, f)
+        grads0 = conss0 = f(0.0)
+        if sz != 0.0 and nqmn > 1:
+            grads0 = f(f(data[d, nqmn] - sz) / f(qq[nqmn] - qq[1]))
+            conss0 = sz
+        qthr = qq[nqmn] if qq[nqmn] > f(qmin) else f(qmin)
+        for i in range(nq + 1):
+            if qq[i] < qthr:
+                qt = f(f(conss0 + f(grads0 * f(qq[i] - qq[1]))) - s[i]) if sz != 0.0 else f(0.0)
+            elif nqmn <= i <= nqmx:
+                qt = f(data[d, i] - s[i])
+            else:
+                qt = f(0.0)
+            out[d, i] = -qt
     return out
 
 

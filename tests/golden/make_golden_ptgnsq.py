@@ -14,7 +14,9 @@ pairs in two coefficient sets (pairs 1 and 3 share set 1), real*8 weights cwt an
 are not float32 values, seeded previous fit coefficients pcoefd, EP coefficients pcoefp and
 tables.  tests/golden/ptgnsq.npz receives the inputs, the Q basis expsq the reference built,
 the ran1 state before and after, and the refined state: pcoefd, pstepd, potnoi, pcoefp,
-pwtold and the four EP tables.
+pwtold and the four EP tables.  tests/golden/ptgnsq_window.npz repeats it with the Q window
+of :3856-3867 in use (qminp 1 A^-1, nqmin 6 and 4, the first data set extrapolated to
+szeros = -0.3 below its window).
 """
 
 from __future__ import annotations
@@ -37,7 +39,7 @@ f32 = np.float32
 REF = "/root/reference"
 
 
-def run(ep, out, nq=100, nterms=30, nits=200, seed=21):
+def run(ep, out, nq=100, nterms=30, nits=200, seed=21, qminp=0.0, nqmin=(1, 1), szeros=(0.0, 0.0)):
     from epsr26.common import clustercom, epsr16, epsrinput_par, molecom, potential_par as pp, weights
     from epsr26.fortran import r4
     from epsr26.fortran.arrays import real_array
@@ -91,13 +93,13 @@ def run(ep, out, nq=100, nterms=30, nits=200, seed=21):
     # data sets, weights and the previous fits
     q = configs.qgrid(nq, 0.3)
     epsr16.nfile = nfile
-    epsr16.qminp, epsr16.qminm = f32(0.0), f32(0.0)
+    epsr16.qminp, epsr16.qminm = f32(qminp), f32(0.0)
     cwt = rng.uniform(0.1, 0.6, (nfile, npairs))
     cwtpot = rng.uniform(0.1, 0.6, (npairs, nfile))
     pcoefd = np.zeros((nterms + 1, nfile), f32)
     pstepd = np.array([0.01, 0.02], f32)
     for d in range(1, nfile + 1):
-        epsr16.nqmin[d], epsr16.nqmax[d] = 1, nq
+        epsr16.nqmin[d], epsr16.nqmax[d] = int(nqmin[d - 1]), nq
         epsr16.sigma2[d] = pp.psigma2
         weights.xfile[d] = 0
         pp.npcoeff[d] = nterms
@@ -131,14 +133,16 @@ def run(ep, out, nq=100, nterms=30, nits=200, seed=21):
         out["in_" + k] = v.T.copy()
     for k, v in refstate.ran1_state().items():
         out["ran1_before_" + k] = v
-    szeros = real_array(8)
+    szeros_a = real_array(8)
+    szeros_a[1: nfile + 1] = np.array(szeros, f32)
+    out["window"] = np.array([qminp, *nqmin, *szeros], f32)
     rminp = real_array(8)
     potnoi = real_array(8)
     cwd = os.getcwd()
     with tempfile.TemporaryDirectory(dir=HERE) as tmp:
         os.chdir(tmp)
         try:
-            ep.ptgnsq(1, nq, qa, real_array(2, 8, 8), data, qwind, f32(9.0), f32(12.0), szeros, real_array(8),
+            ep.ptgnsq(1, nq, qa, real_array(2, 8, 8), data, qwind, f32(9.0), f32(12.0), szeros_a, real_array(8),
                       real_array(8), rminp, potnoi, f32(0.1), f32(0.0), f32(0.0), 0)
         finally:
             os.chdir(cwd)
@@ -158,9 +162,13 @@ if __name__ == "__main__":
     common, _ = refstate.load_reference(os.path.join(REF, "src"))
     import importlib
     ep = importlib.import_module("epsr26.programs.epsr_standalone_rev3")
-    out = {}
-    common.reset()
-    run(ep, out)
-    path = os.path.join(HERE, "ptgnsq.npz")
-    np.savez_compressed(path, **out)
-    print("wrote", path, "mcall", int(out["ran1_after_mcall"]) - int(out["ran1_before_mcall"]))
+    for name, kw in (("ptgnsq", {}),
+                     # the Q window: data from Q index 6 (set 1) and 4 (set 2), Q below 1.0 A^-1 outside it,
+                     # set 1 extrapolated to szeros at Q = q(1)
+                     ("ptgnsq_window", dict(qminp=1.0, nqmin=(6, 4), szeros=(-0.3, 0.0)))):
+        out = {}
+        common.reset()
+        run(ep, out, **kw)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **out)
+        print("wrote", path, "mcall", int(out["ran1_after_mcall"]) - int(out["ran1_before_mcall"]))

@@ -9,7 +9,7 @@ import pytest
 import torch
 
 from tests.goldens import assert_bits_equal
-from tests.test_ptgnsq_oracle import TABS, check_refined, load
+from tests.test_ptgnsq_oracle import CASES, TABS, check_refined, load
 
 pytestmark = pytest.mark.gpu
 f32 = np.float32
@@ -19,11 +19,13 @@ def _dev(a, dtype=torch.float32):
     return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
 
 
-def test_ptgnsq_refinement_device_matches_reference():
+@pytest.mark.parametrize("name", CASES)
+def test_ptgnsq_refinement_device_matches_reference(name):
     from epsr_python_translation_b200 import potential, transforms
     from epsr_python_translation_b200.box import Ran1State
-    z, n = load()
-    dt = transforms.ptgnsq_difference(_dev(z["data"]), _dev(z["cwt"], torch.float64), _dev(z["qwind"]))
+    z, n = load(name)
+    dt = transforms.ptgnsq_difference(_dev(z["data"]), _dev(z["cwt"], torch.float64), _dev(z["qwind"]), q=z["q"],
+                                      nqmin=n["nqmin"], nqmax=n["nqmax"], szeros=n["szeros"], qmin=n["qmin"])
     expr = np.concatenate([np.zeros(1, f32), z["expsq"]])
     ran1 = _dev(Ran1State.from_golden(z, "ran1_before_").as_array(), torch.int32)
     res = transforms.fit_expansion_batch(dt, expr, z["pcoefd_in"], z["pstepd_in"], 1, n["nq"], 1, n["nterms"],

@@ -5,6 +5,7 @@ own ptgnsq run on seeded state (tests/golden/ptgnsq.npz, made by
 tests/golden/make_golden_ptgnsq.py), bit for bit, ran1 stream included."""
 
 import numpy as np
+import pytest
 
 from epsr_python_translation_b200.box import Ran1State
 from oracle import oracle
@@ -14,15 +15,22 @@ f32 = np.float32
 TABS = ("xavs", "xavs1", "xavtot", "xavtot1")
 
 
-def load():
-    z = np.load(GOLDEN + "/ptgnsq.npz")
+CASES = ["ptgnsq", "ptgnsq_window"]
+
+
+def load(name="ptgnsq"):
+    z = np.load(GOLDEN + f"/{name}.npz")
     npairs, nsets, nfile, nq, nterms, nits, npt, npt2 = (int(v) for v in z["dims"])
-    return z, dict(npairs=npairs, nsets=nsets, nfile=nfile, nq=nq, nterms=nterms, nits=nits, npt=npt, npt2=npt2)
+    w = z["window"]
+    return z, dict(npairs=npairs, nsets=nsets, nfile=nfile, nq=nq, nterms=nterms, nits=nits, npt=npt, npt2=npt2,
+                   qmin=f32(w[0]), nqmin=w[1: 1 + nfile].astype(np.int32), szeros=w[1 + nfile: 1 + 2 * nfile],
+                   nqmax=np.full(nfile, nq, np.int32))
 
 
 def refine_oracle(z, n):
     """The oracle's chain on the golden inputs; returns the refined state."""
-    dt = oracle.ptgnsq_difference(z["data"], z["cwt"], z["qwind"])
+    dt = oracle.ptgnsq_difference(z["data"], z["cwt"], z["qwind"], z["q"], n["nqmin"], n["nqmax"], n["szeros"],
+                                  n["qmin"])
     expr = np.concatenate([np.zeros(1, f32), z["expsq"]])
     ran1 = Ran1State.from_golden(z, "ran1_before_")
     pcoefd = z["pcoefd_in"].copy()
@@ -58,8 +66,9 @@ def check_refined(got, z, n, who):
         assert_bits_equal(got["tabs"][k], z[k], f"{who} {k}")
 
 
-def test_ptgnsq_refinement_oracle_matches_reference():
-    z, n = load()
+@pytest.mark.parametrize("name", CASES)
+def test_ptgnsq_refinement_oracle_matches_reference(name):
+    z, n = load(name)
     got = refine_oracle(z, n)
     check_refined(got, z, n, "oracle")
     r = got["ran1"]
@@ -68,3 +77,6 @@ def test_ptgnsq_refinement_oracle_matches_reference():
     # the case exercises what it is for: shared sets, weights that are not float32 values
     assert len(set(z["iref"].tolist())) < n["npairs"]
     assert not np.array_equal(z["cwt"].astype(f32).astype(np.float64), z["cwt"])
+    if name == "ptgnsq_window":                         # the window rules are all in use
+        assert n["nqmin"].min() > 1 and (n["szeros"] != 0).any() and (n["szeros"] == 0).any()
+        assert (z["q"][1:] < n["qmin"]).any()
