@@ -127,7 +127,7 @@ _SIGS = {
     "epsr_press": (C.c_int, [C.POINTER(Box), C.POINTER(Store), I32, P, I64, I32, P, P]),
     "epsr_press_scratch_bytes": (I64, [I32, I32]),
     "epsr_gensq": (C.c_int, [I32, I32, I32, P, I32, P, I64, I64, P, P, P, P, P]),
-    "epsr_ptgnsq_difference": (C.c_int, [I32, I32, I32, P, P, P, P, P, P, P, F32, P, P]),
+    "epsr_ptgnsq_difference": (C.c_int, [I32, I32, I32, P, P, P, P, P, P, P, F32, P, P, P, P]),
     "epsr_sumgr": (C.c_int, [I32, I32, P, I32, P, C.c_double, C.c_double, P, P, P, P, P, P]),
     "epsr_sumsq": (C.c_int, [I32, I32, P, I32, C.c_double, C.c_double, P, P, P, P, P]),
     "epsr_generate_ep": (C.c_int, [I32, I32, I32, I32, P, P, I32, I32, P, F32, P, P, P, P, P, P, P, I32, P, F32, F32,

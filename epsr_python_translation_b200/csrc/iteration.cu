@@ -166,7 +166,7 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
     if (rc) return rc;
     const float *inter = it->sofq + (size_t)b->npairs * ldq;   // intermolecular S(Q) per pair
     rc = epsr_ptgnsq_difference(it->ndata, b->npairs, it->nq, it->data, it->cwt, inter, nullptr, nullptr, nullptr,
-                                nullptr, 0.0f, it->dt, stream);
+                                nullptr, 0.0f, nullptr, nullptr, it->dt, stream);
     if (rc) return rc;
     mark(it, 4, 1, s);
 

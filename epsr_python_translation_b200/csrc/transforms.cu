@@ -91,17 +91,22 @@ __global__ void stog_kernel(float rho, const float *q, int ldq, const float *sof
 // are replaced by 0 or, when szeros is set, by the straight line from szeros at Q = q(1) to the
 // data at nqmin; between nqmin and nqmax qtemp = data - sum; above nqmax 0.  Without window
 // arrays (NULL) nqmin = 1, nqmax = nq, szeros = 0 and qmin = 0.  Thread per (set, Q).
+// An X-ray data set (xray[d] != 0) weights each pair by its Q-dependent real*8 weight
+// wq[d][ic][i] (x_rayf0.weightx) instead of cwt[d][ic] (:3850-3852).
 __global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *data, const double *cwt,
                                    const float *qwind, const float *q, const int32_t *nqmin, const int32_t *nqmax,
-                                   const float *szeros, float qmin, float *out) {
+                                   const float *szeros, float qmin, const double *wq, const int32_t *xray,
+                                   float *out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int d = blockIdx.y;
     if (i > nq) return;
-    const double *w = cwt + (size_t)d * npairs;
+    const bool xr = wq && xray && xray[d] != 0;
+    const double *w = xr ? wq + (size_t)d * npairs * (nq + 1) + i : cwt + (size_t)d * npairs;
+    const size_t ws = xr ? (size_t)(nq + 1) : 1;
     const float *dd = data + (size_t)d * (nq + 1);
     float sum = 0.0f;
     for (int ic = 0; ic < npairs; ++ic)
-        sum = __double2float_rn(__dadd_rn((double)sum, __dmul_rn(__ldg(w + ic),
+        sum = __double2float_rn(__dadd_rn((double)sum, __dmul_rn(__ldg(w + ic * ws),
                                                                  (double)__ldg(qwind + (size_t)ic * (nq + 1) + i))));
     float qtemp;
     if (!q) {
@@ -137,13 +142,14 @@ using namespace epsr;
 
 extern "C" int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const double *cwt,
                                       const float *qwind, const float *q, const int32_t *nqmin, const int32_t *nqmax,
-                                      const float *szeros, float qmin, float *out, void *stream) {
+                                      const float *szeros, float qmin, const double *wq, const int32_t *xray,
+                                      float *out, void *stream) {
     if (ndata <= 0 || npairs <= 0 || nq <= 0 || !data || !cwt || !qwind || !out) {
         epsr_set_error("epsr_ptgnsq_difference: bad arguments");
         return EPSR_ERR_ARG;
     }
     ptgnsq_diff_kernel<<<dim3((nq + 1 + 127) / 128, ndata), 128, 0, (cudaStream_t)stream>>>(
-        ndata, npairs, nq, data, cwt, qwind, q, nqmin, nqmax, szeros, qmin, out);
+        ndata, npairs, nq, data, cwt, qwind, q, nqmin, nqmax, szeros, qmin, wq, xray, out);
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
 }

@@ -40,14 +40,16 @@ def gensq(nq, npt1, wav, ldw, foqols, sj, si, ycoh, n2extr, natomsphere, npairs)
     return out
 
 
-def ptgnsq_difference(data, cwt, qwind, out=None, q=None, nqmin=None, nqmax=None, szeros=None, qmin=0.0):
+def ptgnsq_difference(data, cwt, qwind, out=None, q=None, nqmin=None, nqmax=None, szeros=None, qmin=0.0, wq=None,
+                      xray=None):
     """The simulated fit of each data set and its negated difference from the data
     (ptgnsq epsr_standalone_rev3.py:3844-3867): -(data - cwt @ qwind), the sum over atom
     pairs sequential, each step in double and rounded to float32 (the weights are real*8).
     data (ndata, nq+1) float32, cwt (ndata, npairs) float64, qwind (npairs, nq+1) float32,
     all on the device.  With q ((nq+1,), 1-based) the reference's Q window applies: per data
     set nqmin, nqmax, szeros (host or device; None: 1, nq, 0) and qmin (qminp, or qminm when
-    qminp <= 0)."""
+    qminp <= 0).  X-ray data sets: xray (ndata,) flags and wq (ndata, npairs, nq+1) float64
+    Q-dependent weights used in place of cwt where the flag is set."""
     if cwt.dtype != torch.float64:
         raise ValueError("ptgnsq_difference: cwt is real*8 in the reference; pass a float64 tensor")
     lib = _lib.load(require_device=True)
@@ -60,8 +62,12 @@ def ptgnsq_difference(data, cwt, qwind, out=None, q=None, nqmin=None, nqmax=None
         win = [_dev(q), None if nqmin is None else _dev(nqmin, torch.int32),
                None if nqmax is None else _dev(nqmax, torch.int32), None if szeros is None else _dev(szeros)]
     qp, n0, n1, sz = (win + [None] * 4)[:4]
+    wqd = None if wq is None else _dev(wq, torch.float64)
+    if wqd is not None and tuple(wqd.shape) != (ndata, npairs, ld):
+        raise ValueError(f"ptgnsq_difference: wq must be (ndata, npairs, nq+1) = {(ndata, npairs, ld)}")
+    xrd = None if xray is None else _dev(xray, torch.int32)
     check(lib.epsr_ptgnsq_difference(ndata, npairs, ld - 1, _p(data), _p(cwt), _p(qwind), _p(qp), _p(n0), _p(n1), _p(sz),
-                                     f32(qmin), _p(out), _s()))
+                                     f32(qmin), _p(wqd), _p(xrd), _p(out), _s()))
     return out
 
 

@@ -284,11 +284,14 @@ int epsr_gensq(int32_t nq, int32_t npairs, int32_t npt1, const float *wav, int32
  * [ndata][npairs] double; qwind: [npairs][nq+1] (the intermolecular S(Q) of gensq).  The Q
  * window of :3856-3867 when q [nq+1] (1-based) is given: per data set nqmin, nqmax [ndata]
  * and szeros [ndata] (each may be NULL: 1, nq, 0) and qmin (the reference's qminptemp: qminp,
- * or qminm when qminp <= 0); with q NULL, out = -(data - sum) at every point.  Device
- * pointers; asynchronous on `stream`.  Bit-identical. */
+ * or qminm when qminp <= 0); with q NULL, out = -(data - sum) at every point.  X-ray data
+ * sets (:3850-3852): where xray[d] != 0 the pair weights are wq[d][ic][i] (double,
+ * [ndata][npairs][nq+1], x_rayf0.weightx of the set's X-ray file) instead of cwt[d][ic]; wq
+ * and xray may be NULL.  Device pointers; asynchronous on `stream`.  Bit-identical. */
 int epsr_ptgnsq_difference(int32_t ndata, int32_t npairs, int32_t nq, const float *data, const double *cwt,
                            const float *qwind, const float *q, const int32_t *nqmin, const int32_t *nqmax,
-                           const float *szeros, float qmin, float *out, void *stream);
+                           const float *szeros, float qmin, const double *wq, const int32_t *xray, float *out,
+                           void *stream);
 
 /* stog ato_manipulation_rev4.py:4067-4121 (+ lorch :4113).  q [ldq] 1-based, sofq
  * [npairs*ldq] (sofq(i,in) at [in*ldq+i]), r [nr+1] 1-based, gofr out [npairs*(nr+1)],

@@ -375,7 +375,7 @@ def atogen(box, ngrsamples, ran1, rminex, ycoh=None, sizefactor=1.0):
 
 
 # ----------------------------------------------------------------------------- transforms
-def ptgnsq_difference(data, cwt, qwind, q=None, nqmin=None, nqmax=None, szeros=None, qmin=0.0):
+def ptgnsq_difference(data, cwt, qwind, q=None, nqmin=None, nqmax=None, szeros=None, qmin=0.0, wq=None, xray=None):
     """ptgnsq epsr_standalone_rev3.py:3844-3867: the simulated fit of data set d at Q index i
     is the sum over atom pairs ic, in order, of cwt[d, ic] * qwind[ic, i] (:3853-3854); the
     weights are real*8 (weights.py:23), so each step is sum = real(dble(sum) + cwt *
@@ -388,8 +388,10 @@ def ptgnsq_difference(data, cwt, qwind, q=None, nqmin=None, nqmax=None, szeros=N
     out = np.empty_like(data)
     for d in range(data.shape[0]):
         s = np.zeros(qwind.shape[1], np.float32)
+        xr = wq is not None and xray is not None and int(xray[d]) != 0   # x_rayf0.weightx (:3850-3852)
         for ic in range(qwind.shape[0]):
-            s = (s.astype(np.float64) + cwt[d, ic] * qwind[ic].astype(np.float64)).astype(np.float32)
+            w = np.asarray(wq[d, ic], np.float64) if xr else cwt[d, ic]
+            s = (s.astype(np.float64) + w * qwind[ic].astype(np.float64)).astype(np.float32)
         if q is None:
             out[d] = -(data[d] - s)
             continue

@@ -16,7 +16,9 @@ tables.  tests/golden/ptgnsq.npz receives the inputs, the Q basis expsq the refe
 the ran1 state before and after, and the refined state: pcoefd, pstepd, potnoi, pcoefp,
 pwtold and the four EP tables.  tests/golden/ptgnsq_window.npz repeats it with the Q window
 of :3856-3867 in use (qminp 1 A^-1, nqmin 6 and 4, the first data set extrapolated to
-szeros = -0.3 below its window).
+szeros = -0.3 below its window).  tests/golden/ptgnsq_xray.npz repeats the first with data set 1
+an X-ray set (weights.xfile 1): its pairs are weighted by seeded Q-dependent real*8 weights
+x_rayf0.weightx instead of cwt (:3849-3852); wq [set][pair][i] and the xray flags are saved.
 """
 
 from __future__ import annotations
@@ -39,8 +41,8 @@ f32 = np.float32
 REF = "/root/reference"
 
 
-def run(ep, out, nq=100, nterms=30, nits=200, seed=21, qminp=0.0, nqmin=(1, 1), szeros=(0.0, 0.0)):
-    from epsr26.common import clustercom, epsr16, epsrinput_par, molecom, potential_par as pp, weights
+def run(ep, out, nq=100, nterms=30, nits=200, seed=21, qminp=0.0, nqmin=(1, 1), szeros=(0.0, 0.0), xray=(0, 0)):
+    from epsr26.common import clustercom, epsr16, epsrinput_par, molecom, potential_par as pp, weights, x_rayf0
     from epsr26.fortran import r4
     from epsr26.fortran.arrays import real_array
     from epsr26.library import auxiliary_routines
@@ -101,7 +103,7 @@ def run(ep, out, nq=100, nterms=30, nits=200, seed=21, qminp=0.0, nqmin=(1, 1), 
     for d in range(1, nfile + 1):
         epsr16.nqmin[d], epsr16.nqmax[d] = int(nqmin[d - 1]), nq
         epsr16.sigma2[d] = pp.psigma2
-        weights.xfile[d] = 0
+        weights.xfile[d] = int(xray[d - 1])
         pp.npcoeff[d] = nterms
         pp.pstepd[d] = pstepd[d - 1]
         pcoefd[1:, d - 1] = (rng.standard_normal(nterms) * 0.01).astype(f32)
@@ -117,6 +119,14 @@ def run(ep, out, nq=100, nterms=30, nits=200, seed=21, qminp=0.0, nqmin=(1, 1), 
                               + rng.normal(0, 0.005, nq)).astype(f32)
     for ic in range(1, npairs + 1):
         qwind[1: nq + 1, ic] = (0.04 * np.cos(2.1 * qq[1:] + ic) * np.exp(-0.04 * qq[1:])).astype(f32)
+    wq = np.zeros((nfile, npairs, nq + 1))
+    for d in range(1, nfile + 1):
+        ix = int(xray[d - 1])
+        if ix > 0:
+            w = rng.uniform(0.05, 0.5, (npairs, nq)) * np.exp(-0.01 * qq[1:])
+            x_rayf0.weightx[1: nq + 1, 1: npairs + 1, ix] = w.T
+            wq[d - 1, :, 1:] = w
+    out["wq"], out["xray"] = wq, np.array(xray, np.int32)
     qa = real_array(nq + 8)
     qa[1: nq + 1] = q[1:]
     for _ in range(53):
@@ -165,7 +175,9 @@ if __name__ == "__main__":
     for name, kw in (("ptgnsq", {}),
                      # the Q window: data from Q index 6 (set 1) and 4 (set 2), Q below 1.0 A^-1 outside it,
                      # set 1 extrapolated to szeros at Q = q(1)
-                     ("ptgnsq_window", dict(qminp=1.0, nqmin=(6, 4), szeros=(-0.3, 0.0)))):
+                     ("ptgnsq_window", dict(qminp=1.0, nqmin=(6, 4), szeros=(-0.3, 0.0))),
+                     # data set 1 an X-ray set with Q-dependent pair weights
+                     ("ptgnsq_xray", dict(xray=(1, 0)))):
         out = {}
         common.reset()
         run(ep, out, **kw)

@@ -25,7 +25,8 @@ def test_ptgnsq_refinement_device_matches_reference(name):
     from epsr_python_translation_b200.box import Ran1State
     z, n = load(name)
     dt = transforms.ptgnsq_difference(_dev(z["data"]), _dev(z["cwt"], torch.float64), _dev(z["qwind"]), q=z["q"],
-                                      nqmin=n["nqmin"], nqmax=n["nqmax"], szeros=n["szeros"], qmin=n["qmin"])
+                                      nqmin=n["nqmin"], nqmax=n["nqmax"], szeros=n["szeros"], qmin=n["qmin"],
+                                      wq=_dev(z["wq"], torch.float64), xray=z["xray"])
     expr = np.concatenate([np.zeros(1, f32), z["expsq"]])
     ran1 = _dev(Ran1State.from_golden(z, "ran1_before_").as_array(), torch.int32)
     res = transforms.fit_expansion_batch(dt, expr, z["pcoefd_in"], z["pstepd_in"], 1, n["nq"], 1, n["nterms"],

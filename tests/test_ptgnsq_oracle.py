@@ -15,7 +15,7 @@ f32 = np.float32
 TABS = ("xavs", "xavs1", "xavtot", "xavtot1")
 
 
-CASES = ["ptgnsq", "ptgnsq_window"]
+CASES = ["ptgnsq", "ptgnsq_window", "ptgnsq_xray"]
 
 
 def load(name="ptgnsq"):
@@ -30,7 +30,7 @@ def load(name="ptgnsq"):
 def refine_oracle(z, n):
     """The oracle's chain on the golden inputs; returns the refined state."""
     dt = oracle.ptgnsq_difference(z["data"], z["cwt"], z["qwind"], z["q"], n["nqmin"], n["nqmax"], n["szeros"],
-                                  n["qmin"])
+                                  n["qmin"], z["wq"], z["xray"])
     expr = np.concatenate([np.zeros(1, f32), z["expsq"]])
     ran1 = Ran1State.from_golden(z, "ran1_before_")
     pcoefd = z["pcoefd_in"].copy()
@@ -80,3 +80,8 @@ def test_ptgnsq_refinement_oracle_matches_reference(name):
     if name == "ptgnsq_window":                         # the window rules are all in use
         assert n["nqmin"].min() > 1 and (n["szeros"] != 0).any() and (n["szeros"] == 0).any()
         assert (z["q"][1:] < n["qmin"]).any()
+    if name == "ptgnsq_xray":                           # one X-ray set, one weighted by cwt
+        assert z["xray"].tolist() == [1, 0] and (z["wq"][0, :, 1:] > 0).all()
+        plain = oracle.ptgnsq_difference(z["data"], z["cwt"], z["qwind"], z["q"], n["nqmin"], n["nqmax"], n["szeros"],
+                                         n["qmin"])
+        assert not np.array_equal(plain[0], got["dt"][0]) and np.array_equal(plain[1], got["dt"][1])
