@@ -696,21 +696,21 @@ extern "C" int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const f
                                         int64_t scratch_bytes, int32_t strict, int64_t *trials_host, void *stream) {
     if (nprob <= 0 || !yin || !expr || !yout || !wt || !wtold || !scal_host || !ran1 || !scratch || !trials_host ||
         npt <= 0 || nterms <= 0 || nmin < 1 || nmin > npt || ncfirst < 1 || ncfirst > nterms) {
-        epsr_set_error("epsr_fit_expansion: bad arguments");
+        epsr_set_error("epsr_fit_expansion_batch: bad arguments");
         return EPSR_ERR_ARG;
     }
     if (scratch_bytes < epsr_fit_expansion_batch_scratch_bytes(nprob, npt, nterms)) {
-        epsr_set_error("epsr_fit_expansion: scratch too small");
+        epsr_set_error("epsr_fit_expansion_batch: scratch too small");
         return EPSR_ERR_CAPACITY;
     }
     if (nterms - ncfirst + 1 > FX_SLOTS) {
-        epsr_set_error("epsr_fit_expansion: at most %d perturbed terms", FX_SLOTS);
+        epsr_set_error("epsr_fit_expansion_batch: at most %d perturbed terms", FX_SLOTS);
         return EPSR_ERR_UNSUPPORTED;
     }
     int rpc = 0;
     const int nw = fx_workers(npt, nterms, &rpc);
     if (!nw) {
-        epsr_set_error("epsr_fit_expansion: %d rows x %d terms exceed 8 CTAs of shared memory", npt, nterms);
+        epsr_set_error("epsr_fit_expansion_batch: %d rows x %d terms exceed 8 CTAs of shared memory", npt, nterms);
         return EPSR_ERR_UNSUPPORTED;
     }
     cudaStream_t s = (cudaStream_t)stream;

@@ -76,3 +76,33 @@ def test_device_path_refuses_without_gpu():
     with pytest.raises(_lib.EpsrGpuError):
         from epsr_python_translation_b200.device import DeviceBox
         DeviceBox(BoxArrays.from_golden(goldens.load("c1_water")))
+
+
+def _zero_args(argtypes):
+    vals = []
+    for a in argtypes:
+        if a in (C.c_float, C.c_double):
+            vals.append(a(0.0))
+        elif a in (C.c_int8, C.c_int16, C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_size_t):
+            vals.append(a(0))
+        else:
+            vals.append(None)
+    return vals
+
+
+def test_every_entry_point_rejects_null_and_zero_arguments():
+    """Each status-returning entry point, given null pointers and zero sizes, returns the
+    argument-error status with a message naming the entry -- checked before any CUDA call, so
+    no GPU is needed and nothing is dereferenced."""
+    from epsr_python_translation_b200 import _lib
+    L = _lib.load()
+    checked = 0
+    for name, (restype, argtypes) in _lib._SIGS.items():
+        if not argtypes or name.endswith("_scratch_bytes") or name == "epsr_last_error":
+            continue
+        rc = getattr(L, name)(*_zero_args(argtypes))
+        assert rc == 1, (name, rc)
+        msg = L.epsr_last_error().decode()
+        assert name in msg, (name, msg)
+        checked += 1
+    assert checked >= 25
