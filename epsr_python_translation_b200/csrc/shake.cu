@@ -308,15 +308,24 @@ __device__ __noinline__ float metropolis_etest_call(float enew, float eold, floa
 }
 
 // The ordered pass (:119-170 per molecule) and the step adaptation (:465-536).  Per tile of
-// molecules: every thread loads one molecule's inputs and forms its Metropolis value against
-// its own first stored energy; one thread walks the tile in order carrying ergold(1) and faddb
-// in registers and writing only the decisions; the threads then count tries and rejections
-// per type.
+// molecules: every thread loads one molecule's inputs and forms its Metropolis decisions against
+// its own first stored energy and, where an earlier molecule shares that stored slot, against
+// that molecule's trial energy (what the slot holds once that molecule is accepted); one thread
+// walks the tile in order carrying ergold(1) and faddb in registers, reading eight molecules'
+// inputs ahead of the chain and picking the decision by the earlier molecule's acceptance (only a
+// molecule with an empty list, compared against the carried energy, forms its own); the threads
+// then count tries and rejections per type.
+#define SHF_MV 1      // the molecule was moved (a trial)
+#define SHF_NN 2      // its stored list is not empty
+#define SHF_PREV 4    // an earlier molecule shares its first stored slot
+#define SHF_ACC 8     // the decision against its own first stored energy
+#define SHF_ACCP 16   // the decision against the trial energy of the earlier molecule sharing it
+#define SH_AHEAD 8
 __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
-    __shared__ float s_enew[SH_TILE], s_r[SH_TILE], s_v1[SH_TILE], s_et[SH_TILE];
-    __shared__ int s_nn[SH_TILE], s_prev[SH_TILE], s_mt[SH_TILE];
+    __shared__ float s_enew[SH_TILE], s_r[SH_TILE], s_v1[SH_TILE], s_enp[SH_TILE];
+    __shared__ int s_prev[SH_TILE], s_mt[SH_TILE];
     __shared__ int s_slot[SH_TILE];
-    __shared__ unsigned char s_mv[SH_TILE], s_acc[SH_TILE];
+    __shared__ unsigned char s_fl[SH_TILE], s_acc[SH_TILE];
     __shared__ int cnt[2 * 64];
     __shared__ float s_faddb, s_ergold1;
     const int tid = threadIdx.x;
@@ -329,17 +338,26 @@ __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
     __syncthreads();
     for (int base = 0; base < D.nmol; base += SH_TILE) {
         const int nt = min(SH_TILE, D.nmol - base);
-        for (int k = tid; k < nt; k += blockDim.x) {
+        const int ntp = (nt + SH_AHEAD - 1) / SH_AHEAD * SH_AHEAD;   // <= SH_TILE (a multiple of SH_AHEAD)
+        for (int k = tid; k < ntp; k += blockDim.x) {
+            if (k >= nt) {              // padding: no trial, no list -- the walk leaves the chain alone
+                s_fl[k] = 0;
+                s_enew[k] = s_r[k] = s_v1[k] = s_enp[k] = 0.0f;
+                s_prev[k] = -1;
+                s_slot[k] = 0;
+                continue;
+            }
             const int m = base + k;
             const long long o = D.off[m];
             const int nn = D.nergpairm[m];
-            s_nn[k] = nn;
             s_mt[k] = D.I.mtype[m];
-            s_mv[k] = o >= 0;
+            float en = 0.0f, r = 0.0f;
             if (o >= 0) {
-                s_enew[k] = D.enew[m];
-                s_r[k] = D.vals[o + 3LL * D.I.nato[m]];
+                en = D.enew[m];
+                r = D.vals[o + 3LL * D.I.nato[m]];
             }
+            s_enew[k] = en;
+            s_r[k] = r;
             int prev = -1, slot = 0;
             float v1 = 0.0f;
             if (nn >= 1) {
@@ -351,40 +369,58 @@ __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
                 const int p = D.molergpair[row];
                 if (p >= 0 && p < m && D.nergpairm[p] >= 1 && D.ergpairref[(size_t)p * D.M] == slot) prev = p;
             }
+            const float enp = prev >= 0 ? D.enew[prev] : 0.0f;
             s_slot[k] = slot;
             s_v1[k] = v1;
             s_prev[k] = prev;
-            if (o >= 0 && nn >= 1) s_et[k] = metropolis_etest(s_enew[k], v1, temp);   // the usual case
+            s_enp[k] = enp;
+            int fl = (o >= 0 ? SHF_MV : 0) | (nn >= 1 ? SHF_NN : 0) | (prev >= 0 ? SHF_PREV : 0);
+            if (o >= 0 && nn >= 1 && r < metropolis_etest(en, v1, temp)) fl |= SHF_ACC;
+            if (o >= 0 && prev >= 0 && r < metropolis_etest(en, enp, temp)) fl |= SHF_ACCP;
+            s_fl[k] = (unsigned char)fl;
         }
         __syncthreads();
         if (tid == 0) {
             float faddb = s_faddb, ergold1 = s_ergold1;
-            for (int k = 0; k < nt; ++k) {
-                const int nn = s_nn[k];
-                if (nn >= 1) {
-                    const int p = s_prev[k];
-                    ergold1 = s_v1[k];                                   // make_neighbour_list_from_mols
-                    if (p >= 0 && (p >= base ? s_acc[p - base] : D.acc[p])) ergold1 = D.enew[p];
+            for (int k0 = 0; k0 < ntp; k0 += SH_AHEAD) {
+                int fl[SH_AHEAD], pv[SH_AHEAD];
+                float en[SH_AHEAD], v1[SH_AHEAD], enp[SH_AHEAD];
+#pragma unroll
+                for (int j = 0; j < SH_AHEAD; ++j) {
+                    fl[j] = s_fl[k0 + j];
+                    en[j] = s_enew[k0 + j];
+                    v1[j] = s_v1[k0 + j];
+                    enp[j] = s_enp[k0 + j];
+                    pv[j] = s_prev[k0 + j];
                 }
-                int a = 0;
-                if (s_mv[k]) {
-                    const float en = s_enew[k];
-                    const float fdiffb = __fsub_rn(en, ergold1);
-                    // the test value was formed in parallel against the molecule's own first stored
-                    // energy; it is formed again only when the chain changed that energy
-                    float etest;
-                    if (nn >= 1 && __float_as_uint(ergold1) == __float_as_uint(s_v1[k])) etest = s_et[k];
-                    else etest = metropolis_etest_call(en, ergold1, temp);
-                    a = s_r[k] < etest;
-                    if (a) {
-                        faddb = __fadd_rn(faddb, fdiffb);
-                        if (nn >= 1) {                                   // save_energies + save_erg_pairs
-                            ergold1 = en;
-                            D.ergpair[s_slot[k] - 1] = en;
+#pragma unroll
+                for (int j = 0; j < SH_AHEAD; ++j) {
+                    const int k = k0 + j, f = fl[j];
+                    int pa = 0;
+                    if (f & SHF_NN) {
+                        ergold1 = v1[j];                                 // make_neighbour_list_from_mols
+                        if (f & SHF_PREV) {
+                            const int p = pv[j];
+                            pa = p >= base ? s_acc[p - base] : D.acc[p];
+                            if (pa) ergold1 = enp[j];
                         }
                     }
+                    int a = 0;
+                    if (f & SHF_MV) {
+                        // the decisions were formed in parallel against both energies the slot can
+                        // hold here; only a molecule with an empty list compares against the carried one
+                        if (f & SHF_NN) a = (f & (pa ? SHF_ACCP : SHF_ACC)) != 0;
+                        else a = s_r[k] < metropolis_etest_call(en[j], ergold1, temp);
+                        if (a) {
+                            faddb = __fadd_rn(faddb, __fsub_rn(en[j], ergold1));
+                            if (f & SHF_NN) {                            // save_energies + save_erg_pairs
+                                ergold1 = en[j];
+                                D.ergpair[s_slot[k] - 1] = en[j];
+                            }
+                        }
+                    }
+                    s_acc[k] = (unsigned char)a;
                 }
-                s_acc[k] = (unsigned char)a;
             }
             s_faddb = faddb;
             s_ergold1 = ergold1;
@@ -393,7 +429,7 @@ __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
         for (int k = tid; k < nt; k += blockDim.x) {
             const int a = s_acc[k];
             D.acc[base + k] = a;
-            if (s_mv[k] && s_mt[k] < 64) {
+            if ((s_fl[k] & SHF_MV) && s_mt[k] < 64) {
                 atomicAdd(&cnt[s_mt[k]], 1);
                 if (!a) atomicAdd(&cnt[64 + s_mt[k]], 1);
             }
