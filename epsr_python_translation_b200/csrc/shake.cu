@@ -396,29 +396,25 @@ __global__ void __launch_bounds__(SH_THREADS) shake_resolve_kernel(ShakeDev D) {
 #pragma unroll
                 for (int j = 0; j < SH_AHEAD; ++j) {
                     const int k = k0 + j, f = fl[j];
+                    const bool nn = (f & SHF_NN) != 0, mv = (f & SHF_MV) != 0;
                     int pa = 0;
-                    if (f & SHF_NN) {
-                        ergold1 = v1[j];                                 // make_neighbour_list_from_mols
-                        if (f & SHF_PREV) {
-                            const int p = pv[j];
-                            pa = p >= base ? s_acc[p - base] : D.acc[p];
-                            if (pa) ergold1 = enp[j];
-                        }
+                    if (f & SHF_PREV) {
+                        const int p = pv[j];
+                        pa = p >= base ? s_acc[p - base] : D.acc[p];
                     }
-                    int a = 0;
-                    if (f & SHF_MV) {
-                        // the decisions were formed in parallel against both energies the slot can
-                        // hold here; only a molecule with an empty list compares against the carried one
-                        if (f & SHF_NN) a = (f & (pa ? SHF_ACCP : SHF_ACC)) != 0;
-                        else a = s_r[k] < metropolis_etest_call(en[j], ergold1, temp);
-                        if (a) {
-                            faddb = __fadd_rn(faddb, __fsub_rn(en[j], ergold1));
-                            if (f & SHF_NN) {                            // save_energies + save_erg_pairs
-                                ergold1 = en[j];
-                                D.ergpair[s_slot[k] - 1] = en[j];
-                            }
-                        }
-                    }
+                    // make_neighbour_list_from_mols: ergold(1) is the first stored energy (as the
+                    // sharing molecule left it); a molecule with an empty list keeps the carried one
+                    const float e1 = nn ? (pa ? enp[j] : v1[j]) : ergold1;
+                    // the decisions were formed in parallel against both energies the slot can
+                    // hold here; only a molecule with an empty list compares against the carried one
+                    int a;
+                    if (mv && !nn) a = s_r[k] < metropolis_etest_call(en[j], e1, temp);
+                    else a = mv && (f & (pa ? SHF_ACCP : SHF_ACC)) != 0;
+                    const float fsum = __fadd_rn(faddb, __fsub_rn(en[j], e1));
+                    faddb = a ? fsum : faddb;
+                    const bool save = a && nn;                          // save_energies + save_erg_pairs
+                    ergold1 = save ? en[j] : e1;
+                    if (save) D.ergpair[s_slot[k] - 1] = en[j];
                     s_acc[k] = (unsigned char)a;
                 }
             }
