@@ -10,7 +10,6 @@
 //     (potex) are counted alongside;
 // (4) normalisation in float32 exactly as the reference (counts are exact integers; the
 //     reference's float accumulation equals them while a bin stays below 2^24).
-#include <mutex>
 
 #include "common.cuh"
 
@@ -275,6 +274,11 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
         epsr_set_error("epsr_atogen: at most 64 molecule types");
         return EPSR_ERR_UNSUPPORTED;
     }
+    // refused before any device work: a rejected call leaves the counts and the ran1 state as given
+    if (box->ntype > 64) {
+        epsr_set_error("epsr_atogen: at most 64 atom types");
+        return EPSR_ERR_UNSUPPORTED;
+    }
     if (scratch_bytes < epsr_atogen_scratch_bytes(nmol, natom, box->nmoltype, box->ntype)) {
         epsr_set_error("epsr_atogen: scratch too small");
         return EPSR_ERR_CAPACITY;
@@ -342,10 +346,6 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
         rc = epsr_ran1_fill(ran1, draws, ncand, stream);
         if (rc) return rc;
     }
-    if (box->ntype > 64) {
-        epsr_set_error("epsr_atogen: at most 64 atom types");
-        return EPSR_ERR_UNSUPPORTED;
-    }
     ag_select_kernel<<<1, 1024, 0, s>>>(A, draws, im1, im2, probaccept, box->itype, origins, prefix, misc, csampled,
                                          pairc);
     ag_intra_kernel<<<(nmol + 127) / 128, 128, 0, s>>>(A, box->itype, counts, pairc + 1);
@@ -394,12 +394,7 @@ constexpr int64_t NOALLOC_MAX_NATOM = 150000;
 constexpr int64_t NOALLOC_MAX_COUNTS = 1 << 19;   // 2*npairs*ldw + npairs
 constexpr int64_t NOALLOC_COUNTS_BYTES = NOALLOC_MAX_COUNTS * 8;
 constexpr int64_t NOALLOC_WORK_BYTES = 4 << 20;   // >= epsr_atogen_scratch_bytes at the maxima
-constexpr int NOALLOC_MAX_DEVICES = 64;
-
 static __device__ __align__(256) unsigned char g_atogen_noalloc[NOALLOC_COUNTS_BYTES + NOALLOC_WORK_BYTES];
-
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[NOALLOC_MAX_DEVICES];
 }  // namespace
 
 extern "C" int epsr_atogen_noalloc(const epsr_box_t *box, int32_t npt1, float sizefactor, float dmax,
@@ -424,23 +419,13 @@ extern "C" int epsr_atogen_noalloc(const epsr_box_t *box, int32_t npt1, float si
                        (long long)NOALLOC_WORK_BYTES);
         return EPSR_ERR_CAPACITY;
     }
-    // the device address of the array, looked up once per device with that device current
-    int dev = 0;
-    EPSR_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
-        epsr_set_error("epsr_atogen_noalloc: device ordinal %d out of range", dev);
-        return EPSR_ERR_ARG;
-    }
+    // The device address of the array in the current device's context.  It is looked up on
+    // every call (a cheap host query) rather than cached, so a context that was re-created
+    // (after cudaDeviceReset) is served at its own address.
     void *base = nullptr;
     {
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_atogen_noalloc);
-            if (e != cudaSuccess) return epsr_cuda_check(e, "cudaGetSymbolAddress(g_atogen_noalloc)");
-            g_noalloc_addr[dev] = p;
-        }
-        base = g_noalloc_addr[dev];
+        cudaError_t e = cudaGetSymbolAddress(&base, g_atogen_noalloc);
+        if (e != cudaSuccess) return epsr_cuda_check(e, "cudaGetSymbolAddress(g_atogen_noalloc)");
     }
     unsigned long long *counts = (unsigned long long *)base;  // zeroed inside epsr_atogen
     void *work = (unsigned char *)base + NOALLOC_COUNTS_BYTES;

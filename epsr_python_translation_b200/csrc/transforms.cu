@@ -112,7 +112,10 @@ __global__ void ptgnsq_diff_kernel(int ndata, int npairs, int nq, const float *d
     if (!q) {
         qtemp = __fsub_rn(dd[i], sum);
     } else {
-        const int nqmn = nqmin ? nqmin[d] : 1, nqmx = nqmax ? nqmax[d] : nq;
+        // the window as given, kept inside the row [1, nq] (the reference's window always is)
+        int nqmn = nqmin ? nqmin[d] : 1, nqmx = nqmax ? nqmax[d] : nq;
+        nqmn = nqmn < 1 ? 1 : (nqmn > nq ? nq : nqmn);
+        nqmx = nqmx > nq ? nq : nqmx;
         const float sz = szeros ? szeros[d] : 0.0f;
         const float qn = q[nqmn];
         const float qthr = qn > qmin ? qn : qmin;          // max(qminptemp, q(nqmn))

@@ -243,12 +243,13 @@ int64_t epsr_atogen_last_pair_updates(void);
  * with no device allocator of its own, or a host whose device memory belongs to another
  * allocator that must not be bypassed.  Arguments and results are those of epsr_atogen
  * minus counts/scratch/scratch_bytes; the results are identical to epsr_atogen's.
- * Working memory is one file-scope device array of 10 MiB per device (histogram counts plus
- * work space), so the call allocates nothing.  Limits: nmol <= 50000, natom <= 150000 and
+ * Working memory is one file-scope device array of 8 MiB per device (4 MiB of histogram counts
+ * plus 4 MiB of work space), so the call allocates nothing.  Limits: nmol <= 50000, natom <= 150000 and
  * 2*npairs*ldw + npairs <= 524288; larger boxes return EPSR_ERR_CAPACITY with the limits in
  * epsr_last_error.  Nothing needs to start at zero: the counts are cleared inside each call.
- * The first call on a device (with that device current) looks up the array's address once;
- * make that first call before any stream capture.  The array is shared by every call on the
+ * Every call looks up the array's address in the current device's context (the device the
+ * call runs on must be current); the first call on a device may load the library's device
+ * code there, so make that first call before any stream capture.  The array is shared by every call on the
  * device, so two calls that overlap in time (other streams or host threads) race on it and
  * give wrong results: serialise them. */
 int epsr_atogen_noalloc(const epsr_box_t *box, int32_t npt1, float sizefactor, float dmax, const float *rminex,

@@ -511,6 +511,7 @@ typedef struct {
     int32_t ncos;
     double *den64;   /* [nmol] FP64 energy change of the proposed move, or NULL */
     double *scale64; /* [nmol] sum of |FP64 pair energies| before and after the move */
+    float *u;        /* [nmol] the ran1 value of the Metropolis test, or NULL */
 } oracle_trace;
 
 /* FP64 restatement of en_atom_inter_scale (molfit.py:1251-1279): the same tables and bin
@@ -683,7 +684,9 @@ int oracle_molfit(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_
             if (ediff <= 0.0f) etest = 10.0f;
             else if (ediff < 20.0f) etest = expf(-ediff);
             else etest = 0.0f;
-            int acc = oracle_ran1(R) < etest;
+            const float udraw = oracle_ran1(R);
+            int acc = udraw < etest;
+            if (T && T->u) T->u[T->nmoves] = udraw;
             if (acc) {
                 P->nstepreject[im] = 0;
                 fadd = fadd + fdiff;
@@ -1397,9 +1400,41 @@ static void smoop(int nqmin, int nqmax, int nsmoo, float *diff) {
     }
 }
 
+/* chi^2 over rows nmin..npt of (yin - expand)^2: the reference's sequential float sum, or
+ * (fast) the same float32 squares summed in double and rounded once to float32 -- the
+ * summation the device's fast fit mode uses inside its trial loop. */
+static float fit_chisq(const float *yin, const float *expr, const float *wt, int nmin, int npt, int nterms,
+                       float summax, int fast) {
+    if (fast) {
+        double c = 0.0;
+        for (int i = nmin; i <= npt; ++i) {
+            float term = yin[i] - expand(nterms, i, expr, wt, summax);
+            c += (double)(term * term);
+        }
+        return (float)c;
+    }
+    float c = 0.0f;
+    for (int i = nmin; i <= npt; ++i) {
+        float term = yin[i] - expand(nterms, i, expr, wt, summax);
+        c = c + term * term;
+    }
+    return c;
+}
+
+int64_t oracle_fit_expansion_mode(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
+                                  float *scal, int nmin, int npt, int ncfirst, int nterms, int nits, int nfreq,
+                                  oracle_ran1_state *R, int fast);
+
 int64_t oracle_fit_expansion(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
                              float *scal, int nmin, int npt, int ncfirst, int nterms, int nits, int nfreq,
                              oracle_ran1_state *R) {
+    return oracle_fit_expansion_mode(yin, expr, yout, wt, wtold, scal, nmin, npt, ncfirst, nterms, nits, nfreq, R,
+                                     0);
+}
+
+int64_t oracle_fit_expansion_mode(const float *yin, const float *expr, float *yout, float *wt, float *wtold,
+                                  float *scal, int nmin, int npt, int ncfirst, int nterms, int nits, int nfreq,
+                                  oracle_ran1_state *R, int fast) {
     const float summax = expf(25.0f);
     const int nstep = 100, ntry = 150;
     float stepr = scal[0];
@@ -1418,11 +1453,7 @@ int64_t oracle_fit_expansion(const float *yin, const float *expr, float *yout, f
     if (nits > 0) {
         float chisqold;
         int icount = 0;
-        chisqnew = 0.0f;
-        for (int i = nmin; i <= npt; ++i) {
-            float term = yin[i] - expand(nterms, i, expr, wt, summax);
-            chisqnew = chisqnew + term * term;
-        }
+        chisqnew = fit_chisq(yin, expr, wt, nmin, npt, nterms, summax, fast);
         chisqold = chisqnew;
         float chisqtest = -1.0f, chisqfinish = 0.0f;
         int itry = 0;
@@ -1439,11 +1470,7 @@ int64_t oracle_fit_expansion(const float *yin, const float *expr, float *yout, f
                     else
                         wt[ic] = wtold[ic] * (1.0f + stepr * (2.0f * oracle_ran1(R) - 1.0f));
                 }
-                chisqnew = 0.0f;
-                for (int i = nmin; i <= npt; ++i) {
-                    float term = yin[i] - expand(nterms, i, expr, wt, summax);
-                    chisqnew = chisqnew + term * term;
-                }
+                chisqnew = fit_chisq(yin, expr, wt, nmin, npt, nterms, summax, fast);
                 float exponent = (chisqnew - chisqold) / accept;
                 float test;
                 if (exponent > 0.0f && exponent <= 20.0f) test = expf(-exponent) - oracle_ran1(R);
@@ -1454,11 +1481,7 @@ int64_t oracle_fit_expansion(const float *yin, const float *expr, float *yout, f
                     if (icount == nfreq) {
                         icount = 0;
                         smoop(ncfirst, nterms, 1, wt);
-                        chisqnew = 0.0f;
-                        for (int i = nmin; i <= npt; ++i) {
-                            float term = yin[i] - expand(nterms, i, expr, wt, summax);
-                            chisqnew = chisqnew + term * term;
-                        }
+                        chisqnew = fit_chisq(yin, expr, wt, nmin, npt, nterms, summax, fast);
                     }
                     chisqold = chisqnew;
                     for (int ic = 1; ic <= nterms; ++ic) wtold[ic] = wt[ic];

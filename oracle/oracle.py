@@ -42,6 +42,7 @@ def lib():
         _lib.oracle_ran1.restype = C.c_float
         _lib.oracle_en_mole_pair.restype = C.c_float
         _lib.oracle_fit_expansion.restype = C.c_int64
+        _lib.oracle_fit_expansion_mode.restype = C.c_int64
     return _lib
 
 
@@ -94,7 +95,7 @@ class McParC(C.Structure):
 
 class TraceC(C.Structure):
     _fields_ = [("nmoves", C.c_int32), ("im", P), ("den", P), ("acc", P), ("cosv", P), ("ncos", C.c_int32),
-                ("den64", P), ("scale64", P)]
+                ("den64", P), ("scale64", P), ("u", P)]
 
 
 class SysHandle:
@@ -267,9 +268,10 @@ def molfit(box, cells, st, mc, ran1, fadds=0.0, record_cos=True):
     par.nstepreject, par.ngrot = ptr(mc["nstepreject"]), ptr(mc["ngrot"])
     tr = dict(im=np.zeros(box.nmol, np.int32), den=np.zeros(box.nmol, f32), acc=np.zeros(box.nmol, np.int32),
               cosv=np.zeros(3 * box.nmol, f32) if record_cos else None,
-              den64=np.zeros(box.nmol, np.float64), scale64=np.zeros(box.nmol, np.float64))
+              den64=np.zeros(box.nmol, np.float64), scale64=np.zeros(box.nmol, np.float64),
+              u=np.zeros(box.nmol, f32))
     T = TraceC()
-    T.den64, T.scale64 = ptr(tr["den64"]), ptr(tr["scale64"])
+    T.den64, T.scale64, T.u = ptr(tr["den64"]), ptr(tr["scale64"]), ptr(tr["u"])
     T.im, T.den, T.acc = ptr(tr["im"]), ptr(tr["den"]), ptr(tr["acc"])
     T.cosv = ptr(tr["cosv"]) if record_cos else None
     r = Ran1C.of(ran1)
@@ -521,8 +523,10 @@ def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
     return out
 
 
-def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1):
-    """1-based arrays (index 0 unused).  Returns dict and the new ran1 state."""
+def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1, fast=False):
+    """1-based arrays (index 0 unused).  Returns dict and the new ran1 state.  fast: the trial
+    loop's chi^2 summed in double and rounded once to float32 (the device's fast mode); the
+    final chi^2 keeps the reference's sequential float sum in both modes."""
     yin = np.ascontiguousarray(yin, f32)
     expr = np.ascontiguousarray(expr, f32)
     wt = np.zeros(nterms + 1, f32)
@@ -530,8 +534,8 @@ def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfr
     yout = np.zeros(npt + 1, f32)
     scal = np.array([stepr, 0.0, 0.0, 0.0], f32)
     r = Ran1C.of(ran1)
-    trials = lib().oracle_fit_expansion(ptr(yin), ptr(expr), ptr(yout), ptr(wt), ptr(wto), ptr(scal), nmin, npt,
-                                        ncfirst, nterms, nits, nfreq, C.byref(r))
+    trials = lib().oracle_fit_expansion_mode(ptr(yin), ptr(expr), ptr(yout), ptr(wt), ptr(wto), ptr(scal), nmin,
+                                             npt, ncfirst, nterms, nits, nfreq, C.byref(r), 1 if fast else 0)
     return dict(wt=wt, wtold=wto, yout=yout, stepr=scal[0], acceptr=scal[1], rejrat=scal[2], chisq=scal[3],
                 trials=int(trials)), r.to_state()
 

@@ -3,7 +3,7 @@
 Run in a container where the reference is importable (it is read-only; nothing is written
 there):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [case ...]
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [case ...]
 
 Each case writes ``tests/golden/<case>.npz`` with the system inputs and, per routine, the
 reference's outputs:
@@ -39,7 +39,7 @@ from epsr_python_translation_b200 import configs  # noqa: E402
 import refstate  # noqa: E402
 
 f32 = np.float32
-REF = "/root/reference"
+REF = refstate.reference_root()
 
 
 def system_arrays(s):
@@ -317,6 +317,10 @@ CASES = {
                                   ngrsamples=0, nq=300, qstep=0.1),
     "silica": lambda: run_case("silica", configs.silica(seed=4, natom=240), cycles=2, ngrsamples=0,
                                transforms=False, wholerot=0.0),
+    # a translation step far below the float32 spacing of the centres: movem's displacement
+    # rounds away and its retry doubles the step until a centre moves (molfit.py:752-758)
+    "c1_retry": lambda: run_case("c1_retry", configs.c1_water(seed=5), cycles=2, ngrsamples=0, transforms=False,
+                                 wholetrans_A=1.0e-9),
     "c2_mixture": lambda: run_case("c2_mixture", configs.c2_mixture(seed=1), cycles=1, ngrsamples=0,
                                    transforms=False),
     "fitexp": lambda: run_fit(),

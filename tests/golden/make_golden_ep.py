@@ -5,7 +5,7 @@ on seeded state.
 Run in a container where the reference is importable (it is read-only; nothing is written
 there):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_ep.py
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_ep.py
 
 Each case fills potential_par (Poisson basis of the reference's own default size for
 rminpt 9 / rmaxpt 12 A: pdstep 0.1, pdmin 1 + pdstep/rminpt, 116 terms), the r grid of
@@ -34,7 +34,7 @@ from epsr_python_translation_b200 import configs  # noqa: E402
 import refstate  # noqa: E402
 
 f32 = np.float32
-REF = "/root/reference"
+REF = refstate.reference_root()
 
 
 def run_case(name, ep, npairs, rmaxgr, absolute_energy, erequnit, ereqstep, seed, out, ncalls=2, iref=None,

@@ -4,7 +4,7 @@ reference translation (epsr26) on the golden systems.
 Run in a container where the reference is importable (it is read-only; nothing is written
 there):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_press.py [case ...]
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_press.py [case ...]
 
 For each case the system is rebuilt with the seed that make_golden.py used, the cell list
 and the pair store are made by the reference (initialise_cellneighbourlist, fmolec1) as in
@@ -36,7 +36,7 @@ from epsr_python_translation_b200 import configs  # noqa: E402
 import refstate  # noqa: E402
 
 f32 = np.float32
-REF = "/root/reference"
+REF = refstate.reference_root()
 
 
 def run_press(name, s, out, *, rejrate=0.75, nmolcell=10):

@@ -7,7 +7,7 @@ data set on the reference's own Q-space basis (calc_pwrexpq), the coefficient in
 Run in a container where the reference is importable (it is read-only; nothing is written
 there; ptgnsq's diagnostic file delfit.dat goes to a temporary folder that is removed):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_ptgnsq.py
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_ptgnsq.py
 
 The state: two data sets (no X-ray weighting, szeros 0, the whole Q range fitted), three atom
 pairs in two coefficient sets (pairs 1 and 3 share set 1), real*8 weights cwt and cwtpot that
@@ -38,7 +38,7 @@ from epsr_python_translation_b200 import configs  # noqa: E402
 import refstate  # noqa: E402
 
 f32 = np.float32
-REF = "/root/reference"
+REF = refstate.reference_root()
 
 
 def run(ep, out, nq=100, nterms=30, nits=200, seed=21, qminp=0.0, nqmin=(1, 1), szeros=(0.0, 0.0), xray=(0, 0)):

@@ -5,7 +5,7 @@ translation (epsr26) on seeded parameters.
 Run in a container where the reference is importable (it is read-only; nothing is written
 there):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_rp.py
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_rp.py
 
 Cases: "lj" (power 12, charged spheres of radii 0, 0.5 and 1.0 A so that every branch of chsph
 is taken, the exponential repulsive core without a gradient limit), "gauss" (power 10, two
@@ -32,7 +32,7 @@ from epsr_python_translation_b200 import configs  # noqa: E402
 import refstate  # noqa: E402
 
 f32 = np.float32
-REF = "/root/reference"
+REF = refstate.reference_root()
 TABS = ("epot", "epot1", "ecoul", "ecoul1", "xav", "xav1")
 
 

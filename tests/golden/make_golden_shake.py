@@ -5,7 +5,7 @@ on seeded systems.
 Run in a container where the reference is importable (it is read-only; nothing is written
 there):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_shake.py
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_shake.py
 
 Each case loads a configs system into the COMMON blocks (refstate.populate: harmonic bonds
 from the molecule templates, water's H-H pair as a bond-angle pair), then sets what this branch
@@ -36,7 +36,7 @@ import refstate  # noqa: E402
 from make_golden import system_arrays  # noqa: E402
 
 f32 = np.float32
-REF = "/root/reference"
+REF = refstate.reference_root()
 
 
 def run_case(name, s, out, *, refine_intra=False, seed=0, cycles=2, interntrans_A=0.05):

@@ -4,7 +4,7 @@ and :3642-3677), made by running the reference translation (epsr26) on seeded st
 Run in a container where the reference is importable (it is read-only; nothing is written
 there):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_sums.py
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_sums.py
 
 For each case the accumulators (gorintra/gorinter/gr2intra/gr2inter, soqintra/...) are
 filled with seeded running values, the new histograms wav(2, nz, npairs) and S(Q)
@@ -26,7 +26,7 @@ sys.path.insert(0, HERE)
 import refstate  # noqa: E402
 
 f32 = np.float32
-REF = "/root/reference"
+REF = refstate.reference_root()
 
 
 def run_case(name, npairs, nz, nq, nsum, ncalls, seed, out):

@@ -19,9 +19,21 @@ import numpy as np
 f32 = np.float32
 
 
-def load_reference(src="/root/reference/src"):
+def reference_root():
+    """The checkout of the reference (its top directory, holding src/epsr26), from the
+    environment variable EPSR_REFERENCE.  Only the fixture generators read it."""
+    import os
+    root = os.environ.get("EPSR_REFERENCE")
+    if not root or not os.path.isdir(os.path.join(root, "src", "epsr26")):
+        raise SystemExit("set EPSR_REFERENCE to the reference checkout (the directory holding src/epsr26)")
+    return root
+
+
+def load_reference(src=None):
     import os
     import sys
+    if src is None:
+        src = os.path.join(reference_root(), "src")
     os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")
     sys.dont_write_bytecode = True
     if src not in sys.path:

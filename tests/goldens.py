@@ -5,7 +5,7 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["c1_water", "c1_sampled", "mix_small", "silica", "c2_mixture"]
+CASES = ["c1_water", "c1_sampled", "mix_small", "silica", "c2_mixture", "c1_retry"]
 
 
 def load(name):
@@ -55,3 +55,22 @@ def golden_store(z, prefix):
         partners.append(mol[:k, im] - 1)
         energies.append(erg[ref[:k, im] - 1])
     return partners, energies
+
+
+def point_box(lat6, pts):
+    """A BoxArrays of single-atom molecules at the given centres on a non-cubic lattice
+    (lat6 = alatx, blatx, clatx, blaty, claty, clatz), for the minimum-image goldens; the
+    tables are a one-point stub that nothing here evaluates."""
+    from epsr_python_translation_b200.box import BoxArrays
+    n = pts.shape[0]
+    f32 = np.float32
+    z1 = np.zeros((1, 4), f32)
+    return BoxArrays(
+        naf=np.arange(n, dtype=np.int32), nato=np.ones(n, np.int32), mtype=np.zeros(n, np.int32),
+        itype=np.zeros(n, np.int32), xa=np.zeros(n, f32), ya=np.zeros(n, f32), za=np.zeros(n, f32),
+        xadd=np.ascontiguousarray(pts[:, 0], f32), yadd=np.ascontiguousarray(pts[:, 1], f32),
+        zadd=np.ascontiguousarray(pts[:, 2], f32), npairref=np.zeros((1, 1), np.int32),
+        n1extr=np.zeros(1, np.int32), n2extr=np.zeros(1, np.int32), nmoltype=1, dmax=f32(1.0),
+        cellst=f32(0.03), x=np.zeros(4, f32), xstar=np.zeros(4, f32), npt=3, npt1=2, npt2=1, nptmax=2,
+        xavs=z1.copy(), xavs1=z1.copy(), ecoul=z1.copy(), ecoul1=z1.copy(), simt=f32(2.477),
+        cfrac=np.ones(1, f32), natomr=n, cubic=False, lat6=np.ascontiguousarray(lat6, f32))

@@ -106,3 +106,24 @@ def test_every_entry_point_rejects_null_and_zero_arguments():
         assert name in msg, (name, msg)
         checked += 1
     assert checked >= 25
+
+
+def test_atogen_refuses_too_many_atom_types_before_device_work():
+    """More than 64 atom types is refused by epsr_atogen (and so by epsr_atogen_noalloc) before
+    any memset or ran1 draw: the check runs before any CUDA call, so no GPU is needed, and a
+    ran1 state handed in is left as it was."""
+    from epsr_python_translation_b200 import _lib
+    L = _lib.load()
+    b = _lib.Box()
+    b.nmol, b.natom, b.npairs, b.ntype, b.nmoltype = 100, 300, 65 * 66 // 2, 65, 1
+    b.ld = 101
+    ngr = np.array([1000], np.int32)
+    buf = np.zeros(64, np.float32)
+    p = buf.ctypes.data_as(C.c_void_p)
+    ran1 = np.arange(35, dtype=np.int32)
+    before = ran1.copy()
+    rc = L.epsr_atogen(C.byref(b), 100, 1.0, 30.0, p, p, p, p, p, 3, ngr.ctypes.data_as(C.c_void_p),
+                       ran1.ctypes.data_as(C.c_void_p), p, 101, p, p, p, 1 << 30, None)
+    assert rc == 4   # EPSR_ERR_UNSUPPORTED
+    assert "64 atom types" in L.epsr_last_error().decode()
+    assert np.array_equal(ran1, before)

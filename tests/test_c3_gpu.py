@@ -70,3 +70,46 @@ def test_c3_cells_store_molfit_atogen_match_oracle(c3):
     assert_bits_equal(dwav, wav, "wav")
     assert_bits_equal(dpotex, potex, "potex")
     assert np.array_equal(t.cpu().numpy(), rst.as_array())
+
+
+def test_c3_fast_store_and_speculative_cycle_match_oracle(c3):
+    """The fast modes the iteration and the benchmark run, at full C3 size: the pair store
+    built with fast sums is bit-identical to the oracle's (only ftest is summed in another
+    order, within 1e-5 of the oracle's), and one speculative molfit cycle with the oracle's
+    cosines takes the oracle's decisions -- every energy change within the tolerance of the
+    FP64 change, every decision the Metropolis rule on the device's own change and draw, a
+    different decision only at the threshold of its draw -- and, while the chains agree,
+    leaves coordinates, stored energies and the ran1 state bit-identical."""
+    from epsr_python_translation_b200.device import DeviceBox
+    from tests.chain_check import check_decisions
+    s, eintra = c3
+    ob = BoxArrays.from_system(s)
+    d = DeviceBox(BoxArrays.from_system(s))
+    d.cell_list(10, f32(ob.sepmax))
+    oc = oracle.cell_list(ob, 10, f32(ob.sepmax))
+    ft, _ = d.fmolec1(eintra, strict=False)
+    ost = oracle.fmolec1(ob, oc, eintra)
+    st = d.download_store()
+    assert st["nergpair"] == ost["nergpair"]
+    assert_bits_equal(st["ergpair"], ost["ergpair"][: ost["nergpair"]], "ergpair (fast)")
+    assert abs(float(ft) - float(ost["ftest"])) <= 1e-5 * abs(float(ost["ftest"])) + 1e-3
+    nmt = ob.nmoltype
+    tmax, tmin = trsteps(ob.natomr)
+    rot, tra = np.full(nmt, f32(10.0 / 180.0), f32), np.full(nmt, f32(0.5) / f32(ob.dmax), f32)
+    ran1 = Ran1State(idum=-5)
+    d.mc_setup(rejrate=f32(0.75), stepr=f32(1.0), stepm=f32(1.0), wholerot=rot, wholetrans=tra,
+               internrot=np.zeros(nmt, f32), interntrans=np.zeros(nmt, f32), ran1=ran1, trstepmax=tmax,
+               trstepmin=tmin)
+    omc = dict(rejrate=f32(0.75), stepr=f32(1.0), stepm=f32(1.0), wholerot=rot.copy(), wholetrans=tra.copy(),
+               internrot=np.zeros(nmt, f32), interntrans=np.zeros(nmt, f32), ireset=0)
+    _, tr, ran1_after = oracle.molfit(ob, oc, ost, omc, ran1)
+    d.molfit(strict=False, cos_override=tr["cosv"])
+    d.check_status()
+    m = d.download_mc()
+    if check_decisions(m["den"], m["acc"], tr, ob.simt, 1e-5) == "parted":
+        return
+    co = d.download_coords()
+    for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+        assert_bits_equal(co[k], getattr(ob, k), k)
+    assert_bits_equal(d.download_store()["ergpair"], ost["ergpair"][: ost["nergpair"]], "ergpair after molfit")
+    assert m["ran1"].idum == ran1_after.idum and np.array_equal(m["ran1"].iv, ran1_after.iv)
