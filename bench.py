@@ -1,21 +1,27 @@
 #!/usr/bin/env python
-"""Benchmark of the EPSR pair path on B200: MC molecule-moves/s (+ g(r) pair-updates/s).
+"""Benchmark of the EPSR pair path on B200: MC molecule-moves/s and g(r) pair-updates/s.
 
-One step = one EPSR iteration of the hot path on configuration C2 (200 DMSO + 400 water,
-3200 atoms, 21 pair types) for each of R independent boxes on the GPU (``--replicas``,
-default 16): cell list, fmolec1, 5 molfit cycles (3000 whole-molecule moves), atogen over
-all 5,118,400 atom pairs, gensq, press, fit_expansion for three datasets, stog.  Each box has its
-own ran1 seed, CUDA stream and host thread; a box's chain is sequential (Metropolis, one
-ran1 stream), so independent boxes are how one GPU is filled.  ``value`` = molecule moves
-of all boxes per second of device time, inputs resident in HBM; ``single_box`` reports one
-box alone (its stage breakdown feeds the roofline).
+Headline workload: configuration C3, 20,000 rigid water (60,000 atoms, L = 84.3 A, EP on,
+g(r) bin 0.03 A).  One step = one EPSR iteration of the hot path for each of R independent
+boxes on the GPU (``--replicas``): cell list, fmolec1, 100 molfit sweeps (2,000,000
+whole-molecule moves), atogen over 1,000 sampled origin molecules, gensq, ptgnsq's
+difference, press, fit_expansion against one synthetic S(Q) (1,000 Q points), the EP
+refinement, the running averages and stog.  Each box has its own ran1 seed, CUDA stream and
+host thread; a box's chain is sequential (Metropolis, one ran1 stream), so independent boxes
+are how one GPU is filled.  ``value`` = molecule moves of all boxes per second of device
+time, inputs resident in HBM; ``pair_updates_per_s`` the atogen pair-updates of all boxes
+per second of the same time; ``single_box`` reports one box alone.  A secondary line
+(``secondary``) measures configuration C2 (200 DMSO + 400 water, 16 boxes, 5 sweeps per
+iteration) the same way.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--replicas R] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c3_water|c2_mixture|c4_batch]
+                    [--replicas R] [--sweeps S] [--impl ours|reference]
 
 Under torchrun each rank advances its own R boxes: there is no data-path collective, so
 ``scaling`` is "weak".  ``--impl reference`` times the reference's algorithm (the C
 restatement in oracle/, single-threaded per process) on all host cores with one
-independent box per core.
+independent box per core; at C3 each of its steps is one sweep, and the iteration time is
+the sampled sweeps scaled to the iteration's sweep count plus the other stages timed once.
 """
 
 from __future__ import annotations
@@ -31,7 +37,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "MC molecule-moves/s"
+METRIC = "MC molecule-moves/s (+ g(r) pair-updates/s)"
 # dram__bytes_read.sum + dram__bytes_write.sum of one fitexp_cluster_kernel launch on the C2
 # fit, from an ncu --set full capture of one launch (independent of the trial count: the
 # basis is read from HBM once per launch)
@@ -39,7 +45,19 @@ FIT_DRAM_BYTES_PER_LAUNCH = 409856
 # SM cycles per ran1 value of the warp shuffle chain (two shuffles a step) on an otherwise
 # idle SM (clock64 timing of 640,000 values)
 FIT_CHAIN_CYCLES_PER_VALUE = 40.0
+# FP32 operations per atom pair of a pair energy (3 sub, 6 minimum image, 5 d^2, 1 sqrt,
+# 2 div, 4 table arithmetic, 2 adds, 1 scale, 2 more) and per atogen pair-update
+# dram__bytes_read.sum + dram__bytes_write.sum per atom pair of one spec_energy_kernel launch
+# (an ncu capture of one launch), or None while no capture has been taken
+SPEC_ENERGY_TRAFFIC_PER_PAIR = None
+OPS_PER_ENERGY_PAIR = 26
+OPS_PER_PAIR_UPDATE = 17
 UNIT = "moves/s"
+DEFAULT_SWEEPS = {"c3_water": 100}          # molfit sweeps per iteration (others: 5)
+DEFAULT_REPLICAS = {"c3_water": 2, "c2_mixture": 16}
+# kernels the library brackets with CUDA events while timing is enabled
+TIMED_KERNELS = ("spec_energy_kernel", "spec_corr_kernel", "spec_resolve_kernel", "molfit_seq_kernel",
+                 "fm_count_kernel", "ag_inter_kernel", "fitexp_cluster_kernel")
 
 
 def parse():
@@ -48,8 +66,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2_mixture")
-    ap.add_argument("--replicas", type=int, default=16, help="independent boxes per GPU (one stream each)")
+    ap.add_argument("--config", default="c3_water")
+    ap.add_argument("--replicas", type=int, default=None,
+                    help="independent boxes per GPU (one stream each; default 2 at C3, 16 at C2)")
+    ap.add_argument("--sweeps", type=int, default=None, help="molfit sweeps per iteration (default 100 at C3, else 5)")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the secondary C2 x 16 measurement")
     ap.add_argument("--strict", action="store_true", help="bit-identical sequential sums")
     ap.add_argument("--cpu-sample-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -57,25 +78,56 @@ def parse():
                     help="flexible molecules: an intramolecular molfit cycle every INTRA cycles (0: rigid)")
     ap.add_argument("--python-driver", action="store_true",
                     help="drive each iteration's routines from Python instead of epsr_iteration_step")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.sweeps is None:
+        a.sweeps = DEFAULT_SWEEPS.get(a.config, 5)
+    if a.replicas is None:
+        a.replicas = DEFAULT_REPLICAS.get(a.config, 16)
+    return a
 
 
 # ----------------------------------------------------------------------------- CPU side
+SAMPLED_SWEEPS_ABOVE = 5   # iterations with more sweeps than this are timed as a bounded sample
+
+
 def _cpu_worker(args):
-    config, seed, steps, warmup, intra = args
+    """One process, one core: the oracle (the C restatement of the reference) on one box.
+    Returns (seconds per iteration, stage seconds of one iteration, pair-updates per
+    iteration, moves per iteration, sample description).  Iterations of at most
+    SAMPLED_SWEEPS_ABOVE sweeps run whole (warmup, then steps timed); longer ones run one
+    iteration with a single sweep (its other stages timed once), then warmup + steps single
+    sweeps, and the iteration time is those stages plus the mean sweep x the sweep count."""
+    config, seed, steps, warmup, intra, sweeps = args
     from epsr_python_translation_b200 import configs
     from oracle.workload import CpuIteration
-    wl = configs.make_workload(config, intra=intra)
+    wl = configs.make_workload(config, intra=intra, ntimes=sweeps)
     it = CpuIteration(wl, ran1_seed=seed)
+    moves = wl.ntimes * wl.system.nmol
+    if sweeps <= SAMPLED_SWEEPS_ABOVE:
+        for _ in range(warmup):
+            it.step()
+        per = []
+        for _ in range(steps):
+            a = time.perf_counter()
+            it.step()
+            per.append(time.perf_counter() - a)
+        return (statistics.mean(per), dict(it.stage_s), it.pair_updates, moves,
+                f"{steps} full EPSR iterations of {config} ({moves} moves each) after {warmup} warm-up")
+    it.step(sample_sweeps=1)
+    fixed = {k: v for k, v in it.stage_s.items() if k != "molfit"}
     for _ in range(warmup):
-        it.step()
-    t0 = time.perf_counter()
+        it.sweep()
     per = []
     for _ in range(steps):
         a = time.perf_counter()
-        it.step()
+        it.sweep()
         per.append(time.perf_counter() - a)
-    return time.perf_counter() - t0, per, it.stage_s, it.pair_updates, wl.ntimes * wl.system.nmol
+    sw = statistics.mean(per)
+    stages = dict(fixed, molfit=sw * wl.ntimes)
+    return (sum(stages.values()), stages, it.pair_updates, moves,
+            f"one {config} iteration sampled: its stages other than molfit timed once, {steps} molfit sweeps "
+            f"({wl.system.nmol} moves each) timed after {warmup} warm-up, the iteration = those stages + "
+            f"{wl.ntimes} x the mean sweep ({sw:.2f} s)")
 
 
 def cpu_info():
@@ -90,16 +142,17 @@ def cpu_info():
     return model, os.cpu_count() or 1
 
 
-def cpu_baseline(config, steps, intra=0):
+def cpu_baseline(config, steps, intra=0, sweeps=5):
     """Single core: the oracle (C restatement of the reference) on a bounded sample of the
     same workload."""
-    wall, per, stages, pairs, moves = _cpu_worker((config, -7, steps, 1, intra))
+    if sweeps > SAMPLED_SWEEPS_ABOVE:
+        steps = min(steps, 2)
+    t_iter, stages, pairs, moves, sample = _cpu_worker((config, -7, steps, 1, intra, sweeps))
     model, n = cpu_info()
-    ms = 1000.0 * statistics.mean(per)
-    return {"value": moves / statistics.mean(per), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{steps} full EPSR iterations of {config} ({moves} moves each) after 1 warm-up, "
-                      f"single-threaded C oracle, {ms:.0f} ms/iteration; pair-updates/s "
-                      f"{pairs / stages.get('atogen', 1e9):.3e}; host {model}, nproc {n}",
+    return {"value": moves / t_iter, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{sample}; single-threaded C oracle, {1000.0 * t_iter:.0f} ms/iteration; pair-updates/s "
+                      f"{pairs / stages.get('atogen', 1e9):.3e} (atogen alone); host {model}, nproc {n}",
+            "pair_updates_per_s": pairs / t_iter,
             "stage_s": {k: round(v, 4) for k, v in stages.items()}}
 
 
@@ -111,25 +164,30 @@ def reference_arm(a):
     model, ncpu = cpu_info()
     nproc = max(1, ncpu)
     steps, warmup = a.steps, a.warmup
-    # bounded: a few minutes at most (one C2 iteration is about 1.4 s on one core)
+    # bounded: a few minutes at most (one C2 iteration is about 1 s on one core; a C3 sweep
+    # about 1.3 s, plus about 40 s of set-up and the other stages once)
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(nproc) as pool:
-        res = pool.map(_cpu_worker, [(a.config, -(11 + i), steps, warmup, a.intra) for i in range(nproc)])
+        res = pool.map(_cpu_worker, [(a.config, -(11 + i), steps, warmup, a.intra, a.sweeps) for i in range(nproc)])
     wall = time.perf_counter() - t0
-    moves = res[0][4]
+    moves = res[0][3]
     slowest = max(r[0] for r in res)
-    value = nproc * steps * moves / slowest
+    value = nproc * moves / slowest
+    pairs = nproc * res[0][2] / slowest
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": steps,
-        "warmup": warmup, "ms_per_step": 1000.0 * slowest / steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded C2 mixture box)",
-        "config": {"workload": a.config, "moves_per_step_per_replica": moves, "replicas": nproc,
-                   "stages": "cells+fmolec1+5 molfit+atogen+gensq+ptgnsq differences+press+fit_expansion+"
-                             "EP refinement+sums+stog"},
+        "warmup": warmup, "ms_per_step": 1000.0 * slowest, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {a.config} box per core)",
+        "config": {"workload": a.config, "moves_per_step_per_box": moves, "boxes_per_gpu": nproc,
+                   "sweeps_per_iteration": a.sweeps,
+                   "stages": f"cells+fmolec1+{a.sweeps} molfit+atogen+gensq+ptgnsq differences+press+fit_expansion+"
+                             "EP refinement+sums+stog",
+                   "parallelism": f"replicas: one box per host core ({nproc})"},
+        "pair_updates_per_s": pairs,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
-                         "sample": f"{nproc} independent replicas x {steps} iterations (+{warmup} warm-up) of the "
-                                   f"single-threaded C restatement, one process per core; host {model}"},
+                         "sample": f"{nproc} independent boxes, one process per core, each: {res[0][4]}; "
+                                   f"the slowest box's iteration time counts; host {model}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(wall, 2),
     }
@@ -198,10 +256,90 @@ def max_over_ranks(x, dist, device):
     return float(t.item())
 
 
-def gpu_arm(a):
-    import threading
+class Replicas:
+    """R independent boxes of one workload, each with its own ran1 seed, CUDA stream and
+    persistent host thread.  run(body) advances every box by body(r) concurrently and returns
+    the device time of that round (ms): events on a common stream that every box stream waits
+    on at the start and that waits on every box stream at the end."""
 
-    import numpy as np  # noqa: F401
+    def __init__(self, wl, R, rank, strict, native):
+        import threading
+
+        import torch
+
+        from epsr_python_translation_b200.iteration import EpsrIteration
+        self.R = R
+        self.streams = [torch.cuda.Stream() for _ in range(R)]
+        self.its = []
+        for r in range(R):
+            with torch.cuda.stream(self.streams[r]):
+                self.its.append(EpsrIteration(wl, strict=strict, ran1_seed=box_seed(rank, R, r), native=native))
+        torch.cuda.synchronize()
+        self.main = torch.cuda.current_stream()
+        self.go = [threading.Event() for _ in range(R)]
+        self.fin = [threading.Event() for _ in range(R)]
+        self.body = None
+        self.e0 = None
+        self.done = [torch.cuda.Event() for _ in range(R)]
+        self.err = []
+        self.th = [threading.Thread(target=self._loop, args=(r,), daemon=True) for r in range(R)]
+        for t in self.th:
+            t.start()
+
+    def _loop(self, r):
+        import torch
+        while True:
+            self.go[r].wait()
+            self.go[r].clear()
+            if self.body is None:
+                return
+            try:
+                with torch.cuda.stream(self.streams[r]):
+                    self.streams[r].wait_event(self.e0)
+                    self.body(r)
+                    self.done[r].record(self.streams[r])
+            except Exception as e:  # reported by run()
+                self.err.append(e)
+            self.fin[r].set()
+
+    def run(self, body):
+        import torch
+        self.body = body
+        self.e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.e0.record(self.main)
+        for ev in self.go:
+            ev.set()
+        for ev in self.fin:
+            ev.wait()
+            ev.clear()
+        if self.err:
+            raise self.err[0]
+        for ev in self.done:
+            self.main.wait_event(ev)
+        e1.record(self.main)
+        e1.synchronize()
+        return self.e0.elapsed_time(e1)
+
+    def close(self):
+        self.body = None
+        for ev in self.go:
+            ev.set()
+        for t in self.th:
+            t.join()
+
+
+def kernel_times(lib):
+    """{kernel: (total ms, launches)} of the kernels the library timed."""
+    import ctypes as C
+    out = {}
+    for k in TIMED_KERNELS:
+        ms, n = C.c_double(0.0), C.c_int64(0)
+        if lib.epsr_timing_read(k.encode(), C.byref(ms), C.byref(n)) == 0 and n.value > 0:
+            out[k] = (ms.value, int(n.value))
+    return out
+
+
+def gpu_arm(a):
     import torch
     import torch.distributed as dist
 
@@ -212,80 +350,18 @@ def gpu_arm(a):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    from epsr_python_translation_b200 import configs
-    from epsr_python_translation_b200.iteration import STAGES, EpsrIteration
+    from epsr_python_translation_b200 import _lib, configs
+    from epsr_python_translation_b200.iteration import STAGES
+    lib = _lib.load(require_device=True)
 
-    wl = configs.make_workload(a.config, intra=a.intra)
+    wl = configs.make_workload(a.config, intra=a.intra, ntimes=a.sweeps)
     R = max(1, a.replicas)
-    # independent boxes (own ran1 seeds), each driven by its own host thread on its own stream
-    streams = [torch.cuda.Stream() for _ in range(R)]
-    its = []
-    for r in range(R):
-        with torch.cuda.stream(streams[r]):
-            its.append(EpsrIteration(wl, strict=a.strict, ran1_seed=box_seed(rank, R, r), native=not a.python_driver))
-    torch.cuda.synchronize()
+    reps = Replicas(wl, R, rank, a.strict, not a.python_driver)
+    its, streams, main = reps.its, reps.streams, reps.main
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
-    main = torch.cuda.current_stream()
-
-    class Boxes:
-        """R persistent host threads, one per box; run(body) advances every box by one step
-        concurrently and returns the device time of that round (ms)."""
-
-        def __init__(self):
-            self.go = [threading.Event() for _ in range(R)]
-            self.fin = [threading.Event() for _ in range(R)]
-            self.body = None
-            self.e0 = None
-            self.done = [torch.cuda.Event() for _ in range(R)]
-            self.err = []
-            self.th = [threading.Thread(target=self._loop, args=(r,), daemon=True) for r in range(R)]
-            for t in self.th:
-                t.start()
-
-        def _loop(self, r):
-            while True:
-                self.go[r].wait()
-                self.go[r].clear()
-                if self.body is None:
-                    return
-                try:
-                    with torch.cuda.stream(streams[r]):
-                        streams[r].wait_event(self.e0)
-                        self.body(r)
-                        self.done[r].record(streams[r])
-                except Exception as e:  # reported by run()
-                    self.err.append(e)
-                self.fin[r].set()
-
-        def run(self, body):
-            self.body = body
-            self.e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            self.e0.record(main)
-            for ev in self.go:
-                ev.set()
-            for ev in self.fin:
-                ev.wait()
-                ev.clear()
-            if self.err:
-                raise self.err[0]
-            for ev in self.done:
-                main.wait_event(ev)
-            e1.record(main)
-            e1.synchronize()
-            return self.e0.elapsed_time(e1)
-
-        def close(self):
-            self.body = None
-            for ev in self.go:
-                ev.set()
-            for t in self.th:
-                t.join()
-
-    boxes = Boxes()
-    run_round = boxes.run
 
     for _ in range(max(3, a.warmup)):
-        run_round(lambda r: its[r].step())
+        reps.run(lambda r: its[r].step())
     torch.cuda.synchronize()
 
     # ---------------- device-resident timing (value): R boxes x K steps
@@ -299,7 +375,8 @@ def gpu_arm(a):
     time.sleep(0.3)
     # every box advances through its K iterations independently (no barrier between the boxes'
     # iterations, as replicas of a production run do), each iteration preceded on the box's own
-    # stream by a 256 MB write that flushes L2 (inside the timed region)
+    # stream by a 256 MB write that flushes L2 (inside the timed region); the library brackets
+    # its main kernels with events on their streams meanwhile (kernel_ms)
     flush_box = [torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") for _ in range(R)]
 
     def free_steps(r):
@@ -307,16 +384,20 @@ def gpu_arm(a):
             flush_box[r].fill_(float(k))
             its[r].step()
 
-    round_ms = [run_round(free_steps)]
+    lib.epsr_timing_enable(1)
+    round_ms = reps.run(free_steps)
     torch.cuda.synchronize()
+    lib.epsr_timing_enable(0)
+    ktimes = kernel_times(lib)
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    tmax_ms = max_over_ranks(sum(round_ms), dist, "cuda")
+    tmax_ms = max_over_ranks(round_ms, dist, "cuda")
     moves = its[0].moves_per_step
     value = world * R * a.steps * moves / (tmax_ms / 1000.0)
+    pair_value = world * R * a.steps * its[0].pair_updates / (tmax_ms / 1000.0)
 
-    # ---------------- one box alone: stage breakdown and the roofline of the dominant kernel
+    # ---------------- one box alone: stage breakdown
     it = its[0]
     stage_tot = {k: 0.0 for k in STAGES}
     single_ms = 0.0
@@ -351,32 +432,41 @@ def gpu_arm(a):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+
     def e2e_free(r):
         for k in range(a.steps):
             flush_box[r].fill_(float(k))
             e2e_body(r)
 
-    e2e_ms = max_over_ranks(run_round(e2e_free), dist, "cuda")
+    e2e_ms = max_over_ranks(reps.run(e2e_free), dist, "cuda")
     e2e_value = world * R * a.steps * moves / (e2e_ms / 1000.0)
 
-    boxes.close()
-    intra = intra_cycle(it, wl, a) if rank == 0 else None
+    reps.close()
+    intra = intra_cycle(it, wl, a) if rank == 0 and a.config != "c3_water" else None
     stage_ms = {k: v / a.steps for k, v in stage_tot.items()}
-    roof, extra = roofline(it, stage_ms, a)
+    roof, extra = roofline(it, ktimes, a)
     launches = kernel_launches(it, wl)
+    pairs_box, fit_trials = it.pair_updates, it.fit_trials
+    secondary = None
+    if rank == 0 and world == 1 and a.config != "c2_mixture" and not a.no_secondary:
+        del reps, its, it
+        torch.cuda.empty_cache()
+        secondary = secondary_c2(a)
 
     if rank == 0:
+        b = wl.system
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": tmax_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": f"synthetic (seeded {a.config} boxes, synthetic data sets)",
-            "config": {"workload": a.config, "nmol": it.box.nmol, "natom": it.box.natom, "npairs": it.box.npairs,
+            "pair_updates_per_s": pair_value,
+            "config": {"workload": a.config, "nmol": int(b.nmol), "natom": int(b.natom), "npairs": int(b.npairs),
                        "molecules": "flexible: every %d-th molfit cycle intramolecular" % a.intra if a.intra > 0
                        else "rigid (whole-molecule moves only)",
-                       "moves_per_step_per_box": moves, "boxes_per_gpu": R,
-                       "pair_updates_per_step_per_box": it.pair_updates,
+                       "sweeps_per_iteration": wl.ntimes, "moves_per_step_per_box": moves, "boxes_per_gpu": R,
+                       "pair_updates_per_step_per_box": pairs_box,
                        "stages": f"cells+fmolec1+{wl.ntimes} molfit+atogen+gensq+ptgnsq differences+press+"
-                                 f"fit_expansion ({wl.data.shape[0]} data sets)+"
+                                 f"fit_expansion ({wl.data.shape[0]} data set{'s' if wl.data.shape[0] > 1 else ''})+"
                                  f"{'EP refinement (coefficient increment, generate_ep, packed tables)+' if wl.ep else ''}"
                                  "sums (sumsq, sumgr)+stog",
                        "step": f"one EPSR iteration of each of the {R} independent boxes on this GPU, each box on "
@@ -388,9 +478,11 @@ def gpu_arm(a):
             "single_box": {"ms_per_step": single_ms / a.steps,
                            "moves_per_s": moves / (single_ms / a.steps / 1000.0),
                            "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
-                           "pair_updates_per_s": it.pair_updates / (stage_ms["atogen"] / 1000.0),
+                           "pair_updates_per_s_atogen": pairs_box / (stage_ms["atogen"] / 1000.0),
                            "mc_moves_per_s_molfit_only": moves / (stage_ms["molfit"] / 1000.0),
-                           "fit_trials_per_step": it.fit_trials},
+                           "fit_trials_per_step": fit_trials},
+            "kernel_ms": {k: {"total_ms": round(v[0], 3), "launches": v[1], "mean_us": round(1000 * v[0] / v[1], 2)}
+                          for k, v in ktimes.items()},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": R * h2d,
                     "d2h_bytes_per_step": sum(d2h)},
             "roofline": roof, **extra,
@@ -398,13 +490,43 @@ def gpu_arm(a):
             "gpu_launches": launches * a.steps * R,
             "clocks": clk,
         }
+        if secondary is not None:
+            line["secondary"] = secondary
         if not a.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(a.config, a.cpu_sample_steps, a.intra)
+            line["cpu_baseline"] = cpu_baseline(a.config, a.cpu_sample_steps, a.intra, a.sweeps)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def secondary_c2(a):
+    """Configuration C2 (200 DMSO + 400 water, 3,200 atoms, 5 sweeps per iteration) on 16
+    independent boxes, timed as the headline (no L2 flush difference, same rules)."""
+    import torch
+
+    from epsr_python_translation_b200 import configs
+    wl = configs.make_workload("c2_mixture", ntimes=5)
+    R = 16
+    reps = Replicas(wl, R, 0, a.strict, not a.python_driver)
+    its = reps.its
+    for _ in range(3):
+        reps.run(lambda r: its[r].step())
+    flush_box = [torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") for _ in range(R)]
+    steps = max(5, min(a.steps, 20))
+
+    def free_steps(r):
+        for k in range(steps):
+            flush_box[r].fill_(float(k))
+            its[r].step()
+
+    ms = reps.run(free_steps)
+    reps.close()
+    moves = its[0].moves_per_step
+    return {"workload": "c2_mixture", "boxes_per_gpu": R, "sweeps_per_iteration": 5, "steps": steps,
+            "value": R * steps * moves / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / steps,
+            "pair_updates_per_s": R * steps * its[0].pair_updates / (ms / 1000.0)}
 
 
 def intra_cycle(it, wl, a):
@@ -476,68 +598,107 @@ def kernel_launches(it, wl):
     return n
 
 
-def roofline(it, stage_ms, a):
-    """Roofline of the dominant stage (largest share of the step)."""
+def _peaks():
     import json as _j
-
-    import numpy as np
-    peaks = {}
     try:
         peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         src = "of measured"
     except (OSError, ValueError):
-        src = "of fallback"
+        peaks, src = {}, "of fallback"
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    fp32_peak = 148 * 128 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12  # Top/s, 1 op/lane/clock
-    dom = max(stage_ms, key=stage_ms.get)
-    b = it.box
+    mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    # FP32 CUDA-core issue peak: 148 SMs x 128 FP32 lanes x the SM clock, one operation per
+    # lane per clock (no FMA contraction: the path is built with -fmad=false).  No measured
+    # FP32 figure exists for this pool, so this one is nominal.
+    fp32 = 148 * 128 * mhz * 1e6 / 1e12
+    return hbm, fp32, mhz, src
+
+
+def spec_energy_pairs(it):
+    """Atom pairs one spec_energy_kernel launch evaluates on box ``it`` as it stands: for every
+    move k (molecule m in visit order) and stored partner p, E(new m, old p) always and
+    E(new m, new p) when p is earlier in the visit order -- na(m) x na(p) atom pairs each.
+    Returns (those pairs, stored entries, partner atoms over the entries, atom pairs with each
+    entry evaluated once)."""
+    import numpy as np
+    d = it.d
+    st = d.download_store()
+    cells = d.download_cells()
+    nato = it.box.nato.astype(np.int64)
+    visit = cells["cell_mols"][: it.box.nmol]
+    vpos = np.empty_like(visit)
+    vpos[visit] = np.arange(visit.size)
+    nn = st["nergpairm"].astype(np.int64)
+    M = st["nnbrefmax"]
+    cols = np.arange(M)[None, :]
+    valid = (cols >= 1) & (cols < nn[:, None])
+    part = np.where(valid, st["molergpair"], 0)
+    pa = nato[part] * valid
+    earlier = (vpos[part] < vpos[:, None]) & valid
+    per_mol = (pa + pa * earlier).sum(axis=1) * nato
+    entries = int(valid.sum())
+    once = int((pa.sum(axis=1) * nato).sum())
+    return int(per_mol.sum()), entries, int(pa.sum()), once
+
+
+def roofline(it, ktimes, a):
+    """Roofline of the kernel with the largest device time in the timed region (the library's
+    per-launch events), against the bound that applies to it."""
+    import numpy as np  # noqa: F401
+    hbm, fp32, mhz, src = _peaks()
+    extra = {}
+    if not ktimes:
+        return None, extra
+    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    tot, n = ktimes[dom]
+    launch_ms = tot / n
+    extra["dominant_kernel"] = dom
+    extra["kernel_share_of_timed"] = {k: round(v[0] / sum(x[0] for x in ktimes.values()), 4)
+                                      for k, v in ktimes.items()}
     wl = it.wl
-    extra = {"dominant_stage": dom}
-    if dom == "molfit":
-        # algorithmic bytes of one sweep: per move its stored list (partner, ref, old energy,
-        # new energy write: 16 B/entry) and the coordinates of every neighbour atom (16 B/atom)
-        st = it.d.download_store()
-        nn = st["nergpairm"].astype(np.int64)
-        nato = b.nato.astype(np.int64)
-        atoms_per_mol = np.array([int(np.sum(nato[st["molergpair"][m, 1:nn[m]]])) for m in range(b.nmol)])
-        bytes_sweep = int(np.sum(16 * np.maximum(nn - 1, 0)) + np.sum(16 * atoms_per_mol))
-        pairs_sweep = int(np.sum(atoms_per_mol * nato))
-        per_launch_ms = stage_ms["molfit"] / wl.ntimes
-        ach = bytes_sweep / (per_launch_ms / 1000.0) / 1e9
-        extra["fp32_issue"] = {"achieved_Tops": pairs_sweep * 26 / (per_launch_ms / 1000.0) / 1e12,
-                               "peak_Tops": fp32_peak, "ops_per_atom_pair": 26,
-                               "atom_pairs_per_sweep": pairs_sweep}
-        return {"bound": "hbm", "kernel": "molfit_seq_kernel", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": None, "peak_source": src,
-                "algorithmic_bytes_per_launch": bytes_sweep, "launch_ms": per_launch_ms}, extra
-    if dom == "fit_expansion":
-        # one cluster launch per step fits every data set; per trial the basis is read once
-        # (npt * nterms * 4 bytes, from shared memory after the first load)
-        per_launch_ms = stage_ms["fit_expansion"]
-        byt = it.fit_trials * wl.nq * wl.nterms * 4
-        ach = byt / (per_launch_ms / 1000.0) / 1e9
-        us_trial = 1000.0 * per_launch_ms / max(it.fit_trials, 1)
-        extra["fit_us_per_trial"] = us_trial
-        # The kernel is latency-bound: every trial consumes nterms+1 ran1 values from one
-        # sequential shuffle chain, measured at 40 SM cycles per value on an otherwise idle SM.
-        chain_us = (wl.nterms + 1) * FIT_CHAIN_CYCLES_PER_VALUE / (float(peaks.get("sm_max_mhz", 1965.0)))
-        extra["fit_chain_bound"] = {"us_per_trial": chain_us, "frac": chain_us / us_trial,
-                                    "cycles_per_value": FIT_CHAIN_CYCLES_PER_VALUE}
-        return {"bound": "hbm", "kernel": "fitexp_cluster_kernel", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": FIT_DRAM_BYTES_PER_LAUNCH, "peak_source": src,
-                "algorithmic_bytes_per_launch": byt, "launch_ms": per_launch_ms}, extra
-    if dom == "atogen":
-        per_launch_ms = stage_ms["atogen"]
-        byt = 16 * b.natom * max(1, b.natom // 256)
-        ach = byt / (per_launch_ms / 1000.0) / 1e9
-        extra["fp32_issue"] = {"achieved_Tops": it.pair_updates * 17 / (per_launch_ms / 1000.0) / 1e12,
-                               "peak_Tops": fp32_peak}
-        return {"bound": "hbm", "kernel": "ag_inter_kernel", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": byt,
-                "launch_ms": per_launch_ms}, extra
-    per_launch_ms = stage_ms[dom]
-    return {"bound": "hbm", "kernel": dom, "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
-            "traffic": None, "peak_source": src, "launch_ms": per_launch_ms}, extra
+    if dom in ("spec_energy_kernel", "molfit_seq_kernel"):
+        pairs, entries, partner_atoms, once = spec_energy_pairs(it)
+        if dom == "molfit_seq_kernel":
+            pairs = once          # the sequential kernel evaluates E(new m, cur p) once per entry
+        ops = OPS_PER_ENERGY_PAIR * pairs
+        ach = ops / (launch_ms / 1000.0) / 1e12
+        # bytes the kernel must move at least: per stored entry its partner index and reference
+        # (8 B) and the energy written (4 B), per partner atom its float4 position (16 B) for the
+        # old and, when earlier in the visit order, the new position
+        byt = 12 * entries + 16 * partner_atoms
+        extra["hbm_algorithmic"] = {"bytes_per_launch": byt, "achieved_GBs": byt / (launch_ms / 1000.0) / 1e9,
+                                    "peak_GBs": hbm, "frac": byt / (launch_ms / 1000.0) / 1e9 / hbm,
+                                    "peak_source": src}
+        return {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": fp32, "unit": "Tops/s (FP32 issue)",
+                "frac": ach / fp32, "traffic": SPEC_ENERGY_TRAFFIC_PER_PAIR and int(SPEC_ENERGY_TRAFFIC_PER_PAIR * pairs),
+                "peak_source": "nominal (148 SMs x 128 lanes x %.0f MHz)" % mhz,
+                "ops_per_launch": ops, "atom_pairs_per_launch": pairs, "ops_per_atom_pair": OPS_PER_ENERGY_PAIR,
+                "launch_ms": launch_ms, "launches": n}, extra
+    if dom == "spec_resolve_kernel":
+        ns = 1e6 * launch_ms / it.box.nmol
+        return {"bound": "latency", "kernel": dom, "achieved": ns, "peak": None, "unit": "ns per move (ordered walk)",
+                "frac": None, "traffic": None, "launch_ms": launch_ms, "launches": n}, extra
+    if dom == "fitexp_cluster_kernel":
+        trials = max(it.fit_trials, 1)
+        flops = 2.0 * wl.nq * wl.nterms * trials
+        ach = flops / (launch_ms / 1000.0) / 1e12
+        us_trial = 1000.0 * launch_ms / trials
+        chain_us = (wl.nterms + 1) * FIT_CHAIN_CYCLES_PER_VALUE / mhz
+        extra["fit_chain_bound"] = {"us_per_trial": chain_us, "measured_us_per_trial": us_trial,
+                                    "frac": chain_us / us_trial, "cycles_per_value": FIT_CHAIN_CYCLES_PER_VALUE}
+        return {"bound": "ran1 chain (latency)", "kernel": dom, "achieved": ach, "peak": fp32,
+                "unit": "Tops/s (FP32 issue)", "frac": ach / fp32, "traffic": FIT_DRAM_BYTES_PER_LAUNCH,
+                "peak_source": "nominal (148 SMs x 128 lanes x %.0f MHz)" % mhz, "launch_ms": launch_ms,
+                "launches": n}, extra
+    if dom == "ag_inter_kernel":
+        pu = it.pair_updates
+        ops = OPS_PER_PAIR_UPDATE * pu
+        ach = ops / (launch_ms / 1000.0) / 1e12
+        return {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": fp32, "unit": "Tops/s (FP32 issue)",
+                "frac": ach / fp32, "traffic": None, "peak_source": "nominal (148 SMs x 128 lanes x %.0f MHz)" % mhz,
+                "pair_updates_per_launch": pu, "launch_ms": launch_ms, "launches": n}, extra
+    return {"bound": "unknown", "kernel": dom, "achieved": None, "peak": None, "unit": None, "frac": None,
+            "traffic": None, "launch_ms": launch_ms, "launches": n}, extra
 
 
 def c4_arm(a):

@@ -52,6 +52,13 @@ class Mc(C.Structure):
                 ("status", P)]
 
 
+class Mlp(C.Structure):
+    """epsr_mlp_t: the surrogate network's parameters, gradients and Adam moments (device)."""
+    _fields_ = [("w1", P), ("b1", P), ("w2", P), ("b2", P), ("w3", P), ("b3", P), ("w1h", P), ("w2h", P),
+                ("w2th", P), ("dw1", P), ("db1", P), ("dw2", P), ("db2", P), ("dw3", P), ("db3", P), ("m1", P),
+                ("v1", P), ("status", P)]
+
+
 class Intra(C.Structure):
     """epsr_intra_t: the intramolecular model of en_atom_intra (device pointers)."""
     _fields_ = [("nbond", P), ("iabond", P), ("tbond", P), ("maxbond", I32), ("imageatom", P), ("qtype", P),
@@ -124,6 +131,18 @@ _SIGS = {
     "epsr_atogen_scratch_bytes": (I64, [I32, I32, I32, I32]),
     "epsr_atogen_last_pair_updates": (I64, []),
     "epsr_atogen_noalloc": (C.c_int, [C.POINTER(Box), I32, F32, F32, P, P, P, P, P, I32, P, P, P, I32, P, P]),
+    "epsr_timing_enable": (C.c_int, [I32]),
+    "epsr_umma_gemm_f32": (C.c_int, [P, I32, P, I32, I32, I32, P, I32, I32, P, P]),
+    "epsr_bmc_begin_sweep": (C.c_int, [P, P]),
+    "epsr_bmc_propose": (C.c_int, [P, I32, P, P]),
+    "epsr_bmc_decide": (C.c_int, [P, I32, I32, P, P, P]),
+    "epsr_bmc_end_sweep": (C.c_int, [P, P]),
+    "epsr_bmc_total_energy": (C.c_int, [P, P]),
+    "epsr_mlp_work_bytes": (I64, [I32]),
+    "epsr_mlp_sync_weights": (C.c_int, [C.POINTER(Mlp), P]),
+    "epsr_mlp_forward": (C.c_int, [C.POINTER(Mlp), P, I32, P, P, I64, P]),
+    "epsr_mlp_train_step": (C.c_int, [C.POINTER(Mlp), P, P, I64, I32, I32, P, F32, I32, P, P, I64, P]),
+    "epsr_timing_read": (C.c_int, [C.c_char_p, P, P]),
     "epsr_press": (C.c_int, [C.POINTER(Box), C.POINTER(Store), I32, P, I64, I32, P, P]),
     "epsr_press_scratch_bytes": (I64, [I32, I32]),
     "epsr_gensq": (C.c_int, [I32, I32, I32, P, I32, P, I64, I64, P, P, P, P, P]),

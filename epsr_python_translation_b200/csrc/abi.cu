@@ -1,6 +1,13 @@
 // abi.cu -- error plumbing and library information of the C ABI (include/epsr_gpu.h).
 #include <stdarg.h>
 #include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 
@@ -50,4 +57,78 @@ extern "C" int epsr_device_count(void) {
         if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10) ++k;
     }
     return k;
+}
+
+// ----------------------------------------------------------------- kernel timing
+// One record per bracketed launch: the two events, kept until the next enable.  Events come
+// from a pool that is reused across enables, so a long run creates no more events than the
+// launches of one measurement.
+int g_epsr_timing_on = 0;
+namespace {
+std::mutex g_tm_mu;
+std::map<std::string, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> g_tm;
+std::map<std::string, cudaEvent_t> g_tm_open;   // name + stream -> start event
+std::vector<cudaEvent_t> g_tm_pool;
+size_t g_tm_used = 0;
+
+cudaEvent_t tm_event() {
+    if (g_tm_used == g_tm_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        g_tm_pool.push_back(e);
+    }
+    return g_tm_pool[g_tm_used++];
+}
+}  // namespace
+
+void epsr_timing_mark(const char *name, cudaStream_t s, int end) {
+    std::lock_guard<std::mutex> lk(g_tm_mu);
+    char key[160];
+    snprintf(key, sizeof(key), "%s@%p", name, (void *)s);
+    if (!end) {
+        cudaEvent_t e = tm_event();
+        if (!e) return;
+        cudaEventRecord(e, s);
+        g_tm_open[key] = e;
+        return;
+    }
+    auto it = g_tm_open.find(key);
+    if (it == g_tm_open.end()) return;
+    cudaEvent_t e1 = tm_event();
+    if (!e1) return;
+    cudaEventRecord(e1, s);
+    g_tm[name].push_back({it->second, e1});
+    g_tm_open.erase(it);
+}
+
+extern "C" int epsr_timing_enable(int32_t on) {
+    std::lock_guard<std::mutex> lk(g_tm_mu);
+    g_tm.clear();
+    g_tm_open.clear();
+    g_tm_used = 0;
+    g_epsr_timing_on = on ? 1 : 0;
+    return EPSR_OK;
+}
+
+extern "C" int epsr_timing_read(const char *kernel, double *total_ms, int64_t *launches) {
+    if (!kernel || !total_ms || !launches) {
+        epsr_set_error("epsr_timing_read: null pointer");
+        return EPSR_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_tm_mu);
+    double t = 0.0;
+    int64_t n = 0;
+    auto it = g_tm.find(kernel);
+    if (it != g_tm.end()) {
+        for (auto &pr : it->second) {
+            EPSR_CUDA(cudaEventSynchronize(pr.second));
+            float ms = 0.0f;
+            EPSR_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            t += ms;
+            ++n;
+        }
+    }
+    *total_ms = t;
+    *launches = n;
+    return EPSR_OK;
 }

@@ -369,7 +369,7 @@ extern "C" int epsr_atogen(const epsr_box_t *box, int32_t npt1, float sizefactor
         EPSR_SMEM_OPTIN(ag_inter_kernel);
     if (noatoms > 0) {
         dim3 grid((natom + tile - 1) / tile, ychunks);
-        ag_inter_kernel<<<grid, AG_THREADS, shm, s>>>(A, oatoms, misc + 1, molof, tile, counts, counts + 2 * nbins);
+        EPSR_TIMED("ag_inter_kernel", s, ag_inter_kernel<<<grid, AG_THREADS, shm, s>>>(A, oatoms, misc + 1, molof, tile, counts, counts + 2 * nbins));
     }
     ag_norm_kernel<<<box->npairs, 256, 0, s>>>(A, counts, counts + 2 * nbins, csampled, cfrac, n1extr, n2extr, natomr,
                                                 addwav, ycoh, wav, potex);

@@ -18,7 +18,7 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libepsr_gpu.so")
 SOURCES = ["abi.cu", "ran1.cu", "cells.cu", "store.cu", "mc.cu", "atogen.cu", "transforms.cu", "fitexp.cu",
-           "mc_spec.cu", "press.cu", "iteration.cu", "sums.cu", "ep.cu", "shake.cu", "rp.cu"]
+           "mc_spec.cu", "press.cu", "iteration.cu", "sums.cu", "ep.cu", "shake.cu", "rp.cu", "mlp.cu", "batch.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
          "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]

@@ -294,6 +294,17 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }  // namespace epsr
 
 // Error plumbing shared by the ABI translation units.
+// Kernel timing for measurement (epsr_timing_enable / epsr_timing_read): while enabled, the
+// launches of the main kernels are bracketed by CUDA events on their launch stream.
+// epsr_timing_mark(name, s, 0) before the launch, epsr_timing_mark(name, s, 1) after it.
+extern int g_epsr_timing_on;
+void epsr_timing_mark(const char *name, cudaStream_t s, int end);
+#define EPSR_TIMED(name, s, ...)                           \
+    do {                                                   \
+        if (g_epsr_timing_on) epsr_timing_mark(name, s, 0); \
+        __VA_ARGS__;                                       \
+        if (g_epsr_timing_on) epsr_timing_mark(name, s, 1); \
+    } while (0)
 void epsr_set_error(const char *fmt, ...);
 int epsr_cuda_check(cudaError_t e, const char *what);
 int epsr_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s);

@@ -755,7 +755,7 @@ extern "C" int epsr_fit_expansion_batch(int32_t nprob, const float *yin, const f
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    EPSR_CUDA(cudaLaunchKernelEx(&cfg, fitexp_cluster_kernel, F));
+    EPSR_TIMED("fitexp_cluster_kernel", s, EPSR_CUDA(cudaLaunchKernelEx(&cfg, fitexp_cluster_kernel, F)));
     int hstatus = 0;
     EPSR_D2H(scal_host, scal, sizeof(float) * 4 * (size_t)nprob, s);
     EPSR_D2H(trials_host, trials, sizeof(long long) * (size_t)nprob, s);

@@ -424,7 +424,7 @@ int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_sto
     }
     if (shm > 48 * 1024)
         EPSR_SMEM_OPTIN(molfit_seq_kernel);
-    molfit_seq_kernel<<<1, MC_THREADS, shm, s>>>(D);
+    EPSR_TIMED("molfit_seq_kernel", s, molfit_seq_kernel<<<1, MC_THREADS, shm, s>>>(D));
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
 }

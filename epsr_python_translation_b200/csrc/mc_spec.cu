@@ -717,12 +717,12 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     spec_propose_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
     const size_t en_bytes = sizeof(int) * ((((size_t)box->ntype * box->ntype + 3) & ~(size_t)3) + 2 * (size_t)M);
     if (en_bytes > 48 * 1024) EPSR_SMEM_OPTIN(spec_energy_kernel);
-    spec_energy_kernel<<<N, SP_ET, en_bytes, s>>>(S);
+    EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, SP_ET, en_bytes, s>>>(S));
     EPSR_CUDA(cudaMemsetAsync(S.nearc, 0, sizeof(double) * (size_t)N * SP_W, s));
-    spec_corr_kernel<<<N, 128, 0, s>>>(S);
+    EPSR_TIMED("spec_corr_kernel", s, spec_corr_kernel<<<N, 128, 0, s>>>(S));
     const size_t bits = sizeof(unsigned) * (((size_t)N + 31) / 32);
     if (bits > 48 * 1024) EPSR_SMEM_OPTIN(spec_resolve_kernel);
-    spec_resolve_kernel<<<1, SP_RT, bits, s>>>(S);
+    EPSR_TIMED("spec_resolve_kernel", s, spec_resolve_kernel<<<1, SP_RT, bits, s>>>(S));
     spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
     spec_commit_store_kernel<<<N, 128, 0, s>>>(S);
     spec_epilogue_kernel<<<1, 32, 0, s>>>(S);

@@ -491,8 +491,8 @@ extern "C" int epsr_fmolec1(const epsr_box_t *box, const epsr_cells_t *cells, co
         cells->ncelldivc, M, reg, nn, err);
     const size_t list_bytes = sizeof(int) * (size_t)M;
     if (list_bytes > 48 * 1024) EPSR_SMEM_OPTIN(fm_count_kernel);
-    fm_count_kernel<<<nmol, FM_THREADS, list_bytes, s>>>(B, P, cells->cell_mols, cells->molcellno, reg, nn, M, ebuf,
-                                                         cnt);
+    EPSR_TIMED("fm_count_kernel", s, fm_count_kernel<<<nmol, FM_THREADS, list_bytes, s>>>(B, P, cells->cell_mols, cells->molcellno, reg, nn, M, ebuf,
+                                                         cnt));
     scan1_kernel<<<1, 1024, 0, s>>>(cnt, nmol, off, 0, nullptr);
     scan1_kernel<<<1, 1024, 0, s>>>(nullptr, nmol, iidx, 1, eintra);
     EPSR_CUDA(cudaGetLastError());

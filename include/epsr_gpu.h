@@ -223,6 +223,131 @@ int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, epsr_mc_t *mc,
                       float stepmi, int32_t *nmovei, float *faddbs, void *scratch, int64_t scratch_bytes,
                       void *stream);
 
+/* ------------------------------------------------------------------ batched checkerboard MC
+ * No counterpart in the reference: many independent cubic boxes advanced together by a
+ * parallel Metropolis scheme whose sampled distribution is the reference method's (the same
+ * tabulated pair energies, bin rule and temperature; molfit.py:401-408 for the test).  Each
+ * sweep bins every box's molecule centres into a grid of ncell^3 cells shifted by a random
+ * offset; the cells are coloured with stride^3 colours so that two cells of one colour are
+ * at least (stride-1) cells apart (>= the box's interaction range rint).  A step moves, in
+ * every box, one randomly chosen molecule in every cell of one colour; moves that take a
+ * centre out of its cell are rejected.  Moves of one step never interact, so they run in
+ * parallel and are exact.  The proposal is symmetric: a rotation by an angle uniform in
+ * [-rotmax, rotmax] about a uniformly random axis through the centre, then a translation
+ * uniform in [-transmax, transmax]^3 (box units).  Random numbers come from Philox4x32-10
+ * keyed by the box and counted by (sweep, step, slot).
+ * Delayed acceptance: with a surrogate, a move is first accepted with min(1, exp(-s)) where s
+ * is the network's antisymmetric estimate of beta*dE from the radial histograms of the moved
+ * molecule (64 bins of 0.125 A to 8 A, 10 element-pair classes, before and after the move),
+ * and only then evaluated exactly and accepted with min(1, exp(-(beta*dE - s))), which leaves
+ * the sampled distribution exactly that of the single-stage test. */
+typedef struct {
+    int32_t mol0, nmol, atom0, natom;            /* this box's molecules and atoms in the packed arrays */
+    int32_t ncell, stride, cell0, slot0, nslot;  /* cells per side, colour stride, offsets, (ncell/stride)^3 */
+    int32_t tab0, ld, izcut, npairref0, ntype, xstar0;   /* tables: float4 offset, ld, cutoff, pair map */
+    int32_t nrange, nrange_feat;                 /* cells scanned on each side for energies / features */
+    float stepcl, beta, dmax, rint, rfeat;       /* rint, rfeat: box units */
+    float rotmax, transmax;                      /* radians, box units */
+    uint32_t key0, key1;                         /* Philox key */
+    float shift[3];                              /* written by each sweep's binning */
+    int32_t colour_off;                          /* written by each sweep's binning */
+    int64_t sweep;                               /* the sweep being run (written by the binning) */
+} epsr_bmc_box_t;
+
+typedef struct {
+    int32_t nbox, nmol, natom, ncell, nslot;
+    epsr_bmc_box_t *box;          /* [nbox] */
+    const int32_t *slot_box;      /* [nslot] box of each slot */
+    const int32_t *mol_box;       /* [nmol] box of each molecule */
+    const int32_t *naf, *nato;    /* [nmol] first atom (packed index) and atom count (<= 64) */
+    const int32_t *fclass;        /* [natom] element class 0..3 of each atom (features) */
+    float *xa, *ya, *za;          /* [natom] offsets from the centre (box units) */
+    float *xadd, *yadd, *zadd;    /* [nmol] centres in [-0.5, 0.5) */
+    float *pos;                   /* [4*natom] absolute positions, w = atom type bits */
+    const float *tab;             /* packed float4 tables {xavs, xavs1, ecoul, ecoul1} of every box */
+    const float *xstar;           /* packed r grids / dmax */
+    const int32_t *npairref;      /* packed type-pair maps */
+    int32_t *cell_start;          /* [ncell + nbox] per box ncell^3+1 starts */
+    int32_t *cell_mols;           /* [nmol] */
+    int32_t *mol_cell;            /* [nmol + 2*ncell + nbox] scratch: cell of each molecule, bin cursors,
+                                     then the box of each packed cell (host-written, after the cursors) */
+    int32_t *slot_mol;            /* [nslot] molecule moved in the step, -1 none, -2 left its cell */
+    float *slot_new;              /* [nslot*64*4] proposed absolute positions */
+    float *slot_off;              /* [nslot*64*4] proposed offsets */
+    float *slot_centre;           /* [nslot*4] proposed centre */
+    double *energy;               /* [nbox] running total energy (kJ/mol) */
+    double *emol;                 /* [nmol] scratch of the total-energy kernel */
+    long long *counters;          /* [nbox*4] attempts, first-stage accepts, accepts, left-cell */
+    int64_t *sweep_counter;       /* [1] sweeps begun */
+    int32_t *status;
+} epsr_bmc_t;
+
+/* Bin every box's centres for a new sweep (random shift and colour order per box). */
+int epsr_bmc_begin_sweep(const epsr_bmc_t *b, void *stream);
+/* Step `step` of the sweep: propose a move per slot; with x (device BF16 [2*nslot][1280],
+ * rows 2k and 2k+1 = slot k's features before|after and after|before) also the features. */
+int epsr_bmc_propose(const epsr_bmc_t *b, int32_t step, void *x, void *stream);
+/* Decide the step's moves.  mode 0: single-stage Metropolis; 1: delayed acceptance with the
+ * network outputs y [2*nslot] (s = (y[2k]-y[2k+1])/2); 2: single-stage for training.  target
+ * [nslot] (optional in modes 0 and 1, required in 2) receives beta*dE - s for every move that
+ * was evaluated exactly (s = 0 outside mode 1) and NaN for the others. */
+int epsr_bmc_decide(const epsr_bmc_t *b, int32_t step, int32_t mode, const float *y, float *target, void *stream);
+/* The sweep counter advances (after the sweep's steps). */
+int epsr_bmc_end_sweep(const epsr_bmc_t *b, void *stream);
+/* Total energy of every box from scratch into energy[] (sum over molecule pairs within rint). */
+int epsr_bmc_total_energy(const epsr_bmc_t *b, void *stream);
+
+/* ------------------------------------------------------------------ surrogate network
+ * No counterpart in the reference: the first-stage screen of the delayed-acceptance Monte
+ * Carlo (learned.py) -- a 1280 -> 128 -> 128 -> 1 perceptron with SiLU activations, BF16
+ * weights and activations, FP32 accumulation, evaluated and trained by hand-written tcgen05
+ * GEMM kernels (TMA-staged operands, accumulators in tensor memory).  All pointers are device
+ * memory.  w1 [128][1280], b1 [128], w2 [128][128] (row = output unit), b2 [128], w3 [128],
+ * b3 [1] are the FP32 master weights; w1h, w2h (BF16 copies) and w2th (BF16 w2 transposed)
+ * are what the kernels read (epsr_mlp_sync_weights refreshes them from the masters; the
+ * training step keeps them current).  dw1..db3 are FP32 gradient accumulators of the same
+ * shapes (zero before the first training step; each step leaves them zero); m1 and v1 the Adam
+ * moments of all parameters packed in the order w1, b1, w2, b2, w3, b3 (165,633 floats
+ * each).  status [1]: set to 1 when a bounded wait inside a kernel gave up. */
+typedef struct {
+    float *w1, *b1, *w2, *b2, *w3, *b3;
+    void *w1h, *w2h, *w2th;
+    float *dw1, *db1, *dw2, *db2, *dw3, *db3;
+    float *m1, *v1;
+    int32_t *status;
+} epsr_mlp_t;
+
+/* D = A . B^T on the tensor cores, for tests: a [m][k] and b [n][k] row-major BF16 (k a
+ * multiple of 64), out [m][ldo] FP32, stored (accumulate = 0) or added atomically (1), with the
+ * k range split over kslices CTAs. */
+int epsr_umma_gemm_f32(const void *a, int32_t m, const void *b, int32_t n, int32_t k, int32_t kslices, float *out,
+                       int32_t ldo, int32_t accumulate, int32_t *status, void *stream);
+/* device bytes of the work area for `rows` rows (forward or one training step) */
+int64_t epsr_mlp_work_bytes(int32_t rows);
+int epsr_mlp_sync_weights(const epsr_mlp_t *net, void *stream);
+/* y[r] = net(x[r]) for x [rows][1280] BF16 (16-byte aligned rows). */
+int epsr_mlp_forward(const epsr_mlp_t *net, const void *x, int32_t rows, float *y, void *work, int64_t work_bytes,
+                     void *stream);
+/* One Adam step (lr, bias correction for step >= 1) on rows row0..row0+rows-1 of x [.][1280]
+ * (rows and row0 multiples of 128; row pairs 2p, 2p+1 hold the features of one move in both
+ * orders) with xt = x transposed ([1280][ldxt] BF16).  The loss is the mean over pairs of
+ * ((y(2p) - y(2p+1))/2 - target[row0/2 + p])^2; *loss_out (device, may be null) receives the
+ * summed squared error of the batch. */
+int epsr_mlp_train_step(const epsr_mlp_t *net, const void *x, const void *xt, int64_t ldxt, int32_t row0,
+                        int32_t rows, const float *target, float lr, int32_t step, float *loss_out, void *work,
+                        int64_t work_bytes, void *stream);
+
+/* ------------------------------------------------------------------ kernel timing
+ * For measurement; no counterpart in the reference.  While enabled, the library brackets each
+ * launch of its main kernels (spec_energy_kernel, spec_corr_kernel, spec_resolve_kernel,
+ * molfit_seq_kernel, fm_count_kernel, ag_inter_kernel, fitexp_cluster_kernel) with CUDA events
+ * recorded on the launch stream.  epsr_timing_enable(1) clears earlier records and starts;
+ * epsr_timing_enable(0) stops.  epsr_timing_read waits for the recorded events of one kernel
+ * and returns the summed device time and the launch count.  Records are shared by all host
+ * threads of the process. */
+int epsr_timing_enable(int32_t on);
+int epsr_timing_read(const char *kernel, double *total_ms, int64_t *launches);
+
 /* ------------------------------------------------------------------ atogen */
 /* atogen ato_manipulation_rev4.py:3640-3899 (no coarse graining, no container forces).
  * wav: device [2*npairs*ldw] (wav(1,iz,ic) at [ic*ldw+iz], wav(2,..) at [(npairs+ic)*ldw+iz]),

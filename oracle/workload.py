@@ -43,8 +43,12 @@ class CpuIteration:
                             "xavtot1": (b.ecoul1 + b.xavs1).astype(f32)}
             self.ep_par = np.array([ep.absolute_energy, ep.erequnit, ep.ereqstep, ep.potfacamp], f32)
 
-    def step(self, stages=None):
+    def step(self, stages=None, sample_sweeps=None):
+        """One iteration.  sample_sweeps: run only that many of the iteration's molfit sweeps
+        and charge the molfit stage their mean time x the iteration's sweep count (a bounded
+        sample of a long iteration; stage_s then holds the extrapolated iteration)."""
         wl, b = self.wl, self.box
+        nsw = wl.ntimes if not sample_sweeps else max(1, min(int(sample_sweeps), wl.ntimes))
         t = {}
         t0 = time.perf_counter()
         cells = oracle.cell_list(b, wl.nmolcell, b.sepmax)
@@ -56,8 +60,9 @@ class CpuIteration:
             model = configs.intra_model(wl.system)
         st = oracle.fmolec1(b, cells, wl.eintra if model is None else oracle.en_mole_intra_all(b, model))
         t["fmolec1"] = time.perf_counter() - t0
+        self.cells, self.st = cells, st
         t0 = time.perf_counter()
-        for _ in range(wl.ntimes):
+        for _ in range(nsw):
             if model is not None and self.nisum_mc >= wl.intra:
                 # molfit's intramolecular branch, then runepsr17's minimage and store rebuild
                 self.fadds, self.faddbs, _, self.ergold1, self.ran1 = oracle.molfit_shake(
@@ -68,7 +73,8 @@ class CpuIteration:
             else:
                 _, _, self.ran1 = oracle.molfit(b, cells, st, self.mc, self.ran1, record_cos=False)
                 self.nisum_mc += 1
-        t["molfit"] = time.perf_counter() - t0
+        t["molfit"] = (time.perf_counter() - t0) * (wl.ntimes / nsw)
+        self.sampled_sweeps = nsw
         if stages == "mc":
             self.stage_s = t
             return
@@ -76,11 +82,15 @@ class CpuIteration:
         wav, potex, ngr, self.ran1 = oracle.atogen(b, wl.ngrsamples, self.ran1, np.full(b.npairs, -2.0, f32),
                                                    ycoh=wl.ycoh)
         t["atogen"] = time.perf_counter() - t0
-        # pair-updates of a full (probaccept >= 1) histogram: intra pairs + all inter pairs
+        # pair-updates: a full (probaccept >= 1) histogram visits every atom pair once; a sampled
+        # one visits, per origin molecule, its atoms against every other atom (counted here
+        # with the mean molecule size), plus the intramolecular pairs of every molecule
         n_at = b.natom
         intra = int(sum(int(n) * (int(n) - 1) // 2 for n in b.nato))
-        self.pair_updates = n_at * (n_at - 1) // 2 if ngr >= b.nmol else 0
-        self.pair_updates = self.pair_updates if self.pair_updates else intra
+        if ngr >= b.nmol:
+            self.pair_updates = n_at * (n_at - 1) // 2
+        else:
+            self.pair_updates = intra + int(ngr * (n_at / b.nmol) * n_at)
         t0 = time.perf_counter()
         nq = wl.nq
         sofq = oracle.gensq(nq, b.npt1, wav, self.rows, wl.ycoh[: b.npt + 1], b.n2extr, np.ones(b.ntype, f32))
@@ -132,3 +142,8 @@ class CpuIteration:
                     np.full(b.npairs, nq, np.int32), wl.xwt)
         t["stog"] = time.perf_counter() - t0
         self.stage_s = t
+
+    def sweep(self):
+        """One molfit sweep on the cell list and store of the last step (the reference does not
+        rebuild them between the sweeps of an iteration)."""
+        _, _, self.ran1 = oracle.molfit(self.box, self.cells, self.st, self.mc, self.ran1, record_cos=False)
