@@ -71,6 +71,11 @@ def parse():
                     help="independent boxes per GPU (one stream each; default 2 at C3, 16 at C2)")
     ap.add_argument("--sweeps", type=int, default=None, help="molfit sweeps per iteration (default 100 at C3, else 5)")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary C2 x 16 measurement")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned delayed-acceptance comparison on C5 (learned vs plain ESS/s)")
+    ap.add_argument("--c5-boxes", type=int, default=16, help="C5 boxes advanced together by the batched arms")
+    ap.add_argument("--c5-sweeps", type=int, default=200, help="timed sweeps of each C5 arm")
+    ap.add_argument("--c5-pairs", type=int, default=1000000, help="(features, beta dE) pairs the surrogate trains on")
     ap.add_argument("--strict", action="store_true", help="bit-identical sequential sums")
     ap.add_argument("--cpu-sample-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -452,6 +457,10 @@ def gpu_arm(a):
         del reps, its, it
         torch.cuda.empty_cache()
         secondary = secondary_c2(a)
+    learned = None
+    if rank == 0 and world == 1 and not a.no_learned:
+        torch.cuda.empty_cache()
+        learned = learned_c5(a)
 
     if rank == 0:
         b = wl.system
@@ -492,6 +501,8 @@ def gpu_arm(a):
         }
         if secondary is not None:
             line["secondary"] = secondary
+        if learned is not None:
+            line["learned_c5"] = learned
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a.config, a.cpu_sample_steps, a.intra, a.sweeps)
         print(json.dumps(line), flush=True)
@@ -702,112 +713,86 @@ def roofline(it, ktimes, a):
 
 
 def c4_arm(a):
-    """Configuration C4: 64 independent boxes of uneven size (300-30,000 atoms, water and SiO2,
-    298-1500 K).  A step is, for every box, its cell list, pair store (fmolec1), one molfit
-    sweep (the speculative cycle) and atogen over every origin (int64 histogram counts).  The
-    boxes are spread over host threads by size (longest first onto the least-loaded thread),
-    each thread driving its boxes in turn on its own stream; the threads advance through the K
-    steps independently, each box step preceded by an L2-flushing 256 MB write on its stream."""
-    import threading
-
+    """Configuration C4: 64 independent boxes of uneven size (300-30,000 atoms, water and
+    SiO2-like, 298-1500 K) advanced together by the batched checkerboard scheme.  A step is one
+    sweep of every box -- one CUDA graph launch whose kernels each cover every box (binning,
+    then per step one propose and one decide launch) -- and the partial g(r) histograms of every
+    box over all atom pairs (int64 counts, one launch).  Launch shapes come from the project's
+    autotuner.  Each step is preceded by a 256 MB L2-flushing write inside the timed region."""
     import numpy as np
     import torch
 
-    from epsr_python_translation_b200 import configs
-    from epsr_python_translation_b200.box import BoxArrays, Ran1State, trsteps
-    from epsr_python_translation_b200.device import DeviceBox
+    from epsr_python_translation_b200 import autotune, configs
+    from epsr_python_translation_b200.batch import BatchBoxes
+    from epsr_python_translation_b200.box import BoxArrays, Ran1State
     from oracle import oracle
     torch.cuda.set_device(0)
     systems = configs.c4_batch(seed=1)
-    nthreads = max(1, min(a.replicas, len(systems)))
-    order = sorted(range(len(systems)), key=lambda i: -systems[i].natom)
-    load, groups = [0] * nthreads, [[] for _ in range(nthreads)]
-    for i in order:
-        t = load.index(min(load))
-        groups[t].append(i)
-        load[t] += systems[i].natom
-    streams = [torch.cuda.Stream() for _ in range(nthreads)]
-    boxes = [None] * len(systems)
-    eintra = [configs.intra_energies(s) for s in systems]
-    for t in range(nthreads):
-        with torch.cuda.stream(streams[t]):
-            for i in groups[t]:
-                s = systems[i]
-                d = DeviceBox(BoxArrays.from_system(s))
-                tmax, tmin = trsteps(d.host.natomr)
-                nmt = s.nmoltype
-                d.mc_setup(rejrate=0.75, stepr=1.0, stepm=1.0, wholerot=np.full(nmt, 10.0 / 180.0, np.float32),
-                           wholetrans=np.full(nmt, 0.5, np.float32) / np.float32(s.dmax), ran1=Ran1State(idum=-(i + 1)),
-                           trstepmax=tmax, trstepmin=tmin)
-                boxes[i] = d
-    rminex = [torch.full((s.npairs,), -2.0, dtype=torch.float32, device="cuda") for s in systems]
-    flush = [torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") for _ in range(nthreads)]
-    pupd = [0] * len(systems)
-
-    def box_step(i, k, t):
-        d = boxes[i]
-        flush[t].fill_(float(k))
-        d.cell_list(10, d.host.sepmax)
-        d.fmolec1(eintra[i], strict=False)
-        d.molfit(strict=False)
-        d.atogen(0, d.m_ran1, rminex[i])
-        pupd[i] = d.last_pair_updates
-
-    def run(nsteps, k0):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        main = torch.cuda.current_stream()
-        e0.record(main)
-        errs = []
-
-        def worker(t):
-            try:
-                with torch.cuda.stream(streams[t]):
-                    streams[t].wait_event(e0)
-                    for k in range(nsteps):
-                        for i in groups[t]:
-                            box_step(i, k0 + k, t)
-            except Exception as e:   # reported below
-                errs.append(e)
-        th = [threading.Thread(target=worker, args=(t,)) for t in range(nthreads)]
-        for x in th:
-            x.start()
-        for x in th:
-            x.join()
-        if errs:
-            raise errs[0]
-        for s_ in streams:
-            main.wait_stream(s_)
-        e1.record(main)
-        e1.synchronize()
-        return e0.elapsed_time(e1)
-
-    run(max(3, a.warmup), 0)
+    bb = BatchBoxes(systems, rot_deg=10.0, trans_A=0.5, seed=1)
+    bb.total_energy()
+    choice = autotune.tune(bb, "plain")
+    g = bb.capture("plain")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for k in range(max(3, a.warmup)):
+        flush.fill_(float(k))
+        g.replay()
+        bb.histograms()
     torch.cuda.synchronize()
+    c0 = bb.counters.clone()
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     clocks = ClockSampler(vis.split(",")[0] if vis else "0")
     clocks.start()
     time.sleep(0.3)
-    ms = run(a.steps, 100)
+    import ctypes as C
+    bb.lib.epsr_timing_enable(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pairs = torch.zeros(1, dtype=torch.int64, device="cuda")
+    e0.record()
+    for k in range(a.steps):
+        flush.fill_(float(k))
+        g.replay()
+        _, hp = bb.histograms()
+        pairs += hp.sum()
+    e1.record()
+    torch.cuda.synchronize()
+    bb.lib.epsr_timing_enable(0)
+    ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    moves = sum(s.nmol for s in systems)
-    value = a.steps * moves / (ms / 1000.0)
-    pairs = sum(pupd)
-    fp32_peak = 148 * 128 * 1965.0e6
+    bb.check_status()
+    kt = {}
+    for kname in ("bmc_propose_kernel", "bmc_decide_kernel", "bmc_hist_inter_kernel"):
+        tms, n = C.c_double(0.0), C.c_int64(0)
+        bb.lib.epsr_timing_read(kname.encode(), C.byref(tms), C.byref(n))
+        if n.value:
+            kt[kname] = {"total_ms": round(tms.value, 3), "launches": int(n.value),
+                         "mean_us": round(1000 * tms.value / n.value, 2)}
+    cnt = (bb.counters - c0).cpu().numpy().reshape(bb.nbox, 4)
+    moves = int(cnt[:, 0].sum())
+    npairs = int(pairs.item())
+    value = moves / (ms / 1000.0)
+    hbm, fp32, mhz, src = _peaks()
+    hist_ms = kt.get("bmc_hist_inter_kernel", {}).get("total_ms", 0.0)
+    launches_per_step = 6 + 2 * bb.steps_per_sweep + 3
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (64 seeded boxes: water and SiO2-like, log-uniform sizes)",
+        "pair_updates_per_s": npairs / (ms / 1000.0),
         "config": {"workload": "c4_batch", "boxes": len(systems), "atoms": int(sum(s.natom for s in systems)),
                    "atoms_min_max": [int(min(s.natom for s in systems)), int(max(s.natom for s in systems))],
-                   "moves_per_step": moves, "host_threads": nthreads,
-                   "step": "every box: cell list, fmolec1, one molfit sweep, atogen over every origin",
-                   "l2": "flushed before every box step by a 256 MB write on its stream, inside the timed region",
-                   "deviation": "boxes on concurrent streams, not one persistent launch per sweep"},
-        "pair_updates_per_s": a.steps * pairs / (ms / 1000.0),
-        "fp32_issue_atogen_lower_bound": {"achieved_Tops": 17.0 * a.steps * pairs / (ms / 1000.0) / 1e12,
-                                          "peak_Tops": fp32_peak / 1e12, "ops_per_pair_update": 17,
-                                          "note": "whole step time charged to atogen's 17 FP32 ops per pair-update"},
-        "roofline": None, "clocks": clk,
+                   "moves_per_step": moves // a.steps, "steps_per_sweep": bb.steps_per_sweep,
+                   "launches_per_step": launches_per_step, "launches_depend_on_box_count": False,
+                   "autotuned": {"threads": choice["threads"], "hist_tile": choice["tile"]},
+                   "step": "one graph launch per sweep of every box (checkerboard scheme) + all-pairs g(r) "
+                           "histograms of every box (int64 counts) in one launch",
+                   "l2": "flushed before every step by a 256 MB write, inside the timed region"},
+        "acceptance": float(cnt[:, 2].sum() / max(moves, 1)), "kernel_ms": kt,
+        "roofline": {"bound": "fp32", "kernel": "bmc_hist_inter_kernel",
+                     "achieved": (OPS_PER_PAIR_UPDATE * npairs / (hist_ms / 1000.0) / 1e12) if hist_ms else None,
+                     "peak": fp32, "unit": "Tops/s (FP32 issue)",
+                     "frac": (OPS_PER_PAIR_UPDATE * npairs / (hist_ms / 1000.0) / 1e12 / fp32) if hist_ms else None,
+                     "traffic": None, "peak_source": "nominal (148 SMs x 128 lanes x %.0f MHz)" % mhz},
+        "gpu_launches": launches_per_step * a.steps, "clocks": clk,
     }
     if not a.no_cpu_baseline:
         small = sorted(range(len(systems)), key=lambda i: systems[i].natom)[:4]
@@ -817,19 +802,127 @@ def c4_arm(a):
             s = systems[i]
             ob = BoxArrays.from_system(s)
             oc = oracle.cell_list(ob, 10, ob.sepmax)
-            st = oracle.fmolec1(ob, oc, eintra[i])
+            st = oracle.fmolec1(ob, oc, configs.intra_energies(s))
             nmt = s.nmoltype
             omc = dict(rejrate=np.float32(0.75), stepr=np.float32(1.0), stepm=np.float32(1.0),
                        wholerot=np.full(nmt, 10.0 / 180.0, np.float32),
                        wholetrans=np.full(nmt, 0.5, np.float32) / np.float32(s.dmax), internrot=np.zeros(nmt, np.float32),
                        interntrans=np.zeros(nmt, np.float32), ireset=0)
             _, _, r = oracle.molfit(ob, oc, st, omc, Ran1State(idum=-(i + 1)), record_cos=False)
-            oracle.atogen(ob, 0, r, np.full(s.npairs, -2.0, np.float32))
+            oracle.atogen(ob, s.nmol, r, np.full(s.npairs, -2.0, np.float32))
             mv += s.nmol
         wall = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": mv / wall, "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": f"one step (cell list, fmolec1, sweep, full atogen) of the 4 smallest boxes "
-                                          f"({mv} molecules), single-threaded C oracle"}
+                                "sample": f"one step (cell list, fmolec1, one reference-order sweep, all-pairs atogen) "
+                                          f"of the 4 smallest boxes ({mv} molecules), single-threaded C oracle"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def learned_c5(a, steps=None):
+    """Configuration C5 (2,700 DMSO + 5,300 water, 8,000 molecules): decorrelated moves per
+    second of (1) the plain GPU path in the reference's visit order (the speculative molfit
+    cycle on one box, the path the headline measures), (2) the plain single-stage test on
+    ``--c5-boxes`` boxes advanced together by the batched checkerboard scheme, one CUDA graph
+    per sweep, and (3) the same boxes with the learned delayed-acceptance first stage, its
+    network trained on the batched plain run's (features, beta dE) pairs by the tcgen05
+    kernels.  ESS of the total energy from its integrated autocorrelation time per box, summed
+    over boxes; every arm starts from the same equilibrated configuration."""
+    import numpy as np
+    import torch
+
+    from epsr_python_translation_b200 import configs
+    from epsr_python_translation_b200.box import BoxArrays, Ran1State, trsteps
+    from epsr_python_translation_b200.device import DeviceBox
+    from epsr_python_translation_b200.learned import RMSE_BOUND, LearnedMC, ess
+    nsw = a.c5_sweeps
+    s0 = configs.c5_learned(seed=1)
+    B = max(1, a.c5_boxes)
+    t0 = time.perf_counter()
+    lm = LearnedMC([s0] * B, rot_deg=10.0, trans_A=0.5, seed=11)
+    lm.run(100, "plain")                                       # equilibration from the random start
+    out = {"workload": "c5_learned", "nmol": s0.nmol, "natom": s0.natom, "boxes": B,
+           "grid": {"stride": lm.bb.grid[0][0], "ncell": lm.bb.grid[0][1], "moves_in_parallel_per_box":
+                    lm.bb.descs[0].nslot, "steps_per_sweep": lm.bb.steps_per_sweep},
+           "proposal": "rotation <= 10 deg about a random axis + translation <= 0.5 A (every arm)"}
+    # (2) batched plain
+    sp, ms_p, cp, _ = lm.run(nsw, "plain")
+    e_p, tau_p = ess(sp[1:])
+    mv_p = int(cp[:, 0].sum())
+    out["batched_plain"] = {"sweeps": nsw, "ms": ms_p, "moves_per_s": mv_p / (ms_p / 1e3),
+                            "acceptance": float(cp[:, 2].sum() / max(cp[:, 0].sum(), 1)),
+                            "left_cell": float(cp[:, 3].sum() / max(cp[:, 0].sum(), 1)),
+                            "tau_sweeps_median": float(np.median(tau_p)), "ess": float(e_p.sum()),
+                            "ess_per_s": float(e_p.sum() / (ms_p / 1e3))}
+    # (3) learned: record, train, run
+    tr0 = time.perf_counter()
+    x, t = lm.collect(a.c5_pairs)
+    torch.cuda.synchronize()
+    rec_s = time.perf_counter() - tr0
+    rep = lm.train(x, t, epochs=4, batch=2048, lr=1e-3)
+    del x, t
+    torch.cuda.empty_cache()
+    sd, ms_d, cd, mode = lm.run(nsw, "da")
+    e_d, tau_d = ess(sd[1:])
+    mv_d = int(cd[:, 0].sum())
+    out["learned"] = {"mode": mode, "sweeps": nsw, "ms": ms_d, "moves_per_s": mv_d / (ms_d / 1e3),
+                      "first_stage_accept": float(cd[:, 1].sum() / max(cd[:, 0].sum() - cd[:, 3].sum(), 1)),
+                      "acceptance": float(cd[:, 2].sum() / max(cd[:, 0].sum(), 1)),
+                      "tau_sweeps_median": float(np.median(tau_d)), "ess": float(e_d.sum()),
+                      "ess_per_s": float(e_d.sum() / (ms_d / 1e3)),
+                      "training": {k: v for k, v in rep.items()}, "record_s": rec_s,
+                      "heldout_bound_kT": RMSE_BOUND, "residual_rmse_last_step_kT": lm.residual_rmse()}
+    # (1) the reference-order plain GPU path on one box from box 0's configuration
+    co = lm.bb.download()
+    ms_, as_ = lm.bb.box_slices(0)
+    box = BoxArrays.from_system(s0)
+    for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+        getattr(box, k)[:] = co[k][as_ if k in ("xa", "ya", "za") else ms_]
+    d = DeviceBox(box)
+    d.cell_list(10, box.sepmax)
+    d.fmolec1(configs.intra_energies(s0), strict=False)
+    tmax, tmin = trsteps(box.natomr)
+    nmt = box.nmoltype
+    d.mc_setup(rejrate=np.float32(0.75), stepr=1.0, stepm=1.0, wholerot=np.full(nmt, 10.0 / 180.0, np.float32),
+               wholetrans=np.full(nmt, 0.5, np.float32) / np.float32(s0.dmax), ran1=Ran1State(idum=-5),
+               trstepmax=tmax, trstepmin=tmin)
+    nref = max(20, nsw // 4)
+    for _ in range(5):
+        d.molfit(strict=False)
+    ser = torch.zeros(nref, dtype=torch.float32, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(nref):
+        d.molfit(strict=False)
+        ser[i] = d.m_fadds[0]
+    e1.record()
+    torch.cuda.synchronize()
+    d.check_status()
+    ms_r = e0.elapsed_time(e1)
+    e_r, tau_r = ess(ser.cpu().numpy().astype(np.float64)[:, None])
+    out["reference_order_plain"] = {"boxes": 1, "sweeps": nref, "ms": ms_r, "moves_per_s": nref * s0.nmol / (ms_r / 1e3),
+                                    "tau_sweeps": float(tau_r[0]), "ess": float(e_r.sum()),
+                                    "ess_per_s": float(e_r.sum() / (ms_r / 1e3)),
+                                    "note": "the speculative molfit cycle, fast sums, adaptive steps as molfit"}
+    base = out["reference_order_plain"]["ess_per_s"]
+    out["learned_vs_plain_ess_per_s"] = out["learned"]["ess_per_s"] / base if base > 0 else None
+    out["batched_plain_vs_plain_ess_per_s"] = out["batched_plain"]["ess_per_s"] / base if base > 0 else None
+    out["learned_vs_batched_plain_ess_per_s"] = (out["learned"]["ess_per_s"] / out["batched_plain"]["ess_per_s"]
+                                                 if out["batched_plain"]["ess_per_s"] > 0 else None)
+    out["wall_s"] = time.perf_counter() - t0
+    return out
+
+
+def c5_arm(a):
+    import torch
+    torch.cuda.set_device(0)
+    r = learned_c5(a)
+    line = {"metric": "ESS/s of total energy (learned delayed-acceptance vs plain)", "value": r["learned"]["ess_per_s"],
+            "unit": "effective samples/s", "n_gpus": 1, "steps": a.c5_sweeps, "warmup": 100,
+            "ms_per_step": r["learned"]["ms"] / a.c5_sweeps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (surrogate bf16/f32)", "data": "synthetic (seeded c5_learned boxes)",
+            "config": {"workload": "c5_learned", "boxes": r["boxes"]}, "c5": r}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -840,6 +933,8 @@ def main():
         return reference_arm(a)
     if a.config == "c4_batch":
         return c4_arm(a)
+    if a.config == "c5_learned":
+        return c5_arm(a)
     return gpu_arm(a)
 
 

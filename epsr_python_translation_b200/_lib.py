@@ -138,6 +138,7 @@ _SIGS = {
     "epsr_bmc_decide": (C.c_int, [P, I32, I32, P, P, P]),
     "epsr_bmc_end_sweep": (C.c_int, [P, P]),
     "epsr_bmc_total_energy": (C.c_int, [P, P]),
+    "epsr_bmc_histograms": (C.c_int, [P, P, I64, P]),
     "epsr_mlp_work_bytes": (I64, [I32]),
     "epsr_mlp_sync_weights": (C.c_int, [C.POINTER(Mlp), P]),
     "epsr_mlp_forward": (C.c_int, [C.POINTER(Mlp), P, I32, P, P, I64, P]),

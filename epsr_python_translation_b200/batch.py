@@ -23,12 +23,19 @@ import torch
 
 from . import _lib
 from ._lib import check
-from .device import table_cutoff
 
 f32 = np.float32
 FEAT_IN = 1280
 FEAT_RMAX_A = 8.0
-ELEMENT_CLASS = {"S": 0, "Si": 0, "C": 1, "N": 1, "O": 2, "OW": 2, "H": 3, "HW": 3}
+FIRST_LETTER_CLASS = {"S": 0, "C": 1, "N": 1, "O": 2, "H": 3}
+
+
+def element_class(label):
+    """Feature class of an atom label by its element: S and Si 0, C and N 1, O 2, H 3 (others 1);
+    the ten unordered class pairs are the features' pair types."""
+    if label.startswith("Si"):
+        return 0
+    return FIRST_LETTER_CLASS.get(label[:1].upper(), 1)
 
 
 class BoxDesc(C.Structure):
@@ -37,14 +44,15 @@ class BoxDesc(C.Structure):
                 ("nslot", C.c_int32), ("tab0", C.c_int32), ("ld", C.c_int32), ("izcut", C.c_int32),
                 ("npairref0", C.c_int32), ("ntype", C.c_int32), ("xstar0", C.c_int32), ("nrange", C.c_int32),
                 ("nrange_feat", C.c_int32), ("stepcl", C.c_float), ("beta", C.c_float), ("dmax", C.c_float),
-                ("rint", C.c_float), ("rfeat", C.c_float), ("rotmax", C.c_float), ("transmax", C.c_float),
+                ("rint", C.c_float), ("rfeat", C.c_float), ("rfeat_c", C.c_float), ("rotmax", C.c_float),
+                ("transmax", C.c_float),
                 ("key0", C.c_uint32), ("key1", C.c_uint32), ("shift", C.c_float * 3), ("colour_off", C.c_int32),
                 ("sweep", C.c_int64)]
 
 
 class Bmc(C.Structure):
     _fields_ = [("nbox", C.c_int32), ("nmol", C.c_int32), ("natom", C.c_int32), ("ncell", C.c_int32),
-                ("nslot", C.c_int32), ("box", C.c_void_p), ("slot_box", C.c_void_p), ("mol_box", C.c_void_p),
+                ("nslot", C.c_int32), ("threads", C.c_int32), ("box", C.c_void_p), ("slot_box", C.c_void_p), ("mol_box", C.c_void_p),
                 ("naf", C.c_void_p), ("nato", C.c_void_p), ("fclass", C.c_void_p), ("xa", C.c_void_p),
                 ("ya", C.c_void_p), ("za", C.c_void_p), ("xadd", C.c_void_p), ("yadd", C.c_void_p),
                 ("zadd", C.c_void_p), ("pos", C.c_void_p), ("tab", C.c_void_p), ("xstar", C.c_void_p),
@@ -53,6 +61,15 @@ class Bmc(C.Structure):
                 ("slot_off", C.c_void_p), ("slot_centre", C.c_void_p), ("energy", C.c_void_p),
                 ("emol", C.c_void_p), ("counters", C.c_void_p), ("sweep_counter", C.c_void_p),
                 ("status", C.c_void_p)]
+
+
+class BmcHist(C.Structure):
+    _fields_ = [("nitems", C.c_int32), ("tile", C.c_int32), ("max_bins", C.c_int32), ("items", C.c_void_p),
+                ("hist0", C.c_void_p), ("wav0", C.c_void_p), ("npairs", C.c_void_p), ("npt1", C.c_void_p),
+                ("ldw", C.c_void_p), ("pair0", C.c_void_p), ("type0", C.c_void_p), ("n1extr", C.c_void_p),
+                ("n2extr", C.c_void_p), ("atom_mol", C.c_void_p), ("rminex", C.c_void_p), ("cfrac", C.c_void_p),
+                ("csampled", C.c_void_p), ("counts", C.c_void_p), ("wav", C.c_void_p), ("potex", C.c_void_p),
+                ("pairs", C.c_void_p)]
 
 
 def _p(t):
@@ -86,6 +103,30 @@ def choose_grid(R, transmax, max_stride=8):
     return None if best is None else (best[1], best[2])
 
 
+def value_cutoff(*tabs):
+    """Last grid index at which any table entry is nonzero in value (a -0 entry adds nothing to
+    an energy, so the interaction range ends before it)."""
+    last = 1
+    for t in tabs:
+        nz = np.nonzero(np.any(np.asarray(t, np.float32) != 0, axis=0))[0]
+        if nz.size:
+            last = max(last, int(nz[-1]))
+    return last
+
+
+def partition_boxes(natoms, world):
+    """Boxes split over `world` GPUs, greedily by atom count (the largest box next onto the
+    least-loaded rank): returns per rank the list of box indices, each in ascending order.
+    The boxes are independent, so the ranks need no exchange during a sweep."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(natoms)), key=lambda k: (-natoms[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += natoms[i]
+    return [sorted(p) for p in parts]
+
+
 def molecular_radius(s):
     """Largest distance of an atom from its molecule's centre (box units)."""
     r = np.sqrt(s.xa.astype(np.float64) ** 2 + s.ya.astype(np.float64) ** 2 + s.za.astype(np.float64) ** 2)
@@ -108,7 +149,7 @@ class BatchBoxes:
             L = float(s.L)
             dmax = float(s.dmax)
             ld = s.grid["npt"] + 1
-            izcut = min(table_cutoff(s.xavs, s.xavs1, s.ecoul, s.ecoul1), int(s.grid["npt2"]))
+            izcut = min(value_cutoff(s.xavs, s.xavs1, s.ecoul, s.ecoul1), int(s.grid["npt2"]))
             stepcl = f32(s.cellst) / f32(s.dmax)
             rc = (izcut + 1) * float(stepcl)          # no table entry beyond this distance (box units)
             rext = molecular_radius(s)
@@ -128,6 +169,7 @@ class BatchBoxes:
             d.stepcl, d.beta, d.dmax = float(stepcl), float(f32(1.0) / f32(s.simt)), dmax
             d.rint = R + math.sqrt(3.0) * transmax + 1e-6
             d.rfeat = FEAT_RMAX_A / dmax
+            d.rfeat_c = d.rfeat + 2.0 * rext + math.sqrt(3.0) * transmax + 1e-6
             d.rotmax, d.transmax = math.radians(rot_deg), transmax
             d.key0 = (0x9E3779B1 * (seed + 1) + 0x7F4A7C15 * b) & 0xFFFFFFFF
             d.key1 = (0x85EBCA6B * (b + 1) ^ (seed * 0xC2B2AE35)) & 0xFFFFFFFF
@@ -139,7 +181,7 @@ class BatchBoxes:
             naf.append(s.naf + atom0)
             nato.append(s.nato)
             itype.append(s.itype)
-            fclass.append(np.array([ELEMENT_CLASS.get(s.type_labels[t], 1) for t in s.itype], np.int32))
+            fclass.append(np.array([element_class(s.type_labels[t]) for t in s.itype], np.int32))
             xa.append(s.xa), ya.append(s.ya), za.append(s.za)
             xadd.append(s.xadd), yadd.append(s.yadd), zadd.append(s.zadd)
             slot_box.append(np.full(d.nslot, b, np.int32))
@@ -192,6 +234,7 @@ class BatchBoxes:
         self.status = z(1, torch.int32)
         c = Bmc()
         c.nbox, c.nmol, c.natom, c.ncell, c.nslot = self.nbox, self.nmol, self.natom, self.ncell, self.nslot
+        c.threads = 256
         for k in ("slot_box", "mol_box", "naf", "nato", "fclass", "xa", "ya", "za", "xadd", "yadd", "zadd", "pos",
                   "tab", "xstar", "npairref", "cell_start", "cell_mols", "mol_cell", "slot_mol", "slot_new",
                   "slot_off", "slot_centre", "energy", "emol", "counters", "sweep_counter", "status"):
@@ -271,6 +314,73 @@ class BatchBoxes:
             self.sweep(mode, net)
         self.graphs[mode] = g
         return g
+
+    def histograms(self, rminex=-2.0, tile=None):
+        """Every box's partial g(r) histograms over all atom pairs in one launch (integer counts,
+        normalised as atogen with every molecule an origin).  Returns per box (wav [2][npairs][ld],
+        potex [npairs]) as device tensor views and the pair-updates counted."""
+        tile = tile or getattr(self, "hist_tile", 1024)
+        if getattr(self, "_hist", None) is None or self._hist.tile != tile:
+            self._hist_setup(rminex, tile)
+        check(self.lib.epsr_bmc_histograms(C.byref(self.c), C.byref(self._hist), self.h_counts.numel(), _stream()))
+        out = []
+        for b, s in enumerate(self.systems):
+            ld = s.grid["npt"] + 1
+            w0 = int(self._wav0[b])
+            out.append((self.h_wav[w0:w0 + 2 * s.npairs * ld].view(2, s.npairs, ld),
+                        self.h_potex[int(self._pair0[b]):int(self._pair0[b]) + s.npairs]))
+        return out, self.h_pairs
+
+    def _hist_setup(self, rminex, tile):
+        items, hist0, wav0, npairs, npt1, ldw, pair0, type0 = [], [], [], [], [], [], [], []
+        n1, n2, rmx, cfrac, csam = [], [], [], [], []
+        h0 = w0 = p0 = t0 = 0
+        max_bins = 1
+        for b, s in enumerate(self.systems):
+            ld = s.grid["npt"] + 1
+            if s.npairs > 64:
+                raise _lib.EpsrGpuError(4, "histograms: at most 64 pair types per box")
+            for t_ in range(0, s.natom, tile):
+                for o_ in range(0, s.natom, 256):
+                    items.append((b, t_, o_))
+            hist0.append(h0)
+            wav0.append(w0)
+            npairs.append(s.npairs)
+            npt1.append(int(s.grid["npt1"]))
+            ldw.append(ld)
+            pair0.append(p0)
+            type0.append(t0)
+            n1.append(s.n1extr)
+            n2.append(s.n2extr)
+            rmx.append(np.full(s.npairs, rminex, f32))
+            cfrac.append(s.cfrac.astype(f32))
+            last = s.naf[-1]            # atoms of molecules 0..nmol-2 (the origins of atogen's full sampling)
+            cs = np.bincount(s.itype[:last], minlength=s.ntype).astype(f32)
+            csam.append(cs)
+            max_bins = max(max_bins, s.npairs * ld + s.npairs)
+            h0 += 2 * s.npairs * ld + s.npairs
+            w0 += 2 * s.npairs * ld
+            p0 += s.npairs
+            t0 += s.ntype
+        t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(self.dev)  # noqa: E731
+        self._h_items = t(np.array(items, np.int32).reshape(-1), np.int32)
+        self._h_arrays = [t(hist0, np.int32), t(wav0, np.int32), t(npairs, np.int32), t(npt1, np.int32),
+                          t(ldw, np.int32), t(pair0, np.int32), t(type0, np.int32), t(np.concatenate(n1), np.int32),
+                          t(np.concatenate(n2), np.int32), t(np.repeat(np.arange(self.nmol),
+                                                                     self.nato.cpu().numpy()), np.int32),
+                          t(np.concatenate(rmx), f32), t(np.concatenate(cfrac), f32), t(np.concatenate(csam), f32)]
+        self._wav0, self._pair0 = wav0, pair0
+        self.h_counts = torch.zeros(max(h0, 1), dtype=torch.int64, device=self.dev)
+        self.h_wav = torch.zeros(max(w0, 1), dtype=torch.float32, device=self.dev)
+        self.h_potex = torch.zeros(max(p0, 1), dtype=torch.float32, device=self.dev)
+        self.h_pairs = torch.zeros(self.nbox, dtype=torch.int64, device=self.dev)
+        h = BmcHist()
+        h.nitems, h.tile, h.max_bins = len(items), tile, max_bins
+        h.items = _p(self._h_items)
+        (h.hist0, h.wav0, h.npairs, h.npt1, h.ldw, h.pair0, h.type0, h.n1extr, h.n2extr, h.atom_mol, h.rminex,
+         h.cfrac, h.csampled) = (_p(x) for x in self._h_arrays)
+        h.counts, h.wav, h.potex, h.pairs = _p(self.h_counts), _p(self.h_wav), _p(self.h_potex), _p(self.h_pairs)
+        self._hist = h
 
     def counters_host(self):
         return self.counters.cpu().numpy().reshape(self.nbox, 4)

@@ -405,6 +405,15 @@ def c3_water(seed=1, nmol=20000, rho_atoms=0.1):
                         ep_coeffs=30, min_heavy=2.5)
 
 
+def c5_learned(seed=1, ndmso=2700, nwater=5300, rho_atoms=0.1, ep_coeffs=30):
+    """Configuration C5: 2,700 DMSO + 5,300 water (8,000 molecules, 42,900 atoms, L = 75.4 A)
+    at 0.1 atoms/A^3, T = 298 K, 30-term seeded EP -- the box of the delayed-acceptance runs."""
+    natom = 10 * ndmso + 3 * nwater
+    L = (natom / rho_atoms) ** (1.0 / 3.0)
+    return build_system("c5_learned", [dmso_template(), water_template()], [ndmso, nwater], L,
+                        temperature=298.0, seed=seed, ep_coeffs=ep_coeffs, min_heavy=2.0)
+
+
 def silica(seed=1, natom=300, rho_atoms=0.0662, temperature=1500.0):
     """Amorphous-SiO2-like box of single-atom molecules (Si +2 e / O -1 e)."""
     nsi = natom // 3
@@ -631,6 +640,7 @@ class Workload:
     ep: EpRefinement = None  # potential refinement after the fits (None: the EP stays fixed)
     intra: int = 0           # molfit cycles between intramolecular cycles (0: rigid molecules, none)
     stepmi: float = 1.0      # intramolecular step flag (> 0 moves the atoms of multi-atom molecules)
+    data_source: str = "analytic"   # where the data sets come from
 
     @property
     def nq(self):
@@ -638,7 +648,7 @@ class Workload:
 
 
 def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, ndata=None, ntimes=5, refine=True,
-                  intra=0):
+                  intra=0, data_source="auto"):
     """One iteration's inputs on a named configuration, 5 MC sweeps per iteration and a
     116-term Poisson-like EP basis.  C2 (c2_mixture): 200 DMSO + 400 water, three isotope
     data sets (deuterated, protiated, 50:50), Q to 30 A^-1 (600 points).  C3 (c3_water):
@@ -672,10 +682,19 @@ def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, nd
     for d in range(ndata):
         data[d, 1:] = (0.05 * np.sin(2.9 * qq[1:] + d) * np.exp(-0.05 * qq[1:])
                        + rng.normal(0, 0.005, size=nq)).astype(f32)
+    # the data sets the method produced under a perturbed potential (synthdata.py), when they
+    # have been generated for this box and Q grid; otherwise the analytic stand-in above
+    src = "analytic"
+    if data_source == "auto" and seed == 1:
+        from . import synthdata
+        got = synthdata.load(name)
+        if got is not None and got[1].shape[1] == nq + 1 and got[0].shape[1] == s.npairs:
+            w, data = got
+            src = "method under a perturbed potential (synthdata.py)"
     nmt = s.nmoltype
     wholerot = np.full(nmt, f32(10.0 / 180.0), dtype=f32)
     wholetrans = np.full(nmt, f32(0.5) / s.dmax, dtype=f32)
     xwt = np.linspace(0.5, 1.5, s.npairs).astype(f32)
     return Workload(name=name, system=s, eintra=intra_energies(s), q=q, foqols=F, ycoh=ycoh, expr=expr,
                     nterms=nterms, data=data, weights=w, wholerot=wholerot, wholetrans=wholetrans, ntimes=ntimes,
-                    xwt=xwt, ep=ep, intra=int(intra))
+                    xwt=xwt, ep=ep, intra=int(intra), data_source=src)

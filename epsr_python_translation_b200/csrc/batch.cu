@@ -300,9 +300,18 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_propose_kernel(epsr_bmc_t B, 
     const int mol = s_mol, na_ = s_n;
     const float rf = X.rfeat;
     const float binf = (float)FEAT_BINS / FEAT_RMAX * X.dmax;   // bins per box unit
+    const float mx = B.xadd[mol], my = B.yadd[mol], mz = B.zadd[mol];
+    const float rfc2 = __fmul_rn(X.rfeat_c, X.rfeat_c);
     for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
         const int jm = list[p];
         if (jm == mol) continue;
+        // no atom of a partner whose centre is beyond rfeat_c is within 8 A of an atom of the
+        // moved molecule, before or after the move
+        float dx = __fsub_rn(B.xadd[jm], mx), dy = __fsub_rn(B.yadd[jm], my), dz = __fsub_rn(B.zadd[jm], mz);
+        dx = __fsub_rn(dx, nint_f(dx));
+        dy = __fsub_rn(dy, nint_f(dy));
+        dz = __fsub_rn(dz, nint_f(dz));
+        if (__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)) > rfc2) continue;
         const int b0 = B.naf[jm], nb = B.nato[jm];
         for (int q = 0; q < nb; ++q) {
             const float4 pb = atom_pos(B, b0 + q);
@@ -506,6 +515,118 @@ __global__ void bmc_box_energy_kernel(epsr_bmc_t B) {
     B.energy[b] = e;
 }
 
+// ----------------------------------------------------------------- histograms (atogen, all origins)
+__global__ void bmc_hist_intra_kernel(epsr_bmc_t B, epsr_bmc_hist_t H) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= B.nmol) return;
+    const int b = B.mol_box[m];
+    const epsr_bmc_box_t &X = B.box[b];
+    const int a0 = B.naf[m], n = B.nato[m];
+    if (n <= 1) return;
+    Lattice L;
+    L.cubic = 1;
+    const int ld = H.ldw[b], npt1 = H.npt1[b];
+    unsigned long long *cnt = H.counts + H.hist0[b];
+    const int *pr = B.npairref + X.npairref0;
+    long long np = 0;
+    for (int ia = a0; ia < a0 + n - 1; ++ia) {
+        for (int ja = ia + 1; ja < a0 + n; ++ja) {
+            const int icref = pr[__float_as_int(((const float4 *)B.pos)[ia].w) * X.ntype +
+                                 __float_as_int(((const float4 *)B.pos)[ja].w)];
+            const float d = dist_f(L, __fsub_rn(B.xa[ia], B.xa[ja]), __fsub_rn(B.ya[ia], B.ya[ja]),
+                                   __fsub_rn(B.za[ia], B.za[ja]));
+            const int iz1 = nint_i(__fdiv_rn(d, X.stepcl)) + 2;
+            if (iz1 > 1 && iz1 <= npt1) atomicAdd(cnt + (size_t)icref * ld + iz1, 1ull);
+            ++np;
+        }
+    }
+    atomicAdd((unsigned long long *)(H.pairs + b), (unsigned long long)np);
+}
+
+__global__ void __launch_bounds__(256) bmc_hist_inter_kernel(epsr_bmc_t B, epsr_bmc_hist_t H) {
+    extern __shared__ unsigned char sm[];
+    const int it = blockIdx.x;
+    const int b = H.items[3 * it], t0 = H.items[3 * it + 1], o0 = H.items[3 * it + 2];
+    const epsr_bmc_box_t &X = B.box[b];
+    const int np = H.npairs[b], ld = H.ldw[b], npt1 = H.npt1[b];
+    const int nbins = np * ld;
+    unsigned int *hist = (unsigned int *)sm;
+    unsigned int *hpot = hist + nbins;
+    const size_t tp_off = ((sizeof(unsigned int) * ((size_t)H.max_bins)) + 15) & ~(size_t)15;
+    float4 *tp = (float4 *)(sm + tp_off);
+    int *tm = (int *)(tp + H.tile);
+    const int tn = min(H.tile, X.natom - t0);
+    for (int i = threadIdx.x; i < nbins + np; i += blockDim.x) hist[i] = 0;
+    const float4 *pos = (const float4 *)B.pos + X.atom0;
+    const int *amol = H.atom_mol + X.atom0;
+    for (int i = threadIdx.x; i < tn; i += blockDim.x) {
+        tp[i] = pos[t0 + i];
+        tm[i] = amol[t0 + i];
+    }
+    __syncthreads();
+    Lattice L;
+    L.cubic = 1;
+    const int o = o0 + threadIdx.x;
+    long long npairs_done = 0;
+    if (o < X.natom) {
+        const float4 p1 = pos[o];
+        const int im = amol[o];
+        const int *pr = B.npairref + X.npairref0 + __float_as_int(p1.w) * X.ntype;
+        const float *rmx = H.rminex + H.pair0[b];
+        for (int q = 0; q < tn; ++q) {
+            if (tm[q] <= im) continue;
+            const float4 p2 = tp[q];
+            const int icref = pr[__float_as_int(p2.w)];
+            // xx = x1 - x2 (ato_manipulation_rev4.py:3798)
+            const float d = dist_f(L, __fsub_rn(p1.x, p2.x), __fsub_rn(p1.y, p2.y), __fsub_rn(p1.z, p2.z));
+            const int iz1 = nint_i(__fdiv_rn(d, X.stepcl)) + 2;
+            if (iz1 > 1 && iz1 <= npt1) atomicAdd(hist + icref * ld + iz1, 1u);
+            if (__fmul_rn(d, X.dmax) < fabsf(rmx[icref])) atomicAdd(hpot + icref, 1u);
+            ++npairs_done;
+        }
+    }
+    npairs_done = (long long)warp_sum_d((double)npairs_done);
+    if ((threadIdx.x & 31) == 0 && npairs_done) atomicAdd((unsigned long long *)(H.pairs + b),
+                                                          (unsigned long long)npairs_done);
+    __syncthreads();
+    unsigned long long *cnt = H.counts + H.hist0[b];
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x)
+        if (hist[i]) atomicAdd(cnt + (size_t)nbins + i, (unsigned long long)hist[i]);
+    for (int i = threadIdx.x; i < np; i += blockDim.x)
+        if (hpot[i]) atomicAdd(cnt + (size_t)2 * nbins + i, (unsigned long long)hpot[i]);
+}
+
+// normalisation (:3857-3897) of box blockIdx.y, pair blockIdx.x
+__global__ void bmc_hist_norm_kernel(epsr_bmc_t B, epsr_bmc_hist_t H) {
+    const int b = blockIdx.y, ic = blockIdx.x;
+    const int np = H.npairs[b];
+    if (ic >= np) return;
+    const epsr_bmc_box_t &X = B.box[b];
+    const int ld = H.ldw[b], npt1 = H.npt1[b];
+    const int p0 = H.pair0[b], t0 = H.type0[b];
+    const int it = H.n1extr[p0 + ic], jt = H.n2extr[p0 + ic];
+    const float *cfrac = H.cfrac + t0, *csampled = H.csampled + t0;
+    float cprod = __fmul_rn(__fmul_rn(cfrac[it], cfrac[jt]), (float)X.natom);
+    float cprod2 = __fmul_rn(csampled[it], cfrac[jt]);
+    if (it != jt) {
+        cprod = __fmul_rn(cprod, 2.0f);
+        cprod2 = __fadd_rn(cprod2, __fmul_rn(csampled[jt], cfrac[it]));
+    }
+    const unsigned long long *cnt = H.counts + H.hist0[b];
+    float *wav = H.wav + H.wav0[b];
+    float *w1 = wav + (size_t)ic * ld, *w2 = wav + (size_t)(np + ic) * ld;
+    const unsigned long long *c1 = cnt + (size_t)ic * ld, *c2 = cnt + (size_t)(np + ic) * ld;
+    for (int iz = 1 + threadIdx.x; iz <= npt1; iz += blockDim.x) {
+        const float v1 = (float)(2ull * c1[iz]);
+        const float v2 = __fmul_rn((float)c2[iz], 2.0f);
+        w1[iz] = cprod > 0.0f ? __fdiv_rn(v1, cprod) : 0.0f;
+        w2[iz] = cprod2 > 0.0f ? __fdiv_rn(v2, cprod2) : 0.0f;
+    }
+    const unsigned long long pc = cnt[(size_t)2 * np * ld + ic];
+    if (threadIdx.x == 0) H.potex[p0 + ic] = cprod2 > 0.0f ? __fdiv_rn(__fmul_rn((float)pc, cfrac[jt]), cprod2)
+                                                           : (float)pc;
+}
+
 }  // namespace epsr
 
 using namespace epsr;
@@ -515,7 +636,8 @@ int check_bmc(const epsr_bmc_t *b, const char *who) {
     if (!b || !b->box || !b->slot_box || !b->mol_box || !b->naf || !b->nato || !b->fclass || !b->xa || !b->xadd ||
         !b->pos || !b->tab || !b->xstar || !b->npairref || !b->cell_start || !b->cell_mols || !b->mol_cell ||
         !b->slot_mol || !b->slot_new || !b->slot_off || !b->slot_centre || !b->energy || !b->counters ||
-        !b->sweep_counter || !b->status || b->nbox <= 0 || b->nmol <= 0 || b->nslot <= 0) {
+        !b->sweep_counter || !b->status || b->nbox <= 0 || b->nmol <= 0 || b->nslot <= 0 ||
+        (b->threads != 64 && b->threads != 128 && b->threads != 256)) {
         epsr_set_error("%s: null pointer or empty batch", who);
         return EPSR_ERR_ARG;
     }
@@ -550,7 +672,7 @@ extern "C" int epsr_bmc_propose(const epsr_bmc_t *b, int32_t step, void *x, void
     }
     cudaStream_t s = (cudaStream_t)stream;
     EPSR_TIMED("bmc_propose_kernel", s,
-               bmc_propose_kernel<<<b->nslot, BMC_THREADS, 0, s>>>(*b, step, (__nv_bfloat16 *)x));
+               bmc_propose_kernel<<<b->nslot, b->threads, 0, s>>>(*b, step, (__nv_bfloat16 *)x));
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
 }
@@ -564,7 +686,8 @@ extern "C" int epsr_bmc_decide(const epsr_bmc_t *b, int32_t step, int32_t mode, 
         return EPSR_ERR_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    EPSR_TIMED("bmc_decide_kernel", s, bmc_decide_kernel<<<b->nslot, BMC_THREADS, 0, s>>>(*b, step, mode, y, target));
+    EPSR_TIMED("bmc_decide_kernel", s,
+               bmc_decide_kernel<<<b->nslot, b->threads, 0, s>>>(*b, step, mode, y, target));
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
 }
@@ -587,6 +710,33 @@ extern "C" int epsr_bmc_total_energy(const epsr_bmc_t *b, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     bmc_mol_energy_kernel<<<b->nmol, BMC_THREADS, 0, s>>>(*b);
     bmc_box_energy_kernel<<<(b->nbox + 127) / 128, 128, 0, s>>>(*b);
+    EPSR_CUDA(cudaGetLastError());
+    return EPSR_OK;
+}
+
+extern "C" int epsr_bmc_histograms(const epsr_bmc_t *b, const epsr_bmc_hist_t *h, int64_t counts_len, void *stream) {
+    int rc = check_bmc(b, "epsr_bmc_histograms");
+    if (rc) return rc;
+    if (!h || !h->items || !h->hist0 || !h->wav0 || !h->npairs || !h->npt1 || !h->ldw || !h->pair0 || !h->type0 ||
+        !h->n1extr || !h->n2extr || !h->atom_mol || !h->rminex || !h->cfrac || !h->csampled || !h->counts || !h->wav ||
+        !h->potex || !h->pairs || h->nitems <= 0 || h->tile <= 0 || h->tile > 4096 || h->max_bins <= 0 ||
+        counts_len <= 0) {
+        epsr_set_error("epsr_bmc_histograms: null pointer or bad sizes");
+        return EPSR_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t shm = (((sizeof(unsigned int) * (size_t)h->max_bins) + 15) & ~(size_t)15) +
+                       (sizeof(float4) + sizeof(int)) * (size_t)h->tile;
+    if (shm > 220 * 1024) {
+        epsr_set_error("epsr_bmc_histograms: %zu bytes of shared histogram and tile", shm);
+        return EPSR_ERR_UNSUPPORTED;
+    }
+    if (shm > 48 * 1024) EPSR_SMEM_OPTIN(bmc_hist_inter_kernel);
+    EPSR_CUDA(cudaMemsetAsync(h->counts, 0, sizeof(unsigned long long) * (size_t)counts_len, s));
+    EPSR_CUDA(cudaMemsetAsync(h->pairs, 0, sizeof(long long) * (size_t)b->nbox, s));
+    bmc_hist_intra_kernel<<<(b->nmol + 127) / 128, 128, 0, s>>>(*b, *h);
+    EPSR_TIMED("bmc_hist_inter_kernel", s, bmc_hist_inter_kernel<<<h->nitems, 256, shm, s>>>(*b, *h));
+    bmc_hist_norm_kernel<<<dim3(64, b->nbox), 256, 0, s>>>(*b, *h);
     EPSR_CUDA(cudaGetLastError());
     return EPSR_OK;
 }

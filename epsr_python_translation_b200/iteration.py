@@ -177,6 +177,7 @@ class EpsrIteration:
                                              self.ran1, strict=self.strict, scratch=self._fit_scratch)
         self.pwtold = res["wtold"]
         self.stepp = res["stepr"]
+        self.chisq = res["chisq"]
         self.fit_trials = int(res["trials"].sum())
         self._mark("fit_expansion", True)
         self._mark("ep")

@@ -247,6 +247,7 @@ typedef struct {
     int32_t tab0, ld, izcut, npairref0, ntype, xstar0;   /* tables: float4 offset, ld, cutoff, pair map */
     int32_t nrange, nrange_feat;                 /* cells scanned on each side for energies / features */
     float stepcl, beta, dmax, rint, rfeat;       /* rint, rfeat: box units */
+    float rfeat_c;                               /* centre distance beyond which no feature pair exists */
     float rotmax, transmax;                      /* radians, box units */
     uint32_t key0, key1;                         /* Philox key */
     float shift[3];                              /* written by each sweep's binning */
@@ -256,6 +257,7 @@ typedef struct {
 
 typedef struct {
     int32_t nbox, nmol, natom, ncell, nslot;
+    int32_t threads;              /* threads per move's CTA in propose and decide: 64, 128 or 256 */
     epsr_bmc_box_t *box;          /* [nbox] */
     const int32_t *slot_box;      /* [nslot] box of each slot */
     const int32_t *mol_box;       /* [nmol] box of each molecule */
@@ -281,6 +283,28 @@ typedef struct {
     int64_t *sweep_counter;       /* [1] sweeps begun */
     int32_t *status;
 } epsr_bmc_t;
+
+/* Partial g(r) histograms of every box over all atom pairs (atogen ato_manipulation_rev4.py:
+ * 3640-3899 with every molecule an origin: intramolecular pairs once each (nint bin, weight 2
+ * at normalisation), intermolecular pairs jm > im, close contacts d*dmax < |rminex|), counted
+ * in 64-bit integers, then normalised in float32 as atogen does (:3857-3897, csampled = the
+ * atoms of molecules 0..nmol-2, addwav 2, ycoh 0).  One launch covers every box's pairs.
+ * Offsets are per box; types and pairs are box-local indices into the packed arrays; at most
+ * 64 pair types per box. */
+typedef struct {
+    int32_t nitems, tile, max_bins;  /* inter-pass work items, target atoms per item, shared bins per CTA */
+    const int32_t *items;            /* [nitems*3] box, first target atom, first origin atom (box-local) */
+    const int32_t *hist0;            /* [nbox] box's counts: [2][npairs][ldw] then potex [npairs] (uint64 units) */
+    const int32_t *wav0;             /* [nbox] box's wav: [2][npairs][ldw] (float units) */
+    const int32_t *npairs, *npt1, *ldw, *pair0, *type0;   /* [nbox] */
+    const int32_t *n1extr, *n2extr;  /* packed pair -> box-local types */
+    const int32_t *atom_mol;         /* [natom] molecule of each atom (packed index) */
+    const float *rminex, *cfrac, *csampled;   /* packed per pair / per type */
+    unsigned long long *counts;      /* zeroed inside */
+    float *wav, *potex;              /* outputs; potex [sum npairs] */
+    long long *pairs;                /* [nbox] pair-updates counted */
+} epsr_bmc_hist_t;
+int epsr_bmc_histograms(const epsr_bmc_t *b, const epsr_bmc_hist_t *h, int64_t counts_len, void *stream);
 
 /* Bin every box's centres for a new sweep (random shift and colour order per box). */
 int epsr_bmc_begin_sweep(const epsr_bmc_t *b, void *stream);

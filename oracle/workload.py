@@ -101,12 +101,16 @@ class CpuIteration:
         t0 = time.perf_counter()
         inter = sofq[1]
         dts = oracle.ptgnsq_difference(wl.data, wl.weights, inter)
+        chis = []
         for k in range(wl.data.shape[0]):
             dt = dts[k]
             res, self.ran1 = oracle.fit_expansion(dt, wl.expr, self.pwtold[k], self.stepp[k], 1, nq, 1, wl.nterms,
                                                   1000, 10, self.ran1)
             self.pwtold[k] = res["wtold"]
             self.stepp[k] = res["stepr"]
+            chis.append(float(res["chisq"]))
+        self.chisq = chis
+        self.wav, self.sofq = wav, sofq
         t["fit_expansion"] = time.perf_counter() - t0
         t0 = time.perf_counter()
         ep = wl.ep
