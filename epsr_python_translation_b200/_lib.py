@@ -49,7 +49,9 @@ class Mc(C.Structure):
                 ("trstepmin", F32), ("ireset", I32), ("wholerot", P), ("wholetrans", P), ("internrot", P),
                 ("interntrans", P), ("nwhole", P), ("nmovem", P), ("nstepreject", P), ("fadds", P), ("ran1", P),
                 ("cos_override", P), ("trace_den", P), ("trace_acc", P), ("strict", I32),
-                ("status", P)]
+                ("status", P), ("intra", P), ("rot_nrf", P), ("rot_nrl", P), ("rot_axis", P), ("rot_first", P),
+                ("rot_last", P), ("rot_atoms", P), ("stepri", F32), ("rotcycle", I32), ("ninter", P),
+                ("faddbs", P)]
 
 
 class Mlp(C.Structure):

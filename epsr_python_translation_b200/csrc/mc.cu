@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include "common.cuh"
+#include "intra.cuh"
 
 namespace epsr {
 
@@ -39,7 +40,44 @@ struct McDev {
     int use_smem;
     int32_t *status;
     const int32_t *run_if;  // when set, the kernel runs only if *run_if != 0
+    // internal rotations of rotational groups (molfit.py:295-360), when has_rot
+    int has_rot, rotcycle;
+    float stepri;
+    IntraDev I;
+    const int32_t *ngrot, *rot_nrf, *rot_nrl, *rot_axis, *rot_first, *rot_last, *rot_atoms;
+    int32_t *ninter;
+    float *faddbs;
 };
+
+// rotati molfit.py:589-660 after its angle: rotate the atoms of group ig about the axis from
+// its first axis atom to its second by the angle whose cosine and sine are cphi and sphi, on
+// the molecule's offsets x/y/z (local atom index = global - a0), in the reference's float
+// operation order (scapro, vecpro auxiliary_routines.py:231-244).
+__device__ __forceinline__ void rotati_d(const McDev &D, int a0, int ig, float cphi, float sphi, float *x, float *y,
+                                        float *z) {
+    const int k1 = D.rot_axis[2 * ig] - a0, k2 = D.rot_axis[2 * ig + 1] - a0;
+    float p1 = __fsub_rn(x[k2], x[k1]), p2 = __fsub_rn(y[k2], y[k1]), p3 = __fsub_rn(z[k2], z[k1]);
+    const float rab2 = __fadd_rn(__fadd_rn(__fmul_rn(p1, p1), __fmul_rn(p2, p2)), __fmul_rn(p3, p3));
+    if (!(rab2 > 0.0f)) return;
+    const float rab = __fsqrt_rn(rab2);
+    p1 = __fdiv_rn(p1, rab);
+    p2 = __fdiv_rn(p2, rab);
+    p3 = __fdiv_rn(p3, rab);
+    for (int ia = D.rot_first[ig]; ia <= D.rot_last[ig]; ++ia) {
+        const int k = D.rot_atoms[ia] - a0;
+        const float v1 = __fsub_rn(x[k], x[k1]), v2 = __fsub_rn(y[k], y[k1]), v3 = __fsub_rn(z[k], z[k1]);
+        const float frac = __fadd_rn(__fadd_rn(__fmul_rn(p1, v1), __fmul_rn(p2, v2)), __fmul_rn(p3, v3));
+        const float q1 = __fmul_rn(frac, p1), q2 = __fmul_rn(frac, p2), q3 = __fmul_rn(frac, p3);
+        const float r1 = __fsub_rn(v1, q1), r2 = __fsub_rn(v2, q2), r3 = __fsub_rn(v3, q3);
+        const float w1 = __fsub_rn(__fmul_rn(p2, r3), __fmul_rn(p3, r2));
+        const float w2 = __fsub_rn(__fmul_rn(p3, r1), __fmul_rn(p1, r3));
+        const float w3 = __fsub_rn(__fmul_rn(p1, r2), __fmul_rn(p2, r1));
+        const float xs = __fadd_rn(x[k1], q1), ys = __fadd_rn(y[k1], q2), zs = __fadd_rn(z[k1], q3);
+        x[k] = __fadd_rn(__fadd_rn(xs, __fmul_rn(r1, cphi)), __fmul_rn(w1, sphi));
+        y[k] = __fadd_rn(__fadd_rn(ys, __fmul_rn(r2, cphi)), __fmul_rn(w2, sphi));
+        z[k] = __fadd_rn(__fadd_rn(zs, __fmul_rn(r3, cphi)), __fmul_rn(w3, sphi));
+    }
+}
 
 __device__ __forceinline__ float next_cos(const McDev &D, int &kcos, float phi) {
     if (D.cos_override) return D.cos_override[kcos++];
@@ -52,8 +90,9 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
     __shared__ Ran1 R;
     __shared__ float4 mv[MC_MAXAT];
     __shared__ float nx[MC_MAXAT], ny[MC_MAXAT], nz[MC_MAXAT];
-    __shared__ int sh_im, sh_n, sh_acc, sh_bad;
-    __shared__ float sh_cx, sh_cy, sh_cz;
+    __shared__ float sx[MC_MAXAT], sy[MC_MAXAT], sz[MC_MAXAT];
+    __shared__ int sh_im, sh_n, sh_acc, sh_bad, sh_rot;
+    __shared__ float sh_cx, sh_cy, sh_cz, sh_fdiff;
     __shared__ double red[MC_THREADS / 32];
     if (D.run_if && *D.run_if == 0) return;
     float *ergnew = D.use_smem ? dyn : D.ergnew_g;
@@ -63,16 +102,66 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
     const float pi = 3.14159265358979323846f;
     const float rotstepmin = 1.0e-5f, rotstepmax = 1.0f;
     int kcos = 0;
-    float fadd = 0.0f;
+    float fadd = 0.0f, faddb = 0.0f;
+    // the reference's ergold(1) (molfit's work array): the first stored energy of the last
+    // molecule whose list was loaded, as updated by that molecule's accepted moves
+    float eold0 = 0.0f, p0 = 0.0f;
     if (tid == 0) {
         ran1_load(R, D.ran1);
         for (int k = 0; k < 2 * nmt; ++k) {
             D.nwhole[k] = 0;
             D.nmovem[k] = 0;
+            if (D.ninter) D.ninter[k] = 0;
         }
     }
     const float temp = __fdiv_rn(1.0f, D.simt);
     __syncthreads();
+    // en_change (molfit.py:806-919) of molecule sh_im at positions mv[] over its stored list:
+    // ergnew/ergold filled for slots 1.., the change summed in list order (strict) or in double
+    auto en_change_mv = [&](int im, int n) -> float {
+        const size_t row = (size_t)im * D.M;
+        const int nn = D.nergpairm[im];
+        double part = 0.0;
+        for (int inn = 1 + tid; inn < nn; inn += MC_THREADS) {
+            const int jm = D.molergpair[row + inn];
+            const int b0 = D.naf[jm], b1 = b0 + D.nato[jm];
+            float sume = 0.0f;
+            for (int ia = 0; ia < n; ++ia) {
+                const float4 p1 = mv[ia];
+                const int it = __float_as_int(p1.w);
+                for (int ja = b0; ja < b1; ++ja) {
+                    const float4 p2 = D.pos[ja];
+                    const int icref = __ldg(D.npairref + it * D.ntype + __float_as_int(p2.w));
+                    sume = __fadd_rn(sume, pair_energy(D.L, D.T, p1, p2, icref));
+                }
+            }
+            const float en = __fadd_rn(0.0f, sume);
+            const float eo = D.ergpair[D.ergpairref[row + inn] - 1];
+            ergnew[inn] = en;
+            ergold[inn] = eo;
+            part += (double)en - (double)eo;
+        }
+        float fdiff;
+        if (D.strict) {
+            __syncthreads();
+            if (tid == 0) {
+                float f = 0.0f;
+                for (int inn = 1; inn < nn; ++inn) f = __fsub_rn(__fadd_rn(f, ergnew[inn]), ergold[inn]);
+                red[0] = (double)f;
+            }
+            __syncthreads();
+            fdiff = (float)red[0];
+        } else {
+            part = warp_sum_d(part);
+            if ((tid & 31) == 0) red[tid >> 5] = part;
+            __syncthreads();
+            double t = 0.0;
+            for (int w = 0; w < MC_THREADS / 32; ++w) t += red[w];
+            fdiff = (float)t;
+        }
+        __syncthreads();
+        return fdiff;
+    };
     for (int v = 0; v < D.nmol; ++v) {
         if (tid == 0) {
             const int im = D.visit[v];
@@ -84,9 +173,97 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
             if (tid == 0 && D.status) D.status[0] = 1;
             return;
         }
+        // ---- internal rotations of the molecule's rotational groups (molfit.py:295-360)
         if (tid == 0) {
             const int im = D.visit[v];
             const int n = D.nato[im];
+            const int mt = D.mtype[im];
+            const size_t row = (size_t)im * D.M;
+            if (D.nergpairm[im] >= 1) eold0 = D.ergpair[D.ergpairref[row] - 1];   // make_neighbour_list_from_mols
+            const int ng = D.ngrot ? D.ngrot[im] : 0;
+            sh_rot = D.has_rot && D.stepri > 0.0f && ng > 0 && D.rotcycle;
+            sh_im = im;
+            sh_n = n;
+            if (sh_rot) {
+                if (D.internrot[mt] == 0.0f) D.internrot[mt] = rotstepmin;
+                D.ninter[mt]++;
+                const int a0 = D.naf[im];
+                for (int k = 0; k < n; ++k) {
+                    sx[k] = D.xa[a0 + k];
+                    sy[k] = D.ya[a0 + k];
+                    sz[k] = D.za[a0 + k];
+                    nx[k] = sx[k];
+                    ny[k] = sy[k];
+                    nz[k] = sz[k];
+                }
+                const float step = D.internrot[mt];
+                for (int ig = D.rot_nrf[im]; ig <= D.rot_nrl[im]; ++ig) {
+                    const float phi = __fmul_rn(__fmul_rn(pi, step), __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f));
+                    const float c = next_cos(D, kcos, phi);
+                    const float sp = fsign(__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(c, c))), phi);
+                    rotati_d(D, a0, ig, c, sp, nx, ny, nz);
+                }
+                const float cx = D.xadd[im], cy = D.yadd[im], cz = D.zadd[im];
+                for (int k = 0; k < n; ++k) {
+                    D.xa[a0 + k] = nx[k];   // the trial lives in the offsets, as the reference's
+                    D.ya[a0 + k] = ny[k];
+                    D.za[a0 + k] = nz[k];
+                    mv[k] = make_float4(__fadd_rn(nx[k], cx), __fadd_rn(ny[k], cy), __fadd_rn(nz[k], cz),
+                                        D.pos[a0 + k].w);
+                }
+            } else if (!D.ngrot || D.ngrot[im] == 0) {
+                D.internrot[mt] = 0.0f;
+            }
+        }
+        __syncthreads();
+        if (sh_rot) {
+            const int im = sh_im, n = sh_n;
+            const float fdiff = en_change_mv(im, n);
+            if (tid == 0) {
+                const int mt = D.mtype[im];
+                const int a0 = D.naf[im];
+                // en_change_intra: the new intramolecular energy against ergold(1)
+                const float enew0 = en_mole_intra_d(D.I, im, D.xa, D.ya, D.za);
+                const float fdiffb = __fsub_rn(enew0, eold0);
+                p0 = enew0;
+                const float ediff = __fmul_rn(__fadd_rn(fdiff, fdiffb), temp);
+                float etest;
+                if (ediff <= 0.0f) etest = 10.0f;
+                else if (ediff < 20.0f) etest = exp_r(-ediff);
+                else etest = 0.0f;
+                const int acc = ran1_next(R) < etest;
+                const size_t row = (size_t)im * D.M;
+                const int nn = D.nergpairm[im];
+                if (acc) {
+                    D.nstepreject[im] = 0;
+                    fadd = __fadd_rn(fadd, fdiff);
+                    faddb = __fadd_rn(faddb, fdiffb);
+                    eold0 = enew0;
+                    if (nn >= 1) D.ergpair[D.ergpairref[row] - 1] = enew0;
+                    for (int k = 0; k < n; ++k) D.pos[a0 + k] = mv[k];
+                } else {
+                    D.nstepreject[im]++;
+                    for (int k = 0; k < n; ++k) {
+                        D.xa[a0 + k] = sx[k];
+                        D.ya[a0 + k] = sy[k];
+                        D.za[a0 + k] = sz[k];
+                    }
+                    D.ninter[nmt + mt]++;
+                }
+                sh_acc = acc;
+            }
+            __syncthreads();
+            if (sh_acc) {
+                const size_t row = (size_t)im * D.M;
+                const int nn = D.nergpairm[im];
+                for (int inn = 1 + tid; inn < nn; inn += MC_THREADS) D.ergpair[D.ergpairref[row + inn] - 1] = ergnew[inn];
+            }
+            __syncthreads();
+        }
+        // ---- whole-molecule rotation and translation (molfit.py:362-448)
+        if (tid == 0) {
+            const int im = sh_im;
+            const int n = sh_n;
             const int a0 = D.naf[im];
             const int mt = D.mtype[im];
             for (int k = 0; k < n; ++k) {
@@ -147,51 +324,12 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
             sh_cx = cx;
             sh_cy = cy;
             sh_cz = cz;
-            sh_im = im;
-            sh_n = n;
         }
         __syncthreads();
         const int im = sh_im, n = sh_n;
         const size_t row = (size_t)im * D.M;
         const int nn = D.nergpairm[im];
-        double part = 0.0;
-        for (int inn = 1 + tid; inn < nn; inn += MC_THREADS) {
-            const int jm = D.molergpair[row + inn];
-            const int b0 = D.naf[jm], b1 = b0 + D.nato[jm];
-            float sume = 0.0f;
-            for (int ia = 0; ia < n; ++ia) {
-                const float4 p1 = mv[ia];
-                const int it = __float_as_int(p1.w);
-                for (int ja = b0; ja < b1; ++ja) {
-                    const float4 p2 = D.pos[ja];
-                    const int icref = __ldg(D.npairref + it * D.ntype + __float_as_int(p2.w));
-                    sume = __fadd_rn(sume, pair_energy(D.L, D.T, p1, p2, icref));
-                }
-            }
-            const float en = __fadd_rn(0.0f, sume);
-            const float eo = D.ergpair[D.ergpairref[row + inn] - 1];
-            ergnew[inn] = en;
-            ergold[inn] = eo;
-            part += (double)en - (double)eo;
-        }
-        float fdiff;
-        if (D.strict) {
-            __syncthreads();
-            if (tid == 0) {
-                float f = 0.0f;
-                for (int inn = 1; inn < nn; ++inn) f = __fsub_rn(__fadd_rn(f, ergnew[inn]), ergold[inn]);
-                red[0] = (double)f;
-            }
-            __syncthreads();
-            fdiff = (float)red[0];
-        } else {
-            part = warp_sum_d(part);
-            if ((tid & 31) == 0) red[tid >> 5] = part;
-            __syncthreads();
-            double t = 0.0;
-            for (int w = 0; w < MC_THREADS / 32; ++w) t += red[w];
-            fdiff = (float)t;
-        }
+        const float fdiff = en_change_mv(im, n);
         if (tid == 0) {
             const int mt = D.mtype[im];
             const float ediff = __fmul_rn(__fadd_rn(fdiff, 0.0f), temp);
@@ -203,6 +341,13 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
             if (acc) {
                 D.nstepreject[im] = 0;
                 fadd = __fadd_rn(fadd, fdiff);
+                // save_energies copies every slot, the first one included: after an internal
+                // rotation of this visit it holds the rotation's intramolecular energy even when
+                // that rotation was rejected (molfit.py:215, :419; ergpairreference.py:192-210)
+                if (sh_rot) {
+                    eold0 = p0;
+                    if (nn >= 1) D.ergpair[D.ergpairref[row] - 1] = p0;
+                }
             } else {
                 D.nstepreject[im]++;
                 if (D.stepr > 0.0f) D.nwhole[nmt + mt]++;
@@ -231,18 +376,26 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
         __syncthreads();
     }
     if (tid == 0) {
-        // step adaptation (molfit.py:465-536); nmovei and ninter are 0 in this branch
+        // step adaptation (molfit.py:465-536); nmovei is 0 in this branch
         if (D.ireset != 1) {
             for (int t = 0; t < nmt; ++t) {
                 float it = __fmul_rn(D.interntrans[t], 1.0f);
                 if (it > D.trstepmax) it = D.trstepmax;
                 if (it < D.trstepmin && it != 0.0f) it = D.trstepmin;
                 D.interntrans[t] = it;
-                float ir = __fmul_rn(D.internrot[t], 1.0f);
+                float rat;
+                const int ni1 = D.ninter ? D.ninter[t] : 0, ni2 = D.ninter ? D.ninter[nmt + t] : 0;
+                if (ni2 > 0) {
+                    rat = __fdiv_rn(__fmul_rn(D.rejrate, (float)ni1), (float)ni2);
+                    if (rat > 1.1f) rat = 1.1f;
+                    if (rat < 0.9f) rat = 0.9f;
+                } else {
+                    rat = ni1 > 0 ? 1.1f : 1.0f;
+                }
+                float ir = __fmul_rn(D.internrot[t], rat);
                 if (ir > rotstepmax) ir = rotstepmax;
                 if (ir < rotstepmin && ir != 0.0f) ir = rotstepmin;
                 D.internrot[t] = ir;
-                float rat;
                 if (D.nwhole[nmt + t] > 0) {
                     rat = __fdiv_rn(__fmul_rn(D.rejrate, (float)D.nwhole[t]), (float)D.nwhole[nmt + t]);
                     if (rat > 1.1f) rat = 1.1f;
@@ -268,8 +421,10 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
             }
         }
         D.fadds[0] = __fadd_rn(D.fadds[0], __fdiv_rn(fadd, (float)D.nmol));
+        if (D.faddbs) D.faddbs[0] = __fadd_rn(D.faddbs[0], __fdiv_rn(faddb, (float)D.nmol));
         ran1_store(R, D.ran1);
     }
+    (void)sh_fdiff;
 }
 
 // en_change for one molecule at its current coordinates (no move)
@@ -409,6 +564,26 @@ int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_sto
     D.trace_acc = mc->trace_acc;
     D.status = mc->status;
     D.run_if = run_if;
+    D.faddbs = mc->faddbs;
+    if (mc->intra) {
+        const epsr_intra_t *in = (const epsr_intra_t *)mc->intra;
+        D.I = make_intradev(box, in);
+        D.ngrot = in->ngrot;
+        D.has_rot = mc->rot_nrf && mc->rot_nrl && mc->rot_axis && mc->rot_first && mc->rot_last && mc->rot_atoms;
+        D.rot_nrf = mc->rot_nrf;
+        D.rot_nrl = mc->rot_nrl;
+        D.rot_axis = mc->rot_axis;
+        D.rot_first = mc->rot_first;
+        D.rot_last = mc->rot_last;
+        D.rot_atoms = mc->rot_atoms;
+        D.stepri = mc->stepri;
+        D.rotcycle = mc->rotcycle;
+        D.ninter = mc->ninter;
+        if (D.has_rot && !D.ninter) {
+            epsr_set_error("epsr_molfit: internal rotations need the ninter counters");
+            return EPSR_ERR_ARG;
+        }
+    }
     const size_t need = sizeof(float) * 2 * (size_t)(D.M > 0 ? D.M : 1);
     size_t shm = 0;
     if (need <= 160 * 1024) {
@@ -442,8 +617,10 @@ extern "C" int epsr_molfit(const epsr_box_t *box, const epsr_cells_t *cells, eps
         epsr_set_error("epsr_molfit: null pointer");
         return EPSR_ERR_ARG;
     }
-    if (mc->strict) return molfit_seq_launch(box, cells, store, mc, scratch, scratch_bytes, (cudaStream_t)stream,
-                                             nullptr);
+    // internal rotations (and the internrot rule that needs every molecule's ngrot) run in the
+    // sequential kernel
+    if (mc->strict || mc->intra)
+        return molfit_seq_launch(box, cells, store, mc, scratch, scratch_bytes, (cudaStream_t)stream, nullptr);
     return epsr_molfit_spec(box, cells, store, mc, scratch, scratch_bytes, stream);
 }
 

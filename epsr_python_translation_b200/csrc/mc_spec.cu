@@ -156,6 +156,9 @@ __global__ void spec_plan_kernel(SpecDev S) {
     // per-type first-visit initialisation (molfit.py:377-394): a type whose molecules rotate
     // starts at rotstepmin if its step is not positive; otherwise its step is set to 0
     for (int t = tid; t < S.nmoltype; t += blockDim.x) {
+        // no molecule of this path has rotational groups: every visited type's internrot is
+        // set to 0 (molfit.py:358-360)
+        if (S.cnt_type[t] > 0) S.internrot[t] = 0.0f;
         if (S.tries_rot[t] > 0) {
             if (S.rotstep[t] <= 0.0f) S.rotstep[t] = 1.0e-5f;
         }

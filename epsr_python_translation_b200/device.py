@@ -247,12 +247,31 @@ class DeviceBox:
         self.cmc = m
         return m
 
-    def molfit(self, strict=True, cos_override=None):
+    def set_rotations(self, intra_model, nrf, nrl, axis, first, last, atoms, stepri=1.0, faddbs=0.0):
+        """Internal rotations of rotational groups (type ROT: the dihedral terms of DIH groups
+        are not evaluated) before each molecule's whole-molecule move, every rotfreq cycles
+        (molfit.py:295-360, rotati :589).  intra_model: intra.IntraModel of this box (its ngrot
+        per molecule); nrf/nrl per molecule (0-based group range, nrl < nrf for none); axis
+        (groups x 2) axis atoms, rotation about the first; first/last per group into atoms
+        (0-based atom indices).  faddbs: the running intramolecular energy change."""
+        t = lambda a: self._t(np.asarray(a).reshape(-1), np.int32)  # noqa: E731
+        self.r_model = intra_model
+        self.r_arrays = [t(nrf), t(nrl), t(axis), t(first), t(last), t(atoms)]
+        self.m_ninter = torch.zeros(2 * self.host.nmoltype, dtype=torch.int32, device=self.dev)
+        self.m_faddbs = self._t(np.array([faddbs], f32), f32)
+        m = self.cmc
+        m.intra = C.cast(C.pointer(intra_model.c), C.c_void_p)
+        m.rot_nrf, m.rot_nrl, m.rot_axis, m.rot_first, m.rot_last, m.rot_atoms = (_ptr(a) for a in self.r_arrays)
+        m.stepri = float(f32(stepri))
+        m.ninter, m.faddbs = _ptr(self.m_ninter), _ptr(self.m_faddbs)
+
+    def molfit(self, strict=True, cos_override=None, rotcycle=True):
         b = self.host
         if int(np.max(b.nato)) > 64:
             raise _lib.EpsrGpuError(4, "molfit: molecules of more than 64 atoms are not supported")
         m = self.cmc
         m.strict = 1 if strict else 0
+        m.rotcycle = 1 if rotcycle else 0
         self._cos = None
         if cos_override is not None:
             self._cos = self._t(cos_override, f32)

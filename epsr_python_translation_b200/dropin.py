@@ -350,7 +350,7 @@ class PairPath:
         mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
         b = self._sync_in()
         self._check_cells()
-        model = self._intra_model(b)
+        model = self._intra_model(b, allow_rot=self._rot_groups() is not None)
         if model is not None:
             # intramolecular energies (molfit.py:1327) on the device
             eintra = model.en_mole_intra()
@@ -368,16 +368,43 @@ class PairPath:
         nmol = f32(b.nmol)
         return 0, num_threads_input, f32(ft), f32(fb), f32(0.0) / nmol, f32(0.0) / nmol
 
-    def _intra_model(self, b):
+    def _rot_groups(self):
+        """The box's rotational groups as the device takes them -- (nrf, nrl, axis, first, last,
+        atoms), 0-based -- when every group is of type ROT with no dihedral angle (the dihedral
+        terms of DIH groups, en_mole_dihedral molfit.py:1353, are not on the device); () when no
+        molecule has groups; None otherwise."""
+        c = self.c
+        cc, mc = c.clustercom, c.molecom
+        nmol = int(cc.nmol)
+        ngrot = np.asarray(cc.ngrot[1:nmol + 1])
+        if not bool(np.any(ngrot > 0)):
+            return ()
+        mm = getattr(c, "molecom_mod", None)
+        if mm is None or getattr(mm, "labaxi", None) is None:
+            return None
+        ng = int(mm.ngrrot)
+        if any(str(mm.rotgrp[i]).strip() != "ROT" for i in range(1, ng + 1)):
+            return None
+        nd = getattr(mc, "ndihedralang", None)
+        if nd is not None and bool(np.any(np.asarray(nd[1:ng + 1]) > 0)):
+            return None
+        nrot = int(mm.nrottot)
+        return (np.asarray(cc.nrf[1:nmol + 1], np.int32) - 1, np.asarray(cc.nrl[1:nmol + 1], np.int32) - 1,
+                np.asarray(mm.labaxi)[1:ng + 1, 1:3].astype(np.int32) - 1,
+                np.asarray(mm.rotf[1:ng + 1], np.int32) - 1, np.asarray(mm.rotl[1:ng + 1], np.int32) - 1,
+                np.asarray(mm.labrot[1:nrot + 1], np.int32) - 1)
+
+    def _intra_model(self, b, allow_rot=False):
         """The device intramolecular model (en_atom_intra molfit.py:923) from molecom, or None
-        when a molecule has rotational groups (their dihedral terms and internal rotations stay
-        on the host) or the COMMON blocks carry no bond lists."""
+        when the COMMON blocks carry no bond lists, or when a molecule has rotational groups and
+        allow_rot is false (groups with dihedral terms stay on the host)."""
         from .intra import IntraModel
         c = self.c
         mc, cc, pp, e16 = c.molecom, c.clustercom, c.potential_par, c.epsr16
         nmol, natom, npairs = b.nmol, b.natom, b.npairs
+        ngrot = np.asarray(cc.ngrot[1:nmol + 1], np.int32)
         if getattr(mc, "nbond", None) is None or getattr(pp, "xav", None) is None or \
-                bool(np.any(np.asarray(cc.ngrot[1:nmol + 1]) > 0)):
+                (bool(np.any(ngrot > 0)) and not allow_rot):
             return None
         nb = np.asarray(mc.nbond[1:natom + 1], np.int32)
         mb = max(1, int(nb.max()) if natom else 1)
@@ -390,7 +417,7 @@ class PairPath:
                           xav=np.asarray(pp.xav)[:ld, 1:npairs + 1].T, xav1=np.asarray(pp.xav1)[:ld, 1:npairs + 1].T,
                           stepcl=f32(e16.cellst) / f32(mc.dmaxmol), simt=f32(mc.simt), sizefactor=f32(mc.sizefactor),
                           tempb=f32(mc.tempb), tempang=f32(mc.tempang), refine_intra=bool(getattr(mc, "refine_intra", False)),
-                          refine_intra_fac=f32(getattr(mc, "refine_intra_fac", 0.0)))
+                          refine_intra_fac=f32(getattr(mc, "refine_intra_fac", 0.0)), ngrot=ngrot)
 
     def molfit(self, fadds, faddbs, nisum, intra, rotfreq, ireset):
         """molfit.py:52-541: the whole-molecule branch and, for boxes without rotational groups,
@@ -398,15 +425,13 @@ class PairPath:
         c = self.c
         mc, cc = c.molecom, c.clustercom
         nmol = int(cc.nmol)
-        internal = False
-        if float(mc.stepri) > 0.0:
-            ngrot = np.asarray(cc.ngrot[1:nmol + 1])
-            internal = bool(np.any(ngrot > 0)) and nisum == rotfreq * _idiv(nisum, rotfreq)
+        groups = self._rot_groups()
+        rotcycle = nisum == rotfreq * _idiv(nisum, rotfreq)
         if nisum >= intra and not self._outside_path():
             r = self._molfit_intra(fadds, faddbs, ireset)
             if r is not None:
                 return r
-        if nisum >= intra or internal or self._outside_path():
+        if nisum >= intra or groups is None or self._outside_path():
             return self._host("molfit", fadds, faddbs, nisum, intra, rotfreq, ireset)
         b = self._sync_in()
         self._check_cells()
@@ -428,9 +453,12 @@ class PairPath:
                    trstepmax=tmax, trstepmin=tmin, ireset=int(ireset), fadds=f32(fadds))
         d.m_ran1 = self._ran1_in()
         d.cmc.ran1 = C.c_void_p(d.m_ran1.data_ptr())
+        if groups:
+            # internal rotations of the ROT groups every rotfreq cycles (molfit.py:295-360)
+            d.set_rotations(self._intra_model(b, allow_rot=True), *groups, stepri=f32(mc.stepri), faddbs=f32(faddbs))
         cos = self.cos_override
         self.cos_override = None
-        d.molfit(strict=self.strict or not self._mirror_ok, cos_override=cos)
+        d.molfit(strict=self.strict or not self._mirror_ok, cos_override=cos, rotcycle=rotcycle)
         d.check_status()
         out = d.download_mc()
         self._ran1_out(d.m_ran1)
@@ -441,7 +469,11 @@ class PairPath:
         cc.nstepreject[1:nmol + 1] = out["nstepreject"]
         self._coords_out()
         self._store_out(values_only=True)
-        faddbs = f32(faddbs) + f32(0.0) / f32(nmol)     # faddb stays 0 in the whole-molecule branch
+        if groups:
+            cc.ninter[1:3, 1:nmt + 1] = d.m_ninter.cpu().numpy().reshape(2, nmt)
+            faddbs = f32(d.m_faddbs.cpu().numpy()[0])
+        else:
+            faddbs = f32(faddbs) + f32(0.0) / f32(nmol)     # faddb stays 0 without internal rotations
         return out["fadds"], faddbs, nisum + 1
 
     def _molfit_intra(self, fadds, faddbs, ireset):

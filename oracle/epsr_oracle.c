@@ -637,115 +637,6 @@ static float movem(oracle_sys *S, int im, float stepsz, oracle_ran1_state *R) {
     return stepsz;
 }
 
-/* One molfit cycle, whole-molecule branch (molfit.py:268-448) plus step adaptation
- * (:465-536).  fadds is updated in place (molfit.py:538).  Returns 0. */
-int oracle_molfit(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_mcpar *P,
-                  oracle_ran1_state *R, float *fadds, oracle_trace *T) {
-    const int nmt = S->nmoltype;
-    const float temp = 1.0f / P->simt;
-    const float rotstepmax = 1.0f, rotstepmin = 1.0e-5f;
-    for (int k = 0; k < 2 * nmt; ++k) { P->nwhole[k] = 0; P->nmovem[k] = 0; }
-    float fadd = 0.0f;
-    const int M = E->nnbrefmax;
-    float *ergnew = (float *)malloc(sizeof(float) * (size_t)(M > 0 ? M : 1));
-    float xr[4096], yr[4096], zr[4096];
-    if (T) { T->nmoves = 0; T->ncos = 0; }
-    for (int ic = 0; ic < C->ncell; ++ic) {
-        for (int p = C->cell_start[ic]; p < C->cell_start[ic + 1]; ++p) {
-            const int im = C->cell_mols[p];
-            const int n = S->nato[im];
-            const int mt = S->mtype[im];
-            if (P->ngrot[im] == 0) P->internrot[mt] = 0.0f;
-            const int a0 = S->naf[im];
-            for (int k = 0; k < n; ++k) { xr[k] = S->xa[a0 + k]; yr[k] = S->ya[a0 + k]; zr[k] = S->za[a0 + k]; }
-            const float xs = S->xadd[im], ys = S->yadd[im], zs = S->zadd[im];
-            if (P->stepr > 0.0f && n > 1) {
-                if (P->wholerot[mt] <= 0.0f) P->wholerot[mt] = rotstepmin;
-                P->nwhole[mt]++;
-                rotatm(S, im, P->wholerot[mt], R, T);
-            } else {
-                P->wholerot[mt] = 0.0f;
-            }
-            if (P->stepm > 0.0f) {
-                if (P->wholetrans[mt] <= 0.0f) P->wholetrans[mt] = P->trstepmin;
-                P->nmovem[mt]++;
-                P->wholetrans[mt] = movem(S, im, P->wholetrans[mt], R);
-            } else {
-                P->wholetrans[mt] = 0.0f;
-            }
-            double d64 = 0.0, sc64 = 0.0;
-            float fdiff = en_change(S, im, E, ergnew, &d64, &sc64);
-            if (T && T->den64) {
-                T->den64[T->nmoves] = d64;
-                T->scale64[T->nmoves] = sc64;
-            }
-            float ediff = (fdiff + 0.0f) * temp;
-            float etest;
-            if (ediff <= 0.0f) etest = 10.0f;
-            else if (ediff < 20.0f) etest = expf(-ediff);
-            else etest = 0.0f;
-            const float udraw = oracle_ran1(R);
-            int acc = udraw < etest;
-            if (T && T->u) T->u[T->nmoves] = udraw;
-            if (acc) {
-                P->nstepreject[im] = 0;
-                fadd = fadd + fdiff;
-                const int32_t *rf = E->ergpairref + (size_t)im * M;
-                for (int inn = 1; inn < E->nergpairm[im]; ++inn) E->ergpair[rf[inn] - 1] = ergnew[inn];
-            } else {
-                P->nstepreject[im]++;
-                for (int k = 0; k < n; ++k) { S->xa[a0 + k] = xr[k]; S->ya[a0 + k] = yr[k]; S->za[a0 + k] = zr[k]; }
-                S->xadd[im] = xs;
-                S->yadd[im] = ys;
-                S->zadd[im] = zs;
-                if (P->stepr > 0.0f) P->nwhole[nmt + mt]++;
-                if (P->stepm > 0.0f) P->nmovem[nmt + mt]++;
-            }
-            if (T) {
-                T->im[T->nmoves] = im;
-                T->den[T->nmoves] = fdiff;
-                T->acc[T->nmoves] = acc;
-                T->nmoves++;
-            }
-        }
-    }
-    free(ergnew);
-    if (P->ireset != 1) {
-        for (int t = 0; t < nmt; ++t) {
-            float rat;
-            /* nmovei and ninter stay 0 in this branch, so their ratio is 1.0 (molfit.py:469-497) */
-            P->interntrans[t] = P->interntrans[t] * 1.0f;
-            if (P->interntrans[t] > P->trstepmax) P->interntrans[t] = P->trstepmax;
-            if (P->interntrans[t] < P->trstepmin && P->interntrans[t] != 0.0f) P->interntrans[t] = P->trstepmin;
-            P->internrot[t] = P->internrot[t] * 1.0f;
-            if (P->internrot[t] > rotstepmax) P->internrot[t] = rotstepmax;
-            if (P->internrot[t] < rotstepmin && P->internrot[t] != 0.0f) P->internrot[t] = rotstepmin;
-            if (P->nwhole[nmt + t] > 0) {
-                rat = P->rejrate * (float)P->nwhole[t] / (float)P->nwhole[nmt + t];
-                if (rat > 1.1f) rat = 1.1f;
-                if (rat < 0.9f) rat = 0.9f;
-            } else {
-                rat = P->nwhole[t] > 0 ? 1.1f : 1.0f;
-            }
-            P->wholerot[t] = P->wholerot[t] * rat;
-            if (P->wholerot[t] > rotstepmax) P->wholerot[t] = rotstepmax;
-            if (P->wholerot[t] < rotstepmin && P->wholerot[t] != 0.0f) P->wholerot[t] = rotstepmin;
-            if (P->nmovem[nmt + t] > 0) {
-                rat = P->rejrate * (float)P->nmovem[t] / (float)P->nmovem[nmt + t];
-                if (rat > 1.1f) rat = 1.1f;
-                if (rat < 0.9f) rat = 0.9f;
-            } else {
-                rat = P->nmovem[t] > 0 ? 1.1f : 1.0f;
-            }
-            P->wholetrans[t] = P->wholetrans[t] * rat;
-            if (P->wholetrans[t] > P->trstepmax) P->wholetrans[t] = P->trstepmax;
-            if (P->wholetrans[t] < P->trstepmin && P->wholetrans[t] != 0.0f) P->wholetrans[t] = P->trstepmin;
-        }
-    }
-    *fadds = *fadds + fadd / (float)S->nmol;
-    return 0;
-}
-
 /* trstepmax/trstepmin of molfit.py:96-101 */
 void oracle_trsteps(int natomr, float *out2) {
     float t = 1.0f / (float)natomr;
@@ -1056,6 +947,226 @@ float oracle_en_mole_intra(const oracle_sys *S, const oracle_intra *I, int im) {
 void oracle_en_mole_intra_all(const oracle_sys *S, const oracle_intra *I, float *out) {
     for (int im = 0; im < S->nmol; ++im) out[im] = oracle_en_mole_intra(S, I, im);
 }
+
+/* ------------------------------------------------------------------ internal rotations */
+/* Rotational groups (molfit.py:295-360): per molecule the group range nrf..nrl, per group the
+ * two axis atoms and the range first..last of its rotated atoms in atoms[] (0-based, global). */
+typedef struct {
+    const oracle_intra *I;
+    const int32_t *nrf, *nrl, *axis, *first, *last, *atoms;
+    float stepri;
+    int32_t rotcycle;
+    int32_t *ninter;   /* [2*nmoltype] tries then rejections */
+    float *faddbs;     /* in/out, or NULL */
+} oracle_rot;
+
+/* rotati molfit.py:589-660 with scapro / vecpro auxiliary_routines.py:231-244 */
+static void rotati(oracle_sys *S, const oracle_rot *RT, int ig, float steprithis, oracle_ran1_state *R,
+                   oracle_trace *T) {
+    const float pi = 3.14159265358979323846f;
+    float phi = pi * steprithis * (2.0f * oracle_ran1(R) - 1.0f);
+    float cphi = cosf(phi);
+    if (T && T->cosv) T->cosv[T->ncos++] = cphi;
+    float sphi = f_sign(sqrtf(1.0f - cphi * cphi), phi);
+    const int a1 = RT->axis[2 * ig], a2 = RT->axis[2 * ig + 1];
+    float p1 = S->xa[a2] - S->xa[a1], p2 = S->ya[a2] - S->ya[a1], p3 = S->za[a2] - S->za[a1];
+    float rab2 = p1 * p1 + p2 * p2 + p3 * p3;
+    if (rab2 > 0.0f) {
+        float rab = sqrtf(rab2);
+        p1 = p1 / rab;
+        p2 = p2 / rab;
+        p3 = p3 / rab;
+        for (int ia = RT->first[ig]; ia <= RT->last[ig]; ++ia) {
+            const int nat = RT->atoms[ia];
+            float v1 = S->xa[nat] - S->xa[a1], v2 = S->ya[nat] - S->ya[a1], v3 = S->za[nat] - S->za[a1];
+            float frac = p1 * v1 + p2 * v2 + p3 * v3;
+            float q1 = frac * p1, q2 = frac * p2, q3 = frac * p3;
+            float r1 = v1 - q1, r2 = v2 - q2, r3 = v3 - q3;
+            float w1 = p2 * r3 - p3 * r2, w2 = p3 * r1 - p1 * r3, w3 = p1 * r2 - p2 * r1;
+            S->xa[nat] = S->xa[a1] + q1;
+            S->ya[nat] = S->ya[a1] + q2;
+            S->za[nat] = S->za[a1] + q3;
+            S->xa[nat] = S->xa[nat] + r1 * cphi + w1 * sphi;
+            S->ya[nat] = S->ya[nat] + r2 * cphi + w2 * sphi;
+            S->za[nat] = S->za[nat] + r3 * cphi + w3 * sphi;
+        }
+    }
+}
+
+/* One molfit cycle, whole-molecule branch (molfit.py:268-448) with the internal rotations of
+ * rotational groups of type ROT every rotfreq cycles (:295-360, rotati :589) when RT is given,
+ * plus step adaptation (:465-536).  fadds (and RT->faddbs) are updated in place (:538-539). */
+static int molfit_impl(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_mcpar *P,
+                       oracle_ran1_state *R, float *fadds, oracle_trace *T, const oracle_rot *RT) {
+    const int nmt = S->nmoltype;
+    const float temp = 1.0f / P->simt;
+    const float rotstepmax = 1.0f, rotstepmin = 1.0e-5f;
+    for (int k = 0; k < 2 * nmt; ++k) {
+        P->nwhole[k] = 0;
+        P->nmovem[k] = 0;
+        if (RT && RT->ninter) RT->ninter[k] = 0;
+    }
+    float fadd = 0.0f, faddb = 0.0f;
+    /* molfit's work array ergold(1): the first stored energy of the last loaded list */
+    float eold0 = 0.0f, p0 = 0.0f;
+    const int M = E->nnbrefmax;
+    float *ergnew = (float *)malloc(sizeof(float) * (size_t)(M > 0 ? M : 1));
+    float xr[4096], yr[4096], zr[4096];
+    if (T) { T->nmoves = 0; T->ncos = 0; }
+    for (int ic = 0; ic < C->ncell; ++ic) {
+        for (int p = C->cell_start[ic]; p < C->cell_start[ic + 1]; ++p) {
+            const int im = C->cell_mols[p];
+            const int n = S->nato[im];
+            const int mt = S->mtype[im];
+            const int a0 = S->naf[im];
+            const int32_t *rf0 = E->ergpairref + (size_t)im * M;
+            const int nn = E->nergpairm[im];
+            if (nn >= 1) eold0 = E->ergpair[rf0[0] - 1];
+            const int rot = RT && RT->stepri > 0.0f && P->ngrot[im] > 0 && RT->rotcycle;
+            if (rot) {
+                if (P->internrot[mt] == 0.0f) P->internrot[mt] = rotstepmin;
+                RT->ninter[mt]++;
+                for (int k = 0; k < n; ++k) { xr[k] = S->xa[a0 + k]; yr[k] = S->ya[a0 + k]; zr[k] = S->za[a0 + k]; }
+                for (int ig = RT->nrf[im]; ig <= RT->nrl[im]; ++ig) rotati(S, RT, ig, P->internrot[mt], R, T);
+                const float enew0 = oracle_en_mole_intra(S, RT->I, im);
+                const float fdiffb = enew0 - eold0;
+                p0 = enew0;
+                double r64 = 0.0, rs64 = 0.0;
+                const float fdiff = en_change(S, im, E, ergnew, &r64, &rs64);
+                const float ediff = (fdiff + fdiffb) * temp;
+                float etest;
+                if (ediff <= 0.0f) etest = 10.0f;
+                else if (ediff < 20.0f) etest = expf(-ediff);
+                else etest = 0.0f;
+                if (oracle_ran1(R) < etest) {
+                    P->nstepreject[im] = 0;
+                    fadd = fadd + fdiff;
+                    faddb = faddb + fdiffb;
+                    eold0 = enew0;
+                    if (nn >= 1) E->ergpair[rf0[0] - 1] = enew0;
+                    for (int inn = 1; inn < nn; ++inn) E->ergpair[rf0[inn] - 1] = ergnew[inn];
+                } else {
+                    P->nstepreject[im]++;
+                    for (int k = 0; k < n; ++k) { S->xa[a0 + k] = xr[k]; S->ya[a0 + k] = yr[k]; S->za[a0 + k] = zr[k]; }
+                    RT->ninter[nmt + mt]++;
+                }
+            } else if (P->ngrot[im] == 0) {
+                P->internrot[mt] = 0.0f;
+            }
+            for (int k = 0; k < n; ++k) { xr[k] = S->xa[a0 + k]; yr[k] = S->ya[a0 + k]; zr[k] = S->za[a0 + k]; }
+            const float xs = S->xadd[im], ys = S->yadd[im], zs = S->zadd[im];
+            if (P->stepr > 0.0f && n > 1) {
+                if (P->wholerot[mt] <= 0.0f) P->wholerot[mt] = rotstepmin;
+                P->nwhole[mt]++;
+                rotatm(S, im, P->wholerot[mt], R, T);
+            } else {
+                P->wholerot[mt] = 0.0f;
+            }
+            if (P->stepm > 0.0f) {
+                if (P->wholetrans[mt] <= 0.0f) P->wholetrans[mt] = P->trstepmin;
+                P->nmovem[mt]++;
+                P->wholetrans[mt] = movem(S, im, P->wholetrans[mt], R);
+            } else {
+                P->wholetrans[mt] = 0.0f;
+            }
+            double d64 = 0.0, sc64 = 0.0;
+            float fdiff = en_change(S, im, E, ergnew, &d64, &sc64);
+            if (T && T->den64) {
+                T->den64[T->nmoves] = d64;
+                T->scale64[T->nmoves] = sc64;
+            }
+            float ediff = (fdiff + 0.0f) * temp;
+            float etest;
+            if (ediff <= 0.0f) etest = 10.0f;
+            else if (ediff < 20.0f) etest = expf(-ediff);
+            else etest = 0.0f;
+            const float udraw = oracle_ran1(R);
+            int acc = udraw < etest;
+            if (T && T->u) T->u[T->nmoves] = udraw;
+            if (acc) {
+                P->nstepreject[im] = 0;
+                fadd = fadd + fdiff;
+                const int32_t *rf = E->ergpairref + (size_t)im * M;
+                for (int inn = 1; inn < E->nergpairm[im]; ++inn) E->ergpair[rf[inn] - 1] = ergnew[inn];
+                /* save_energies copies ergnew(1) too: the rotation's intramolecular energy of this
+                 * visit, accepted or not (ergpairreference.py:192-210) */
+                if (rot) {
+                    eold0 = p0;
+                    if (nn >= 1) E->ergpair[rf[0] - 1] = p0;
+                }
+            } else {
+                P->nstepreject[im]++;
+                for (int k = 0; k < n; ++k) { S->xa[a0 + k] = xr[k]; S->ya[a0 + k] = yr[k]; S->za[a0 + k] = zr[k]; }
+                S->xadd[im] = xs;
+                S->yadd[im] = ys;
+                S->zadd[im] = zs;
+                if (P->stepr > 0.0f) P->nwhole[nmt + mt]++;
+                if (P->stepm > 0.0f) P->nmovem[nmt + mt]++;
+            }
+            if (T) {
+                T->im[T->nmoves] = im;
+                T->den[T->nmoves] = fdiff;
+                T->acc[T->nmoves] = acc;
+                T->nmoves++;
+            }
+        }
+    }
+    free(ergnew);
+    if (P->ireset != 1) {
+        for (int t = 0; t < nmt; ++t) {
+            float rat;
+            /* nmovei stays 0 in this branch, so its ratio is 1.0 (molfit.py:469-483) */
+            P->interntrans[t] = P->interntrans[t] * 1.0f;
+            if (P->interntrans[t] > P->trstepmax) P->interntrans[t] = P->trstepmax;
+            if (P->interntrans[t] < P->trstepmin && P->interntrans[t] != 0.0f) P->interntrans[t] = P->trstepmin;
+            const int ni1 = RT && RT->ninter ? RT->ninter[t] : 0, ni2 = RT && RT->ninter ? RT->ninter[nmt + t] : 0;
+            if (ni2 > 0) {
+                rat = P->rejrate * (float)ni1 / (float)ni2;
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = ni1 > 0 ? 1.1f : 1.0f;
+            }
+            P->internrot[t] = P->internrot[t] * rat;
+            if (P->internrot[t] > rotstepmax) P->internrot[t] = rotstepmax;
+            if (P->internrot[t] < rotstepmin && P->internrot[t] != 0.0f) P->internrot[t] = rotstepmin;
+            if (P->nwhole[nmt + t] > 0) {
+                rat = P->rejrate * (float)P->nwhole[t] / (float)P->nwhole[nmt + t];
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = P->nwhole[t] > 0 ? 1.1f : 1.0f;
+            }
+            P->wholerot[t] = P->wholerot[t] * rat;
+            if (P->wholerot[t] > rotstepmax) P->wholerot[t] = rotstepmax;
+            if (P->wholerot[t] < rotstepmin && P->wholerot[t] != 0.0f) P->wholerot[t] = rotstepmin;
+            if (P->nmovem[nmt + t] > 0) {
+                rat = P->rejrate * (float)P->nmovem[t] / (float)P->nmovem[nmt + t];
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = P->nmovem[t] > 0 ? 1.1f : 1.0f;
+            }
+            P->wholetrans[t] = P->wholetrans[t] * rat;
+            if (P->wholetrans[t] > P->trstepmax) P->wholetrans[t] = P->trstepmax;
+            if (P->wholetrans[t] < P->trstepmin && P->wholetrans[t] != 0.0f) P->wholetrans[t] = P->trstepmin;
+        }
+    }
+    *fadds = *fadds + fadd / (float)S->nmol;
+    if (RT && RT->faddbs) *RT->faddbs = *RT->faddbs + faddb / (float)S->nmol;
+    return 0;
+}
+
+int oracle_molfit(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_mcpar *P,
+                  oracle_ran1_state *R, float *fadds, oracle_trace *T) {
+    return molfit_impl(S, C, E, P, R, fadds, T, NULL);
+}
+
+int oracle_molfit_rot(oracle_sys *S, const oracle_cells *C, oracle_store *E, oracle_mcpar *P,
+                      oracle_ran1_state *R, float *fadds, oracle_trace *T, const oracle_rot *RT) {
+    return molfit_impl(S, C, E, P, R, fadds, T, RT);
+}
+
 
 /* The intramolecular branch of molfit (molfit.py:119-174 with :246-247; no rotational groups),
  * then the step adaptation :465-536, in the reference's order.  *ergold1 is the reference's

@@ -245,9 +245,18 @@ def trsteps(natomr):
     return out[0], out[1]
 
 
-def molfit(box, cells, st, mc, ran1, fadds=0.0, record_cos=True):
+class RotC(C.Structure):
+    _fields_ = [("I", P), ("nrf", P), ("nrl", P), ("axis", P), ("first", P), ("last", P), ("atoms", P),
+                ("stepri", C.c_float), ("rotcycle", C.c_int32), ("ninter", P), ("faddbs", P)]
+
+
+def molfit(box, cells, st, mc, ran1, fadds=0.0, record_cos=True, rot=None):
     """One whole-molecule cycle; mutates box coordinates, st['ergpair'] and the step arrays
-    in ``mc`` (dict of NumPy arrays).  Returns (fadds, trace dict, ran1 state)."""
+    in ``mc`` (dict of NumPy arrays).  Returns (fadds, trace dict, ran1 state).  ``rot``: the
+    internal rotations of rotational groups (type ROT) before each molecule's move, a dict with
+    model (the intramolecular model of molfit_shake, its ngrot included), nrf, nrl (per
+    molecule), axis (groups x 2), first, last (per group, into atoms), atoms (0-based), stepri,
+    rotcycle and faddbs; the trace then also holds ninter (2*nmoltype) and faddbs."""
     h = SysHandle(box)
     E = store_c(st)
     nmt = box.nmoltype
@@ -276,8 +285,28 @@ def molfit(box, cells, st, mc, ran1, fadds=0.0, record_cos=True):
     T.cosv = ptr(tr["cosv"]) if record_cos else None
     r = Ran1C.of(ran1)
     fa = C.c_float(f32(fadds))
-    lib().oracle_molfit(C.byref(h.c), C.byref(cells["_c"]), C.byref(E), C.byref(par), C.byref(r), C.byref(fa),
-                        C.byref(T))
+    if rot is None:
+        lib().oracle_molfit(C.byref(h.c), C.byref(cells["_c"]), C.byref(E), C.byref(par), C.byref(r), C.byref(fa),
+                            C.byref(T))
+    else:
+        T.cosv = ptr(tr["cosv"]) if record_cos else None
+        if record_cos:
+            tr["cosv"] = np.zeros(3 * box.nmol + int(np.asarray(rot["first"]).size) * box.nmol, f32)
+            T.cosv = ptr(tr["cosv"])
+        ih = IntraHandle(box, rot["model"])
+        arrs = {k: np.ascontiguousarray(rot[k], np.int32) for k in ("nrf", "nrl", "axis", "first", "last", "atoms")}
+        ninter = np.zeros(2 * nmt, np.int32)
+        fb = np.array([f32(rot.get("faddbs", 0.0))], f32)
+        rc = RotC()
+        rc.I = C.cast(C.pointer(ih.c), P)
+        for k, v in arrs.items():
+            setattr(rc, k, ptr(v))
+        rc.stepri, rc.rotcycle = f32(rot["stepri"]), int(rot["rotcycle"])
+        rc.ninter, rc.faddbs = ptr(ninter), ptr(fb)
+        lib().oracle_molfit_rot(C.byref(h.c), C.byref(cells["_c"]), C.byref(E), C.byref(par), C.byref(r),
+                                C.byref(fa), C.byref(T), C.byref(rc))
+        tr["ninter"] = ninter
+        tr["faddbs"] = f32(fb[0])
     tr["nmoves"] = T.nmoves
     if record_cos:
         tr["cosv"] = tr["cosv"][: T.ncos].copy()

@@ -1,0 +1,148 @@
+"""Internal rotations of rotational groups in the device's whole-molecule cycle (molfit.py:
+295-360, rotati :589, en_change_intra :763) against the reference run on a 20 DMSO + 40 water
+box whose methyl groups are ROT groups (tests/golden/rot.npz), with the reference's cosines
+injected: coordinates, stored energies (including the first-slot rule after a rejected rotation
+followed by an accepted move), step sizes, ninter/nwhole/nmovem, fadds/faddbs and the ran1
+state bit for bit over two cycles."""
+
+import numpy as np
+import pytest
+
+from epsr_python_translation_b200.box import Ran1State, trsteps
+from tests.goldens import assert_bits_equal
+from tests.test_rot_oracle import load
+
+pytestmark = pytest.mark.gpu
+f32 = np.float32
+
+
+def test_rotation_cycles_device_match_reference():
+    from epsr_python_translation_b200.device import DeviceBox
+    from epsr_python_translation_b200.intra import IntraModel
+    z, box, st, mc, rot = load()
+    d = DeviceBox(box)
+    d.cell_list(int(z["in_nmolcell"]), f32(z["in_sepmax"]))
+    d.fmolec1(z["eintra"], strict=True)
+    s0 = d.download_store()
+    assert_bits_equal(s0["ergpair"], st["ergpair"], "store before the cycles")
+    tmax, tmin = trsteps(box.natomr)
+    d.mc_setup(rejrate=f32(0.75), stepr=f32(z["in_stepr"]), stepm=f32(z["in_stepm"]), wholerot=z["wholerot_in"],
+               wholetrans=z["wholetrans_in"], internrot=z["internrot_in"], ran1=Ran1State.from_golden(z, "ran1_before_"),
+               trstepmax=tmax, trstepmin=tmin, fadds=f32(z["fadds_in"]))
+    model = dict(rot["model"])
+    im = IntraModel(d, **model)
+    d.set_rotations(im, z["rot_nrf"], z["rot_nrl"], z["rot_axis"], z["rot_first"], z["rot_last"], z["rot_atoms"],
+                    stepri=1.0, faddbs=f32(z["faddbs_in"]))
+    for c in range(int(z["cycles"])):
+        q = f"c{c}_"
+        d.molfit(strict=True, cos_override=z[q + "cos"], rotcycle=True)
+        d.check_status()
+        m = d.download_mc()
+        co = d.download_coords()
+        for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+            assert_bits_equal(co[k], z[q + k], f"cycle {c} {k}")
+        assert_bits_equal(d.download_store()["ergpair"], z[q + "ergpair"], f"cycle {c} ergpair")
+        for k in ("internrot", "wholerot", "wholetrans"):
+            assert_bits_equal(m[k], z[q + k], f"cycle {c} {k}")
+        assert np.array_equal(d.m_ninter.cpu().numpy(), z[q + "ninter"].reshape(-1))
+        assert np.array_equal(m["nwhole"].reshape(-1), z[q + "nwhole"].reshape(-1))
+        assert np.array_equal(m["nmovem"].reshape(-1), z[q + "nmovem"].reshape(-1))
+        assert_bits_equal(np.array([m["fadds"], d.m_faddbs.cpu().numpy()[0]], f32),
+                          np.array([z[q + "fadds"], z[q + "faddbs"]], f32), f"cycle {c} fadds, faddbs")
+        assert m["ran1"].idum == int(z[q + "ran1_after_idum"])
+        assert np.array_equal(m["ran1"].iv, z[q + "ran1_after_iv"])
+
+
+class _Aliased:
+    """The rot golden seen under the key names the COMMON stand-ins read."""
+    ALIAS = {"in_wholerot": "wholerot_in", "in_wholetrans": "wholetrans_in", "in_eintra": "eintra"}
+
+    def __init__(self, z):
+        self.z = z
+
+    def __getitem__(self, k):
+        return self.z[self.ALIAS.get(k, k)]
+
+    @property
+    def files(self):
+        return list(self.z.files) + list(self.ALIAS)
+
+
+def test_rotation_dropin_matches_reference():
+    """PairPath.molfit on COMMON stand-ins that carry the reference's rotational groups
+    (molecom_mod labaxi/rotf/rotl/labrot, clustercom ngrot/nrf/nrl, all of type ROT) and
+    intramolecular model: the whole-molecule cycles with internal rotations run on the device
+    and leave the COMMON state equal to the reference's; no host routine ran."""
+    from types import SimpleNamespace as NS
+
+    from epsr_python_translation_b200 import dropin
+    from tests import fake_common
+    z = np.load(__import__("tests.goldens", fromlist=["GOLDEN"]).GOLDEN + "/rot.npz")
+    p = _Aliased(z)
+    calls = []
+    mods = fake_common.routine_modules(p, calls)
+    c = fake_common.common_from_golden(p)
+    mc, cc, pp, erd, r = c.molecom, c.clustercom, c.potential_par, c.ergpairreference, c.ran1com
+    natom, nmol, ntype = mc.natom, cc.nmol, mc.ntype
+    npairs, npt, nmt = mc.npairs, c.epsr16.npt, int(cc.nmoltype)
+    fa = fake_common.fa
+    iab = z["iabond"]
+    mb = iab.shape[1]
+    mc.nbond = fa(natom, dtype=np.int32)
+    mc.nbond[1:] = z["nbond"]
+    mc.iabond = fa(natom, mb, dtype=np.int32)
+    mc.iabond[1:, 1:] = iab + 1
+    mc.tbond = fa(natom, mb)
+    mc.tbond[1:, 1:] = z["tbond"]
+    mc.imageatom, mc.qtype = fa(natom, dtype=np.int32), fa(natom, dtype=np.int32)
+    mc.amassa, mc.amassr = fa(ntype), fa(npairs)
+    mc.amassa[1:], mc.amassr[1:] = z["amassa"], z["amassr"]
+    sc = z["scal"]
+    mc.sizefactor, mc.tempb, mc.tempangreq, mc.tempangwt = f32(sc[1]), f32(sc[2]), f32(sc[3]), f32(sc[3])
+    mc.refine_intra, mc.refine_intra_fac, mc.stepri = False, f32(0.0), f32(1.0)
+    mpz = pp.xavs.shape[0] - 1
+    pp.xav, pp.xav1 = fa(mpz, npairs), fa(mpz, npairs)
+    pp.xav[: npt + 1, 1:], pp.xav1[: npt + 1, 1:] = z["xav"].T, z["xav1"].T
+    cc.internrot[1:] = z["internrot_in"]
+    # the rotational groups, 1-based as the reference holds them
+    ng = z["rot_first"].size
+    cc.ngrot[1:] = z["ngrot"]
+    cc.nrf, cc.nrl = fa(nmol, dtype=np.int32), fa(nmol, dtype=np.int32)
+    cc.nrf[1:], cc.nrl[1:] = z["rot_nrf"] + 1, z["rot_nrl"] + 1
+    lab = fa(ng, 2, dtype=np.int32)
+    lab[1:, 1:] = z["rot_axis"] + 1
+    rotf, rotl = fa(ng, dtype=np.int32), fa(ng, dtype=np.int32)
+    rotf[1:], rotl[1:] = z["rot_first"] + 1, z["rot_last"] + 1
+    labrot = fa(z["rot_atoms"].size, dtype=np.int32)
+    labrot[1:] = z["rot_atoms"] + 1
+    c.molecom_mod = NS(coarsegraining=False, natomsphere=c.molecom_mod.natomsphere, ngrrot=ng,
+                       rotgrp=np.array(["   "] + ["ROT"] * ng, dtype=object), labaxi=lab, rotf=rotf, rotl=rotl,
+                       labrot=labrot, nrottot=int(z["rot_atoms"].size))
+    mc.ndihedralang = fa(ng, dtype=np.int32)
+    path = dropin.PairPath(c, mods, strict=True)
+    path.install(dropin.ROUTINES)
+    mods["cellneighbourlist"].initialise_cellneighbourlist(int(z["in_nmolcell"]), cc.xadd, cc.yadd, cc.zadd, nmol,
+                                                          f32(z["in_sepmax"]))
+    mods["ato_manipulation_rev4"].fmolec1(0, 0, f32(0), f32(0), f32(0), f32(0))
+    assert_bits_equal(erd.ergpair[1:erd.nergpair + 1], z["in_ergpair"], "store before the cycles")
+    fake_common.set_ran1(c, z, "ran1_before_")
+    fadds, faddbs = f32(z["fadds_in"]), f32(z["faddbs_in"])
+    nisum = 1
+    for cyc in range(int(z["cycles"])):
+        q = f"c{cyc}_"
+        path.cos_override = z[q + "cos"]
+        fadds, faddbs, nisum = mods["molfit"].molfit(fadds, faddbs, nisum, 100, 1, 0)
+        assert nisum == int(z[q + "nisum"])
+        assert_bits_equal(np.array([fadds, faddbs], f32), np.array([z[q + "fadds"], z[q + "faddbs"]], f32),
+                          q + "fadds, faddbs")
+        for k, arr in (("xa", mc.xa), ("ya", mc.ya), ("za", mc.za), ("xadd", cc.xadd), ("yadd", cc.yadd),
+                       ("zadd", cc.zadd)):
+            assert_bits_equal(arr[1:], z[q + k], q + k)
+        assert_bits_equal(erd.ergpair[1:erd.nergpair + 1], z[q + "ergpair"], q + "ergpair")
+        for k in ("internrot", "wholerot", "wholetrans"):
+            assert_bits_equal(getattr(cc, k)[1:], z[q + k], q + k)
+        for k in ("ninter", "nwhole", "nmovem"):
+            assert np.array_equal(getattr(cc, k)[1:3, 1:nmt + 1], z[q + k]), k
+        assert (r.idum, r.iy, r.mcall) == (int(z[q + "ran1_after_idum"]), int(z[q + "ran1_after_iy"]),
+                                           int(z[q + "ran1_after_mcall"]))
+    assert not [k for k in calls if k.startswith("host:")], calls
