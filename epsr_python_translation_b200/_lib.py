@@ -105,7 +105,8 @@ class Iteration(C.Structure):
                 ("absolute_energy", F32), ("erequnit", F32), ("ereqstep", F32), ("potfacamp", F32), ("tab", P),
                 ("intra", I32), ("nisum", I32), ("stepmi", F32), ("intra_model", P), ("faddbs", P),
                 ("eintra_work", P), ("nmovei", P),
-                ("scratch", P), ("scratch_bytes", I64), ("strict", I32), ("stage_events", P * 20)]
+                ("scratch", P), ("scratch_bytes", I64), ("strict", I32), ("stage_events", P * 20),
+                ("rotfreq", I32)]
 
 
 class IterationReport(C.Structure):

@@ -354,8 +354,8 @@ class BatchBoxes:
             n2.append(s.n2extr)
             rmx.append(np.full(s.npairs, rminex, f32))
             cfrac.append(s.cfrac.astype(f32))
-            last = s.naf[-1]            # atoms of molecules 0..nmol-2 (the origins of atogen's full sampling)
-            cs = np.bincount(s.itype[:last], minlength=s.ntype).astype(f32)
+            # atoms of every molecule by type (atogen's sampled-atom counts when all are sampled)
+            cs = np.bincount(s.itype, minlength=s.ntype).astype(f32)
             csam.append(cs)
             max_bins = max(max_bins, s.npairs * ld + s.npairs)
             h0 += 2 * s.npairs * ld + s.npairs

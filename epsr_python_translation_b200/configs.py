@@ -39,7 +39,7 @@ class MolTemplate:
     labels: list          # atom type label per atom
     pos: np.ndarray       # (n,3) float64 Angstrom, relative to the molecule centre
     bonds: list = field(default_factory=list)   # (i, j, length_A) harmonic constraints
-    rot_groups: int = 0
+    rot_groups: list = field(default_factory=list)  # (axis atom 1, axis atom 2, [rotated atoms]), type ROT
 
 
 def water_template() -> MolTemplate:
@@ -86,7 +86,8 @@ def dmso_template() -> MolTemplate:
     for ci, h0 in ((2, 4), (3, 7)):
         for k in range(3):
             bonds.append((ci, h0 + k, 1.09))
-    return MolTemplate("dmso", labels, pos, bonds=bonds)
+    # the two methyl groups rotate about their S-C axis (ROT groups, as 200DMSO400Water.ato)
+    return MolTemplate("dmso", labels, pos, bonds=bonds, rot_groups=[(0, 2, [4, 5, 6]), (0, 3, [7, 8, 9])])
 
 
 def atom_template(label: str) -> MolTemplate:
@@ -556,6 +557,31 @@ def intra_model(s: System):
                 tempang=f32(1.0), refine_intra=False, refine_intra_fac=f32(0.0))
 
 
+def rotations(s: System):
+    """The rotational groups of every molecule of ``s`` from its templates, as the device takes
+    them (0-based): ngrot, nrf, nrl per molecule (nrl < nrf: none), axis (groups x 2), first,
+    last per group into atoms.  None when no template has groups."""
+    if not any(t.rot_groups for t in s.moltemplates):
+        return None
+    ngrot = np.zeros(s.nmol, np.int32)
+    nrf = np.zeros(s.nmol, np.int32)
+    nrl = np.full(s.nmol, -1, np.int32)
+    axis, first, last, atoms = [], [], [], []
+    for m in range(s.nmol):
+        groups = s.moltemplates[int(s.mtype[m])].rot_groups
+        a0 = int(s.naf[m])
+        nrf[m] = len(axis)
+        for (i, j, rot) in groups:
+            axis.append((a0 + i, a0 + j))
+            first.append(len(atoms))
+            atoms.extend(a0 + k for k in rot)
+            last.append(len(atoms) - 1)
+        nrl[m] = len(axis) - 1
+        ngrot[m] = len(groups)
+    return dict(ngrot=ngrot, nrf=nrf, nrl=nrl, axis=np.array(axis, np.int32).reshape(-1, 2),
+                first=np.array(first, np.int32), last=np.array(last, np.int32), atoms=np.array(atoms, np.int32))
+
+
 # ----------------------------------------------------------------------------- workloads
 def intra_energies(s: System, k_bond=1000.0):
     """Per-molecule harmonic bond energies (float32) of the seeded geometry.
@@ -641,6 +667,8 @@ class Workload:
     intra: int = 0           # molfit cycles between intramolecular cycles (0: rigid molecules, none)
     stepmi: float = 1.0      # intramolecular step flag (> 0 moves the atoms of multi-atom molecules)
     data_source: str = "analytic"   # where the data sets come from
+    rotfreq: int = 0         # internal rotations of the templates' ROT groups every rotfreq cycles (0: none)
+    internrot: np.ndarray = None    # (nmoltype,) starting internal-rotation step (fraction of pi)
 
     @property
     def nq(self):
@@ -648,7 +676,7 @@ class Workload:
 
 
 def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, ndata=None, ntimes=5, refine=True,
-                  intra=0, data_source="auto"):
+                  intra=0, data_source="auto", rotfreq=0):
     """One iteration's inputs on a named configuration, 5 MC sweeps per iteration and a
     116-term Poisson-like EP basis.  C2 (c2_mixture): 200 DMSO + 400 water, three isotope
     data sets (deuterated, protiated, 50:50), Q to 30 A^-1 (600 points).  C3 (c3_water):
@@ -697,4 +725,6 @@ def make_workload(name="c2_mixture", seed=1, nq=None, qstep=0.05, nterms=116, nd
     xwt = np.linspace(0.5, 1.5, s.npairs).astype(f32)
     return Workload(name=name, system=s, eintra=intra_energies(s), q=q, foqols=F, ycoh=ycoh, expr=expr,
                     nterms=nterms, data=data, weights=w, wholerot=wholerot, wholetrans=wholetrans, ntimes=ntimes,
-                    xwt=xwt, ep=ep, intra=int(intra), data_source=src)
+                    xwt=xwt, ep=ep, intra=int(intra), data_source=src,
+                    rotfreq=int(rotfreq) if rotations(s) is not None else 0,
+                    internrot=np.array([f32(0.05) if t.rot_groups else f32(0.0) for t in s.moltemplates], f32))

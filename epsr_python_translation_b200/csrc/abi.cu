@@ -103,9 +103,11 @@ void epsr_timing_mark(const char *name, cudaStream_t s, int end) {
 
 extern "C" int epsr_timing_enable(int32_t on) {
     std::lock_guard<std::mutex> lk(g_tm_mu);
-    g_tm.clear();
-    g_tm_open.clear();
-    g_tm_used = 0;
+    if (on) {   // a new measurement: earlier records go (disabling keeps them for reading)
+        g_tm.clear();
+        g_tm_open.clear();
+        g_tm_used = 0;
+    }
     g_epsr_timing_on = on ? 1 : 0;
     return EPSR_OK;
 }

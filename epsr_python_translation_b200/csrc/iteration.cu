@@ -107,7 +107,7 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
     store.nergpair = it->nergpair;
     store.mirror = it->mirror;
     const float *eintra = it->eintra;
-    if (it->intra > 0) {   // the intramolecular energies of the model the intramolecular cycles use
+    if (it->intra_model) {   // the intramolecular energies of the box's model, as fmolec1 forms them
         rc = epsr_en_mole_intra(b, it->intra_model, it->eintra_work, stream);
         if (rc) return rc;
         eintra = it->eintra_work;
@@ -137,6 +137,7 @@ extern "C" int epsr_iteration_step(const epsr_iteration_t *it, epsr_iteration_re
                               rep->ftest, stream);
             if (rc) return rc;
         } else {
+            mc->rotcycle = it->rotfreq > 0 && nisum % it->rotfreq == 0;   // molfit.py:295
             rc = epsr_molfit(b, &cells, &store, mc, it->scratch, it->scratch_bytes, stream);
             if (rc) return rc;
             nisum += 1;

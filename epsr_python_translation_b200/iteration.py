@@ -71,13 +71,23 @@ class EpsrIteration:
         # flexible molecules: intramolecular cycles every wl.intra molfit cycles (molfit.py:124)
         self.intra_model = None
         self.nisum_mc = 1
-        if wl.intra > 0:
+        self.rot = None
+        if wl.intra > 0 or wl.rotfreq > 0:
             from . import configs
             from .intra import IntraModel
-            self.intra_model = IntraModel(self.d, **configs.intra_model(wl.system))
+            self.rot = configs.rotations(wl.system) if wl.rotfreq > 0 else None
+            ngrot = self.rot["ngrot"] if self.rot is not None else None
+            self.intra_model = IntraModel(self.d, **configs.intra_model(wl.system), ngrot=ngrot)
             self.faddbs = torch.zeros(1, dtype=torch.float32, device=dev)
             self._eintra_work = torch.zeros(b.nmol, dtype=torch.float32, device=dev)
             self._nmovei = torch.zeros(2 * b.nmoltype, dtype=torch.int32, device=dev)
+        if self.rot is not None:
+            # internal rotations of the templates' ROT groups every rotfreq whole-molecule cycles
+            # (molfit.py:295-360), the intramolecular change accumulated in faddbs
+            r = self.rot
+            self.d.set_rotations(self.intra_model, r["nrf"], r["nrl"], r["axis"], r["first"], r["last"], r["atoms"],
+                                 stepri=1.0, faddbs=0.0)
+            self.d.m_internrot.copy_(torch.from_numpy(wl.internrot))
         self.events = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                        for k in STAGES}
         self.moves_per_step = wl.ntimes * b.nmol
@@ -144,14 +154,14 @@ class EpsrIteration:
         self._mark("fmolec1", True)
         self._mark("molfit")
         for _ in range(wl.ntimes):
-            if self.intra_model is not None and self.nisum_mc >= wl.intra:
+            if wl.intra > 0 and self.nisum_mc >= wl.intra:
                 # molfit's intramolecular branch, then runepsr17's minimage and store rebuild
                 self._nmovei.copy_(self.intra_model.molfit_shake(wl.stepmi, self.faddbs))
                 self.nisum_mc = 1
                 d.minimage_centres()
                 self.ftest = d.fmolec1(self.intra_model.en_mole_intra(self._eintra_work), strict=self.strict)
             else:
-                d.molfit(strict=self.strict)
+                d.molfit(strict=self.strict, rotcycle=wl.rotfreq > 0 and self.nisum_mc % wl.rotfreq == 0)
                 self.nisum_mc += 1
         self._mark("molfit", True)
         self._mark("atogen")
@@ -268,6 +278,7 @@ class EpsrIteration:
             it.intra_model = C.cast(C.pointer(self.intra_model.c), C.c_void_p)
             it.faddbs, it.eintra_work, it.nmovei = P(self.faddbs), P(self._eintra_work), P(self._nmovei)
         it.strict = 1 if self.strict else 0
+        it.rotfreq = wl.rotfreq if self.rot is not None else 0
         for k, name in enumerate(STAGES):       # the Python step has created these events
             it.stage_events[2 * k] = self.events[name][0].cuda_event
             it.stage_events[2 * k + 1] = self.events[name][1].cuda_event
@@ -286,7 +297,7 @@ class EpsrIteration:
                                                   C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         r = self._rep
         self.d.nnbrefmax = int(r.nnbrefmax)
-        if self.intra_model is not None:
+        if self.intra_model is not None or self.rot is not None:
             self.nisum_mc = int(r.nisum)
         if self.d.store is not None:        # the store struct other calls take follows the driver's layout
             self.d.store.nnbrefmax = int(r.nnbrefmax)

@@ -301,7 +301,7 @@ typedef struct {
  * 3640-3899 with every molecule an origin: intramolecular pairs once each (nint bin, weight 2
  * at normalisation), intermolecular pairs jm > im, close contacts d*dmax < |rminex|), counted
  * in 64-bit integers, then normalised in float32 as atogen does (:3857-3897, csampled = the
- * atoms of molecules 0..nmol-2, addwav 2, ycoh 0).  One launch covers every box's pairs.
+ * atoms of every molecule by type, addwav 2, ycoh 0).  One launch covers every box's pairs.
  * Offsets are per box; types and pairs are box-local indices into the packed arrays; at most
  * 64 pair types per box. */
 typedef struct {
@@ -685,6 +685,8 @@ typedef struct {
     void *stage_events[20];           /* NULL or CUDA events recorded at the start and end of
                                          cells, fmolec1, molfit, atogen, gensq, press, fit, ep,
                                          sums, stog */
+    int32_t rotfreq;                  /* > 0 with mc's rotational groups: internal rotations in the
+                                         whole-molecule cycles where nisum is a multiple of rotfreq */
 } epsr_iteration_t;
 
 typedef struct {

@@ -34,6 +34,15 @@ class CpuIteration:
         self.stage_s = {}
         self.pair_updates = 0
         self.nisum_mc, self.fadds, self.faddbs, self.ergold1 = 1, f32(0.0), f32(0.0), f32(0.0)
+        self.rot = None
+        if wl.rotfreq > 0:
+            from epsr_python_translation_b200 import configs
+            r = configs.rotations(wl.system)
+            m = dict(configs.intra_model(wl.system), ngrot=r["ngrot"])
+            self.rot = dict(model=m, nrf=r["nrf"], nrl=r["nrl"], axis=r["axis"].reshape(-1), first=r["first"],
+                            last=r["last"], atoms=r["atoms"], stepri=f32(1.0), rotcycle=0, faddbs=f32(0.0))
+            self.mc["ngrot"] = r["ngrot"]
+            self.mc["internrot"] = np.array(wl.internrot, f32)
         ep = wl.ep
         if ep is not None:
             b = self.box
@@ -58,12 +67,14 @@ class CpuIteration:
         if wl.intra > 0:
             from epsr_python_translation_b200 import configs
             model = configs.intra_model(wl.system)
+        if self.rot is not None:
+            model = self.rot["model"]
         st = oracle.fmolec1(b, cells, wl.eintra if model is None else oracle.en_mole_intra_all(b, model))
         t["fmolec1"] = time.perf_counter() - t0
         self.cells, self.st = cells, st
         t0 = time.perf_counter()
         for _ in range(nsw):
-            if model is not None and self.nisum_mc >= wl.intra:
+            if wl.intra > 0 and self.nisum_mc >= wl.intra:
                 # molfit's intramolecular branch, then runepsr17's minimage and store rebuild
                 self.fadds, self.faddbs, _, self.ergold1, self.ran1 = oracle.molfit_shake(
                     b, st, self.mc, model, wl.stepmi, self.ran1, self.fadds, self.faddbs, self.ergold1)
@@ -71,7 +82,13 @@ class CpuIteration:
                 oracle.minimage_centres(b)
                 st = oracle.fmolec1(b, cells, oracle.en_mole_intra_all(b, model))
             else:
-                _, _, self.ran1 = oracle.molfit(b, cells, st, self.mc, self.ran1, record_cos=False)
+                rot = self.rot
+                if rot is not None:
+                    rot["rotcycle"] = int(self.nisum_mc % wl.rotfreq == 0)
+                    rot["faddbs"] = self.faddbs
+                _, tr, self.ran1 = oracle.molfit(b, cells, st, self.mc, self.ran1, record_cos=False, rot=rot)
+                if rot is not None:
+                    self.faddbs = tr["faddbs"]
                 self.nisum_mc += 1
         t["molfit"] = (time.perf_counter() - t0) * (wl.ntimes / nsw)
         self.sampled_sweeps = nsw

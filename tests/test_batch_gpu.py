@@ -95,12 +95,21 @@ def test_total_energy_matches_fp64(bb):
 
 
 def test_step_proposals_features_decisions(bb):
+    """Eight steps of one sweep, each checked in full (every box has few slots, so several
+    steps are needed to see many moves)."""
     torch.cuda.synchronize()
-    co = bb.download()
     sweep = int(bb.sweep_counter.item())
     bb.begin_sweep()
     x, y = bb.feature_buffers()
-    step = 3
+    seen = 0
+    for step in range(8):
+        seen += _check_step(bb, sweep, step, x)
+    bb.end_sweep()
+    assert seen >= 6, seen
+
+
+def _check_step(bb, sweep, step, x):
+    co = bb.download()
     bb.propose(step, x)
     torch.cuda.synchronize()
     bb.check_status()
@@ -142,7 +151,6 @@ def test_step_proposals_features_decisions(bb):
             assert np.array_equal(feats[2 * k], (h * 0.25).astype(f32)), (s.name, k)
             assert np.array_equal(feats[2 * k + 1], np.concatenate([h[640:], h[:640]]).astype(f32) * f32(0.25))
             props[k] = (b, pr)
-    assert len(props) >= 3
     # decisions: the FP64 energy change of each move against every other molecule
     e0 = bb.energy.clone()
     bb.decide(step, 0)
@@ -183,9 +191,11 @@ def test_step_proposals_features_decisions(bb):
             assert np.array_equal(co2["xa"][as_][a0:a0 + na].view(np.uint32), pr["off"][:, 0].view(np.uint32))
     # the running energy moved by the accepted changes only
     de_run = (bb.energy - e0).cpu().numpy()
-    bb.end_sweep()
     assert np.all(np.isfinite(de_run))
     del parted
+    return len(props)
+
+
 
 
 def test_running_energy_and_graph_replay(bb):

@@ -92,7 +92,13 @@ def test_c3_fast_store_and_speculative_cycle_match_oracle(c3):
     st = d.download_store()
     assert st["nergpair"] == ost["nergpair"]
     assert_bits_equal(st["ergpair"], ost["ergpair"][: ost["nergpair"]], "ergpair (fast)")
-    assert abs(float(ft) - float(ost["ftest"])) <= 1e-5 * abs(float(ost["ftest"])) + 1e-3
+    # ftest: the stored intermolecular energies (after the intramolecular block) over nmol; the
+    # fast sum is a double sum, checked against the exact sum of the same float32 entries (the
+    # reference's sequential float32 sum of 3 million terms is itself off by ~0.3%)
+    e = ost["ergpair"][: ost["nergpair"]].astype(np.float64)
+    nintra = int(np.count_nonzero(eintra))
+    exact = e[nintra:].sum() / ob.nmol
+    assert abs(float(ft) - exact) <= 1e-6 * np.abs(e[nintra:]).sum() / ob.nmol + 1e-6, (float(ft), exact)
     nmt = ob.nmoltype
     tmax, tmin = trsteps(ob.natomr)
     rot, tra = np.full(nmt, f32(10.0 / 180.0), f32), np.full(nmt, f32(0.5) / f32(ob.dmax), f32)

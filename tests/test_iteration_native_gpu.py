@@ -85,3 +85,28 @@ def test_native_iteration_with_intramolecular_cycles_matches_python_driver(confi
     sa, sb = a.d.download_store(), b.d.download_store()
     assert np.array_equal(sa["ergpair"].view(np.uint32), sb["ergpair"].view(np.uint32))
     assert np.array_equal(a._nmovei.cpu().numpy(), b._nmovei.cpu().numpy())
+
+
+def test_native_iteration_with_methyl_rotations_matches_python_driver():
+    """C2 with the DMSO methyl groups rotated internally in every second whole-molecule cycle
+    (rotfreq 2): the native driver and the Python driver leave identical coordinates, stored
+    energies, internal-rotation steps and ran1 streams, and rotations were tried and accepted."""
+    from epsr_python_translation_b200 import configs
+    from epsr_python_translation_b200.iteration import EpsrIteration
+    wl = configs.make_workload("c2_mixture", ntimes=4, rotfreq=2)
+    assert wl.rotfreq == 2
+    a = EpsrIteration(wl, ran1_seed=-13, native=True)
+    b = EpsrIteration(wl, ran1_seed=-13, native=False)
+    for _ in range(3):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    ca, cb = a.d.download_coords(), b.d.download_coords()
+    for k in ca:
+        assert np.array_equal(ca[k].view(np.uint32), cb[k].view(np.uint32)), k
+    assert np.array_equal(a.ran1.cpu().numpy(), b.ran1.cpu().numpy())
+    assert np.array_equal(a.d.m_internrot.cpu().numpy(), b.d.m_internrot.cpu().numpy())
+    assert np.array_equal(a.d.m_faddbs.cpu().numpy().view(np.uint32), b.d.m_faddbs.cpu().numpy().view(np.uint32))
+    ni = b.d.m_ninter.cpu().numpy()
+    assert ni[0] > 0 and ni[nmt_rej := wl.system.nmoltype] < ni[0]
+    del nmt_rej
