@@ -51,7 +51,7 @@ class Mc(C.Structure):
                 ("cos_override", P), ("trace_den", P), ("trace_acc", P), ("strict", I32),
                 ("status", P), ("intra", P), ("rot_nrf", P), ("rot_nrl", P), ("rot_axis", P), ("rot_first", P),
                 ("rot_last", P), ("rot_atoms", P), ("stepri", F32), ("rotcycle", I32), ("ninter", P),
-                ("faddbs", P)]
+                ("faddbs", P), ("ahead", P), ("ahead_cap", I64)]
 
 
 class Mlp(C.Structure):

@@ -243,8 +243,7 @@ class BatchBoxes:
         self.c = c
         # per-step buffers of the surrogate path
         self.rows = ((2 * self.nslot + 127) // 128) * 128
-        self.x = None
-        self.y = None
+        self.x = self.y = self.resid = None
         self.graphs = {}
 
     # ------------------------------------------------------------------ calls

@@ -7,15 +7,25 @@
 // exactly when p was visited earlier and accepted.  So:
 //
 //   plan     per-move draw offsets; per-type step sizes (the first-visit initialisation);
-//   draws    the cycle's ran1 values in one stream pass;
+//   draws    the cycle's ran1 values in one stream pass -- or, when the caller gave a
+//            draws-ahead buffer and the previous cycle left the stream where the values in it
+//            start, those values, generated on a second stream while the previous cycle ran;
 //   propose  every proposal (rotatm + movem) and its Metropolis threshold, in parallel;
 //   energy   for every stored entry (k, p): A = E(new k, old p) and, if p is earlier in
 //            the visit order, B = E(new k, new p) -- each in the reference's (ia, ja) order;
 //   corr     per move the energy change assuming no earlier partner accepted (base) and
 //            the correction c = (B - old') - (A - S) that applies if partner p accepted;
-//   resolve  one CTA walks the moves in order: helper warps sum the corrections of
-//            partners resolved more than 32 moves ago, the resolver warp adds those of the
-//            last 32 with one shuffle reduction and compares with the precomputed threshold;
+//            the corrections of partners visited at most 64 moves earlier are kept by the
+//            earlier move (its row: the effect of its acceptance on each of the next 64 moves)
+//   resolve  one CTA walks the moves in order.  The resolver warp holds a running sum for
+//            each of the next 64 moves (two per lane); deciding a move is one comparison in
+//            the lane that holds its sum and a ballot, after which every lane adds the
+//            decided move's row entry for its two moves -- no reduction on the decision
+//            chain.  The rows and thresholds arrive by bulk copies into a four-block ring of
+//            shared memory.  Helper warps sum, per move, the corrections of accepted partners
+//            visited more than 64 moves earlier, reading the decisions the resolver publishes
+//            once per 32 moves; each handoff is a 64-bit word carrying its own tag, so no
+//            fence sits on the decision chain;
 //   commit   coordinates, the energy store (the later accepted writer of a shared slot
 //            wins), counters, step adaptation, fadds and the ran1 state.
 //
@@ -25,14 +35,18 @@
 // doubles the step and draws again, molfit.py:752-758) shifts every later draw; the cycle is
 // then discarded and the sequential kernel runs it instead, from the unchanged state.
 #include "common.cuh"
+#include "umma.cuh"
 
 namespace epsr {
 
-constexpr int SP_W = 32;        // near window of the resolver (moves)
-constexpr int SP_RING = 64;     // far-sum ring (moves)
+constexpr int SP_W = 64;        // near window of the resolver (moves): two running sums per lane
+constexpr int SP_FR = 128;      // far-sum ring (moves)
+constexpr int SP_BLK = 32;      // moves per staged block (and per published decision word)
+constexpr int SP_NSLOT = 4;     // staged blocks held in shared memory
+constexpr int SP_NH = 18;       // helper warps: warps 1..23 outside scheduler 0
 constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
 constexpr int SP_ET = 256;      // threads of a move's energy CTA (its stored partners)
-constexpr int SP_RT = 1024;     // resolver CTA: the resolver warp and 31 far-sum helper warps
+constexpr int SP_RT = 768;      // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
 
 struct SpecDev {
@@ -58,18 +72,21 @@ struct SpecDev {
     int32_t *trace_acc;
     int32_t *status;
     // scratch
-    int32_t *vpos, *off, *rotidx, *flags;  // flags[0] retry, flags[1] resolver timeout
+    int32_t *vpos, *off, *rotidx, *flags;  // flags[0] retry, [1] resolver timeout, [2] values to walk, [3] draws ahead taken
     float *rotstep, *transstep;            // [nmoltype]
     int32_t *tries_rot, *tries_tr, *rej_rot, *rej_tr, *cnt_type;  // [nmoltype]
     int32_t *ran1_next;                    // [35]
     float *draws;
+    const float *ahead_vals;               // the draws-ahead values, or NULL
+    const int32_t *use_ahead;              // [1] 1: this cycle reads ahead_vals (NULL: never)
     float *nx, *ny, *nz;                   // [natom] proposed offsets
     float4 *nc;                            // [N] proposed centres (by molecule)
     float4 *npos;                          // [natom] proposed absolute positions
     float *thr;                            // [N] Metropolis thresholds (by visit position)
     float *A, *B;                          // [N*M]
-    double *base, *nearc, *farc;           // [N], [N*W], [N*M]
-    int32_t *fv;                           // [N*M]
+    double *base, *nearT, *farc;           // [N], [Npad*W] by the earlier move, [N*M]
+    int32_t *fv;                           // [N*M] by visit position
+    int32_t *nnk;                          // [N] entries of each move's list
     int32_t *acc;                          // [N] by visit position
     float *fdiff;                          // [N] by visit position
     double *fadd_acc;                      // [1]
@@ -190,7 +207,7 @@ __global__ void spec_propose_kernel(SpecDev S) {
     const int n = S.nato[m];
     const int a0 = S.naf[m];
     const int t = S.mtype[m];
-    const float *u = S.draws + S.off[k];
+    const float *u = (S.use_ahead && *S.use_ahead ? S.ahead_vals : S.draws) + S.off[k];
     int q = 0;
     float x[SP_MAXAT], y[SP_MAXAT], z[SP_MAXAT];
     for (int i = 0; i < n; ++i) {
@@ -342,123 +359,214 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
             const double c = ((double)S.B[e] - oldp) - d0;
             const int dist = k - kp;
             if (dist <= SP_W) {
-                S.nearc[(size_t)k * SP_W + dist - 1] = c;
+                S.nearT[(size_t)kp * SP_W + dist - 1] = c;
             } else {
-                S.farc[e] = c;
+                S.farc[(size_t)k * S.M + s] = c;
                 fvv = kp;
             }
         }
-        S.fv[e] = fvv;
+        S.fv[(size_t)k * S.M + s] = fvv;   // the far partners by visit position, for the helpers
     }
     d0s = warp_sum_d(d0s);
     __shared__ double ws[4];
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = d0s;
     __syncthreads();
-    if (threadIdx.x == 0) S.base[k] = ws[0] + ws[1] + ws[2] + ws[3];
+    if (threadIdx.x == 0) {
+        S.base[k] = ws[0] + ws[1] + ws[2] + ws[3];
+        S.nnk[k] = nn;
+    }
 }
 
 // ----------------------------------------------------------------- resolve
+// Shared memory of the resolver CTA (dynamic): the staged rows, the staged thresholds, the
+// blocks' mbarriers, the far-sum ring (two tagged words a move: high and low halves of the
+// double) and the published decision words (tag in the high half, one bit a move in the low).
+constexpr int SP_SROWS = SP_NSLOT * SP_BLK * SP_W * 8;
+constexpr int SP_STHR = SP_NSLOT * SP_BLK * 4;
+constexpr int SP_SHDR = SP_SROWS + SP_STHR + SP_NSLOT * 8 + SP_FR * 16;
+
+__host__ __device__ constexpr size_t spec_resolve_smem(int N) {
+    return (size_t)SP_SHDR + 8 * (size_t)((N + SP_BLK - 1) / SP_BLK);
+}
+
 __global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
-    extern __shared__ unsigned accbits_raw[];
-    volatile unsigned *accbits = accbits_raw;
-    __shared__ volatile int progress;
+    extern __shared__ __align__(128) unsigned char rsm[];
+    double *srows = reinterpret_cast<double *>(rsm);
+    float *sthr = reinterpret_cast<float *>(rsm + SP_SROWS);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(rsm + SP_SROWS + SP_STHR);
+    volatile uint64_t *vfar = reinterpret_cast<volatile uint64_t *>(rsm + SP_SROWS + SP_STHR + SP_NSLOT * 8);
+    volatile uint64_t *vpub = reinterpret_cast<volatile uint64_t *>(rsm + SP_SHDR);
     __shared__ volatile int abort_flag;
-    __shared__ volatile int far_ready[SP_RING];
-    __shared__ volatile double far_ring[SP_RING];
     if (S.flags[0]) return;
+    const int N = S.N;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int nwords = (S.N + 31) >> 5;
-    for (int i = tid; i < nwords; i += blockDim.x) accbits[i] = 0u;
-    for (int i = tid; i < SP_RING; i += blockDim.x) far_ready[i] = 0;
+    const int nblk = (N + SP_BLK - 1) / SP_BLK;
+    for (int i = tid; i < 2 * SP_FR; i += blockDim.x) vfar[i] = 0ull;
+    for (int i = tid; i < nblk; i += blockDim.x) vpub[i] = 0ull;
     if (tid == 0) {
-        progress = 0;
         abort_flag = 0;
+        for (int i = 0; i < SP_NSLOT; ++i) umma::mbar_init(&bars[i], 1);
+        umma::fence_mbar_init();
     }
     __syncthreads();
     const float temp = __fdiv_rn(1.0f, S.simt);
+    auto fail = [&]() {
+        abort_flag = 1;
+        S.flags[1] = 1;
+    };
+
     if (wid == 0) {
-        unsigned accmask = 0u;
+        // ---- the resolver warp
+        auto stage = [&](int b) {   // lane 0: rows and thresholds of block b into its slot
+            const int slot = b % SP_NSLOT;
+            const int nr = min(SP_BLK, N - SP_BLK * b);
+            const uint32_t rb = (uint32_t)nr * SP_W * 8, tb = ((uint32_t)nr * 4 + 15u) & ~15u;
+            umma::mbar_expect_tx(&bars[slot], rb + tb);
+            umma::bulk_load(srows + (size_t)slot * SP_BLK * SP_W, S.nearT + (size_t)b * SP_BLK * SP_W, rb, &bars[slot]);
+            umma::bulk_load(sthr + slot * SP_BLK, S.thr + (size_t)b * SP_BLK, tb, &bars[slot]);
+        };
+        int issued = 0, waited = 0;
+        if (lane == 0)
+            for (; issued < min(nblk, SP_NSLOT - 1); ++issued) stage(issued);
+        double A0 = 0.0, A1 = 0.0;   // running sums of the pending moves = lane, lane + 32 (mod 64)
         double fadd = 0.0;
-        double cnext = S.N > 0 ? S.nearc[lane] : 0.0;
-        float tnext = S.N > 0 ? S.thr[0] : 0.0f;
-        for (int k = 0; k < S.N; ++k) {
-            const double c = cnext;
-            const float thr = tnext;
-            if (k + 1 < S.N) {
-                cnext = S.nearc[(size_t)(k + 1) * SP_W + lane];
-                tnext = S.thr[k + 1];
+        int err = 0;
+        for (int b = 0; b < nblk && !err; ++b) {
+            const int slot = b % SP_NSLOT;
+            if (lane == 0 && issued < nblk) {   // the slot block b-1 used: this warp has read it
+                umma::fence_proxy_async();
+                stage(issued++);
             }
-            const int slot = k % SP_RING;
-            long long it = 0;
-            while (far_ready[slot] != k + 1) {
-                if (++it > SP_SPIN_LIMIT || abort_flag) break;
-            }
-            if (it > SP_SPIN_LIMIT || abort_flag) {
-                if (lane == 0) {
-                    abort_flag = 1;
-                    S.flags[1] = 1;
-                }
+            // every lane waits on the block's mbarrier (its completion makes the copied bytes visible)
+            const bool got = umma::mbar_wait(&bars[slot], (uint32_t)((b / SP_NSLOT) & 1), nullptr);
+            if (__any_sync(0xffffffffu, !got)) {
+                err = 1;
                 break;
             }
-            __threadfence_block();
-            const double f = far_ring[slot];
-            double v = ((accmask >> lane) & 1u) ? c : 0.0;
-            v = warp_sum_d(v);
-            const float fd = (float)(f + v);
-            const float ediff = __fmul_rn(__fadd_rn(fd, 0.0f), temp);
-            const unsigned a = ediff < thr ? 1u : 0u;
-            accmask = (accmask << 1) | a;
-            if (a) fadd += (double)fd;
-            if (lane == 0) {
-                S.acc[k] = (int)a;
-                S.fdiff[k] = fd;
-                if (a) accbits[k >> 5] |= 1u << (k & 31);
-                __threadfence_block();
-                progress = k + 1;
+            ++waited;
+            const double *rows = srows + (size_t)slot * SP_BLK * SP_W;
+            const float *th = sthr + slot * SP_BLK;
+            const int nr = min(SP_BLK, N - SP_BLK * b);
+            unsigned wbits = 0u;
+            for (int i = 0; i < nr; ++i) {
+                const int k = SP_BLK * b + i;
+                const int i0 = (lane + SP_W - 1 - (k & (SP_W - 1))) & (SP_W - 1);   // distance - 1 of this lane's first move
+                const double c0 = rows[i * SP_W + i0], c1 = rows[i * SP_W + ((i0 + 32) & (SP_W - 1))];
+                const float thr = th[i];
+                const int fs = 2 * (k % SP_FR);
+                uint64_t h = vfar[fs], l = vfar[fs + 1];
+                const uint64_t tag = (uint64_t)(uint32_t)(k + 1) << 32;
+                if ((h & 0xffffffff00000000ull) != tag || (l & 0xffffffff00000000ull) != tag) {
+                    long long it = 0;
+                    while (true) {
+                        h = vfar[fs];
+                        l = vfar[fs + 1];
+                        if ((h & 0xffffffff00000000ull) == tag && (l & 0xffffffff00000000ull) == tag) break;
+                        if (++it > SP_SPIN_LIMIT || abort_flag) break;
+                    }
+                    if (__any_sync(0xffffffffu, it > SP_SPIN_LIMIT || abort_flag)) {
+                        err = 1;
+                        break;
+                    }
+                }
+                const double f = __hiloint2double((int)(uint32_t)h, (int)(uint32_t)l);
+                const bool r1 = (k & 32) != 0;   // the register of move k in its lane (k & 31)
+                const float fd = (float)(f + (r1 ? A1 : A0));
+                const float ediff = __fmul_rn(__fadd_rn(fd, 0.0f), temp);
+                const bool a = __ballot_sync(0xffffffffu, lane == (k & 31) && ediff < thr) != 0u;
+                // every pending move takes this move's correction; move k's sum restarts as move k+64's
+                const double d0 = a ? c0 : 0.0, d1 = a ? c1 : 0.0;
+                const bool own = lane == (k & 31);
+                A0 = (own && !r1) ? d0 : A0 + d0;
+                A1 = (own && r1) ? d1 : A1 + d1;
+                if (own) {
+                    S.acc[k] = a ? 1 : 0;
+                    S.fdiff[k] = fd;
+                }
+                const float fdk = __shfl_sync(0xffffffffu, fd, k & 31);
+                if (a) fadd += (double)fdk;
+                wbits |= (a ? 1u : 0u) << i;
             }
-            __syncwarp();
+            if (err) break;
+            if (lane == 0) vpub[b] = ((uint64_t)(uint32_t)(b + 1) << 32) | wbits;
         }
-        if (lane == 0) *S.fadd_acc = fadd;
-    } else {
-        const int nh = (blockDim.x >> 5) - 1;
-        for (int k = wid - 1; k < S.N; k += nh) {
-            const int need = max(k - SP_W, k - SP_RING + 1);
-            long long it = 0;
-            while (progress < need) {
-                if (++it > SP_SPIN_LIMIT || abort_flag) break;
+        if (lane == 0) {
+            if (err) {
+                fail();
+                // the copies still in flight land before the CTA's shared memory goes away
+                for (int b = waited; b < issued; ++b) umma::mbar_wait(&bars[b % SP_NSLOT], (uint32_t)((b / SP_NSLOT) & 1), nullptr);
             }
-            if (it > SP_SPIN_LIMIT || abort_flag) {
-                if (lane == 0) {
-                    abort_flag = 1;
-                    S.flags[1] = 1;
-                }
-                break;
-            }
-            __threadfence_block();
-            const int m = S.visit[k];
-            const int nn = S.nergpairm[m];
-            const size_t row = (size_t)m * S.M;
-            // two partners per lane in flight; the correction is read whether or not it applies
-            // (a stale value is masked), so its load does not wait for the partner's index
+            *S.fadd_acc = fadd;
+        }
+    } else if ((wid & 3) != 0) {
+        // ---- helper warps: the far part of each move's change.  The loads of a helper's next
+        // move are issued before it waits for the decisions its current move needs.
+        const int h = wid - 1 - (wid >> 2);
+        const int M = S.M;
+        int nn = 0, kp0 = -1, kp1 = -1;
+        double bk = 0.0, f0 = 0.0, f1 = 0.0;
+        auto load = [&](int kk, int &nn_, double &bk_, int &kp0_, int &kp1_, double &f0_, double &f1_) {
+            const size_t r = (size_t)kk * M;
+            nn_ = S.nnk[kk];
+            bk_ = S.base[kk];
+            kp0_ = 1 + lane < M ? S.fv[r + 1 + lane] : -1;
+            kp1_ = 33 + lane < M ? S.fv[r + 33 + lane] : -1;
+            f0_ = 1 + lane < M ? S.farc[r + 1 + lane] : 0.0;
+            f1_ = 33 + lane < M ? S.farc[r + 33 + lane] : 0.0;
+        };
+        if (h < N) load(h, nn, bk, kp0, kp1, f0, f1);
+        for (int k = h; k < N; k += SP_NH) {
+            int nn_n = 0, kp0_n = -1, kp1_n = -1;
+            double bk_n = 0.0, f0_n = 0.0, f1_n = 0.0;
+            if (k + SP_NH < N) load(k + SP_NH, nn_n, bk_n, kp0_n, kp1_n, f0_n, f1_n);
             double sum = 0.0;
-            for (int s = 1 + lane; s < nn; s += 64) {
-                const bool h2 = s + 32 < nn;
-                const int kp0 = S.fv[row + s];
-                const int kp1 = h2 ? S.fv[row + s + 32] : -1;
-                const double f0 = S.farc[row + s];
-                const double f1 = h2 ? S.farc[row + s + 32] : 0.0;
-                const bool u0 = kp0 >= 0 && ((accbits[kp0 >> 5] >> (kp0 & 31)) & 1u);
-                const bool u1 = kp1 >= 0 && ((accbits[kp1 >> 5] >> (kp1 & 31)) & 1u);
-                sum += u0 ? f0 : 0.0;
-                sum += u1 ? f1 : 0.0;
+            bool bad = false;
+            // the decision of partner kp (published in word kp / 32), waiting for the word
+            auto accepted = [&](int kp) -> bool {
+                const int w = kp / SP_BLK;
+                uint64_t v = vpub[w];
+                long long it = 0;
+                while ((uint32_t)(v >> 32) != (uint32_t)(w + 1)) {
+                    if (++it > SP_SPIN_LIMIT || abort_flag) {
+                        bad = true;
+                        return false;
+                    }
+                    __nanosleep(32);
+                    v = vpub[w];
+                }
+                return (v >> (kp % SP_BLK)) & 1ull;
+            };
+            if (1 + lane < nn && kp0 >= 0 && accepted(kp0)) sum += f0;
+            if (33 + lane < nn && kp1 >= 0 && accepted(kp1)) sum += f1;
+            for (int s0 = 65; s0 < nn; s0 += 64) {   // lists longer than 65 entries
+                const size_t r = (size_t)k * M;
+                const int sa = s0 + lane, sb = s0 + 32 + lane;
+                const int q0 = sa < nn ? S.fv[r + sa] : -1;
+                const int q1 = sb < nn ? S.fv[r + sb] : -1;
+                if (q0 >= 0 && accepted(q0)) sum += S.farc[r + sa];
+                if (q1 >= 0 && accepted(q1)) sum += S.farc[r + sb];
+            }
+            // the ring slot of move k was last read by the resolver at move k - SP_FR
+            if (k >= SP_FR && lane == 0) accepted(k - SP_FR);
+            if (__any_sync(0xffffffffu, bad)) {
+                if (lane == 0) fail();
+                break;
             }
             sum = warp_sum_d(sum);
             if (lane == 0) {
-                far_ring[k % SP_RING] = S.base[k] + sum;
-                __threadfence_block();
-                far_ready[k % SP_RING] = k + 1;
+                const double fk = bk + sum;
+                const uint64_t tag = (uint64_t)(uint32_t)(k + 1) << 32;
+                const int fs = 2 * (k % SP_FR);
+                vfar[fs] = tag | (uint32_t)__double2hiint(fk);
+                vfar[fs + 1] = tag | (uint32_t)__double2loint(fk);
             }
             __syncwarp();
+            nn = nn_n;
+            bk = bk_n;
+            kp0 = kp0_n;
+            kp1 = kp1_n;
+            f0 = f0_n;
+            f1 = f1_n;
         }
     }
 }
@@ -580,6 +688,92 @@ namespace epsr {
 __global__ void ran1_copy_kernel(const int32_t *src, int32_t *dst) {
     if (threadIdx.x < 35) dst[threadIdx.x] = src[threadIdx.x];
 }
+
+// Draws ahead.  The values a cycle draws are the next off[N] values of the one ran1 stream, a
+// function of the state the cycle starts from and of that count only.  While a cycle runs, a
+// second stream walks the stream on from where this cycle's draws end, into the caller's
+// buffer (int32 words):
+//   [AH_VALID] 1 once the values are complete   [AH_COUNT] how many   [AH_USES] cycles that took them
+//   [AH_START..+35) the state they start from   [AH_END..+35) the state after them
+//   [AH_VALS..) the values (float bits)
+// The next cycle takes them only when its starting state equals AH_START word for word and
+// it needs exactly AH_COUNT values; otherwise (another stage drew from the stream in
+// between, the cycle was redone by the sequential kernel, the caller set a new state) it
+// walks the stream itself.  Either way it draws the same values.
+constexpr int AH_VALID = 0, AH_COUNT = 1, AH_USES = 2, AH_START = 4, AH_END = 40, AH_VALS = 80;
+
+__global__ void ahead_adopt_kernel(const int32_t *state, int32_t *ahead, const int32_t *count, int32_t *next_state,
+                                   int32_t *nfill, int32_t *use) {
+    const int lane = threadIdx.x;
+    bool same = ahead[AH_START + lane] == state[lane];
+    if (lane < 3) same = same && ahead[AH_START + 32 + lane] == state[32 + lane];
+    const bool ok = __all_sync(0xffffffffu, same) && ahead[AH_VALID] == 1 && ahead[AH_COUNT] == *count;
+    if (ok) {
+        next_state[lane] = ahead[AH_END + lane];
+        if (lane < 3) next_state[32 + lane] = ahead[AH_END + 32 + lane];
+    }
+    if (lane == 0) {
+        *nfill = ok ? 0 : *count;
+        *use = ok ? 1 : 0;
+        if (ok) ahead[AH_USES] += 1;
+    }
+}
+
+__global__ void ahead_fill_kernel(const int32_t *state, int32_t *ahead, const int32_t *count) {
+    const int lane = threadIdx.x;
+    __shared__ int32_t tab[34];
+    const int64_t n = *count;
+    if (lane == 0) ahead[AH_VALID] = 0;
+    ahead[AH_START + lane] = state[lane];
+    if (lane < 3) ahead[AH_START + 32 + lane] = state[32 + lane];
+    Ran1Warp g;
+    g.load(state);
+    const int32_t mcall = state[2];
+    float *out = reinterpret_cast<float *>(ahead + AH_VALS);
+    __syncwarp();
+    int64_t done = 0;
+    while (done < n) {
+        const int64_t left = n - done;
+        int32_t mine;
+        const int cnt = g.next(left > 32 ? 32 : (int)left, mine, tab);
+        if (lane < cnt) out[done + lane] = ran1_out(mine);
+        done += cnt;
+    }
+    ahead[AH_END + 3 + lane] = g.iv;
+    if (lane == 0) {
+        ahead[AH_END + 0] = g.idum;
+        ahead[AH_END + 1] = g.iy;
+        ahead[AH_END + 2] = (int32_t)((uint32_t)mcall + (uint32_t)n);
+        ahead[AH_COUNT] = (int32_t)n;
+        __threadfence();
+        ahead[AH_VALID] = 1;
+    }
+}
+
+// The second stream and its two events, one set per host thread and device: boxes driven
+// from different threads never share them, and one thread's cycles run one after another.
+struct AheadStream {
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+static thread_local AheadStream g_ahead_streams[16];
+
+static int ahead_stream(AheadStream **out) {
+    int dev = 0;
+    EPSR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16) {
+        epsr_set_error("epsr_molfit: device ordinal %d beyond the draws-ahead table", dev);
+        return EPSR_ERR_ARG;
+    }
+    AheadStream &a = g_ahead_streams[dev];
+    if (!a.st) {
+        EPSR_CUDA(cudaStreamCreateWithFlags(&a.st, cudaStreamNonBlocking));
+        EPSR_CUDA(cudaEventCreateWithFlags(&a.fork, cudaEventDisableTiming));
+        EPSR_CUDA(cudaEventCreateWithFlags(&a.join, cudaEventDisableTiming));
+    }
+    *out = &a;
+    return EPSR_OK;
+}
 int ran1_fill_device_count(int32_t *state, float *out, const int32_t *n_dev, int64_t n_max, cudaStream_t s);
 int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
                       void *scratch, int64_t scratch_bytes, cudaStream_t s, const int32_t *run_if);
@@ -597,10 +791,11 @@ static size_t spec_bytes(int N, int natom, int M, int nmt) {
     b += spal(sizeof(int32_t) * 35);
     b += spal(sizeof(float) * ((size_t)N * 10 + 64));              // draws
     b += 3 * spal(sizeof(float) * natom) + spal(sizeof(float4) * N) + spal(sizeof(float4) * natom);
-    b += spal(sizeof(float) * N);                                  // thr
+    b += spal(sizeof(float) * ((size_t)N + SP_BLK));                 // thr (+ the last staged block's tail)
     b += 2 * spal(sizeof(float) * (size_t)N * M);                  // A, B
-    b += spal(sizeof(double) * N) + spal(sizeof(double) * (size_t)N * SP_W) + spal(sizeof(double) * (size_t)N * M);
-    b += spal(sizeof(int32_t) * (size_t)N * M);                    // fv
+    const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
+    b += spal(sizeof(double) * N) + spal(sizeof(double) * npad * SP_W) + spal(sizeof(double) * (size_t)N * M);
+    b += spal(sizeof(int32_t) * (size_t)N * M) + spal(sizeof(int32_t) * N);   // fv, nnk
     b += spal(sizeof(int32_t) * N) + spal(sizeof(float) * N) + spal(sizeof(double));
     return b;
 }
@@ -615,6 +810,16 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     if (!store->mirror) {
         epsr_set_error("epsr_molfit: the fast path needs the store's mirror index (built by epsr_fmolec1)");
         return EPSR_ERR_ARG;
+    }
+    {
+        int dev = 0, optin = 0;
+        EPSR_CUDA(cudaGetDevice(&dev));
+        EPSR_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        if (spec_resolve_smem(N) > (size_t)optin) {
+            epsr_set_error("epsr_molfit: %d molecules need %zu bytes of shared memory in the resolver (at most %d)", N,
+                           spec_resolve_smem(N), optin);
+            return EPSR_ERR_CAPACITY;
+        }
     }
     if ((int64_t)spec_bytes(N, natom, M, nmt) > scratch_bytes || !scratch) {
         epsr_set_error("epsr_molfit: scratch needs %lld bytes", (long long)spec_bytes(N, natom, M, nmt));
@@ -702,34 +907,57 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     S.nz = (float *)take(sizeof(float) * natom);
     S.nc = (float4 *)take(sizeof(float4) * N);
     S.npos = (float4 *)take(sizeof(float4) * natom);
-    S.thr = (float *)take(sizeof(float) * N);
+    S.thr = (float *)take(sizeof(float) * ((size_t)N + SP_BLK));
     S.A = (float *)take(sizeof(float) * (size_t)N * M);
     S.B = (float *)take(sizeof(float) * (size_t)N * M);
     S.base = (double *)take(sizeof(double) * N);
-    S.nearc = (double *)take(sizeof(double) * (size_t)N * SP_W);
+    const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
+    S.nearT = (double *)take(sizeof(double) * npad * SP_W);
     S.farc = (double *)take(sizeof(double) * (size_t)N * M);
     S.fv = (int32_t *)take(sizeof(int32_t) * (size_t)N * M);
+    S.nnk = (int32_t *)take(sizeof(int32_t) * N);
     S.acc = (int32_t *)take(sizeof(int32_t) * N);
     S.fdiff = (float *)take(sizeof(float) * N);
     S.fadd_acc = (double *)take(sizeof(double));
 
+    // draws ahead: only with a buffer that holds a whole cycle's values (at most 7 a move)
+    const bool ahead = mc->ahead && mc->ahead_cap >= (int64_t)N * 7;
+    int32_t *nfill = S.flags + 2, *use = S.flags + 3;
+    if (ahead) {
+        S.ahead_vals = reinterpret_cast<const float *>(mc->ahead + AH_VALS);
+        S.use_ahead = use;
+    }
     spec_plan_kernel<<<1, 1024, 0, s>>>(S);
     ran1_copy_kernel<<<1, 64, 0, s>>>(mc->ran1, S.ran1_next);
-    int rc = ran1_fill_device_count(S.ran1_next, S.draws, S.off + N, (int64_t)N * 7 + 1, s);
+    if (ahead) ahead_adopt_kernel<<<1, 32, 0, s>>>(mc->ran1, mc->ahead, S.off + N, S.ran1_next, nfill, use);
+    int rc = ran1_fill_device_count(S.ran1_next, S.draws, ahead ? nfill : S.off + N, (int64_t)N * 7 + 1, s);
     if (rc) return rc;
     spec_propose_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
+    // the next cycle's values, from the state after this cycle's draws, on the second stream
+    // once nothing of this cycle reads the buffer any more; joined before this call returns
+    AheadStream *as = nullptr;
+    if (ahead) {
+        rc = ahead_stream(&as);
+        if (rc) return rc;
+        EPSR_CUDA(cudaEventRecord(as->fork, s));
+        EPSR_CUDA(cudaStreamWaitEvent(as->st, as->fork, 0));
+        ahead_fill_kernel<<<1, 32, 0, as->st>>>(S.ran1_next, mc->ahead, S.off + N);
+        EPSR_CUDA(cudaGetLastError());
+        EPSR_CUDA(cudaEventRecord(as->join, as->st));
+    }
     const size_t en_bytes = sizeof(int) * ((((size_t)box->ntype * box->ntype + 3) & ~(size_t)3) + 2 * (size_t)M);
     if (en_bytes > 48 * 1024) EPSR_SMEM_OPTIN(spec_energy_kernel);
     EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, SP_ET, en_bytes, s>>>(S));
-    EPSR_CUDA(cudaMemsetAsync(S.nearc, 0, sizeof(double) * (size_t)N * SP_W, s));
+    EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(double) * npad * SP_W, s));
     EPSR_TIMED("spec_corr_kernel", s, spec_corr_kernel<<<N, 128, 0, s>>>(S));
-    const size_t bits = sizeof(unsigned) * (((size_t)N + 31) / 32);
-    if (bits > 48 * 1024) EPSR_SMEM_OPTIN(spec_resolve_kernel);
-    EPSR_TIMED("spec_resolve_kernel", s, spec_resolve_kernel<<<1, SP_RT, bits, s>>>(S));
+    const size_t rsmem = spec_resolve_smem(N);
+    EPSR_SMEM_OPTIN(spec_resolve_kernel);
+    EPSR_TIMED("spec_resolve_kernel", s, spec_resolve_kernel<<<1, SP_RT, rsmem, s>>>(S));
     spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
     spec_commit_store_kernel<<<N, 128, 0, s>>>(S);
     spec_epilogue_kernel<<<1, 32, 0, s>>>(S);
     EPSR_CUDA(cudaGetLastError());
+    if (ahead) EPSR_CUDA(cudaStreamWaitEvent(s, as->join, 0));
     // a cycle with a translation retry runs on the sequential kernel (no-op otherwise)
     return molfit_seq_launch(box, cells, store, mc, nullptr, 0, s, S.flags);
 }

@@ -244,8 +244,17 @@ class DeviceBox:
         m.strict = 1
         self.m_status = torch.zeros(1, dtype=torch.int32, device=self.dev)
         m.status = _ptr(self.m_status)
+        # the next cycle's ran1 values walked on a second stream while a fast cycle runs
+        self.m_ahead = torch.zeros(80 + 7 * b.nmol, dtype=torch.int32, device=self.dev)
+        m.ahead, m.ahead_cap = _ptr(self.m_ahead), 7 * b.nmol
         self.cmc = m
         return m
+
+    def draws_ahead(self, on=True):
+        """Enable or disable the fast path's draws ahead; returns how many cycles took them."""
+        m = self.cmc
+        m.ahead, m.ahead_cap = (_ptr(self.m_ahead), 7 * self.host.nmol) if on else (None, 0)
+        return int(self.m_ahead[2].item())
 
     def set_rotations(self, intra_model, nrf, nrl, axis, first, last, atoms, stepri=1.0, faddbs=0.0):
         """Internal rotations of rotational groups (type ROT: the dihedral terms of DIH groups

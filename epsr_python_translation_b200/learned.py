@@ -174,5 +174,7 @@ class LearnedMC:
     def residual_rmse(self):
         """RMS of beta dE - s over the moves of the last DA step that passed the first stage."""
         r = self.bb.resid
+        if r is None:     # no delayed-acceptance step has run
+            return None
         r = r[torch.isfinite(r)]
         return float(torch.sqrt(torch.mean(r * r)).item()) if r.numel() else None

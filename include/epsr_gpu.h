@@ -164,6 +164,14 @@ typedef struct {
     int32_t rotcycle;               /* nonzero in a cycle where nisum is a multiple of rotfreq */
     int32_t *ninter;                /* [2*nmoltype] device: internal-rotation tries then rejections */
     float *faddbs;                  /* [1] device or NULL: faddbs += sum(accepted intra changes)/nmol */
+    /* Draws ahead (fast path only): NULL, or device int32 [80 + ahead_cap].  While a cycle runs,
+     * a second stream walks the ran1 stream on from where the cycle's draws end and keeps the
+     * values here with the states they start from and lead to; the next cycle takes them when
+     * it starts from exactly that state, and walks the stream itself otherwise -- the values
+     * are the same either way.  Word 2 counts the cycles that took them.  ahead_cap >= 7*nmol
+     * enables it; zero the buffer once before the first cycle. */
+    int32_t *ahead;
+    int64_t ahead_cap;
 } epsr_mc_t;
 
 /* molfit molfit.py:52-541, whole-molecule branch (:268-448) and step adaptation
