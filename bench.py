@@ -859,7 +859,7 @@ def learned_c5(a, steps=None):
     x, t = lm.collect(a.c5_pairs)
     torch.cuda.synchronize()
     rec_s = time.perf_counter() - tr0
-    rep = lm.train(x, t, epochs=4, batch=2048, lr=1e-3)
+    rep = lm.train(x, t, epochs=24, batch=2048, lr=1e-3)
     del x, t
     torch.cuda.empty_cache()
     sd, ms_d, cd, mode = lm.run(nsw, "da")

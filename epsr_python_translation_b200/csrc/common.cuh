@@ -170,20 +170,27 @@ __device__ __forceinline__ uint32_t r1_mulmod(uint32_t a, uint32_t b) {
 }
 
 // 32 steps of the shuffle when no value of the batch can be zero: idl is this lane's Park-
-// Miller value of the batch (step lane+1), iv this lane's table entry, iy warp-uniform.  A
-// step is two shuffles: the value in slot j (whose top 5 bits give the next slot: the only
-// dependence from step to step) and the step's Park-Miller value from the lane that holds
-// it, which the lane owning slot j keeps.  Returns the value of step `lane`; updates iv, iy.
+// Miller value of the batch (step lane+1), iv this lane's table entry, iy warp-uniform.  The
+// only dependence from step to step is the next slot, the top 5 bits of the value in slot
+// j; each lane keeps those bits of its entry beside it, so a step's critical path is one
+// shuffle of the 5-bit slot numbers.  The value itself and the step's Park-Miller value
+// (which the lane owning slot j keeps) are shuffled beside it.  Returns the value of step
+// `lane`; updates iv, iy.
 __device__ __forceinline__ int32_t ran1_chain32(int32_t idl, int32_t &iv, int32_t &iy) {
     const int lane = threadIdx.x & 31;
     int32_t y = iy, mine = 0;
+    int j = y >> 26;            // iy / NDIV, NDIV = 2^26
+    int t5 = iv >> 26;          // the next slot after this lane's entry
 #pragma unroll
     for (int s = 0; s < 32; ++s) {
-        const int j = y >> 26;   // iy / NDIV, NDIV = 2^26
+        const int jn = __shfl_sync(0xffffffffu, t5, j);
         const int32_t id = __shfl_sync(0xffffffffu, idl, s);
         y = __shfl_sync(0xffffffffu, iv, j);
-        iv = (lane == j) ? id : iv;
+        const bool own = lane == j;
+        iv = own ? id : iv;
+        t5 = own ? (id >> 26) : t5;
         mine = (lane == s) ? y : mine;
+        j = jn;
     }
     iy = y;
     return mine;

@@ -86,7 +86,7 @@ struct SpecDev {
     float *A, *B;                          // [N*M]
     double *base, *nearT, *farc;           // [N], [Npad*W] by the earlier move, [N*M]
     int32_t *fv;                           // [N*M] by visit position
-    int32_t *nnk;                          // [N] entries of each move's list
+    int32_t *nnk;                          // [N] far partners listed for each move
     int32_t *acc;                          // [N] by visit position
     float *fdiff;                          // [N] by visit position
     double *fadd_acc;                      // [1]
@@ -261,119 +261,116 @@ __global__ void spec_propose_kernel(SpecDev S) {
 // ----------------------------------------------------------------- energies
 // E(a, b): a's atoms in shared memory (sa), b's absolute positions in global memory (read
 // through the L1 cache for every atom of a, which keeps registers -- and so resident warps --
-// free for latency hiding).  The sum runs ia outer, ja inner as en_change (molfit.py:851-882).
-__device__ __forceinline__ float mol_energy(const Lattice &L, const Tables &T, const float4 *sa, int na,
-                                            const float4 *__restrict__ pb, int nb, const int *spr, int ntype) {
-    float sume = 0.0f;
+// free for latency hiding).
+// Both energies of one partner in one pass over its atoms: A against its cycle-start
+// position (pa), B against its proposed position (pn) when has_b; each summed ia outer, ja
+// inner as en_change, so each is the reference's value.
+__device__ __forceinline__ void mol_energy_ab(const Lattice &L, const Tables &T, const float4 *sa, int na,
+                                              const float4 *__restrict__ pa, const float4 *__restrict__ pn, int nb,
+                                              bool has_b, const int *spr, int ntype, float &ea, float &eb) {
+    float xa = 0.0f, xb = 0.0f;
     for (int ia = 0; ia < na; ++ia) {
         const float4 p1 = sa[ia];
         const int *row = spr + __float_as_int(p1.w) * ntype;
-#pragma unroll 4
+#pragma unroll 2
         for (int j = 0; j < nb; ++j) {
-            const float4 p2 = __ldg(pb + j);
-            sume = __fadd_rn(sume, pair_energy(L, T, p1, p2, row[__float_as_int(p2.w)]));
+            const float4 p2 = __ldg(pa + j);
+            const int ic = row[__float_as_int(p2.w)];
+            xa = __fadd_rn(xa, pair_energy(L, T, p1, p2, ic));
+            if (has_b) xb = __fadd_rn(xb, pair_energy(L, T, p1, __ldg(pn + j), ic));
         }
     }
-    return sume;
+    ea = xa;
+    eb = xb;
 }
 
+// One CTA per move, one thread per stored partner: the partner's A and, if it is visited
+// earlier in the cycle, its B.
 __global__ void __launch_bounds__(SP_ET) spec_energy_kernel(SpecDev S) {
-    extern __shared__ int sdyn[];   // npairref [ntype*ntype], then the work list [2*M]
+    extern __shared__ int spr[];   // npairref [ntype*ntype]
     __shared__ float4 sa[SP_MAXAT];
-    __shared__ int cnt[SP_MAXAT + 2];
     if (S.flags[0]) return;
-    int *spr = sdyn;
-    int *list = sdyn + ((S.ntype * S.ntype + 3) & ~3);
     const int k = blockIdx.x;
     const int m = S.visit[k];
     const int na = S.nato[m], a0 = S.naf[m];
     for (int i = threadIdx.x; i < S.ntype * S.ntype; i += blockDim.x) spr[i] = S.npairref[i];
     for (int i = threadIdx.x; i < na; i += blockDim.x) sa[i] = S.npos[a0 + i];
-    for (int i = threadIdx.x; i < SP_MAXAT + 2; i += blockDim.x) cnt[i] = 0;
     __syncthreads();
     const int nn = S.nergpairm[m];
     const size_t row = (size_t)m * S.M;
-    // work items: A for partners 1..nn-1 (item s-1), then B for the same partners (item
-    // np+s-1) when the partner is earlier in the visit order.  The items are listed by the
-    // partner's atom count, so the lanes of a warp run loops of the same length.
-    const int np = nn - 1;
-    auto item_nb = [&](int it) -> int {   // atom count (1..SP_MAXAT) of the item's partner, 0 if no item
-        const bool second = it >= np;
-        const int p = S.molergpair[row + 1 + (second ? it - np : it)];
-        if (second && S.vpos[p] >= k) return 0;
-        return S.nato[p];
-    };
-    for (int it = threadIdx.x; it < 2 * np; it += blockDim.x) {
-        const int nb = item_nb(it);
-        if (nb > 0) atomicAdd(&cnt[nb], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {   // cnt[b] -> first list position of atom count b; cnt[SP_MAXAT+1] = total
-        int a = 0;
-        for (int b = 0; b <= SP_MAXAT; ++b) {
-            const int c = cnt[b];
-            cnt[b] = a;
-            a += c;
-        }
-        cnt[SP_MAXAT + 1] = a;
-    }
-    __syncthreads();
-    for (int it = threadIdx.x; it < 2 * np; it += blockDim.x) {
-        const int nb = item_nb(it);
-        if (nb > 0) list[atomicAdd(&cnt[nb], 1)] = it;
-    }
-    __syncthreads();
-    const int total = cnt[SP_MAXAT + 1];
-    for (int q = threadIdx.x; q < total; q += blockDim.x) {
-        const int it = list[q];
-        const bool second = it >= np;
-        const int s = 1 + (second ? it - np : it);
+    for (int s = 1 + threadIdx.x; s < nn; s += blockDim.x) {
         const int p = S.molergpair[row + s];
         const int b0 = S.naf[p], nb = S.nato[p];
-        const float e = __fadd_rn(0.0f, mol_energy(S.L, S.T, sa, na, (second ? S.npos : S.pos) + b0, nb, spr, S.ntype));
-        if (second) S.B[row + s] = e;
-        else S.A[row + s] = e;
+        const bool hb = S.vpos[p] < k;
+        float ea, eb;
+        mol_energy_ab(S.L, S.T, sa, na, S.pos + b0, S.npos + b0, nb, hb, spr, S.ntype, ea, eb);
+        S.A[row + s] = __fadd_rn(0.0f, ea);
+        if (hb) S.B[row + s] = __fadd_rn(0.0f, eb);
     }
 }
 
 // ----------------------------------------------------------------- corrections
+// Per move k (one CTA): base[k] = sum over its stored partners of A - S (the change if no
+// earlier partner accepted), and for each partner p visited earlier the correction c that
+// applies if p accepted.  Partners at most SP_W moves earlier go into p's row of nearT (the
+// resolver adds them as decisions are taken); the others are listed for the helpers in
+// store order, compacted to the front of k's row of fv/farc (nfar[k] of them).
 __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
+    __shared__ double ws[4];
+    __shared__ int wcount[4];
     if (S.flags[0]) return;
     const int k = blockIdx.x;
     const int m = S.visit[k];
     const int nn = S.nergpairm[m];
-    const size_t row = (size_t)m * S.M;
+    const size_t row = (size_t)m * S.M, krow = (size_t)k * S.M;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     double d0s = 0.0;
-    for (int s = 1 + threadIdx.x; s < nn; s += blockDim.x) {
-        const size_t e = row + s;
-        const int p = S.molergpair[e];
-        const int kp = S.vpos[p];
-        const double sv = (double)S.ergpair[S.ergpairref[e] - 1];
-        const double d0 = (double)S.A[e] - sv;
-        d0s += d0;
-        int fvv = -1;
-        if (kp < k) {
-            const int e2 = S.mirror[e];
-            const int s2 = e2 % S.M;
-            const double oldp = s2 >= 1 ? (double)S.A[e2] : sv;
-            const double c = ((double)S.B[e] - oldp) - d0;
-            const int dist = k - kp;
-            if (dist <= SP_W) {
-                S.nearT[(size_t)kp * SP_W + dist - 1] = c;
-            } else {
-                S.farc[(size_t)k * S.M + s] = c;
-                fvv = kp;
+    int nfar = 0;   // far partners listed so far (block-uniform)
+    for (int s0 = 1; s0 < nn; s0 += blockDim.x) {
+        const int s = s0 + threadIdx.x;
+        bool far = false;
+        int kp = -1;
+        double c = 0.0;
+        if (s < nn) {
+            const size_t e = row + s;
+            const int p = S.molergpair[e];
+            kp = S.vpos[p];
+            const double sv = (double)S.ergpair[S.ergpairref[e] - 1];
+            const double d0 = (double)S.A[e] - sv;
+            d0s += d0;
+            if (kp < k) {
+                const int e2 = S.mirror[e];
+                const int s2 = e2 % S.M;
+                const double oldp = s2 >= 1 ? (double)S.A[e2] : sv;
+                c = ((double)S.B[e] - oldp) - d0;
+                const int dist = k - kp;
+                if (dist <= SP_W) S.nearT[(size_t)kp * SP_W + dist - 1] = c;
+                else far = true;
             }
         }
-        S.fv[(size_t)k * S.M + s] = fvv;   // the far partners by visit position, for the helpers
+        // ordered compaction of this chunk's far partners
+        const unsigned bal = __ballot_sync(0xffffffffu, far);
+        if (lane == 0) wcount[wid] = __popc(bal);
+        __syncthreads();
+        int off = nfar, tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            if (w < wid) off += wcount[w];
+            tot += wcount[w];
+        }
+        if (far) {
+            const int i = off + __popc(bal & ((1u << lane) - 1u));
+            S.fv[krow + i] = kp;
+            S.farc[krow + i] = c;
+        }
+        nfar += tot;
+        __syncthreads();
     }
     d0s = warp_sum_d(d0s);
-    __shared__ double ws[4];
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = d0s;
+    if (lane == 0) ws[wid] = d0s;
     __syncthreads();
     if (threadIdx.x == 0) {
         S.base[k] = ws[0] + ws[1] + ws[2] + ws[3];
-        S.nnk[k] = nn;
+        S.nnk[k] = nfar;
     }
 }
 
@@ -389,7 +386,7 @@ __host__ __device__ constexpr size_t spec_resolve_smem(int N) {
     return (size_t)SP_SHDR + 8 * (size_t)((N + SP_BLK - 1) / SP_BLK);
 }
 
-__global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
+__global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
     extern __shared__ __align__(128) unsigned char rsm[];
     double *srows = reinterpret_cast<double *>(rsm);
     float *sthr = reinterpret_cast<float *>(rsm + SP_SROWS);
@@ -448,13 +445,15 @@ __global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
             const float *th = sthr + slot * SP_BLK;
             const int nr = min(SP_BLK, N - SP_BLK * b);
             unsigned wbits = 0u;
+            // the far words of the next move are read as soon as a decision is out
+            uint64_t hn = vfar[2 * ((SP_BLK * b) % SP_FR)], ln = vfar[2 * ((SP_BLK * b) % SP_FR) + 1];
             for (int i = 0; i < nr; ++i) {
                 const int k = SP_BLK * b + i;
                 const int i0 = (lane + SP_W - 1 - (k & (SP_W - 1))) & (SP_W - 1);   // distance - 1 of this lane's first move
                 const double c0 = rows[i * SP_W + i0], c1 = rows[i * SP_W + ((i0 + 32) & (SP_W - 1))];
                 const float thr = th[i];
                 const int fs = 2 * (k % SP_FR);
-                uint64_t h = vfar[fs], l = vfar[fs + 1];
+                uint64_t h = hn, l = ln;
                 const uint64_t tag = (uint64_t)(uint32_t)(k + 1) << 32;
                 if ((h & 0xffffffff00000000ull) != tag || (l & 0xffffffff00000000ull) != tag) {
                     long long it = 0;
@@ -474,6 +473,10 @@ __global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
                 const float fd = (float)(f + (r1 ? A1 : A0));
                 const float ediff = __fmul_rn(__fadd_rn(fd, 0.0f), temp);
                 const bool a = __ballot_sync(0xffffffffu, lane == (k & 31) && ediff < thr) != 0u;
+                if (i + 1 < nr) {
+                    hn = vfar[2 * ((k + 1) % SP_FR)];
+                    ln = vfar[2 * ((k + 1) % SP_FR) + 1];
+                }
                 // every pending move takes this move's correction; move k's sum restarts as move k+64's
                 const double d0 = a ? c0 : 0.0, d1 = a ? c1 : 0.0;
                 const bool own = lane == (k & 31);
@@ -500,30 +503,33 @@ __global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
         }
     } else if ((wid & 3) != 0) {
         // ---- helper warps: the far part of each move's change.  The loads of a helper's next
-        // move are issued before it waits for the decisions its current move needs.
+        // move (its first 128 listed far partners) are issued before it waits for the
+        // decisions its current move needs.
         const int h = wid - 1 - (wid >> 2);
         const int M = S.M;
-        int nn = 0, kp0 = -1, kp1 = -1;
-        double bk = 0.0, f0 = 0.0, f1 = 0.0;
-        auto load = [&](int kk, int &nn_, double &bk_, int &kp0_, int &kp1_, double &f0_, double &f1_) {
+        int nf = 0, kp[4];
+        double bk = 0.0, cf[4];
+        auto load = [&](int kk, int &nf_, double &bk_, int (&kp_)[4], double (&cf_)[4]) {
             const size_t r = (size_t)kk * M;
-            nn_ = S.nnk[kk];
+            nf_ = S.nnk[kk];
             bk_ = S.base[kk];
-            kp0_ = 1 + lane < M ? S.fv[r + 1 + lane] : -1;
-            kp1_ = 33 + lane < M ? S.fv[r + 33 + lane] : -1;
-            f0_ = 1 + lane < M ? S.farc[r + 1 + lane] : 0.0;
-            f1_ = 33 + lane < M ? S.farc[r + 33 + lane] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = lane + 32 * q;
+                kp_[q] = i < M ? S.fv[r + i] : -1;
+                cf_[q] = i < M ? S.farc[r + i] : 0.0;
+            }
         };
-        if (h < N) load(h, nn, bk, kp0, kp1, f0, f1);
+        if (h < N) load(h, nf, bk, kp, cf);
         for (int k = h; k < N; k += SP_NH) {
-            int nn_n = 0, kp0_n = -1, kp1_n = -1;
-            double bk_n = 0.0, f0_n = 0.0, f1_n = 0.0;
-            if (k + SP_NH < N) load(k + SP_NH, nn_n, bk_n, kp0_n, kp1_n, f0_n, f1_n);
+            int nf_n = 0, kp_n[4] = {-1, -1, -1, -1};
+            double bk_n = 0.0, cf_n[4] = {0.0, 0.0, 0.0, 0.0};
+            if (k + SP_NH < N) load(k + SP_NH, nf_n, bk_n, kp_n, cf_n);
             double sum = 0.0;
             bool bad = false;
             // the decision of partner kp (published in word kp / 32), waiting for the word
-            auto accepted = [&](int kp) -> bool {
-                const int w = kp / SP_BLK;
+            auto accepted = [&](int kq) -> bool {
+                const int w = kq / SP_BLK;
                 uint64_t v = vpub[w];
                 long long it = 0;
                 while ((uint32_t)(v >> 32) != (uint32_t)(w + 1)) {
@@ -534,17 +540,16 @@ __global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
                     __nanosleep(32);
                     v = vpub[w];
                 }
-                return (v >> (kp % SP_BLK)) & 1ull;
+                return (v >> (kq % SP_BLK)) & 1ull;
             };
-            if (1 + lane < nn && kp0 >= 0 && accepted(kp0)) sum += f0;
-            if (33 + lane < nn && kp1 >= 0 && accepted(kp1)) sum += f1;
-            for (int s0 = 65; s0 < nn; s0 += 64) {   // lists longer than 65 entries
+            // the listed order, lane by lane: entry lane + 32 q
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (lane + 32 * q < nf && accepted(kp[q])) sum += cf[q];
+            for (int i = 128 + lane; i < nf; i += 32) {   // lists longer than 128 entries
                 const size_t r = (size_t)k * M;
-                const int sa = s0 + lane, sb = s0 + 32 + lane;
-                const int q0 = sa < nn ? S.fv[r + sa] : -1;
-                const int q1 = sb < nn ? S.fv[r + sb] : -1;
-                if (q0 >= 0 && accepted(q0)) sum += S.farc[r + sa];
-                if (q1 >= 0 && accepted(q1)) sum += S.farc[r + sb];
+                const int q0 = S.fv[r + i];
+                if (accepted(q0)) sum += S.farc[r + i];
             }
             // the ring slot of move k was last read by the resolver at move k - SP_FR
             if (k >= SP_FR && lane == 0) accepted(k - SP_FR);
@@ -561,12 +566,13 @@ __global__ void __launch_bounds__(SP_RT) spec_resolve_kernel(SpecDev S) {
                 vfar[fs + 1] = tag | (uint32_t)__double2loint(fk);
             }
             __syncwarp();
-            nn = nn_n;
+            nf = nf_n;
             bk = bk_n;
-            kp0 = kp0_n;
-            kp1 = kp1_n;
-            f0 = f0_n;
-            f1 = f1_n;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                kp[q] = kp_n[q];
+                cf[q] = cf_n[q];
+            }
         }
     }
 }
@@ -945,9 +951,10 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
         EPSR_CUDA(cudaGetLastError());
         EPSR_CUDA(cudaEventRecord(as->join, as->st));
     }
-    const size_t en_bytes = sizeof(int) * ((((size_t)box->ntype * box->ntype + 3) & ~(size_t)3) + 2 * (size_t)M);
+    const size_t en_bytes = sizeof(int) * (size_t)box->ntype * box->ntype;
     if (en_bytes > 48 * 1024) EPSR_SMEM_OPTIN(spec_energy_kernel);
-    EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, SP_ET, en_bytes, s>>>(S));
+    const int en_threads = min(SP_ET, max(32, (M - 1 + 31) / 32 * 32));   // one thread per stored partner
+    EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, en_threads, en_bytes, s>>>(S));
     EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(double) * npad * SP_W, s));
     EPSR_TIMED("spec_corr_kernel", s, spec_corr_kernel<<<N, 128, 0, s>>>(S));
     const size_t rsmem = spec_resolve_smem(N);

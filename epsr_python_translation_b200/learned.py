@@ -12,9 +12,9 @@ the surrogate changes only how much exact work a move costs, never what is sampl
 
 The network (surrogate.SurrogateNet: 1280 -> 128 -> 128 -> 1, SiLU, BF16 weights, FP32
 accumulation, hand-written tcgen05 kernels) is trained on (features, beta dE) pairs that the
-plain batched run records, with a held-out split; when the held-out RMS error exceeds
-``RMSE_BOUND`` (in units of kT) -- or the residual beta dE - s of the moves the run evaluates
-exactly drifts above it -- the plain single-stage path takes over.
+plain batched run records, with a held-out split; when the held-out RMS error (estimates and
+targets clipped at ``TARGET_CLIP``, beyond which both stages reject anyway) exceeds
+``RMSE_BOUND`` (in units of kT) the plain single-stage path takes over.
 
 The boxes advance by the batched checkerboard scheme of batch.BatchBoxes, each sweep replayed
 from a CUDA graph.  The effective sample size of each box's total-energy series is estimated
@@ -32,7 +32,8 @@ from .batch import FEAT_IN, BatchBoxes
 from .surrogate import SurrogateNet
 
 RMSE_BOUND = 2.0        # kT: above this held-out error the plain single-stage path runs
-TARGET_CLIP = 30.0      # kT: training targets are clipped (a larger beta dE is a certain rejection)
+TARGET_CLIP = 12.0      # kT: targets (and, for the held-out error, estimates) are clipped here:
+                        # beyond it both stages reject with probability above 1 - 6e-6
 
 
 def integrated_time(x, c=5.0):
@@ -99,9 +100,10 @@ class LearnedMC:
 
     # ------------------------------------------------------------------ training
     def train(self, x, t, epochs=4, batch=2048, lr=1e-3, heldout=0.05, seed=0):
-        """Adam on the pairs (clipped targets), a held-out fraction kept aside; returns dict with
-        the loss per epoch and the held-out RMS error of s (kT).  Batches are contiguous runs of
-        pairs after one random permutation."""
+        """Adam on the pairs (clipped targets), a held-out fraction kept aside, the learning
+        rate decayed over the epochs on a half cosine; returns dict with the loss per epoch and
+        the held-out RMS error of s (kT).  Batches are contiguous runs of pairs after one random
+        permutation."""
         npairs = t.numel()
         g = torch.Generator(device="cpu").manual_seed(seed)
         perm = torch.randperm(npairs, generator=g).to(self.dev)
@@ -120,8 +122,9 @@ class LearnedMC:
             tot = 0.0
             order = torch.randperm(nb, generator=g).tolist()
             acc = torch.zeros(1, dtype=torch.float64, device=self.dev)
+            lr_ep = lr * 0.5 * (1.0 + np.cos(np.pi * ep / max(epochs, 1)))
             for bi in order:
-                self.net.train_step(xtr, xtt, bi * batch, batch, ttr, lr, loss=loss)
+                self.net.train_step(xtr, xtt, bi * batch, batch, ttr, lr_ep, loss=loss)
                 acc += loss.double()
             tot = float(acc.item()) / ntr
             hist.append(tot)
@@ -143,7 +146,7 @@ class LearnedMC:
     def heldout_error(self, x, t, idx):
         rows = torch.stack([2 * idx, 2 * idx + 1], 1).reshape(-1)
         xh = x[rows].contiguous()
-        s = self.surrogate(xh)
+        s = self.surrogate(xh).clamp(-TARGET_CLIP, TARGET_CLIP)
         tt = t[idx].clamp(-TARGET_CLIP, TARGET_CLIP)
         return float(torch.sqrt(torch.mean((s - tt) ** 2)).item())
 
