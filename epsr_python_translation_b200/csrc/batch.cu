@@ -302,6 +302,7 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_propose_kernel(epsr_bmc_t B, 
     const float binf = (float)FEAT_BINS / FEAT_RMAX * X.dmax;   // bins per box unit
     const float mx = B.xadd[mol], my = B.yadd[mol], mz = B.zadd[mol];
     const float rfc2 = __fmul_rn(X.rfeat_c, X.rfeat_c);
+    const float rsq_skip = (float)((double)rf * (double)rf * (1.0 + 1e-5));   // d >= rf beyond it
     for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
         const int jm = list[p];
         if (jm == mol) continue;
@@ -319,12 +320,23 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_propose_kernel(epsr_bmc_t B, 
             for (int a = 0; a < na_; ++a) {
                 const int ca = B.fclass[B.naf[mol] + a];
                 const int fc = feat_class(ca, cb) * FEAT_BINS;
-                const float d0 = dist_f(L, __fsub_rn(pb.x, p_old[a].x), __fsub_rn(pb.y, p_old[a].y),
-                                        __fsub_rn(pb.z, p_old[a].z));
-                const float d1 = dist_f(L, __fsub_rn(pb.x, p_new[a].x), __fsub_rn(pb.y, p_new[a].y),
-                                        __fsub_rn(pb.z, p_new[a].z));
-                if (d0 < rf) atomicAdd(&hist[fc + min((int)__fmul_rn(d0, binf), FEAT_BINS - 1)], 1);
-                if (d1 < rf) atomicAdd(&hist[FEAT_HALF + fc + min((int)__fmul_rn(d1, binf), FEAT_BINS - 1)], 1);
+                // the square root only for pairs that can be within rf
+                float x0 = __fsub_rn(pb.x, p_old[a].x), y0 = __fsub_rn(pb.y, p_old[a].y),
+                      z0 = __fsub_rn(pb.z, p_old[a].z);
+                float x1 = __fsub_rn(pb.x, p_new[a].x), y1 = __fsub_rn(pb.y, p_new[a].y),
+                      z1 = __fsub_rn(pb.z, p_new[a].z);
+                minimagec(L, x0, y0, z0);
+                minimagec(L, x1, y1, z1);
+                const float q0 = __fadd_rn(__fadd_rn(__fmul_rn(x0, x0), __fmul_rn(y0, y0)), __fmul_rn(z0, z0));
+                const float q1 = __fadd_rn(__fadd_rn(__fmul_rn(x1, x1), __fmul_rn(y1, y1)), __fmul_rn(z1, z1));
+                if (q0 <= rsq_skip) {
+                    const float d0 = __fsqrt_rn(q0);
+                    if (d0 < rf) atomicAdd(&hist[fc + min((int)__fmul_rn(d0, binf), FEAT_BINS - 1)], 1);
+                }
+                if (q1 <= rsq_skip) {
+                    const float d1 = __fsqrt_rn(q1);
+                    if (d1 < rf) atomicAdd(&hist[FEAT_HALF + fc + min((int)__fmul_rn(d1, binf), FEAT_BINS - 1)], 1);
+                }
             }
         }
     }
@@ -410,6 +422,7 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_decide_kernel(epsr_bmc_t B, i
     Lattice L;
     L.cubic = 1;
     const Tables T = box_tables(B, X);
+    const float dsq_skip = skip_dsq(T.stepcl, T.izcut);
     const int *pr = B.npairref + X.npairref0;
     const float cx = B.xadd[mol], cy = B.yadd[mol], cz = B.zadd[mol];
     const float rint = X.rint;
@@ -432,8 +445,8 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_decide_kernel(epsr_bmc_t B, i
             for (int q = 0; q < nb; ++q) {
                 const float4 pb = atom_pos(B, b0 + q);
                 const int icref = row[__float_as_int(pb.w)];
-                e_new = __fadd_rn(e_new, pair_energy(L, T, p_new[a], pb, icref));
-                e_old = __fadd_rn(e_old, pair_energy(L, T, p_old[a], pb, icref));
+                e_new = __fadd_rn(e_new, pair_energy_far(L, T, dsq_skip, p_new[a], pb, icref));
+                e_old = __fadd_rn(e_old, pair_energy_far(L, T, dsq_skip, p_old[a], pb, icref));
             }
         }
         de += (double)e_new - (double)e_old;
@@ -484,6 +497,7 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_mol_energy_kernel(epsr_bmc_t 
     Lattice L;
     L.cubic = 1;
     const Tables T = box_tables(B, X);
+    const float dsq_skip = skip_dsq(T.stepcl, T.izcut);
     const int *pr = B.npairref + X.npairref0;
     const int a0 = B.naf[mol], na_ = B.nato[mol];
     double e = 0.0;
@@ -497,7 +511,7 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_mol_energy_kernel(epsr_bmc_t 
             const int *row = pr + __float_as_int(pa.w) * X.ntype;
             for (int q = 0; q < nb; ++q) {
                 const float4 pb = atom_pos(B, b0 + q);
-                s = __fadd_rn(s, pair_energy(L, T, pa, pb, row[__float_as_int(pb.w)]));
+                s = __fadd_rn(s, pair_energy_far(L, T, dsq_skip, pa, pb, row[__float_as_int(pb.w)]));
             }
         }
         e += (double)s;

@@ -95,6 +95,27 @@ __device__ __forceinline__ float pair_energy_d(const Tables &T, float d, int icr
     return in ? sume : 0.0f;
 }
 
+// A squared distance beyond which a pair is certainly past izcut (its value +0): the last
+// table point's distance stepcl*(izcut-1), widened by 1e-5 twice to cover the roundings of
+// the division and the square root, rounded up to float.
+__host__ __device__ inline float skip_dsq(float stepcl, int izcut) {
+    const double dc = (double)stepcl * (double)(izcut - 1) * (1.0 + 1e-5);
+    return (float)(dc * dc * (1.0 + 1e-5)) * (1.0f + 1e-6f);
+}
+
+// pair_energy for a caller that expects most pairs out of range: a pair whose squared
+// minimum-image distance exceeds dsq_skip (skip_dsq) contributes +0 without the square root,
+// the division or the table reads; every other pair is evaluated exactly as pair_energy.
+// Adding +0 to a sum started at +0 never changes it, so skipping is exact.
+__device__ __forceinline__ float pair_energy_far(const Lattice &L, const Tables &T, float dsq_skip, float4 p1,
+                                                 float4 p2, int icref) {
+    float xd = __fsub_rn(p2.x, p1.x), yd = __fsub_rn(p2.y, p1.y), zd = __fsub_rn(p2.z, p1.z);
+    minimagec(L, xd, yd, zd);
+    const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(xd, xd), __fmul_rn(yd, yd)), __fmul_rn(zd, zd));
+    if (dsq > dsq_skip) return 0.0f;
+    return pair_energy_d(T, __fsqrt_rn(dsq), icref);
+}
+
 __device__ __forceinline__ float pair_energy(const Lattice &L, const Tables &T, float4 p1, float4 p2,
                                              int icref) {
     // xdif = x2 - x1 (molfit.py:1257)

@@ -444,51 +444,90 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
             const double *rows = srows + (size_t)slot * SP_BLK * SP_W;
             const float *th = sthr + slot * SP_BLK;
             const int nr = min(SP_BLK, N - SP_BLK * b);
+            // lane i owns move 32 b + i of the block: its threshold and its far part (which the
+            // helpers completed while the block before was walked) are read once, by that lane
+            const int ko = SP_BLK * b + lane;
+            const bool mine = lane < nr;
+            const float thr_own = mine ? th[lane] : 0.0f;
+            const int fs = 2 * (ko % SP_FR);
+            const uint64_t tag = (uint64_t)(uint32_t)(ko + 1) << 32;
+            uint64_t h = 0ull, l = 0ull;
+            bool ready = true;
+            if (mine) {
+                h = vfar[fs];
+                l = vfar[fs + 1];
+                ready = (h & 0xffffffff00000000ull) == tag && (l & 0xffffffff00000000ull) == tag;
+            }
+            for (long long it = 0; !__all_sync(0xffffffffu, ready);) {
+                if (__any_sync(0xffffffffu, ++it > SP_SPIN_LIMIT || abort_flag)) {
+                    err = 1;
+                    break;
+                }
+                if (!ready) {
+                    h = vfar[fs];
+                    l = vfar[fs + 1];
+                    ready = (h & 0xffffffff00000000ull) == tag && (l & 0xffffffff00000000ull) == tag;
+                }
+            }
+            if (err) break;
+            const double f_own = __hiloint2double((int)(uint32_t)h, (int)(uint32_t)l);
+            float fd_own = 0.0f;
             unsigned wbits = 0u;
-            // the far words of the next move are read as soon as a decision is out
-            uint64_t hn = vfar[2 * ((SP_BLK * b) % SP_FR)], ln = vfar[2 * ((SP_BLK * b) % SP_FR) + 1];
-            for (int i = 0; i < nr; ++i) {
-                const int k = SP_BLK * b + i;
-                const int i0 = (lane + SP_W - 1 - (k & (SP_W - 1))) & (SP_W - 1);   // distance - 1 of this lane's first move
-                const double c0 = rows[i * SP_W + i0], c1 = rows[i * SP_W + ((i0 + 32) & (SP_W - 1))];
-                const float thr = th[i];
-                const int fs = 2 * (k % SP_FR);
-                uint64_t h = hn, l = ln;
-                const uint64_t tag = (uint64_t)(uint32_t)(k + 1) << 32;
-                if ((h & 0xffffffff00000000ull) != tag || (l & 0xffffffff00000000ull) != tag) {
-                    long long it = 0;
-                    while (true) {
-                        h = vfar[fs];
-                        l = vfar[fs + 1];
-                        if ((h & 0xffffffff00000000ull) == tag && (l & 0xffffffff00000000ull) == tag) break;
-                        if (++it > SP_SPIN_LIMIT || abort_flag) break;
-                    }
-                    if (__any_sync(0xffffffffu, it > SP_SPIN_LIMIT || abort_flag)) {
-                        err = 1;
-                        break;
-                    }
-                }
-                const double f = __hiloint2double((int)(uint32_t)h, (int)(uint32_t)l);
-                const bool r1 = (k & 32) != 0;   // the register of move k in its lane (k & 31)
-                const float fd = (float)(f + (r1 ? A1 : A0));
-                const float ediff = __fmul_rn(__fadd_rn(fd, 0.0f), temp);
-                const bool a = __ballot_sync(0xffffffffu, lane == (k & 31) && ediff < thr) != 0u;
-                if (i + 1 < nr) {
-                    hn = vfar[2 * ((k + 1) % SP_FR)];
-                    ln = vfar[2 * ((k + 1) % SP_FR) + 1];
-                }
-                // every pending move takes this move's correction; move k's sum restarts as move k+64's
-                const double d0 = a ? c0 : 0.0, d1 = a ? c1 : 0.0;
-                const bool own = lane == (k & 31);
-                A0 = (own && !r1) ? d0 : A0 + d0;
-                A1 = (own && r1) ? d1 : A1 + d1;
-                if (own) {
-                    S.acc[k] = a ? 1 : 0;
-                    S.fdiff[k] = fd;
-                }
-                const float fdk = __shfl_sync(0xffffffffu, fd, k & 31);
-                if (a) fadd += (double)fdk;
-                wbits |= (a ? 1u : 0u) << i;
+            // this lane's two entries of row i (the corrections move 32 b + i brings to the two
+            // pending moves this lane holds)
+            auto row_c = [&](int i, double &c0, double &c1) {
+                const int j0 = (lane + SP_W - 1 - ((SP_BLK * b + i) & (SP_W - 1))) & (SP_W - 1);
+                c0 = rows[i * SP_W + j0];
+                c1 = rows[i * SP_W + ((j0 + 32) & (SP_W - 1))];
+            };
+            const bool r1 = (b & 1) != 0;   // the register of the block's moves: (32 b + i) & 32
+            double c0n, c1n;
+            row_c(0, c0n, c1n);
+            int i = 0;
+            // two moves a step: the second move's test is formed for both outcomes of the first
+            // (its sum with and without the first's correction), so one ballot round decides both
+            for (; i + 1 < nr; i += 2) {
+                const double ca0 = c0n, ca1 = c1n;
+                double cb0, cb1;
+                row_c(i + 1, cb0, cb1);
+                const double asel = r1 ? A1 : A0;
+                const float fdA = (float)(f_own + asel);
+                const float fdB = (float)(f_own + (asel + (r1 ? ca1 : ca0)));
+                const float eA = __fmul_rn(__fadd_rn(fdA, 0.0f), temp);
+                const float eB = __fmul_rn(__fadd_rn(fdB, 0.0f), temp);
+                const bool own0 = lane == i, own1 = lane == i + 1;
+                const unsigned bk = __ballot_sync(0xffffffffu, own0 && eA < thr_own);
+                const unsigned b0 = __ballot_sync(0xffffffffu, own1 && eA < thr_own);
+                const unsigned b1 = __ballot_sync(0xffffffffu, own1 && eB < thr_own);
+                if (i + 2 < nr) row_c(i + 2, c0n, c1n);
+                const bool ak = bk != 0u;
+                const bool ak1 = ak ? b1 != 0u : b0 != 0u;
+                const double dk0 = ak ? ca0 : 0.0, dk1 = ak ? ca1 : 0.0;
+                A0 = (own0 && !r1) ? dk0 : A0 + dk0;
+                A1 = (own0 && r1) ? dk1 : A1 + dk1;
+                const double dl0 = ak1 ? cb0 : 0.0, dl1 = ak1 ? cb1 : 0.0;
+                A0 = (own1 && !r1) ? dl0 : A0 + dl0;
+                A1 = (own1 && r1) ? dl1 : A1 + dl1;
+                fd_own = own0 ? fdA : (own1 ? (ak ? fdB : fdA) : fd_own);
+                wbits |= ((ak ? 1u : 0u) | (ak1 ? 2u : 0u)) << i;
+            }
+            if (i < nr) {   // an odd last move
+                const double ca0 = c0n, ca1 = c1n;
+                const float fdA = (float)(f_own + (r1 ? A1 : A0));
+                const float eA = __fmul_rn(__fadd_rn(fdA, 0.0f), temp);
+                const bool own0 = lane == i;
+                const bool ak = __ballot_sync(0xffffffffu, own0 && eA < thr_own) != 0u;
+                const double dk0 = ak ? ca0 : 0.0, dk1 = ak ? ca1 : 0.0;
+                A0 = (own0 && !r1) ? dk0 : A0 + dk0;
+                A1 = (own0 && r1) ? dk1 : A1 + dk1;
+                fd_own = own0 ? fdA : fd_own;
+                wbits |= (ak ? 1u : 0u) << i;
+            }
+            if (mine) {
+                const bool acc = (wbits >> lane) & 1u;
+                S.acc[ko] = acc ? 1 : 0;
+                S.fdiff[ko] = fd_own;
+                if (acc) fadd += (double)fd_own;
             }
             if (err) break;
             if (lane == 0) vpub[b] = ((uint64_t)(uint32_t)(b + 1) << 32) | wbits;
@@ -499,8 +538,9 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 // the copies still in flight land before the CTA's shared memory goes away
                 for (int b = waited; b < issued; ++b) umma::mbar_wait(&bars[b % SP_NSLOT], (uint32_t)((b / SP_NSLOT) & 1), nullptr);
             }
-            *S.fadd_acc = fadd;
         }
+        fadd = warp_sum_d(fadd);   // each lane's accepted moves, then the lanes in a fixed order
+        if (lane == 0) *S.fadd_acc = fadd;
     } else if ((wid & 3) != 0) {
         // ---- helper warps: the far part of each move's change.  The loads of a helper's next
         // move (its first 128 listed far partners) are issued before it waits for the
@@ -542,10 +582,18 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 }
                 return (v >> (kq % SP_BLK)) & 1ull;
             };
-            // the listed order, lane by lane: entry lane + 32 q
+            // the listed order, lane by lane: entry lane + 32 q; the four decision words are
+            // read together, then checked
+            uint64_t v[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (lane + 32 * q < nf && accepted(kp[q])) sum += cf[q];
+            for (int q = 0; q < 4; ++q) v[q] = (lane + 32 * q < nf && kp[q] >= 0) ? vpub[kp[q] / SP_BLK] : 0ull;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (lane + 32 * q < nf && kp[q] >= 0) {
+                    const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kp[q] / SP_BLK + 1);
+                    if (got ? ((v[q] >> (kp[q] % SP_BLK)) & 1ull) != 0ull : accepted(kp[q])) sum += cf[q];
+                }
+            }
             for (int i = 128 + lane; i < nf; i += 32) {   // lists longer than 128 entries
                 const size_t r = (size_t)k * M;
                 const int q0 = S.fv[r + i];
