@@ -303,40 +303,59 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_propose_kernel(epsr_bmc_t B, 
     const float mx = B.xadd[mol], my = B.yadd[mol], mz = B.zadd[mol];
     const float rfc2 = __fmul_rn(X.rfeat_c, X.rfeat_c);
     const float rsq_skip = (float)((double)rf * (double)rf * (1.0 + 1e-5));   // d >= rf beyond it
-    for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
-        const int jm = list[p];
-        if (jm == mol) continue;
-        // no atom of a partner whose centre is beyond rfeat_c is within 8 A of an atom of the
-        // moved molecule, before or after the move
-        float dx = __fsub_rn(B.xadd[jm], mx), dy = __fsub_rn(B.yadd[jm], my), dz = __fsub_rn(B.zadd[jm], mz);
-        dx = __fsub_rn(dx, nint_f(dx));
-        dy = __fsub_rn(dy, nint_f(dy));
-        dz = __fsub_rn(dz, nint_f(dz));
-        if (__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)) > rfc2) continue;
+    // 1. the partners whose centre is within rfeat_c: no atom of a partner beyond it is within
+    // 8 A of an atom of the moved molecule, before or after the move (compacted in list order)
+    __shared__ int wcnt[BMC_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    int ncomp = 0;
+    for (int c0 = 0; c0 < cnt; c0 += blockDim.x) {
+        const int p = c0 + threadIdx.x;
+        const int jm = p < cnt ? list[p] : -1;
+        bool in = false;
+        if (jm >= 0 && jm != mol) {
+            float dx = __fsub_rn(B.xadd[jm], mx), dy = __fsub_rn(B.yadd[jm], my), dz = __fsub_rn(B.zadd[jm], mz);
+            dx = __fsub_rn(dx, nint_f(dx));
+            dy = __fsub_rn(dy, nint_f(dy));
+            dz = __fsub_rn(dz, nint_f(dz));
+            in = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)) <= rfc2;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) wcnt[wid] = __popc(bal);
+        __syncthreads();
+        int off = ncomp, tot = 0;
+        for (int w = 0; w < nwarp; ++w) {
+            if (w < wid) off += wcnt[w];
+            tot += wcnt[w];
+        }
+        if (in) list[off + __popc(bal & ((1u << lane) - 1u))] = jm;
+        ncomp += tot;
+        __syncthreads();
+    }
+    // 2. one item per (partner, atom of the moved molecule): its distances to the partner's
+    // atoms before and after the move, binned
+    const int a00 = B.naf[mol];
+    for (int it = threadIdx.x; it < ncomp * na_; it += blockDim.x) {
+        const int jm = list[it / na_], a = it - (it / na_) * na_;
         const int b0 = B.naf[jm], nb = B.nato[jm];
+        const int ca = B.fclass[a00 + a];
+        const float4 po = p_old[a], pn = p_new[a];
         for (int q = 0; q < nb; ++q) {
             const float4 pb = atom_pos(B, b0 + q);
-            const int cb = B.fclass[b0 + q];
-            for (int a = 0; a < na_; ++a) {
-                const int ca = B.fclass[B.naf[mol] + a];
-                const int fc = feat_class(ca, cb) * FEAT_BINS;
-                // the square root only for pairs that can be within rf
-                float x0 = __fsub_rn(pb.x, p_old[a].x), y0 = __fsub_rn(pb.y, p_old[a].y),
-                      z0 = __fsub_rn(pb.z, p_old[a].z);
-                float x1 = __fsub_rn(pb.x, p_new[a].x), y1 = __fsub_rn(pb.y, p_new[a].y),
-                      z1 = __fsub_rn(pb.z, p_new[a].z);
-                minimagec(L, x0, y0, z0);
-                minimagec(L, x1, y1, z1);
-                const float q0 = __fadd_rn(__fadd_rn(__fmul_rn(x0, x0), __fmul_rn(y0, y0)), __fmul_rn(z0, z0));
-                const float q1 = __fadd_rn(__fadd_rn(__fmul_rn(x1, x1), __fmul_rn(y1, y1)), __fmul_rn(z1, z1));
-                if (q0 <= rsq_skip) {
-                    const float d0 = __fsqrt_rn(q0);
-                    if (d0 < rf) atomicAdd(&hist[fc + min((int)__fmul_rn(d0, binf), FEAT_BINS - 1)], 1);
-                }
-                if (q1 <= rsq_skip) {
-                    const float d1 = __fsqrt_rn(q1);
-                    if (d1 < rf) atomicAdd(&hist[FEAT_HALF + fc + min((int)__fmul_rn(d1, binf), FEAT_BINS - 1)], 1);
-                }
+            const int fc = feat_class(ca, B.fclass[b0 + q]) * FEAT_BINS;
+            // the square root only for pairs that can be within rf
+            float x0 = __fsub_rn(pb.x, po.x), y0 = __fsub_rn(pb.y, po.y), z0 = __fsub_rn(pb.z, po.z);
+            float x1 = __fsub_rn(pb.x, pn.x), y1 = __fsub_rn(pb.y, pn.y), z1 = __fsub_rn(pb.z, pn.z);
+            minimagec(L, x0, y0, z0);
+            minimagec(L, x1, y1, z1);
+            const float q0 = __fadd_rn(__fadd_rn(__fmul_rn(x0, x0), __fmul_rn(y0, y0)), __fmul_rn(z0, z0));
+            const float q1 = __fadd_rn(__fadd_rn(__fmul_rn(x1, x1), __fmul_rn(y1, y1)), __fmul_rn(z1, z1));
+            if (q0 <= rsq_skip) {
+                const float d0 = __fsqrt_rn(q0);
+                if (d0 < rf) atomicAdd(&hist[fc + min((int)__fmul_rn(d0, binf), FEAT_BINS - 1)], 1);
+            }
+            if (q1 <= rsq_skip) {
+                const float d1 = __fsqrt_rn(q1);
+                if (d1 < rf) atomicAdd(&hist[FEAT_HALF + fc + min((int)__fmul_rn(d1, binf), FEAT_BINS - 1)], 1);
             }
         }
     }
@@ -425,29 +444,50 @@ __global__ void __launch_bounds__(BMC_THREADS) bmc_decide_kernel(epsr_bmc_t B, i
     const float dsq_skip = skip_dsq(T.stepcl, T.izcut);
     const int *pr = B.npairref + X.npairref0;
     const float cx = B.xadd[mol], cy = B.yadd[mol], cz = B.zadd[mol];
-    const float rint = X.rint;
+    const float rint2 = __fmul_rn(X.rint, X.rint);
+    // 1. the partners whose centre is within rint of the old centre (rint covers the cutoff,
+    // both molecules' extents and the largest displacement), compacted in list order
+    __shared__ int wcnt[BMC_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    int ncomp = 0;
+    for (int c0 = 0; c0 < cnt; c0 += blockDim.x) {
+        const int p = c0 + threadIdx.x;
+        const int jm = p < cnt ? list[p] : -1;
+        bool in = false;
+        if (jm >= 0 && jm != mol) {
+            float dx = __fsub_rn(B.xadd[jm], cx), dy = __fsub_rn(B.yadd[jm], cy), dz = __fsub_rn(B.zadd[jm], cz);
+            dx = __fsub_rn(dx, nint_f(dx));
+            dy = __fsub_rn(dy, nint_f(dy));
+            dz = __fsub_rn(dz, nint_f(dz));
+            in = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)) <= rint2;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) wcnt[wid] = __popc(bal);
+        __syncthreads();   // every thread has read its entry of this chunk
+        int off = ncomp, tot = 0;
+        for (int w = 0; w < nwarp; ++w) {
+            if (w < wid) off += wcnt[w];
+            tot += wcnt[w];
+        }
+        if (in) list[off + __popc(bal & ((1u << lane) - 1u))] = jm;   // positions below this chunk's end
+        ncomp += tot;
+        __syncthreads();
+    }
+    // 2. one item per (partner, atom of the moved molecule): the partner's atoms against that
+    // atom before and after the move, float sums over the partner's atoms, the change in double
     double de = 0.0;
-    for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
-        const int jm = list[p];
-        if (jm == mol) continue;
-        // partners whose centre is beyond rint of the old centre cannot interact (rint covers
-        // the cutoff, both molecules' extents and the largest displacement)
-        float dx = __fsub_rn(B.xadd[jm], cx), dy = __fsub_rn(B.yadd[jm], cy), dz = __fsub_rn(B.zadd[jm], cz);
-        dx = __fsub_rn(dx, nint_f(dx));
-        dy = __fsub_rn(dy, nint_f(dy));
-        dz = __fsub_rn(dz, nint_f(dz));
-        if (__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)) > __fmul_rn(rint, rint))
-            continue;
+    const int nitems = ncomp * na_;
+    for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
+        const int jm = list[it / na_], a = it - (it / na_) * na_;
         const int b0 = B.naf[jm], nb = B.nato[jm];
+        const int *row = pr + __float_as_int(p_old[a].w) * X.ntype;
+        const float4 pn = p_new[a], po = p_old[a];
         float e_new = 0.0f, e_old = 0.0f;
-        for (int a = 0; a < na_; ++a) {
-            const int *row = pr + __float_as_int(p_old[a].w) * X.ntype;
-            for (int q = 0; q < nb; ++q) {
-                const float4 pb = atom_pos(B, b0 + q);
-                const int icref = row[__float_as_int(pb.w)];
-                e_new = __fadd_rn(e_new, pair_energy_far(L, T, dsq_skip, p_new[a], pb, icref));
-                e_old = __fadd_rn(e_old, pair_energy_far(L, T, dsq_skip, p_old[a], pb, icref));
-            }
+        for (int q = 0; q < nb; ++q) {
+            const float4 pb = atom_pos(B, b0 + q);
+            const int icref = row[__float_as_int(pb.w)];
+            e_new = __fadd_rn(e_new, pair_energy_far(L, T, dsq_skip, pn, pb, icref));
+            e_old = __fadd_rn(e_old, pair_energy_far(L, T, dsq_skip, po, pb, icref));
         }
         de += (double)e_new - (double)e_old;
     }

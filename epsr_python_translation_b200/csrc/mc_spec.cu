@@ -995,7 +995,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
         if (rc) return rc;
         EPSR_CUDA(cudaEventRecord(as->fork, s));
         EPSR_CUDA(cudaStreamWaitEvent(as->st, as->fork, 0));
-        ahead_fill_kernel<<<1, 32, 0, as->st>>>(S.ran1_next, mc->ahead, S.off + N);
+        EPSR_TIMED("ahead_fill_kernel", as->st, ahead_fill_kernel<<<1, 32, 0, as->st>>>(S.ran1_next, mc->ahead, S.off + N));
         EPSR_CUDA(cudaGetLastError());
         EPSR_CUDA(cudaEventRecord(as->join, as->st));
     }
