@@ -84,8 +84,9 @@ struct SpecDev {
     float4 *npos;                          // [natom] proposed absolute positions
     float *thr;                            // [N] Metropolis thresholds (by visit position)
     float *A, *B;                          // [N*M]
-    double *base, *nearT, *farc;           // [N], [Npad*W] by the earlier move, [N*M]
-    int32_t *fv;                           // [N*M] by visit position
+    double *base;                          // [N] each move's change if no earlier partner accepted
+    float *nearT;                          // [Npad*W] near corrections, by the earlier move
+    uint64_t *farw;                        // [N*M] far partners by visit position: kp << 32 | c (float bits)
     int32_t *nnk;                          // [N] far partners listed for each move
     int32_t *acc;                          // [N] by visit position
     float *fdiff;                          // [N] by visit position
@@ -314,7 +315,8 @@ __global__ void __launch_bounds__(SP_ET) spec_energy_kernel(SpecDev S) {
 // earlier partner accepted), and for each partner p visited earlier the correction c that
 // applies if p accepted.  Partners at most SP_W moves earlier go into p's row of nearT (the
 // resolver adds them as decisions are taken); the others are listed for the helpers in
-// store order, compacted to the front of k's row of fv/farc (nfar[k] of them).
+// store order, compacted to the front of k's row of farw as (partner's visit position,
+// correction) words (nnk[k] of them).
 __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
     __shared__ double ws[4];
     __shared__ int wcount[4];
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
                 const double oldp = s2 >= 1 ? (double)S.A[e2] : sv;
                 c = ((double)S.B[e] - oldp) - d0;
                 const int dist = k - kp;
-                if (dist <= SP_W) S.nearT[(size_t)kp * SP_W + dist - 1] = c;
+                if (dist <= SP_W) S.nearT[(size_t)kp * SP_W + dist - 1] = (float)c;
                 else far = true;
             }
         }
@@ -359,8 +361,7 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
         }
         if (far) {
             const int i = off + __popc(bal & ((1u << lane) - 1u));
-            S.fv[krow + i] = kp;
-            S.farc[krow + i] = c;
+            S.farw[krow + i] = ((uint64_t)(uint32_t)kp << 32) | __float_as_uint((float)c);
         }
         nfar += tot;
         __syncthreads();
@@ -375,12 +376,13 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
 }
 
 // ----------------------------------------------------------------- resolve
-// Shared memory of the resolver CTA (dynamic): the staged rows, the staged thresholds, the
-// blocks' mbarriers, the far-sum ring (two tagged words a move: high and low halves of the
-// double) and the published decision words (tag in the high half, one bit a move in the low).
-constexpr int SP_SROWS = SP_NSLOT * SP_BLK * SP_W * 8;
+// Shared memory of the resolver CTA (dynamic): the staged rows (float), the staged
+// thresholds, the blocks' mbarriers, the far-sum ring (one tagged word a move: the tag in the
+// high half, the float far part in the low) and the published decision words (tag in the
+// high half, one bit a move in the low).
+constexpr int SP_SROWS = SP_NSLOT * SP_BLK * SP_W * 4;
 constexpr int SP_STHR = SP_NSLOT * SP_BLK * 4;
-constexpr int SP_SHDR = SP_SROWS + SP_STHR + SP_NSLOT * 8 + SP_FR * 16;
+constexpr int SP_SHDR = SP_SROWS + SP_STHR + SP_NSLOT * 8 + SP_FR * 8;
 
 __host__ __device__ constexpr size_t spec_resolve_smem(int N) {
     return (size_t)SP_SHDR + 8 * (size_t)((N + SP_BLK - 1) / SP_BLK);
@@ -388,7 +390,7 @@ __host__ __device__ constexpr size_t spec_resolve_smem(int N) {
 
 __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
     extern __shared__ __align__(128) unsigned char rsm[];
-    double *srows = reinterpret_cast<double *>(rsm);
+    float *srows = reinterpret_cast<float *>(rsm);
     float *sthr = reinterpret_cast<float *>(rsm + SP_SROWS);
     uint64_t *bars = reinterpret_cast<uint64_t *>(rsm + SP_SROWS + SP_STHR);
     volatile uint64_t *vfar = reinterpret_cast<volatile uint64_t *>(rsm + SP_SROWS + SP_STHR + SP_NSLOT * 8);
@@ -398,7 +400,7 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
     const int N = S.N;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int nblk = (N + SP_BLK - 1) / SP_BLK;
-    for (int i = tid; i < 2 * SP_FR; i += blockDim.x) vfar[i] = 0ull;
+    for (int i = tid; i < SP_FR; i += blockDim.x) vfar[i] = 0ull;
     for (int i = tid; i < nblk; i += blockDim.x) vpub[i] = 0ull;
     if (tid == 0) {
         abort_flag = 0;
@@ -417,7 +419,7 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         auto stage = [&](int b) {   // lane 0: rows and thresholds of block b into its slot
             const int slot = b % SP_NSLOT;
             const int nr = min(SP_BLK, N - SP_BLK * b);
-            const uint32_t rb = (uint32_t)nr * SP_W * 8, tb = ((uint32_t)nr * 4 + 15u) & ~15u;
+            const uint32_t rb = (uint32_t)nr * SP_W * 4, tb = ((uint32_t)nr * 4 + 15u) & ~15u;
             umma::mbar_expect_tx(&bars[slot], rb + tb);
             umma::bulk_load(srows + (size_t)slot * SP_BLK * SP_W, S.nearT + (size_t)b * SP_BLK * SP_W, rb, &bars[slot]);
             umma::bulk_load(sthr + slot * SP_BLK, S.thr + (size_t)b * SP_BLK, tb, &bars[slot]);
@@ -425,7 +427,7 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         int issued = 0, waited = 0;
         if (lane == 0)
             for (; issued < min(nblk, SP_NSLOT - 1); ++issued) stage(issued);
-        double A0 = 0.0, A1 = 0.0;   // running sums of the pending moves = lane, lane + 32 (mod 64)
+        float A0 = 0.0f, A1 = 0.0f;   // running sums of the pending moves = lane, lane + 32 (mod 64)
         double fadd = 0.0;
         int err = 0;
         for (int b = 0; b < nblk && !err; ++b) {
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 break;
             }
             ++waited;
-            const double *rows = srows + (size_t)slot * SP_BLK * SP_W;
+            const float *rows = srows + (size_t)slot * SP_BLK * SP_W;
             const float *th = sthr + slot * SP_BLK;
             const int nr = min(SP_BLK, N - SP_BLK * b);
             // lane i owns move 32 b + i of the block: its threshold and its far part (which the
@@ -449,14 +451,13 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
             const int ko = SP_BLK * b + lane;
             const bool mine = lane < nr;
             const float thr_own = mine ? th[lane] : 0.0f;
-            const int fs = 2 * (ko % SP_FR);
-            const uint64_t tag = (uint64_t)(uint32_t)(ko + 1) << 32;
-            uint64_t h = 0ull, l = 0ull;
+            const int fs = ko % SP_FR;
+            const uint32_t tag = (uint32_t)(ko + 1);
+            uint64_t w = 0ull;
             bool ready = true;
             if (mine) {
-                h = vfar[fs];
-                l = vfar[fs + 1];
-                ready = (h & 0xffffffff00000000ull) == tag && (l & 0xffffffff00000000ull) == tag;
+                w = vfar[fs];
+                ready = (uint32_t)(w >> 32) == tag;
             }
             for (long long it = 0; !__all_sync(0xffffffffu, ready);) {
                 if (__any_sync(0xffffffffu, ++it > SP_SPIN_LIMIT || abort_flag)) {
@@ -464,62 +465,62 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                     break;
                 }
                 if (!ready) {
-                    h = vfar[fs];
-                    l = vfar[fs + 1];
-                    ready = (h & 0xffffffff00000000ull) == tag && (l & 0xffffffff00000000ull) == tag;
+                    w = vfar[fs];
+                    ready = (uint32_t)(w >> 32) == tag;
                 }
             }
             if (err) break;
-            const double f_own = __hiloint2double((int)(uint32_t)h, (int)(uint32_t)l);
+            const float f_own = __uint_as_float((uint32_t)w);
             float fd_own = 0.0f;
             unsigned wbits = 0u;
             // this lane's two entries of row i (the corrections move 32 b + i brings to the two
             // pending moves this lane holds)
-            auto row_c = [&](int i, double &c0, double &c1) {
+            auto row_c = [&](int i, float &c0, float &c1) {
                 const int j0 = (lane + SP_W - 1 - ((SP_BLK * b + i) & (SP_W - 1))) & (SP_W - 1);
                 c0 = rows[i * SP_W + j0];
                 c1 = rows[i * SP_W + ((j0 + 32) & (SP_W - 1))];
             };
             const bool r1 = (b & 1) != 0;   // the register of the block's moves: (32 b + i) & 32
-            double c0n, c1n;
+            float c0n, c1n;
             row_c(0, c0n, c1n);
             int i = 0;
             // two moves a step: the second move's test is formed for both outcomes of the first
-            // (its sum with and without the first's correction), so one ballot round decides both
+            // (its sum with and without the first's correction), and two ballots decide both --
+            // bit i and i+1 of the first the tests on the sums as they stand, the second the
+            // second move's test on its sum with the first's correction
             for (; i + 1 < nr; i += 2) {
-                const double ca0 = c0n, ca1 = c1n;
-                double cb0, cb1;
+                const float ca0 = c0n, ca1 = c1n;
+                float cb0, cb1;
                 row_c(i + 1, cb0, cb1);
-                const double asel = r1 ? A1 : A0;
-                const float fdA = (float)(f_own + asel);
-                const float fdB = (float)(f_own + (asel + (r1 ? ca1 : ca0)));
+                const float asel = r1 ? A1 : A0;
+                const float fdA = __fadd_rn(f_own, asel);
+                const float fdB = __fadd_rn(f_own, __fadd_rn(asel, r1 ? ca1 : ca0));
                 const float eA = __fmul_rn(__fadd_rn(fdA, 0.0f), temp);
                 const float eB = __fmul_rn(__fadd_rn(fdB, 0.0f), temp);
                 const bool own0 = lane == i, own1 = lane == i + 1;
-                const unsigned bk = __ballot_sync(0xffffffffu, own0 && eA < thr_own);
-                const unsigned b0 = __ballot_sync(0xffffffffu, own1 && eA < thr_own);
-                const unsigned b1 = __ballot_sync(0xffffffffu, own1 && eB < thr_own);
+                const unsigned bA = __ballot_sync(0xffffffffu, (own0 || own1) && eA < thr_own);
+                const unsigned bB = __ballot_sync(0xffffffffu, own1 && eB < thr_own);
                 if (i + 2 < nr) row_c(i + 2, c0n, c1n);
-                const bool ak = bk != 0u;
-                const bool ak1 = ak ? b1 != 0u : b0 != 0u;
-                const double dk0 = ak ? ca0 : 0.0, dk1 = ak ? ca1 : 0.0;
-                A0 = (own0 && !r1) ? dk0 : A0 + dk0;
-                A1 = (own0 && r1) ? dk1 : A1 + dk1;
-                const double dl0 = ak1 ? cb0 : 0.0, dl1 = ak1 ? cb1 : 0.0;
-                A0 = (own1 && !r1) ? dl0 : A0 + dl0;
-                A1 = (own1 && r1) ? dl1 : A1 + dl1;
+                const bool ak = (bA >> i) & 1u;
+                const bool ak1 = ak ? bB != 0u : ((bA >> (i + 1)) & 1u) != 0u;
+                const float dk0 = ak ? ca0 : 0.0f, dk1 = ak ? ca1 : 0.0f;
+                A0 = (own0 && !r1) ? dk0 : __fadd_rn(A0, dk0);
+                A1 = (own0 && r1) ? dk1 : __fadd_rn(A1, dk1);
+                const float dl0 = ak1 ? cb0 : 0.0f, dl1 = ak1 ? cb1 : 0.0f;
+                A0 = (own1 && !r1) ? dl0 : __fadd_rn(A0, dl0);
+                A1 = (own1 && r1) ? dl1 : __fadd_rn(A1, dl1);
                 fd_own = own0 ? fdA : (own1 ? (ak ? fdB : fdA) : fd_own);
                 wbits |= ((ak ? 1u : 0u) | (ak1 ? 2u : 0u)) << i;
             }
             if (i < nr) {   // an odd last move
-                const double ca0 = c0n, ca1 = c1n;
-                const float fdA = (float)(f_own + (r1 ? A1 : A0));
+                const float ca0 = c0n, ca1 = c1n;
+                const float fdA = __fadd_rn(f_own, r1 ? A1 : A0);
                 const float eA = __fmul_rn(__fadd_rn(fdA, 0.0f), temp);
                 const bool own0 = lane == i;
                 const bool ak = __ballot_sync(0xffffffffu, own0 && eA < thr_own) != 0u;
-                const double dk0 = ak ? ca0 : 0.0, dk1 = ak ? ca1 : 0.0;
-                A0 = (own0 && !r1) ? dk0 : A0 + dk0;
-                A1 = (own0 && r1) ? dk1 : A1 + dk1;
+                const float dk0 = ak ? ca0 : 0.0f, dk1 = ak ? ca1 : 0.0f;
+                A0 = (own0 && !r1) ? dk0 : __fadd_rn(A0, dk0);
+                A1 = (own0 && r1) ? dk1 : __fadd_rn(A1, dk1);
                 fd_own = own0 ? fdA : fd_own;
                 wbits |= (ak ? 1u : 0u) << i;
             }
@@ -529,7 +530,6 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 S.fdiff[ko] = fd_own;
                 if (acc) fadd += (double)fd_own;
             }
-            if (err) break;
             if (lane == 0) vpub[b] = ((uint64_t)(uint32_t)(b + 1) << 32) | wbits;
         }
         if (lane == 0) {
@@ -542,32 +542,43 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         fadd = warp_sum_d(fadd);   // each lane's accepted moves, then the lanes in a fixed order
         if (lane == 0) *S.fadd_acc = fadd;
     } else if ((wid & 3) != 0) {
-        // ---- helper warps: the far part of each move's change.  The loads of a helper's next
-        // move (its first 128 listed far partners) are issued before it waits for the
-        // decisions its current move needs.
+        // ---- helper warps: the far part of each move's change, two consecutive moves a step,
+        // one per half-warp (16 lanes x 4 listed partners; longer lists loop).  A move's list
+        // length is read one step before its entries, and the entries one step before they are
+        // used, so no load waits on another and none reads past a list.
         const int h = wid - 1 - (wid >> 2);
         const int M = S.M;
-        int nf = 0, kp[4];
-        double bk = 0.0, cf[4];
-        auto load = [&](int kk, int &nf_, double &bk_, int (&kp_)[4], double (&cf_)[4]) {
+        const int half = lane >> 4, hl = lane & 15;
+        const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
+        (void)hmask;
+        uint64_t e[4] = {0ull, 0ull, 0ull, 0ull};
+        int nf = 0;
+        double bk = 0.0;
+        auto load_entries = [&](int kk, int nfk, uint64_t (&e_)[4]) {
             const size_t r = (size_t)kk * M;
-            nf_ = S.nnk[kk];
-            bk_ = S.base[kk];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int i = lane + 32 * q;
-                kp_[q] = i < M ? S.fv[r + i] : -1;
-                cf_[q] = i < M ? S.farc[r + i] : 0.0;
-            }
+            for (int q = 0; q < 4; ++q) e_[q] = hl + 16 * q < nfk ? S.farw[r + hl + 16 * q] : 0ull;
         };
-        if (h < N) load(h, nf, bk, kp, cf);
-        for (int k = h; k < N; k += SP_NH) {
-            int nf_n = 0, kp_n[4] = {-1, -1, -1, -1};
-            double bk_n = 0.0, cf_n[4] = {0.0, 0.0, 0.0, 0.0};
-            if (k + SP_NH < N) load(k + SP_NH, nf_n, bk_n, kp_n, cf_n);
+        const int step = 2 * SP_NH;
+        int k = 2 * h + half;
+        if (k < N) {
+            nf = S.nnk[k];
+            bk = S.base[k];
+            load_entries(k, nf, e);
+        }
+        int nf_n = k + step < N ? S.nnk[k + step] : 0;
+        for (int k0 = 2 * h; k0 < N; k0 += step, k += step) {
+            // the next step's entries and base, the count of the step after
+            uint64_t e_n[4] = {0ull, 0ull, 0ull, 0ull};
+            double bk_n = 0.0;
+            if (k + step < N) {
+                load_entries(k + step, nf_n, e_n);
+                bk_n = S.base[k + step];
+            }
+            const int nf_nn = k + 2 * step < N ? S.nnk[k + 2 * step] : 0;
             double sum = 0.0;
             bool bad = false;
-            // the decision of partner kp (published in word kp / 32), waiting for the word
+            // the decision of partner kq (published in word kq / 32), waiting for the word
             auto accepted = [&](int kq) -> bool {
                 const int w = kq / SP_BLK;
                 uint64_t v = vpub[w];
@@ -582,45 +593,45 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 }
                 return (v >> (kq % SP_BLK)) & 1ull;
             };
-            // the listed order, lane by lane: entry lane + 32 q; the four decision words are
-            // read together, then checked
-            uint64_t v[4];
+            if (k < N) {
+                // the listed order, lane by lane: entry hl + 16 q; the four decision words are
+                // read together, then checked
+                uint64_t v[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) v[q] = (lane + 32 * q < nf && kp[q] >= 0) ? vpub[kp[q] / SP_BLK] : 0ull;
+                for (int q = 0; q < 4; ++q) v[q] = hl + 16 * q < nf ? vpub[(int)(e[q] >> 32) / SP_BLK] : 0ull;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (lane + 32 * q < nf && kp[q] >= 0) {
-                    const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kp[q] / SP_BLK + 1);
-                    if (got ? ((v[q] >> (kp[q] % SP_BLK)) & 1ull) != 0ull : accepted(kp[q])) sum += cf[q];
+                for (int q = 0; q < 4; ++q) {
+                    if (hl + 16 * q < nf) {
+                        const int kq = (int)(e[q] >> 32);
+                        const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kq / SP_BLK + 1);
+                        if (got ? ((v[q] >> (kq % SP_BLK)) & 1ull) != 0ull : accepted(kq))
+                            sum += (double)__uint_as_float((uint32_t)e[q]);
+                    }
                 }
+                for (int i = 64 + hl; i < nf; i += 16) {   // lists longer than 64 entries
+                    const uint64_t x = S.farw[(size_t)k * M + i];
+                    if (accepted((int)(x >> 32))) sum += (double)__uint_as_float((uint32_t)x);
+                }
+                // the ring slot of move k was last read by the resolver in move k - SP_FR's block
+                if (k >= SP_FR && hl == 0) accepted(k - SP_FR);
             }
-            for (int i = 128 + lane; i < nf; i += 32) {   // lists longer than 128 entries
-                const size_t r = (size_t)k * M;
-                const int q0 = S.fv[r + i];
-                if (accepted(q0)) sum += S.farc[r + i];
-            }
-            // the ring slot of move k was last read by the resolver at move k - SP_FR
-            if (k >= SP_FR && lane == 0) accepted(k - SP_FR);
             if (__any_sync(0xffffffffu, bad)) {
                 if (lane == 0) fail();
                 break;
             }
-            sum = warp_sum_d(sum);
-            if (lane == 0) {
-                const double fk = bk + sum;
-                const uint64_t tag = (uint64_t)(uint32_t)(k + 1) << 32;
-                const int fs = 2 * (k % SP_FR);
-                vfar[fs] = tag | (uint32_t)__double2hiint(fk);
-                vfar[fs + 1] = tag | (uint32_t)__double2loint(fk);
+            // the half-warp's sum, in a fixed order
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (hl == 0 && k < N) {
+                const float fk = (float)(bk + sum);
+                vfar[k % SP_FR] = ((uint64_t)(uint32_t)(k + 1) << 32) | __float_as_uint(fk);
             }
             __syncwarp();
-            nf = nf_n;
-            bk = bk_n;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                kp[q] = kp_n[q];
-                cf[q] = cf_n[q];
-            }
+            for (int q = 0; q < 4; ++q) e[q] = e_n[q];
+            nf = nf_n;
+            nf_n = nf_nn;
+            bk = bk_n;
         }
     }
 }
@@ -848,8 +859,8 @@ static size_t spec_bytes(int N, int natom, int M, int nmt) {
     b += spal(sizeof(float) * ((size_t)N + SP_BLK));                 // thr (+ the last staged block's tail)
     b += 2 * spal(sizeof(float) * (size_t)N * M);                  // A, B
     const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
-    b += spal(sizeof(double) * N) + spal(sizeof(double) * npad * SP_W) + spal(sizeof(double) * (size_t)N * M);
-    b += spal(sizeof(int32_t) * (size_t)N * M) + spal(sizeof(int32_t) * N);   // fv, nnk
+    b += spal(sizeof(double) * N) + spal(sizeof(float) * npad * SP_W) + spal(sizeof(uint64_t) * (size_t)N * M);
+    b += spal(sizeof(int32_t) * N);   // nnk
     b += spal(sizeof(int32_t) * N) + spal(sizeof(float) * N) + spal(sizeof(double));
     return b;
 }
@@ -966,9 +977,8 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     S.B = (float *)take(sizeof(float) * (size_t)N * M);
     S.base = (double *)take(sizeof(double) * N);
     const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
-    S.nearT = (double *)take(sizeof(double) * npad * SP_W);
-    S.farc = (double *)take(sizeof(double) * (size_t)N * M);
-    S.fv = (int32_t *)take(sizeof(int32_t) * (size_t)N * M);
+    S.nearT = (float *)take(sizeof(float) * npad * SP_W);
+    S.farw = (uint64_t *)take(sizeof(uint64_t) * (size_t)N * M);
     S.nnk = (int32_t *)take(sizeof(int32_t) * N);
     S.acc = (int32_t *)take(sizeof(int32_t) * N);
     S.fdiff = (float *)take(sizeof(float) * N);
@@ -1003,7 +1013,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     if (en_bytes > 48 * 1024) EPSR_SMEM_OPTIN(spec_energy_kernel);
     const int en_threads = min(SP_ET, max(32, (M - 1 + 31) / 32 * 32));   // one thread per stored partner
     EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, en_threads, en_bytes, s>>>(S));
-    EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(double) * npad * SP_W, s));
+    EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(float) * npad * SP_W, s));
     EPSR_TIMED("spec_corr_kernel", s, spec_corr_kernel<<<N, 128, 0, s>>>(S));
     const size_t rsmem = spec_resolve_smem(N);
     EPSR_SMEM_OPTIN(spec_resolve_kernel);
