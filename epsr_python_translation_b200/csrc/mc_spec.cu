@@ -85,8 +85,8 @@ struct SpecDev {
     float *thr;                            // [N] Metropolis thresholds (by visit position)
     float *A, *B;                          // [N*M]
     double *base;                          // [N] each move's change if no earlier partner accepted
-    float *nearT;                          // [Npad*W] near corrections, by the earlier move
-    uint64_t *farw;                        // [N*M] far partners by visit position: kp << 32 | c (float bits)
+    float2 *nearT;                         // [Npad*W] near terms {rejected, accepted}, by the earlier move
+    uint4 *farw;                           // [N*M] far partners by visit position: {kp, rejected, accepted, 0}
     int32_t *nnk;                          // [N] far partners listed for each move
     int32_t *acc;                          // [N] by visit position
     float *fdiff;                          // [N] by visit position
@@ -311,12 +311,14 @@ __global__ void __launch_bounds__(SP_ET) spec_energy_kernel(SpecDev S) {
 }
 
 // ----------------------------------------------------------------- corrections
-// Per move k (one CTA): base[k] = sum over its stored partners of A - S (the change if no
-// earlier partner accepted), and for each partner p visited earlier the correction c that
-// applies if p accepted.  Partners at most SP_W moves earlier go into p's row of nearT (the
-// resolver adds them as decisions are taken); the others are listed for the helpers in
-// store order, compacted to the front of k's row of farw as (partner's visit position,
-// correction) words (nnk[k] of them).
+// Per move k (one CTA): base[k] = sum over its partners visited later of A - S, and for each
+// partner p visited earlier both terms it can bring: A - S if p was rejected, B - (p's stored
+// energy after its move) if it was accepted.  Partners at most SP_W moves earlier go into p's
+// row of nearT (the resolver adds the term that applies as decisions are taken); the others
+// are listed for the helpers in store order, compacted to the front of k's row of farw as
+// (partner's visit position, both terms) words (nnk[k] of them).  Carrying both terms, never
+// their difference, keeps an energy that the final configuration does not contain (A against
+// a partner that has moved away) out of every sum.
 __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
     __shared__ double ws[4];
     __shared__ int wcount[4];
@@ -332,22 +334,26 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
         const int s = s0 + threadIdx.x;
         bool far = false;
         int kp = -1;
-        double c = 0.0;
+        float ca = 0.0f, cb = 0.0f;
         if (s < nn) {
             const size_t e = row + s;
             const int p = S.molergpair[e];
             kp = S.vpos[p];
             const double sv = (double)S.ergpair[S.ergpairref[e] - 1];
             const double d0 = (double)S.A[e] - sv;
-            d0s += d0;
             if (kp < k) {
+                // the term if p was rejected (A - S) and if it was accepted (B against p's stored
+                // energy after its move); the resolver or a helper adds the one that applies
                 const int e2 = S.mirror[e];
                 const int s2 = e2 % S.M;
                 const double oldp = s2 >= 1 ? (double)S.A[e2] : sv;
-                c = ((double)S.B[e] - oldp) - d0;
+                ca = (float)d0;
+                cb = (float)((double)S.B[e] - oldp);
                 const int dist = k - kp;
-                if (dist <= SP_W) S.nearT[(size_t)kp * SP_W + dist - 1] = (float)c;
+                if (dist <= SP_W) S.nearT[(size_t)kp * SP_W + dist - 1] = make_float2(ca, cb);
                 else far = true;
+            } else {
+                d0s += d0;   // a later partner: its term is A - S
             }
         }
         // ordered compaction of this chunk's far partners
@@ -361,7 +367,7 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
         }
         if (far) {
             const int i = off + __popc(bal & ((1u << lane) - 1u));
-            S.farw[krow + i] = ((uint64_t)(uint32_t)kp << 32) | __float_as_uint((float)c);
+            S.farw[krow + i] = make_uint4((uint32_t)kp, __float_as_uint(ca), __float_as_uint(cb), 0u);
         }
         nfar += tot;
         __syncthreads();
@@ -380,7 +386,7 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
 // thresholds, the blocks' mbarriers, the far-sum ring (one tagged word a move: the tag in the
 // high half, the float far part in the low) and the published decision words (tag in the
 // high half, one bit a move in the low).
-constexpr int SP_SROWS = SP_NSLOT * SP_BLK * SP_W * 4;
+constexpr int SP_SROWS = SP_NSLOT * SP_BLK * SP_W * 8;
 constexpr int SP_STHR = SP_NSLOT * SP_BLK * 4;
 constexpr int SP_SHDR = SP_SROWS + SP_STHR + SP_NSLOT * 8 + SP_FR * 8;
 
@@ -390,7 +396,7 @@ __host__ __device__ constexpr size_t spec_resolve_smem(int N) {
 
 __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
     extern __shared__ __align__(128) unsigned char rsm[];
-    float *srows = reinterpret_cast<float *>(rsm);
+    float2 *srows = reinterpret_cast<float2 *>(rsm);
     float *sthr = reinterpret_cast<float *>(rsm + SP_SROWS);
     uint64_t *bars = reinterpret_cast<uint64_t *>(rsm + SP_SROWS + SP_STHR);
     volatile uint64_t *vfar = reinterpret_cast<volatile uint64_t *>(rsm + SP_SROWS + SP_STHR + SP_NSLOT * 8);
@@ -419,7 +425,7 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         auto stage = [&](int b) {   // lane 0: rows and thresholds of block b into its slot
             const int slot = b % SP_NSLOT;
             const int nr = min(SP_BLK, N - SP_BLK * b);
-            const uint32_t rb = (uint32_t)nr * SP_W * 4, tb = ((uint32_t)nr * 4 + 15u) & ~15u;
+            const uint32_t rb = (uint32_t)nr * SP_W * 8, tb = ((uint32_t)nr * 4 + 15u) & ~15u;
             umma::mbar_expect_tx(&bars[slot], rb + tb);
             umma::bulk_load(srows + (size_t)slot * SP_BLK * SP_W, S.nearT + (size_t)b * SP_BLK * SP_W, rb, &bars[slot]);
             umma::bulk_load(sthr + slot * SP_BLK, S.thr + (size_t)b * SP_BLK, tb, &bars[slot]);
@@ -443,7 +449,7 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 break;
             }
             ++waited;
-            const float *rows = srows + (size_t)slot * SP_BLK * SP_W;
+            const float2 *rows = srows + (size_t)slot * SP_BLK * SP_W;
             const float *th = sthr + slot * SP_BLK;
             const int nr = min(SP_BLK, N - SP_BLK * b);
             // lane i owns move 32 b + i of the block: its threshold and its far part (which the
@@ -473,52 +479,54 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
             const float f_own = __uint_as_float((uint32_t)w);
             float fd_own = 0.0f;
             unsigned wbits = 0u;
-            // this lane's two entries of row i (the corrections move 32 b + i brings to the two
-            // pending moves this lane holds)
-            auto row_c = [&](int i, float &c0, float &c1) {
+            // this lane's two entries of row i (the terms move 32 b + i brings to the two pending
+            // moves this lane holds, {rejected, accepted})
+            auto row_c = [&](int i, float2 &c0, float2 &c1) {
                 const int j0 = (lane + SP_W - 1 - ((SP_BLK * b + i) & (SP_W - 1))) & (SP_W - 1);
                 c0 = rows[i * SP_W + j0];
                 c1 = rows[i * SP_W + ((j0 + 32) & (SP_W - 1))];
             };
             const bool r1 = (b & 1) != 0;   // the register of the block's moves: (32 b + i) & 32
-            float c0n, c1n;
+            float2 c0n, c1n;
             row_c(0, c0n, c1n);
             int i = 0;
             // two moves a step: the second move's test is formed for both outcomes of the first
-            // (its sum with and without the first's correction), and two ballots decide both --
-            // bit i and i+1 of the first the tests on the sums as they stand, the second the
-            // second move's test on its sum with the first's correction
+            // (its sum with the first's rejected or accepted term), and two ballots decide both --
+            // bit i and i+1 of the first the first move's test and the second's if the first
+            // rejects, the second the second's if the first accepts
             for (; i + 1 < nr; i += 2) {
-                const float ca0 = c0n, ca1 = c1n;
-                float cb0, cb1;
+                const float2 ca0 = c0n, ca1 = c1n;
+                float2 cb0, cb1;
                 row_c(i + 1, cb0, cb1);
                 const float asel = r1 ? A1 : A0;
-                const float fdA = __fadd_rn(f_own, asel);
-                const float fdB = __fadd_rn(f_own, __fadd_rn(asel, r1 ? ca1 : ca0));
+                const float2 cs = r1 ? ca1 : ca0;
+                const bool own0 = lane == i, own1 = lane == i + 1;
+                // lane i: move i's own sum; lane i+1: its sum with move i rejected / accepted
+                const float fdA = __fadd_rn(f_own, own1 ? __fadd_rn(asel, cs.x) : asel);
+                const float fdB = __fadd_rn(f_own, __fadd_rn(asel, cs.y));
                 const float eA = __fmul_rn(__fadd_rn(fdA, 0.0f), temp);
                 const float eB = __fmul_rn(__fadd_rn(fdB, 0.0f), temp);
-                const bool own0 = lane == i, own1 = lane == i + 1;
                 const unsigned bA = __ballot_sync(0xffffffffu, (own0 || own1) && eA < thr_own);
                 const unsigned bB = __ballot_sync(0xffffffffu, own1 && eB < thr_own);
                 if (i + 2 < nr) row_c(i + 2, c0n, c1n);
                 const bool ak = (bA >> i) & 1u;
                 const bool ak1 = ak ? bB != 0u : ((bA >> (i + 1)) & 1u) != 0u;
-                const float dk0 = ak ? ca0 : 0.0f, dk1 = ak ? ca1 : 0.0f;
+                const float dk0 = ak ? ca0.y : ca0.x, dk1 = ak ? ca1.y : ca1.x;
                 A0 = (own0 && !r1) ? dk0 : __fadd_rn(A0, dk0);
                 A1 = (own0 && r1) ? dk1 : __fadd_rn(A1, dk1);
-                const float dl0 = ak1 ? cb0 : 0.0f, dl1 = ak1 ? cb1 : 0.0f;
+                const float dl0 = ak1 ? cb0.y : cb0.x, dl1 = ak1 ? cb1.y : cb1.x;
                 A0 = (own1 && !r1) ? dl0 : __fadd_rn(A0, dl0);
                 A1 = (own1 && r1) ? dl1 : __fadd_rn(A1, dl1);
                 fd_own = own0 ? fdA : (own1 ? (ak ? fdB : fdA) : fd_own);
                 wbits |= ((ak ? 1u : 0u) | (ak1 ? 2u : 0u)) << i;
             }
             if (i < nr) {   // an odd last move
-                const float ca0 = c0n, ca1 = c1n;
+                const float2 ca0 = c0n, ca1 = c1n;
                 const float fdA = __fadd_rn(f_own, r1 ? A1 : A0);
                 const float eA = __fmul_rn(__fadd_rn(fdA, 0.0f), temp);
                 const bool own0 = lane == i;
                 const bool ak = __ballot_sync(0xffffffffu, own0 && eA < thr_own) != 0u;
-                const float dk0 = ak ? ca0 : 0.0f, dk1 = ak ? ca1 : 0.0f;
+                const float dk0 = ak ? ca0.y : ca0.x, dk1 = ak ? ca1.y : ca1.x;
                 A0 = (own0 && !r1) ? dk0 : __fadd_rn(A0, dk0);
                 A1 = (own0 && r1) ? dk1 : __fadd_rn(A1, dk1);
                 fd_own = own0 ? fdA : fd_own;
@@ -551,14 +559,16 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         const int half = lane >> 4, hl = lane & 15;
         const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
         (void)hmask;
-        uint64_t e[4] = {0ull, 0ull, 0ull, 0ull};
+        uint4 e[4];
         int nf = 0;
         double bk = 0.0;
-        auto load_entries = [&](int kk, int nfk, uint64_t (&e_)[4]) {
+        auto load_entries = [&](int kk, int nfk, uint4 (&e_)[4]) {
             const size_t r = (size_t)kk * M;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) e_[q] = hl + 16 * q < nfk ? S.farw[r + hl + 16 * q] : 0ull;
+            for (int q = 0; q < 4; ++q) e_[q] = hl + 16 * q < nfk ? S.farw[r + hl + 16 * q] : make_uint4(0u, 0u, 0u, 0u);
         };
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e[q] = make_uint4(0u, 0u, 0u, 0u);
         const int step = 2 * SP_NH;
         int k = 2 * h + half;
         if (k < N) {
@@ -569,7 +579,9 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         int nf_n = k + step < N ? S.nnk[k + step] : 0;
         for (int k0 = 2 * h; k0 < N; k0 += step, k += step) {
             // the next step's entries and base, the count of the step after
-            uint64_t e_n[4] = {0ull, 0ull, 0ull, 0ull};
+            uint4 e_n[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) e_n[q] = make_uint4(0u, 0u, 0u, 0u);
             double bk_n = 0.0;
             if (k + step < N) {
                 load_entries(k + step, nf_n, e_n);
@@ -598,19 +610,19 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 // read together, then checked
                 uint64_t v[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) v[q] = hl + 16 * q < nf ? vpub[(int)(e[q] >> 32) / SP_BLK] : 0ull;
+                for (int q = 0; q < 4; ++q) v[q] = hl + 16 * q < nf ? vpub[(int)e[q].x / SP_BLK] : 0ull;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if (hl + 16 * q < nf) {
-                        const int kq = (int)(e[q] >> 32);
+                        const int kq = (int)e[q].x;
                         const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kq / SP_BLK + 1);
-                        if (got ? ((v[q] >> (kq % SP_BLK)) & 1ull) != 0ull : accepted(kq))
-                            sum += (double)__uint_as_float((uint32_t)e[q]);
+                        const bool acc = got ? ((v[q] >> (kq % SP_BLK)) & 1ull) != 0ull : accepted(kq);
+                        sum += (double)__uint_as_float(acc ? e[q].z : e[q].y);
                     }
                 }
                 for (int i = 64 + hl; i < nf; i += 16) {   // lists longer than 64 entries
-                    const uint64_t x = S.farw[(size_t)k * M + i];
-                    if (accepted((int)(x >> 32))) sum += (double)__uint_as_float((uint32_t)x);
+                    const uint4 x = S.farw[(size_t)k * M + i];
+                    sum += (double)__uint_as_float(accepted((int)x.x) ? x.z : x.y);
                 }
                 // the ring slot of move k was last read by the resolver in move k - SP_FR's block
                 if (k >= SP_FR && hl == 0) accepted(k - SP_FR);
@@ -859,7 +871,7 @@ static size_t spec_bytes(int N, int natom, int M, int nmt) {
     b += spal(sizeof(float) * ((size_t)N + SP_BLK));                 // thr (+ the last staged block's tail)
     b += 2 * spal(sizeof(float) * (size_t)N * M);                  // A, B
     const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
-    b += spal(sizeof(double) * N) + spal(sizeof(float) * npad * SP_W) + spal(sizeof(uint64_t) * (size_t)N * M);
+    b += spal(sizeof(double) * N) + spal(sizeof(float2) * npad * SP_W) + spal(sizeof(uint4) * (size_t)N * M);
     b += spal(sizeof(int32_t) * N);   // nnk
     b += spal(sizeof(int32_t) * N) + spal(sizeof(float) * N) + spal(sizeof(double));
     return b;
@@ -977,8 +989,8 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     S.B = (float *)take(sizeof(float) * (size_t)N * M);
     S.base = (double *)take(sizeof(double) * N);
     const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
-    S.nearT = (float *)take(sizeof(float) * npad * SP_W);
-    S.farw = (uint64_t *)take(sizeof(uint64_t) * (size_t)N * M);
+    S.nearT = (float2 *)take(sizeof(float2) * npad * SP_W);
+    S.farw = (uint4 *)take(sizeof(uint4) * (size_t)N * M);
     S.nnk = (int32_t *)take(sizeof(int32_t) * N);
     S.acc = (int32_t *)take(sizeof(int32_t) * N);
     S.fdiff = (float *)take(sizeof(float) * N);
@@ -1013,7 +1025,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     if (en_bytes > 48 * 1024) EPSR_SMEM_OPTIN(spec_energy_kernel);
     const int en_threads = min(SP_ET, max(32, (M - 1 + 31) / 32 * 32));   // one thread per stored partner
     EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, en_threads, en_bytes, s>>>(S));
-    EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(float) * npad * SP_W, s));
+    EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(float2) * npad * SP_W, s));
     EPSR_TIMED("spec_corr_kernel", s, spec_corr_kernel<<<N, 128, 0, s>>>(S));
     const size_t rsmem = spec_resolve_smem(N);
     EPSR_SMEM_OPTIN(spec_resolve_kernel);
