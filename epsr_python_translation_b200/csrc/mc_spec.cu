@@ -43,10 +43,10 @@ constexpr int SP_W = 64;        // near window of the resolver (moves): two runn
 constexpr int SP_FR = 128;      // far-sum ring (moves)
 constexpr int SP_BLK = 32;      // moves per staged block (and per published decision word)
 constexpr int SP_NSLOT = 4;     // staged blocks held in shared memory
-constexpr int SP_NH = 18;       // helper warps: warps 1..23 outside scheduler 0
+constexpr int SP_NH = 15;       // helper warps: warps 1..19 outside scheduler 0
 constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
 constexpr int SP_ET = 256;      // threads of a move's energy CTA (its stored partners)
-constexpr int SP_RT = 768;      // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
+constexpr int SP_RT = 640;      // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
 
 struct SpecDev {
@@ -550,44 +550,39 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         fadd = warp_sum_d(fadd);   // each lane's accepted moves, then the lanes in a fixed order
         if (lane == 0) *S.fadd_acc = fadd;
     } else if ((wid & 3) != 0) {
-        // ---- helper warps: the far part of each move's change, two consecutive moves a step,
-        // one per half-warp (16 lanes x 4 listed partners; longer lists loop).  A move's list
-        // length is read one step before its entries, and the entries one step before they are
-        // used, so no load waits on another and none reads past a list.
+        // ---- helper warps: the far part of each move's change, one move a step (32 lanes x 4
+        // listed partners; longer lists loop).  A move's list length is read three steps before
+        // it is used and its entries two steps before, so the loads are in flight while earlier
+        // moves are summed, and none reads past a list.
         const int h = wid - 1 - (wid >> 2);
         const int M = S.M;
-        const int half = lane >> 4, hl = lane & 15;
-        const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
-        (void)hmask;
-        uint4 e[4];
-        int nf = 0;
-        double bk = 0.0;
         auto load_entries = [&](int kk, int nfk, uint4 (&e_)[4]) {
             const size_t r = (size_t)kk * M;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) e_[q] = hl + 16 * q < nfk ? S.farw[r + hl + 16 * q] : make_uint4(0u, 0u, 0u, 0u);
+            for (int q = 0; q < 4; ++q)
+                e_[q] = lane + 32 * q < nfk ? S.farw[r + lane + 32 * q] : make_uint4(0u, 0u, 0u, 0u);
         };
-#pragma unroll
-        for (int q = 0; q < 4; ++q) e[q] = make_uint4(0u, 0u, 0u, 0u);
-        const int step = 2 * SP_NH;
-        int k = 2 * h + half;
-        if (k < N) {
-            nf = S.nnk[k];
-            bk = S.base[k];
-            load_entries(k, nf, e);
+        uint4 e0[4], e1[4];
+        int nf0 = 0, nf1 = 0, nf2 = 0;
+        double bk0 = 0.0, bk1 = 0.0;
+        const int st = SP_NH;
+        if (h < N) {
+            nf0 = S.nnk[h];
+            bk0 = S.base[h];
         }
-        int nf_n = k + step < N ? S.nnk[k + step] : 0;
-        for (int k0 = 2 * h; k0 < N; k0 += step, k += step) {
-            // the next step's entries and base, the count of the step after
-            uint4 e_n[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) e_n[q] = make_uint4(0u, 0u, 0u, 0u);
-            double bk_n = 0.0;
-            if (k + step < N) {
-                load_entries(k + step, nf_n, e_n);
-                bk_n = S.base[k + step];
-            }
-            const int nf_nn = k + 2 * step < N ? S.nnk[k + 2 * step] : 0;
+        if (h + st < N) {
+            nf1 = S.nnk[h + st];
+            bk1 = S.base[h + st];
+        }
+        if (h + 2 * st < N) nf2 = S.nnk[h + 2 * st];
+        load_entries(h, h < N ? nf0 : 0, e0);
+        load_entries(h + st, h + st < N ? nf1 : 0, e1);
+        for (int k = h; k < N; k += st) {
+            // two steps ahead: the entries and base of move k + 2 st, the length of k + 3 st
+            uint4 e2[4];
+            load_entries(k + 2 * st, k + 2 * st < N ? nf2 : 0, e2);
+            const double bk2 = k + 2 * st < N ? S.base[k + 2 * st] : 0.0;
+            const int nf3 = k + 3 * st < N ? S.nnk[k + 3 * st] : 0;
             double sum = 0.0;
             bool bad = false;
             // the decision of partner kq (published in word kq / 32), waiting for the word
@@ -605,45 +600,48 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 }
                 return (v >> (kq % SP_BLK)) & 1ull;
             };
-            if (k < N) {
-                // the listed order, lane by lane: entry hl + 16 q; the four decision words are
-                // read together, then checked
-                uint64_t v[4];
+            // the ring slot of move k was last read by the resolver in move k - SP_FR's block
+            uint64_t vring = (k >= SP_FR && lane == 0) ? vpub[(k - SP_FR) / SP_BLK] : 0ull;
+            // the listed order, lane by lane: entry lane + 32 q; the four decision words are
+            // read together, then checked
+            uint64_t v[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) v[q] = hl + 16 * q < nf ? vpub[(int)e[q].x / SP_BLK] : 0ull;
+            for (int q = 0; q < 4; ++q) v[q] = lane + 32 * q < nf0 ? vpub[(int)e0[q].x / SP_BLK] : 0ull;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (hl + 16 * q < nf) {
-                        const int kq = (int)e[q].x;
-                        const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kq / SP_BLK + 1);
-                        const bool acc = got ? ((v[q] >> (kq % SP_BLK)) & 1ull) != 0ull : accepted(kq);
-                        sum += (double)__uint_as_float(acc ? e[q].z : e[q].y);
-                    }
+            for (int q = 0; q < 4; ++q) {
+                if (lane + 32 * q < nf0) {
+                    const int kq = (int)e0[q].x;
+                    const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kq / SP_BLK + 1);
+                    const bool acc = got ? ((v[q] >> (kq % SP_BLK)) & 1ull) != 0ull : accepted(kq);
+                    sum += (double)__uint_as_float(acc ? e0[q].z : e0[q].y);
                 }
-                for (int i = 64 + hl; i < nf; i += 16) {   // lists longer than 64 entries
-                    const uint4 x = S.farw[(size_t)k * M + i];
-                    sum += (double)__uint_as_float(accepted((int)x.x) ? x.z : x.y);
-                }
-                // the ring slot of move k was last read by the resolver in move k - SP_FR's block
-                if (k >= SP_FR && hl == 0) accepted(k - SP_FR);
             }
+            for (int i = 128 + lane; i < nf0; i += 32) {   // lists longer than 128 entries
+                const uint4 x = S.farw[(size_t)k * M + i];
+                sum += (double)__uint_as_float(accepted((int)x.x) ? x.z : x.y);
+            }
+            if (k >= SP_FR && lane == 0 && (uint32_t)(vring >> 32) != (uint32_t)((k - SP_FR) / SP_BLK + 1))
+                accepted(k - SP_FR);
             if (__any_sync(0xffffffffu, bad)) {
                 if (lane == 0) fail();
                 break;
             }
-            // the half-warp's sum, in a fixed order
-#pragma unroll
-            for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            if (hl == 0 && k < N) {
-                const float fk = (float)(bk + sum);
+            sum = warp_sum_d(sum);
+            if (lane == 0) {
+                const float fk = (float)(bk0 + sum);
                 vfar[k % SP_FR] = ((uint64_t)(uint32_t)(k + 1) << 32) | __float_as_uint(fk);
             }
             __syncwarp();
 #pragma unroll
-            for (int q = 0; q < 4; ++q) e[q] = e_n[q];
-            nf = nf_n;
-            nf_n = nf_nn;
-            bk = bk_n;
+            for (int q = 0; q < 4; ++q) {
+                e0[q] = e1[q];
+                e1[q] = e2[q];
+            }
+            nf0 = nf1;
+            nf1 = nf2;
+            nf2 = nf3;
+            bk0 = bk1;
+            bk1 = bk2;
         }
     }
 }
