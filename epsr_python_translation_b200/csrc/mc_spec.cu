@@ -551,38 +551,33 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         if (lane == 0) *S.fadd_acc = fadd;
     } else if ((wid & 3) != 0) {
         // ---- helper warps: the far part of each move's change, one move a step (32 lanes x 4
-        // listed partners; longer lists loop).  A move's list length is read three steps before
-        // it is used and its entries two steps before, so the loads are in flight while earlier
-        // moves are summed, and none reads past a list.
+        // listed partners; longer lists loop).  A move's entries, list length and base are
+        // loaded two steps before they are used, into one of three register sets that take
+        // turns (the loop body is written out three times, so no register copy waits on a
+        // load in flight).
         const int h = wid - 1 - (wid >> 2);
         const int M = S.M;
-        auto load_entries = [&](int kk, int nfk, uint4 (&e_)[4]) {
-            const size_t r = (size_t)kk * M;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                e_[q] = lane + 32 * q < nfk ? S.farw[r + lane + 32 * q] : make_uint4(0u, 0u, 0u, 0u);
-        };
-        uint4 e0[4], e1[4];
-        int nf0 = 0, nf1 = 0, nf2 = 0;
-        double bk0 = 0.0, bk1 = 0.0;
         const int st = SP_NH;
-        if (h < N) {
-            nf0 = S.nnk[h];
-            bk0 = S.base[h];
-        }
-        if (h + st < N) {
-            nf1 = S.nnk[h + st];
-            bk1 = S.base[h + st];
-        }
-        if (h + 2 * st < N) nf2 = S.nnk[h + 2 * st];
-        load_entries(h, h < N ? nf0 : 0, e0);
-        load_entries(h + st, h + st < N ? nf1 : 0, e1);
-        for (int k = h; k < N; k += st) {
-            // two steps ahead: the entries and base of move k + 2 st, the length of k + 3 st
-            uint4 e2[4];
-            load_entries(k + 2 * st, k + 2 * st < N ? nf2 : 0, e2);
-            const double bk2 = k + 2 * st < N ? S.base[k + 2 * st] : 0.0;
-            const int nf3 = k + 3 * st < N ? S.nnk[k + 3 * st] : 0;
+        struct Stage {
+            uint4 e[4];
+            int nf;
+            double bk;
+        };
+        auto load = [&](int kk, Stage &g) {
+            if (kk < N) {
+                const size_t r = (size_t)kk * M;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    g.e[q] = lane + 32 * q < M ? S.farw[r + lane + 32 * q] : make_uint4(0u, 0u, 0u, 0u);
+                g.nf = S.nnk[kk];
+                g.bk = S.base[kk];
+            } else {
+                g.nf = 0;
+                g.bk = 0.0;
+            }
+        };
+        // the far part of move kk; false when a wait gave up (uniform over the warp)
+        auto process = [&](int kk, const Stage &g) -> bool {
             double sum = 0.0;
             bool bad = false;
             // the decision of partner kq (published in word kq / 32), waiting for the word
@@ -600,48 +595,50 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 }
                 return (v >> (kq % SP_BLK)) & 1ull;
             };
-            // the ring slot of move k was last read by the resolver in move k - SP_FR's block
-            uint64_t vring = (k >= SP_FR && lane == 0) ? vpub[(k - SP_FR) / SP_BLK] : 0ull;
+            // the ring slot of move kk was last read by the resolver in move kk - SP_FR's block
+            const uint64_t vring = (kk >= SP_FR && lane == 0) ? vpub[(kk - SP_FR) / SP_BLK] : 0ull;
             // the listed order, lane by lane: entry lane + 32 q; the four decision words are
             // read together, then checked
             uint64_t v[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) v[q] = lane + 32 * q < nf0 ? vpub[(int)e0[q].x / SP_BLK] : 0ull;
+            for (int q = 0; q < 4; ++q) v[q] = lane + 32 * q < g.nf ? vpub[(int)g.e[q].x / SP_BLK] : 0ull;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                if (lane + 32 * q < nf0) {
-                    const int kq = (int)e0[q].x;
+                if (lane + 32 * q < g.nf) {
+                    const int kq = (int)g.e[q].x;
                     const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kq / SP_BLK + 1);
                     const bool acc = got ? ((v[q] >> (kq % SP_BLK)) & 1ull) != 0ull : accepted(kq);
-                    sum += (double)__uint_as_float(acc ? e0[q].z : e0[q].y);
+                    sum += (double)__uint_as_float(acc ? g.e[q].z : g.e[q].y);
                 }
             }
-            for (int i = 128 + lane; i < nf0; i += 32) {   // lists longer than 128 entries
-                const uint4 x = S.farw[(size_t)k * M + i];
+            for (int i = 128 + lane; i < g.nf; i += 32) {   // lists longer than 128 entries
+                const uint4 x = S.farw[(size_t)kk * M + i];
                 sum += (double)__uint_as_float(accepted((int)x.x) ? x.z : x.y);
             }
-            if (k >= SP_FR && lane == 0 && (uint32_t)(vring >> 32) != (uint32_t)((k - SP_FR) / SP_BLK + 1))
-                accepted(k - SP_FR);
+            if (kk >= SP_FR && lane == 0 && (uint32_t)(vring >> 32) != (uint32_t)((kk - SP_FR) / SP_BLK + 1))
+                accepted(kk - SP_FR);
             if (__any_sync(0xffffffffu, bad)) {
                 if (lane == 0) fail();
-                break;
+                return false;
             }
             sum = warp_sum_d(sum);
             if (lane == 0) {
-                const float fk = (float)(bk0 + sum);
-                vfar[k % SP_FR] = ((uint64_t)(uint32_t)(k + 1) << 32) | __float_as_uint(fk);
+                const float fk = (float)(g.bk + sum);
+                vfar[kk % SP_FR] = ((uint64_t)(uint32_t)(kk + 1) << 32) | __float_as_uint(fk);
             }
             __syncwarp();
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                e0[q] = e1[q];
-                e1[q] = e2[q];
-            }
-            nf0 = nf1;
-            nf1 = nf2;
-            nf2 = nf3;
-            bk0 = bk1;
-            bk1 = bk2;
+            return true;
+        };
+        Stage g0, g1, g2;
+        load(h, g0);
+        load(h + st, g1);
+        for (int k = h; k < N; k += 3 * st) {
+            load(k + 2 * st, g2);
+            if (!process(k, g0) || k + st >= N) break;
+            load(k + 3 * st, g0);
+            if (!process(k + st, g1) || k + 2 * st >= N) break;
+            load(k + 4 * st, g1);
+            if (!process(k + 2 * st, g2)) break;
         }
     }
 }
