@@ -86,7 +86,8 @@ struct SpecDev {
     float *A, *B;                          // [N*M]
     double *base;                          // [N] each move's change if no earlier partner accepted
     float2 *nearT;                         // [Npad*W] near terms {rejected, accepted}, by the earlier move
-    uint4 *farw;                           // [N*M] far partners by visit position: {kp, rejected, accepted, 0}
+    int32_t *farkp;                        // [N*M] far partners by visit position: the partner's visit position
+    float2 *fart;                          // [N*M] and its two terms {rejected, accepted}
     int32_t *nnk;                          // [N] far partners listed for each move
     int32_t *acc;                          // [N] by visit position
     float *fdiff;                          // [N] by visit position
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(SP_ET) spec_energy_kernel(SpecDev S) {
 // partner p visited earlier both terms it can bring: A - S if p was rejected, B - (p's stored
 // energy after its move) if it was accepted.  Partners at most SP_W moves earlier go into p's
 // row of nearT (the resolver adds the term that applies as decisions are taken); the others
-// are listed for the helpers in store order, compacted to the front of k's row of farw as
+// are listed for the helpers in store order, compacted to the front of k's rows of farkp/fart as
 // (partner's visit position, both terms) words (nnk[k] of them).  Carrying both terms, never
 // their difference, keeps an energy that the final configuration does not contain (A against
 // a partner that has moved away) out of every sum.
@@ -367,7 +368,8 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
         }
         if (far) {
             const int i = off + __popc(bal & ((1u << lane) - 1u));
-            S.farw[krow + i] = make_uint4((uint32_t)kp, __float_as_uint(ca), __float_as_uint(cb), 0u);
+            S.farkp[krow + i] = kp;
+            S.fart[krow + i] = make_float2(ca, cb);
         }
         nfar += tot;
         __syncthreads();
@@ -382,13 +384,38 @@ __global__ void __launch_bounds__(128) spec_corr_kernel(SpecDev S) {
 }
 
 // ----------------------------------------------------------------- resolve
-// Shared memory of the resolver CTA (dynamic): the staged rows (float), the staged
-// thresholds, the blocks' mbarriers, the far-sum ring (one tagged word a move: the tag in the
-// high half, the float far part in the low) and the published decision words (tag in the
-// high half, one bit a move in the low).
+// Loads of data the previous kernels wrote and this one only reads, issued at their place in
+// the program (the compiler neither sinks them to their first use nor merges them away).
+__device__ __forceinline__ int ldg_pinned(const int32_t *p) {
+    int r;
+    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(r) : "l"(p));
+    return r;
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(umma::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(umma::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ double ldg_pinned(const double *p) {
+    double r;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(r) : "l"(p));
+    return r;
+}
+
+// Shared memory of the resolver CTA (dynamic): the staged rows ({rejected, accepted} terms),
+// the staged thresholds, the blocks' mbarriers, the far-sum ring (one tagged word a move: the
+// tag in the high half, the float far part in the low), each helper's two staged far lists,
+// and the published decision words (tag in the high half, one bit a move in the low).
 constexpr int SP_SROWS = SP_NSLOT * SP_BLK * SP_W * 8;
 constexpr int SP_STHR = SP_NSLOT * SP_BLK * 4;
-constexpr int SP_SHDR = SP_SROWS + SP_STHR + SP_NSLOT * 8 + SP_FR * 8;
+constexpr int SP_HCAP = 320;                                  // far partners a helper stages per move
+constexpr int SP_HSTAGE = SP_HCAP * 12;                       // one staged list: terms, then positions
+constexpr int SP_HOFF = SP_SROWS + SP_STHR + SP_NSLOT * 8 + SP_FR * 8;
+constexpr int SP_SHDR = SP_HOFF + SP_NH * 2 * SP_HSTAGE;
 
 __host__ __device__ constexpr size_t spec_resolve_smem(int N) {
     return (size_t)SP_SHDR + 8 * (size_t)((N + SP_BLK - 1) / SP_BLK);
@@ -494,7 +521,7 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
             // (its sum with the first's rejected or accepted term), and two ballots decide both --
             // bit i and i+1 of the first the first move's test and the second's if the first
             // rejects, the second the second's if the first accepts
-            for (; i + 1 < nr; i += 2) {
+            auto pair = [&](int i) {
                 const float2 ca0 = c0n, ca1 = c1n;
                 float2 cb0, cb1;
                 row_c(i + 1, cb0, cb1);
@@ -519,6 +546,13 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 A1 = (own1 && r1) ? dl1 : __fadd_rn(A1, dl1);
                 fd_own = own0 ? fdA : (own1 ? (ak ? fdB : fdA) : fd_own);
                 wbits |= ((ak ? 1u : 0u) | (ak1 ? 2u : 0u)) << i;
+            };
+            if (nr == SP_BLK) {   // a full block: the walk written out, its registers renamed by the compiler
+#pragma unroll
+                for (int i2 = 0; i2 < SP_BLK; i2 += 2) pair(i2);
+                i = SP_BLK;
+            } else {
+                for (; i + 1 < nr; i += 2) pair(i);
             }
             if (i < nr) {   // an odd last move
                 const float2 ca0 = c0n, ca1 = c1n;
@@ -550,34 +584,41 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
         fadd = warp_sum_d(fadd);   // each lane's accepted moves, then the lanes in a fixed order
         if (lane == 0) *S.fadd_acc = fadd;
     } else if ((wid & 3) != 0) {
-        // ---- helper warps: the far part of each move's change, one move a step (32 lanes x 4
-        // listed partners; longer lists loop).  A move's entries, list length and base are
-        // loaded two steps before they are used, into one of three register sets that take
-        // turns (the loop body is written out three times, so no register copy waits on a
-        // load in flight).
+        // ---- helper warps: the far part of each move's change, one move a step.  A move's
+        // listed far partners (up to SP_HCAP; a longer list reads the rest from global memory)
+        // are copied into one of the helper's two shared-memory stages by cp.async one step
+        // before they are summed, with its list length and base loaded two steps before; those
+        // two scalars live in three register sets that take turns (the loop body is written
+        // out three times), so nothing waits on a load in flight.
         const int h = wid - 1 - (wid >> 2);
         const int M = S.M;
         const int st = SP_NH;
-        struct Stage {
-            uint4 e[4];
+        unsigned char *hb = rsm + SP_HOFF + (size_t)h * 2 * SP_HSTAGE;
+        struct Scal {
             int nf;
             double bk;
         };
-        auto load = [&](int kk, Stage &g) {
+        auto load = [&](int kk, Scal &g) {
+            g.nf = kk < N ? ldg_pinned(S.nnk + kk) : 0;
+            g.bk = kk < N ? ldg_pinned(S.base + kk) : 0.0;
+        };
+        auto issue = [&](int kk, int nfk, int sg) {   // move kk's list into stage sg
             if (kk < N) {
                 const size_t r = (size_t)kk * M;
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    g.e[q] = lane + 32 * q < M ? S.farw[r + lane + 32 * q] : make_uint4(0u, 0u, 0u, 0u);
-                g.nf = S.nnk[kk];
-                g.bk = S.base[kk];
-            } else {
-                g.nf = 0;
-                g.bk = 0.0;
+                float2 *t = reinterpret_cast<float2 *>(hb + sg * SP_HSTAGE);
+                int *q = reinterpret_cast<int *>(hb + sg * SP_HSTAGE + SP_HCAP * 8);
+                const int n = min(nfk, SP_HCAP);
+                for (int i = lane; i < n; i += 32) {
+                    cp_async8(t + i, S.fart + r + i);
+                    cp_async4(q + i, S.farkp + r + i);
+                }
             }
+            cp_async_commit();
         };
-        // the far part of move kk; false when a wait gave up (uniform over the warp)
-        auto process = [&](int kk, const Stage &g) -> bool {
+        // the far part of move kk from stage sg; false when a wait gave up (uniform over the warp)
+        auto process = [&](int kk, const Scal &g, int sg) -> bool {
+            const float2 *t = reinterpret_cast<const float2 *>(hb + sg * SP_HSTAGE);
+            const int *q = reinterpret_cast<const int *>(hb + sg * SP_HSTAGE + SP_HCAP * 8);
             double sum = 0.0;
             bool bad = false;
             // the decision of partner kq (published in word kq / 32), waiting for the word
@@ -597,23 +638,29 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
             };
             // the ring slot of move kk was last read by the resolver in move kk - SP_FR's block
             const uint64_t vring = (kk >= SP_FR && lane == 0) ? vpub[(kk - SP_FR) / SP_BLK] : 0ull;
-            // the listed order, lane by lane: entry lane + 32 q; the four decision words are
-            // read together, then checked
-            uint64_t v[4];
+            // the listed order, lane by lane (entry lane + 32 j), four entries at a time: their
+            // positions, then their decision words, are read together
+            const int n = min(g.nf, SP_HCAP);
+            for (int c0 = 0; c0 < n; c0 += 128) {
+                int kq[4];
+                uint64_t v[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) v[q] = lane + 32 * q < g.nf ? vpub[(int)g.e[q].x / SP_BLK] : 0ull;
+                for (int j = 0; j < 4; ++j) kq[j] = c0 + lane + 32 * j < n ? q[c0 + lane + 32 * j] : -1;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (lane + 32 * q < g.nf) {
-                    const int kq = (int)g.e[q].x;
-                    const bool got = (uint32_t)(v[q] >> 32) == (uint32_t)(kq / SP_BLK + 1);
-                    const bool acc = got ? ((v[q] >> (kq % SP_BLK)) & 1ull) != 0ull : accepted(kq);
-                    sum += (double)__uint_as_float(acc ? g.e[q].z : g.e[q].y);
+                for (int j = 0; j < 4; ++j) v[j] = kq[j] >= 0 ? vpub[kq[j] / SP_BLK] : 0ull;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (kq[j] >= 0) {
+                        const bool got = (uint32_t)(v[j] >> 32) == (uint32_t)(kq[j] / SP_BLK + 1);
+                        const bool acc = got ? ((v[j] >> (kq[j] % SP_BLK)) & 1ull) != 0ull : accepted(kq[j]);
+                        const float2 tt = t[c0 + lane + 32 * j];
+                        sum += (double)(acc ? tt.y : tt.x);
+                    }
                 }
             }
-            for (int i = 128 + lane; i < g.nf; i += 32) {   // lists longer than 128 entries
-                const uint4 x = S.farw[(size_t)kk * M + i];
-                sum += (double)__uint_as_float(accepted((int)x.x) ? x.z : x.y);
+            for (int i = SP_HCAP + lane; i < g.nf; i += 32) {   // lists longer than SP_HCAP
+                const float2 tt = S.fart[(size_t)kk * M + i];
+                sum += (double)(accepted(S.farkp[(size_t)kk * M + i]) ? tt.y : tt.x);
             }
             if (kk >= SP_FR && lane == 0 && (uint32_t)(vring >> 32) != (uint32_t)((kk - SP_FR) / SP_BLK + 1))
                 accepted(kk - SP_FR);
@@ -626,20 +673,31 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
                 const float fk = (float)(g.bk + sum);
                 vfar[kk % SP_FR] = ((uint64_t)(uint32_t)(kk + 1) << 32) | __float_as_uint(fk);
             }
-            __syncwarp();
             return true;
         };
-        Stage g0, g1, g2;
+        // one step: stage the next move's list, load the scalars of the move after it, wait
+        // for this move's list and sum it
+        int sg = 0;
+        auto body = [&](int kk, const Scal &cur, const Scal &nxt, Scal &fill) -> bool {
+            issue(kk + st, nxt.nf, sg ^ 1);
+            load(kk + 2 * st, fill);
+            cp_async_wait1();   // this lane's copies of move kk
+            __syncwarp();       // and every lane's
+            const bool ok = process(kk, cur, sg);
+            __syncwarp();       // stage sg is read; the next step but one refills it
+            sg ^= 1;
+            return ok;
+        };
+        Scal g0, g1, g2;
         load(h, g0);
         load(h + st, g1);
+        issue(h, g0.nf, 0);
         for (int k = h; k < N; k += 3 * st) {
-            load(k + 2 * st, g2);
-            if (!process(k, g0) || k + st >= N) break;
-            load(k + 3 * st, g0);
-            if (!process(k + st, g1) || k + 2 * st >= N) break;
-            load(k + 4 * st, g1);
-            if (!process(k + 2 * st, g2)) break;
+            if (!body(k, g0, g1, g2) || k + st >= N) break;
+            if (!body(k + st, g1, g2, g0) || k + 2 * st >= N) break;
+            if (!body(k + 2 * st, g2, g0, g1)) break;
         }
+        cp_async_wait_all();   // no copy lands after the CTA's shared memory goes away
     }
 }
 
@@ -866,7 +924,8 @@ static size_t spec_bytes(int N, int natom, int M, int nmt) {
     b += spal(sizeof(float) * ((size_t)N + SP_BLK));                 // thr (+ the last staged block's tail)
     b += 2 * spal(sizeof(float) * (size_t)N * M);                  // A, B
     const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
-    b += spal(sizeof(double) * N) + spal(sizeof(float2) * npad * SP_W) + spal(sizeof(uint4) * (size_t)N * M);
+    b += spal(sizeof(double) * N) + spal(sizeof(float2) * npad * SP_W) + spal(sizeof(int32_t) * (size_t)N * M) +
+         spal(sizeof(float2) * (size_t)N * M);
     b += spal(sizeof(int32_t) * N);   // nnk
     b += spal(sizeof(int32_t) * N) + spal(sizeof(float) * N) + spal(sizeof(double));
     return b;
@@ -985,7 +1044,8 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     S.base = (double *)take(sizeof(double) * N);
     const size_t npad = ((size_t)N + SP_BLK - 1) / SP_BLK * SP_BLK;
     S.nearT = (float2 *)take(sizeof(float2) * npad * SP_W);
-    S.farw = (uint4 *)take(sizeof(uint4) * (size_t)N * M);
+    S.farkp = (int32_t *)take(sizeof(int32_t) * (size_t)N * M);
+    S.fart = (float2 *)take(sizeof(float2) * (size_t)N * M);
     S.nnk = (int32_t *)take(sizeof(int32_t) * N);
     S.acc = (int32_t *)take(sizeof(int32_t) * N);
     S.fdiff = (float *)take(sizeof(float) * N);
