@@ -54,10 +54,14 @@ OPS_PER_ENERGY_PAIR = 26
 OPS_PER_PAIR_UPDATE = 17
 UNIT = "moves/s"
 DEFAULT_SWEEPS = {"c3_water": 100}          # molfit sweeps per iteration (others: 5)
-DEFAULT_REPLICAS = {"c3_water": 2, "c2_mixture": 16}
+DEFAULT_REPLICAS = {"c3_water": 4, "c2_mixture": 16}
 # kernels the library brackets with CUDA events while timing is enabled
 TIMED_KERNELS = ("spec_energy_kernel", "spec_corr_kernel", "spec_resolve_kernel", "molfit_seq_kernel",
-                 "fm_count_kernel", "ag_inter_kernel", "fitexp_cluster_kernel")
+                 "fm_count_kernel", "ag_inter_kernel", "fitexp_cluster_kernel", "ahead_fill_kernel",
+                 "ran1_fill_kernel")
+# the ordered walk of spec_resolve_kernel on its own (one warp, rows in shared memory, no far
+# parts to wait for), measured on B200: the latency floor of a resolved move
+RESOLVE_WALK_CYCLES_PER_MOVE = 88.5
 
 
 def parse():
@@ -687,8 +691,15 @@ def roofline(it, ktimes, a):
                 "launch_ms": launch_ms, "launches": n}, extra
     if dom == "spec_resolve_kernel":
         ns = 1e6 * launch_ms / it.box.nmol
-        return {"bound": "latency", "kernel": dom, "achieved": ns, "peak": None, "unit": "ns per move (ordered walk)",
-                "frac": None, "traffic": None, "launch_ms": launch_ms, "launches": n}, extra
+        floor_ns = RESOLVE_WALK_CYCLES_PER_MOVE / mhz * 1000.0
+        fill = ktimes.get("ahead_fill_kernel")
+        if fill:
+            extra["ran1_fill_ns_per_move"] = 1e6 * fill[0] / fill[1] / it.box.nmol
+        return {"bound": "latency (ordered walk)", "kernel": dom, "achieved": floor_ns / ns, "peak": 1.0,
+                "unit": "walk floor / measured time per move", "frac": floor_ns / ns, "traffic": None,
+                "ns_per_move": ns, "floor_ns_per_move": floor_ns,
+                "floor_source": "the walk alone on B200, %.1f cycles per move at %.0f MHz" % (RESOLVE_WALK_CYCLES_PER_MOVE, mhz),
+                "launch_ms": launch_ms, "launches": n}, extra
     if dom == "fitexp_cluster_kernel":
         trials = max(it.fit_trials, 1)
         flops = 2.0 * wl.nq * wl.nterms * trials
