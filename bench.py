@@ -62,6 +62,8 @@ TIMED_KERNELS = ("spec_energy_kernel", "spec_corr_kernel", "spec_resolve_kernel"
 # the ordered walk of spec_resolve_kernel on its own (one warp, rows in shared memory, no far
 # parts to wait for), measured on B200: the latency floor of a resolved move
 RESOLVE_WALK_CYCLES_PER_MOVE = 88.5
+# a dependent warp shuffle on B200 (the step of the ran1 walk)
+RAN1_SHUFFLE_CYCLES = 32
 
 
 def parse():
@@ -699,6 +701,16 @@ def roofline(it, ktimes, a):
                 "unit": "walk floor / measured time per move", "frac": floor_ns / ns, "traffic": None,
                 "ns_per_move": ns, "floor_ns_per_move": floor_ns,
                 "floor_source": "the walk alone on B200, %.1f cycles per move at %.0f MHz" % (RESOLVE_WALK_CYCLES_PER_MOVE, mhz),
+                "launch_ms": launch_ms, "launches": n}, extra
+    if dom in ("ahead_fill_kernel", "ran1_fill_kernel"):
+        # the next cycle's ran1 values: 7 a move (3 rotation, 3 translation, 1 acceptance), one
+        # dependent warp shuffle per value
+        values = 7 * it.box.nmol
+        floor_ms = values * RAN1_SHUFFLE_CYCLES / mhz / 1000.0
+        return {"bound": "latency (ran1 shuffle chain)", "kernel": dom, "achieved": floor_ms / launch_ms, "peak": 1.0,
+                "unit": "chain floor / measured time per launch", "frac": floor_ms / launch_ms, "traffic": None,
+                "values_per_launch": values, "floor_ms": floor_ms,
+                "floor_source": "one dependent warp shuffle per value, %d cycles on B200 at %.0f MHz" % (RAN1_SHUFFLE_CYCLES, mhz),
                 "launch_ms": launch_ms, "launches": n}, extra
     if dom == "fitexp_cluster_kernel":
         trials = max(it.fit_trials, 1)

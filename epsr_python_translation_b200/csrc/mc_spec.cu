@@ -888,9 +888,16 @@ struct AheadStream {
 };
 static thread_local AheadStream g_ahead_streams[16];
 
+static size_t g_ahead_smem = 0;   // dynamic shared memory of the draws-ahead walk
+
 static int ahead_stream(AheadStream **out) {
     int dev = 0;
     EPSR_CUDA(cudaGetDevice(&dev));
+    if (!g_ahead_smem) {
+        int optin = 0;
+        EPSR_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        g_ahead_smem = (size_t)optin - 256;   // room for the kernel's own static table
+    }
     if (dev < 0 || dev >= 16) {
         epsr_set_error("epsr_molfit: device ordinal %d beyond the draws-ahead table", dev);
         return EPSR_ERR_ARG;
@@ -1072,7 +1079,12 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
         if (rc) return rc;
         EPSR_CUDA(cudaEventRecord(as->fork, s));
         EPSR_CUDA(cudaStreamWaitEvent(as->st, as->fork, 0));
-        EPSR_TIMED("ahead_fill_kernel", as->st, ahead_fill_kernel<<<1, 32, 0, as->st>>>(S.ran1_next, mc->ahead, S.off + N));
+        // the walk is one warp's chain of dependent shuffles: other CTAs on its SM would take
+        // issue slots from it, so it asks for all the shared memory a CTA may have, which keeps
+        // the SM to itself for the 2-3 ms it runs
+        EPSR_SMEM_OPTIN(ahead_fill_kernel);
+        EPSR_TIMED("ahead_fill_kernel", as->st,
+                   ahead_fill_kernel<<<1, 32, g_ahead_smem, as->st>>>(S.ran1_next, mc->ahead, S.off + N));
         EPSR_CUDA(cudaGetLastError());
         EPSR_CUDA(cudaEventRecord(as->join, as->st));
     }
@@ -1082,7 +1094,16 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, en_threads, en_bytes, s>>>(S));
     EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(float2) * npad * SP_W, s));
     EPSR_TIMED("spec_corr_kernel", s, spec_corr_kernel<<<N, 128, 0, s>>>(S));
-    const size_t rsmem = spec_resolve_smem(N);
+    // the walk is latency-bound on its scheduler: the CTA asks for all the shared memory a CTA
+    // may have (its own need, spec_resolve_smem(N), is checked above), so no other kernel's CTA
+    // shares the SM and takes issue slots from it
+    size_t rsmem = spec_resolve_smem(N);
+    {
+        int dev = 0, optin = 0;
+        EPSR_CUDA(cudaGetDevice(&dev));
+        EPSR_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        rsmem = max(rsmem, (size_t)optin - 1024);
+    }
     EPSR_SMEM_OPTIN(spec_resolve_kernel);
     EPSR_TIMED("spec_resolve_kernel", s, spec_resolve_kernel<<<1, SP_RT, rsmem, s>>>(S));
     spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
