@@ -745,13 +745,25 @@ def c4_arm(a):
     import numpy as np
     import torch
 
+    import torch.distributed as dist
+
     from epsr_python_translation_b200 import autotune, configs
-    from epsr_python_translation_b200.batch import BatchBoxes
+    from epsr_python_translation_b200.batch import BatchBoxes, partition_boxes
     from epsr_python_translation_b200.box import BoxArrays, Ran1State
     from oracle import oracle
-    torch.cuda.set_device(0)
-    systems = configs.c4_batch(seed=1)
-    bb = BatchBoxes(systems, rot_deg=10.0, trans_A=0.5, seed=1)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    all_systems = configs.c4_batch(seed=1)
+    # the boxes are independent: each rank advances its share, split greedily by atom count,
+    # with no exchange during a sweep
+    mine = partition_boxes([s.natom for s in all_systems], world)[rank]
+    systems = [all_systems[i] for i in mine]
+    bb = BatchBoxes(systems, rot_deg=10.0, trans_A=0.5, seed=1 + 1000 * rank)
     bb.total_energy()
     choice = autotune.tune(bb, "plain")
     g = bb.capture("plain")
@@ -779,7 +791,7 @@ def c4_arm(a):
     e1.record()
     torch.cuda.synchronize()
     bb.lib.epsr_timing_enable(0)
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     clk = clocks.stop()
     bb.check_status()
     kt = {}
@@ -790,26 +802,30 @@ def c4_arm(a):
             kt[kname] = {"total_ms": round(tms.value, 3), "launches": int(n.value),
                          "mean_us": round(1000 * tms.value / n.value, 2)}
     cnt = (bb.counters - c0).cpu().numpy().reshape(bb.nbox, 4)
-    moves = int(cnt[:, 0].sum())
-    npairs = int(pairs.item())
+    tot = torch.tensor([float(cnt[:, 0].sum()), float(pairs.item()), float(cnt[:, 2].sum())], dtype=torch.float64,
+                       device="cuda")
+    if world > 1:   # the moves and pair-updates of every rank's boxes
+        dist.all_reduce(tot)
+    moves, npairs, accepted = int(tot[0].item()), int(tot[1].item()), float(tot[2].item())
     value = moves / (ms / 1000.0)
     hbm, fp32, mhz, src = _peaks()
     hist_ms = kt.get("bmc_hist_inter_kernel", {}).get("total_ms", 0.0)
     launches_per_step = 6 + 2 * bb.steps_per_sweep + 3
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (64 seeded boxes: water and SiO2-like, log-uniform sizes)",
         "pair_updates_per_s": npairs / (ms / 1000.0),
-        "config": {"workload": "c4_batch", "boxes": len(systems), "atoms": int(sum(s.natom for s in systems)),
-                   "atoms_min_max": [int(min(s.natom for s in systems)), int(max(s.natom for s in systems))],
+        "config": {"workload": "c4_batch", "boxes": len(all_systems), "atoms": int(sum(s.natom for s in all_systems)),
+                   "atoms_min_max": [int(min(s.natom for s in all_systems)), int(max(s.natom for s in all_systems))],
+                   "boxes_per_gpu": "split over %d GPU(s) greedily by atom count, no exchange during a sweep" % world,
                    "moves_per_step": moves // a.steps, "steps_per_sweep": bb.steps_per_sweep,
                    "launches_per_step": launches_per_step, "launches_depend_on_box_count": False,
                    "autotuned": {"threads": choice["threads"], "hist_tile": choice["tile"]},
                    "step": "one graph launch per sweep of every box (checkerboard scheme) + all-pairs g(r) "
                            "histograms of every box (int64 counts) in one launch",
                    "l2": "flushed before every step by a 256 MB write, inside the timed region"},
-        "acceptance": float(cnt[:, 2].sum() / max(moves, 1)), "kernel_ms": kt,
+        "acceptance": accepted / max(moves, 1), "kernel_ms": kt,
         "roofline": {"bound": "fp32", "kernel": "bmc_hist_inter_kernel",
                      "achieved": (OPS_PER_PAIR_UPDATE * npairs / (hist_ms / 1000.0) / 1e12) if hist_ms else None,
                      "peak": fp32, "unit": "Tops/s (FP32 issue)",
@@ -817,7 +833,12 @@ def c4_arm(a):
                      "traffic": None, "peak_source": "nominal (148 SMs x 128 lanes x %.0f MHz)" % mhz},
         "gpu_launches": launches_per_step * a.steps, "clocks": clk,
     }
-    if not a.no_cpu_baseline:
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    if not a.no_cpu_baseline and world == 1:
         small = sorted(range(len(systems)), key=lambda i: systems[i].natom)[:4]
         t0 = time.perf_counter()
         mv = 0

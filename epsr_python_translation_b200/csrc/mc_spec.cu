@@ -45,7 +45,7 @@ constexpr int SP_BLK = 32;      // moves per staged block (and per published dec
 constexpr int SP_NSLOT = 4;     // staged blocks held in shared memory
 constexpr int SP_NH = 15;       // helper warps: warps 1..19 outside scheduler 0
 constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
-constexpr int SP_ET = 256;      // threads of a move's energy CTA (its stored partners)
+constexpr int SP_ET = 320;      // threads of a move's energy CTA (its stored partners: about 300 at 0.1 atoms/A^3)
 constexpr int SP_RT = 640;      // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
 
