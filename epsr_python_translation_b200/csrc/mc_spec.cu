@@ -115,23 +115,32 @@ __global__ void spec_plan_kernel(SpecDev S) {
     __syncthreads();
     for (int base = 0; base < S.N; base += blockDim.x) {
         const int k = base + tid;
-        int nd = 0, nr = 0;
+        int nd = 0, nr = 0, t = -1;
+        bool istr = false;
         if (k < S.N) {
             const int m = S.visit[k];
             S.vpos[m] = k;
             const int n = S.nato[m];
-            const int t = S.mtype[m];
-            atomicAdd(S.cnt_type + t, 1);
+            t = S.mtype[m];
             if (S.stepr > 0.0f && n > 1) {
                 nd += 3;
                 nr = 1;
-                atomicAdd(S.tries_rot + t, 1);
             }
             if (S.stepm > 0.0f) {
                 nd += 3;
-                atomicAdd(S.tries_tr + t, 1);
+                istr = true;
             }
             nd += 1;
+        }
+        // per-type counts, one atomic per type present in the warp (integers: any order)
+        {
+            const unsigned same = __match_any_sync(0xffffffffu, t);
+            const unsigned rotb = __ballot_sync(0xffffffffu, nr != 0), trb = __ballot_sync(0xffffffffu, istr);
+            if (t >= 0 && (int)(threadIdx.x & 31) == __ffs(same) - 1) {
+                atomicAdd(S.cnt_type + t, __popc(same));
+                if (rotb & same) atomicAdd(S.tries_rot + t, __popc(rotb & same));
+                if (trb & same) atomicAdd(S.tries_tr + t, __popc(trb & same));
+            }
         }
         // block exclusive scans of nd and nr
         __shared__ int wsd[32], wsr[32];
