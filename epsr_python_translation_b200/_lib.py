@@ -30,7 +30,8 @@ class Box(C.Structure):
     _fields_ = [("nmol", I32), ("natom", I32), ("ntype", I32), ("npairs", I32), ("nmoltype", I32),
                 ("naf", P), ("nato", P), ("mtype", P), ("itype", P), ("xa", P), ("ya", P), ("za", P),
                 ("xadd", P), ("yadd", P), ("zadd", P), ("pos", P), ("npairref", P), ("xstar", P), ("tab", P),
-                ("ld", I32), ("npt2", I32), ("izcut", I32), ("stepcl", F32), ("cubic", I32), ("lat", F32 * 6)]
+                ("ld", I32), ("npt2", I32), ("izcut", I32), ("stepcl", F32), ("cubic", I32), ("lat", F32 * 6),
+                ("maxat", I32)]
 
 
 class Cells(C.Structure):

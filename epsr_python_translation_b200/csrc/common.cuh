@@ -123,6 +123,79 @@ __device__ __forceinline__ float pair_energy(const Lattice &L, const Tables &T, 
     return pair_energy_d(T, d, icref);
 }
 
+// ----------------------------------------------------------------- pair energy by bin edges
+// The table index of en_atom_inter_scale is iz = ifix(d / stepcl) + 2 with the quotient
+// rounded to float.  The rounded quotient is a non-decreasing function of d, so
+// ifix(d / stepcl) >= n exactly when d >= D[n], D[n] being the smallest float whose rounded
+// quotient is at least n (bin_edge, found by bisection over the float bit patterns with the
+// same IEEE division).  An estimate n0 = ifix(d * cinv), with cinv chosen below 1/stepcl by
+// about 2^-20 relative (bins_cinv), never exceeds the true index and falls short of it by at
+// most one while n0 + 1 < 2^18, so the index is n0 + (d >= D[n0 + 1]): one multiplication, one
+// conversion and one comparison against a tabulated edge instead of the division.  Beyond
+// the last nonzero table point (n0 > izcut - 2) the pair is out of range whatever the
+// correction, since the estimate never exceeds the index.  A NaN distance gives n0 = 0 and
+// no correction, as ifix(NaN) = 0 in the division form, so the NaN propagates the same way.
+struct Bins {
+    const float4 *tab;    // [npairs*ld] {xavs, xavs1, ecoul, ecoul1}
+    const float4 *edge;   // [max(izcut - 1, 1)] {D[n+1], xstar[n+2], xstar[n+3], 0} at n
+    int ld, izcut;
+    float cinv;
+};
+
+__device__ __forceinline__ float bin_edge(float stepcl, int n) {
+    unsigned lo = 0u, hi = 0x7f800000u;   // +0 .. +inf
+    const float fn = (float)n;
+    while (lo < hi) {
+        const unsigned mid = lo + ((hi - lo) >> 1);
+        if (__fdiv_rn(__uint_as_float(mid), stepcl) >= fn) hi = mid;
+        else lo = mid + 1u;
+    }
+    return __uint_as_float(lo);
+}
+
+// one entry of Bins::edge (n = 0 .. max(izcut - 2, 0)); xstar has ld entries
+__device__ __forceinline__ float4 bin_edge_entry(float stepcl, const float *xstar, int ld, int n) {
+    return make_float4(bin_edge(stepcl, n + 1), xstar[min(n + 2, ld - 1)], xstar[min(n + 3, ld - 1)], 0.0f);
+}
+
+// the estimate's multiplier: below 1/stepcl by 2^-20 relative, rounded down (host, double)
+inline float bins_cinv(float stepcl) {
+    const double c = (1.0 / (double)stepcl) * (1.0 - 1.0 / 1048576.0);
+    float f = (float)c;
+    if ((double)f > c) f = nextafterf(f, 0.0f);
+    return f;
+}
+
+// x - nint(x) of minimagec's cubic branch, the rounding step written as selects
+__device__ __forceinline__ float wrap_cubic(float x) {
+    float t = truncf(x);
+    const float fr = __fsub_rn(x, t);
+    t = fr >= 0.5f ? __fadd_rn(t, 1.0f) : t;
+    t = fr <= -0.5f ? __fsub_rn(t, 1.0f) : t;
+    return __fsub_rn(x, t);
+}
+
+// pair_energy for a cubic box, bit for bit: the same distance, index, table entry and sum
+__device__ __forceinline__ float pair_energy_cubic_bins(const Bins &B, float4 p1, float4 p2, int icref) {
+    const float xd = wrap_cubic(__fsub_rn(p2.x, p1.x));
+    const float yd = wrap_cubic(__fsub_rn(p2.y, p1.y));
+    const float zd = wrap_cubic(__fsub_rn(p2.z, p1.z));
+    const float d = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(xd, xd), __fmul_rn(yd, yd)), __fmul_rn(zd, zd)));
+    const int n0 = __float2int_rz(__fmul_rn(d, B.cinv));
+    const int izm2 = B.izcut - 2;
+    const int nc = max(min(n0, izm2), 0);
+    const float4 e = __ldg(B.edge + nc);
+    const bool up = d >= e.x;
+    const int iz = nc + 2 + (up ? 1 : 0);
+    const bool in = n0 <= izm2 && iz <= B.izcut;
+    const int izc = min(iz, B.izcut);
+    const float4 t = __ldg(B.tab + (size_t)icref * B.ld + izc);
+    const float dt = __fsub_rn(d, up ? e.z : e.y);
+    float sume = __fadd_rn(t.x, __fmul_rn(t.y, dt));
+    sume = __fadd_rn(__fadd_rn(sume, t.z), __fmul_rn(t.w, dt));
+    return in ? sume : 0.0f;
+}
+
 // ----------------------------------------------------------------- ran1 (device, one lane)
 // auxiliary_routines.py:324-391 with state {idum, iy, mcall, iv[32]}.
 struct Ran1 {

@@ -48,6 +48,7 @@ constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
 constexpr int SP_ET = 320;      // threads of a move's energy CTA (its stored partners: about 300 at 0.1 atoms/A^3)
 constexpr int SP_RT = 640;      // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
+constexpr int SP_MAXEDGE = 16384;  // table points indexed by bin edges (beyond: the energy pass divides)
 
 struct SpecDev {
     Lattice L;
@@ -92,6 +93,10 @@ struct SpecDev {
     int32_t *acc;                          // [N] by visit position
     float *fdiff;                          // [N] by visit position
     double *fadd_acc;                      // [1]
+    Bins bins;                             // the energy pass's table index by bin edges (cubic boxes)
+    float4 *edge_w;                        // [nedge] written by the propose pass
+    int nedge;                             // 0: the energy pass divides (triclinic box, or too many bins)
+    int ev;                                // the energy pass's staged values per chunk (>= 2 maxat^2)
 };
 
 // ----------------------------------------------------------------- plan
@@ -212,10 +217,15 @@ __device__ __forceinline__ float metropolis_threshold(float u) {
 
 __global__ void spec_propose_kernel(SpecDev S) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < S.nedge) S.edge_w[k] = bin_edge_entry(S.T.stepcl, S.T.xstar, S.T.ld, k);
     if (k >= S.N) return;
     const float pi = 3.14159265358979323846f;
     const int m = S.visit[k];
     const int n = S.nato[m];
+    if (n > SP_MAXAT) {   // beyond this path's per-molecule arrays: the sequential kernel refuses the cycle
+        atomicExch(S.flags, 1);
+        return;
+    }
     const int a0 = S.naf[m];
     const int t = S.mtype[m];
     const float *u = (S.use_ahead && *S.use_ahead ? S.ahead_vals : S.draws) + S.off[k];
@@ -295,28 +305,137 @@ __device__ __forceinline__ void mol_energy_ab(const Lattice &L, const Tables &T,
     eb = xb;
 }
 
-// One CTA per move, one thread per stored partner: the partner's A and, if it is visited
-// earlier in the cycle, its B.
-__global__ void __launch_bounds__(SP_ET) spec_energy_kernel(SpecDev S) {
-    extern __shared__ int spr[];   // npairref [ntype*ntype]
+// One CTA per move.  The stored partners are taken in chunks of at most one per thread whose
+// pair values fit the staging area; a chunk is spread over the CTA as items (partner, partner
+// atom ja, which position: cycle start or proposed), each item evaluating its atom against
+// every atom ia of the moved molecule into the staging area at [ia][ja], and then one thread
+// per partner sums its values in the reference's order (ia outer, ja inner, from +0).  Every
+// pair value is pair_energy of the same operands as en_change, so A and B are the values of
+// mol_energy_ab bit for bit; the items keep a partner's nine (water) or more pair evaluations
+// independent of each other instead of one thread's dependent chain of table loads.
+constexpr int SP_EV = 2 * SP_MAXAT * SP_MAXAT;   // staged pair values per chunk at most (one partner's A and B)
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
+}
+
+template <bool BINS>
+#ifndef SP_EN_MINB
+#define SP_EN_MINB 4
+#endif
+__global__ void __launch_bounds__(SP_ET, SP_EN_MINB) spec_energy_kernel(SpecDev S) {
+    extern __shared__ __align__(16) unsigned char en_smem[];
+    const int ev = S.ev;                                                 // staged values per chunk
+    float *vals = reinterpret_cast<float *>(en_smem);                  // [ev]
+    uint16_t *items = reinterpret_cast<uint16_t *>(vals + ev);           // [ev] (chunk thread << 7) | item
+    int *spr = reinterpret_cast<int *>(items + ((ev + 1) & ~1));          // npairref [ntype*ntype]
     __shared__ float4 sa[SP_MAXAT];
+    __shared__ int c_b0[SP_ET], c_nb[SP_ET], c_voff[SP_ET];
+    __shared__ int ws_v[SP_ET / 32], ws_i[SP_ET / 32];
+    __shared__ int s_nitems;
     if (S.flags[0]) return;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int k = blockIdx.x;
     const int m = S.visit[k];
     const int na = S.nato[m], a0 = S.naf[m];
-    for (int i = threadIdx.x; i < S.ntype * S.ntype; i += blockDim.x) spr[i] = S.npairref[i];
-    for (int i = threadIdx.x; i < na; i += blockDim.x) sa[i] = S.npos[a0 + i];
-    __syncthreads();
+    const int ntype = S.ntype;
+    const Lattice L = S.L;
+    const Tables T = S.T;
+    const float4 *__restrict__ pos = S.pos;
+    const float4 *__restrict__ npos = S.npos;
+    for (int i = tid; i < ntype * ntype; i += blockDim.x) spr[i] = S.npairref[i];
+    for (int i = tid; i < na; i += blockDim.x) sa[i] = S.npos[a0 + i];
     const int nn = S.nergpairm[m];
     const size_t row = (size_t)m * S.M;
-    for (int s = 1 + threadIdx.x; s < nn; s += blockDim.x) {
-        const int p = S.molergpair[row + s];
-        const int b0 = S.naf[p], nb = S.nato[p];
-        const bool hb = S.vpos[p] < k;
-        float ea, eb;
-        mol_energy_ab(S.L, S.T, sa, na, S.pos + b0, S.npos + b0, nb, hb, spr, S.ntype, ea, eb);
-        S.A[row + s] = __fadd_rn(0.0f, ea);
-        if (hb) S.B[row + s] = __fadd_rn(0.0f, eb);
+    __syncthreads();
+    for (int s0 = 1; s0 < nn;) {
+        // 1. this thread's partner (slot s0 + tid) and the value / item offsets of the chunk
+        const int s = s0 + tid;
+        int b0 = 0, nb = 0, nv = 0, ni = 0;
+        bool hb = false;
+        if (s < nn) {
+            const int p = S.molergpair[row + s];
+            b0 = S.naf[p];
+            nb = S.nato[p];
+            hb = S.vpos[p] < k;
+            ni = hb ? 2 * nb : nb;
+            nv = na * ni;
+        }
+        int iv = warp_incl_scan(nv, lane), ii = warp_incl_scan(ni, lane);
+        if (lane == 31) {
+            ws_v[wid] = iv;
+            ws_i[wid] = ii;
+        }
+        __syncthreads();
+        for (int w = 0; w < wid; ++w) {
+            iv += ws_v[w];
+            ii += ws_i[w];
+        }
+        // the chunk is the prefix of partners whose values fit (at least the first: nv <= ev)
+        const bool take = s < nn && iv <= ev;
+        if (take) {
+            c_b0[tid] = b0;
+            c_nb[tid] = nb;
+            c_voff[tid] = iv - nv;
+            for (int j = 0; j < ni; ++j) items[ii - ni + j] = (uint16_t)((tid << 7) | j);
+        }
+        const int ntake = __syncthreads_count(take);
+        if (take && tid == ntake - 1) s_nitems = ii;
+        __syncthreads();
+        // 2. items: (partner, ja, position) against every atom of the moved molecule
+        const int nit = s_nitems;
+        for (int it = tid; it < nit; it += blockDim.x) {
+            const int code = items[it];
+            const int t = code >> 7, j = code & 127;
+            const int pb = c_b0[t], pn = c_nb[t];
+            const bool nw_pos = j >= pn;
+            const int ja = nw_pos ? j - pn : j;
+            const float4 p2 = nw_pos ? npos[pb + ja] : __ldg(pos + pb + ja);
+            float *v = vals + c_voff[t] + (nw_pos ? na * pn : 0) + ja;
+            const int *col = spr + __float_as_int(p2.w);
+            // three atoms of the moved molecule at a time (independent evaluations in flight; a
+            // short last group repeats the molecule's last atom and stores nothing for it)
+            for (int ia = 0; ia < na; ia += 3) {
+                const int i1 = min(ia + 1, na - 1), i2 = min(ia + 2, na - 1);
+                const float4 q0 = sa[ia], q1 = sa[i1], q2 = sa[i2];
+                const int c0 = col[__float_as_int(q0.w) * ntype], c1 = col[__float_as_int(q1.w) * ntype],
+                          c2 = col[__float_as_int(q2.w) * ntype];
+                float e0, e1, e2;
+                if (BINS) {
+                    e0 = pair_energy_cubic_bins(S.bins, q0, p2, c0);
+                    e1 = pair_energy_cubic_bins(S.bins, q1, p2, c1);
+                    e2 = pair_energy_cubic_bins(S.bins, q2, p2, c2);
+                } else {
+                    e0 = pair_energy(L, T, q0, p2, c0);
+                    e1 = pair_energy(L, T, q1, p2, c1);
+                    e2 = pair_energy(L, T, q2, p2, c2);
+                }
+                v[ia * pn] = e0;
+                if (ia + 1 < na) v[i1 * pn] = e1;
+                if (ia + 2 < na) v[i2 * pn] = e2;
+            }
+        }
+        __syncthreads();
+        // 3. each taken partner's A (and B) summed in the reference's order
+        if (take) {
+            const float *v = vals + c_voff[tid];
+            const int n2 = na * nb;
+            float xa = 0.0f;
+            for (int q = 0; q < n2; ++q) xa = __fadd_rn(xa, v[q]);
+            S.A[row + s] = xa;
+            if (hb) {
+                float xb = 0.0f;
+                for (int q = 0; q < n2; ++q) xb = __fadd_rn(xb, v[n2 + q]);
+                S.B[row + s] = xb;
+            }
+        }
+        s0 += ntake;
+        __syncthreads();   // the staging area and chunk tables are rewritten by the next chunk
     }
 }
 
@@ -944,6 +1063,7 @@ static size_t spec_bytes(int N, int natom, int M, int nmt) {
          spal(sizeof(float2) * (size_t)N * M);
     b += spal(sizeof(int32_t) * N);   // nnk
     b += spal(sizeof(int32_t) * N) + spal(sizeof(float) * N) + spal(sizeof(double));
+    b += spal(sizeof(float4) * SP_MAXEDGE);   // bin edges of the energy pass
     return b;
 }
 
@@ -1066,6 +1186,19 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     S.acc = (int32_t *)take(sizeof(int32_t) * N);
     S.fdiff = (float *)take(sizeof(float) * N);
     S.fadd_acc = (double *)take(sizeof(double));
+    {
+        float4 *edge = (float4 *)take(sizeof(float4) * SP_MAXEDGE);
+        const int nedge = max(S.T.izcut - 1, 1);
+        if (box->cubic && nedge <= SP_MAXEDGE && S.T.stepcl > 0.0f) {
+            S.nedge = nedge;
+            S.edge_w = edge;
+            S.bins.tab = S.T.tab;
+            S.bins.edge = edge;
+            S.bins.ld = S.T.ld;
+            S.bins.izcut = S.T.izcut;
+            S.bins.cinv = bins_cinv(S.T.stepcl);
+        }
+    }
 
     // draws ahead: only with a buffer that holds a whole cycle's values (at most 7 a move)
     const bool ahead = mc->ahead && mc->ahead_cap >= (int64_t)N * 7;
@@ -1074,12 +1207,12 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
         S.ahead_vals = reinterpret_cast<const float *>(mc->ahead + AH_VALS);
         S.use_ahead = use;
     }
-    spec_plan_kernel<<<1, 1024, 0, s>>>(S);
+    EPSR_TIMED("spec_plan_kernel", s, spec_plan_kernel<<<1, 1024, 0, s>>>(S));
     ran1_copy_kernel<<<1, 64, 0, s>>>(mc->ran1, S.ran1_next);
     if (ahead) ahead_adopt_kernel<<<1, 32, 0, s>>>(mc->ran1, mc->ahead, S.off + N, S.ran1_next, nfill, use);
     int rc = ran1_fill_device_count(S.ran1_next, S.draws, ahead ? nfill : S.off + N, (int64_t)N * 7 + 1, s);
     if (rc) return rc;
-    spec_propose_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
+    EPSR_TIMED("spec_propose_kernel", s, spec_propose_kernel<<<(max(N, S.nedge) + 127) / 128, 128, 0, s>>>(S));
     // the next cycle's values, from the state after this cycle's draws, on the second stream
     // once nothing of this cycle reads the buffer any more; joined before this call returns
     AheadStream *as = nullptr;
@@ -1097,10 +1230,19 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
         EPSR_CUDA(cudaGetLastError());
         EPSR_CUDA(cudaEventRecord(as->join, as->st));
     }
-    const size_t en_bytes = sizeof(int) * (size_t)box->ntype * box->ntype;
-    if (en_bytes > 48 * 1024) EPSR_SMEM_OPTIN(spec_energy_kernel);
-    const int en_threads = min(SP_ET, max(32, (M - 1 + 31) / 32 * 32));   // one thread per stored partner
-    EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<<<N, en_threads, en_bytes, s>>>(S));
+    {
+        const int ma = box->maxat > 0 && box->maxat <= SP_MAXAT ? box->maxat : SP_MAXAT;
+        S.ev = max(2 * ma * ma, 4096);
+    }
+    const size_t en_bytes = sizeof(float) * (size_t)S.ev + sizeof(uint16_t) * (size_t)((S.ev + 1) & ~1) +
+                            sizeof(int) * (size_t)box->ntype * box->ntype;
+    if (S.nedge) {
+        EPSR_SMEM_OPTIN(spec_energy_kernel<true>);
+        EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<true><<<N, SP_ET, en_bytes, s>>>(S));
+    } else {
+        EPSR_SMEM_OPTIN(spec_energy_kernel<false>);
+        EPSR_TIMED("spec_energy_kernel", s, spec_energy_kernel<false><<<N, SP_ET, en_bytes, s>>>(S));
+    }
     EPSR_CUDA(cudaMemsetAsync(S.nearT, 0, sizeof(float2) * npad * SP_W, s));
     EPSR_TIMED("spec_corr_kernel", s, spec_corr_kernel<<<N, 128, 0, s>>>(S));
     // the walk is latency-bound on its scheduler: the CTA asks for all the shared memory a CTA
@@ -1115,9 +1257,8 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     }
     EPSR_SMEM_OPTIN(spec_resolve_kernel);
     EPSR_TIMED("spec_resolve_kernel", s, spec_resolve_kernel<<<1, SP_RT, rsmem, s>>>(S));
-    spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
-    spec_commit_store_kernel<<<N, 128, 0, s>>>(S);
-    spec_epilogue_kernel<<<1, 32, 0, s>>>(S);
+    EPSR_TIMED("spec_commit_kernels", s, spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
+               spec_commit_store_kernel<<<N, 128, 0, s>>>(S); spec_epilogue_kernel<<<1, 32, 0, s>>>(S));
     EPSR_CUDA(cudaGetLastError());
     if (ahead) EPSR_CUDA(cudaStreamWaitEvent(s, as->join, 0));
     // a cycle with a translation retry runs on the sequential kernel (no-op otherwise)

@@ -90,6 +90,7 @@ class DeviceBox:
         s.cubic = 1 if b.cubic else 0
         for i in range(6):
             s.lat[i] = float(b.lat6[i])
+        s.maxat = int(np.max(b.nato)) if b.nmol else 0
         self.cbox = s
         check(self.lib.epsr_box_positions(C.byref(s), _stream()))
 

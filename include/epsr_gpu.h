@@ -54,6 +54,7 @@ typedef struct {
     float stepcl;            /* cellst/dmax */
     int32_t cubic;           /* 1: cubic minimum image; 0: triclinic via lat */
     float lat[6];            /* alatx, blatx, clatx, blaty, claty, clatz (box units) */
+    int32_t maxat;           /* largest nato, or 0 (unknown: taken as 64); sizes shared-memory staging */
 } epsr_box_t;
 
 /* Cell list (CSR).  cell_mols in cell order is also the molfit visit order. */
