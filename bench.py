@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned delayed-acceptance comparison on C5 (learned vs plain ESS/s)")
     ap.add_argument("--c5-boxes", type=int, default=16, help="C5 boxes advanced together by the batched arms")
+    ap.add_argument("--c5-spec-boxes", type=int, default=4,
+                    help="C5 boxes advanced at once on the reference-order (speculative) path")
     ap.add_argument("--c5-sweeps", type=int, default=200, help="timed sweeps of each C5 arm")
     ap.add_argument("--c5-pairs", type=int, default=1000000, help="(features, beta dE) pairs the surrogate trains on")
     ap.add_argument("--strict", action="store_true", help="bit-identical sequential sums")
@@ -916,46 +918,94 @@ def learned_c5(a, steps=None):
                       "ess_per_s": float(e_d.sum() / (ms_d / 1e3)),
                       "training": {k: v for k, v in rep.items()}, "record_s": rec_s,
                       "heldout_bound_kT": RMSE_BOUND, "residual_rmse_last_step_kT": lm.residual_rmse()}
-    # (1) the reference-order plain GPU path on one box from box 0's configuration
-    co = lm.bb.download()
-    ms_, as_ = lm.bb.box_slices(0)
-    box = BoxArrays.from_system(s0)
-    for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
-        getattr(box, k)[:] = co[k][as_ if k in ("xa", "ya", "za") else ms_]
-    d = DeviceBox(box)
-    d.cell_list(10, box.sepmax)
-    d.fmolec1(configs.intra_energies(s0), strict=False)
-    tmax, tmin = trsteps(box.natomr)
-    nmt = box.nmoltype
-    d.mc_setup(rejrate=np.float32(0.75), stepr=1.0, stepm=1.0, wholerot=np.full(nmt, 10.0 / 180.0, np.float32),
-               wholetrans=np.full(nmt, 0.5, np.float32) / np.float32(s0.dmax), ran1=Ran1State(idum=-5),
-               trstepmax=tmax, trstepmin=tmin)
+    # (1) the reference-order plain GPU path on one box from box 0's configuration, and (4) on
+    # R boxes at once (boxes 0..R-1 of the batched run), each on its own stream and host thread
     nref = max(20, nsw // 4)
-    for _ in range(5):
-        d.molfit(strict=False)
-    ser = torch.zeros(nref, dtype=torch.float32, device="cuda")
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for i in range(nref):
-        d.molfit(strict=False)
-        ser[i] = d.m_fadds[0]
-    e1.record()
-    torch.cuda.synchronize()
-    d.check_status()
-    ms_r = e0.elapsed_time(e1)
-    e_r, tau_r = ess(ser.cpu().numpy().astype(np.float64)[:, None])
-    out["reference_order_plain"] = {"boxes": 1, "sweeps": nref, "ms": ms_r, "moves_per_s": nref * s0.nmol / (ms_r / 1e3),
-                                    "tau_sweeps": float(tau_r[0]), "ess": float(e_r.sum()),
-                                    "ess_per_s": float(e_r.sum() / (ms_r / 1e3)),
-                                    "note": "the speculative molfit cycle, fast sums, adaptive steps as molfit"}
+    r1 = reference_order_boxes(lm, s0, 1, nref)
+    out["reference_order_plain"] = dict(r1, note="the speculative molfit cycle, fast sums, adaptive steps as molfit")
+    R = max(1, min(a.c5_spec_boxes, B))
+    rR = reference_order_boxes(lm, s0, R, nref)
+    out["reference_order_plain_concurrent"] = dict(
+        rR, note="the same path on %d boxes at once (own stream and host thread each); ESS summed over boxes" % R)
     base = out["reference_order_plain"]["ess_per_s"]
     out["learned_vs_plain_ess_per_s"] = out["learned"]["ess_per_s"] / base if base > 0 else None
     out["batched_plain_vs_plain_ess_per_s"] = out["batched_plain"]["ess_per_s"] / base if base > 0 else None
     out["learned_vs_batched_plain_ess_per_s"] = (out["learned"]["ess_per_s"] / out["batched_plain"]["ess_per_s"]
                                                  if out["batched_plain"]["ess_per_s"] > 0 else None)
+    out["concurrent_plain_vs_plain_ess_per_s"] = out["reference_order_plain_concurrent"]["ess_per_s"] / base if base > 0 else None
     out["wall_s"] = time.perf_counter() - t0
     return out
+
+
+def reference_order_boxes(lm, s0, R, nref):
+    """The speculative molfit cycle on R C5 boxes at once, started from boxes 0..R-1 of the
+    batched run: nref timed sweeps of every box after 5 untimed ones, each box on its own stream
+    and host thread; device time from events on a common stream that every box stream joins at
+    both ends.  ESS of each box's energy series (molfit's running fadds), summed over boxes."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    from epsr_python_translation_b200 import configs
+    from epsr_python_translation_b200.box import BoxArrays, Ran1State, trsteps
+    from epsr_python_translation_b200.device import DeviceBox
+    from epsr_python_translation_b200.learned import ess
+    co = lm.bb.download()
+    main = torch.cuda.current_stream()
+    streams = [torch.cuda.Stream() for _ in range(R)]
+    boxes, sers = [], []
+    for r in range(R):
+        ms_, as_ = lm.bb.box_slices(r)
+        box = BoxArrays.from_system(s0)
+        for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+            getattr(box, k)[:] = co[k][as_ if k in ("xa", "ya", "za") else ms_]
+        with torch.cuda.stream(streams[r]):
+            d = DeviceBox(box)
+            d.cell_list(10, box.sepmax)
+            d.fmolec1(configs.intra_energies(s0), strict=False)
+            tmax, tmin = trsteps(box.natomr)
+            nmt = box.nmoltype
+            d.mc_setup(rejrate=np.float32(0.75), stepr=1.0, stepm=1.0,
+                       wholerot=np.full(nmt, 10.0 / 180.0, np.float32),
+                       wholetrans=np.full(nmt, 0.5, np.float32) / np.float32(s0.dmax), ran1=Ran1State(idum=-5 - r),
+                       trstepmax=tmax, trstepmin=tmin)
+            for _ in range(5):
+                d.molfit(strict=False)
+            sers.append(torch.zeros(nref, dtype=torch.float32, device="cuda"))
+        boxes.append(d)
+    torch.cuda.synchronize()
+    errs = []
+
+    def body(r):
+        try:
+            with torch.cuda.stream(streams[r]):
+                streams[r].wait_event(ev0)
+                for i in range(nref):
+                    boxes[r].molfit(strict=False)
+                    sers[r][i] = boxes[r].m_fadds[0]
+        except Exception as e:  # noqa: BLE001  (re-raised on the main thread)
+            errs.append(e)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(main)
+    th = [threading.Thread(target=body, args=(r,)) for r in range(R)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    if errs:
+        raise errs[0]
+    for st in streams:
+        main.wait_stream(st)
+    ev1.record(main)
+    torch.cuda.synchronize()
+    for d in boxes:
+        d.check_status()
+    ms_r = ev0.elapsed_time(ev1)
+    e_r, tau_r = ess(torch.stack(sers, 1).cpu().numpy().astype(np.float64))
+    return {"boxes": R, "sweeps": nref, "ms": ms_r, "moves_per_s": R * nref * s0.nmol / (ms_r / 1e3),
+            "tau_sweeps": [float(t) for t in tau_r], "ess": float(e_r.sum()), "ess_per_s": float(e_r.sum() / (ms_r / 1e3))}
 
 
 def c5_arm(a):

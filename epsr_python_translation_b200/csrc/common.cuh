@@ -166,21 +166,20 @@ inline float bins_cinv(float stepcl) {
     return f;
 }
 
-// x - nint(x) of minimagec's cubic branch, the rounding step written as selects
-__device__ __forceinline__ float wrap_cubic(float x) {
-    float t = truncf(x);
-    const float fr = __fsub_rn(x, t);
-    t = fr >= 0.5f ? __fadd_rn(t, 1.0f) : t;
-    t = fr <= -0.5f ? __fsub_rn(t, 1.0f) : t;
-    return __fsub_rn(x, t);
+// The square of minimagec's cubic branch, (x - nint(x))^2.  nint rounds halves away from zero,
+// rint to even; the two differ only when x is an odd multiple of one half, where x - nint(x)
+// and x - rint(x) are +0.5 and -0.5 in some order -- the same square.  Away from those points
+// they are the same integer, and x - rint(x) is exact (|x| < 2^23; beyond, both are x - x).
+// rint is one instruction where the truncation form of nint takes six.
+__device__ __forceinline__ float wrap_sq(float x) {
+    const float r = __fsub_rn(x, rintf(x));
+    return __fmul_rn(r, r);
 }
 
 // pair_energy for a cubic box, bit for bit: the same distance, index, table entry and sum
 __device__ __forceinline__ float pair_energy_cubic_bins(const Bins &B, float4 p1, float4 p2, int icref) {
-    const float xd = wrap_cubic(__fsub_rn(p2.x, p1.x));
-    const float yd = wrap_cubic(__fsub_rn(p2.y, p1.y));
-    const float zd = wrap_cubic(__fsub_rn(p2.z, p1.z));
-    const float d = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(xd, xd), __fmul_rn(yd, yd)), __fmul_rn(zd, zd)));
+    const float d = __fsqrt_rn(__fadd_rn(__fadd_rn(wrap_sq(__fsub_rn(p2.x, p1.x)), wrap_sq(__fsub_rn(p2.y, p1.y))),
+                                         wrap_sq(__fsub_rn(p2.z, p1.z))));
     const int n0 = __float2int_rz(__fmul_rn(d, B.cinv));
     const int izm2 = B.izcut - 2;
     const int nc = max(min(n0, izm2), 0);
