@@ -1277,6 +1277,158 @@ int oracle_molfit_shake(oracle_sys *S, oracle_store *E, oracle_mcpar *P, const o
     return 0;
 }
 
+/* centreofmassi ato_manipulation_rev4.py:442: the molecule's offsets moved so that their
+ * centre of mass (atoms that are not q-type, weighted by amassa) is at the molecule centre */
+static void centreofmassi(oracle_sys *S, const oracle_intra *I, int im) {
+    const int a0 = S->naf[im], n = S->nato[im];
+    float x1 = 0.0f, y1 = 0.0f, z1 = 0.0f, summass = 0.0f;
+    for (int k = 0; k < n; ++k) {
+        const int a = a0 + k;
+        if (I->qtype[a] == 0) {
+            const float am = I->amassa[S->itype[a]];
+            x1 = x1 + S->xa[a] * am;
+            y1 = y1 + S->ya[a] * am;
+            z1 = z1 + S->za[a] * am;
+            summass = summass + am;
+        }
+    }
+    if (summass > 0.0f) {
+        x1 = x1 / summass;
+        y1 = y1 / summass;
+        z1 = z1 / summass;
+    }
+    for (int k = 0; k < n; ++k) {
+        S->xa[a0 + k] = S->xa[a0 + k] - x1;
+        S->ya[a0 + k] = S->ya[a0 + k] - y1;
+        S->za[a0 + k] = S->za[a0 + k] - z1;
+    }
+}
+
+/* The intramolecular branch of molfit for a box with rotational groups of type ROT
+ * (molfit.py:124-267): molecules in index order; each one's atoms moved at random (movei :545,
+ * movea :556) and tested on its intramolecular change against ergold(1) (en_change_intra :763),
+ * the centre of mass restored on acceptance; then, when stepri > 0 and the molecule has groups,
+ * every group rotated (rotati :589) and the rotation tested on the intramolecular change plus
+ * the intermolecular change over the stored list (en_change :806).  Then the step adaptation
+ * :465-536 with nmovei and RT->ninter.  *ergold1 is molfit's work value ergold(1) (in/out);
+ * T->cosv (optional) records rotati's cosines in order.  fadds gains the rotations' accepted
+ * intermolecular changes, *faddbs the accepted intramolecular ones, over nmol. */
+int oracle_molfit_shake_rot(oracle_sys *S, oracle_store *E, oracle_mcpar *P, const oracle_rot *RT, float stepmi,
+                            oracle_ran1_state *R, float *fadds, float *faddbs, int32_t *nmovei, float *ergold1,
+                            oracle_trace *T) {
+    const int nmt = S->nmoltype, M = E->nnbrefmax;
+    const float rotstepmin = 1.0e-5f, rotstepmax = 1.0f;
+    for (int t = 0; t < 2 * nmt; ++t) {
+        nmovei[t] = 0;
+        RT->ninter[t] = 0;
+        P->nwhole[t] = 0;
+        P->nmovem[t] = 0;
+    }
+    if (T) T->ncos = 0;
+    const float temp = 1.0f / P->simt;
+    float fadd = 0.0f, faddb = 0.0f, eo1 = *ergold1;
+    float *ergnew = (float *)malloc(sizeof(float) * (size_t)(M > 0 ? M : 1));
+    float xr[4096], yr[4096], zr[4096];
+    for (int im = 0; im < S->nmol; ++im) {
+        const int nn = E->nergpairm[im];
+        const int32_t *rf = E->ergpairref + (size_t)im * M;
+        if (nn >= 1) eo1 = E->ergpair[rf[0] - 1];   /* make_neighbour_list_from_mols */
+        const int n = S->nato[im], a0 = S->naf[im], mt = S->mtype[im];
+        if (n > 4096) { free(ergnew); return 1; }
+        if (n > 1 && stepmi > 0.0f) {
+            float step = P->interntrans[mt];
+            if (stepmi > 0.0f && step == 0.0f) step = P->trstepmin;
+            P->interntrans[mt] = step;
+            for (int k = 0; k < n; ++k) { xr[k] = S->xa[a0 + k]; yr[k] = S->ya[a0 + k]; zr[k] = S->za[a0 + k]; }
+            nmovei[mt] += 1;
+            for (int k = 0; k < n; ++k) {                                    /* movei / movea */
+                const int a = a0 + k;
+                S->za[a] = S->za[a] + step * (2.0f * oracle_ran1(R) - 1.0f);
+                S->ya[a] = S->ya[a] + step * (2.0f * oracle_ran1(R) - 1.0f);
+                S->xa[a] = S->xa[a] + step * (2.0f * oracle_ran1(R) - 1.0f);
+            }
+            const float enew = oracle_en_mole_intra(S, RT->I, im);
+            const float fdiffb = enew - eo1;
+            const float ediff = fdiffb * temp;
+            const float etest = ediff <= 0.0f ? 10.0f : (ediff < 20.0f ? expf(-ediff) : 0.0f);
+            if (oracle_ran1(R) < etest) {
+                faddb = faddb + fdiffb;
+                if (nn >= 1) {                                 /* save_energies, save_erg_pairs */
+                    eo1 = enew;
+                    E->ergpair[rf[0] - 1] = eo1;
+                }
+                centreofmassi(S, RT->I, im);
+            } else {
+                nmovei[nmt + mt] += 1;
+                for (int k = 0; k < n; ++k) { S->xa[a0 + k] = xr[k]; S->ya[a0 + k] = yr[k]; S->za[a0 + k] = zr[k]; }
+            }
+        }
+        if (RT->stepri > 0.0f && P->ngrot[im] > 0) {
+            if (P->internrot[mt] == 0.0f) P->internrot[mt] = rotstepmin;
+            RT->ninter[mt]++;
+            for (int k = 0; k < n; ++k) { xr[k] = S->xa[a0 + k]; yr[k] = S->ya[a0 + k]; zr[k] = S->za[a0 + k]; }
+            for (int ig = RT->nrf[im]; ig <= RT->nrl[im]; ++ig) rotati(S, RT, ig, P->internrot[mt], R, T);
+            const float enew = oracle_en_mole_intra(S, RT->I, im);
+            const float fdiffb = enew - eo1;
+            const float fdiff = en_change(S, im, E, ergnew, NULL, NULL);
+            const float ediff = (fdiff + fdiffb) * temp;
+            const float etest = ediff <= 0.0f ? 10.0f : (ediff < 20.0f ? expf(-ediff) : 0.0f);
+            if (oracle_ran1(R) < etest) {
+                P->nstepreject[im] = 0;
+                fadd = fadd + fdiff;
+                faddb = faddb + fdiffb;
+                if (nn >= 1) {                                 /* save_energies, save_erg_pairs */
+                    eo1 = enew;
+                    E->ergpair[rf[0] - 1] = enew;
+                }
+                for (int inn = 1; inn < nn; ++inn) E->ergpair[rf[inn] - 1] = ergnew[inn];
+            } else {
+                P->nstepreject[im]++;
+                for (int k = 0; k < n; ++k) { S->xa[a0 + k] = xr[k]; S->ya[a0 + k] = yr[k]; S->za[a0 + k] = zr[k]; }
+                RT->ninter[nmt + mt]++;
+            }
+        } else if (P->ngrot[im] == 0) {
+            P->internrot[mt] = 0.0f;
+        }
+    }
+    free(ergnew);
+    if (P->ireset != 1) {
+        for (int t = 0; t < nmt; ++t) {
+            float rat;
+            if (nmovei[nmt + t] > 0) {
+                rat = P->rejrate * (float)nmovei[t] / (float)nmovei[nmt + t];
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = nmovei[t] > 0 ? 1.1f : 1.0f;
+            }
+            P->interntrans[t] = P->interntrans[t] * rat;
+            if (P->interntrans[t] > P->trstepmax) P->interntrans[t] = P->trstepmax;
+            if (P->interntrans[t] < P->trstepmin && P->interntrans[t] != 0.0f) P->interntrans[t] = P->trstepmin;
+            if (RT->ninter[nmt + t] > 0) {
+                rat = P->rejrate * (float)RT->ninter[t] / (float)RT->ninter[nmt + t];
+                if (rat > 1.1f) rat = 1.1f;
+                if (rat < 0.9f) rat = 0.9f;
+            } else {
+                rat = RT->ninter[t] > 0 ? 1.1f : 1.0f;
+            }
+            P->internrot[t] = P->internrot[t] * rat;
+            if (P->internrot[t] > rotstepmax) P->internrot[t] = rotstepmax;
+            if (P->internrot[t] < rotstepmin && P->internrot[t] != 0.0f) P->internrot[t] = rotstepmin;
+            P->wholerot[t] = P->wholerot[t] * 1.0f;
+            if (P->wholerot[t] > rotstepmax) P->wholerot[t] = rotstepmax;
+            if (P->wholerot[t] < rotstepmin && P->wholerot[t] != 0.0f) P->wholerot[t] = rotstepmin;
+            P->wholetrans[t] = P->wholetrans[t] * 1.0f;
+            if (P->wholetrans[t] > P->trstepmax) P->wholetrans[t] = P->trstepmax;
+            if (P->wholetrans[t] < P->trstepmin && P->wholetrans[t] != 0.0f) P->wholetrans[t] = P->trstepmin;
+        }
+    }
+    *fadds = *fadds + fadd / (float)S->nmol;
+    *faddbs = *faddbs + faddb / (float)S->nmol;
+    *ergold1 = eo1;
+    return 0;
+}
+
 /* ------------------------------------------------------------------ generate_ep */
 /* generate_ep epsr_standalone_rev3.py:5876-5995 with the Poisson basis already built
  * (calc_pwrexpr_grad, host): expgr [npt2][nterms] (row j-1 of the reference's flat expgr).

@@ -388,6 +388,49 @@ def molfit_shake(box, st, mc, m, stepmi, ran1, fadds, faddbs, ergold1=0.0):
     return f32(fa.value), f32(fb.value), nmovei, f32(eo.value), r.to_state()
 
 
+def molfit_shake_rot(box, st, mc, rot, stepmi, ran1, fadds, faddbs, ergold1=0.0):
+    """The intramolecular cycle of molfit for a box with ROT groups (molfit.py:124-267: random
+    atom moves, then the internal rotations tested with the intermolecular change; step
+    adaptation :465-536), C restatement.  ``rot`` as for molfit (model, nrf, nrl, axis, first,
+    last, atoms, stepri); ``mc`` holds ngrot and nstepreject besides the step arrays.  Mutates
+    the box coordinates, st["ergpair"] and ``mc``.  Returns (fadds, faddbs, nmovei (2*nmt,),
+    ninter (2*nmt,), ergold1, ran1 state, the cosines rotati drew)."""
+    h, ih = SysHandle(box), IntraHandle(box, rot["model"])
+    E = store_c(st)
+    nmt = box.nmoltype
+    par = McParC()
+    par.simt, par.rejrate = box.simt, f32(mc["rejrate"])
+    tmax, tmin = trsteps(box.natomr)
+    par.trstepmax, par.trstepmin = tmax, tmin
+    par.ireset = int(mc.get("ireset", 0))
+    for k in ("wholerot", "wholetrans", "internrot", "interntrans"):
+        mc[k] = np.ascontiguousarray(mc[k], dtype=f32)
+        setattr(par, k, ptr(mc[k]))
+    mc["nwhole"] = np.zeros(2 * nmt, np.int32)
+    mc["nmovem"] = np.zeros(2 * nmt, np.int32)
+    mc["nstepreject"] = np.ascontiguousarray(mc.get("nstepreject", np.zeros(box.nmol, np.int32)), np.int32)
+    mc["ngrot"] = np.ascontiguousarray(mc["ngrot"], np.int32)
+    par.nwhole, par.nmovem = ptr(mc["nwhole"]), ptr(mc["nmovem"])
+    par.nstepreject, par.ngrot = ptr(mc["nstepreject"]), ptr(mc["ngrot"])
+    arrs = {k: np.ascontiguousarray(rot[k], np.int32) for k in ("nrf", "nrl", "axis", "first", "last", "atoms")}
+    ninter = np.zeros(2 * nmt, np.int32)
+    rc = RotC()
+    rc.I = C.cast(C.pointer(ih.c), P)
+    for k, v in arrs.items():
+        setattr(rc, k, ptr(v))
+    rc.stepri, rc.rotcycle, rc.ninter, rc.faddbs = f32(rot["stepri"]), 1, ptr(ninter), None
+    cosv = np.zeros(int(arrs["first"].size) + 1, f32)
+    T = TraceC()
+    T.cosv = ptr(cosv)
+    nmovei = np.zeros(2 * nmt, np.int32)
+    r = Ran1C.of(ran1)
+    fa, fb, eo = C.c_float(f32(fadds)), C.c_float(f32(faddbs)), C.c_float(f32(ergold1))
+    if lib().oracle_molfit_shake_rot(C.byref(h.c), C.byref(E), C.byref(par), C.byref(rc), C.c_float(f32(stepmi)),
+                                     C.byref(r), C.byref(fa), C.byref(fb), ptr(nmovei), C.byref(eo), C.byref(T)):
+        raise ValueError("molfit_shake_rot: a molecule of more than 4096 atoms")
+    return f32(fa.value), f32(fb.value), nmovei, ninter, f32(eo.value), r.to_state(), cosv[: T.ncos].copy()
+
+
 # ----------------------------------------------------------------------------- atogen
 def atogen(box, ngrsamples, ran1, rminex, ycoh=None, sizefactor=1.0):
     ld = box.npt + 1

@@ -14,6 +14,12 @@ in order (rotati's and rotatm's), so the device and the oracle can reproduce the
 bit.  tests/golden/rot.npz receives the inputs, the groups (0-based), and after each cycle the
 coordinates, the store energies, the step arrays, ninter/nwhole/nmovem, fadds/faddbs and the
 ran1 state.
+
+The same box also runs two intramolecular cycles (nisum >= intra, molfit.py:124-267): every
+molecule's atoms moved at random and tested on its intramolecular energy, then its methyl
+groups rotated and tested on the intramolecular and intermolecular change, molecules in index
+order; stepmi > 0 and a starting interntrans as make_golden_shake.py.  tests/golden/shake_rot.npz
+receives the same fields plus nmovei per cycle.
 """
 
 from __future__ import annotations
@@ -36,7 +42,7 @@ f32 = np.float32
 REF = refstate.reference_root()
 
 
-def run(s, out, seed=21, cycles=2, internrot=0.08):
+def run(s, out, seed=21, cycles=2, internrot=0.08, shake=False, interntrans_A=0.05):
     from epsr26.common import clustercom, epsr16, molecom, molecom_mod, potential_par
     from epsr26.fortran import f32 as F, r4
     from epsr26.fortran.arrays import int_array
@@ -109,6 +115,14 @@ def run(s, out, seed=21, cycles=2, internrot=0.08):
     molecom.stepri = f32(1.0)
     ir0 = np.array([internrot] + [0.0] * (nmt - 1), f32)
     clustercom.internrot[1: nmt + 1] = ir0
+    if shake:
+        # the intramolecular moves: stepmi > 0, interntrans 0 for the first type (the trstepmin
+        # start is taken) and interntrans_A for the others
+        molecom.stepmi = f32(1.0)
+        it0 = np.array([0.0] + [interntrans_A / float(s.dmax)] * (nmt - 1), f32)
+        clustercom.interntrans[1: nmt + 1] = it0
+        out["interntrans_in"] = it0
+        out["stepmi"] = f32(molecom.stepmi)
     out.update(rot_axis=np.array(axis, np.int32), rot_first=np.array(first, np.int32),
                rot_last=np.array(last, np.int32), rot_atoms=np.array(atoms, np.int32), rot_nrf=nrf, rot_nrl=nrl,
                ngrot=ngrot, internrot_in=ir0,
@@ -154,7 +168,10 @@ def run(s, out, seed=21, cycles=2, internrot=0.08):
     try:
         for c in range(cycles):
             n0 = len(rec)
-            fadds, faddbs, nisum = molfit.molfit(fadds, faddbs, nisum, 100, 1, 0)
+            if shake:
+                fadds, faddbs, nisum = molfit.molfit(fadds, faddbs, 1, 1, 5, 0)
+            else:
+                fadds, faddbs, nisum = molfit.molfit(fadds, faddbs, nisum, 100, 1, 0)
             q = f"c{c}_"
             out[q + "cos"] = np.array(rec[n0:], f32)
             out[q + "fadds"], out[q + "faddbs"], out[q + "nisum"] = f32(fadds), f32(faddbs), np.int32(nisum)
@@ -163,11 +180,12 @@ def run(s, out, seed=21, cycles=2, internrot=0.08):
             out[q + "ergpair"] = refstate.store_state()["ergpair"]
             for k in ("interntrans", "internrot", "wholerot", "wholetrans"):
                 out[q + k] = np.array(getattr(clustercom, k)[1: nmt + 1], f32)
-            for k in ("ninter", "nwhole", "nmovem"):
+            for k in ("ninter", "nwhole", "nmovem", "nmovei"):
                 out[q + k] = np.array(getattr(clustercom, k)[1:3, 1: nmt + 1], np.int32)
+            out[q + "nstepreject"] = np.array(clustercom.nstepreject[1: s.nmol + 1], np.int32)
             for k, v in refstate.ran1_state().items():
                 out[q + "ran1_after_" + k] = v
-            print(f"cycle {c}: ninter {out[q + 'ninter'].tolist()} nwhole {out[q + 'nwhole'].tolist()} "
+            print(f"cycle {c}: ninter {out[q + 'ninter'].tolist()} nmovei {out[q + 'nmovei'].tolist()} "
                   f"faddbs {faddbs} cos {len(rec) - n0}", flush=True)
     finally:
         molfit.cosf = orig_cosf
@@ -177,8 +195,17 @@ def run(s, out, seed=21, cycles=2, internrot=0.08):
 if __name__ == "__main__":
     common, _ = refstate.load_reference(os.path.join(REF, "src"))
     out = {}
-    common.reset()
-    run(configs.c2_mixture(seed=5, ndmso=20, nwater=40), out)
-    path = os.path.join(HERE, "rot.npz")
-    np.savez_compressed(path, **out)
-    print("wrote", path)
+    which = sys.argv[1] if len(sys.argv) > 1 else "both"
+    if which in ("both", "rot"):
+        common.reset()
+        run(configs.c2_mixture(seed=5, ndmso=20, nwater=40), out)
+        path = os.path.join(HERE, "rot.npz")
+        np.savez_compressed(path, **out)
+        print("wrote", path)
+    if which in ("both", "shake_rot"):
+        out = {}
+        common.reset()
+        run(configs.c2_mixture(seed=5, ndmso=20, nwater=40), out, seed=23, shake=True)
+        path = os.path.join(HERE, "shake_rot.npz")
+        np.savez_compressed(path, **out)
+        print("wrote", path)
