@@ -47,6 +47,11 @@ struct McDev {
     const int32_t *ngrot, *rot_nrf, *rot_nrl, *rot_axis, *rot_first, *rot_last, *rot_atoms;
     int32_t *ninter;
     float *faddbs;
+    // the intramolecular cycle of a box with rotational groups (molfit.py:124-267), when shake:
+    // molecules in index order, atom moves (stepmi) then internal rotations, no whole-molecule move
+    int shake;
+    float stepmi;
+    int32_t *nmovei;   // [2*nmoltype] tries then rejections of the atom moves
 };
 
 // rotati molfit.py:589-660 after its angle: rotate the atoms of group ig about the axis from
@@ -112,6 +117,7 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
             D.nwhole[k] = 0;
             D.nmovem[k] = 0;
             if (D.ninter) D.ninter[k] = 0;
+            if (D.nmovei) D.nmovei[k] = 0;
         }
     }
     const float temp = __fdiv_rn(1.0f, D.simt);
@@ -164,7 +170,7 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
     };
     for (int v = 0; v < D.nmol; ++v) {
         if (tid == 0) {
-            const int im = D.visit[v];
+            const int im = D.shake ? v : D.visit[v];
             const int n = D.nato[im];
             sh_bad = n > MC_MAXAT;
         }
@@ -173,15 +179,83 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
             if (tid == 0 && D.status) D.status[0] = 1;
             return;
         }
-        // ---- internal rotations of the molecule's rotational groups (molfit.py:295-360)
+        // ---- internal rotations of the molecule's rotational groups (molfit.py:295-360), in
+        // the intramolecular cycle after the molecule's atom moves (:141-267)
         if (tid == 0) {
-            const int im = D.visit[v];
+            const int im = D.shake ? v : D.visit[v];
             const int n = D.nato[im];
             const int mt = D.mtype[im];
             const size_t row = (size_t)im * D.M;
             if (D.nergpairm[im] >= 1) eold0 = D.ergpair[D.ergpairref[row] - 1];   // make_neighbour_list_from_mols
+            if (D.shake && n > 1 && D.stepmi > 0.0f) {
+                // movei/movea (:545-567) on the offsets, en_change_intra against ergold(1), the
+                // Metropolis test; on acceptance the store's first slot (save_energies,
+                // save_erg_pairs) and the centre of mass put back (centreofmassi)
+                float step = D.interntrans[mt];
+                if (step == 0.0f) step = D.trstepmin;
+                D.interntrans[mt] = step;
+                const int a0 = D.naf[im];
+                for (int k = 0; k < n; ++k) {
+                    sx[k] = D.xa[a0 + k];
+                    sy[k] = D.ya[a0 + k];
+                    sz[k] = D.za[a0 + k];
+                }
+                D.nmovei[mt]++;
+                for (int k = 0; k < n; ++k) {
+                    const int a = a0 + k;
+                    D.za[a] = __fadd_rn(D.za[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                    D.ya[a] = __fadd_rn(D.ya[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                    D.xa[a] = __fadd_rn(D.xa[a], __fmul_rn(step, __fsub_rn(__fmul_rn(2.0f, ran1_next(R)), 1.0f)));
+                }
+                const float enew = en_mole_intra_d(D.I, im, D.xa, D.ya, D.za);
+                const float fdiffb = __fsub_rn(enew, eold0);
+                const float ediff = __fmul_rn(fdiffb, temp);
+                float etest;
+                if (ediff <= 0.0f) etest = 10.0f;
+                else if (ediff < 20.0f) etest = exp_r(-ediff);
+                else etest = 0.0f;
+                if (ran1_next(R) < etest) {
+                    faddb = __fadd_rn(faddb, fdiffb);
+                    if (D.nergpairm[im] >= 1) {
+                        eold0 = enew;
+                        D.ergpair[D.ergpairref[row] - 1] = enew;
+                    }
+                    float x1 = 0.0f, y1 = 0.0f, z1 = 0.0f, summass = 0.0f;
+                    for (int k = 0; k < n; ++k) {
+                        const int a = a0 + k;
+                        if (D.I.qtype[a] == 0) {
+                            const float am = D.I.amassa[D.I.itype[a]];
+                            x1 = __fadd_rn(x1, __fmul_rn(D.xa[a], am));
+                            y1 = __fadd_rn(y1, __fmul_rn(D.ya[a], am));
+                            z1 = __fadd_rn(z1, __fmul_rn(D.za[a], am));
+                            summass = __fadd_rn(summass, am);
+                        }
+                    }
+                    if (summass > 0.0f) {
+                        x1 = __fdiv_rn(x1, summass);
+                        y1 = __fdiv_rn(y1, summass);
+                        z1 = __fdiv_rn(z1, summass);
+                    }
+                    const float cx = D.xadd[im], cy = D.yadd[im], cz = D.zadd[im];
+                    for (int k = 0; k < n; ++k) {
+                        const int a = a0 + k;
+                        D.xa[a] = __fsub_rn(D.xa[a], x1);
+                        D.ya[a] = __fsub_rn(D.ya[a], y1);
+                        D.za[a] = __fsub_rn(D.za[a], z1);
+                        D.pos[a] = make_float4(__fadd_rn(D.xa[a], cx), __fadd_rn(D.ya[a], cy), __fadd_rn(D.za[a], cz),
+                                               D.pos[a].w);
+                    }
+                } else {
+                    D.nmovei[nmt + mt]++;
+                    for (int k = 0; k < n; ++k) {
+                        D.xa[a0 + k] = sx[k];
+                        D.ya[a0 + k] = sy[k];
+                        D.za[a0 + k] = sz[k];
+                    }
+                }
+            }
             const int ng = D.ngrot ? D.ngrot[im] : 0;
-            sh_rot = D.has_rot && D.stepri > 0.0f && ng > 0 && D.rotcycle;
+            sh_rot = D.has_rot && D.stepri > 0.0f && ng > 0 && (D.rotcycle || D.shake);
             sh_im = im;
             sh_n = n;
             if (sh_rot) {
@@ -260,6 +334,7 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
             }
             __syncthreads();
         }
+        if (D.shake) continue;   // the intramolecular cycle moves no molecule whole (uniform branch)
         // ---- whole-molecule rotation and translation (molfit.py:362-448)
         if (tid == 0) {
             const int im = sh_im;
@@ -376,10 +451,19 @@ __global__ void __launch_bounds__(MC_THREADS) molfit_seq_kernel(McDev D) {
         __syncthreads();
     }
     if (tid == 0) {
-        // step adaptation (molfit.py:465-536); nmovei is 0 in this branch
+        // step adaptation (molfit.py:465-536); nmovei counts only in the intramolecular cycle
         if (D.ireset != 1) {
             for (int t = 0; t < nmt; ++t) {
-                float it = __fmul_rn(D.interntrans[t], 1.0f);
+                float rat0;
+                const int nm1 = D.nmovei ? D.nmovei[t] : 0, nm2 = D.nmovei ? D.nmovei[nmt + t] : 0;
+                if (nm2 > 0) {
+                    rat0 = __fdiv_rn(__fmul_rn(D.rejrate, (float)nm1), (float)nm2);
+                    if (rat0 > 1.1f) rat0 = 1.1f;
+                    if (rat0 < 0.9f) rat0 = 0.9f;
+                } else {
+                    rat0 = nm1 > 0 ? 1.1f : 1.0f;
+                }
+                float it = __fmul_rn(D.interntrans[t], rat0);
                 if (it > D.trstepmax) it = D.trstepmax;
                 if (it < D.trstepmin && it != 0.0f) it = D.trstepmin;
                 D.interntrans[t] = it;
@@ -539,8 +623,34 @@ static int check_box(const epsr_box_t *b, const char *who) {
 }
 
 namespace epsr {
+// The intramolecular cycle's settings when the sequential kernel runs it (shake mode).
+struct ShakeRot {
+    const epsr_intra_t *intra;
+    float stepmi;
+    int32_t *nmovei;
+    float *faddbs;
+};
+
+static int seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
+                      void *scratch, int64_t scratch_bytes, cudaStream_t s, const int32_t *run_if, const ShakeRot *sr);
+
 int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
                       void *scratch, int64_t scratch_bytes, cudaStream_t s, const int32_t *run_if) {
+    return seq_launch(box, cells, store, mc, scratch, scratch_bytes, s, run_if, nullptr);
+}
+
+// molfit's intramolecular cycle (nisum >= intra) for a box whose molecules have rotational
+// groups, on the sequential kernel: the rotations test the intermolecular change, which chains
+// every molecule to the ones before it.  mc must carry the groups (rot_*), ninter and stepri.
+int molfit_shake_rot_launch(const epsr_box_t *box, epsr_store_t *store, epsr_mc_t *mc, const epsr_intra_t *in,
+                            float stepmi, int32_t *nmovei, float *faddbs, void *scratch, int64_t scratch_bytes,
+                            cudaStream_t s) {
+    const ShakeRot sr{in, stepmi, nmovei, faddbs};
+    return seq_launch(box, nullptr, store, mc, scratch, scratch_bytes, s, nullptr, &sr);
+}
+
+static int seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
+                      void *scratch, int64_t scratch_bytes, cudaStream_t s, const int32_t *run_if, const ShakeRot *sr) {
     McDev D = make_mcdev(box, cells, store);
     D.simt = mc->simt;
     D.rejrate = mc->rejrate;
@@ -565,8 +675,8 @@ int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_sto
     D.status = mc->status;
     D.run_if = run_if;
     D.faddbs = mc->faddbs;
-    if (mc->intra) {
-        const epsr_intra_t *in = (const epsr_intra_t *)mc->intra;
+    if (sr || mc->intra) {
+        const epsr_intra_t *in = sr ? sr->intra : (const epsr_intra_t *)mc->intra;
         D.I = make_intradev(box, in);
         D.ngrot = in->ngrot;
         D.has_rot = mc->rot_nrf && mc->rot_nrl && mc->rot_axis && mc->rot_first && mc->rot_last && mc->rot_atoms;
@@ -583,6 +693,18 @@ int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_sto
             epsr_set_error("epsr_molfit: internal rotations need the ninter counters");
             return EPSR_ERR_ARG;
         }
+    }
+    if (sr) {
+        if (!D.has_rot || !sr->nmovei) {
+            epsr_set_error("epsr_molfit_shake: a box with rotational groups needs the groups (rot_*), ninter and nmovei");
+            return EPSR_ERR_ARG;
+        }
+        D.shake = 1;
+        D.strict = 1;
+        D.stepmi = sr->stepmi;
+        D.nmovei = sr->nmovei;
+        D.faddbs = sr->faddbs;
+        D.visit = nullptr;
     }
     const size_t need = sizeof(float) * 2 * (size_t)(D.M > 0 ? D.M : 1);
     size_t shm = 0;

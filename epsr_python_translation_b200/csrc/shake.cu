@@ -2,9 +2,9 @@
 // nisum >= intra): every molecule's atoms moved at random (movei :545, movea :556), the change of
 // its intramolecular energy (en_change_intra :763 -> en_mole_intra :1327 -> en_atom_intra :923),
 // the Metropolis test and, on acceptance, the centre of mass put back at the molecule centre
-// (centreofmassi ato_manipulation_rev4.py:442); then the step adaptation (:465-536).  The
-// internal rotations of rotational groups (:175-245) are not part of this path: a box with
-// rotational groups is refused.
+// (centreofmassi ato_manipulation_rev4.py:442); then the step adaptation (:465-536).  A box
+// with rotational groups also rotates each molecule's groups after its atom moves (:175-245),
+// tested with the intermolecular change; that cycle runs on the sequential kernel of mc.cu.
 //
 // Every moved molecule draws three values per atom and one for its test, so its place in the
 // ran1 stream is known before the cycle starts.  The stream is generated once; every
@@ -393,6 +393,12 @@ size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 }  // namespace epsr
 
+namespace epsr {
+int molfit_shake_rot_launch(const epsr_box_t *box, epsr_store_t *store, epsr_mc_t *mc, const epsr_intra_t *in,
+                            float stepmi, int32_t *nmovei, float *faddbs, void *scratch, int64_t scratch_bytes,
+                            cudaStream_t s);
+}
+
 using namespace epsr;
 
 static int intra_check(const epsr_box_t *box, const epsr_intra_t *in, const char *who) {
@@ -515,9 +521,18 @@ extern "C" int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, eps
     const long long total = tot2[0];
     const int32_t status = (int32_t)(tot2[1] & 0xffffffff);
     if (status) {
-        epsr_set_error("epsr_molfit_shake: molecules with rotational groups (internal rotations and dihedral terms "
-                       "are outside this path)");
-        return EPSR_ERR_UNSUPPORTED;
+        // molecules with rotational groups: after each molecule's atom moves its groups are
+        // rotated and tested with the intermolecular change (molfit.py:175-245), which chains the
+        // molecules in index order -- the sequential kernel runs the whole cycle
+        if (!mc->rot_nrf || !mc->rot_nrl || !mc->rot_axis || !mc->rot_first || !mc->rot_last || !mc->rot_atoms ||
+            !mc->ninter || !mc->nstepreject) {
+            epsr_set_error("epsr_molfit_shake: molecules with rotational groups need the groups (rot_*), ninter and "
+                           "nstepreject in the mc state");
+            return EPSR_ERR_UNSUPPORTED;
+        }
+        rc = molfit_shake_rot_launch(box, store, mc, in, stepmi, nmovei, faddbs, scratch, scratch_bytes, s);
+        if (rc) return rc;
+        return epsr_box_positions(box, stream);
     }
     if (total > 3LL * box->natom + D.nmol) {
         epsr_set_error("epsr_molfit_shake: %lld draws exceed the stream buffer", total);

@@ -275,6 +275,16 @@ class DeviceBox:
         m.stepri = float(f32(stepri))
         m.ninter, m.faddbs = _ptr(self.m_ninter), _ptr(self.m_faddbs)
 
+    def set_cos_override(self, cos_override=None):
+        """Cosines the next MC cycle uses in draw order instead of its own (a test hook that
+        proves the chain bit for bit against the reference's cosf values); None: its own."""
+        self._cos = None
+        if cos_override is not None:
+            self._cos = self._t(cos_override, f32)
+            self.cmc.cos_override = _ptr(self._cos)
+        else:
+            self.cmc.cos_override = None
+
     def molfit(self, strict=True, cos_override=None, rotcycle=True):
         b = self.host
         if int(np.max(b.nato)) > 64:
@@ -282,12 +292,7 @@ class DeviceBox:
         m = self.cmc
         m.strict = 1 if strict else 0
         m.rotcycle = 1 if rotcycle else 0
-        self._cos = None
-        if cos_override is not None:
-            self._cos = self._t(cos_override, f32)
-            m.cos_override = _ptr(self._cos)
-        else:
-            m.cos_override = None
+        self.set_cos_override(cos_override)
         nb = self.lib.epsr_molfit_scratch_bytes(b.nmol, b.natom, self.nnbrefmax)
         scr = self.scratch("molfit", nb)
         check(self.lib.epsr_molfit(C.byref(self.cbox), C.byref(self.cells), C.byref(self.store), C.byref(m), _ptr(scr),

@@ -28,10 +28,11 @@ the wrapper compares the COMMON arrays it depends on with what it last wrote or 
 (coordinates, potential tables, stored pair energies) and uploads what the host changed;
 the ran1 state is always uploaded.  On return it writes everything the routine changes
 back into the COMMON arrays in place (same array objects, so aliases held by other
-routines stay valid).  A call that needs a feature outside the pair path (shake or
-internal-rotation cycles, tethering, three-body terms, coordination constraints,
-container forces, coarse graining, molecules of more than 64 atoms) runs the reference's
-own routine on the host instead; the next device call picks up whatever it changed.
+routines stay valid).  A call that needs a feature outside the pair path (rotational
+groups with dihedral angles or of a type other than ROT, tethering, three-body terms,
+coordination constraints, container forces, coarse graining, molecules of more than 64 atoms)
+runs the reference's own routine on the host instead; the next device call picks up whatever
+it changed.
 
 The cell list must come from the installed ``initialise_cellneighbourlist`` (the
 reference loop rebuilds it every iteration, epsr_standalone_rev3.py:1265); a cell list
@@ -420,8 +421,8 @@ class PairPath:
                           refine_intra_fac=f32(getattr(mc, "refine_intra_fac", 0.0)), ngrot=ngrot)
 
     def molfit(self, fadds, faddbs, nisum, intra, rotfreq, ireset):
-        """molfit.py:52-541: the whole-molecule branch and, for boxes without rotational groups,
-        the intramolecular branch (:124-174) on the device; returns (fadds, faddbs, nisum)."""
+        """molfit.py:52-541: the whole-molecule branch and the intramolecular branch (:124-267),
+        internal rotations of ROT groups included, on the device; returns (fadds, faddbs, nisum)."""
         c = self.c
         mc, cc = c.molecom, c.clustercom
         nmol = int(cc.nmol)
@@ -477,12 +478,15 @@ class PairPath:
         return out["fadds"], faddbs, nisum + 1
 
     def _molfit_intra(self, fadds, faddbs, ireset):
-        """The intramolecular cycle of molfit (:119-174, :246-247, step adaptation :465-536) on
-        the device; None when the box has rotational groups (the host runs the cycle)."""
+        """The intramolecular cycle of molfit (:119-267, step adaptation :465-536) on the
+        device, the internal rotations of ROT groups included; None when a group is not of type
+        ROT or has dihedral angles, or the COMMON blocks carry no bond lists (the host runs the
+        cycle)."""
         c = self.c
         mc, cc = c.molecom, c.clustercom
         nmol = int(cc.nmol)
-        if bool(np.any(np.asarray(cc.ngrot[1:nmol + 1]) > 0)) or getattr(mc, "nbond", None) is None:
+        groups = self._rot_groups()
+        if groups is None or getattr(mc, "nbond", None) is None:
             return None
         b = self._sync_in()
         self._check_cells()
@@ -493,7 +497,7 @@ class PairPath:
             getattr(cc, name)[1:3, 1:nmt + 1] = 0
         mc.tempang = mc.tempangwt
         mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
-        model = self._intra_model(b)
+        model = self._intra_model(b, allow_rot=bool(groups))
         tmax, tmin = trsteps(b.natomr)
         d = self.d
         d.mc_setup(rejrate=f32(c.epsr16.rejrate), stepr=f32(mc.stepr), stepm=f32(mc.stepm),
@@ -504,13 +508,23 @@ class PairPath:
                    trstepmax=tmax, trstepmin=tmin, ireset=int(ireset), fadds=f32(fadds))
         d.m_ran1 = self._ran1_in()
         d.cmc.ran1 = C.c_void_p(d.m_ran1.data_ptr())
+        if groups:
+            # each molecule's groups rotated after its atom moves (:175-245)
+            d.set_rotations(model, *groups, stepri=f32(mc.stepri), faddbs=f32(faddbs))
+        cos = self.cos_override
+        self.cos_override = None
+        d.set_cos_override(cos)
         fb = torch.tensor([float(f32(faddbs))], dtype=torch.float32, device=d.dev)
         nmovei = model.molfit_shake(f32(mc.stepmi), fb).cpu().numpy()
+        d.check_status()
         out = d.download_mc()
         self._ran1_out(d.m_ran1)
         cc.wholerot[1:nmt + 1], cc.wholetrans[1:nmt + 1] = out["wholerot"], out["wholetrans"]
         cc.internrot[1:nmt + 1], cc.interntrans[1:nmt + 1] = out["internrot"], out["interntrans"]
         cc.nmovei[1:3, 1:nmt + 1] = nmovei.reshape(2, nmt)
+        if groups:
+            cc.ninter[1:3, 1:nmt + 1] = d.m_ninter.cpu().numpy().reshape(2, nmt)
+            cc.nstepreject[1:nmol + 1] = out["nstepreject"]
         self._coords_out()
         self._store_out(values_only=True)
         return out["fadds"], f32(fb.cpu().numpy()[0]), 1

@@ -237,8 +237,14 @@ int epsr_en_mole_intra(const epsr_box_t *box, const epsr_intra_t *intra, float *
  * molecule types without rotational groups), nwhole/nmovem zeroed, fadds, ran1.  nmovei
  * [2*nmoltype] device out (tries, then rejections); faddbs [1] device in/out.  A molecule
  * with an empty pair list before any loaded one compares against 0 (the reference uses
- * whatever its work array last held).  Returns EPSR_ERR_UNSUPPORTED, before any change, for
- * molecules with rotational groups.  Bit-identical with the reference's exp values.
+ * whatever its work array last held).  Molecules with rotational groups of type ROT
+ * (molfit.py:124-267): in index order, each molecule's atom moves and then, when mc->stepri > 0,
+ * its groups rotated (rotati :589, one ran1 value each, mc->cos_override consumed in order when
+ * set) and tested on the intramolecular change against ergold(1) plus the intermolecular change
+ * over its stored list (en_change :806, summed in list order); mc must then carry the groups
+ * (rot_*), ninter (counted and used for internrot's adaptation) and nstepreject, else
+ * EPSR_ERR_UNSUPPORTED before any change; fadds gains the accepted intermolecular changes.
+ * Bit-identical with the reference's exp values (and, for rotations, its cos values).
  * Synchronous (reads the draw count); scratch from epsr_molfit_shake_scratch_bytes. */
 int64_t epsr_molfit_shake_scratch_bytes(int32_t nmol, int32_t natom);
 int epsr_molfit_shake(const epsr_box_t *box, epsr_store_t *store, epsr_mc_t *mc, const epsr_intra_t *intra,

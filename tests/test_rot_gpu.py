@@ -1,7 +1,7 @@
 """Internal rotations of rotational groups in the device's whole-molecule cycle (molfit.py:
-295-360, rotati :589, en_change_intra :763) against the reference run on a 20 DMSO + 40 water
-box whose methyl groups are ROT groups (tests/golden/rot.npz), with the reference's cosines
-injected: coordinates, stored energies (including the first-slot rule after a rejected rotation
+295-360, rotati :589, en_change_intra :763) and in its intramolecular cycle (:124-267) against
+the reference run on a 20 DMSO + 40 water box whose methyl groups are ROT groups
+(tests/golden/rot.npz, shake_rot.npz), with the reference's cosines injected: coordinates, stored energies (including the first-slot rule after a rejected rotation
 followed by an accepted move), step sizes, ninter/nwhole/nmovem, fadds/faddbs and the ran1
 state bit for bit over two cycles."""
 
@@ -73,11 +73,22 @@ def test_rotation_dropin_matches_reference():
     (molecom_mod labaxi/rotf/rotl/labrot, clustercom ngrot/nrf/nrl, all of type ROT) and
     intramolecular model: the whole-molecule cycles with internal rotations run on the device
     and leave the COMMON state equal to the reference's; no host routine ran."""
+    _rotation_dropin("rot.npz", shake=False)
+
+
+def test_shake_rotation_dropin_matches_reference():
+    """As above for the intramolecular cycles (nisum >= intra) of the same box: atom moves and
+    internal rotations on the device, the COMMON state (nmovei, ninter, nstepreject and
+    interntrans included) equal to the reference's; no host routine ran."""
+    _rotation_dropin("shake_rot.npz", shake=True)
+
+
+def _rotation_dropin(name, shake):
     from types import SimpleNamespace as NS
 
     from epsr_python_translation_b200 import dropin
     from tests import fake_common
-    z = np.load(__import__("tests.goldens", fromlist=["GOLDEN"]).GOLDEN + "/rot.npz")
+    z = np.load(__import__("tests.goldens", fromlist=["GOLDEN"]).GOLDEN + "/" + name)
     p = _Aliased(z)
     calls = []
     mods = fake_common.routine_modules(p, calls)
@@ -104,6 +115,9 @@ def test_rotation_dropin_matches_reference():
     pp.xav, pp.xav1 = fa(mpz, npairs), fa(mpz, npairs)
     pp.xav[: npt + 1, 1:], pp.xav1[: npt + 1, 1:] = z["xav"].T, z["xav1"].T
     cc.internrot[1:] = z["internrot_in"]
+    if shake:
+        mc.stepmi = f32(z["stepmi"])
+        cc.interntrans[1:] = z["interntrans_in"]
     # the rotational groups, 1-based as the reference holds them
     ng = z["rot_first"].size
     cc.ngrot[1:] = z["ngrot"]
@@ -131,7 +145,10 @@ def test_rotation_dropin_matches_reference():
     for cyc in range(int(z["cycles"])):
         q = f"c{cyc}_"
         path.cos_override = z[q + "cos"]
-        fadds, faddbs, nisum = mods["molfit"].molfit(fadds, faddbs, nisum, 100, 1, 0)
+        if shake:
+            fadds, faddbs, nisum = mods["molfit"].molfit(fadds, faddbs, 1, 1, 5, 0)
+        else:
+            fadds, faddbs, nisum = mods["molfit"].molfit(fadds, faddbs, nisum, 100, 1, 0)
         assert nisum == int(z[q + "nisum"])
         assert_bits_equal(np.array([fadds, faddbs], f32), np.array([z[q + "fadds"], z[q + "faddbs"]], f32),
                           q + "fadds, faddbs")
@@ -139,10 +156,58 @@ def test_rotation_dropin_matches_reference():
                        ("zadd", cc.zadd)):
             assert_bits_equal(arr[1:], z[q + k], q + k)
         assert_bits_equal(erd.ergpair[1:erd.nergpair + 1], z[q + "ergpair"], q + "ergpair")
-        for k in ("internrot", "wholerot", "wholetrans"):
+        for k in ("internrot", "wholerot", "wholetrans") + (("interntrans",) if shake else ()):
             assert_bits_equal(getattr(cc, k)[1:], z[q + k], q + k)
-        for k in ("ninter", "nwhole", "nmovem"):
+        for k in ("ninter", "nwhole", "nmovem") + (("nmovei",) if shake else ()):
             assert np.array_equal(getattr(cc, k)[1:3, 1:nmt + 1], z[q + k]), k
+        if shake:
+            assert np.array_equal(cc.nstepreject[1:], z[q + "nstepreject"])
         assert (r.idum, r.iy, r.mcall) == (int(z[q + "ran1_after_idum"]), int(z[q + "ran1_after_iy"]),
                                            int(z[q + "ran1_after_mcall"]))
     assert not [k for k in calls if k.startswith("host:")], calls
+
+
+def test_shake_rotation_cycles_device_match_reference():
+    """molfit's intramolecular cycle on a box with ROT groups (molfit.py:124-267: each
+    molecule's atom moves, then its methyl groups rotated and tested with the intermolecular
+    change, molecules in index order) through epsr_molfit_shake with the reference's cosines
+    injected: coordinates, stored energies, step sizes, nmovei/ninter, nstepreject, fadds/faddbs
+    and the ran1 state equal the reference's bit for bit over two cycles
+    (tests/golden/shake_rot.npz)."""
+    import torch
+
+    from epsr_python_translation_b200.device import DeviceBox
+    from epsr_python_translation_b200.intra import IntraModel
+    from tests.test_rot_oracle import load_shake
+    z, box, st, mc, rot = load_shake()
+    d = DeviceBox(box)
+    d.cell_list(int(z["in_nmolcell"]), f32(z["in_sepmax"]))
+    d.fmolec1(z["eintra"], strict=True)
+    assert_bits_equal(d.download_store()["ergpair"], st["ergpair"], "store before the cycles")
+    tmax, tmin = trsteps(box.natomr)
+    d.mc_setup(rejrate=f32(0.75), stepr=f32(z["in_stepr"]), stepm=f32(z["in_stepm"]), wholerot=z["wholerot_in"],
+               wholetrans=z["wholetrans_in"], internrot=z["internrot_in"], interntrans=z["interntrans_in"],
+               ran1=Ran1State.from_golden(z, "ran1_before_"), trstepmax=tmax, trstepmin=tmin, fadds=f32(z["fadds_in"]))
+    im = IntraModel(d, **dict(rot["model"]))
+    d.set_rotations(im, z["rot_nrf"], z["rot_nrl"], z["rot_axis"], z["rot_first"], z["rot_last"], z["rot_atoms"],
+                    stepri=1.0)
+    fb = torch.tensor([float(z["faddbs_in"])], dtype=torch.float32, device=d.dev)
+    for c in range(int(z["cycles"])):
+        q = f"c{c}_"
+        d.set_cos_override(z[q + "cos"])
+        nmovei = im.molfit_shake(f32(z["stepmi"]), fb).cpu().numpy()
+        d.check_status()
+        m = d.download_mc()
+        co = d.download_coords()
+        for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+            assert_bits_equal(co[k], z[q + k], f"cycle {c} {k}")
+        assert_bits_equal(d.download_store()["ergpair"], z[q + "ergpair"], f"cycle {c} ergpair")
+        for k in ("interntrans", "internrot", "wholerot", "wholetrans"):
+            assert_bits_equal(m[k], z[q + k], f"cycle {c} {k}")
+        assert np.array_equal(nmovei, z[q + "nmovei"].reshape(-1))
+        assert np.array_equal(d.m_ninter.cpu().numpy(), z[q + "ninter"].reshape(-1))
+        assert np.array_equal(m["nstepreject"], z[q + "nstepreject"])
+        assert_bits_equal(np.array([m["fadds"], fb.cpu().numpy()[0]], f32),
+                          np.array([z[q + "fadds"], z[q + "faddbs"]], f32), f"cycle {c} fadds, faddbs")
+        assert m["ran1"].idum == int(z[q + "ran1_after_idum"])
+        assert np.array_equal(m["ran1"].iv, z[q + "ran1_after_iv"])
