@@ -879,11 +879,86 @@ typedef struct {
     float stepcl, sizefactor, tempb, tempang, simt;
     int32_t refine_intra;
     float refine_intra_fac;
+    /* dihedral angles of the rotational groups (molecom labrotdih / ndihedralang / dihedralang):
+     * their energy for DIH groups (en_mole_dihedral molfit.py:1353), and their atom pairs left
+     * out of the reference potential (en_atom_intra :999-1020).  grp_nrf NULL: no groups. */
+    int32_t ndih;
+    const int32_t *grp_nrf, *grp_nrl;   /* [nmol] 0-based group range (nrl < nrf: none) */
+    const int32_t *grp_axis;            /* [ngroups*2] the two base atoms (labaxi) */
+    const int32_t *grp_dih0;            /* [ngroups+1] each group's range in dih_* */
+    const int32_t *grp_isdih;           /* [ngroups] 1 for a group of type DIH */
+    const int32_t *dih_atoms;           /* [ndih*2] io1 (by base atom 1), io2 (by base atom 2) */
+    const float *dih_cos, *dih_sin;     /* [ndih] cosf, sinf of the dihedral angle */
+    float tempdih;                      /* molecom.tempdih */
 } oracle_intra;
 
-/* en_atom_intra molfit.py:923-1045 (molecules without rotational groups: no dihedral pairs) */
-static float en_atom_intra(const oracle_sys *S, const oracle_intra *I, int ia, int ja, float x1, float y1, float z1,
-                           float x2, float y2, float z2) {
+/* en_atom_intra :999-1016: is (ia, ja) one of the dihedral atom pairs of molecule im's groups? */
+static int dihedral_pair(const oracle_intra *I, int im, int ia, int ja) {
+    if (!I->grp_nrf) return 0;
+    for (int ir = I->grp_nrf[im]; ir <= I->grp_nrl[im]; ++ir)
+        for (int kd = I->grp_dih0[ir]; kd < I->grp_dih0[ir + 1]; ++kd) {
+            const int io1 = I->dih_atoms[2 * kd], io2 = I->dih_atoms[2 * kd + 1];
+            if ((io1 == ia && io2 == ja) || (io1 == ja && io2 == ia)) return 1;
+        }
+    return 0;
+}
+
+/* en_dihedral molfit.py:1487-1524 with vecpro / scapro auxiliary_routines.py:231-244: the
+ * dihedral angle's cosine and sine already taken (cosf, sinf of dihedralang) */
+static float en_dihedral(const float *co1, const float *co2, const float *cd, float cosdih, float sindih) {
+    float cv1[3], cv2[3], cpar[3];
+    cv1[0] = co1[1] * cd[2] - co1[2] * cd[1];
+    cv1[1] = co1[2] * cd[0] - co1[0] * cd[2];
+    cv1[2] = co1[0] * cd[1] - co1[1] * cd[0];
+    cv2[0] = co2[1] * cd[2] - co2[2] * cd[1];
+    cv2[1] = co2[2] * cd[0] - co2[0] * cd[2];
+    cv2[2] = co2[0] * cd[1] - co2[1] * cd[0];
+    float dmag = sqrtf(cv1[0] * cv1[0] + cv1[1] * cv1[1] + cv1[2] * cv1[2]);
+    cv1[0] = cv1[0] / dmag;
+    cv1[1] = cv1[1] / dmag;
+    cv1[2] = cv1[2] / dmag;
+    dmag = sqrtf(cv2[0] * cv2[0] + cv2[1] * cv2[1] + cv2[2] * cv2[2]);
+    cv2[0] = cv2[0] / dmag;
+    cv2[1] = cv2[1] / dmag;
+    cv2[2] = cv2[2] / dmag;
+    float cosphi = cv1[0] * cv2[0] + cv1[1] * cv2[1] + cv1[2] * cv2[2];
+    if (cosphi > 1.0f) cosphi = 1.0f;
+    if (cosphi < -1.0f) cosphi = -1.0f;
+    cpar[0] = cv1[1] * cv2[2] - cv1[2] * cv2[1];
+    cpar[1] = cv1[2] * cv2[0] - cv1[0] * cv2[2];
+    cpar[2] = cv1[0] * cv2[1] - cv1[1] * cv2[0];
+    const float sinphi = cpar[0] * cd[0] + cpar[1] * cd[1] + cpar[2] * cd[2];
+    const float difc = cosdih - cosphi, difs = sindih - sinphi;
+    return difc * difc + difs * difs;
+}
+
+/* en_mole_dihedral molfit.py:1353-1410: the DIH groups of molecule im at its offsets */
+static float en_mole_dihedral(const oracle_sys *S, const oracle_intra *I, int im) {
+    float e = 0.0f;
+    if (!I->grp_nrf) return e;
+    for (int ir = I->grp_nrf[im]; ir <= I->grp_nrl[im]; ++ir) {
+        if (!I->grp_isdih[ir]) continue;
+        const int ia1 = I->grp_axis[2 * ir], ia2 = I->grp_axis[2 * ir + 1];
+        const float x1 = S->xa[ia1], y1 = S->ya[ia1], z1 = S->za[ia1];
+        const float x2 = S->xa[ia2], y2 = S->ya[ia2], z2 = S->za[ia2];
+        float cd[3] = {x2 - x1, y2 - y1, z2 - z1};
+        const float dmag = sqrtf(cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
+        cd[0] = cd[0] / dmag;
+        cd[1] = cd[1] / dmag;
+        cd[2] = cd[2] / dmag;
+        for (int kd = I->grp_dih0[ir]; kd < I->grp_dih0[ir + 1]; ++kd) {
+            const int io1 = I->dih_atoms[2 * kd], io2 = I->dih_atoms[2 * kd + 1];
+            const float co1[3] = {S->xa[io1] - x1, S->ya[io1] - y1, S->za[io1] - z1};
+            const float co2[3] = {S->xa[io2] - x2, S->ya[io2] - y2, S->za[io2] - z2};
+            e = e + en_dihedral(co1, co2, cd, I->dih_cos[kd], I->dih_sin[kd]);
+        }
+    }
+    return e;
+}
+
+/* en_atom_intra molfit.py:923-1045 */
+static float en_atom_intra(const oracle_sys *S, const oracle_intra *I, int im, int ia, int ja, float x1, float y1,
+                           float z1, float x2, float y2, float z2) {
     if (ja == I->imageatom[ia]) return 0.0f;
     const int icref = S->npairref[S->itype[ia] * S->ntype + S->itype[ja]];
     const int notq = I->qtype[ia] == 0 && I->qtype[ja] == 0;
@@ -914,7 +989,7 @@ static float en_atom_intra(const oracle_sys *S, const oracle_intra *I, int ia, i
             const size_t k = (size_t)icref * S->ld + iz;
             sume = sume + I->refine_intra_fac * (S->xavs[k] + S->xavs1[k] * dtdif);
         }
-    } else {
+    } else if (!dihedral_pair(I, im, ia, ja)) {
         float xdif = xdifs * I->sizefactor, ydif = ydifs * I->sizefactor, zdif = zdifs * I->sizefactor;
         minimagec(S, &xdif, &ydif, &zdif);
         const float dtest = sqrtf(xdif * xdif + ydif * ydif + zdif * zdif);
@@ -940,7 +1015,11 @@ float oracle_en_mole_intra(const oracle_sys *S, const oracle_intra *I, int im) {
     float e = 0.0f;
     for (int ia = a0; ia < a0 + n - 1; ++ia)
         for (int ja = ia + 1; ja < a0 + n; ++ja)
-            e = e + en_atom_intra(S, I, ia, ja, S->xa[ia], S->ya[ia], S->za[ia], S->xa[ja], S->ya[ja], S->za[ja]);
+            e = e + en_atom_intra(S, I, im, ia, ja, S->xa[ia], S->ya[ia], S->za[ia], S->xa[ja], S->ya[ja], S->za[ja]);
+    if (I->tempdih > 0.0f && I->ngrot && I->ngrot[im] > 0) {   /* :1345-1348 */
+        const float sume = I->tempdih * I->simt * en_mole_dihedral(S, I, im);
+        e = e + sume;
+    }
     return e;
 }
 

@@ -318,14 +318,18 @@ class IntraC(C.Structure):
     _fields_ = [("nbond", P), ("iabond", P), ("tbond", P), ("maxbond", C.c_int32), ("imageatom", P), ("qtype", P),
                 ("amassa", P), ("amassr", P), ("xav", P), ("xav1", P), ("ngrot", P), ("stepcl", C.c_float),
                 ("sizefactor", C.c_float), ("tempb", C.c_float), ("tempang", C.c_float), ("simt", C.c_float),
-                ("refine_intra", C.c_int32), ("refine_intra_fac", C.c_float)]
+                ("refine_intra", C.c_int32), ("refine_intra_fac", C.c_float), ("ndih", C.c_int32), ("grp_nrf", P),
+                ("grp_nrl", P), ("grp_axis", P), ("grp_dih0", P), ("grp_isdih", P), ("dih_atoms", P), ("dih_cos", P),
+                ("dih_sin", P), ("tempdih", C.c_float)]
 
 
 class IntraHandle:
     """Keeps the NumPy arrays of an intramolecular model alive for its IntraC view.  ``m``: dict
     with nbond (natom,), iabond/tbond (natom, maxbond) 0-based, amassa, amassr, xav/xav1
     (npairs, ld), stepcl, sizefactor, tempb, tempang, simt, refine_intra, refine_intra_fac and
-    optional imageatom/qtype/ngrot."""
+    optional imageatom/qtype/ngrot; optional ``dih``: the rotational groups' dihedral angles, a
+    dict with grp_nrf, grp_nrl (per molecule, 0-based), grp_axis (groups x 2), grp_dih0
+    (groups + 1), grp_isdih (groups), dih_atoms (dihedrals x 2), dih_cos, dih_sin, tempdih."""
 
     def __init__(self, box, m):
         self.a = dict(nbond=np.ascontiguousarray(m["nbond"], np.int32),
@@ -343,6 +347,16 @@ class IntraHandle:
         for k in ("stepcl", "sizefactor", "tempb", "tempang", "simt", "refine_intra_fac"):
             setattr(c, k, f32(m[k]))
         c.refine_intra = int(bool(m["refine_intra"]))
+        dh = m.get("dih")
+        if dh is not None:
+            for k in ("grp_nrf", "grp_nrl", "grp_axis", "grp_dih0", "grp_isdih", "dih_atoms"):
+                self.a[k] = np.ascontiguousarray(dh[k], np.int32).reshape(-1)
+                setattr(c, k, ptr(self.a[k]))
+            for k in ("dih_cos", "dih_sin"):
+                self.a[k] = np.ascontiguousarray(dh[k], f32)
+                setattr(c, k, ptr(self.a[k]))
+            c.ndih = int(self.a["dih_cos"].size)
+            c.tempdih = f32(dh["tempdih"])
         self.c = c
 
 

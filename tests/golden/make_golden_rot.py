@@ -20,6 +20,13 @@ molecule's atoms moved at random and tested on its intramolecular energy, then i
 groups rotated and tested on the intramolecular and intermolecular change, molecules in index
 order; stepmi > 0 and a starting interntrans as make_golden_shake.py.  tests/golden/shake_rot.npz
 receives the same fields plus nmovei per cycle.
+
+With dihedral angles (dih_rot.npz, dih_shake.npz) the methyl groups are of type DIH, each with
+one dihedral angle (base atoms S and C, orientation atoms O and the group's first H; 1.0 and 2.5
+rad for the two methyls), dihtemp (tempdihreq) 1: en_mole_intra then adds tempdih * simt * en_mole_dihedral
+(molfit.py:1345-1348, :1353) and en_atom_intra leaves the O-H pairs out of the reference potential
+(:999-1020).  The cosines en_dihedral takes of the dihedral angles are not part of the recorded
+draw cosines; their cosf/sinf values are written as dih_cos/dih_sin.
 """
 
 from __future__ import annotations
@@ -42,7 +49,7 @@ f32 = np.float32
 REF = refstate.reference_root()
 
 
-def run(s, out, seed=21, cycles=2, internrot=0.08, shake=False, interntrans_A=0.05):
+def run(s, out, seed=21, cycles=2, internrot=0.08, shake=False, interntrans_A=0.05, dih=False):
     from epsr26.common import clustercom, epsr16, molecom, molecom_mod, potential_par
     from epsr26.fortran import f32 as F, r4
     from epsr26.fortran.arrays import int_array
@@ -74,7 +81,7 @@ def run(s, out, seed=21, cycles=2, internrot=0.08, shake=False, interntrans_A=0.
     dmso = [m for m in range(s.nmol) if s.mtype[m] == 0]
     ng = 2 * len(dmso)
     molecom_mod.ngrrot = ng
-    molecom_mod.rotgrp = np.array(["   "] + ["ROT"] * ng, dtype=object)
+    molecom_mod.rotgrp = np.array(["   "] + ["DIH" if dih else "ROT"] * ng, dtype=object)
     molecom_mod.labaxi = int_array(ng, 2)
     molecom_mod.nrot = int_array(ng)
     molecom_mod.rotf = int_array(ng)
@@ -112,6 +119,27 @@ def run(s, out, seed=21, cycles=2, internrot=0.08, shake=False, interntrans_A=0.
     for m in range(s.nmol):
         for a in range(int(s.naf[m]), int(s.naf[m]) + int(s.nato[m])):
             molecom.mref[a + 1] = m + 1
+    angles = (F(1.0), F(2.5))
+    if dih:
+        # one dihedral angle per methyl group: base atoms S, C; orientation atoms O (bonded to S)
+        # and the group's first H (bonded to C)
+        dih_atoms, dih_ang = [], []
+        for ig in range(1, ng + 1):
+            a_s, a_c = int(molecom_mod.labaxi[ig, 1]), int(molecom_mod.labaxi[ig, 2])
+            a_h = int(molecom_mod.labrot[molecom_mod.rotf[ig]])
+            a_o = a_s + 1
+            molecom.ndihedralang[ig] = 1
+            molecom.labrotdih[1, 1, ig] = a_o
+            molecom.labrotdih[2, 1, ig] = a_h
+            molecom.dihedralang[1, ig] = angles[(ig - 1) % 2]
+            dih_atoms.append((a_o - 1, a_h - 1))
+            dih_ang.append(angles[(ig - 1) % 2])
+        molecom.tempdihreq = f32(1.0)    # fmolec1 and molfit set tempdihwt from it
+        molecom.tempdihwt = molecom.tempdihreq
+        molecom.tempdih = f32(f32(molecom.tempdihwt) * f32(molecom.tempb))
+        out.update(dih_atoms=np.array(dih_atoms, np.int32), dih_grp0=np.arange(ng + 1, dtype=np.int32),
+                   dih_isdih=np.ones(ng, np.int32), dih_cos=np.array([molfit.cosf(a) for a in dih_ang], f32),
+                   dih_sin=np.array([molfit.sinf(a) for a in dih_ang], f32), tempdih=f32(molecom.tempdih))
     molecom.stepri = f32(1.0)
     ir0 = np.array([internrot] + [0.0] * (nmt - 1), f32)
     clustercom.internrot[1: nmt + 1] = ir0
@@ -159,7 +187,8 @@ def run(s, out, seed=21, cycles=2, internrot=0.08, shake=False, interntrans_A=0.
 
     def cosf_rec(x):
         v = orig_cosf(x)
-        rec.append(v)
+        if not (dih and any(x == a for a in angles)):   # en_dihedral's fixed angles are not draws
+            rec.append(v)
         return v
 
     molfit.cosf = cosf_rec
@@ -202,6 +231,14 @@ if __name__ == "__main__":
         path = os.path.join(HERE, "rot.npz")
         np.savez_compressed(path, **out)
         print("wrote", path)
+    if which in ("dih",):
+        for name, shake in (("dih_rot", False), ("dih_shake", True)):
+            out = {}
+            common.reset()
+            run(configs.c2_mixture(seed=5, ndmso=20, nwater=40), out, seed=29, shake=shake, dih=True)
+            path = os.path.join(HERE, name + ".npz")
+            np.savez_compressed(path, **out)
+            print("wrote", path)
     if which in ("both", "shake_rot"):
         out = {}
         common.reset()

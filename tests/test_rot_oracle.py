@@ -5,6 +5,7 @@ tests/golden/make_golden_rot.py), bit for bit over two cycles: coordinates, stor
 step sizes, ninter/nwhole/nmovem, fadds/faddbs and the ran1 stream."""
 
 import numpy as np
+import pytest
 
 from epsr_python_translation_b200.box import BoxArrays, Ran1State
 from oracle import oracle
@@ -13,15 +14,24 @@ from tests.goldens import GOLDEN, assert_bits_equal
 f32 = np.float32
 
 
-def load():
-    z = np.load(GOLDEN + "/rot.npz")
+def _dih(z):
+    """The golden's dihedral angles as the intramolecular model takes them, or None."""
+    if "dih_cos" not in z.files:
+        return None
+    return dict(grp_nrf=z["rot_nrf"], grp_nrl=z["rot_nrl"], grp_axis=z["rot_axis"], grp_dih0=z["dih_grp0"],
+                grp_isdih=z["dih_isdih"], dih_atoms=z["dih_atoms"], dih_cos=z["dih_cos"], dih_sin=z["dih_sin"],
+                tempdih=z["tempdih"])
+
+
+def load(name="rot.npz"):
+    z = np.load(GOLDEN + "/" + name)
     box = BoxArrays.from_golden(z)
     for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
         getattr(box, k)[:] = z["in_" + k]
     sc = z["scal"]
     model = dict(nbond=z["nbond"], iabond=z["iabond"], tbond=z["tbond"], amassa=z["amassa"], amassr=z["amassr"],
                  xav=z["xav"], xav1=z["xav1"], stepcl=sc[0], sizefactor=sc[1], tempb=sc[2], tempang=sc[3], simt=sc[4],
-                 refine_intra=False, refine_intra_fac=f32(0.0), ngrot=z["ngrot"])
+                 refine_intra=False, refine_intra_fac=f32(0.0), ngrot=z["ngrot"], dih=_dih(z))
     M = int(z["in_nnbrefmax"])
     n = int(z["in_nergpair"])
     st = dict(nnbrefmax=M, nergpair=n, nergpairm=np.ascontiguousarray(z["in_nergpairm"], np.int32),
@@ -38,15 +48,20 @@ def load():
     return z, box, st, mc, rot
 
 
-def test_rotation_golden_exercises_both_outcomes():
-    z = np.load(GOLDEN + "/rot.npz")
+@pytest.mark.parametrize("name", ["rot.npz", "dih_rot.npz"])
+def test_rotation_golden_exercises_both_outcomes(name):
+    z = np.load(GOLDEN + "/" + name)
     for c in range(int(z["cycles"])):
         ni = z[f"c{c}_ninter"]
         assert ni[0, 0] > 0 and 0 < ni[1, 0] < ni[0, 0]       # DMSO rotations tried, some rejected
 
 
-def test_rotation_cycles_oracle_matches_reference():
-    z, box, st, mc, rot = load()
+@pytest.mark.parametrize("name", ["rot.npz", "dih_rot.npz"])
+def test_rotation_cycles_oracle_matches_reference(name):
+    z, box, st, mc, rot = load(name)
+    if name == "dih_rot.npz":
+        # the stored intramolecular energies include the dihedral term (en_mole_intra :1345)
+        assert_bits_equal(oracle.en_mole_intra_all(box, rot["model"]), z["eintra"], "eintra with dihedrals")
     cells = oracle.cell_list(box, int(z["in_nmolcell"]), f32(z["in_sepmax"]))
     ran1 = Ran1State.from_golden(z, "ran1_before_")
     fadds = f32(z["fadds_in"])
@@ -69,16 +84,16 @@ def test_rotation_cycles_oracle_matches_reference():
                                                      int(z[q + "ran1_after_mcall"]))
 
 
-def load_shake():
-    """tests/golden/shake_rot.npz: the same box through two intramolecular cycles."""
-    z = np.load(GOLDEN + "/shake_rot.npz")
+def load_shake(name="shake_rot.npz"):
+    """tests/golden/shake_rot.npz (dih_shake.npz): the same box through two intramolecular cycles."""
+    z = np.load(GOLDEN + "/" + name)
     box = BoxArrays.from_golden(z)
     for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
         getattr(box, k)[:] = z["in_" + k]
     sc = z["scal"]
     model = dict(nbond=z["nbond"], iabond=z["iabond"], tbond=z["tbond"], amassa=z["amassa"], amassr=z["amassr"],
                  xav=z["xav"], xav1=z["xav1"], stepcl=sc[0], sizefactor=sc[1], tempb=sc[2], tempang=sc[3], simt=sc[4],
-                 refine_intra=False, refine_intra_fac=f32(0.0), ngrot=z["ngrot"])
+                 refine_intra=False, refine_intra_fac=f32(0.0), ngrot=z["ngrot"], dih=_dih(z))
     M = int(z["in_nnbrefmax"])
     n = int(z["in_nergpair"])
     st = dict(nnbrefmax=M, nergpair=n, nergpairm=np.ascontiguousarray(z["in_nergpairm"], np.int32),
@@ -93,19 +108,21 @@ def load_shake():
     return z, box, st, mc, rot
 
 
-def test_shake_rotation_golden_exercises_both_outcomes():
-    z = np.load(GOLDEN + "/shake_rot.npz")
+@pytest.mark.parametrize("name", ["shake_rot.npz", "dih_shake.npz"])
+def test_shake_rotation_golden_exercises_both_outcomes(name):
+    z = np.load(GOLDEN + "/" + name)
     for c in range(int(z["cycles"])):
         ni, nm = z[f"c{c}_ninter"], z[f"c{c}_nmovei"]
         assert ni[0, 0] > 0 and 0 < ni[1, 0] < ni[0, 0]       # DMSO rotations tried, some rejected
         assert nm[0].sum() > 0 and nm[1].sum() > 0            # atom moves tried, some rejected
 
 
-def test_shake_rotation_cycles_oracle_matches_reference():
-    """The intramolecular cycle of a box with ROT groups (molfit.py:124-267: atom moves, then the
-    groups' rotations tested with the intermolecular change, molecules in index order), C
+@pytest.mark.parametrize("name", ["shake_rot.npz", "dih_shake.npz"])
+def test_shake_rotation_cycles_oracle_matches_reference(name):
+    """The intramolecular cycle of a box with ROT (DIH) groups (molfit.py:124-267: atom moves, then
+    the groups' rotations tested with the intermolecular change, molecules in index order), C
     restatement against the reference bit for bit over two cycles."""
-    z, box, st, mc, rot = load_shake()
+    z, box, st, mc, rot = load_shake(name)
     ran1 = Ran1State.from_golden(z, "ran1_before_")
     fadds, faddbs, eo1 = f32(z["fadds_in"]), f32(z["faddbs_in"]), f32(0.0)
     for c in range(int(z["cycles"])):
