@@ -67,7 +67,9 @@ class Intra(C.Structure):
     _fields_ = [("nbond", P), ("iabond", P), ("tbond", P), ("maxbond", I32), ("imageatom", P), ("qtype", P),
                 ("amassa", P), ("amassr", P), ("xav", P), ("xav1", P), ("ngrot", P), ("stepcl", F32),
                 ("sizefactor", F32), ("tempb", F32), ("tempang", F32), ("simt", F32), ("refine_intra", I32),
-                ("refine_intra_fac", F32)]
+                ("refine_intra_fac", F32), ("ndih", I32), ("grp_nrf", P), ("grp_nrl", P), ("grp_axis", P),
+                ("grp_dih0", P), ("grp_isdih", P), ("dih_atoms", P), ("dih_cos", P), ("dih_sin", P),
+                ("tempdih", F32)]
 
 
 class Rp(C.Structure):

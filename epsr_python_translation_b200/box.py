@@ -159,6 +159,17 @@ def _powf(x, y):
     return f32(_libm.powf(float(x), float(y)))
 
 
+def libm_f1(name, x):
+    """glibc's float function ``name`` (cosf, sinf, ...) of x, the function the reference calls
+    through ctypes (fortran/fmath.py:67)."""
+    import ctypes
+    _powf(f32(1.0), f32(1.0))   # loads the library
+    fn = getattr(_libm, name)
+    fn.restype = ctypes.c_float
+    fn.argtypes = [ctypes.c_float]
+    return f32(fn(float(x)))
+
+
 def trsteps(natomr: int):
     """Largest and smallest translational step of molfit (molfit.py:96-101), float32."""
     tmax = _powf(f32(1.0) / f32(natomr), f32(1.0) / f32(3.0))

@@ -45,12 +45,14 @@ __device__ float warp_en_mole_intra(const IntraDev &I, int im, const float *x, c
             ++i;
         }
         const int ia = a0 + i, ja = a0 + i + 1 + q;
-        pe[p] = en_atom_intra_d(I, ia, ja, x[ia], y[ia], z[ia], x[ja], y[ja], z[ja]);
+        pe[p] = en_atom_intra_d(I, im, ia, ja, x[ia], y[ia], z[ia], x[ja], y[ja], z[ja]);
     }
     __syncwarp();
     float e = 0.0f;
-    if (lane == 0)
+    if (lane == 0) {
         for (int p = 0; p < np; ++p) e = __fadd_rn(e, pe[p]);
+        if (has_dihedral_term(I, im)) e = __fadd_rn(e, dihedral_term_d(I, im, x, y, z));
+    }
     return e;
 }
 

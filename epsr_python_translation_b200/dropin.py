@@ -29,7 +29,7 @@ the wrapper compares the COMMON arrays it depends on with what it last wrote or 
 the ran1 state is always uploaded.  On return it writes everything the routine changes
 back into the COMMON arrays in place (same array objects, so aliases held by other
 routines stay valid).  A call that needs a feature outside the pair path (rotational
-groups with dihedral angles or of a type other than ROT, tethering, three-body terms,
+groups of a type other than ROT or DIH, tethering, three-body terms,
 coordination constraints, container forces, coarse graining, molecules of more than 64 atoms)
 runs the reference's own routine on the host instead; the next device call picks up whatever
 it changed.
@@ -356,7 +356,7 @@ class PairPath:
             # intramolecular energies (molfit.py:1327) on the device
             eintra = model.en_mole_intra()
         else:
-            # rotational groups (dihedral terms): the reference's own host routine
+            # rotational groups of another type: the reference's own host routine
             en_mole_intra = self.mods["molfit"].en_mole_intra
             sv = sa = sd = f32(0.0)
             eintra = np.zeros(b.nmol, f32)
@@ -371,11 +371,10 @@ class PairPath:
 
     def _rot_groups(self):
         """The box's rotational groups as the device takes them -- (nrf, nrl, axis, first, last,
-        atoms), 0-based -- when every group is of type ROT with no dihedral angle (the dihedral
-        terms of DIH groups, en_mole_dihedral molfit.py:1353, are not on the device); () when no
-        molecule has groups; None otherwise."""
+        atoms), 0-based -- when every group is of type ROT or DIH; () when no molecule has
+        groups; None otherwise (the host runs what needs them)."""
         c = self.c
-        cc, mc = c.clustercom, c.molecom
+        cc = c.clustercom
         nmol = int(cc.nmol)
         ngrot = np.asarray(cc.ngrot[1:nmol + 1])
         if not bool(np.any(ngrot > 0)):
@@ -384,10 +383,9 @@ class PairPath:
         if mm is None or getattr(mm, "labaxi", None) is None:
             return None
         ng = int(mm.ngrrot)
-        if any(str(mm.rotgrp[i]).strip() != "ROT" for i in range(1, ng + 1)):
+        if any(str(mm.rotgrp[i]).strip() not in ("ROT", "DIH") for i in range(1, ng + 1)):
             return None
-        nd = getattr(mc, "ndihedralang", None)
-        if nd is not None and bool(np.any(np.asarray(nd[1:ng + 1]) > 0)):
+        if self._dihedrals(ng) is False:
             return None
         nrot = int(mm.nrottot)
         return (np.asarray(cc.nrf[1:nmol + 1], np.int32) - 1, np.asarray(cc.nrl[1:nmol + 1], np.int32) - 1,
@@ -395,10 +393,43 @@ class PairPath:
                 np.asarray(mm.rotf[1:ng + 1], np.int32) - 1, np.asarray(mm.rotl[1:ng + 1], np.int32) - 1,
                 np.asarray(mm.labrot[1:nrot + 1], np.int32) - 1)
 
+    def _dihedrals(self, ng=None):
+        """The rotational groups' dihedral angles as the device's intramolecular model takes
+        them (molecom labrotdih / ndihedralang / dihedralang, molecom_mod rotgrp): a dict, or
+        None when no group has any; False when a group has dihedral angles but the COMMON blocks
+        do not carry their atoms or angles."""
+        from .box import libm_f1
+        c = self.c
+        cc, mc = c.clustercom, c.molecom
+        mm = getattr(c, "molecom_mod", None)
+        if mm is None or getattr(mm, "labaxi", None) is None:
+            return None
+        ng = int(mm.ngrrot) if ng is None else ng
+        nd = getattr(mc, "ndihedralang", None)
+        isdih = np.array([1 if str(mm.rotgrp[i]).strip() == "DIH" else 0 for i in range(1, ng + 1)], np.int32)
+        ndih = np.zeros(ng, np.int32) if nd is None else np.asarray(nd[1:ng + 1], np.int32)
+        if not bool(np.any(ndih > 0)) and not bool(np.any(isdih)):
+            return None
+        if bool(np.any(ndih > 0)) and (getattr(mc, "labrotdih", None) is None or getattr(mc, "dihedralang", None) is None):
+            return False
+        nmol = int(cc.nmol)
+        atoms, cs, sn = [], [], []
+        for ir in range(1, ng + 1):
+            for kd in range(1, int(ndih[ir - 1]) + 1):
+                atoms.append((int(mc.labrotdih[1, kd, ir]) - 1, int(mc.labrotdih[2, kd, ir]) - 1))
+                a = f32(mc.dihedralang[kd, ir])
+                cs.append(libm_f1("cosf", a))
+                sn.append(libm_f1("sinf", a))
+        return dict(grp_nrf=np.asarray(cc.nrf[1:nmol + 1], np.int32) - 1, grp_nrl=np.asarray(cc.nrl[1:nmol + 1], np.int32) - 1,
+                    grp_axis=np.asarray(mm.labaxi)[1:ng + 1, 1:3].astype(np.int32) - 1,
+                    grp_dih0=np.concatenate([[0], np.cumsum(ndih)]).astype(np.int32), grp_isdih=isdih,
+                    dih_atoms=np.array(atoms, np.int32).reshape(-1, 2), dih_cos=np.array(cs, f32),
+                    dih_sin=np.array(sn, f32), tempdih=f32(mc.tempdih))
+
     def _intra_model(self, b, allow_rot=False):
         """The device intramolecular model (en_atom_intra molfit.py:923) from molecom, or None
         when the COMMON blocks carry no bond lists, or when a molecule has rotational groups and
-        allow_rot is false (groups with dihedral terms stay on the host)."""
+        allow_rot is false; with allow_rot the groups' dihedral angles come with it."""
         from .intra import IntraModel
         c = self.c
         mc, cc, pp, e16 = c.molecom, c.clustercom, c.potential_par, c.epsr16
@@ -418,11 +449,12 @@ class PairPath:
                           xav=np.asarray(pp.xav)[:ld, 1:npairs + 1].T, xav1=np.asarray(pp.xav1)[:ld, 1:npairs + 1].T,
                           stepcl=f32(e16.cellst) / f32(mc.dmaxmol), simt=f32(mc.simt), sizefactor=f32(mc.sizefactor),
                           tempb=f32(mc.tempb), tempang=f32(mc.tempang), refine_intra=bool(getattr(mc, "refine_intra", False)),
-                          refine_intra_fac=f32(getattr(mc, "refine_intra_fac", 0.0)), ngrot=ngrot)
+                          refine_intra_fac=f32(getattr(mc, "refine_intra_fac", 0.0)), ngrot=ngrot,
+                          dih=self._dihedrals() if allow_rot and bool(np.any(ngrot > 0)) else None)
 
     def molfit(self, fadds, faddbs, nisum, intra, rotfreq, ireset):
         """molfit.py:52-541: the whole-molecule branch and the intramolecular branch (:124-267),
-        internal rotations of ROT groups included, on the device; returns (fadds, faddbs, nisum)."""
+        internal rotations of ROT and DIH groups included, on the device; returns (fadds, faddbs, nisum)."""
         c = self.c
         mc, cc = c.molecom, c.clustercom
         nmol = int(cc.nmol)
@@ -479,9 +511,8 @@ class PairPath:
 
     def _molfit_intra(self, fadds, faddbs, ireset):
         """The intramolecular cycle of molfit (:119-267, step adaptation :465-536) on the
-        device, the internal rotations of ROT groups included; None when a group is not of type
-        ROT or has dihedral angles, or the COMMON blocks carry no bond lists (the host runs the
-        cycle)."""
+        device, the internal rotations of ROT and DIH groups included; None when a group is of
+        another type, or the COMMON blocks carry no bond lists (the host runs the cycle)."""
         c = self.c
         mc, cc = c.molecom, c.clustercom
         nmol = int(cc.nmol)

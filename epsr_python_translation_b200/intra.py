@@ -32,7 +32,11 @@ class IntraModel:
 
     def __init__(self, d, *, nbond, iabond, tbond, amassa, amassr, xav, xav1, stepcl, simt, imageatom=None,
                  qtype=None, ngrot=None, sizefactor=1.0, tempb=1.0, tempang=1.0, refine_intra=False,
-                 refine_intra_fac=0.0):
+                 refine_intra_fac=0.0, dih=None):
+        """dih: the rotational groups' dihedral angles, or None -- a dict with grp_nrf, grp_nrl
+        (per molecule, 0-based group range), grp_axis (groups x 2 base atoms), grp_dih0 (groups + 1),
+        grp_isdih (groups: 1 for DIH), dih_atoms (dihedrals x 2), dih_cos, dih_sin (the host C
+        library's cosf/sinf of each angle, as the reference takes them) and tempdih."""
         self.lib = _lib.load(require_device=True)
         self.d = d
         b = d.host
@@ -61,6 +65,19 @@ class IntraModel:
         s.stepcl, s.sizefactor, s.tempb, s.tempang, s.simt = (float(f32(v)) for v in (stepcl, sizefactor, tempb, tempang,
                                                                                        simt))
         s.refine_intra, s.refine_intra_fac = int(bool(refine_intra)), float(f32(refine_intra_fac))
+        self.dih = None
+        if dih is not None:
+            self.dih = {k: t(np.asarray(dih[k]).reshape(-1), np.int32)
+                        for k in ("grp_nrf", "grp_nrl", "grp_axis", "grp_dih0", "grp_isdih")}
+            na = np.asarray(dih["dih_atoms"], np.int32).reshape(-1)
+            self.dih["dih_atoms"] = t(na if na.size else np.zeros(2, np.int32), np.int32)
+            for k in ("dih_cos", "dih_sin"):
+                v = np.asarray(dih[k], f32).reshape(-1)
+                self.dih[k] = t(v if v.size else np.zeros(1, f32), f32)
+            for k, v in self.dih.items():
+                setattr(s, k, _p(v))
+            s.ndih = int(np.asarray(dih["dih_cos"]).size)
+            s.tempdih = float(f32(dih["tempdih"]))
         self.c = s
 
     def en_mole_intra(self, out=None):

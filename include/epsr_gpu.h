@@ -199,9 +199,12 @@ int epsr_en_mole_pair(const epsr_box_t *box, const int32_t *im, const int32_t *j
 
 /* ------------------------------------------------------------------ intramolecular moves */
 
-/* The intramolecular model of en_atom_intra molfit.py:923-1045 (molecom arrays; all pointers
- * device, atoms 0-based).  Molecules with rotational groups (ngrot > 0: dihedral terms and the
- * internal rotations of rotati :589) are outside this path. */
+/* The intramolecular model of en_atom_intra molfit.py:923-1045 and en_mole_intra :1327
+ * (molecom arrays; all pointers device, atoms 0-based).  The dihedral block carries the
+ * rotational groups' dihedral angles (molecom labrotdih / ndihedralang / dihedralang): the
+ * energy tempdih * simt * en_mole_dihedral (:1345-1348, :1353, DIH groups) of a molecule with
+ * groups, and their atom pairs left out of the reference potential (:999-1020); grp_nrf NULL
+ * (the block zeroed) for a model without dihedral angles. */
 typedef struct {
     const int32_t *nbond;      /* [natom] bonds listed for each atom */
     const int32_t *iabond;     /* [natom*maxbond] 0-based partner atom of each bond */
@@ -217,6 +220,14 @@ typedef struct {
     float sizefactor, tempb, tempang, simt;
     int32_t refine_intra;      /* 1: add refine_intra_fac x EP (box->tab) to non-q pairs */
     float refine_intra_fac;
+    int32_t ndih;                       /* dihedral angles over all groups */
+    const int32_t *grp_nrf, *grp_nrl;   /* [nmol] first and last group of each molecule (0-based) */
+    const int32_t *grp_axis;            /* [ngroups*2] the two base atoms of each group (labaxi) */
+    const int32_t *grp_dih0;            /* [ngroups+1] each group's range in dih_* */
+    const int32_t *grp_isdih;           /* [ngroups] 1 for a group of type DIH */
+    const int32_t *dih_atoms;           /* [ndih*2] orientation atoms io1 (by base atom 1), io2 (by 2) */
+    const float *dih_cos, *dih_sin;     /* [ndih] cosf, sinf of the angle (the host C library, as the reference) */
+    float tempdih;                      /* molecom.tempdih (tempdihwt * tempb) */
 } epsr_intra_t;
 
 /* The molecule centres put back in the box (minimagec minimagec.py:13-62 of xadd, yadd, zadd),

@@ -16,10 +16,11 @@ pytestmark = pytest.mark.gpu
 f32 = np.float32
 
 
-def test_rotation_cycles_device_match_reference():
+@pytest.mark.parametrize("name", ["rot.npz", "dih_rot.npz"])
+def test_rotation_cycles_device_match_reference(name):
     from epsr_python_translation_b200.device import DeviceBox
     from epsr_python_translation_b200.intra import IntraModel
-    z, box, st, mc, rot = load()
+    z, box, st, mc, rot = load(name)
     d = DeviceBox(box)
     d.cell_list(int(z["in_nmolcell"]), f32(z["in_sepmax"]))
     d.fmolec1(z["eintra"], strict=True)
@@ -31,6 +32,9 @@ def test_rotation_cycles_device_match_reference():
                trstepmax=tmax, trstepmin=tmin, fadds=f32(z["fadds_in"]))
     model = dict(rot["model"])
     im = IntraModel(d, **model)
+    if name == "dih_rot.npz":
+        # the stored intramolecular energies with the dihedral term, on the device
+        assert_bits_equal(im.en_mole_intra().cpu().numpy(), z["eintra"], "eintra with dihedrals")
     d.set_rotations(im, z["rot_nrf"], z["rot_nrl"], z["rot_axis"], z["rot_first"], z["rot_last"], z["rot_atoms"],
                     stepri=1.0, faddbs=f32(z["faddbs_in"]))
     for c in range(int(z["cycles"])):
@@ -68,19 +72,22 @@ class _Aliased:
         return list(self.z.files) + list(self.ALIAS)
 
 
-def test_rotation_dropin_matches_reference():
+@pytest.mark.parametrize("name", ["rot.npz", "dih_rot.npz"])
+def test_rotation_dropin_matches_reference(name):
     """PairPath.molfit on COMMON stand-ins that carry the reference's rotational groups
-    (molecom_mod labaxi/rotf/rotl/labrot, clustercom ngrot/nrf/nrl, all of type ROT) and
-    intramolecular model: the whole-molecule cycles with internal rotations run on the device
-    and leave the COMMON state equal to the reference's; no host routine ran."""
-    _rotation_dropin("rot.npz", shake=False)
+    (molecom_mod labaxi/rotf/rotl/labrot, clustercom ngrot/nrf/nrl, of type ROT or DIH with
+    their dihedral angles) and intramolecular model: the whole-molecule cycles with internal
+    rotations run on the device and leave the COMMON state equal to the reference's; no host
+    routine ran."""
+    _rotation_dropin(name, shake=False)
 
 
-def test_shake_rotation_dropin_matches_reference():
+@pytest.mark.parametrize("name", ["shake_rot.npz", "dih_shake.npz"])
+def test_shake_rotation_dropin_matches_reference(name):
     """As above for the intramolecular cycles (nisum >= intra) of the same box: atom moves and
     internal rotations on the device, the COMMON state (nmovei, ninter, nstepreject and
     interntrans included) equal to the reference's; no host routine ran."""
-    _rotation_dropin("shake_rot.npz", shake=True)
+    _rotation_dropin(name, shake=True)
 
 
 def _rotation_dropin(name, shake):
@@ -129,10 +136,21 @@ def _rotation_dropin(name, shake):
     rotf[1:], rotl[1:] = z["rot_first"] + 1, z["rot_last"] + 1
     labrot = fa(z["rot_atoms"].size, dtype=np.int32)
     labrot[1:] = z["rot_atoms"] + 1
+    dih = "dih_cos" in z.files
     c.molecom_mod = NS(coarsegraining=False, natomsphere=c.molecom_mod.natomsphere, ngrrot=ng,
-                       rotgrp=np.array(["   "] + ["ROT"] * ng, dtype=object), labaxi=lab, rotf=rotf, rotl=rotl,
-                       labrot=labrot, nrottot=int(z["rot_atoms"].size))
+                       rotgrp=np.array(["   "] + ["DIH" if dih else "ROT"] * ng, dtype=object), labaxi=lab,
+                       rotf=rotf, rotl=rotl, labrot=labrot, nrottot=int(z["rot_atoms"].size))
     mc.ndihedralang = fa(ng, dtype=np.int32)
+    if dih:
+        # one dihedral angle per group, as the reference held them (1.0 and 2.5 rad alternately)
+        mc.ndihedralang[1:] = np.diff(z["dih_grp0"])
+        mc.labrotdih = np.zeros((3, 2, ng + 1), np.int32)
+        mc.dihedralang = np.zeros((2, ng + 1), f32)
+        for ir in range(1, ng + 1):
+            mc.labrotdih[1, 1, ir], mc.labrotdih[2, 1, ir] = z["dih_atoms"][ir - 1] + 1
+            mc.dihedralang[1, ir] = f32(1.0) if (ir - 1) % 2 == 0 else f32(2.5)
+        mc.tempdihreq = mc.tempdihwt = f32(1.0)
+        mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
     path = dropin.PairPath(c, mods, strict=True)
     path.install(dropin.ROUTINES)
     mods["cellneighbourlist"].initialise_cellneighbourlist(int(z["in_nmolcell"]), cc.xadd, cc.yadd, cc.zadd, nmol,
@@ -167,7 +185,8 @@ def _rotation_dropin(name, shake):
     assert not [k for k in calls if k.startswith("host:")], calls
 
 
-def test_shake_rotation_cycles_device_match_reference():
+@pytest.mark.parametrize("name", ["shake_rot.npz", "dih_shake.npz"])
+def test_shake_rotation_cycles_device_match_reference(name):
     """molfit's intramolecular cycle on a box with ROT groups (molfit.py:124-267: each
     molecule's atom moves, then its methyl groups rotated and tested with the intermolecular
     change, molecules in index order) through epsr_molfit_shake with the reference's cosines
@@ -179,7 +198,7 @@ def test_shake_rotation_cycles_device_match_reference():
     from epsr_python_translation_b200.device import DeviceBox
     from epsr_python_translation_b200.intra import IntraModel
     from tests.test_rot_oracle import load_shake
-    z, box, st, mc, rot = load_shake()
+    z, box, st, mc, rot = load_shake(name)
     d = DeviceBox(box)
     d.cell_list(int(z["in_nmolcell"]), f32(z["in_sepmax"]))
     d.fmolec1(z["eintra"], strict=True)
