@@ -153,9 +153,9 @@ typedef struct {
     int32_t *status;                /* [1] device: 0 ok, 1 a molecule exceeds 64 atoms,
                                        2 the fast path's resolver timed out (cycle not applied) */
     /* Internal rotations of rotational groups before each molecule's whole-molecule move
-     * (molfit.py:295-360, rotati :589): set intra (NULL: none).  Groups of type ROT only -- the
-     * dihedral terms of DIH groups (en_mole_dihedral :1353) are not evaluated, so a caller with
-     * DIH groups must not pass them.  With intra set, every cycle runs the sequential kernel. */
+     * (molfit.py:295-360, rotati :589): set intra (NULL: none).  Groups of type ROT or DIH; the
+     * dihedral terms of DIH groups (en_mole_dihedral :1353) come from the dihedral block of the
+     * epsr_intra_t.  With intra set, every cycle runs the sequential kernel. */
     const void *intra;              /* host pointer to the epsr_intra_t of the intramolecular model (its ngrot) */
     const int32_t *rot_nrf, *rot_nrl;   /* [nmol] first and last group of each molecule (0-based) */
     const int32_t *rot_axis;        /* [ngroups*2] axis atoms (0-based); the rotation is about the first */
