@@ -58,7 +58,7 @@ DEFAULT_REPLICAS = {"c3_water": 4, "c2_mixture": 16}
 # kernels the library brackets with CUDA events while timing is enabled
 TIMED_KERNELS = ("spec_energy_kernel", "spec_corr_kernel", "spec_resolve_kernel", "molfit_seq_kernel",
                  "fm_count_kernel", "ag_inter_kernel", "fitexp_cluster_kernel", "ahead_fill_kernel",
-                 "ran1_fill_kernel", "spec_plan_kernel", "spec_propose_kernel", "spec_commit_kernels")
+                 "ran1_fill_kernel", "spec_plan_kernel", "spec_propose_kernel", "spec_commit_kernel")
 # the ordered walk of spec_resolve_kernel on its own (one warp, rows in shared memory, no far
 # parts to wait for), measured on B200: the latency floor of a resolved move
 RESOLVE_WALK_CYCLES_PER_MOVE = 88.5

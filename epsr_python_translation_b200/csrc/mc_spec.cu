@@ -48,6 +48,8 @@ constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
 constexpr int SP_ET = 320;      // threads of a move's energy CTA (its stored partners: about 300 at 0.1 atoms/A^3)
 constexpr int SP_RT = 640;      // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
+// words of the draws-ahead buffer (described with the draws-ahead kernels below)
+constexpr int AH_VALID = 0, AH_COUNT = 1, AH_USES = 2, AH_START = 4, AH_END = 40, AH_VALS = 80;
 constexpr int SP_MAXEDGE = 16384;  // table points indexed by bin edges (beyond: the energy pass divides)
 
 struct SpecDev {
@@ -73,11 +75,13 @@ struct SpecDev {
     int32_t *trace_acc;
     int32_t *status;
     // scratch
-    int32_t *vpos, *off, *rotidx, *flags;  // flags[0] retry, [1] resolver timeout, [2] values to walk, [3] draws ahead taken
+    int32_t *vpos, *off, *rotidx, *flags;  // flags[0] retry, [1] resolver timeout, [2] values to walk, [3] draws ahead
+                                           // taken, [4] CTAs of the commit pass done
     float *rotstep, *transstep;            // [nmoltype]
     int32_t *tries_rot, *tries_tr, *rej_rot, *rej_tr, *cnt_type;  // [nmoltype]
     int32_t *ran1_next;                    // [35]
     float *draws;
+    int32_t *ahead;                        // the draws-ahead buffer (AH_* words), or NULL
     const float *ahead_vals;               // the draws-ahead values, or NULL
     const int32_t *use_ahead;              // [1] 1: this cycle reads ahead_vals (NULL: never)
     float *nx, *ny, *nz;                   // [natom] proposed offsets
@@ -115,6 +119,7 @@ __global__ void spec_plan_kernel(SpecDev S) {
     if (tid == 0) {
         S.flags[0] = 0;
         S.flags[1] = 0;
+        S.flags[4] = 0;
         *S.fadd_acc = 0.0;
     }
     __syncthreads();
@@ -198,6 +203,52 @@ __global__ void spec_plan_kernel(SpecDev S) {
         if (S.tries_tr[t] > 0) {
             if (S.transstep[t] <= 0.0f) S.transstep[t] = S.trstepmin;
         }
+    }
+    __syncthreads();   // off[N], the cycle's draw count
+    if (tid >= 32) return;
+    // the cycle's ran1 values, from a copy of the state (a discarded cycle leaves the real state
+    // untouched): the draws ahead when the previous cycle left them for exactly this state and
+    // count, else walked here by this warp
+    const int lane = tid;
+    for (int i = lane; i < 35; i += 32) S.ran1_next[i] = S.ran1[i];
+    const int32_t count = S.off[S.N];
+    bool ok = false;
+    if (S.ahead) {
+        bool same = S.ahead[AH_START + lane] == S.ran1[lane];
+        if (lane < 3) same = same && S.ahead[AH_START + 32 + lane] == S.ran1[32 + lane];
+        ok = __all_sync(0xffffffffu, same) && S.ahead[AH_VALID] == 1 && S.ahead[AH_COUNT] == count;
+    }
+    __syncwarp();
+    if (ok) {
+        S.ran1_next[lane] = S.ahead[AH_END + lane];
+        if (lane < 3) S.ran1_next[32 + lane] = S.ahead[AH_END + 32 + lane];
+    }
+    if (lane == 0) {
+        S.flags[2] = ok ? 0 : count;
+        S.flags[3] = ok ? 1 : 0;
+        if (ok) S.ahead[AH_USES] += 1;
+    }
+    __syncwarp();
+    if (ok || count == 0) return;
+    __shared__ int32_t tab[34];
+    Ran1Warp g;
+    g.load(S.ran1_next);
+    const int32_t mcall = S.ran1_next[2];
+    __syncwarp();
+    int64_t done = 0;
+    while (done < count) {
+        const int64_t left = count - done;
+        int32_t mine;
+        const int cnt = g.next(left > 32 ? 32 : (int)left, mine, tab);
+        if (lane < cnt) S.draws[done + lane] = ran1_out(mine);
+        done += cnt;
+    }
+    __syncwarp();
+    S.ran1_next[3 + lane] = g.iv;
+    if (lane == 0) {
+        S.ran1_next[0] = g.idum;
+        S.ran1_next[1] = g.iy;
+        S.ran1_next[2] = (int32_t)((uint32_t)mcall + (uint32_t)count);
     }
 }
 
@@ -313,7 +364,6 @@ __device__ __forceinline__ void mol_energy_ab(const Lattice &L, const Tables &T,
 // pair value is pair_energy of the same operands as en_change, so A and B are the values of
 // mol_energy_ab bit for bit; the items keep a partner's nine (water) or more pair evaluations
 // independent of each other instead of one thread's dependent chain of table loads.
-constexpr int SP_EV = 2 * SP_MAXAT * SP_MAXAT;   // staged pair values per chunk at most (one partner's A and B)
 
 __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
 #pragma unroll
@@ -830,56 +880,69 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
 }
 
 // ----------------------------------------------------------------- commit
-__global__ void spec_commit_moves_kernel(SpecDev S) {
-    if (S.flags[0] || S.flags[1]) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= S.N) return;
-    const int m = S.visit[k];
-    const int t = S.mtype[m];
-    const int a0 = S.naf[m], n = S.nato[m];
-    if (S.acc[k]) {
-        for (int i = 0; i < n; ++i) {
-            S.xa_w[a0 + i] = S.nx[a0 + i];
-            S.ya_w[a0 + i] = S.ny[a0 + i];
-            S.za_w[a0 + i] = S.nz[a0 + i];
-            S.pos_w[a0 + i] = S.npos[a0 + i];
-        }
-        const float4 c = S.nc[m];
-        S.xadd_w[m] = c.x;
-        S.yadd_w[m] = c.y;
-        S.zadd_w[m] = c.z;
-        S.nstepreject[m] = 0;
-    } else {
-        S.nstepreject[m]++;
-        if (S.stepr > 0.0f) atomicAdd(S.rej_rot + t, 1);
-        if (S.stepm > 0.0f) atomicAdd(S.rej_tr + t, 1);
-    }
-    if (S.trace_den) S.trace_den[k] = S.fdiff[k];
-    if (S.trace_acc) S.trace_acc[k] = S.acc[k];
-}
+// The cycle's commits in one pass, one CTA per molecule m (visited at position km): if its move
+// was accepted, its stored energies (the later accepted writer of a shared slot wins) and its
+// coordinates; its counters either way.  The CTA that finishes last then runs the epilogue
+// (counts, step adaptation, fadds, the ran1 state), every other CTA's counts being complete.
+__device__ void spec_epilogue(const SpecDev &S);
 
-__global__ void spec_commit_store_kernel(SpecDev S) {
-    if (S.flags[0] || S.flags[1]) return;
+__global__ void __launch_bounds__(128) spec_commit_kernel(SpecDev S) {
+    __shared__ int s_last;
     const int m = blockIdx.x;
-    const int km = S.vpos[m];
-    const int nn = S.nergpairm[m];
-    const size_t row = (size_t)m * S.M;
-    const int am = S.acc[km];
-    if (!am) return;
-    for (int s = 1 + threadIdx.x; s < nn; s += blockDim.x) {
-        const size_t e = row + s;
-        const int p = S.molergpair[e];
-        const int kp = S.vpos[p];
-        const int e2 = S.mirror[e];
-        const int p_writes = S.acc[kp] && (e2 % S.M) >= 1;
-        if (p_writes && kp > km) continue;  // the later accepted writer wins
-        const float v = (kp < km && S.acc[kp]) ? S.B[e] : S.A[e];
-        S.ergpair[S.ergpairref[e] - 1] = v;
+    if (!(S.flags[0] || S.flags[1])) {
+        const int km = S.vpos[m];
+        const int am = S.acc[km];
+        if (am) {
+            const int nn = S.nergpairm[m];
+            const size_t row = (size_t)m * S.M;
+            for (int s = 1 + threadIdx.x; s < nn; s += blockDim.x) {
+                const size_t e = row + s;
+                const int p = S.molergpair[e];
+                const int kp = S.vpos[p];
+                const int e2 = S.mirror[e];
+                const int p_writes = S.acc[kp] && (e2 % S.M) >= 1;
+                if (p_writes && kp > km) continue;  // the later accepted writer wins
+                const float v = (kp < km && S.acc[kp]) ? S.B[e] : S.A[e];
+                S.ergpair[S.ergpairref[e] - 1] = v;
+            }
+            const int a0 = S.naf[m], n = S.nato[m];
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                S.xa_w[a0 + i] = S.nx[a0 + i];
+                S.ya_w[a0 + i] = S.ny[a0 + i];
+                S.za_w[a0 + i] = S.nz[a0 + i];
+                S.pos_w[a0 + i] = S.npos[a0 + i];
+            }
+            if (threadIdx.x == 0) {
+                const float4 c = S.nc[m];
+                S.xadd_w[m] = c.x;
+                S.yadd_w[m] = c.y;
+                S.zadd_w[m] = c.z;
+                S.nstepreject[m] = 0;
+            }
+        } else if (threadIdx.x == 0) {
+            const int t = S.mtype[m];
+            S.nstepreject[m]++;
+            if (S.stepr > 0.0f) atomicAdd(S.rej_rot + t, 1);
+            if (S.stepm > 0.0f) atomicAdd(S.rej_tr + t, 1);
+        }
+        if (threadIdx.x == 0) {
+            if (S.trace_den) S.trace_den[km] = S.fdiff[km];
+            if (S.trace_acc) S.trace_acc[km] = am;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(S.flags + 4, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        spec_epilogue(S);
     }
 }
 
-__global__ void spec_epilogue_kernel(SpecDev S) {
-    if (threadIdx.x != 0) return;
+__device__ void spec_epilogue(const SpecDev &S) {
     if (S.flags[1]) {
         if (S.status) S.status[0] = 2;
         return;
@@ -895,9 +958,9 @@ __global__ void spec_epilogue_kernel(SpecDev S) {
             S.wholetrans[t] = S.tries_tr[t] > 0 ? S.transstep[t] : 0.0f;
         }
         S.nwhole[t] = S.tries_rot[t];
-        S.nwhole[nmt + t] = S.rej_rot[t];
+        S.nwhole[nmt + t] = *(volatile const int32_t *)(S.rej_rot + t);   // counted by other CTAs' atomics
         S.nmovem[t] = S.tries_tr[t];
-        S.nmovem[nmt + t] = S.rej_tr[t];
+        S.nmovem[nmt + t] = *(volatile const int32_t *)(S.rej_tr + t);
     }
     if (S.ireset != 1) {
         for (int t = 0; t < nmt; ++t) {
@@ -941,11 +1004,6 @@ __global__ void spec_epilogue_kernel(SpecDev S) {
 }  // namespace epsr
 
 namespace epsr {
-// ran1 draws for the cycle: n comes from the plan (device), the state is a copy so that a
-// discarded cycle leaves the real state untouched
-__global__ void ran1_copy_kernel(const int32_t *src, int32_t *dst) {
-    if (threadIdx.x < 35) dst[threadIdx.x] = src[threadIdx.x];
-}
 
 // Draws ahead.  The values a cycle draws are the next off[N] values of the one ran1 stream, a
 // function of the state the cycle starts from and of that count only.  While a cycle runs, a
@@ -958,24 +1016,6 @@ __global__ void ran1_copy_kernel(const int32_t *src, int32_t *dst) {
 // it needs exactly AH_COUNT values; otherwise (another stage drew from the stream in
 // between, the cycle was redone by the sequential kernel, the caller set a new state) it
 // walks the stream itself.  Either way it draws the same values.
-constexpr int AH_VALID = 0, AH_COUNT = 1, AH_USES = 2, AH_START = 4, AH_END = 40, AH_VALS = 80;
-
-__global__ void ahead_adopt_kernel(const int32_t *state, int32_t *ahead, const int32_t *count, int32_t *next_state,
-                                   int32_t *nfill, int32_t *use) {
-    const int lane = threadIdx.x;
-    bool same = ahead[AH_START + lane] == state[lane];
-    if (lane < 3) same = same && ahead[AH_START + 32 + lane] == state[32 + lane];
-    const bool ok = __all_sync(0xffffffffu, same) && ahead[AH_VALID] == 1 && ahead[AH_COUNT] == *count;
-    if (ok) {
-        next_state[lane] = ahead[AH_END + lane];
-        if (lane < 3) next_state[32 + lane] = ahead[AH_END + 32 + lane];
-    }
-    if (lane == 0) {
-        *nfill = ok ? 0 : *count;
-        *use = ok ? 1 : 0;
-        if (ok) ahead[AH_USES] += 1;
-    }
-}
 
 __global__ void ahead_fill_kernel(const int32_t *state, int32_t *ahead, const int32_t *count) {
     const int lane = threadIdx.x;
@@ -1039,7 +1079,6 @@ static int ahead_stream(AheadStream **out) {
     *out = &a;
     return EPSR_OK;
 }
-int ran1_fill_device_count(int32_t *state, float *out, const int32_t *n_dev, int64_t n_max, cudaStream_t s);
 int molfit_seq_launch(const epsr_box_t *box, const epsr_cells_t *cells, epsr_store_t *store, epsr_mc_t *mc,
                       void *scratch, int64_t scratch_bytes, cudaStream_t s, const int32_t *run_if);
 }  // namespace epsr
@@ -1202,16 +1241,15 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
 
     // draws ahead: only with a buffer that holds a whole cycle's values (at most 7 a move)
     const bool ahead = mc->ahead && mc->ahead_cap >= (int64_t)N * 7;
-    int32_t *nfill = S.flags + 2, *use = S.flags + 3;
+    int32_t *use = S.flags + 3;
     if (ahead) {
         S.ahead_vals = reinterpret_cast<const float *>(mc->ahead + AH_VALS);
         S.use_ahead = use;
     }
+    if (ahead) S.ahead = mc->ahead;
+    int rc = EPSR_OK;
     EPSR_TIMED("spec_plan_kernel", s, spec_plan_kernel<<<1, 1024, 0, s>>>(S));
-    ran1_copy_kernel<<<1, 64, 0, s>>>(mc->ran1, S.ran1_next);
-    if (ahead) ahead_adopt_kernel<<<1, 32, 0, s>>>(mc->ran1, mc->ahead, S.off + N, S.ran1_next, nfill, use);
-    int rc = ran1_fill_device_count(S.ran1_next, S.draws, ahead ? nfill : S.off + N, (int64_t)N * 7 + 1, s);
-    if (rc) return rc;
+    EPSR_CUDA(cudaGetLastError());
     EPSR_TIMED("spec_propose_kernel", s, spec_propose_kernel<<<(max(N, S.nedge) + 127) / 128, 128, 0, s>>>(S));
     // the next cycle's values, from the state after this cycle's draws, on the second stream
     // once nothing of this cycle reads the buffer any more; joined before this call returns
@@ -1257,8 +1295,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     }
     EPSR_SMEM_OPTIN(spec_resolve_kernel);
     EPSR_TIMED("spec_resolve_kernel", s, spec_resolve_kernel<<<1, SP_RT, rsmem, s>>>(S));
-    EPSR_TIMED("spec_commit_kernels", s, spec_commit_moves_kernel<<<(N + 127) / 128, 128, 0, s>>>(S);
-               spec_commit_store_kernel<<<N, 128, 0, s>>>(S); spec_epilogue_kernel<<<1, 32, 0, s>>>(S));
+    EPSR_TIMED("spec_commit_kernel", s, spec_commit_kernel<<<N, 128, 0, s>>>(S));
     EPSR_CUDA(cudaGetLastError());
     if (ahead) EPSR_CUDA(cudaStreamWaitEvent(s, as->join, 0));
     // a cycle with a translation retry runs on the sequential kernel (no-op otherwise)

@@ -38,13 +38,6 @@ __global__ void ran1_fill_kernel(int32_t *state, float *out, int64_t n_host, con
     }
 }
 
-int ran1_fill_device_count(int32_t *state, float *out, const int32_t *n_dev, int64_t n_max, cudaStream_t s) {
-    (void)n_max;
-    EPSR_TIMED("ran1_fill_kernel", s, ran1_fill_kernel<<<1, 32, 0, s>>>(state, out, 0, n_dev));
-    EPSR_CUDA(cudaGetLastError());
-    return EPSR_OK;
-}
-
 }  // namespace epsr
 
 extern "C" int epsr_ran1_fill(int32_t *state, float *out, int64_t n, void *stream) {
