@@ -110,3 +110,35 @@ def test_native_iteration_with_methyl_rotations_matches_python_driver():
     ni = b.d.m_ninter.cpu().numpy()
     assert ni[0] > 0 and ni[nmt_rej := wl.system.nmoltype] < ni[0]
     del nmt_rej
+
+
+def test_native_iteration_with_rotations_in_intramolecular_cycles_matches_python_driver():
+    """C2 with flexible molecules (intra = 2) and the DMSO methyl groups as rotational groups
+    (rotfreq 2): the intramolecular cycles then rotate the groups after each molecule's atom
+    moves (molfit.py:175-267, on the sequential kernel), the whole-molecule cycles every second
+    time.  The native and the Python drivers leave identical coordinates, stored energies,
+    counters, faddbs and ran1 streams, and both kinds of cycle ran."""
+    from epsr_python_translation_b200 import configs
+    from epsr_python_translation_b200.iteration import EpsrIteration
+    wl = configs.make_workload("c2_mixture", ntimes=3, intra=2, rotfreq=2)
+    assert wl.rotfreq == 2 and wl.intra == 2
+    a = EpsrIteration(wl, ran1_seed=-17, native=True)
+    b = EpsrIteration(wl, ran1_seed=-17, native=False)
+    for _ in range(3):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    ca, cb = a.d.download_coords(), b.d.download_coords()
+    for k in ca:
+        assert np.array_equal(ca[k].view(np.uint32), cb[k].view(np.uint32)), k
+    assert np.array_equal(a.ran1.cpu().numpy(), b.ran1.cpu().numpy())
+    sa, sb = a.d.download_store(), b.d.download_store()
+    assert np.array_equal(sa["ergpair"].view(np.uint32), sb["ergpair"].view(np.uint32))
+    for x, y in ((a.faddbs, b.faddbs), (a.d.m_faddbs, b.d.m_faddbs), (a._nmovei, b._nmovei),
+                 (a.d.m_ninter, b.d.m_ninter), (a.d.m_internrot, b.d.m_internrot)):
+        assert np.array_equal(x.cpu().numpy().view(np.uint32), y.cpu().numpy().view(np.uint32))
+    assert int(b._nmovei.cpu()[0]) > 0                     # atom moves were tried
+    # rotations were tried: the DMSO type's rotation step was adapted away from its start (the
+    # counters hold only the last cycle's, a whole-molecule cycle without rotations here)
+    assert float(b.d.m_internrot.cpu()[0]) != float(wl.internrot[0])
+    assert float(b.faddbs.cpu()[0]) != 0.0
