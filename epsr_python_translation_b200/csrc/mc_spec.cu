@@ -374,10 +374,10 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
     return v;
 }
 
-template <bool BINS>
 // four CTAs of the energy pass per SM (40 warps): its shared memory allows four, and the
 // register budget that gives (51 a thread) holds the three pair evaluations in flight unspilled
 constexpr int SP_EN_MINB = 4;
+template <bool BINS>
 __global__ void __launch_bounds__(SP_ET, SP_EN_MINB) spec_energy_kernel(SpecDev S) {
     extern __shared__ __align__(16) unsigned char en_smem[];
     const int ev = S.ev;                                                 // staged values per chunk
