@@ -43,10 +43,10 @@ constexpr int SP_W = 64;        // near window of the resolver (moves): two runn
 constexpr int SP_FR = 128;      // far-sum ring (moves)
 constexpr int SP_BLK = 32;      // moves per staged block (and per published decision word)
 constexpr int SP_NSLOT = 4;     // staged blocks held in shared memory
-constexpr int SP_NH = 15;       // helper warps: warps 1..19 outside scheduler 0
+constexpr int SP_NH = 24;       // helper warps: warps 1..31 outside scheduler 0
 constexpr int SP_MAXAT = 64;    // atoms of a moved molecule
 constexpr int SP_ET = 320;      // threads of a move's energy CTA (its stored partners: about 300 at 0.1 atoms/A^3)
-constexpr int SP_RT = 640;      // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
+constexpr int SP_RT = 1024;     // resolver CTA: warp 0 resolves, the warps of schedulers 1-3 help
 constexpr long long SP_SPIN_LIMIT = 1ll << 26;
 // words of the draws-ahead buffer (described with the draws-ahead kernels below)
 constexpr int AH_VALID = 0, AH_COUNT = 1, AH_USES = 2, AH_START = 4, AH_END = 40, AH_VALS = 80;
@@ -590,7 +590,7 @@ __device__ __forceinline__ double ldg_pinned(const double *p) {
 // and the published decision words (tag in the high half, one bit a move in the low).
 constexpr int SP_SROWS = SP_NSLOT * SP_BLK * SP_W * 8;
 constexpr int SP_STHR = SP_NSLOT * SP_BLK * 4;
-constexpr int SP_HCAP = 320;                                  // far partners a helper stages per move
+constexpr int SP_HCAP = 256;                                  // far partners a helper stages per move
 constexpr int SP_HSTAGE = SP_HCAP * 12;                       // one staged list: terms, then positions
 constexpr int SP_HOFF = SP_SROWS + SP_STHR + SP_NSLOT * 8 + SP_FR * 8;
 constexpr int SP_SHDR = SP_HOFF + SP_NH * 2 * SP_HSTAGE;
