@@ -880,22 +880,26 @@ __global__ void __launch_bounds__(SP_RT, 1) spec_resolve_kernel(SpecDev S) {
 }
 
 // ----------------------------------------------------------------- commit
-// The cycle's commits in one pass, one CTA per molecule m (visited at position km): if its move
-// was accepted, its stored energies (the later accepted writer of a shared slot wins) and its
-// coordinates; its counters either way.  The CTA that finishes last then runs the epilogue
-// (counts, step adaptation, fadds, the ran1 state), every other CTA's counts being complete.
+// The cycle's commits in one pass, one warp per molecule m (visited at position km), four
+// molecules a CTA: if its move was accepted, its stored energies (the later accepted writer of a
+// shared slot wins) and its coordinates; its counters either way.  The CTA that finishes last
+// then runs the epilogue (counts, step adaptation, fadds, the ran1 state), every other CTA's
+// counts being complete.
+constexpr int SP_CW = 4;   // molecules (warps) per CTA of the commit pass
+
 __device__ void spec_epilogue(const SpecDev &S);
 
-__global__ void __launch_bounds__(128) spec_commit_kernel(SpecDev S) {
+__global__ void __launch_bounds__(32 * SP_CW) spec_commit_kernel(SpecDev S) {
     __shared__ int s_last;
-    const int m = blockIdx.x;
-    if (!(S.flags[0] || S.flags[1])) {
+    const int lane = threadIdx.x & 31;
+    const int m = blockIdx.x * SP_CW + (threadIdx.x >> 5);
+    if (m < S.N && !(S.flags[0] || S.flags[1])) {
         const int km = S.vpos[m];
         const int am = S.acc[km];
         if (am) {
             const int nn = S.nergpairm[m];
             const size_t row = (size_t)m * S.M;
-            for (int s = 1 + threadIdx.x; s < nn; s += blockDim.x) {
+            for (int s = 1 + lane; s < nn; s += 32) {
                 const size_t e = row + s;
                 const int p = S.molergpair[e];
                 const int kp = S.vpos[p];
@@ -906,26 +910,26 @@ __global__ void __launch_bounds__(128) spec_commit_kernel(SpecDev S) {
                 S.ergpair[S.ergpairref[e] - 1] = v;
             }
             const int a0 = S.naf[m], n = S.nato[m];
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            for (int i = lane; i < n; i += 32) {
                 S.xa_w[a0 + i] = S.nx[a0 + i];
                 S.ya_w[a0 + i] = S.ny[a0 + i];
                 S.za_w[a0 + i] = S.nz[a0 + i];
                 S.pos_w[a0 + i] = S.npos[a0 + i];
             }
-            if (threadIdx.x == 0) {
+            if (lane == 0) {
                 const float4 c = S.nc[m];
                 S.xadd_w[m] = c.x;
                 S.yadd_w[m] = c.y;
                 S.zadd_w[m] = c.z;
                 S.nstepreject[m] = 0;
             }
-        } else if (threadIdx.x == 0) {
+        } else if (lane == 0) {
             const int t = S.mtype[m];
             S.nstepreject[m]++;
             if (S.stepr > 0.0f) atomicAdd(S.rej_rot + t, 1);
             if (S.stepm > 0.0f) atomicAdd(S.rej_tr + t, 1);
         }
-        if (threadIdx.x == 0) {
+        if (lane == 0) {
             if (S.trace_den) S.trace_den[km] = S.fdiff[km];
             if (S.trace_acc) S.trace_acc[km] = am;
         }
@@ -1295,7 +1299,7 @@ int epsr_molfit_spec(const epsr_box_t *box, const epsr_cells_t *cells, epsr_stor
     }
     EPSR_SMEM_OPTIN(spec_resolve_kernel);
     EPSR_TIMED("spec_resolve_kernel", s, spec_resolve_kernel<<<1, SP_RT, rsmem, s>>>(S));
-    EPSR_TIMED("spec_commit_kernel", s, spec_commit_kernel<<<N, 128, 0, s>>>(S));
+    EPSR_TIMED("spec_commit_kernel", s, spec_commit_kernel<<<(N + SP_CW - 1) / SP_CW, 32 * SP_CW, 0, s>>>(S));
     EPSR_CUDA(cudaGetLastError());
     if (ahead) EPSR_CUDA(cudaStreamWaitEvent(s, as->join, 0));
     // a cycle with a translation retry runs on the sequential kernel (no-op otherwise)
