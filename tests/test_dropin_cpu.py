@@ -43,7 +43,9 @@ def test_install_reroutes_and_uninstall_restores():
     assert set(p.orig) == set(dropin.DEFAULT_ROUTINES)
 
 
-def test_shake_and_internal_rotation_cycles_run_the_host_routine():
+def test_cycles_without_bond_lists_or_group_tables_run_the_host_routine():
+    """An intramolecular cycle when the COMMON blocks carry no bond lists, and internal
+    rotations when they carry no group tables, keep the reference's own molfit."""
     z = goldens.load("mix_small")
     calls = []
     mods = fake_common.routine_modules(z, calls)
@@ -107,3 +109,37 @@ def test_fortran_helpers():
     assert dropin._mcall_advance(2**32 + 5, 12) == 2**32 + 12
     assert dropin._mcall_advance(2**31 - 2, np.int32(-2**31 + 3)) == 2**31 + 3
     assert dropin._mcall_advance(3 * 2**32 - 1, 4) == 3 * 2**32 + 4
+
+
+@pytest.mark.parametrize("name", ["rot.npz", "dih_rot.npz"])
+def test_rotational_groups_and_dihedrals_from_common(name):
+    """The rotational groups and their dihedral angles as the drop-in hands them to the device,
+    read from COMMON blocks holding them as the reference does: the groups 0-based, each DIH
+    group's dihedral atom pairs, and the glibc cosf/sinf of each angle -- the values the
+    reference's en_dihedral computes (the golden's dih_cos/dih_sin), bit for bit."""
+    z, c, mods, _ = fake_common.common_with_groups(name)
+    p = dropin.PairPath(c, mods)
+    nrf, nrl, axis, first, last, atoms = p._rot_groups()
+    for got, want in ((nrf, z["rot_nrf"]), (nrl, z["rot_nrl"]), (axis, z["rot_axis"]), (first, z["rot_first"]),
+                      (last, z["rot_last"]), (atoms, z["rot_atoms"])):
+        assert np.array_equal(got, want)
+    d = p._dihedrals()
+    if name == "rot.npz":
+        assert d is None
+        return
+    assert np.array_equal(d["grp_dih0"], z["dih_grp0"]) and np.array_equal(d["grp_isdih"], z["dih_isdih"])
+    assert np.array_equal(d["dih_atoms"], z["dih_atoms"])
+    assert np.array_equal(d["dih_cos"].view(np.uint32), z["dih_cos"].view(np.uint32))
+    assert np.array_equal(d["dih_sin"].view(np.uint32), z["dih_sin"].view(np.uint32))
+    assert d["tempdih"] == z["tempdih"]
+
+
+def test_groups_of_another_type_run_the_host_routine():
+    """A rotational group whose type is neither ROT nor DIH keeps the reference's own molfit."""
+    z, c, mods, calls = fake_common.common_with_groups("rot.npz")
+    c.molecom_mod.rotgrp[3] = "XYZ"
+    p = dropin.PairPath(c, mods)
+    assert p._rot_groups() is None
+    p.install()
+    mods["molfit"].molfit(f32(0), f32(0), 1, 100, 1, 0)
+    assert calls == ["host:molfit"]

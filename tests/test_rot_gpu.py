@@ -57,21 +57,6 @@ def test_rotation_cycles_device_match_reference(name):
         assert np.array_equal(m["ran1"].iv, z[q + "ran1_after_iv"])
 
 
-class _Aliased:
-    """The rot golden seen under the key names the COMMON stand-ins read."""
-    ALIAS = {"in_wholerot": "wholerot_in", "in_wholetrans": "wholetrans_in", "in_eintra": "eintra"}
-
-    def __init__(self, z):
-        self.z = z
-
-    def __getitem__(self, k):
-        return self.z[self.ALIAS.get(k, k)]
-
-    @property
-    def files(self):
-        return list(self.z.files) + list(self.ALIAS)
-
-
 @pytest.mark.parametrize("name", ["rot.npz", "dih_rot.npz"])
 def test_rotation_dropin_matches_reference(name):
     """PairPath.molfit on COMMON stand-ins that carry the reference's rotational groups
@@ -91,66 +76,11 @@ def test_shake_rotation_dropin_matches_reference(name):
 
 
 def _rotation_dropin(name, shake):
-    from types import SimpleNamespace as NS
-
     from epsr_python_translation_b200 import dropin
     from tests import fake_common
-    z = np.load(__import__("tests.goldens", fromlist=["GOLDEN"]).GOLDEN + "/" + name)
-    p = _Aliased(z)
-    calls = []
-    mods = fake_common.routine_modules(p, calls)
-    c = fake_common.common_from_golden(p)
-    mc, cc, pp, erd, r = c.molecom, c.clustercom, c.potential_par, c.ergpairreference, c.ran1com
-    natom, nmol, ntype = mc.natom, cc.nmol, mc.ntype
-    npairs, npt, nmt = mc.npairs, c.epsr16.npt, int(cc.nmoltype)
-    fa = fake_common.fa
-    iab = z["iabond"]
-    mb = iab.shape[1]
-    mc.nbond = fa(natom, dtype=np.int32)
-    mc.nbond[1:] = z["nbond"]
-    mc.iabond = fa(natom, mb, dtype=np.int32)
-    mc.iabond[1:, 1:] = iab + 1
-    mc.tbond = fa(natom, mb)
-    mc.tbond[1:, 1:] = z["tbond"]
-    mc.imageatom, mc.qtype = fa(natom, dtype=np.int32), fa(natom, dtype=np.int32)
-    mc.amassa, mc.amassr = fa(ntype), fa(npairs)
-    mc.amassa[1:], mc.amassr[1:] = z["amassa"], z["amassr"]
-    sc = z["scal"]
-    mc.sizefactor, mc.tempb, mc.tempangreq, mc.tempangwt = f32(sc[1]), f32(sc[2]), f32(sc[3]), f32(sc[3])
-    mc.refine_intra, mc.refine_intra_fac, mc.stepri = False, f32(0.0), f32(1.0)
-    mpz = pp.xavs.shape[0] - 1
-    pp.xav, pp.xav1 = fa(mpz, npairs), fa(mpz, npairs)
-    pp.xav[: npt + 1, 1:], pp.xav1[: npt + 1, 1:] = z["xav"].T, z["xav1"].T
-    cc.internrot[1:] = z["internrot_in"]
-    if shake:
-        mc.stepmi = f32(z["stepmi"])
-        cc.interntrans[1:] = z["interntrans_in"]
-    # the rotational groups, 1-based as the reference holds them
-    ng = z["rot_first"].size
-    cc.ngrot[1:] = z["ngrot"]
-    cc.nrf, cc.nrl = fa(nmol, dtype=np.int32), fa(nmol, dtype=np.int32)
-    cc.nrf[1:], cc.nrl[1:] = z["rot_nrf"] + 1, z["rot_nrl"] + 1
-    lab = fa(ng, 2, dtype=np.int32)
-    lab[1:, 1:] = z["rot_axis"] + 1
-    rotf, rotl = fa(ng, dtype=np.int32), fa(ng, dtype=np.int32)
-    rotf[1:], rotl[1:] = z["rot_first"] + 1, z["rot_last"] + 1
-    labrot = fa(z["rot_atoms"].size, dtype=np.int32)
-    labrot[1:] = z["rot_atoms"] + 1
-    dih = "dih_cos" in z.files
-    c.molecom_mod = NS(coarsegraining=False, natomsphere=c.molecom_mod.natomsphere, ngrrot=ng,
-                       rotgrp=np.array(["   "] + ["DIH" if dih else "ROT"] * ng, dtype=object), labaxi=lab,
-                       rotf=rotf, rotl=rotl, labrot=labrot, nrottot=int(z["rot_atoms"].size))
-    mc.ndihedralang = fa(ng, dtype=np.int32)
-    if dih:
-        # one dihedral angle per group, as the reference held them (1.0 and 2.5 rad alternately)
-        mc.ndihedralang[1:] = np.diff(z["dih_grp0"])
-        mc.labrotdih = np.zeros((3, 2, ng + 1), np.int32)
-        mc.dihedralang = np.zeros((2, ng + 1), f32)
-        for ir in range(1, ng + 1):
-            mc.labrotdih[1, 1, ir], mc.labrotdih[2, 1, ir] = z["dih_atoms"][ir - 1] + 1
-            mc.dihedralang[1, ir] = f32(1.0) if (ir - 1) % 2 == 0 else f32(2.5)
-        mc.tempdihreq = mc.tempdihwt = f32(1.0)
-        mc.tempdih = f32(f32(mc.tempdihwt) * f32(mc.tempb))
+    z, c, mods, calls = fake_common.common_with_groups(name, shake)
+    mc, cc, erd, r = c.molecom, c.clustercom, c.ergpairreference, c.ran1com
+    nmol, nmt = cc.nmol, int(cc.nmoltype)
     path = dropin.PairPath(c, mods, strict=True)
     path.install(dropin.ROUTINES)
     mods["cellneighbourlist"].initialise_cellneighbourlist(int(z["in_nmolcell"]), cc.xadd, cc.yadd, cc.zadd, nmol,
