@@ -157,6 +157,29 @@ def cell_list(box, nmolcell, rmax):
     return out
 
 
+def cells_from_arrays(dims, cell_start, cell_mols, molcellno, offsets, nnbrefmax):
+    """A cell list given as arrays (the reference's own, read from its COMMON block): dims =
+    (ncelldiva, ncelldivb, ncelldivc, ncell, ncellneighb, maxcellno), cell_start (ncell+1),
+    cell_mols (0-based molecules in cell order), molcellno (1-based), offsets (ncellneighb x 3)."""
+    ncell, nb = int(dims[3]), int(dims[4])
+    noff = max(ncell, nb)
+    out = dict(molcellno=np.ascontiguousarray(molcellno, np.int32), cell_start=np.ascontiguousarray(cell_start, np.int32),
+               cell_mols=np.ascontiguousarray(cell_mols, np.int32), ia_off=np.zeros(noff, np.int32),
+               ib_off=np.zeros(noff, np.int32), ic_off=np.zeros(noff, np.int32))
+    for i, k in enumerate(("ia_off", "ib_off", "ic_off")):
+        out[k][:nb] = np.asarray(offsets)[:, i]
+    c = CellsC()
+    for k in ("molcellno", "cell_start", "cell_mols", "ia_off", "ib_off", "ic_off"):
+        setattr(c, k, ptr(out[k]))
+    c.ncelldiva, c.ncelldivb, c.ncelldivc, c.ncell, c.ncellneighb, c.maxcellno = (int(v) for v in dims)
+    out["_keep"] = [out[k] for k in ("molcellno", "cell_start", "cell_mols", "ia_off", "ib_off", "ic_off")]
+    out["_c"] = c
+    out["nnbrefmax"] = int(nnbrefmax)
+    out.update(ncelldiva=c.ncelldiva, ncelldivb=c.ncelldivb, ncelldivc=c.ncelldivc, ncell=ncell, ncellneighb=nb,
+               maxcellno=c.maxcellno)
+    return out
+
+
 def region(cells, ic):
     nb = np.zeros(max(cells["nnbrefmax"], 1), dtype=np.int32)
     n = lib().oracle_region(C.byref(cells["_c"]), ic, ptr(nb))

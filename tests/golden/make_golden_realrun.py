@@ -1,0 +1,211 @@
+"""Golden vectors taken from inside the reference's own epsr loop on its shipped run folder
+(EPSR-test: 200 DMSO + 400 water with the DMSO methyl groups as ROT groups), made by running
+the reference translation (epsr26) itself.
+
+    EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_realrun.py
+
+The run folder is copied to a scratch directory and the unchanged epsr program runs on it
+(runepsr17 epsr_standalone_rev3.py:1235: the files read, the potentials built, the cell list,
+fmolec1, then molfit ntimes times).  Its first two molfit calls are captured through the
+module attribute the loop calls (molfit.molfit, as the reference's tracer reroutes routines):
+the run folder's nisum starts at intra, so the first is the intramolecular cycle, each
+molecule's atoms moved and then its methyl groups rotated (molfit.py:124-267), and the second
+a whole-molecule cycle (:268-448).  For each, everything that call reads is written before it and everything it
+changes after it (every array copied, the COMMON arrays being updated in place): the box as
+the COMMON blocks hold it (read by the drop-in's own
+box_from_common), the cell list as the loop built it, the pair store, the step arrays and
+counters, the rotational groups and the intramolecular model, the ran1 state, the call's
+arguments and results, and the cosines molfit drew.  The run is stopped after the second
+captured call.  tests/golden/realrun.npz receives the two calls under the prefixes k0_, k1_.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, HERE)
+
+import refstate  # noqa: E402
+
+f32 = np.float32
+REF = refstate.reference_root()
+
+
+class _Stop(Exception):
+    pass
+
+
+def _fortran_slice(a, *dims):
+    """The 1-based part of a reference array, 0-based, as a copy."""
+    return np.array(np.asarray(a)[tuple(slice(1, d + 1) for d in dims)])
+
+
+def snapshot(common, mods, out, q):
+    """Everything one molfit call reads from the COMMON blocks, under prefix q."""
+    from epsr_python_translation_b200 import dropin
+    p = dropin.PairPath(common, mods)
+    box = p.box_from_common()
+    for k, v in box.__dict__.items():
+        if isinstance(v, np.ndarray):
+            out[q + "box_" + k] = v.copy()
+        else:
+            out[q + "box_" + k] = np.array(v)
+    cc, mc, e16, erd, cnl = common.clustercom, common.molecom, common.epsr16, common.ergpairreference, \
+        common.cellneighbourlist
+    nmol, nmt = int(cc.nmol), int(cc.nmoltype)
+    # the pair store
+    M = int(erd.nnbrefmax)
+    out[q + "st_nnbrefmax"], out[q + "st_nergpair"] = np.int32(M), np.int32(erd.nergpair)
+    out[q + "st_nergpairm"] = np.array(erd.nergpairm[1:nmol + 1], np.int32)
+    out[q + "st_molergpair"] = _fortran_slice(erd.molergpair, M, nmol).T.astype(np.int32) - 1
+    out[q + "st_ergpairref"] = _fortran_slice(erd.ergpairref, M, nmol).T.astype(np.int32)
+    out[q + "st_ergpair"] = np.array(erd.ergpair[1:int(erd.nergpair) + 1], f32)
+    # the cell list as the loop built it (cells in reference order, 1-based molecules)
+    ncell = int(cnl.ncell)
+    n_in = np.array(cnl.nmolsincell[1:ncell + 1], np.int32)
+    mols = [np.array(cnl.molsincell[1:n_in[c] + 1, c + 1], np.int32) - 1 for c in range(ncell)]
+    out[q + "cl_dims"] = np.array([cnl.ncelldiva, cnl.ncelldivb, cnl.ncelldivc, ncell, cnl.ncellneighb,
+                                   cnl.maxcellno], np.int32)
+    out[q + "cl_cell_start"] = np.concatenate([[0], np.cumsum(n_in)]).astype(np.int32)
+    out[q + "cl_cell_mols"] = np.concatenate(mols).astype(np.int32) if mols else np.zeros(0, np.int32)
+    out[q + "cl_molcellno"] = np.array(cnl.molcellno[1:nmol + 1], np.int32)
+    nb = int(cnl.ncellneighb)
+    out[q + "cl_offsets"] = np.stack([np.array(getattr(cnl, k)[1:nb + 1], np.int32)
+                                      for k in ("iacellneighb", "ibcellneighb", "iccellneighb")], 1)
+    # step arrays, counters, parameters
+    for k in ("wholerot", "wholetrans", "internrot", "interntrans"):
+        out[q + k] = np.array(getattr(cc, k)[1:nmt + 1], f32)
+    out[q + "nstepreject"] = np.array(cc.nstepreject[1:nmol + 1], np.int32)
+    out[q + "ngrot"] = np.array(cc.ngrot[1:nmol + 1], np.int32)
+    out[q + "par"] = np.array([e16.rejrate, mc.stepr, mc.stepm, mc.stepri, mc.stepmi], f32)
+    g = p._rot_groups()
+    if g:
+        for k, v in zip(("rot_nrf", "rot_nrl", "rot_axis", "rot_first", "rot_last", "rot_atoms"), g):
+            out[q + k] = np.array(v, np.int32)
+    for k, v in refstate.ran1_state().items():
+        out[q + "ran1_before_" + k] = v
+
+
+def intra_snapshot(common, out, q):
+    """The intramolecular model en_change_intra reads (molecom bond lists, masses, the intra
+    reference potential), as the drop-in hands it to the device."""
+    mc, cc, pp, e16 = common.molecom, common.clustercom, common.potential_par, common.epsr16
+    natom, ntype, npairs = int(mc.natom), int(mc.ntype), int(mc.npairs)
+    nb = np.array(mc.nbond[1:natom + 1], np.int32)
+    mb = max(1, int(nb.max()) if natom else 1)
+    ld = int(e16.npt) + 1
+    out[q + "in_nbond"] = nb
+    out[q + "in_iabond"] = np.array(mc.iabond)[1:natom + 1, 1:mb + 1].astype(np.int32) - 1
+    out[q + "in_tbond"] = np.array(mc.tbond)[1:natom + 1, 1:mb + 1].astype(f32)
+    out[q + "in_imageatom"] = np.array(mc.imageatom[1:natom + 1], np.int32) - 1
+    out[q + "in_qtype"] = np.array(mc.qtype[1:natom + 1], np.int32)
+    out[q + "in_amassa"] = np.array(mc.amassa[1:ntype + 1], f32)
+    out[q + "in_amassr"] = np.array(mc.amassr[1:npairs + 1], f32)
+    out[q + "in_xav"] = np.ascontiguousarray(np.array(pp.xav)[:ld, 1:npairs + 1].T, f32)
+    out[q + "in_xav1"] = np.ascontiguousarray(np.array(pp.xav1)[:ld, 1:npairs + 1].T, f32)
+    out[q + "in_scal"] = np.array([f32(e16.cellst) / f32(mc.dmaxmol), mc.sizefactor, mc.tempb, mc.tempang, mc.simt,
+                                   float(bool(getattr(mc, "refine_intra", False))),
+                                   getattr(mc, "refine_intra_fac", 0.0), mc.tempdih], f32)
+
+
+def after(common, out, q, result, cos):
+    cc, erd = common.clustercom, common.ergpairreference
+    nmol, nmt = int(cc.nmol), int(cc.nmoltype)
+    mc = common.molecom
+    natom = int(mc.natom)
+    for k, src, n in (("xa", mc.xa, natom), ("ya", mc.ya, natom), ("za", mc.za, natom), ("xadd", cc.xadd, nmol),
+                      ("yadd", cc.yadd, nmol), ("zadd", cc.zadd, nmol)):
+        out[q + "after_" + k] = np.array(src[1:n + 1], f32)
+    out[q + "after_ergpair"] = np.array(erd.ergpair[1:int(erd.nergpair) + 1], f32)
+    for k in ("wholerot", "wholetrans", "internrot", "interntrans"):
+        out[q + "after_" + k] = np.array(getattr(cc, k)[1:nmt + 1], f32)
+    for k in ("nwhole", "nmovem", "ninter", "nmovei"):
+        out[q + "after_" + k] = np.array(getattr(cc, k)[1:3, 1:nmt + 1], np.int32)
+    out[q + "after_ergold1"] = f32(erd.ergold[1]) if erd.ergold is not None else f32(0.0)
+    out[q + "after_nstepreject"] = np.array(cc.nstepreject[1:nmol + 1], np.int32)
+    out[q + "result"] = np.array([result[0], result[1]], f32)
+    out[q + "result_nisum"] = np.int32(result[2])
+    out[q + "cos"] = np.array(cos, f32)
+    for k, v in refstate.ran1_state().items():
+        out[q + "ran1_after_" + k] = v
+
+
+def main():
+    src = os.path.join(REF, "EPSR-test")
+    work = tempfile.mkdtemp(prefix="epsr_realrun_")
+    run = os.path.join(work, "EPSR-test")
+    shutil.copytree(src, run)
+    common, _ = refstate.load_reference(os.path.join(REF, "src"))
+    import importlib
+    mods = {"cellneighbourlist": importlib.import_module("epsr26.library.cellneighbourlist"),
+            "ato_manipulation_rev4": importlib.import_module("epsr26.library.ato_manipulation_rev4"),
+            "molfit": importlib.import_module("epsr26.library.molfit")}
+    for name in ("molecom", "clustercom", "epsr16", "potential_par", "lattice", "ran1com", "cellneighbourlist",
+                 "ergpairreference", "molecom_mod", "threebody_mod", "coordconstraints_mod", "containerforces_mod"):
+        importlib.import_module("epsr26.common." + name)
+    common = importlib.import_module("epsr26.common")
+    from epsr26.programs import run_program
+    molfit = mods["molfit"]
+    orig, orig_cos = molfit.molfit, molfit.cosf
+    out, state = {}, {"n": 0, "taken": 0}
+    rec = []
+
+    def cos_rec(x):
+        v = orig_cos(x)
+        rec.append(v)
+        return v
+
+    def wrapped(fadds, faddbs, nisum, intra, rotfreq, ireset):
+        state["n"] += 1
+        rot = nisum >= intra or nisum == rotfreq * (nisum // rotfreq)
+        take = state["taken"] < 2
+        if not take:
+            return orig(fadds, faddbs, nisum, intra, rotfreq, ireset)
+        q = "k%d_" % state["taken"]
+        snapshot(common, mods, out, q)
+        intra_snapshot(common, out, q)
+        erd = common.ergpairreference
+        out[q + "ergold1"] = f32(erd.ergold[1]) if erd.ergold is not None else f32(0.0)
+        out[q + "args"] = np.array([fadds, faddbs], f32)
+        out[q + "args_int"] = np.array([nisum, intra, rotfreq, ireset, state["n"]], np.int32)
+        rec.clear()
+        molfit.cosf = cos_rec
+        try:
+            r = orig(fadds, faddbs, nisum, intra, rotfreq, ireset)
+        finally:
+            molfit.cosf = orig_cos
+        after(common, out, q, r, rec)
+        print(f"captured molfit call {state['n']} (nisum {nisum}, intra {intra}, rotations {rot}) as {q}", flush=True)
+        state["taken"] += 1
+        if state["taken"] == 2:
+            raise _Stop()
+        return r
+
+    molfit.molfit = wrapped
+    cwd = os.getcwd()
+    os.chdir(run)
+    try:
+        run_program("epsr", ["./", "epsr", "200DMSO400Water.EPSR.inp"])
+    except _Stop:
+        pass
+    finally:
+        os.chdir(cwd)
+        molfit.molfit = orig
+        shutil.rmtree(work, ignore_errors=True)
+    if state["taken"] < 2:
+        raise SystemExit("the run ended before two molfit calls")
+    path = os.path.join(HERE, "realrun.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()

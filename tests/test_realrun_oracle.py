@@ -1,0 +1,98 @@
+"""The oracle against the reference's own epsr loop on its shipped run folder (EPSR-test: 200
+DMSO + 400 water, the DMSO methyl groups as ROT groups, the run folder's potentials and
+intramolecular model), tests/golden/realrun.npz made by tests/golden/make_golden_realrun.py:
+the loop's first molfit call (the intramolecular cycle: atom moves, then the methyl rotations
+tested with the intermolecular change, molfit.py:124-267) and its second (a whole-molecule
+cycle, :268-448) replayed from the state the loop held at each call, bit for bit --
+coordinates, stored energies, step sizes, counters, fadds/faddbs and the ran1 stream."""
+
+import os
+
+import numpy as np
+import pytest
+
+from epsr_python_translation_b200.box import BoxArrays, Ran1State
+from oracle import oracle
+from tests.goldens import GOLDEN, assert_bits_equal
+
+f32 = np.float32
+PATH = os.path.join(GOLDEN, "realrun.npz")
+
+
+def _call(z, q):
+    """The box, store, cells, MC parameters and intramolecular model of captured call q."""
+    kw = {}
+    for k in BoxArrays.__dataclass_fields__:
+        v = z[q + "box_" + k]
+        kw[k] = v if v.ndim else v.item()
+    box = BoxArrays(**kw)
+    M, n = int(z[q + "st_nnbrefmax"]), int(z[q + "st_nergpair"])
+    st = dict(nnbrefmax=M, nergpair=n, nergpairm=np.array(z[q + "st_nergpairm"], np.int32),
+              molergpair=np.ascontiguousarray(z[q + "st_molergpair"], np.int32).reshape(-1),
+              ergpairref=np.ascontiguousarray(z[q + "st_ergpairref"], np.int32).reshape(-1),
+              ergpair=np.array(z[q + "st_ergpair"], f32))
+    cells = oracle.cells_from_arrays(z[q + "cl_dims"], z[q + "cl_cell_start"], z[q + "cl_cell_mols"],
+                                     z[q + "cl_molcellno"], z[q + "cl_offsets"], M)
+    par = z[q + "par"]
+    mc = dict(rejrate=f32(par[0]), stepr=f32(par[1]), stepm=f32(par[2]), ireset=int(z[q + "args_int"][3]),
+              wholerot=np.array(z[q + "wholerot"], f32), wholetrans=np.array(z[q + "wholetrans"], f32),
+              internrot=np.array(z[q + "internrot"], f32), interntrans=np.array(z[q + "interntrans"], f32),
+              ngrot=np.array(z[q + "ngrot"], np.int32), nstepreject=np.array(z[q + "nstepreject"], np.int32))
+    sc = z[q + "in_scal"]
+    model = dict(nbond=z[q + "in_nbond"], iabond=z[q + "in_iabond"], tbond=z[q + "in_tbond"],
+                 imageatom=z[q + "in_imageatom"], qtype=z[q + "in_qtype"], amassa=z[q + "in_amassa"],
+                 amassr=z[q + "in_amassr"], xav=z[q + "in_xav"], xav1=z[q + "in_xav1"], stepcl=sc[0], sizefactor=sc[1],
+                 tempb=sc[2], tempang=sc[3], simt=sc[4], refine_intra=bool(sc[5]), refine_intra_fac=sc[6],
+                 ngrot=z[q + "ngrot"])
+    rot = dict(model=model, nrf=z[q + "rot_nrf"], nrl=z[q + "rot_nrl"], axis=z[q + "rot_axis"].reshape(-1),
+               first=z[q + "rot_first"], last=z[q + "rot_last"], atoms=z[q + "rot_atoms"], stepri=f32(par[3]),
+               rotcycle=1)
+    return box, st, cells, mc, rot
+
+
+def _check_after(z, q, box, st, mc, fadds, faddbs, ran1, ninter=None, nmovei=None):
+    for k in ("xa", "ya", "za", "xadd", "yadd", "zadd"):
+        assert_bits_equal(getattr(box, k), z[q + "after_" + k], q + k)
+    assert_bits_equal(st["ergpair"], z[q + "after_ergpair"], q + "ergpair")
+    for k in ("wholerot", "wholetrans", "internrot", "interntrans"):
+        assert_bits_equal(mc[k], z[q + "after_" + k], q + k)
+    assert np.array_equal(mc["nwhole"], z[q + "after_nwhole"].reshape(-1))
+    assert np.array_equal(mc["nmovem"], z[q + "after_nmovem"].reshape(-1))
+    if ninter is not None:
+        assert np.array_equal(ninter, z[q + "after_ninter"].reshape(-1))
+    if nmovei is not None:
+        assert np.array_equal(nmovei, z[q + "after_nmovei"].reshape(-1))
+    assert np.array_equal(mc["nstepreject"], z[q + "after_nstepreject"])
+    assert_bits_equal(np.array([fadds, faddbs], f32), z[q + "result"], q + "fadds, faddbs")
+    assert (ran1.idum, ran1.iy, ran1.mcall) == (int(z[q + "ran1_after_idum"]), int(z[q + "ran1_after_iy"]),
+                                                 int(z[q + "ran1_after_mcall"]))
+    assert np.array_equal(ran1.iv, z[q + "ran1_after_iv"])
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_intramolecular_cycle_with_rotations_oracle_matches_reference():
+    z = np.load(PATH)
+    q = "k0_"
+    nisum, intra = (int(v) for v in z[q + "args_int"][:2])
+    assert nisum >= intra                                   # the loop's first call: the intramolecular branch
+    box, st, _, mc, rot = _call(z, q)
+    assert int(np.max(mc["ngrot"])) > 0
+    fadds, faddbs = (f32(v) for v in z[q + "args"])
+    fadds, faddbs, nmovei, ninter, _, ran1, cosv = oracle.molfit_shake_rot(
+        box, st, mc, rot, f32(z[q + "par"][4]), Ran1State.from_golden(z, q + "ran1_before_"),
+        fadds, faddbs, f32(z[q + "ergold1"]))
+    assert_bits_equal(cosv, z[q + "cos"], "rotati cosines")
+    _check_after(z, q, box, st, mc, fadds, faddbs, ran1, ninter=ninter, nmovei=nmovei)
+    assert ninter[0] > 0 and nmovei.sum() > 0
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_whole_molecule_cycle_oracle_matches_reference():
+    z = np.load(PATH)
+    q = "k1_"
+    box, st, cells, mc, _ = _call(z, q)
+    fadds = f32(z[q + "args"][0])
+    fadds, tr, ran1 = oracle.molfit(box, cells, st, mc, Ran1State.from_golden(z, q + "ran1_before_"), fadds)
+    assert_bits_equal(tr["cosv"], z[q + "cos"], "rotatm cosines")
+    # no rotation this cycle: faddbs is the argument, unchanged by the oracle's whole-molecule cycle
+    _check_after(z, q, box, st, mc, fadds, f32(z[q + "args"][1]) + f32(0.0) / f32(box.nmol), ran1)
