@@ -43,6 +43,27 @@ class _Stop(Exception):
     pass
 
 
+# the molfit calls captured (1-based, in the loop's order): the first intramolecular cycle, the
+# whole-molecule cycle after it, and the first whole-molecule cycle with internal rotations
+# (nisum 5 = rotfreq), which comes after the first potential refinement
+CAPTURE = (1, 2, 6)
+NITER = 2
+
+
+def prepare_run(run):
+    """The run folder as the captures need it: the input file's niter raised to NITER, so
+    that the loop refines the potential once and reaches the sixth molfit call."""
+    import re
+    inp = os.path.join(run, "200DMSO400Water.EPSR.inp")
+    with open(inp) as f:
+        text = f.read()
+    text, n = re.subn(r"^(niter\s+)\d+", lambda m: m.group(1) + str(NITER), text, count=1, flags=re.M)
+    if n != 1:
+        raise SystemExit("no niter line in " + inp)
+    with open(inp, "w") as f:
+        f.write(text)
+
+
 def _fortran_slice(a, *dims):
     """The 1-based part of a reference array, 0-based, as a copy."""
     return np.array(np.asarray(a)[tuple(slice(1, d + 1) for d in dims)])
@@ -143,6 +164,7 @@ def main():
     work = tempfile.mkdtemp(prefix="epsr_realrun_")
     run = os.path.join(work, "EPSR-test")
     shutil.copytree(src, run)
+    prepare_run(run)
     common, _ = refstate.load_reference(os.path.join(REF, "src"))
     import importlib
     mods = {"cellneighbourlist": importlib.import_module("epsr26.library.cellneighbourlist"),
@@ -166,8 +188,7 @@ def main():
     def wrapped(fadds, faddbs, nisum, intra, rotfreq, ireset):
         state["n"] += 1
         rot = nisum >= intra or nisum == rotfreq * (nisum // rotfreq)
-        take = state["taken"] < 2
-        if not take:
+        if state["n"] not in CAPTURE:
             return orig(fadds, faddbs, nisum, intra, rotfreq, ireset)
         q = "k%d_" % state["taken"]
         snapshot(common, mods, out, q)
@@ -185,7 +206,7 @@ def main():
         after(common, out, q, r, rec)
         print(f"captured molfit call {state['n']} (nisum {nisum}, intra {intra}, rotations {rot}) as {q}", flush=True)
         state["taken"] += 1
-        if state["taken"] == 2:
+        if state["taken"] == len(CAPTURE):
             raise _Stop()
         return r
 
@@ -200,8 +221,8 @@ def main():
         os.chdir(cwd)
         molfit.molfit = orig
         shutil.rmtree(work, ignore_errors=True)
-    if state["taken"] < 2:
-        raise SystemExit("the run ended before two molfit calls")
+    if state["taken"] < len(CAPTURE):
+        raise SystemExit("the run ended before molfit call %d" % CAPTURE[-1])
     path = os.path.join(HERE, "realrun.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

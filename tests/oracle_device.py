@@ -1,0 +1,202 @@
+"""A stand-in for the device layer of the drop-in (device.DeviceBox, intra.IntraModel) whose
+every routine is the oracle's C restatement on the host: test infrastructure, so that the
+drop-in's own host side -- reading the COMMON blocks, the cell list and pair store written
+back into them, the routing of molfit by nisum, the ran1 state in and out, the step arrays
+and counters written back -- runs inside the reference's unchanged epsr loop on a machine
+without a GPU.  Only the routines of the cell list, fmolec1 and molfit (the intramolecular
+cycle with rotational groups included) are provided; the device layer itself is checked
+against the same oracle by the GPU tests.
+
+The state the device would hold (coordinates, cells, pair store, MC arrays) is held here as
+NumPy arrays and CPU tensors with the device layer's names and layouts (the drop-in reads and
+writes the store tensors directly)."""
+
+from __future__ import annotations
+
+import copy
+import types
+
+import numpy as np
+import torch
+
+from epsr_python_translation_b200.box import BoxArrays, Ran1State
+from oracle import oracle
+
+f32 = np.float32
+COORDS = ("xa", "ya", "za", "xadd", "yadd", "zadd")
+
+
+def _copy_box(b: BoxArrays) -> BoxArrays:
+    return copy.deepcopy(b)
+
+
+class OracleDeviceBox:
+    """device.DeviceBox's interface over the oracle (see the module docstring).  ``journal``:
+    when a list, every box made appends "box" and then each routine it runs to it."""
+
+    journal = None
+
+    def __init__(self, b, device=None):
+        self.dev = "cpu"
+        self.host = b
+        self.box = _copy_box(b)
+        self.cells = None
+        self.nnbrefmax = 0
+        self.cmc = None
+        self.r = None
+        self._cos = None
+        self.calls = [] if OracleDeviceBox.journal is None else OracleDeviceBox.journal
+        self.calls.append("box")
+
+    # ------------------------------------------------------------------ state in and out
+    def upload(self, b):
+        self.host = b
+        self.box = _copy_box(b)
+
+    def upload_coords(self, xa, ya, za, xadd, yadd, zadd):
+        for k, v in zip(COORDS, (xa, ya, za, xadd, yadd, zadd)):
+            setattr(self.box, k, np.array(v, f32))
+
+    def download_coords(self, stream_only=False):
+        return {k: np.array(getattr(self.box, k), f32) for k in COORDS}
+
+    def ran1_tensor(self, st: Ran1State):
+        return torch.from_numpy(st.as_array().copy())
+
+    # ------------------------------------------------------------------ cells
+    def cell_list(self, nmolcell, rmax):
+        self.calls.append("cell_list")
+        self.cells = oracle.cell_list(self.box, int(nmolcell), f32(rmax))
+        self.nnbrefmax = int(self.cells["nnbrefmax"])
+        return self.cells
+
+    def download_cells(self):
+        c = self.cells
+        nb = int(c["ncellneighb"])
+        off = np.stack([np.asarray(c[k])[:nb] for k in ("ia_off", "ib_off", "ic_off")], 1).astype(np.int32)
+        return dict(ncelldiva=c["ncelldiva"], ncelldivb=c["ncelldivb"], ncelldivc=c["ncelldivc"], ncell=c["ncell"],
+                    ncellneighb=nb, maxcellno=c["maxcellno"], molcellno=np.array(c["molcellno"]),
+                    cell_start=np.array(c["cell_start"]), cell_mols=np.array(c["cell_mols"]), offsets=off,
+                    nnbrefmax=self.nnbrefmax)
+
+    # ------------------------------------------------------------------ pair store
+    def fmolec1(self, eintra, strict=True, capacity=None):
+        self.calls.append("fmolec1")
+        st = oracle.fmolec1(self.box, self.cells, np.asarray(eintra, f32), capacity)
+        self.s_nergpairm = torch.from_numpy(np.ascontiguousarray(st["nergpairm"], np.int32))
+        self.s_mol = torch.from_numpy(np.ascontiguousarray(st["molergpair"], np.int32).reshape(-1))
+        self.s_ref = torch.from_numpy(np.ascontiguousarray(st["ergpairref"], np.int32).reshape(-1))
+        self.s_erg = torch.from_numpy(np.ascontiguousarray(st["ergpair"], f32))
+        self.s_n = torch.tensor([int(st["nergpair"])], dtype=torch.int32)
+        return f32(st["ftest"]), f32(st["ftestb"])
+
+    def _store(self):
+        """The store as the oracle takes it: views of the tensors, so its updates land there."""
+        nm = self.host.nmol * self.nnbrefmax
+        return dict(nnbrefmax=self.nnbrefmax, nergpair=int(self.s_n[0]), nergpairm=self.s_nergpairm.numpy(),
+                    molergpair=self.s_mol.numpy()[:nm], ergpairref=self.s_ref.numpy()[:nm], ergpair=self.s_erg.numpy())
+
+    def download_store(self):
+        M, n = self.nnbrefmax, int(self.s_n[0])
+        nm = self.host.nmol * M
+        return dict(nnbrefmax=M, nergpair=n, nergpairm=self.s_nergpairm.numpy().copy(),
+                    molergpair=self.s_mol.numpy()[:nm].reshape(-1, M).copy(),
+                    ergpairref=self.s_ref.numpy()[:nm].reshape(-1, M).copy(), ergpair=self.s_erg.numpy()[:n].copy())
+
+    # ------------------------------------------------------------------ molfit
+    def mc_setup(self, *, rejrate, stepr, stepm, wholerot, wholetrans, internrot=None, interntrans=None,
+                 nstepreject=None, ran1=None, trstepmax, trstepmin, ireset=0, fadds=0.0):
+        nmt = self.host.nmoltype
+        self.mc = dict(rejrate=f32(rejrate), stepr=f32(stepr), stepm=f32(stepm), ireset=int(ireset),
+                       wholerot=np.array(wholerot, f32), wholetrans=np.array(wholetrans, f32),
+                       internrot=np.array(internrot, f32), interntrans=np.array(interntrans, f32),
+                       nstepreject=np.array(nstepreject, np.int32), nwhole=np.zeros(2 * nmt, np.int32),
+                       nmovem=np.zeros(2 * nmt, np.int32))
+        self.m_fadds = f32(fadds)
+        self.m_ran1 = self.ran1_tensor(ran1 or Ran1State())
+        self.r = None
+        self.cmc = types.SimpleNamespace(ran1=None, cos_override=None)
+        return self.cmc
+
+    def set_rotations(self, intra_model, nrf, nrl, axis, first, last, atoms, stepri=1.0, faddbs=0.0):
+        self.r = dict(model=intra_model.m, nrf=np.asarray(nrf, np.int32), nrl=np.asarray(nrl, np.int32),
+                      axis=np.asarray(axis, np.int32).reshape(-1), first=np.asarray(first, np.int32),
+                      last=np.asarray(last, np.int32), atoms=np.asarray(atoms, np.int32), stepri=f32(stepri),
+                      faddbs=f32(faddbs))
+        self.mc["ngrot"] = np.asarray(intra_model.m["ngrot"], np.int32)
+        self.m_ninter = torch.zeros(2 * self.host.nmoltype, dtype=torch.int32)
+        self.m_faddbs = torch.tensor([float(f32(faddbs))], dtype=torch.float32)
+
+    def set_cos_override(self, cos_override=None):
+        if cos_override is not None:
+            raise NotImplementedError("the oracle stand-in draws its own cosines")
+
+    def _ran1(self):
+        return Ran1State.from_array(self.m_ran1.numpy())
+
+    def _ran1_back(self, st):
+        self.m_ran1.copy_(torch.from_numpy(st.as_array()))
+
+    def molfit(self, strict=True, cos_override=None, rotcycle=True):
+        self.calls.append("molfit")
+        self.set_cos_override(cos_override)
+        rot = None
+        if self.r is not None:
+            rot = dict(self.r, rotcycle=1 if rotcycle else 0)
+        fa, tr, ran1 = oracle.molfit(self.box, self.cells, self._store(), self.mc, self._ran1(), self.m_fadds,
+                                     record_cos=False, rot=rot)
+        self.m_fadds = f32(fa)
+        self._ran1_back(ran1)
+        if rot is not None:
+            self.m_ninter.copy_(torch.from_numpy(tr["ninter"]))
+            self.m_faddbs[0] = float(tr["faddbs"])
+
+    def check_status(self):
+        return None
+
+    def download_mc(self):
+        nmt = self.host.nmoltype
+        m = self.mc
+        return dict(wholerot=m["wholerot"].copy(), wholetrans=m["wholetrans"].copy(),
+                    internrot=m["internrot"].copy(), interntrans=m["interntrans"].copy(),
+                    nwhole=m["nwhole"].reshape(2, nmt).copy(), nmovem=m["nmovem"].reshape(2, nmt).copy(),
+                    nstepreject=m["nstepreject"].copy(), fadds=f32(self.m_fadds), ran1=self._ran1())
+
+
+class OracleIntraModel:
+    """intra.IntraModel's interface over the oracle: ``m`` is the oracle's model dict."""
+
+    def __init__(self, d, *, nbond, iabond, tbond, amassa, amassr, xav, xav1, stepcl, simt, imageatom=None,
+                 qtype=None, ngrot=None, sizefactor=1.0, tempb=1.0, tempang=1.0, refine_intra=False,
+                 refine_intra_fac=0.0, dih=None):
+        b = d.host
+        self.d = d
+        self.m = dict(nbond=nbond, iabond=iabond, tbond=tbond, amassa=amassa, amassr=amassr, xav=xav, xav1=xav1,
+                      stepcl=f32(stepcl), simt=f32(simt), sizefactor=f32(sizefactor), tempb=f32(tempb),
+                      tempang=f32(tempang), refine_intra=bool(refine_intra), refine_intra_fac=f32(refine_intra_fac),
+                      imageatom=np.full(b.natom, -1, np.int32) if imageatom is None else imageatom,
+                      qtype=np.zeros(b.natom, np.int32) if qtype is None else qtype,
+                      ngrot=np.zeros(b.nmol, np.int32) if ngrot is None else ngrot, dih=dih)
+
+    def en_mole_intra(self, out=None):
+        self.d.calls.append("en_mole_intra")
+        return oracle.en_mole_intra_all(self.d.box, self.m)
+
+    def molfit_shake(self, stepmi, faddbs):
+        """The intramolecular cycle; faddbs: (1,) tensor in/out; returns nmovei (2*nmoltype,).
+        The work array's first slot starts at 0, as on the device."""
+        d = self.d
+        d.calls.append("molfit_shake")
+        fb = f32(faddbs[0].item())
+        if d.r is not None:
+            rot = dict(d.r, model=self.m)
+            fa, fb, nmovei, ninter, _, ran1, _ = oracle.molfit_shake_rot(d.box, d._store(), d.mc, rot, f32(stepmi),
+                                                                          d._ran1(), d.m_fadds, fb, 0.0)
+            d.m_ninter.copy_(torch.from_numpy(ninter))
+        else:
+            fa, fb, nmovei, _, ran1 = oracle.molfit_shake(d.box, d._store(), d.mc, self.m, f32(stepmi), d._ran1(),
+                                                          d.m_fadds, fb, 0.0)
+        d.m_fadds = f32(fa)
+        d._ran1_back(ran1)
+        faddbs[0] = float(fb)
+        return torch.from_numpy(np.asarray(nmovei, np.int32))

@@ -1,0 +1,136 @@
+"""The drop-in inside the reference's own epsr loop: runepsr17 (epsr_standalone_rev3.py:1235)
+runs unchanged on a copy of the reference's shipped run folder (EPSR-test: 200 DMSO + 400
+water, the DMSO methyl groups as ROT groups) with dropin.install_reference() in place for the
+cell list, fmolec1 and molfit -- the routines the loop calls through their modules
+(epsr_standalone_rev3.py:1265, :1280, :1318, :1343).  The device layer under the drop-in is the
+oracle-backed stand-in of tests/oracle_device.py, so what runs here is the drop-in's own host
+side with the real epsr26 package: its COMMON modules and reset(), the loop's call order, the
+centres put back in the box and fmolec1 called again after the intramolecular cycle.
+
+The input file's niter is raised to 2 as for the fixture, so that the loop refines the
+potential once on the host (atogen, gensq, the running sums, ptgnsq, generate_ep) between the
+captures and the drop-in then sees the new tables.  Around the loop's first, second and sixth
+molfit calls (the intramolecular cycle with the methyl rotations, a whole-molecule cycle, a
+whole-molecule cycle with the methyl rotations) the COMMON state is captured as
+tests/golden/make_golden_realrun.py captured it from the unmodified loop, and every array must
+equal tests/golden/realrun.npz bit for bit: the box, the cell list and pair store the drop-in wrote, the step arrays, counters,
+ran1 state, fadds/faddbs, and the coordinates and energies after each call.  Only the scratch
+slot ergold(1) is left out (the drop-in does not fill the reference's en_change work arrays).
+
+Needs the reference checkout (EPSR_REFERENCE, the directory holding src/epsr26 and
+EPSR-test); skipped without it.  About two minutes of CPU, most of it the reference's own
+refinement between the second and sixth calls."""
+
+import importlib
+import os
+import shutil
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+from tests.goldens import GOLDEN, assert_bits_equal
+
+ROOT = os.environ.get("EPSR_REFERENCE", "")
+HAVE_REF = bool(ROOT) and os.path.isdir(os.path.join(ROOT, "src", "epsr26")) and \
+    os.path.isdir(os.path.join(ROOT, "EPSR-test"))
+ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit")
+SKIP = ("ergold1", "after_ergold1", "cos")
+
+
+class _Stop(Exception):
+    pass
+
+
+def _host_routine(name):
+    def f(*a, **k):
+        raise AssertionError(f"the reference's own {name} ran: the drop-in routed it to the host")
+    return f
+
+
+def _run_loop_with_dropin(tmp_path, monkeypatch):
+    sys.path.insert(0, GOLDEN)
+    import make_golden_realrun as g
+    import refstate
+    from epsr_python_translation_b200 import device, dropin, intra
+    from tests.oracle_device import OracleDeviceBox, OracleIntraModel
+
+    refstate.load_reference(os.path.join(ROOT, "src"))
+    common = importlib.import_module("epsr26.common")
+    mods = {"cellneighbourlist": importlib.import_module("epsr26.library.cellneighbourlist"),
+            "ato_manipulation_rev4": importlib.import_module("epsr26.library.ato_manipulation_rev4"),
+            "molfit": importlib.import_module("epsr26.library.molfit")}
+    from epsr26.programs import load, run_program
+
+    monkeypatch.setattr(device, "DeviceBox", OracleDeviceBox)
+    monkeypatch.setattr(OracleDeviceBox, "journal", [])
+    monkeypatch.setattr(intra, "IntraModel", OracleIntraModel)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    run = tmp_path / "EPSR-test"
+    shutil.copytree(os.path.join(ROOT, "EPSR-test"), run)
+    g.prepare_run(str(run))
+
+    path = dropin.install_reference(load("epsr"), routines=ROUTINES)
+    real = dict(path.orig)
+    for name in ROUTINES:
+        path.orig[name] = _host_routine(name)
+    installed = mods["molfit"].molfit
+    out, n = {}, {"n": 0, "taken": 0}
+
+    def wrapped(fadds, faddbs, nisum, intra_, rotfreq, ireset):
+        n["n"] += 1
+        if n["n"] not in g.CAPTURE:
+            return installed(fadds, faddbs, nisum, intra_, rotfreq, ireset)
+        q = "k%d_" % n["taken"]
+        g.snapshot(common, mods, out, q)
+        g.intra_snapshot(common, out, q)
+        out[q + "args"] = np.array([fadds, faddbs], np.float32)
+        out[q + "args_int"] = np.array([nisum, intra_, rotfreq, ireset, n["n"]], np.int32)
+        r = installed(fadds, faddbs, nisum, intra_, rotfreq, ireset)
+        g.after(common, out, q, r, [])
+        n["taken"] += 1
+        if n["taken"] == len(g.CAPTURE):
+            raise _Stop()
+        return r
+
+    mods["molfit"].molfit = wrapped
+    cwd = os.getcwd()
+    os.chdir(run)
+    try:
+        run_program("epsr", ["./", "epsr", "200DMSO400Water.EPSR.inp"])
+    except _Stop:
+        pass
+    finally:
+        os.chdir(cwd)
+        mods["molfit"].molfit = installed
+        path.orig = real
+        path.uninstall()
+    return out, OracleDeviceBox.journal
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="needs the reference checkout (EPSR_REFERENCE)")
+def test_dropin_in_the_reference_loop_matches_the_unmodified_loop(tmp_path, monkeypatch):
+    z = np.load(os.path.join(GOLDEN, "realrun.npz"))
+    out, calls = _run_loop_with_dropin(tmp_path, monkeypatch)
+    # routed as the loop's branches ask: the cell list and store, the intramolecular cycle, the
+    # store again, four whole-molecule cycles; after the refinement (which rebuilds the lattice:
+    # its float cos(90 deg) entries become exact zeros, so the drop-in makes a new device box)
+    # the cell list, the store and a fifth whole-molecule cycle, with rotations
+    assert calls == ["box", "cell_list", "en_mole_intra", "fmolec1", "molfit_shake", "en_mole_intra", "fmolec1"] + \
+        ["molfit"] * 4 + ["box", "cell_list", "en_mole_intra", "fmolec1", "molfit"], calls
+    checked = 0
+    for key, v in out.items():
+        if any(key.endswith("_" + s) for s in SKIP):
+            continue
+        assert key in z.files, key
+        ref = z[key]
+        a = np.asarray(v)
+        if a.dtype.kind == "f":
+            assert_bits_equal(a, ref, key)
+        else:
+            assert a.shape == ref.shape and np.array_equal(a, ref), key
+        checked += 1
+    assert checked > 100
+    for q in ("k0_", "k1_", "k2_"):
+        assert int(out[q + "ran1_after_mcall"]) > int(out[q + "ran1_before_mcall"])

@@ -2,9 +2,11 @@
 DMSO + 400 water, the DMSO methyl groups as ROT groups, the run folder's potentials and
 intramolecular model), tests/golden/realrun.npz made by tests/golden/make_golden_realrun.py:
 the loop's first molfit call (the intramolecular cycle: atom moves, then the methyl rotations
-tested with the intermolecular change, molfit.py:124-267) and its second (a whole-molecule
-cycle, :268-448) replayed from the state the loop held at each call, bit for bit --
-coordinates, stored energies, step sizes, counters, fadds/faddbs and the ran1 stream."""
+tested with the intermolecular change, molfit.py:124-267), its second (a whole-molecule
+cycle, :268-448) and its sixth (a whole-molecule cycle with the internal rotations of the
+methyl groups, :295-360, after the first potential refinement) replayed from the state the
+loop held at each call, bit for bit -- coordinates, stored energies, step sizes, counters,
+fadds/faddbs and the ran1 stream."""
 
 import os
 
@@ -96,3 +98,18 @@ def test_realrun_whole_molecule_cycle_oracle_matches_reference():
     assert_bits_equal(tr["cosv"], z[q + "cos"], "rotatm cosines")
     # no rotation this cycle: faddbs is the argument, unchanged by the oracle's whole-molecule cycle
     _check_after(z, q, box, st, mc, fadds, f32(z[q + "args"][1]) + f32(0.0) / f32(box.nmol), ran1)
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_whole_molecule_cycle_with_rotations_oracle_matches_reference():
+    z = np.load(PATH)
+    q = "k2_"
+    nisum, intra, rotfreq = (int(v) for v in z[q + "args_int"][:3])
+    assert nisum < intra and nisum % rotfreq == 0          # a rotation cycle of the whole-molecule branch
+    box, st, cells, mc, rot = _call(z, q)
+    fadds, faddbs = (f32(v) for v in z[q + "args"])
+    rot["faddbs"] = faddbs
+    fadds, tr, ran1 = oracle.molfit(box, cells, st, mc, Ran1State.from_golden(z, q + "ran1_before_"), fadds, rot=rot)
+    assert_bits_equal(tr["cosv"], z[q + "cos"], "rotati and rotatm cosines")
+    _check_after(z, q, box, st, mc, fadds, tr["faddbs"], ran1, ninter=tr["ninter"])
+    assert tr["ninter"][0] > 0
