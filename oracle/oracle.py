@@ -632,16 +632,18 @@ def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
     return out
 
 
-def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1, fast=False):
+def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1, fast=False, acceptr=0.0,
+                  rejrat=0.0, chisqnew=0.0):
     """1-based arrays (index 0 unused).  Returns dict and the new ran1 state.  fast: the trial
     loop's chi^2 summed in double and rounded once to float32 (the device's fast mode); the
-    final chi^2 keeps the reference's sequential float sum in both modes."""
+    final chi^2 keeps the reference's sequential float sum in both modes.  acceptr, rejrat,
+    chisqnew: the caller's values of the in/out arguments (epsr_standalone_rev3.py:4806)."""
     yin = np.ascontiguousarray(yin, f32)
     expr = np.ascontiguousarray(expr, f32)
     wt = np.zeros(nterms + 1, f32)
     wto = np.ascontiguousarray(wtold, f32).copy()
     yout = np.zeros(npt + 1, f32)
-    scal = np.array([stepr, 0.0, 0.0, 0.0], f32)
+    scal = np.array([stepr, acceptr, rejrat, chisqnew], f32)
     r = Ran1C.of(ran1)
     trials = lib().oracle_fit_expansion_mode(ptr(yin), ptr(expr), ptr(yout), ptr(wt), ptr(wto), ptr(scal), nmin,
                                              npt, ncfirst, nterms, nits, nfreq, C.byref(r), 1 if fast else 0)

@@ -3,9 +3,11 @@ every routine is the oracle's C restatement on the host: test infrastructure, so
 drop-in's own host side -- reading the COMMON blocks, the cell list and pair store written
 back into them, the routing of molfit by nisum, the ran1 state in and out, the step arrays
 and counters written back -- runs inside the reference's unchanged epsr loop on a machine
-without a GPU.  Only the routines of the cell list, fmolec1 and molfit (the intramolecular
-cycle with rotational groups included) are provided; the device layer itself is checked
-against the same oracle by the GPU tests.
+without a GPU.  Every routine the drop-in installs by default has its stand-in: the cell
+list, fmolec1 and molfit (the intramolecular cycle with rotational groups included), atogen,
+press, gensq, the running sums, stog, fit_expansion and generate_ep; the host-side library
+routines (the EP basis, generate_rp) run as they are.  The device layer itself is checked
+against the same oracle by the GPU tests.  ``install(monkeypatch)`` puts them in place.
 
 The state the device would hold (coordinates, cells, pair store, MC arrays) is held here as
 NumPy arrays and CPU tensors with the device layer's names and layouts (the drop-in reads and
@@ -200,3 +202,119 @@ class OracleIntraModel:
         d._ran1_back(ran1)
         faddbs[0] = float(fb)
         return torch.from_numpy(np.asarray(nmovei, np.int32))
+
+
+# ---------------------------------------------------------------------- the iteration's other routines
+def _atogen(self, ngrsamples, ran1_t, rminex, ycoh=None, sizefactor=1.0, npt1=None):
+    self.calls.append("atogen")
+    wav, potex, n, ran1 = oracle.atogen(self.box, int(ngrsamples), Ran1State.from_array(ran1_t.numpy()),
+                                        np.asarray(rminex, f32), ycoh, f32(sizefactor))
+    ran1_t.copy_(torch.from_numpy(ran1.as_array()))
+    self._wav = (wav, potex)
+    return n
+
+
+def _download_wav(self):
+    return self._wav
+
+
+def _press(self, npt1=None, strict=True):
+    self.calls.append("press")
+    r = oracle.press(self.box, self._store(), int(npt1), self.box.simt, 1.0)
+    return f32(r["sumc"]), float(r["presst"])
+
+
+OracleDeviceBox.atogen = _atogen
+OracleDeviceBox.download_wav = _download_wav
+OracleDeviceBox.press = _press
+
+def _note(name):
+    j = OracleDeviceBox.journal
+    if j is not None:
+        j.append(name)
+
+
+def gensq(nq, npt1, wav, ldw, foqols, sj, si, ycoh, n2extr, natomsphere, npairs):
+    """transforms.gensq over the oracle (foqols (r points, Q points), strides (nq+1, 1))."""
+    _note("gensq")
+    fq = np.asarray(foqols, f32)
+    assert fq.ndim == 2 and (sj, si) == (fq.shape[1], 1)
+    out = oracle.gensq(int(nq), int(npt1), wav.numpy().reshape(2, npairs, ldw), np.ascontiguousarray(fq.T),
+                       np.asarray(ycoh, f32), np.asarray(n2extr, np.int32), np.asarray(natomsphere, f32))
+    return torch.from_numpy(out.reshape(-1))
+
+
+def sumgr(nz, wav, ycoh, fc1, fc2, acc):
+    """transforms.sumgr over the oracle: acc updated in place."""
+    from epsr_python_translation_b200.transforms import GR_ARRAYS
+    _note("sumgr")
+    npairs, ldw = acc["gorintra"].shape
+    out = oracle.sumgr(int(nz), wav.numpy().reshape(2, npairs, ldw), ycoh.numpy(), fc1, fc2,
+                       {k: acc[k].numpy() for k in GR_ARRAYS})
+    for k in GR_ARRAYS:
+        acc[k].copy_(torch.from_numpy(out[k]))
+    return acc
+
+
+def sumsq(nq, qwind, fc1, fc2, acc):
+    """transforms.sumsq over the oracle: acc updated in place."""
+    from epsr_python_translation_b200.transforms import SQ_ARRAYS
+    _note("sumsq")
+    npairs, ldq = acc["soqintra"].shape
+    out = oracle.sumsq(int(nq), qwind.numpy().reshape(2, npairs, ldq), fc1, fc2, {k: acc[k].numpy() for k in SQ_ARRAYS})
+    for k in SQ_ARRAYS:
+        acc[k].copy_(torch.from_numpy(out[k]))
+    return acc
+
+
+def stog(rho, q, sofq_pairs, r, nqmin, nqmax, xwt):
+    """transforms.stog over the oracle: (npairs, nr+1)."""
+    _note("stog")
+    sp = sofq_pairs.numpy() if isinstance(sofq_pairs, torch.Tensor) else np.asarray(sofq_pairs, f32)
+    return torch.from_numpy(oracle.stog(f32(rho), np.asarray(q, f32), sp, np.asarray(r, f32), nqmin, nqmax, xwt))
+
+
+def fit_expansion(yin, expr, wtold, stepr, nmin, npt, ncfirst, nterms, nits, nfreq, ran1_t, acceptr=0.0, rejrat=0.0,
+                  chisqnew=0.0, strict=True):
+    """transforms.fit_expansion over the oracle (strict: the reference's float sums)."""
+    _note("fit_expansion")
+    res, ran1 = oracle.fit_expansion(np.asarray(yin, f32), np.asarray(expr, f32), np.asarray(wtold, f32), f32(stepr),
+                                     int(nmin), int(npt), int(ncfirst), int(nterms), int(nits), int(nfreq),
+                                     Ran1State.from_array(ran1_t.numpy()), fast=not strict, acceptr=f32(acceptr),
+                                     rejrat=f32(rejrat), chisqnew=f32(chisqnew))
+    ran1_t.copy_(torch.from_numpy(ran1.as_array()))
+    return dict(wt=torch.from_numpy(res["wt"]), wtold=torch.from_numpy(res["wtold"]), yout=torch.from_numpy(res["yout"]),
+                stepr=f32(res["stepr"]), acceptr=f32(res["acceptr"]), rejrat=f32(res["rejrat"]), chisq=f32(res["chisq"]),
+                trials=res["trials"])
+
+
+def generate_ep(npt, npt2, nterms, expgr, pcoefp, iref, dmax, xstar, wfac, ecoul, tabs, pwtold, absolute_energy,
+                erequnit, ereqstep, potfacamp, potfac, changepotfac=True, result=None):
+    """potential.generate_ep over the oracle: tabs, pcoefp, pwtold and potfac updated in place."""
+    _note("generate_ep")
+    out, pc, pw, pf, energabs, pressfac = oracle.generate_ep(
+        int(npt), int(npt2), int(nterms), expgr.numpy(), pcoefp.numpy(), np.asarray(iref, np.int32), f32(dmax),
+        xstar.numpy(), wfac.numpy(), ecoul.numpy(), {k: t.numpy() for k, t in tabs.items()}, pwtold.numpy(),
+        np.array([absolute_energy, erequnit, ereqstep, potfacamp], f32), f32(potfac.numpy()[0]), bool(changepotfac))
+    for k, t in tabs.items():
+        t.copy_(torch.from_numpy(out[k]))
+    pcoefp.copy_(torch.from_numpy(pc))
+    pwtold.copy_(torch.from_numpy(pw))
+    potfac[0] = float(pf)
+    return torch.tensor([float(energabs), float(pressfac)], dtype=torch.float32)
+
+
+def install(monkeypatch):
+    """Put the stand-ins in place of the device layer for the rest of a test."""
+    from epsr_python_translation_b200 import _lib, device, intra, potential, transforms
+    real_load = _lib.load
+    monkeypatch.setattr(device, "DeviceBox", OracleDeviceBox)
+    monkeypatch.setattr(intra, "IntraModel", OracleIntraModel)
+    for name in ("gensq", "sumgr", "sumsq", "stog", "fit_expansion"):
+        monkeypatch.setattr(transforms, name, globals()[name])
+    monkeypatch.setattr(potential, "generate_ep", generate_ep)
+    monkeypatch.setattr(_lib, "load", lambda require_device=False: real_load())
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    monkeypatch.setattr(torch.Tensor, "cuda", lambda self, *a, **k: self)
+    monkeypatch.setattr(OracleDeviceBox, "journal", [])
+    return OracleDeviceBox.journal

@@ -1,15 +1,18 @@
 """The drop-in inside the reference's own epsr loop: runepsr17 (epsr_standalone_rev3.py:1235)
 runs unchanged on a copy of the reference's shipped run folder (EPSR-test: 200 DMSO + 400
-water, the DMSO methyl groups as ROT groups) with dropin.install_reference() in place for the
-cell list, fmolec1 and molfit -- the routines the loop calls through their modules
-(epsr_standalone_rev3.py:1265, :1280, :1318, :1343).  The device layer under the drop-in is the
-oracle-backed stand-in of tests/oracle_device.py, so what runs here is the drop-in's own host
-side with the real epsr26 package: its COMMON modules and reset(), the loop's call order, the
-centres put back in the box and fmolec1 called again after the intramolecular cycle.
+water, the DMSO methyl groups as ROT groups) with dropin.install_reference(strict=True) in
+place for every routine it installs by default -- the cell list, fmolec1, molfit, atogen,
+press, gensq, sumgr, sumsq, stog, fit_expansion, generate_ep, generate_rp, each of which the
+loop calls through its module (e.g. epsr_standalone_rev3.py:1265, :1280, :1318, :1343); the
+reference's own routines are replaced by stubs that fail if the drop-in hands a call back to
+them.  The device layer under the drop-in is the oracle-backed stand-in of
+tests/oracle_device.py, so what runs here is the drop-in's own host side with the real epsr26
+package: its COMMON modules and reset(), the loop's call order, the centres put back in the box
+and fmolec1 called again after the intramolecular cycle, the refinement's ran1 draws.
 
 The input file's niter is raised to 2 as for the fixture, so that the loop refines the
-potential once on the host (atogen, gensq, the running sums, ptgnsq, generate_ep) between the
-captures and the drop-in then sees the new tables.  Around the loop's first, second and sixth
+potential once through the drop-in (atogen, gensq, the running sums, press, ptgnsq's fits,
+generate_ep) between the captures and the drop-in then sees the new tables.  Around the loop's first, second and sixth
 molfit calls (the intramolecular cycle with the methyl rotations, a whole-molecule cycle, a
 whole-molecule cycle with the methyl rotations) the COMMON state is captured as
 tests/golden/make_golden_realrun.py captured it from the unmodified loop, and every array must
@@ -18,8 +21,7 @@ ran1 state, fadds/faddbs, and the coordinates and energies after each call.  Onl
 slot ergold(1) is left out (the drop-in does not fill the reference's en_change work arrays).
 
 Needs the reference checkout (EPSR_REFERENCE, the directory holding src/epsr26 and
-EPSR-test); skipped without it.  About two minutes of CPU, most of it the reference's own
-refinement between the second and sixth calls."""
+EPSR-test); skipped without it.  About ten seconds of CPU."""
 
 import importlib
 import os
@@ -28,14 +30,15 @@ import sys
 
 import numpy as np
 import pytest
-import torch
 
+from epsr_python_translation_b200 import dropin
 from tests.goldens import GOLDEN, assert_bits_equal
 
 ROOT = os.environ.get("EPSR_REFERENCE", "")
 HAVE_REF = bool(ROOT) and os.path.isdir(os.path.join(ROOT, "src", "epsr26")) and \
     os.path.isdir(os.path.join(ROOT, "EPSR-test"))
-ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit")
+ROUTINES = ("initialise_cellneighbourlist", "fmolec1", "molfit", "atogen", "press", "gensq", "sumgr", "sumsq",
+            "stog", "fit_expansion", "generate_ep", "generate_rp")
 SKIP = ("ergold1", "after_ergold1", "cos")
 
 
@@ -53,8 +56,7 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
     sys.path.insert(0, GOLDEN)
     import make_golden_realrun as g
     import refstate
-    from epsr_python_translation_b200 import device, dropin, intra
-    from tests.oracle_device import OracleDeviceBox, OracleIntraModel
+    from tests import oracle_device
 
     refstate.load_reference(os.path.join(ROOT, "src"))
     common = importlib.import_module("epsr26.common")
@@ -63,15 +65,12 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
             "molfit": importlib.import_module("epsr26.library.molfit")}
     from epsr26.programs import load, run_program
 
-    monkeypatch.setattr(device, "DeviceBox", OracleDeviceBox)
-    monkeypatch.setattr(OracleDeviceBox, "journal", [])
-    monkeypatch.setattr(intra, "IntraModel", OracleIntraModel)
-    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    journal = oracle_device.install(monkeypatch)
     run = tmp_path / "EPSR-test"
     shutil.copytree(os.path.join(ROOT, "EPSR-test"), run)
     g.prepare_run(str(run))
 
-    path = dropin.install_reference(load("epsr"), routines=ROUTINES)
+    path = dropin.install_reference(load("epsr"), strict=True, routines=ROUTINES)
     real = dict(path.orig)
     for name in ROUTINES:
         path.orig[name] = _host_routine(name)
@@ -106,19 +105,23 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
         mods["molfit"].molfit = installed
         path.orig = real
         path.uninstall()
-    return out, OracleDeviceBox.journal
+    return out, journal
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="needs the reference checkout (EPSR_REFERENCE)")
 def test_dropin_in_the_reference_loop_matches_the_unmodified_loop(tmp_path, monkeypatch):
     z = np.load(os.path.join(GOLDEN, "realrun.npz"))
     out, calls = _run_loop_with_dropin(tmp_path, monkeypatch)
-    # routed as the loop's branches ask: the cell list and store, the intramolecular cycle, the
-    # store again, four whole-molecule cycles; after the refinement (which rebuilds the lattice:
-    # its float cos(90 deg) entries become exact zeros, so the drop-in makes a new device box)
-    # the cell list, the store and a fifth whole-molecule cycle, with rotations
-    assert calls == ["box", "cell_list", "en_mole_intra", "fmolec1", "molfit_shake", "en_mole_intra", "fmolec1"] + \
-        ["molfit"] * 4 + ["box", "cell_list", "en_mole_intra", "fmolec1", "molfit"], calls
+    assert set(ROUTINES) == set(dropin.DEFAULT_ROUTINES)
+    # routed as the loop asks: the EP at set-up; the cell list and store, the intramolecular
+    # cycle, the store again, four whole-molecule cycles; the refinement (atogen, gensq, the
+    # running sums, press, one fit per data set, generate_ep); then, the lattice rebuilt (its
+    # float cos(90 deg) entries become exact zeros, so the drop-in makes a new device box), the
+    # cell list, the store and a fifth whole-molecule cycle, with rotations.  stog (the output
+    # section) and generate_rp (the multiply_pcoefex command) are not reached before it.
+    assert calls == ["generate_ep", "box", "cell_list", "en_mole_intra", "fmolec1", "molfit_shake", "en_mole_intra",
+                     "fmolec1"] + ["molfit"] * 4 + ["atogen", "gensq", "sumsq", "sumgr", "press"] + \
+        ["fit_expansion"] * 3 + ["generate_ep", "box", "cell_list", "en_mole_intra", "fmolec1", "molfit"], calls
     checked = 0
     for key, v in out.items():
         if any(key.endswith("_" + s) for s in SKIP):
