@@ -20,10 +20,15 @@ equal tests/golden/realrun.npz bit for bit: the box, the cell list and pair stor
 ran1 state, fadds/faddbs, and the coordinates and energies after each call.  Only the scratch
 slot ergold(1) is left out (the drop-in does not fill the reference's en_change work arrays).
 
+A second run takes the shipped input file unchanged to its end (one iteration, then the final
+output section with its four stog calls) and compares every file left in the run folder with
+the unmodified run's (tests/golden/realrun_files.json, digests of the normalised bytes).
+
 Needs the reference checkout (EPSR_REFERENCE, the directory holding src/epsr26 and
-EPSR-test); skipped without it.  About ten seconds of CPU."""
+EPSR-test); skipped without it.  About twenty seconds of CPU."""
 
 import importlib
+import json
 import os
 import shutil
 import sys
@@ -52,28 +57,45 @@ def _host_routine(name):
     return f
 
 
-def _run_loop_with_dropin(tmp_path, monkeypatch):
+def _install(tmp_path, monkeypatch):
+    """The reference loaded, the stand-ins and the drop-in in place, the reference's own
+    routines stubbed out, the run folder copied: (path, originals, journal, run folder)."""
     sys.path.insert(0, GOLDEN)
-    import make_golden_realrun as g
     import refstate
     from tests import oracle_device
 
     refstate.load_reference(os.path.join(ROOT, "src"))
-    common = importlib.import_module("epsr26.common")
-    mods = {"cellneighbourlist": importlib.import_module("epsr26.library.cellneighbourlist"),
-            "ato_manipulation_rev4": importlib.import_module("epsr26.library.ato_manipulation_rev4"),
-            "molfit": importlib.import_module("epsr26.library.molfit")}
-    from epsr26.programs import load, run_program
-
+    from epsr26.programs import load
     journal = oracle_device.install(monkeypatch)
     run = tmp_path / "EPSR-test"
     shutil.copytree(os.path.join(ROOT, "EPSR-test"), run)
-    g.prepare_run(str(run))
-
     path = dropin.install_reference(load("epsr"), strict=True, routines=ROUTINES)
     real = dict(path.orig)
     for name in ROUTINES:
         path.orig[name] = _host_routine(name)
+    return path, real, journal, run
+
+
+def _run_program(run):
+    from epsr26.programs import run_program
+    cwd = os.getcwd()
+    os.chdir(run)
+    try:
+        return run_program("epsr", ["./", "epsr", "200DMSO400Water.EPSR.inp"])
+    finally:
+        os.chdir(cwd)
+
+
+def _run_loop_with_dropin(tmp_path, monkeypatch):
+    sys.path.insert(0, GOLDEN)
+    import make_golden_realrun as g
+
+    path, real, journal, run = _install(tmp_path, monkeypatch)
+    g.prepare_run(str(run))
+    common = importlib.import_module("epsr26.common")
+    mods = {"cellneighbourlist": importlib.import_module("epsr26.library.cellneighbourlist"),
+            "ato_manipulation_rev4": importlib.import_module("epsr26.library.ato_manipulation_rev4"),
+            "molfit": importlib.import_module("epsr26.library.molfit")}
     installed = mods["molfit"].molfit
     out, n = {}, {"n": 0, "taken": 0}
 
@@ -94,18 +116,30 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
         return r
 
     mods["molfit"].molfit = wrapped
-    cwd = os.getcwd()
-    os.chdir(run)
     try:
-        run_program("epsr", ["./", "epsr", "200DMSO400Water.EPSR.inp"])
+        _run_program(run)
     except _Stop:
         pass
     finally:
-        os.chdir(cwd)
         mods["molfit"].molfit = installed
         path.orig = real
         path.uninstall()
     return out, journal
+
+
+def _run_program_with_dropin(tmp_path, monkeypatch):
+    """The shipped run to its end through the drop-in: the digests of the files it leaves."""
+    sys.path.insert(0, GOLDEN)
+    import make_golden_realrun_files as gf
+
+    path, real, journal, run = _install(tmp_path, monkeypatch)
+    try:
+        rc = _run_program(run)
+    finally:
+        path.orig = real
+        path.uninstall()
+    assert rc in (0, None)
+    return gf.output_digests(str(run)), journal
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="needs the reference checkout (EPSR_REFERENCE)")
@@ -137,3 +171,23 @@ def test_dropin_in_the_reference_loop_matches_the_unmodified_loop(tmp_path, monk
     assert checked > 100
     for q in ("k0_", "k1_", "k2_"):
         assert int(out[q + "ran1_after_mcall"]) > int(out[q + "ran1_before_mcall"])
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="needs the reference checkout (EPSR_REFERENCE)")
+def test_dropin_in_the_reference_loop_writes_the_unmodified_runs_files(tmp_path, monkeypatch):
+    """The shipped run (one iteration, then the final output section) to its end through the
+    drop-in: every file it leaves in the run folder -- .erg, .g01, .f01, .pcof, the .ato and
+    the rest, 66 files -- has the bytes the unmodified run left (tests/golden/realrun_files.json
+    from tests/golden/make_golden_realrun_files.py), the run date and molfit's elapsed-time
+    columns excepted."""
+    with open(os.path.join(GOLDEN, "realrun_files.json")) as f:
+        want = json.load(f)
+    got, calls = _run_program_with_dropin(tmp_path, monkeypatch)
+    assert sorted(got) == sorted(want)
+    bad = [k for k in want if got[k] != want[k]]
+    assert not bad, bad
+    for k in ("200DMSO400Water.EPSR.erg", "200DMSO400Water.EPSR.g01", "200DMSO400Water.EPSR.f01",
+              "200DMSO400Water.pcof", "200DMSO400Water.ato"):
+        assert k in want
+    # the output section's four transforms ran through the drop-in too
+    assert calls.count("stog") == 4 and calls.count("molfit") == 4 and calls.count("molfit_shake") == 1, calls
