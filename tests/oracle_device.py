@@ -164,6 +164,25 @@ class OracleDeviceBox:
                     nwhole=m["nwhole"].reshape(2, nmt).copy(), nmovem=m["nmovem"].reshape(2, nmt).copy(),
                     nstepreject=m["nstepreject"].copy(), fadds=f32(self.m_fadds), ran1=self._ran1())
 
+    # ------------------------------------------------------------------ atogen, press
+    def atogen(self, ngrsamples, ran1_t, rminex, ycoh=None, sizefactor=1.0, npt1=None):
+        self.calls.append("atogen")
+        wav, potex, n, ran1 = oracle.atogen(self.box, int(ngrsamples), Ran1State.from_array(ran1_t.numpy()),
+                                            np.asarray(rminex, f32), ycoh, f32(sizefactor))
+        ran1_t.copy_(torch.from_numpy(ran1.as_array()))
+        self._wav = (wav, potex)
+        return n
+
+    def download_wav(self):
+        return self._wav
+
+    def press(self, npt1=None, strict=True):
+        """(sumc, presst) of the stored pairs; the caller forms the energy and pressure from
+        them with the box volume, so the oracle's own scalars (volume 1 here) go unused."""
+        self.calls.append("press")
+        r = oracle.press(self.box, self._store(), int(npt1), self.box.simt, 1.0)
+        return f32(r["sumc"]), float(r["presst"])
+
 
 class OracleIntraModel:
     """intra.IntraModel's interface over the oracle: ``m`` is the oracle's model dict."""
@@ -204,30 +223,7 @@ class OracleIntraModel:
         return torch.from_numpy(np.asarray(nmovei, np.int32))
 
 
-# ---------------------------------------------------------------------- the iteration's other routines
-def _atogen(self, ngrsamples, ran1_t, rminex, ycoh=None, sizefactor=1.0, npt1=None):
-    self.calls.append("atogen")
-    wav, potex, n, ran1 = oracle.atogen(self.box, int(ngrsamples), Ran1State.from_array(ran1_t.numpy()),
-                                        np.asarray(rminex, f32), ycoh, f32(sizefactor))
-    ran1_t.copy_(torch.from_numpy(ran1.as_array()))
-    self._wav = (wav, potex)
-    return n
-
-
-def _download_wav(self):
-    return self._wav
-
-
-def _press(self, npt1=None, strict=True):
-    self.calls.append("press")
-    r = oracle.press(self.box, self._store(), int(npt1), self.box.simt, 1.0)
-    return f32(r["sumc"]), float(r["presst"])
-
-
-OracleDeviceBox.atogen = _atogen
-OracleDeviceBox.download_wav = _download_wav
-OracleDeviceBox.press = _press
-
+# ---------------------------------------------------------------------- transforms and the EP
 def _note(name):
     j = OracleDeviceBox.journal
     if j is not None:
