@@ -191,3 +191,27 @@ def test_dropin_in_the_reference_loop_writes_the_unmodified_runs_files(tmp_path,
         assert k in want
     # the output section's four transforms ran through the drop-in too
     assert calls.count("stog") == 4 and calls.count("molfit") == 4 and calls.count("molfit_shake") == 1, calls
+
+
+def test_oracle_stand_ins_keep_the_device_layers_signatures():
+    """Every stand-in of tests/oracle_device.py takes the arguments of the device-layer call it
+    replaces (device.DeviceBox, intra.IntraModel, transforms, potential.generate_ep), so the
+    drop-in calls both alike.  Needs no reference checkout."""
+    import inspect
+
+    from epsr_python_translation_b200 import device, intra, potential, transforms
+    from tests import oracle_device as od
+
+    def params(f):
+        return [(p.name, p.kind, p.default) for p in inspect.signature(f).parameters.values()]
+
+    pairs = [(getattr(od.OracleDeviceBox, n), getattr(device.DeviceBox, n))
+             for n in ("upload", "upload_coords", "download_coords", "ran1_tensor", "cell_list", "download_cells",
+                       "fmolec1", "download_store", "mc_setup", "set_rotations", "set_cos_override", "molfit",
+                       "check_status", "download_mc", "atogen", "download_wav", "press")]
+    pairs += [(getattr(od.OracleIntraModel, n), getattr(intra.IntraModel, n))
+              for n in ("__init__", "en_mole_intra", "molfit_shake")]
+    pairs += [(getattr(od, n), getattr(transforms, n)) for n in ("gensq", "sumgr", "sumsq", "stog", "fit_expansion")]
+    pairs += [(od.generate_ep, potential.generate_ep)]
+    bad = [f"{a.__qualname__}: {params(a)} vs {params(b)}" for a, b in pairs if params(a) != params(b)]
+    assert not bad, "\n".join(bad)
