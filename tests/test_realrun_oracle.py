@@ -6,7 +6,8 @@ tested with the intermolecular change, molfit.py:124-267), its second (a whole-m
 cycle, :268-448) and its sixth (a whole-molecule cycle with the internal rotations of the
 methyl groups, :295-360, after the first potential refinement) replayed from the state the
 loop held at each call, bit for bit -- coordinates, stored energies, step sizes, counters,
-fadds/faddbs and the ran1 stream."""
+fadds/faddbs and the ran1 stream; and the pair store the loop's fmolec1 had just built before
+each of them, with its ftest and ftestb."""
 
 import os
 
@@ -113,3 +114,26 @@ def test_realrun_whole_molecule_cycle_with_rotations_oracle_matches_reference():
     assert_bits_equal(tr["cosv"], z[q + "cos"], "rotati and rotatm cosines")
     _check_after(z, q, box, st, mc, fadds, tr["faddbs"], ran1, ninter=tr["ninter"])
     assert tr["ninter"][0] > 0
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+@pytest.mark.parametrize("q", ["k0_", "k1_", "k2_"])
+def test_realrun_pair_store_oracle_matches_reference(q):
+    """Each captured call follows the loop's fmolec1 (epsr_standalone_rev3.py:1280 at the start
+    of an iteration, :1343 after the intramolecular cycle): the oracle's en_mole_intra and
+    fmolec1 on the captured coordinates and cell list give the captured store (every used slot
+    of molergpair and ergpairref, nergpairm, the stored energies) and the ftest, ftestb the loop
+    handed to molfit, bit for bit."""
+    z = np.load(PATH)
+    box, st, cells, _, rot = _call(z, q)
+    eintra = oracle.en_mole_intra_all(box, rot["model"])
+    got = oracle.fmolec1(box, cells, eintra)
+    assert got["nnbrefmax"] == st["nnbrefmax"] and got["nergpair"] == st["nergpair"]
+    nm = st["nergpairm"]
+    assert np.array_equal(got["nergpairm"], nm)
+    M = st["nnbrefmax"]
+    used = np.arange(M)[None, :] < nm[:, None]
+    for k in ("molergpair", "ergpairref"):
+        assert np.array_equal(got[k][used], st[k].reshape(-1, M)[used]), k
+    assert_bits_equal(got["ergpair"][: st["nergpair"]], st["ergpair"], q + "ergpair")
+    assert_bits_equal(np.array([got["ftest"], got["ftestb"]], f32), z[q + "args"], q + "ftest, ftestb")
