@@ -4,19 +4,23 @@ the reference translation (epsr26) itself.
 
     EPSR_REFERENCE=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_realrun.py
 
-The run folder is copied to a scratch directory and the unchanged epsr program runs on it
-(runepsr17 epsr_standalone_rev3.py:1235: the files read, the potentials built, the cell list,
-fmolec1, then molfit ntimes times).  Its first two molfit calls are captured through the
+The run folder is copied to a scratch directory, its input file's niter raised to 2
+(prepare_run), and the unchanged epsr program runs on it (runepsr17
+epsr_standalone_rev3.py:1235: the files read, the potentials built, the cell list, fmolec1,
+molfit ntimes times, the refinement, again).  Three molfit calls are captured through the
 module attribute the loop calls (molfit.molfit, as the reference's tracer reroutes routines):
 the run folder's nisum starts at intra, so the first is the intramolecular cycle, each
-molecule's atoms moved and then its methyl groups rotated (molfit.py:124-267), and the second
-a whole-molecule cycle (:268-448).  For each, everything that call reads is written before it and everything it
-changes after it (every array copied, the COMMON arrays being updated in place): the box as
-the COMMON blocks hold it (read by the drop-in's own
-box_from_common), the cell list as the loop built it, the pair store, the step arrays and
-counters, the rotational groups and the intramolecular model, the ran1 state, the call's
-arguments and results, and the cosines molfit drew.  The run is stopped after the second
-captured call.  tests/golden/realrun.npz receives the two calls under the prefixes k0_, k1_.
+molecule's atoms moved and then its methyl groups rotated (molfit.py:124-267); the second a
+whole-molecule cycle (:268-448); the sixth, after the first refinement, a whole-molecule cycle
+with the internal rotations of the methyl groups (:295-360).  For each, everything that call
+reads is written before it and everything it changes after it (every array copied, the
+COMMON arrays being updated in place): the box as the COMMON blocks hold it (read by the
+drop-in's own box_from_common), the cell list as the loop built it, the pair store, the step
+arrays and counters, the rotational groups and the intramolecular model, the ran1 state, the
+call's arguments and results, and the cosines molfit drew.  The refinement's first atogen and
+press calls are captured the same way.  The run is stopped after the sixth molfit call.
+tests/golden/realrun.npz receives the molfit calls under the prefixes k0_, k1_, k2_ and the
+atogen and press calls under ag_ and pr_.
 """
 
 from __future__ import annotations
@@ -115,6 +119,55 @@ def snapshot(common, mods, out, q):
         out[q + "ran1_before_" + k] = v
 
 
+def box_snapshot(common, mods, out, q):
+    """The box as the COMMON blocks hold it and the ran1 state, under prefix q."""
+    from epsr_python_translation_b200 import dropin
+    for k, v in dropin.PairPath(common, mods).box_from_common().__dict__.items():
+        out[q + "box_" + k] = v.copy() if isinstance(v, np.ndarray) else np.array(v)
+    for k, v in refstate.ran1_state().items():
+        out[q + "ran1_before_" + k] = v
+
+
+def capture_atogen(common, mods, out, orig):
+    """The loop's first atogen call (ato_manipulation_rev4.py:3640, from
+    epsr_standalone_rev3.py:1397) under prefix ag_: the box, the ran1 state, the per-pair
+    close-contact radius rminex (of each pair's set), ycoh, sizefactor and ngrsamples before;
+    wav (2, npt1, npairs), potex, the returned count and the ran1 state after."""
+    def wrapped(wav, ngrsamples):
+        if "ag_ngrsamples" in out:
+            return orig(wav, ngrsamples)
+        pp, e16, mc = common.potential_par, common.epsr16, common.molecom
+        npairs, npt1 = int(mc.npairs), int(e16.npt1)
+        box_snapshot(common, mods, out, "ag_")
+        out["ag_rminex"] = np.array([pp.rminex[int(pp.irefpcof[p + 1])] for p in range(npairs)], f32)
+        out["ag_ycoh"] = np.array(e16.ycoh[: int(e16.npt) + 1], f32)
+        out["ag_sizefactor"] = f32(mc.sizefactor)
+        out["ag_ngrsamples"] = np.int32(ngrsamples)
+        n = orig(wav, ngrsamples)
+        out["ag_wav"] = np.array(np.asarray(wav)[1:3, 1:npt1 + 1, 1:npairs + 1], f32)
+        out["ag_potex"] = np.array(pp.potex[1:npairs + 1], f32)
+        out["ag_result"] = np.int32(n)
+        for k, v in refstate.ran1_state().items():
+            out["ag_ran1_after_" + k] = v
+        return n
+    return wrapped
+
+
+def capture_press(common, mods, out, orig):
+    """The loop's first press call (ato_manipulation_rev4.py:3903, from
+    epsr_standalone_rev3.py:1655) under prefix pr_: the box, cells and pair store before
+    (snapshot), npt1, simt and the volume; the returned energy and pressure after."""
+    def wrapped(energy, pressc, energf, pressf, energabs, energthreeb, prthreebout):
+        if "pr_result" in out:
+            return orig(energy, pressc, energf, pressf, energabs, energthreeb, prthreebout)
+        snapshot(common, mods, out, "pr_")
+        out["pr_scal"] = np.array([common.epsr16.npt1, common.molecom.simt, common.clustercom.volume], f32)
+        r = orig(energy, pressc, energf, pressf, energabs, energthreeb, prthreebout)
+        out["pr_result"] = np.array([r[0], r[1]], f32)
+        return r
+    return wrapped
+
+
 def intra_snapshot(common, out, q):
     """The intramolecular model en_change_intra reads (molecom bond lists, masses, the intra
     reference potential), as the drop-in hands it to the device."""
@@ -211,6 +264,10 @@ def main():
         return r
 
     molfit.molfit = wrapped
+    am = mods["ato_manipulation_rev4"]
+    orig_atogen, orig_press = am.atogen, am.press
+    am.atogen = capture_atogen(common, mods, out, orig_atogen)
+    am.press = capture_press(common, mods, out, orig_press)
     cwd = os.getcwd()
     os.chdir(run)
     try:
@@ -220,6 +277,7 @@ def main():
     finally:
         os.chdir(cwd)
         molfit.molfit = orig
+        am.atogen, am.press = orig_atogen, orig_press
         shutil.rmtree(work, ignore_errors=True)
     if state["taken"] < len(CAPTURE):
         raise SystemExit("the run ended before molfit call %d" % CAPTURE[-1])

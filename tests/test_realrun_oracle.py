@@ -6,8 +6,9 @@ tested with the intermolecular change, molfit.py:124-267), its second (a whole-m
 cycle, :268-448) and its sixth (a whole-molecule cycle with the internal rotations of the
 methyl groups, :295-360, after the first potential refinement) replayed from the state the
 loop held at each call, bit for bit -- coordinates, stored energies, step sizes, counters,
-fadds/faddbs and the ran1 stream; and the pair store the loop's fmolec1 had just built before
-each of them, with its ftest and ftestb."""
+fadds/faddbs and the ran1 stream; the pair store the loop's fmolec1 had just built before
+each of them, with its ftest and ftestb; and the refinement's first atogen (histograms, potex,
+the ran1 stream) and press (energy and pressure) between the fifth and sixth calls."""
 
 import os
 
@@ -22,18 +23,27 @@ f32 = np.float32
 PATH = os.path.join(GOLDEN, "realrun.npz")
 
 
-def _call(z, q):
-    """The box, store, cells, MC parameters and intramolecular model of captured call q."""
+def _box(z, q):
     kw = {}
     for k in BoxArrays.__dataclass_fields__:
         v = z[q + "box_" + k]
         kw[k] = v if v.ndim else v.item()
-    box = BoxArrays(**kw)
+    return BoxArrays(**kw)
+
+
+def _store(z, q):
     M, n = int(z[q + "st_nnbrefmax"]), int(z[q + "st_nergpair"])
-    st = dict(nnbrefmax=M, nergpair=n, nergpairm=np.array(z[q + "st_nergpairm"], np.int32),
-              molergpair=np.ascontiguousarray(z[q + "st_molergpair"], np.int32).reshape(-1),
-              ergpairref=np.ascontiguousarray(z[q + "st_ergpairref"], np.int32).reshape(-1),
-              ergpair=np.array(z[q + "st_ergpair"], f32))
+    return dict(nnbrefmax=M, nergpair=n, nergpairm=np.array(z[q + "st_nergpairm"], np.int32),
+                molergpair=np.ascontiguousarray(z[q + "st_molergpair"], np.int32).reshape(-1),
+                ergpairref=np.ascontiguousarray(z[q + "st_ergpairref"], np.int32).reshape(-1),
+                ergpair=np.array(z[q + "st_ergpair"], f32))
+
+
+def _call(z, q):
+    """The box, store, cells, MC parameters and intramolecular model of captured call q."""
+    box = _box(z, q)
+    st = _store(z, q)
+    M = st["nnbrefmax"]
     cells = oracle.cells_from_arrays(z[q + "cl_dims"], z[q + "cl_cell_start"], z[q + "cl_cell_mols"],
                                      z[q + "cl_molcellno"], z[q + "cl_offsets"], M)
     par = z[q + "par"]
@@ -137,3 +147,33 @@ def test_realrun_pair_store_oracle_matches_reference(q):
         assert np.array_equal(got[k][used], st[k].reshape(-1, M)[used]), k
     assert_bits_equal(got["ergpair"][: st["nergpair"]], st["ergpair"], q + "ergpair")
     assert_bits_equal(np.array([got["ftest"], got["ftestb"]], f32), z[q + "args"], q + "ftest, ftestb")
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_atogen_oracle_matches_reference():
+    """The refinement's atogen (ato_manipulation_rev4.py:3640) as the loop called it: the
+    intra- and intermolecular histograms, potex, the returned count and the ran1 stream."""
+    z = np.load(PATH)
+    box = _box(z, "ag_")
+    wav, potex, n, ran1 = oracle.atogen(box, int(z["ag_ngrsamples"]), Ran1State.from_golden(z, "ag_ran1_before_"),
+                                        z["ag_rminex"], z["ag_ycoh"], f32(z["ag_sizefactor"]))
+    ref = z["ag_wav"]
+    npt1 = ref.shape[1]
+    assert_bits_equal(wav[:, :, 1:npt1 + 1].transpose(0, 2, 1), ref, "wav")
+    assert_bits_equal(potex, z["ag_potex"], "potex")
+    assert n == int(z["ag_result"])
+    assert (ran1.idum, ran1.iy, ran1.mcall) == (int(z["ag_ran1_after_idum"]), int(z["ag_ran1_after_iy"]),
+                                                 int(z["ag_ran1_after_mcall"]))
+    assert np.array_equal(ran1.iv, z["ag_ran1_after_iv"])
+    assert float(np.abs(ref[1]).sum()) > 0
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_press_oracle_matches_reference():
+    """The refinement's press (ato_manipulation_rev4.py:3903) as the loop called it, on the
+    store the loop held: the energy per molecule and the pressure it returned."""
+    z = np.load(PATH)
+    box, st = _box(z, "pr_"), _store(z, "pr_")
+    npt1, simt, volume = z["pr_scal"]
+    r = oracle.press(box, st, int(npt1), f32(simt), f32(volume))
+    assert_bits_equal(np.array([r["energy"], r["pressc"]], f32), z["pr_result"], "energy, pressure")
