@@ -17,10 +17,10 @@ reads is written before it and everything it changes after it (every array copie
 COMMON arrays being updated in place): the box as the COMMON blocks hold it (read by the
 drop-in's own box_from_common), the cell list as the loop built it, the pair store, the step
 arrays and counters, the rotational groups and the intramolecular model, the ran1 state, the
-call's arguments and results, and the cosines molfit drew.  The refinement's first atogen and
-press calls are captured the same way.  The run is stopped after the sixth molfit call.
+call's arguments and results, and the cosines molfit drew.  The refinement's first atogen,
+press and fit_expansion calls and its generate_ep call are captured the same way.  The run is stopped after the sixth molfit call.
 tests/golden/realrun.npz receives the molfit calls under the prefixes k0_, k1_, k2_ and the
-atogen and press calls under ag_ and pr_.
+atogen, press, fit_expansion and generate_ep calls under ag_, pr_, fx_ and ge_.
 """
 
 from __future__ import annotations
@@ -168,6 +168,75 @@ def capture_press(common, mods, out, orig):
     return wrapped
 
 
+def capture_fit(common, out, orig):
+    """The refinement's first fit_expansion call (epsr_standalone_rev3.py:4806, from ptgnsq
+    :3936) under prefix fx_: yin, expr, wtold, the scalars stepr/acceptr/rejrat/chisqnew and
+    the integer arguments with the ran1 state before; wt, wtold, yout, the four returned
+    scalars and the ran1 state after."""
+    def wrapped(yin, expr, yout, wt, wtold, stepr, acceptr, rejrat, chisqnew, nmin, npt, ncfirst, nterms, nits,
+                nfreq):
+        if "fx_result" in out:
+            return orig(yin, expr, yout, wt, wtold, stepr, acceptr, rejrat, chisqnew, nmin, npt, ncfirst, nterms,
+                        nits, nfreq)
+        out["fx_yin"] = np.array(yin[: npt + 1], f32)
+        out["fx_expr"] = np.array(expr[: npt * nterms + 1], f32)
+        out["fx_wtold_in"] = np.array(wtold[: nterms + 1], f32)
+        out["fx_scal_in"] = np.array([stepr, acceptr, rejrat, chisqnew], f32)
+        out["fx_int"] = np.array([nmin, npt, ncfirst, nterms, nits, nfreq], np.int32)
+        for k, v in refstate.ran1_state().items():
+            out["fx_ran1_before_" + k] = v
+        r = orig(yin, expr, yout, wt, wtold, stepr, acceptr, rejrat, chisqnew, nmin, npt, ncfirst, nterms, nits,
+                 nfreq)
+        out["fx_wt"] = np.array(wt[: nterms + 1], f32)
+        out["fx_wtold"] = np.array(wtold[: nterms + 1], f32)
+        out["fx_yout"] = np.array(yout[: npt + 1], f32)
+        out["fx_result"] = np.array(r, f32)
+        for k, v in refstate.ran1_state().items():
+            out["fx_ran1_after_" + k] = v
+        return r
+    return wrapped
+
+
+GE_TABLES = ("xavs", "xavs1", "xavtot", "xavtot1")
+
+
+def capture_generate_ep(common, out, orig):
+    """The refinement's generate_ep call (epsr_standalone_rev3.py:5876, from ptgnsq :4014, the
+    program's second) under prefix ge_: the coefficients, weights, grid, tables and scalars it
+    reads before; the tables, coefficients, weights, potfac and the basis expgr it wrote after."""
+    calls = [0]
+
+    def wrapped(changepotfac):
+        calls[0] += 1
+        if calls[0] != 2:
+            return orig(changepotfac)
+        pp, e16, mc = common.potential_par, common.epsr16, common.molecom
+        npt, npt2, nterms = int(e16.npt), int(e16.npt2), int(pp.ncoeffp)
+        npairs, nsets = int(mc.npairs), int(pp.npairspcof)
+        ld = npt + 1
+        tab = lambda a: np.ascontiguousarray(np.asarray(a)[:ld, 1:npairs + 1].T, f32)  # noqa: E731
+        out["ge_int"] = np.array([npt, npt2, nterms, int(bool(changepotfac))], np.int32)
+        out["ge_iref"] = np.array(pp.irefpcof[1:npairs + 1], np.int32) - 1
+        out["ge_pcoefp_in"] = np.ascontiguousarray(np.asarray(pp.pcoefp)[: nterms + 1, 1:nsets + 1].T, f32)
+        out["ge_pwtold_in"] = np.array(pp.pwtold[: nterms + 1], f32)
+        out["ge_scal"] = np.array([common.clustercom.dmax, pp.absolute_energy, pp.erequnit, pp.ereqstep,
+                                   pp.potfacamp, pp.potfac], f32)
+        out["ge_xstar"] = np.array(e16.xstar[:ld], f32)
+        out["ge_wfac"] = np.array(pp.wfac[:ld], f32)
+        out["ge_ecoul"] = tab(pp.ecoul)
+        for k in GE_TABLES:
+            out["ge_" + k + "_in"] = tab(getattr(pp, k))
+        r = orig(changepotfac)
+        for k in GE_TABLES:
+            out["ge_" + k] = tab(getattr(pp, k))
+        out["ge_pcoefp"] = np.ascontiguousarray(np.asarray(pp.pcoefp)[: nterms + 1, 1:nsets + 1].T, f32)
+        out["ge_pwtold"] = np.array(pp.pwtold[: nterms + 1], f32)
+        out["ge_potfac"] = f32(pp.potfac)
+        out["ge_expgr"] = np.array(pp.expgr[1: npt2 * nterms + 1], f32)
+        return r
+    return wrapped
+
+
 def intra_snapshot(common, out, q):
     """The intramolecular model en_change_intra reads (molecom bond lists, masses, the intra
     reference potential), as the drop-in hands it to the device."""
@@ -218,7 +287,7 @@ def main():
     run = os.path.join(work, "EPSR-test")
     shutil.copytree(src, run)
     prepare_run(run)
-    common, _ = refstate.load_reference(os.path.join(REF, "src"))
+    common, program = refstate.load_reference(os.path.join(REF, "src"))
     import importlib
     mods = {"cellneighbourlist": importlib.import_module("epsr26.library.cellneighbourlist"),
             "ato_manipulation_rev4": importlib.import_module("epsr26.library.ato_manipulation_rev4"),
@@ -268,6 +337,9 @@ def main():
     orig_atogen, orig_press = am.atogen, am.press
     am.atogen = capture_atogen(common, mods, out, orig_atogen)
     am.press = capture_press(common, mods, out, orig_press)
+    orig_fit, orig_ge = program.fit_expansion, program.generate_ep
+    program.fit_expansion = capture_fit(common, out, orig_fit)
+    program.generate_ep = capture_generate_ep(common, out, orig_ge)
     cwd = os.getcwd()
     os.chdir(run)
     try:
@@ -278,6 +350,7 @@ def main():
         os.chdir(cwd)
         molfit.molfit = orig
         am.atogen, am.press = orig_atogen, orig_press
+        program.fit_expansion, program.generate_ep = orig_fit, orig_ge
         shutil.rmtree(work, ignore_errors=True)
     if state["taken"] < len(CAPTURE):
         raise SystemExit("the run ended before molfit call %d" % CAPTURE[-1])

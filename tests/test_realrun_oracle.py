@@ -7,8 +7,10 @@ cycle, :268-448) and its sixth (a whole-molecule cycle with the internal rotatio
 methyl groups, :295-360, after the first potential refinement) replayed from the state the
 loop held at each call, bit for bit -- coordinates, stored energies, step sizes, counters,
 fadds/faddbs and the ran1 stream; the pair store the loop's fmolec1 had just built before
-each of them, with its ftest and ftestb; and the refinement's first atogen (histograms, potex,
-the ran1 stream) and press (energy and pressure) between the fifth and sixth calls."""
+each of them, with its ftest and ftestb; and the refinement between the fifth and sixth calls:
+its first atogen (histograms, potex, the ran1 stream), press (energy and pressure),
+fit_expansion (coefficients, fitted curve, step, rates, chi^2, the ran1 stream) and the
+generate_ep on the fitted coefficients (tables, coefficients, weights, potfac)."""
 
 import os
 
@@ -177,3 +179,45 @@ def test_realrun_press_oracle_matches_reference():
     npt1, simt, volume = z["pr_scal"]
     r = oracle.press(box, st, int(npt1), f32(simt), f32(volume))
     assert_bits_equal(np.array([r["energy"], r["pressc"]], f32), z["pr_result"], "energy, pressure")
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_fit_expansion_oracle_matches_reference():
+    """The refinement's first fit_expansion (epsr_standalone_rev3.py:4806, from ptgnsq :3936) as
+    the loop called it: coefficients, the fitted curve, step, acceptance, rejection ratio, chi^2
+    and the ran1 stream."""
+    z = np.load(PATH)
+    nmin, npt, ncfirst, nterms, nits, nfreq = (int(v) for v in z["fx_int"])
+    stepr, acceptr, rejrat, chisqnew = (f32(v) for v in z["fx_scal_in"])
+    res, ran1 = oracle.fit_expansion(z["fx_yin"], z["fx_expr"], z["fx_wtold_in"], stepr, nmin, npt, ncfirst, nterms,
+                                     nits, nfreq, Ran1State.from_golden(z, "fx_ran1_before_"), acceptr=acceptr,
+                                     rejrat=rejrat, chisqnew=chisqnew)
+    for k in ("wt", "wtold"):
+        assert_bits_equal(res[k][1:], z["fx_" + k][1:], k)
+    assert_bits_equal(res["yout"][1:], z["fx_yout"][1:], "yout")
+    assert_bits_equal(np.array([res["stepr"], res["acceptr"], res["rejrat"], res["chisq"]], f32), z["fx_result"],
+                      "stepr, acceptr, rejrat, chisq")
+    assert (ran1.idum, ran1.iy, ran1.mcall) == (int(z["fx_ran1_after_idum"]), int(z["fx_ran1_after_iy"]),
+                                                 int(z["fx_ran1_after_mcall"]))
+    assert np.array_equal(ran1.iv, z["fx_ran1_after_iv"])
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_generate_ep_oracle_matches_reference():
+    """The refinement's generate_ep (epsr_standalone_rev3.py:5876, from ptgnsq :4014) on the
+    coefficients the fits produced, from the basis the reference built: the four tables, the
+    scaled coefficients, the weights and potfac."""
+    z = np.load(PATH)
+    npt, npt2, nterms, change = (int(v) for v in z["ge_int"])
+    dmax, absolute_energy, erequnit, ereqstep, potfacamp, potfac = (f32(v) for v in z["ge_scal"])
+    tabs = {k: z["ge_" + k + "_in"] for k in ("xavs", "xavs1", "xavtot", "xavtot1")}
+    out, pc, pw, pf, _, _ = oracle.generate_ep(npt, npt2, nterms, z["ge_expgr"], z["ge_pcoefp_in"], z["ge_iref"], dmax,
+                                               z["ge_xstar"], z["ge_wfac"], z["ge_ecoul"], tabs, z["ge_pwtold_in"],
+                                               np.array([absolute_energy, erequnit, ereqstep, potfacamp], f32),
+                                               potfac, bool(change))
+    for k in tabs:
+        assert_bits_equal(out[k], z["ge_" + k], k)
+    assert_bits_equal(pc[:, : nterms + 1], z["ge_pcoefp"], "pcoefp")
+    assert_bits_equal(pw, z["ge_pwtold"], "pwtold")
+    assert_bits_equal(np.array([pf], f32), np.array([z["ge_potfac"]], f32), "potfac")
+    assert float(np.abs(z["ge_pcoefp_in"][:, 2:]).max()) > 0      # the fits moved the coefficients
