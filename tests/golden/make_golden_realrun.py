@@ -18,9 +18,11 @@ COMMON arrays being updated in place): the box as the COMMON blocks hold it (rea
 drop-in's own box_from_common), the cell list as the loop built it, the pair store, the step
 arrays and counters, the rotational groups and the intramolecular model, the ran1 state, the
 call's arguments and results, and the cosines molfit drew.  The refinement's first atogen,
-press and fit_expansion calls and its generate_ep call are captured the same way.  The run is stopped after the sixth molfit call.
+press and fit_expansion calls, its running sums and its generate_ep call are captured the
+same way.  The run is stopped after the sixth molfit call.
 tests/golden/realrun.npz receives the molfit calls under the prefixes k0_, k1_, k2_ and the
-atogen, press, fit_expansion and generate_ep calls under ag_, pr_, fx_ and ge_.
+atogen, press, fit_expansion, sumsq, sumgr and generate_ep calls under ag_, pr_, fx_, ss_,
+sg_ and ge_.
 """
 
 from __future__ import annotations
@@ -197,6 +199,47 @@ def capture_fit(common, out, orig):
     return wrapped
 
 
+GR_ARRAYS = ("gorintra", "gorinter", "gr2intra", "gr2inter", "entsig")
+SQ_ARRAYS = ("soqintra", "soqinter", "sq2intra", "sq2inter")
+
+
+def capture_sums(common, out, orig_gr, orig_sq):
+    """The refinement's sumsq and sumgr calls (epsr_standalone_rev3.py:3642 / :3578, from
+    :1637 / :1642) under prefixes ss_ and sg_: the running means and error bars of epsr16 before
+    and after ((npairs, points) each), the sample (qwind or wav, (2, npairs, points)), ycoh,
+    the real*8 weights fc1, fc2 and the point count."""
+    def rows(name, n):
+        npairs = int(common.molecom.npairs)
+        return np.ascontiguousarray(np.asarray(getattr(common.epsr16, name))[: n + 1, 1:npairs + 1].T, f32)
+
+    def sample(a, n):
+        npairs = int(common.molecom.npairs)
+        return np.ascontiguousarray(np.asarray(a)[1:3, : n + 1, 1:npairs + 1].transpose(0, 2, 1), f32)
+
+    def take(q, names, n, a, call):
+        out[q + "n"] = np.int32(n)
+        out[q + "fc"] = np.array([common.sumvalues.fc1, common.sumvalues.fc2], np.float64)
+        out[q + "sample"] = sample(a, n)
+        out[q + "ycoh"] = np.array(common.epsr16.ycoh[: n + 1], f32)
+        for k in names:
+            out[q + k + "_in"] = rows(k, n)
+        r = call()
+        for k in names:
+            out[q + k] = rows(k, n)
+        return r
+
+    def gr(nz, wav):
+        if "sg_n" in out:
+            return orig_gr(nz, wav)
+        return take("sg_", GR_ARRAYS, int(nz), wav, lambda: orig_gr(nz, wav))
+
+    def sq(nq, qwind):
+        if "ss_n" in out:
+            return orig_sq(nq, qwind)
+        return take("ss_", SQ_ARRAYS, int(nq), qwind, lambda: orig_sq(nq, qwind))
+    return gr, sq
+
+
 GE_TABLES = ("xavs", "xavs1", "xavtot", "xavtot1")
 
 
@@ -340,6 +383,8 @@ def main():
     orig_fit, orig_ge = program.fit_expansion, program.generate_ep
     program.fit_expansion = capture_fit(common, out, orig_fit)
     program.generate_ep = capture_generate_ep(common, out, orig_ge)
+    orig_gr, orig_sq = program.sumgr, program.sumsq
+    program.sumgr, program.sumsq = capture_sums(common, out, orig_gr, orig_sq)
     cwd = os.getcwd()
     os.chdir(run)
     try:
@@ -351,6 +396,7 @@ def main():
         molfit.molfit = orig
         am.atogen, am.press = orig_atogen, orig_press
         program.fit_expansion, program.generate_ep = orig_fit, orig_ge
+        program.sumgr, program.sumsq = orig_gr, orig_sq
         shutil.rmtree(work, ignore_errors=True)
     if state["taken"] < len(CAPTURE):
         raise SystemExit("the run ended before molfit call %d" % CAPTURE[-1])

@@ -8,9 +8,10 @@ methyl groups, :295-360, after the first potential refinement) replayed from the
 loop held at each call, bit for bit -- coordinates, stored energies, step sizes, counters,
 fadds/faddbs and the ran1 stream; the pair store the loop's fmolec1 had just built before
 each of them, with its ftest and ftestb; and the refinement between the fifth and sixth calls:
-its first atogen (histograms, potex, the ran1 stream), press (energy and pressure),
-fit_expansion (coefficients, fitted curve, step, rates, chi^2, the ran1 stream) and the
-generate_ep on the fitted coefficients (tables, coefficients, weights, potfac)."""
+its first atogen (histograms, potex, the ran1 stream), press (energy and pressure), the
+running sums sumsq and sumgr, fit_expansion (coefficients, fitted curve, step, rates, chi^2,
+the ran1 stream) and the generate_ep on the fitted coefficients (tables, coefficients,
+weights, potfac)."""
 
 import os
 
@@ -221,3 +222,23 @@ def test_realrun_generate_ep_oracle_matches_reference():
     assert_bits_equal(pw, z["ge_pwtold"], "pwtold")
     assert_bits_equal(np.array([pf], f32), np.array([z["ge_potfac"]], f32), "potfac")
     assert float(np.abs(z["ge_pcoefp_in"][:, 2:]).max()) > 0      # the fits moved the coefficients
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+@pytest.mark.parametrize("q", ["sg_", "ss_"])
+def test_realrun_running_sums_oracle_match_reference(q):
+    """The refinement's sumgr and sumsq (epsr_standalone_rev3.py:3578 / :3642) on the loop's
+    running means and error bars (accumulated over the run folder's earlier iterations) with the
+    real*8 weights fc1, fc2: every updated point, bit for bit."""
+    z = np.load(PATH)
+    n = int(z[q + "n"])
+    fc1, fc2 = (float(v) for v in z[q + "fc"])
+    if q == "sg_":
+        names = ("gorintra", "gorinter", "gr2intra", "gr2inter", "entsig")
+        got = oracle.sumgr(n, z[q + "sample"], z[q + "ycoh"], fc1, fc2, {k: z[q + k + "_in"] for k in names})
+    else:
+        names = ("soqintra", "soqinter", "sq2intra", "sq2inter")
+        got = oracle.sumsq(n, z[q + "sample"], fc1, fc2, {k: z[q + k + "_in"] for k in names})
+    for k in names:
+        assert_bits_equal(got[k][:, 1:], z[q + k][:, 1:], q + k)
+    assert any(not np.array_equal(z[q + k + "_in"], z[q + k]) for k in names)
