@@ -19,10 +19,10 @@ drop-in's own box_from_common), the cell list as the loop built it, the pair sto
 arrays and counters, the rotational groups and the intramolecular model, the ran1 state, the
 call's arguments and results, and the cosines molfit drew.  The refinement's first atogen,
 press and fit_expansion calls, its running sums and its generate_ep call are captured the
-same way.  The run is stopped after the sixth molfit call.
+same way, and its gensq at every 20th Q point.  The run is stopped after the sixth molfit call.
 tests/golden/realrun.npz receives the molfit calls under the prefixes k0_, k1_, k2_ and the
-atogen, press, fit_expansion, sumsq, sumgr and generate_ep calls under ag_, pr_, fx_, ss_,
-sg_ and ge_.
+atogen, press, gensq, fit_expansion, sumsq, sumgr and generate_ep calls under ag_, pr_, gs_,
+fx_, ss_, sg_ and ge_.
 """
 
 from __future__ import annotations
@@ -240,6 +240,33 @@ def capture_sums(common, out, orig_gr, orig_sq):
     return gr, sq
 
 
+GS_EVERY = 20
+
+
+def capture_gensq(common, out, orig):
+    """The refinement's gensq (epsr_standalone_rev3.py:4731, from :1400) under prefix gs_: wav,
+    ycoh, n2extr and natomsphere before; and, at every GS_EVERY-th Q point (each point of S(Q)
+    depends only on its own column of the sine-transform table), the columns of foqols and the
+    intra- and intermolecular S(Q) it wrote."""
+    def wrapped(nq, q, sofq, wav):
+        if "gs_sel" in out:
+            return orig(nq, q, sofq, wav)
+        e16, mc = common.epsr16, common.molecom
+        npairs, npt1, ntype = int(mc.npairs), int(e16.npt1), int(mc.ntype)
+        sel = np.arange(1, int(nq) + 1, GS_EVERY, dtype=np.int32)
+        out["gs_sel"] = sel
+        out["gs_npt1"] = np.int32(npt1)
+        out["gs_wav"] = np.ascontiguousarray(np.asarray(wav)[1:3, : npt1 + 1, 1:npairs + 1].transpose(0, 2, 1), f32)
+        out["gs_ycoh"] = np.array(e16.ycoh[: npt1 + 1], f32)
+        out["gs_n2extr"] = np.array(mc.n2extr[1:npairs + 1], np.int32) - 1
+        out["gs_natomsphere"] = np.array(common.molecom_mod.natomsphere[1:ntype + 1], f32)
+        out["gs_foqols"] = np.ascontiguousarray(np.asarray(e16.foqols)[: npt1 + 1, sel].T, f32)
+        r = orig(nq, q, sofq, wav)
+        out["gs_sofq"] = np.ascontiguousarray(np.asarray(sofq)[1:3, sel, 1:npairs + 1].transpose(0, 2, 1), f32)
+        return r
+    return wrapped
+
+
 GE_TABLES = ("xavs", "xavs1", "xavtot", "xavtot1")
 
 
@@ -383,6 +410,8 @@ def main():
     orig_fit, orig_ge = program.fit_expansion, program.generate_ep
     program.fit_expansion = capture_fit(common, out, orig_fit)
     program.generate_ep = capture_generate_ep(common, out, orig_ge)
+    orig_gs = program.gensq
+    program.gensq = capture_gensq(common, out, orig_gs)
     orig_gr, orig_sq = program.sumgr, program.sumsq
     program.sumgr, program.sumsq = capture_sums(common, out, orig_gr, orig_sq)
     cwd = os.getcwd()
@@ -397,6 +426,7 @@ def main():
         am.atogen, am.press = orig_atogen, orig_press
         program.fit_expansion, program.generate_ep = orig_fit, orig_ge
         program.sumgr, program.sumsq = orig_gr, orig_sq
+        program.gensq = orig_gs
         shutil.rmtree(work, ignore_errors=True)
     if state["taken"] < len(CAPTURE):
         raise SystemExit("the run ended before molfit call %d" % CAPTURE[-1])

@@ -18,7 +18,7 @@ whole-molecule cycle with the methyl rotations) the COMMON state is captured as
 tests/golden/make_golden_realrun.py captured it from the unmodified loop, and every array must
 equal tests/golden/realrun.npz bit for bit: the box, the cell list and pair store the drop-in wrote, the step arrays, counters,
 ran1 state, fadds/faddbs, and the coordinates and energies after each call.  The
-refinement's atogen, press, sumsq, sumgr, fit_expansion and generate_ep calls, as installed,
+refinement's atogen, press, gensq, sumsq, sumgr, fit_expansion and generate_ep calls, as installed,
 are captured the same way and must equal the reference's calls.  Only the scratch slot
 ergold(1) is left out (the drop-in does not fill the reference's en_change work arrays).
 
@@ -121,12 +121,13 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
     # the refinement's routines, as installed, captured as the fixture captured the reference's
     am, program = mods["ato_manipulation_rev4"], path.mods["program"]
     inst = dict(atogen=am.atogen, press=am.press, fit_expansion=program.fit_expansion,
-                generate_ep=program.generate_ep, sumgr=program.sumgr, sumsq=program.sumsq)
+                generate_ep=program.generate_ep, sumgr=program.sumgr, sumsq=program.sumsq, gensq=program.gensq)
     am.atogen = g.capture_atogen(common, mods, out, inst["atogen"])
     am.press = g.capture_press(common, mods, out, inst["press"])
     program.fit_expansion = g.capture_fit(common, out, inst["fit_expansion"])
     program.generate_ep = g.capture_generate_ep(common, out, inst["generate_ep"])
     program.sumgr, program.sumsq = g.capture_sums(common, out, inst["sumgr"], inst["sumsq"])
+    program.gensq = g.capture_gensq(common, out, inst["gensq"])
     try:
         _run_program(run)
     except _Stop:
@@ -134,7 +135,7 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
     finally:
         mods["molfit"].molfit = installed
         am.atogen, am.press = inst["atogen"], inst["press"]
-        for k in ("fit_expansion", "generate_ep", "sumgr", "sumsq"):
+        for k in ("fit_expansion", "generate_ep", "sumgr", "sumsq", "gensq"):
             setattr(program, k, inst[k])
         path.orig = real
         path.uninstall()

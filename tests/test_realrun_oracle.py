@@ -8,8 +8,8 @@ methyl groups, :295-360, after the first potential refinement) replayed from the
 loop held at each call, bit for bit -- coordinates, stored energies, step sizes, counters,
 fadds/faddbs and the ran1 stream; the pair store the loop's fmolec1 had just built before
 each of them, with its ftest and ftestb; and the refinement between the fifth and sixth calls:
-its first atogen (histograms, potex, the ran1 stream), press (energy and pressure), the
-running sums sumsq and sumgr, fit_expansion (coefficients, fitted curve, step, rates, chi^2,
+its first atogen (histograms, potex, the ran1 stream), press (energy and pressure), gensq
+(at every 20th Q point), the running sums sumsq and sumgr, fit_expansion (coefficients, fitted curve, step, rates, chi^2,
 the ran1 stream) and the generate_ep on the fitted coefficients (tables, coefficients,
 weights, potfac)."""
 
@@ -242,3 +242,18 @@ def test_realrun_running_sums_oracle_match_reference(q):
     for k in names:
         assert_bits_equal(got[k][:, 1:], z[q + k][:, 1:], q + k)
     assert any(not np.array_equal(z[q + k + "_in"], z[q + k]) for k in names)
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_gensq_oracle_matches_reference():
+    """The refinement's gensq (epsr_standalone_rev3.py:4731) on the histograms atogen had just
+    made, at every 20th Q point of the run's grid (each point reads only its own column of the
+    sine-transform table): intra- and intermolecular S(Q), bit for bit."""
+    z = np.load(PATH)
+    cols = z["gs_foqols"]
+    rows = np.zeros((cols.shape[0] + 1, cols.shape[1]), f32)
+    rows[1:] = cols
+    got = oracle.gensq(cols.shape[0], int(z["gs_npt1"]), z["gs_wav"], rows, z["gs_ycoh"], z["gs_n2extr"],
+                       z["gs_natomsphere"])
+    assert_bits_equal(got[:, :, 1:], z["gs_sofq"], "sofq")
+    assert float(np.abs(z["gs_sofq"][1]).max()) > 0
