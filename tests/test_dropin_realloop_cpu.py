@@ -24,7 +24,8 @@ ergold(1) is left out (the drop-in does not fill the reference's en_change work 
 
 A second run takes the shipped input file unchanged to its end (one iteration, then the final
 output section with its four stog calls) and compares every file left in the run folder with
-the unmodified run's (tests/golden/realrun_files.json, digests of the normalised bytes).
+the unmodified run's (tests/golden/realrun_files.json, digests of the normalised bytes); its
+first stog call, as installed, must equal the reference's (tests/golden/realrun_stog.npz).
 
 Needs the reference checkout (EPSR_REFERENCE, the directory holding src/epsr26 and
 EPSR-test); skipped without it.  About twenty seconds of CPU."""
@@ -148,13 +149,17 @@ def _run_program_with_dropin(tmp_path, monkeypatch):
     import make_golden_realrun_files as gf
 
     path, real, journal, run = _install(tmp_path, monkeypatch)
+    am = importlib.import_module("epsr26.library.ato_manipulation_rev4")
+    stog, st = am.stog, {}
+    am.stog = gf.capture_stog(st, stog)
     try:
         rc = _run_program(run)
     finally:
+        am.stog = stog
         path.orig = real
         path.uninstall()
     assert rc in (0, None)
-    return gf.output_digests(str(run)), journal
+    return gf.output_digests(str(run)), journal, st
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="needs the reference checkout (EPSR_REFERENCE)")
@@ -197,14 +202,21 @@ def test_dropin_in_the_reference_loop_writes_the_unmodified_runs_files(tmp_path,
     columns excepted."""
     with open(os.path.join(GOLDEN, "realrun_files.json")) as f:
         want = json.load(f)
-    got, calls = _run_program_with_dropin(tmp_path, monkeypatch)
+    got, calls, st = _run_program_with_dropin(tmp_path, monkeypatch)
     assert sorted(got) == sorted(want)
     bad = [k for k in want if got[k] != want[k]]
     assert not bad, bad
     for k in ("200DMSO400Water.EPSR.erg", "200DMSO400Water.EPSR.g01", "200DMSO400Water.EPSR.f01",
               "200DMSO400Water.pcof", "200DMSO400Water.ato"):
         assert k in want
-    # the output section's four transforms ran through the drop-in too
+    # the output section's four transforms ran through the drop-in too; the first as the reference's
+    z = np.load(os.path.join(GOLDEN, "realrun_stog.npz"))
+    assert sorted(st) == sorted(z.files)
+    for k in z.files:
+        if z[k].dtype.kind == "f":
+            assert_bits_equal(st[k], z[k], k)
+        else:
+            assert np.array_equal(st[k], z[k]), k
     assert calls.count("stog") == 4 and calls.count("molfit") == 4 and calls.count("molfit_shake") == 1, calls
 
 

@@ -257,3 +257,17 @@ def test_realrun_gensq_oracle_matches_reference():
                        z["gs_natomsphere"])
     assert_bits_equal(got[:, :, 1:], z["gs_sofq"], "sofq")
     assert float(np.abs(z["gs_sofq"][1]).max()) > 0
+
+
+STOG_PATH = os.path.join(GOLDEN, "realrun_stog.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(STOG_PATH), reason="fixture absent")
+def test_realrun_stog_oracle_matches_reference():
+    """The final output section's first stog (ato_manipulation_rev4.py:4067, from
+    epsr_standalone_rev3.py:2195) on the fits to the run's three data sets, captured by
+    tests/golden/make_golden_realrun_files.py: g(r) of every set at every r point."""
+    z = np.load(STOG_PATH)
+    got = oracle.stog(f32(z["st_rho"]), z["st_q"], z["st_sofq"], z["st_r"], z["st_nqmin"], z["st_nqmax"], z["st_xwt"])
+    assert_bits_equal(got[:, 1:], z["st_gofr"], "gofr")
+    assert float(np.abs(z["st_gofr"]).max()) > 0
