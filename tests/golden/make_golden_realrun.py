@@ -17,7 +17,8 @@ reads is written before it and everything it changes after it (every array copie
 COMMON arrays being updated in place): the box as the COMMON blocks hold it (read by the
 drop-in's own box_from_common), the cell list as the loop built it, the pair store, the step
 arrays and counters, the rotational groups and the intramolecular model, the ran1 state, the
-call's arguments and results, and the cosines molfit drew.  The refinement's first atogen,
+call's arguments and results, and the cosines molfit drew.  The loop's first cell list
+(prefix cl0_) and the refinement's first atogen,
 press and fit_expansion calls, its running sums and its generate_ep call are captured the
 same way, and its gensq at every 20th Q point.  The run is stopped after the sixth molfit call.
 tests/golden/realrun.npz receives the molfit calls under the prefixes k0_, k1_, k2_ and the
@@ -128,6 +129,33 @@ def box_snapshot(common, mods, out, q):
         out[q + "box_" + k] = v.copy() if isinstance(v, np.ndarray) else np.array(v)
     for k, v in refstate.ran1_state().items():
         out[q + "ran1_before_" + k] = v
+
+
+def capture_cells(common, mods, out, orig):
+    """The loop's first initialise_cellneighbourlist call (cellneighbourlist.py:23, from
+    epsr_standalone_rev3.py:1265) under prefix cl0_: the box, nmolcellin and rmax before; the
+    cell list it left in the COMMON block after (as snapshot's cl_ arrays)."""
+    def wrapped(nmolcellin, xadd, yadd, zadd, nmol, rmax):
+        if "cl0_rmax" in out:
+            return orig(nmolcellin, xadd, yadd, zadd, nmol, rmax)
+        box_snapshot(common, mods, out, "cl0_")
+        out["cl0_nmolcellin"] = np.int32(nmolcellin)
+        out["cl0_rmax"] = f32(rmax)
+        r = orig(nmolcellin, xadd, yadd, zadd, nmol, rmax)
+        cnl = common.cellneighbourlist
+        ncell = int(cnl.ncell)
+        n_in = np.array(cnl.nmolsincell[1:ncell + 1], np.int32)
+        out["cl0_dims"] = np.array([cnl.ncelldiva, cnl.ncelldivb, cnl.ncelldivc, ncell, cnl.ncellneighb,
+                                    cnl.maxcellno], np.int32)
+        out["cl0_cell_start"] = np.concatenate([[0], np.cumsum(n_in)]).astype(np.int32)
+        out["cl0_cell_mols"] = np.concatenate([np.array(cnl.molsincell[1:n_in[c] + 1, c + 1], np.int32) - 1
+                                               for c in range(ncell)]).astype(np.int32)
+        out["cl0_molcellno"] = np.array(cnl.molcellno[1:int(nmol) + 1], np.int32)
+        nb = int(cnl.ncellneighb)
+        out["cl0_offsets"] = np.stack([np.array(getattr(cnl, k)[1:nb + 1], np.int32)
+                                       for k in ("iacellneighb", "ibcellneighb", "iccellneighb")], 1)
+        return r
+    return wrapped
 
 
 def capture_atogen(common, mods, out, orig):
@@ -404,6 +432,9 @@ def main():
 
     molfit.molfit = wrapped
     am = mods["ato_manipulation_rev4"]
+    cn = mods["cellneighbourlist"]
+    orig_cells = cn.initialise_cellneighbourlist
+    cn.initialise_cellneighbourlist = capture_cells(common, mods, out, orig_cells)
     orig_atogen, orig_press = am.atogen, am.press
     am.atogen = capture_atogen(common, mods, out, orig_atogen)
     am.press = capture_press(common, mods, out, orig_press)
@@ -424,6 +455,7 @@ def main():
         os.chdir(cwd)
         molfit.molfit = orig
         am.atogen, am.press = orig_atogen, orig_press
+        cn.initialise_cellneighbourlist = orig_cells
         program.fit_expansion, program.generate_ep = orig_fit, orig_ge
         program.sumgr, program.sumsq = orig_gr, orig_sq
         program.gensq = orig_gs

@@ -18,7 +18,7 @@ whole-molecule cycle with the methyl rotations) the COMMON state is captured as
 tests/golden/make_golden_realrun.py captured it from the unmodified loop, and every array must
 equal tests/golden/realrun.npz bit for bit: the box, the cell list and pair store the drop-in wrote, the step arrays, counters,
 ran1 state, fadds/faddbs, and the coordinates and energies after each call.  The
-refinement's atogen, press, gensq, sumsq, sumgr, fit_expansion and generate_ep calls, as installed,
+loop's first cell list and the refinement's atogen, press, gensq, sumsq, sumgr, fit_expansion and generate_ep calls, as installed,
 are captured the same way and must equal the reference's calls.  Only the scratch slot
 ergold(1) is left out (the drop-in does not fill the reference's en_change work arrays).
 
@@ -120,9 +120,10 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
 
     mods["molfit"].molfit = wrapped
     # the refinement's routines, as installed, captured as the fixture captured the reference's
-    am, program = mods["ato_manipulation_rev4"], path.mods["program"]
-    inst = dict(atogen=am.atogen, press=am.press, fit_expansion=program.fit_expansion,
+    am, program, cn = mods["ato_manipulation_rev4"], path.mods["program"], mods["cellneighbourlist"]
+    inst = dict(cells=cn.initialise_cellneighbourlist, atogen=am.atogen, press=am.press, fit_expansion=program.fit_expansion,
                 generate_ep=program.generate_ep, sumgr=program.sumgr, sumsq=program.sumsq, gensq=program.gensq)
+    cn.initialise_cellneighbourlist = g.capture_cells(common, mods, out, inst["cells"])
     am.atogen = g.capture_atogen(common, mods, out, inst["atogen"])
     am.press = g.capture_press(common, mods, out, inst["press"])
     program.fit_expansion = g.capture_fit(common, out, inst["fit_expansion"])
@@ -136,6 +137,7 @@ def _run_loop_with_dropin(tmp_path, monkeypatch):
     finally:
         mods["molfit"].molfit = installed
         am.atogen, am.press = inst["atogen"], inst["press"]
+        cn.initialise_cellneighbourlist = inst["cells"]
         for k in ("fit_expansion", "generate_ep", "sumgr", "sumsq", "gensq"):
             setattr(program, k, inst[k])
         path.orig = real

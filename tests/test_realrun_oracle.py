@@ -6,7 +6,8 @@ tested with the intermolecular change, molfit.py:124-267), its second (a whole-m
 cycle, :268-448) and its sixth (a whole-molecule cycle with the internal rotations of the
 methyl groups, :295-360, after the first potential refinement) replayed from the state the
 loop held at each call, bit for bit -- coordinates, stored energies, step sizes, counters,
-fadds/faddbs and the ran1 stream; the pair store the loop's fmolec1 had just built before
+fadds/faddbs and the ran1 stream; the loop's first cell list; the pair store the loop's fmolec1
+had just built before
 each of them, with its ftest and ftestb; and the refinement between the fifth and sixth calls:
 its first atogen (histograms, potex, the ran1 stream), press (energy and pressure), gensq
 (at every 20th Q point), the running sums sumsq and sumgr, fit_expansion (coefficients, fitted curve, step, rates, chi^2,
@@ -271,3 +272,23 @@ def test_realrun_stog_oracle_matches_reference():
     got = oracle.stog(f32(z["st_rho"]), z["st_q"], z["st_sofq"], z["st_r"], z["st_nqmin"], z["st_nqmax"], z["st_xwt"])
     assert_bits_equal(got[:, 1:], z["st_gofr"], "gofr")
     assert float(np.abs(z["st_gofr"]).max()) > 0
+
+
+@pytest.mark.skipif(not os.path.exists(PATH), reason="fixture absent")
+def test_realrun_cell_list_oracle_matches_reference():
+    """The loop's first initialise_cellneighbourlist (cellneighbourlist.py:23, from
+    epsr_standalone_rev3.py:1265) with its nmolcellin and sepmax: divisions, cell count,
+    neighbour offsets, the molecules of every cell in the reference's order and each
+    molecule's cell."""
+    z = np.load(PATH)
+    box = _box(z, "cl0_")
+    c = oracle.cell_list(box, int(z["cl0_nmolcellin"]), f32(z["cl0_rmax"]))
+    dims = [c["ncelldiva"], c["ncelldivb"], c["ncelldivc"], c["ncell"], c["ncellneighb"], c["maxcellno"]]
+    assert np.array_equal(np.array(dims, np.int32), z["cl0_dims"])
+    nc, nb = int(c["ncell"]), int(c["ncellneighb"])
+    assert np.array_equal(c["cell_start"][: nc + 1], z["cl0_cell_start"])
+    assert np.array_equal(c["cell_mols"], z["cl0_cell_mols"])
+    assert np.array_equal(c["molcellno"], z["cl0_molcellno"])
+    off = np.stack([c[k][:nb] for k in ("ia_off", "ib_off", "ic_off")], 1)
+    assert np.array_equal(off, z["cl0_offsets"])
+    assert nc > 1
